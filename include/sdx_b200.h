@@ -1,0 +1,206 @@
+/*
+ * sdx_b200.h — C-ABI of the B200 implicit soft-body step (libsdx_b200.so).
+ *
+ * Plain pointers and sizes only. Every entry point returns an int status (SDX_OK == 0); the text of
+ * the last error on the calling thread is available from sdx_last_error(). Handles own their device
+ * buffers; a handle is not re-entrant, distinct handles are independent (one per thread is fine).
+ *
+ * Reference interfaces replaced (paths inside superdex_physics/libraries/mochi/):
+ *   - mochi::LinearSolver<T>::Solve / CudaIterativeSolve
+ *       mochi_core/include/mochi_core/solvers/linear_solver.h:265-271, 321-496, 614-662
+ *     with KrylovSolverParams (mochi_core/include/mochi_core/solvers/krylov_solver.h:43-82) and
+ *     LinearSolverStatus (krylov_solver.h:85-116)                       -> sdx_pcg_solve
+ *   - the FEM-body assembly AssembleObjResDRes + soft::MakeBatchedBodyOp
+ *       mochi_core/include/mochi_core/element_operations/element_assembler.h:230-236,
+ *       mochi_physics/src/mochi_soft.h:314-420, mochi_physics/src/mochi_soft.cpp:202-318
+ *     plus the async contact response mochi_physics/src/mochi_soft.cpp:386-474 -> sdx_assemble
+ *   - the island Newton step solver::StepIslandNewtonAsync / NewtonSolver<T>::Solve
+ *       mochi_physics/src/mochi_solve.cpp:1090, mochi_core/src/solvers/newton_solver.cpp:603-876
+ *                                                                         -> sdx_step
+ *   - Scene state access (displacements / velocities of soft actors)
+ *       mochi_physics/src/mochi_soft.cpp:476-495 (EntityGetSolution)      -> sdx_get/set_state
+ */
+#ifndef SDX_B200_H
+#define SDX_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------------------------- */
+#define SDX_OK 0
+#define SDX_ERR_INVALID_ARGUMENT -1
+#define SDX_ERR_CUDA -2
+#define SDX_ERR_NOT_READY -3      /* call order: bodies must be uploaded first */
+#define SDX_ERR_DEVICE_TIMEOUT -4 /* a bounded device-side wait gave up (grid barrier) */
+#define SDX_ERR_OUT_OF_MEMORY -5
+#define SDX_ERR_UNSUPPORTED -6
+
+/* ---- enums (values match the reference enums where one exists) --------------------------------- */
+/* PreconditionerType subset (mochi_core/.../solvers/linear_solver_params.h) */
+#define SDX_PREC_NONE 0
+#define SDX_PREC_JACOBI 1
+#define SDX_PREC_BLOCK_JACOBI 2
+/* LinearSolverConvergenceStatus (krylov_solver.h:85-116) */
+#define SDX_LINEAR_NONE 0
+#define SDX_LINEAR_CONVERGED 1
+#define SDX_LINEAR_STOPPED 2
+#define SDX_LINEAR_DIVERGED 3
+/* InitialGuessHint (linear_solver.h) */
+#define SDX_GUESS_UNKNOWN 0
+#define SDX_GUESS_ZERO 1
+/* MaterialPsdStrategy (mochi_core/.../materials/material_types.h:52) */
+#define SDX_PSD_NONE 0
+#define SDX_PSD_PROJECTION 1
+#define SDX_PSD_ABS_EIGEN 2
+#define SDX_PSD_FAST 3
+/* value types of host matrices */
+#define SDX_F32 0
+#define SDX_F64 1
+/* collider types (plane, capsule) */
+#define SDX_COLLIDER_PLANE 0
+#define SDX_COLLIDER_CAPSULE 1
+/* assembly flags (AssemblyParams: assemObj / assemRes / assemDRes / psdDRes) */
+#define SDX_ASM_OBJ 1
+#define SDX_ASM_RES 2
+#define SDX_ASM_HESS 4
+#define SDX_ASM_PSD 8
+/* warm start of each Newton linear solve */
+#define SDX_WARM_ZERO 0     /* reference behaviour: dx0 = 0 (newton_solver.cpp:746) */
+#define SDX_WARM_PREVIOUS 1 /* dx0 = the previous solve's dx of the same env */
+#define SDX_WARM_LEARNED 2  /* dx0 = per-vertex MLP prediction (sdx_mlp_*) */
+
+/* Mirrors KrylovSolverParams (krylov_solver.h:43-82). Only the residual-L2 norm is supported. */
+typedef struct {
+  double rel_tol;       /* ||r|| <= max(abs_tol, rel_tol ||b||) */
+  double abs_tol;
+  double rel_div_tol;   /* diverged when ||r|| > rel_div_tol ||b|| */
+  int max_iter;
+  int preconditioner;   /* SDX_PREC_* */
+  int abort_if_not_spd; /* stop with DIVERGED on p.Ap <= 0 */
+  int polak_ribiere;    /* 1: Polak-Ribiere beta (reference default) */
+  int replace_every;    /* FP64 true-residual replacement period in iterations (0: default 32) */
+} sdx_linear_params;
+
+/* Mirrors LinearSolverStatus (krylov_solver.h:85-116). */
+typedef struct {
+  int num_iter;
+  double residual_norm;
+  double relative_residual_norm;
+  int convergence; /* SDX_LINEAR_* */
+} sdx_linear_status;
+
+/* Newton / physics parameters of a step (NonLinearSolverParams, nonlinear_solver_params.h:327-466;
+ * ContactParams, contact_params.h:85-183). */
+typedef struct {
+  double dt;
+  double gravity[3];
+  int psd_strategy;            /* SDX_PSD_* (default projection) */
+  double k_contact;            /* penaltyCoefficient [Pa/m] */
+  double t_half;               /* penaltySmoothingHalfDistance [m] */
+  double thr;                  /* penaltyThresholdDefault [m] */
+  double max_align;            /* maxAlignmentNormals */
+  int newton_max_iter;
+  double newton_rel_tol, newton_abs_tol, newton_rel_step_tol;
+  int ls_max_iter;
+  double ls_alpha;
+  int ew_forcing;              /* 0 constant linear tolerance, 2 Eisenstat-Walker choice 2 */
+  double rel_div_tol, abs_div_tol;
+  int warm_start;              /* SDX_WARM_* */
+  sdx_linear_params linear;
+} sdx_step_params;
+
+/* Per-env statistics of the last step (StageSolverStats, mochi_physics/src/mochi_solve.cpp:1144). */
+typedef struct {
+  int newton_iters;
+  int cg_iters;
+  int ls_iters;
+  int convergence;             /* 1 converged, 2 stopped, 3 diverged */
+  double res_norm0, res_norm;
+  int64_t n_contacts;          /* active (sample, collider) pairs at the last assembly */
+} sdx_env_stats;
+
+typedef struct sdx_context sdx_context;
+
+const char* sdx_last_error(void);
+int sdx_version(void);
+/* Fill `p` with the defaults of this path (reference defaults, Newton to rel 1e-6, CG rel 1e-6). */
+void sdx_default_step_params(sdx_step_params* p);
+void sdx_default_linear_params(sdx_linear_params* p);
+
+/* ---- linear solver boundary (LinearSolver<T>::Solve with solverType CudaCG) -------------------- */
+
+/* Solve A x = b, A symmetric positive definite in 3x3 block CSR (row-major blocks, block_rows
+ * rows, nnzb blocks). values: 9*nnzb of SDX_F32 or SDX_F64. b, x: host FP64 vectors of 3*block_rows;
+ * x is the initial guess on entry (ignored when hint == SDX_GUESS_ZERO) and the solution on exit.
+ * The matrix is stored on the device in FP32; dot products and x, r accumulate in FP64. */
+int sdx_pcg_solve(int block_rows, int64_t nnzb, const int64_t* row_ptr, const int32_t* col,
+                  const void* values, int value_type, const double* b, double* x, int hint,
+                  const sdx_linear_params* params, sdx_linear_status* status);
+
+/* Same, with an explicit context whose device workspace and launch tuning are reused. */
+int sdx_pcg_solve_ctx(sdx_context* ctx, int block_rows, int64_t nnzb, const int64_t* row_ptr,
+                      const int32_t* col, const void* values, int value_type, const double* b,
+                      double* x, int hint, const sdx_linear_params* params,
+                      sdx_linear_status* status);
+
+/* ---- context / FEM bodies ----------------------------------------------------------------------- */
+
+sdx_context* sdx_create(int device);
+int sdx_destroy(sdx_context* ctx);
+
+/* Upload n_envs independent soft bodies in the CSR-of-environments layout: env e owns nodes
+ * [node_offsets[e], node_offsets[e+1]) and tets [tet_offsets[e], tet_offsets[e+1]); tets hold GLOBAL
+ * node ids (4 per tet, positive orientation). X: 3 doubles per node. lambda, mu, rho: per tet.
+ * pin: per node, bit c set pins DoF c (Dirichlet). Builds the block pattern, the 3x3 sliced-ELL
+ * matrix layout, boundary faces (P1Q3 contact samples), mass couplings and per-tet scatter slots. */
+int sdx_upload_bodies(sdx_context* ctx, int n_envs, const int64_t* node_offsets,
+                      const int64_t* tet_offsets, const double* X, const int32_t* tets,
+                      const double* lambda, const double* mu, const double* rho, const uint8_t* pin);
+
+/* Kinematic colliders. rows: 11 doubles per collider = (type, p[6], radius, vel[3]);
+ * plane p = (n[3], o) with d = n.x - o; capsule p = (a[3], b[3]). env: owning env of each collider,
+ * non-decreasing. */
+int sdx_set_colliders(sdx_context* ctx, int n_colliders, const int32_t* env, const double* rows);
+
+int sdx_set_params(sdx_context* ctx, const sdx_step_params* params);
+
+/* State in user node order (3 doubles per node): displacement u and velocity v. */
+int sdx_set_state(sdx_context* ctx, const double* u, const double* v, double time);
+int sdx_get_state(sdx_context* ctx, double* u, double* v, double* time);
+
+/* Sizes of the uploaded problem. */
+int sdx_get_sizes(sdx_context* ctx, int64_t* n_nodes, int64_t* n_tets, int64_t* nnzb,
+                  int64_t* n_faces);
+/* Block pattern in user node order (row_ptr: n_nodes+1, col: nnzb), sorted columns. */
+int sdx_get_pattern(sdx_context* ctx, int64_t* row_ptr, int32_t* col);
+/* Boundary faces: 3 user node ids per face (outward), owning tet, rest area. */
+int sdx_get_faces(sdx_context* ctx, int32_t* face_nodes, int32_t* face_tet, double* face_area);
+
+/* Assemble at displacement u (host, user order; NULL = current state) with inertia target
+ * ut = u_state + dt v_state and colliders at time t. Outputs (any may be NULL): obj per env (FP64),
+ * gradient g (FP64, user order), Hessian values (FP32, 9 per block in sdx_get_pattern order),
+ * active contact pairs per env. Dirichlet rows/cols are applied. */
+int sdx_assemble(sdx_context* ctx, const double* u, double t, int flags, double* obj, double* g,
+                 float* hess, int64_t* n_pairs);
+
+/* Active contact pairs of the last assembly as sample*max_colliders_per_env + local collider, per
+ * env ascending (deterministic prefix-sum compaction). pairs_cap bounds the output. */
+int sdx_get_contact_pairs(sdx_context* ctx, int64_t* pairs, int64_t pairs_cap, int64_t* n_pairs);
+
+/* Advance every env n_steps backward-Euler steps from the current state (device resident). */
+int sdx_step(sdx_context* ctx, int n_steps);
+int sdx_get_stats(sdx_context* ctx, sdx_env_stats* per_env);
+
+/* Kernel-level entry points used by the benchmark: y = A x on the context's last assembled matrix
+ * (device resident, FP32), repeated `reps` times; returns the average time per SpMV in ms. */
+int sdx_bench_spmv(sdx_context* ctx, int reps, double* ms_per_spmv, double* bytes_per_spmv);
+/* Count of kernel launches issued by this context since creation (for launch accounting). */
+int64_t sdx_kernel_launches(sdx_context* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,164 @@
+// ref_shim.cpp — C entry points over the REFERENCE's own code, compiled from its sources in the
+// build container by oracle/build_ref.sh into oracle/_ref/libsdx_ref.so (test infrastructure only).
+//
+// Each entry point calls the reference function named beside it, unmodified, in its FP64 build
+// (MOCHI_USE_DOUBLE_PRECISION=1). The shim itself only marshals plain arrays in and out; it is used
+// to pin the C restatement in oracle/sdx_oracle.c and as the CPU "reference" baseline kernels.
+#include <mochi_core/contact/contact_params.h>
+#include <mochi_core/contact/contact_utils.h>
+#include <mochi_core/element_operations/fem_stress.h>
+#include <mochi_core/elements/tetrahedral/finite_element.h>
+#include <mochi_core/linear_algebra/krylov/pcg.h>
+#include <mochi_core/linear_algebra/matrix.h>
+#include <mochi_core/materials/batched_smith_neo_hookean.h>
+#include <mochi_core/solvers/krylov_solver.h>
+#include <mochi_core/utils/activations.h>
+
+#include <cstdint>
+#include <cstring>
+
+using namespace mochi;
+
+namespace {
+MaterialPsdStrategy ToStrategy(int s) {
+  switch (s) {
+    case 0:
+      return MaterialPsdStrategy::None;
+    case 2:
+      return MaterialPsdStrategy::AbsEigenProjection;
+    case 3:
+      return MaterialPsdStrategy::Fast;
+    default:
+      return MaterialPsdStrategy::Projection;
+  }
+}
+} // namespace
+
+extern "C" {
+
+// BatchedSmithNeoHookeanConstitutiveResponse<1> (mochi_core/src/materials/batched_smith_neo_hookean.cpp:29).
+// oracle: 0 None, 1 Correct, 2 Conservative (MaterialPsdOracle).
+void ref_smith_nh(double mu, double lambda, const double* F9, int project, int psd_strategy,
+                  int oracle, double* energy, double* P9, double* C81) {
+  materials::BatchLameParams<1> p;
+  p.mu = BatchReal<1>{mu};
+  p.lambda = BatchReal<1>{lambda};
+  p.psdStrategy = ToStrategy(psd_strategy);
+  BatchReal3x3<1> F{};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) F[i][j] = BatchReal<1>{F9[i * 3 + j]};
+  BatchDouble<1> e{};
+  BatchReal3x3<1> pk1{};
+  NdArray<BatchReal3x3<1>, 3, 3> C{};
+  materials::BatchedSmithNeoHookeanConstitutiveResponse<1>(
+      p, F, &e, &pk1, &C, project != 0, static_cast<materials::MaterialPsdOracle>(oracle));
+  if (energy) *energy = Get0(e);
+  if (P9)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) P9[i * 3 + j] = Get0(pk1[i][j]);
+  if (C81)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        for (int k = 0; k < 3; ++k)
+          for (int l = 0; l < 3; ++l) C81[(i * 3 + j) * 9 + k * 3 + l] = Get0(C[i][j][k][l]);
+}
+
+// PolyReLU (mochi_core/include/mochi_core/utils/activations.h:113).
+void ref_polyrelu(double x, double t, double shift, double* f, double* df, double* ddf) {
+  PolyReLU<double>(x, t, shift, *f, *df, *ddf);
+}
+
+// ComputeBatchContactPenaltyForceDForce<1> (mochi_core/include/mochi_core/contact/contact_utils.h:498).
+// dforce6 = (xx, yy, zz, xy, xz, yz).
+void ref_penalty(double d, const double* grad3, double k, double t_half, double thr, double* energy,
+                 double* force3, double* dforce6) {
+  ContactParams params;
+  params.penaltyCoefficient = k;
+  params.penaltySmoothingHalfDistance = t_half;
+  params.penaltyThresholdDefault = thr;
+  params.penaltyThresholdExtraPadding = 0;
+  ContactEvalConfig config{};
+  config.addPadding = false;
+  BatchDouble<1> e{};
+  BatchReal3<1> f{};
+  BatchReal6<1> df{};
+  BatchReal<1> fn{};
+  BatchReal3<1> g{BatchReal<1>{grad3[0]}, BatchReal<1>{grad3[1]}, BatchReal<1>{grad3[2]}};
+  ComputeBatchContactPenaltyForceDForce<1>(
+      e, f, df, fn, BatchReal<1>{d}, g, ~SimdZero<BatchReal<1>>(), BatchReal<1>{1.0}, params,
+      config, true, true, true, false);
+  *energy = Get0(e);
+  for (int i = 0; i < 3; ++i) force3[i] = Get0(f[i]);
+  for (int i = 0; i < 6; ++i) dforce6[i] = Get0(df[i]);
+}
+
+// fem::StressWork<1> over one Pk3DElement<1,1> built from rest coordinates (mochi_core/include/
+// mochi_core/element_operations/fem_stress.h:107), Smith Neo-Hookean response, PSD oracle Correct.
+// X12 = 4 rest nodes, u12 = 4 nodal displacements. res12 / K144 are overwritten.
+void ref_stress_work(const double* X12, const double* u12, double mu, double lambda, int project,
+                     int psd_strategy, double* energy, double* res12, double* K144) {
+  Real3 coords[4];
+  for (int i = 0; i < 4; ++i) coords[i] = Real3{X12[3 * i], X12[3 * i + 1], X12[3 * i + 2]};
+  Int4 conn[1] = {Int4{0, 1, 2, 3}};
+  using Elem = tetrahedral::Pk3DElement<1, 1>;
+  Elem elem(0, Span<Real3 const>(coords, 4), Span<Int4 const>(conn, 1));
+  NdArray<int, 1> idx{0};
+  fem::BatchElementVector<1, Elem> disp{};
+  for (int i = 0; i < 12; ++i) disp[i] = BatchReal<1>{u12[i]};
+  BatchDouble<1> e{0.0};
+  fem::BatchElementVector<1, Elem> res{};
+  fem::BatchElementMatrix<1, Elem> K{};
+  auto constitutive = [&](NdArray<int, 1> const&, auto const& F, auto* en, auto* pk1, auto* tan,
+                          bool psd) {
+    materials::BatchLameParams<1> p;
+    p.mu = BatchReal<1>{mu};
+    p.lambda = BatchReal<1>{lambda};
+    p.psdStrategy = ToStrategy(psd_strategy);
+    materials::BatchedSmithNeoHookeanConstitutiveResponse<1>(
+        p, F, en, pk1, tan, psd, materials::MaterialPsdOracle::Correct);
+  };
+  fem::StressWork<1>(idx, Span<Elem const>(&elem, 1), disp, &e, &res, &K, project != 0,
+                     constitutive);
+  *energy = Get0(e);
+  for (int i = 0; i < 12; ++i) res12[i] = Get0(res[i]);
+  for (int i = 0; i < 144; ++i) K144[i] = Get0(K[i]);
+}
+
+// krylov::PCG (mochi_core/include/mochi_core/linear_algebra/krylov/pcg.h:70) with the residual-L2
+// stop test (stopping_criterion.h:110), operator = scalar CSR matrix, preconditioner = Jacobi (the
+// inverse diagonal) or identity. Returns the iteration count; writes x, |r|, |r|/|b|, status.
+int ref_pcg_csr(int n, const int64_t* row_ptr, const int32_t* col, const double* val,
+                const double* b, double* x, double rel_tol, double abs_tol, double rel_div_tol,
+                int max_iter, int jacobi, int polak_ribiere, int zero_guess, double* res_norm,
+                double* rel_res_norm, int* convergence) {
+  ColumnVector<double> bv(n), xv(n), dinv(n);
+  for (int i = 0; i < n; ++i) {
+    bv[i] = b[i];
+    xv[i] = x[i];
+    double d = 0.0;
+    for (int64_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
+      if (col[k] == i) d = val[k];
+    dinv[i] = jacobi ? 1.0 / d : 1.0;
+  }
+  auto opA = [&](auto const& in, auto& out) {
+    for (int i = 0; i < n; ++i) {
+      double s = 0.0;
+      for (int64_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) s += val[k] * in[col[k]];
+      out[i] = s;
+    }
+  };
+  auto opP = [&](auto const& in, auto& out) {
+    for (int i = 0; i < n; ++i) out[i] = dinv[i] * in[i];
+  };
+  krylov::StatusResidualL2<krylov::UsualDot, double> stop{rel_tol, abs_tol, rel_div_tol};
+  auto st = krylov::PCG(opA, bv, xv, opP, max_iter, stop, false, VerbosityLevel::Silent,
+                        polak_ribiere != 0,
+                        zero_guess ? InitialGuessHint::Zero : InitialGuessHint::Unknown);
+  for (int i = 0; i < n; ++i) x[i] = xv[i];
+  *res_norm = st.residualNorm;
+  *rel_res_norm = st.relativeResidualNorm;
+  *convergence = static_cast<int>(st.convergence);
+  return st.numIterDone;
+}
+
+} // extern "C"

@@ -1,0 +1,135 @@
+"""ctypes binding of libsdx_b200.so (declarations in include/sdx_b200.h).
+
+The CUDA library is the only implementation: there is no CPU fallback. Loading fails loudly when the
+shared object is missing or was built for another device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsdx_b200.so")
+
+SDX_OK = 0
+SDX_ASM_OBJ, SDX_ASM_RES, SDX_ASM_HESS, SDX_ASM_PSD = 1, 2, 4, 8
+SDX_GUESS_UNKNOWN, SDX_GUESS_ZERO = 0, 1
+SDX_F32, SDX_F64 = 0, 1
+SDX_PREC_NONE, SDX_PREC_JACOBI, SDX_PREC_BLOCK_JACOBI = 0, 1, 2
+SDX_WARM_ZERO, SDX_WARM_PREVIOUS, SDX_WARM_LEARNED = 0, 1, 2
+SDX_LINEAR_CONVERGED, SDX_LINEAR_STOPPED, SDX_LINEAR_DIVERGED = 1, 2, 3
+
+# every entry point include/sdx_b200.h declares
+EXPORTED = [
+    "sdx_last_error", "sdx_version", "sdx_default_step_params", "sdx_default_linear_params",
+    "sdx_pcg_solve", "sdx_pcg_solve_ctx", "sdx_create", "sdx_destroy", "sdx_upload_bodies",
+    "sdx_set_colliders", "sdx_set_params", "sdx_set_state", "sdx_get_state", "sdx_get_sizes",
+    "sdx_get_pattern", "sdx_get_faces", "sdx_assemble", "sdx_get_contact_pairs", "sdx_step",
+    "sdx_get_stats", "sdx_bench_spmv", "sdx_kernel_launches",
+]
+
+
+class LinearParams(C.Structure):
+    """KrylovSolverParams mirror (mochi_core/include/mochi_core/solvers/krylov_solver.h:43-82)."""
+
+    _fields_ = [("rel_tol", C.c_double), ("abs_tol", C.c_double), ("rel_div_tol", C.c_double),
+                ("max_iter", C.c_int), ("preconditioner", C.c_int), ("abort_if_not_spd", C.c_int),
+                ("polak_ribiere", C.c_int), ("replace_every", C.c_int)]
+
+
+class LinearStatus(C.Structure):
+    """LinearSolverStatus mirror (krylov_solver.h:85-116)."""
+
+    _fields_ = [("num_iter", C.c_int), ("residual_norm", C.c_double),
+                ("relative_residual_norm", C.c_double), ("convergence", C.c_int)]
+
+
+class StepParams(C.Structure):
+    _fields_ = [("dt", C.c_double), ("gravity", C.c_double * 3), ("psd_strategy", C.c_int),
+                ("k_contact", C.c_double), ("t_half", C.c_double), ("thr", C.c_double),
+                ("max_align", C.c_double), ("newton_max_iter", C.c_int),
+                ("newton_rel_tol", C.c_double), ("newton_abs_tol", C.c_double),
+                ("newton_rel_step_tol", C.c_double), ("ls_max_iter", C.c_int),
+                ("ls_alpha", C.c_double), ("ew_forcing", C.c_int), ("rel_div_tol", C.c_double),
+                ("abs_div_tol", C.c_double), ("warm_start", C.c_int), ("linear", LinearParams)]
+
+
+class EnvStats(C.Structure):
+    _fields_ = [("newton_iters", C.c_int), ("cg_iters", C.c_int), ("ls_iters", C.c_int),
+                ("convergence", C.c_int), ("res_norm0", C.c_double), ("res_norm", C.c_double),
+                ("n_contacts", C.c_int64)]
+
+
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int32)
+_lp = C.POINTER(C.c_int64)
+_up = C.POINTER(C.c_uint8)
+_vp = C.c_void_p
+
+_lib = None
+
+
+class SdxError(RuntimeError):
+    pass
+
+
+def lib():
+    """Load libsdx_b200.so (raises when it is missing: there is no fallback path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: run `python -m project_superdex_b200.build` "
+                          "(the soft-body step has no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    L.sdx_last_error.restype = C.c_char_p
+    L.sdx_default_step_params.argtypes = [C.POINTER(StepParams)]
+    L.sdx_default_linear_params.argtypes = [C.POINTER(LinearParams)]
+    L.sdx_pcg_solve.argtypes = [C.c_int, C.c_int64, _lp, _ip, _vp, C.c_int, _dp, _dp, C.c_int,
+                                C.POINTER(LinearParams), C.POINTER(LinearStatus)]
+    L.sdx_pcg_solve_ctx.argtypes = [_vp, C.c_int, C.c_int64, _lp, _ip, _vp, C.c_int, _dp, _dp,
+                                    C.c_int, C.POINTER(LinearParams), C.POINTER(LinearStatus)]
+    L.sdx_create.argtypes = [C.c_int]
+    L.sdx_create.restype = _vp
+    L.sdx_destroy.argtypes = [_vp]
+    L.sdx_upload_bodies.argtypes = [_vp, C.c_int, _lp, _lp, _dp, _ip, _dp, _dp, _dp, _up]
+    L.sdx_set_colliders.argtypes = [_vp, C.c_int, _ip, _dp]
+    L.sdx_set_params.argtypes = [_vp, C.POINTER(StepParams)]
+    L.sdx_set_state.argtypes = [_vp, _dp, _dp, C.c_double]
+    L.sdx_get_state.argtypes = [_vp, _dp, _dp, _dp]
+    L.sdx_get_sizes.argtypes = [_vp, _lp, _lp, _lp, _lp]
+    L.sdx_get_pattern.argtypes = [_vp, _lp, _ip]
+    L.sdx_get_faces.argtypes = [_vp, _ip, _ip, _dp]
+    L.sdx_assemble.argtypes = [_vp, _dp, C.c_double, C.c_int, _dp, _dp, _fp, _lp]
+    L.sdx_get_contact_pairs.argtypes = [_vp, _lp, C.c_int64, _lp]
+    L.sdx_step.argtypes = [_vp, C.c_int]
+    L.sdx_get_stats.argtypes = [_vp, C.POINTER(EnvStats)]
+    L.sdx_bench_spmv.argtypes = [_vp, C.c_int, _dp, _dp]
+    L.sdx_kernel_launches.argtypes = [_vp]
+    L.sdx_kernel_launches.restype = C.c_int64
+    _lib = L
+    return L
+
+
+def check(rc: int):
+    if rc != SDX_OK:
+        raise SdxError(f"sdx error {rc}: {lib().sdx_last_error().decode()}")
+
+
+def ptr(a, t=_dp):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+def default_step_params() -> StepParams:
+    p = StepParams()
+    lib().sdx_default_step_params(C.byref(p))
+    return p
+
+
+def default_linear_params() -> LinearParams:
+    p = LinearParams()
+    lib().sdx_default_linear_params(C.byref(p))
+    return p

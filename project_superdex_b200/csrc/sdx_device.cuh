@@ -1,0 +1,413 @@
+// sdx_device.cuh — device math for the soft-body step (sm_100a).
+//
+// Smith et al. 2018 stable Neo-Hookean, as in the reference's
+// mochi_core/src/materials/batched_smith_neo_hookean.cpp:29-269:
+//   * energy and first Piola-Kirchhoff stress in FP64 (they feed the Newton residual and the
+//     line-search residual norms, whose stopping test at rel 1e-6 needs FP64);
+//   * the 9x9 tangent in FP32 (it only feeds the FP32 block Hessian), with the PSD projection done by
+//     clamping the analytic eigensystem (scaling / twist / flip modes) of the tangent.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sdx {
+
+// ------------------------------------------------------------------------------------------------
+// small dense helpers (row-major 3x3)
+
+template <class T>
+__device__ __forceinline__ T det3(const T F[9]) {
+  return F[0] * (F[4] * F[8] - F[5] * F[7]) - F[1] * (F[3] * F[8] - F[5] * F[6]) +
+         F[2] * (F[3] * F[7] - F[4] * F[6]);
+}
+
+// cof(F)_ij = dJ/dF_ij
+template <class T>
+__device__ __forceinline__ void cof3(const T F[9], T C[9]) {
+  C[0] = F[4] * F[8] - F[5] * F[7];
+  C[1] = F[5] * F[6] - F[3] * F[8];
+  C[2] = F[3] * F[7] - F[4] * F[6];
+  C[3] = F[2] * F[7] - F[1] * F[8];
+  C[4] = F[0] * F[8] - F[2] * F[6];
+  C[5] = F[1] * F[6] - F[0] * F[7];
+  C[6] = F[1] * F[5] - F[2] * F[4];
+  C[7] = F[2] * F[3] - F[0] * F[5];
+  C[8] = F[0] * F[4] - F[1] * F[3];
+}
+
+// Levi-Civita sign of distinct (a, b, c) in {0,1,2}.
+__host__ __device__ constexpr int levi(int a, int b, int c) {
+  return (a == b || b == c || a == c) ? 0 : (((b - a + 3) % 3) == 1 ? 1 : -1);
+}
+
+// Entry (ab) of the 9x9 Hessian of J = det F: d2J/dF_ij dF_kl = eps_ikn eps_jlq F_nq, i.e. a single
+// signed entry of F when i != k and j != l (material_utils.h:182-218 writes the same skew blocks).
+__host__ __device__ constexpr int hj_sign(int a, int b) {
+  return ((a / 3) == (b / 3) || (a % 3) == (b % 3))
+             ? 0
+             : levi(a / 3, b / 3, 3 - a / 3 - b / 3) * levi(a % 3, b % 3, 3 - a % 3 - b % 3);
+}
+__host__ __device__ constexpr int hj_index(int a, int b) {
+  return (3 - a / 3 - b / 3) * 3 + (3 - a % 3 - b % 3);
+}
+
+// ------------------------------------------------------------------------------------------------
+// FP64 energy + PK1 (batched_smith_neo_hookean.cpp:46-69, 127-136)
+
+struct SnhConsts {
+  double muHat, lambdaHat, alpha;
+};
+
+__device__ __forceinline__ SnhConsts snh_consts(double mu, double lambda) {
+  SnhConsts c;
+  c.muHat = mu * (4.0 / 3.0);
+  c.lambdaHat = lambda + mu * (5.0 / 6.0);
+  c.alpha = 1.0 + 0.75 * c.muHat / c.lambdaHat;
+  return c;
+}
+
+__device__ __forceinline__ void snh_pk1_f64(const SnhConsts& k, const double F[9], double P[9]) {
+  double Ic = 0.0;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) Ic = fma(F[i], F[i], Ic);
+  const double J = det3(F);
+  double cof[9];
+  cof3(F, cof);
+  const double c0 = k.muHat * (1.0 - 1.0 / (Ic + 1.0));
+  const double c1 = k.lambdaHat * (J - k.alpha);
+#pragma unroll
+  for (int i = 0; i < 9; ++i) P[i] = c0 * F[i] + c1 * cof[i];
+}
+
+__device__ __forceinline__ double snh_energy_f64(const SnhConsts& k, const double F[9]) {
+  double Ic = 0.0;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) Ic = fma(F[i], F[i], Ic);
+  const double Jma = det3(F) - k.alpha;
+  return 0.5 * k.muHat * (Ic - 3.0) + 0.5 * k.lambdaHat * Jma * Jma - 0.5 * k.muHat * log(Ic + 1.0);
+}
+
+// ------------------------------------------------------------------------------------------------
+// FP32 symmetric 3x3 eigen-decomposition (cyclic Jacobi rotations).
+// In: A (row-major, symmetric). Out: w (eigenvalues), V columns = eigenvectors (V[r*3+c]).
+
+__device__ __forceinline__ void jacobi_rot(float A[9], float V[9], int p, int q) {
+  const float apq = A[p * 3 + q];
+  if (fabsf(apq) < 1e-30f) return;
+  const float theta = (A[q * 3 + q] - A[p * 3 + p]) / (2.0f * apq);
+  const float t = copysignf(1.0f, theta) / (fabsf(theta) + sqrtf(fmaf(theta, theta, 1.0f)));
+  const float c = rsqrtf(fmaf(t, t, 1.0f));
+  const float s = t * c;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float akp = A[k * 3 + p], akq = A[k * 3 + q];
+    A[k * 3 + p] = c * akp - s * akq;
+    A[k * 3 + q] = s * akp + c * akq;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float apk = A[p * 3 + k], aqk = A[q * 3 + k];
+    A[p * 3 + k] = c * apk - s * aqk;
+    A[q * 3 + k] = s * apk + c * aqk;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float vkp = V[k * 3 + p], vkq = V[k * 3 + q];
+    V[k * 3 + p] = c * vkp - s * vkq;
+    V[k * 3 + q] = s * vkp + c * vkq;
+  }
+}
+
+__device__ __forceinline__ void sym_eig3(const float Ain[9], float w[3], float V[9]) {
+  float A[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) A[i] = Ain[i];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) V[i] = (i % 4 == 0) ? 1.0f : 0.0f;
+  for (int sweep = 0; sweep < 8; ++sweep) {
+    const float off = A[1] * A[1] + A[2] * A[2] + A[5] * A[5];
+    const float dg = A[0] * A[0] + A[4] * A[4] + A[8] * A[8];
+    if (off <= 1e-14f * dg) break;
+    jacobi_rot(A, V, 0, 1);
+    jacobi_rot(A, V, 0, 2);
+    jacobi_rot(A, V, 1, 2);
+  }
+  w[0] = A[0];
+  w[1] = A[4];
+  w[2] = A[8];
+}
+
+// Rotation-variant SVD F = U diag(s) V^T with det U = det V = +1 and s[2] < 0 iff det F < 0
+// (the convention of the reference's BatchedRotationVariantSvd3x3). V from the eigenvectors of F^T F
+// sorted by decreasing eigenvalue; U from F V with Gram-Schmidt and a cross product.
+__device__ __forceinline__ void svd3_rv(const float F[9], float U[9], float s[3], float V[9]) {
+  float S[9];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      S[i * 3 + j] = F[0 * 3 + i] * F[0 * 3 + j] + F[1 * 3 + i] * F[1 * 3 + j] + F[2 * 3 + i] * F[2 * 3 + j];
+  float w[3];
+  sym_eig3(S, w, V);
+  // sort descending (3-element network), swapping V columns alongside
+#define SDX_SWAP_COL(a, b)                                   \
+  {                                                          \
+    float tw = w[a];                                         \
+    w[a] = w[b];                                             \
+    w[b] = tw;                                               \
+    _Pragma("unroll") for (int r = 0; r < 3; ++r) {          \
+      float tv = V[r * 3 + a];                               \
+      V[r * 3 + a] = V[r * 3 + b];                           \
+      V[r * 3 + b] = tv;                                     \
+    }                                                        \
+  }
+  if (w[0] < w[1]) SDX_SWAP_COL(0, 1);
+  if (w[0] < w[2]) SDX_SWAP_COL(0, 2);
+  if (w[1] < w[2]) SDX_SWAP_COL(1, 2);
+#undef SDX_SWAP_COL
+  // det V = +1
+  const float dv = det3(V);
+  if (dv < 0.0f) {
+    V[2] = -V[2];
+    V[5] = -V[5];
+    V[8] = -V[8];
+  }
+  float fv[3][3];  // F v_k
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      fv[k][r] = F[r * 3 + 0] * V[0 * 3 + k] + F[r * 3 + 1] * V[1 * 3 + k] + F[r * 3 + 2] * V[2 * 3 + k];
+  float u0[3], u1[3], u2[3];
+  float n0 = sqrtf(fv[0][0] * fv[0][0] + fv[0][1] * fv[0][1] + fv[0][2] * fv[0][2]);
+  if (n0 > 1e-30f) {
+    u0[0] = fv[0][0] / n0;
+    u0[1] = fv[0][1] / n0;
+    u0[2] = fv[0][2] / n0;
+  } else {
+    u0[0] = 1.0f;
+    u0[1] = 0.0f;
+    u0[2] = 0.0f;
+  }
+  float d01 = u0[0] * fv[1][0] + u0[1] * fv[1][1] + u0[2] * fv[1][2];
+  u1[0] = fv[1][0] - d01 * u0[0];
+  u1[1] = fv[1][1] - d01 * u0[1];
+  u1[2] = fv[1][2] - d01 * u0[2];
+  float n1 = sqrtf(u1[0] * u1[0] + u1[1] * u1[1] + u1[2] * u1[2]);
+  if (n1 > 1e-6f * fmaxf(n0, 1e-30f)) {
+    u1[0] /= n1;
+    u1[1] /= n1;
+    u1[2] /= n1;
+  } else {
+    // any unit vector orthogonal to u0
+    float a[3] = {fabsf(u0[0]) < 0.9f ? 1.0f : 0.0f, fabsf(u0[0]) < 0.9f ? 0.0f : 1.0f, 0.0f};
+    float dd = a[0] * u0[0] + a[1] * u0[1] + a[2] * u0[2];
+    u1[0] = a[0] - dd * u0[0];
+    u1[1] = a[1] - dd * u0[1];
+    u1[2] = a[2] - dd * u0[2];
+    float nn = rsqrtf(u1[0] * u1[0] + u1[1] * u1[1] + u1[2] * u1[2]);
+    u1[0] *= nn;
+    u1[1] *= nn;
+    u1[2] *= nn;
+  }
+  u2[0] = u0[1] * u1[2] - u0[2] * u1[1];
+  u2[1] = u0[2] * u1[0] - u0[0] * u1[2];
+  u2[2] = u0[0] * u1[1] - u0[1] * u1[0];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    U[r * 3 + 0] = u0[r];
+    U[r * 3 + 1] = u1[r];
+    U[r * 3 + 2] = u2[r];
+  }
+  s[0] = u0[0] * fv[0][0] + u0[1] * fv[0][1] + u0[2] * fv[0][2];
+  s[1] = u1[0] * fv[1][0] + u1[1] * fv[1][1] + u1[2] * fv[1][2];
+  s[2] = u2[0] * fv[2][0] + u2[1] * fv[2][1] + u2[2] * fv[2][2];
+}
+
+// ------------------------------------------------------------------------------------------------
+// FP32 tangent dP/dF (9x9, symmetric, full storage C[a*9+b]) with the reference's PSD handling.
+// psd: 0 none, 1 projection (max(l, eps)), 2 |l| projection, 3 fast (drop d2J when indefinite).
+
+__device__ __forceinline__ void snh_tangent_f32(float mu, float lambda, const float F[9], int project,
+                                                int psd, float min_eig, float C[81]) {
+  const float muHat = mu * (4.0f / 3.0f);
+  const float lambdaHat = lambda + mu * (5.0f / 6.0f);
+  const float alpha = 1.0f + 0.75f * muHat / lambdaHat;
+  float Ic = 0.0f;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) Ic = fmaf(F[i], F[i], Ic);
+  const float IcPlus1 = Ic + 1.0f, IcPlus1Inv = 1.0f / IcPlus1;
+  const float J = det3(F), Jma = J - alpha;
+  const float c2 = muHat * (1.0f - IcPlus1Inv);
+  const float c3 = 2.0f * muHat * IcPlus1Inv * IcPlus1Inv;
+
+  bool projecting = project && psd != 0;
+  if (projecting) {
+    // PSD oracle "Correct" (batched_smith_neo_hookean.cpp:81-104). The conservative bound Ic >=
+    // max sigma^2 decides cheaply when it proves definiteness; otherwise the SVD values decide.
+    const float muHatK2 = c2 * c2;
+    const float lhsBase = (lambdaHat * Jma) * (lambdaHat * Jma);
+    bool indefinite = (J < 0.0f) || (lhsBase * Ic > muHatK2);
+    if (indefinite && J >= 0.0f) {
+      float S[9], w[3], Vt[9];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          S[i * 3 + j] = F[i] * F[j] + F[3 + i] * F[3 + j] + F[6 + i] * F[6 + j];
+      sym_eig3(S, w, Vt);
+      const float maxs2 = fmaxf(w[0], fmaxf(w[1], w[2]));
+      indefinite = lhsBase * maxs2 > muHatK2;
+    }
+    projecting = indefinite;
+  }
+
+  if (projecting && (psd == 1 || psd == 2)) {
+    // Eigensystem path (batched_smith_neo_hookean.cpp:141-203, Smith et al. 2018).
+    float U[9], s[3], V[9];
+    svd3_rv(F, U, s, V);
+    const float coeff0 = muHat - muHat * IcPlus1Inv;
+    const float coeff1 = lambdaHat * Jma;
+    float lam[9];
+    lam[3] = coeff1 * s[0] + coeff0;  // twist, pair (1,2)
+    lam[4] = coeff1 * s[1] + coeff0;  // twist, pair (0,2)
+    lam[5] = coeff1 * s[2] + coeff0;  // twist, pair (0,1)
+    lam[6] = -coeff1 * s[0] + coeff0; // flip
+    lam[7] = -coeff1 * s[1] + coeff0;
+    lam[8] = -coeff1 * s[2] + coeff0;
+    const float Ic2inv = IcPlus1Inv * IcPlus1Inv;
+    const float mu2 = 2.0f * muHat;
+    const float J2al = (2.0f * J - alpha) * lambdaHat;
+    const float s0 = s[0] * s[0], s1 = s[1] * s[1], s2 = s[2] * s[2];
+    float A[9];
+    A[0] = (mu2 * s0 - muHat * IcPlus1) * Ic2inv + lambdaHat * s1 * s2 + muHat;
+    A[4] = (mu2 * s1 - muHat * IcPlus1) * Ic2inv + lambdaHat * s0 * s2 + muHat;
+    A[8] = (mu2 * s2 - muHat * IcPlus1) * Ic2inv + lambdaHat * s0 * s1 + muHat;
+    A[1] = A[3] = J2al * s[2] + mu2 * s[0] * s[1] * Ic2inv;
+    A[2] = A[6] = J2al * s[1] + mu2 * s[0] * s[2] * Ic2inv;
+    A[5] = A[7] = J2al * s[0] + mu2 * s[1] * s[2] * Ic2inv;
+    float wa[3], Va[9];
+    sym_eig3(A, wa, Va);
+    lam[0] = wa[0];
+    lam[1] = wa[1];
+    lam[2] = wa[2];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      float l = (psd == 2) ? fabsf(lam[i]) : lam[i];
+      lam[i] = fmaxf(l, min_eig);
+    }
+    // modes as 9-vectors: Q_i = U diag(a_i) V^T, T_n / L_n = (u_j v_k^T -/+ u_k v_j^T) / sqrt(2)
+    float M[9][9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          M[i][r * 3 + c] = U[r * 3 + 0] * Va[0 * 3 + i] * V[c * 3 + 0] +
+                            U[r * 3 + 1] * Va[1 * 3 + i] * V[c * 3 + 1] +
+                            U[r * 3 + 2] * Va[2 * 3 + i] * V[c * 3 + 2];
+    const float rs2 = 0.70710678118654752f;
+#pragma unroll
+    for (int n = 0; n < 3; ++n) {
+      const int j = (n == 0) ? 1 : 0;
+      const int k = (n == 2) ? 1 : 2;
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const float a = U[r * 3 + j] * V[c * 3 + k];
+          const float b = U[r * 3 + k] * V[c * 3 + j];
+          M[3 + n][r * 3 + c] = (a - b) * rs2;
+          M[6 + n][r * 3 + c] = (a + b) * rs2;
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 9; ++a)
+#pragma unroll
+      for (int b = a; b < 9; ++b) {
+        float v = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) v = fmaf(lam[i] * M[i][a], M[i][b], v);
+        C[a * 9 + b] = v;
+        C[b * 9 + a] = v;
+      }
+    return;
+  }
+
+  // Direct tangent (batched_smith_neo_hookean.cpp:204-266).
+  float cof[9];
+  cof3(F, cof);
+  const float d2c = (projecting && psd == 3) ? 0.0f : lambdaHat * Jma;
+#pragma unroll
+  for (int a = 0; a < 9; ++a)
+#pragma unroll
+    for (int b = a; b < 9; ++b) {
+      float v = c3 * F[a] * F[b] + lambdaHat * cof[a] * cof[b];
+      if (a == b) v += c2;
+      if (hj_sign(a, b) != 0) v += float(hj_sign(a, b)) * d2c * F[hj_index(a, b)];
+      C[a * 9 + b] = v;
+      C[b * 9 + a] = v;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// contact helpers (FP64): PolyReLU and the analytic collider SDFs
+
+// activations.h:113-130
+__device__ __forceinline__ void polyrelu(double x, double t, double shift, double& f, double& df,
+                                         double& ddf) {
+  x -= shift;
+  if (t <= 0.0 || fabs(x) > t) {
+    f = x > 0.0 ? x : 0.0;
+    df = x < 0.0 ? 0.0 : 1.0;
+    ddf = 0.0;
+    return;
+  }
+  const double xt = x / t, x2 = xt * xt, x3 = x2 * xt;
+  const double fv = (3.0 / 16.0) * t + (0.5 + (3.0 / 8.0) * xt - (1.0 / 16.0) * x3) * x;
+  const double dfv = 0.5 + 0.75 * xt - 0.25 * x3;
+  const double ddfv = 0.75 * (1.0 - x2) / t;
+  f = fmax(fv, 0.0);
+  df = fmin(fmax(dfv, 0.0), 1.0);
+  ddf = fmax(ddfv, 0.0);
+}
+
+// collider row: (type, p[6], radius, vel[3])
+__device__ __forceinline__ void collider_sdf(const double* c, const double x[3], double t, double& d,
+                                             double g[3]) {
+  if (c[0] == 0.0) {  // plane
+    const double o = c[4] + (c[1] * c[8] + c[2] * c[9] + c[3] * c[10]) * t;
+    d = c[1] * x[0] + c[2] * x[1] + c[3] * x[2] - o;
+    g[0] = c[1];
+    g[1] = c[2];
+    g[2] = c[3];
+    return;
+  }
+  double a[3], ab[3], ax[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    a[i] = c[1 + i] + c[8 + i] * t;
+    ab[i] = c[4 + i] - c[1 + i];
+    ax[i] = x[i] - a[i];
+  }
+  const double l2 = ab[0] * ab[0] + ab[1] * ab[1] + ab[2] * ab[2];
+  double s = l2 > 0.0 ? (ax[0] * ab[0] + ax[1] * ab[1] + ax[2] * ab[2]) / l2 : 0.0;
+  s = fmin(fmax(s, 0.0), 1.0);
+  double df[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) df[i] = ax[i] - s * ab[i];
+  const double dist = sqrt(df[0] * df[0] + df[1] * df[1] + df[2] * df[2]);
+  d = dist - c[7];
+  if (dist > 0.0) {
+    g[0] = df[0] / dist;
+    g[1] = df[1] / dist;
+    g[2] = df[2] / dist;
+  } else {
+    g[0] = 0.0;
+    g[1] = 0.0;
+    g[2] = 1.0;
+  }
+}
+
+}  // namespace sdx

@@ -1,0 +1,1431 @@
+// sdx_host.cu — host runtime of libsdx_b200.so: C-ABI entry points, topology preprocessing
+// (block pattern, sliced-ELL layout, per-tet scatter slots, boundary faces), the batched Newton driver
+// and the standalone PCG solve. Device buffers are owned by the context.
+#include <cuda_runtime.h>
+#include <omp.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/sdx_b200.h"
+#include "sdx_internal.cuh"
+
+using namespace sdx;
+
+// ------------------------------------------------------------------------------------------------
+// errors
+
+static thread_local std::string g_last_error;
+
+static int set_error(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+#define SDX_CUDA(call)                                                                       \
+  do {                                                                                       \
+    cudaError_t _e = (call);                                                                 \
+    if (_e != cudaSuccess) {                                                                 \
+      return set_error(_e == cudaErrorMemoryAllocation ? SDX_ERR_OUT_OF_MEMORY : SDX_ERR_CUDA, \
+                       "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(_e));   \
+    }                                                                                        \
+  } while (0)
+
+#define SDX_TRY(call)          \
+  do {                         \
+    int _r = (call);           \
+    if (_r != SDX_OK) return _r; \
+  } while (0)
+
+template <class T>
+static int dalloc(T** p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess)
+    return set_error(e == cudaErrorMemoryAllocation ? SDX_ERR_OUT_OF_MEMORY : SDX_ERR_CUDA,
+                     "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+  return SDX_OK;
+}
+
+template <class T>
+static void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+template <class T>
+static int upload(T** d, const std::vector<T>& h) {
+  SDX_TRY(dalloc(d, h.size()));
+  if (!h.empty()) SDX_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return SDX_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// context
+
+struct PcgPartition {
+  int n_cta = 0, threads = 0;
+  int* cta_slice = nullptr;
+  int* cta_env0 = nullptr;
+  int* cta_env1 = nullptr;
+  int* cta_pbase = nullptr;
+  int* env_cta0 = nullptr;
+  int* env_cta1 = nullptr;
+  double* part = nullptr;
+  void release() {
+    dfree(cta_slice);
+    dfree(cta_env0);
+    dfree(cta_env1);
+    dfree(cta_pbase);
+    dfree(env_cta0);
+    dfree(env_cta1);
+    dfree(part);
+  }
+};
+
+struct PcgWork {
+  int64_t n_rows = 0;
+  double* r = nullptr;
+  float* p = nullptr;
+  float* q = nullptr;
+  float4* z = nullptr;
+  float* dinv = nullptr;
+  unsigned* sync = nullptr;
+  int* out_iters = nullptr;
+  double* out_res = nullptr;
+  double* out_relres = nullptr;
+  int* out_conv = nullptr;
+  double* env_rel_tol = nullptr;
+  int n_envs_alloc = 0;
+  void release() {
+    dfree(r);
+    dfree(p);
+    dfree(q);
+    dfree(z);
+    dfree(dinv);
+    dfree(sync);
+    dfree(out_iters);
+    dfree(out_res);
+    dfree(out_relres);
+    dfree(out_conv);
+    dfree(env_rel_tol);
+    n_rows = 0;
+    n_envs_alloc = 0;
+  }
+};
+
+struct sdx_context {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  int64_t launches = 0;
+  sdx_step_params params;
+  bool uploaded = false;
+  // sizes
+  int n_envs = 0;
+  int64_t n_nodes = 0, n_tets = 0, n_rows = 0, nnzb = 0, nb_pad = 0, n_faces = 0;
+  int n_slices = 0;
+  int n_colliders = 0;
+  double time = 0.0;
+  // host topology
+  std::vector<int64_t> h_node_off, h_tet_off, h_row_off;
+  std::vector<int32_t> h_row_of_node;
+  std::vector<int64_t> h_prow;  // user pattern row_ptr
+  std::vector<int32_t> h_pcol;  // user pattern columns (user node ids)
+  std::vector<int> h_slice_ptr, h_slice_w, h_slice_env;
+  std::vector<int32_t> h_face_nodes, h_face_tet;
+  std::vector<double> h_face_area;
+  std::vector<int> h_coll_off;
+  int max_coll_per_env = 0;
+  // device topology
+  int* slice_ptr = nullptr;
+  int* slice_w = nullptr;
+  int* slice_env = nullptr;
+  int* col = nullptr;
+  float* val = nullptr;
+  float* mass = nullptr;
+  int* diag_pos = nullptr;
+  int4* tets = nullptr;
+  float4* rest[4] = {nullptr, nullptr, nullptr, nullptr};
+  int4* slots[4] = {nullptr, nullptr, nullptr, nullptr};
+  uint8_t* pin = nullptr;
+  double* X = nullptr;
+  int4* faces = nullptr;
+  double* face_area = nullptr;
+  int* face_slots = nullptr;
+  int* row_of_node = nullptr;
+  int* coll_off = nullptr;
+  double* colliders = nullptr;
+  // state / work vectors (3 per row, FP64)
+  double *u = nullptr, *v = nullptr, *u0 = nullptr, *ut = nullptr, *g = nullptr, *dx = nullptr,
+         *ubase = nullptr, *uscratch = nullptr, *staging = nullptr;
+  // per env
+  double* env_norm = nullptr;
+  double* env_scale = nullptr;
+  double* env_obj = nullptr;
+  uint8_t* env_mask = nullptr;
+  unsigned long long* env_pairs = nullptr;
+  unsigned* pair_mask = nullptr;
+  std::vector<sdx_env_stats> stats;
+  // PCG
+  PcgPartition part;
+  PcgWork work;
+  // standalone solve matrix (sdx_pcg_solve_ctx)
+  int solo_rows = 0;
+  int64_t solo_nb = 0;
+  int *solo_slice_ptr = nullptr, *solo_slice_w = nullptr, *solo_slice_env = nullptr, *solo_col = nullptr,
+      *solo_diag = nullptr;
+  float* solo_val = nullptr;
+  double *solo_b = nullptr, *solo_x = nullptr;
+  PcgPartition solo_part;
+  PcgWork solo_work;
+};
+
+static void release_topology(sdx_context* c) {
+  dfree(c->slice_ptr);
+  dfree(c->slice_w);
+  dfree(c->slice_env);
+  dfree(c->col);
+  dfree(c->val);
+  dfree(c->mass);
+  dfree(c->diag_pos);
+  dfree(c->tets);
+  for (int k = 0; k < 4; ++k) {
+    dfree(c->rest[k]);
+    dfree(c->slots[k]);
+  }
+  dfree(c->pin);
+  dfree(c->X);
+  dfree(c->faces);
+  dfree(c->face_area);
+  dfree(c->face_slots);
+  dfree(c->row_of_node);
+  dfree(c->coll_off);
+  dfree(c->colliders);
+  dfree(c->u);
+  dfree(c->v);
+  dfree(c->u0);
+  dfree(c->ut);
+  dfree(c->g);
+  dfree(c->dx);
+  dfree(c->ubase);
+  dfree(c->uscratch);
+  dfree(c->staging);
+  dfree(c->env_norm);
+  dfree(c->env_scale);
+  dfree(c->env_obj);
+  dfree(c->env_mask);
+  dfree(c->env_pairs);
+  dfree(c->pair_mask);
+  c->part.release();
+  c->work.release();
+  c->uploaded = false;
+}
+
+static void release_solo(sdx_context* c) {
+  dfree(c->solo_slice_ptr);
+  dfree(c->solo_slice_w);
+  dfree(c->solo_slice_env);
+  dfree(c->solo_col);
+  dfree(c->solo_diag);
+  dfree(c->solo_val);
+  dfree(c->solo_b);
+  dfree(c->solo_x);
+  c->solo_part.release();
+  c->solo_work.release();
+  c->solo_rows = 0;
+  c->solo_nb = 0;
+}
+
+// ------------------------------------------------------------------------------------------------
+// scatter / gather between user node order and padded rows
+
+__global__ void k_scatter_rows(int64_t n_nodes, const int* __restrict__ row_of_node,
+                               const double* __restrict__ src, double* dst) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_nodes) return;
+  const int64_t r = row_of_node[i];
+  dst[3 * r] = src[3 * i];
+  dst[3 * r + 1] = src[3 * i + 1];
+  dst[3 * r + 2] = src[3 * i + 2];
+}
+
+__global__ void k_gather_rows(int64_t n_nodes, const int* __restrict__ row_of_node,
+                              const double* __restrict__ src, double* dst) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_nodes) return;
+  const int64_t r = row_of_node[i];
+  dst[3 * i] = src[3 * r];
+  dst[3 * i + 1] = src[3 * r + 1];
+  dst[3 * i + 2] = src[3 * r + 2];
+}
+
+static int h2d_rows(sdx_context* c, const double* host, double* dev_rows) {
+  SDX_CUDA(cudaMemcpyAsync(c->staging, host, sizeof(double) * 3 * c->n_nodes, cudaMemcpyHostToDevice,
+                           c->stream));
+  k_scatter_rows<<<(unsigned)((c->n_nodes + 255) / 256), 256, 0, c->stream>>>(c->n_nodes, c->row_of_node,
+                                                                               c->staging, dev_rows);
+  c->launches++;
+  return SDX_OK;
+}
+
+static int d2h_rows(sdx_context* c, const double* dev_rows, double* host) {
+  k_gather_rows<<<(unsigned)((c->n_nodes + 255) / 256), 256, 0, c->stream>>>(c->n_nodes, c->row_of_node,
+                                                                              dev_rows, c->staging);
+  c->launches++;
+  SDX_CUDA(cudaMemcpyAsync(host, c->staging, sizeof(double) * 3 * c->n_nodes, cudaMemcpyDeviceToHost,
+                           c->stream));
+  SDX_CUDA(cudaStreamSynchronize(c->stream));
+  return SDX_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// topology
+
+// Faces numbered as the reference's TetFaces: 0:(0,1,2) 1:(0,1,3) 2:(0,2,3) 3:(1,2,3).
+static const int kFaceLocal[4][3] = {{0, 1, 2}, {0, 1, 3}, {0, 2, 3}, {1, 2, 3}};
+static const int kFaceOpp[4] = {3, 2, 1, 0};
+
+struct FaceKey {
+  int32_t a, b, c, tet, face;
+};
+
+static void boundary_faces_env(int64_t t0, int64_t t1, const int32_t* tets, const double* X,
+                               std::vector<int32_t>& fn, std::vector<int32_t>& ft,
+                               std::vector<double>& fa) {
+  std::vector<FaceKey> r;
+  r.reserve((size_t)(t1 - t0) * 4);
+  for (int64_t t = t0; t < t1; ++t)
+    for (int f = 0; f < 4; ++f) {
+      int v[3] = {tets[4 * t + kFaceLocal[f][0]], tets[4 * t + kFaceLocal[f][1]], tets[4 * t + kFaceLocal[f][2]]};
+      std::sort(v, v + 3);
+      r.push_back({v[0], v[1], v[2], (int32_t)t, f});
+    }
+  auto key_less = [](const FaceKey& x, const FaceKey& y) {
+    if (x.a != y.a) return x.a < y.a;
+    if (x.b != y.b) return x.b < y.b;
+    if (x.c != y.c) return x.c < y.c;
+    if (x.tet != y.tet) return x.tet < y.tet;
+    return x.face < y.face;
+  };
+  std::sort(r.begin(), r.end(), key_less);
+  std::vector<FaceKey> keep;
+  for (size_t i = 0; i < r.size();) {
+    size_t j = i + 1;
+    while (j < r.size() && r[j].a == r[i].a && r[j].b == r[i].b && r[j].c == r[i].c) ++j;
+    if (j - i == 1) keep.push_back(r[i]);
+    i = j;
+  }
+  std::sort(keep.begin(), keep.end(), [](const FaceKey& x, const FaceKey& y) {
+    return x.tet != y.tet ? x.tet < y.tet : x.face < y.face;
+  });
+  for (const FaceKey& k : keep) {
+    const int64_t t = k.tet;
+    const int f = k.face;
+    const int32_t n0 = tets[4 * t + kFaceLocal[f][0]], n1 = tets[4 * t + kFaceLocal[f][1]],
+                  n2 = tets[4 * t + kFaceLocal[f][2]], no = tets[4 * t + kFaceOpp[f]];
+    const double *x0 = X + 3 * (int64_t)n0, *x1 = X + 3 * (int64_t)n1, *x2 = X + 3 * (int64_t)n2,
+                 *xo = X + 3 * (int64_t)no;
+    double e1[3], e2[3], eo[3], nr[3];
+    for (int i = 0; i < 3; ++i) {
+      e1[i] = x1[i] - x0[i];
+      e2[i] = x2[i] - x0[i];
+      eo[i] = xo[i] - x0[i];
+    }
+    nr[0] = e1[1] * e2[2] - e1[2] * e2[1];
+    nr[1] = e1[2] * e2[0] - e1[0] * e2[2];
+    nr[2] = e1[0] * e2[1] - e1[1] * e2[0];
+    const double s = nr[0] * eo[0] + nr[1] * eo[1] + nr[2] * eo[2];
+    fn.push_back(n0);
+    fn.push_back(s > 0.0 ? n2 : n1);
+    fn.push_back(s > 0.0 ? n1 : n2);
+    ft.push_back((int32_t)t);
+    fa.push_back(0.5 * std::sqrt(nr[0] * nr[0] + nr[1] * nr[1] + nr[2] * nr[2]));
+  }
+}
+
+// position of block (node a, node b) in the sliced-ELL layout
+static inline int sell_pos(const sdx_context* c, int64_t a, int64_t b) {
+  const int32_t* lo = c->h_pcol.data() + c->h_prow[a];
+  const int32_t* hi = c->h_pcol.data() + c->h_prow[a + 1];
+  const int32_t* it = std::lower_bound(lo, hi, (int32_t)b);
+  if (it == hi || *it != b) return -1;
+  const int k = (int)(it - lo);
+  const int64_t row = c->h_row_of_node[a];
+  return c->h_slice_ptr[row >> 5] + k * kSlice + (int)(row & 31);
+}
+
+static int choose_partition(sdx_context* c, int n_slices, const std::vector<int>& slice_env, int n_envs,
+                            const std::vector<int>& slice_ptr, PcgPartition& P, int threads_req,
+                            int ctas_per_sm_req) {
+  P.release();
+  const int threads = threads_req > 0 ? threads_req : 256;
+  const int max_active = pcg_max_ctas_per_sm(threads);
+  if (max_active <= 0) return set_error(SDX_ERR_CUDA, "PCG kernel cannot be resident with %d threads", threads);
+  // cooperative launch: every CTA must be co-resident (default 2 CTAs per SM)
+  const int per_sm = std::min(max_active, ctas_per_sm_req > 0 ? ctas_per_sm_req : 2);
+  int n_cta = c->num_sms * per_sm;
+  // each CTA may cover at most kPcgMaxEnvsPerCta envs; grow CTAs over weight-balanced slices
+  const int64_t total_w = slice_ptr[n_slices];
+  std::vector<int> cs(1, 0);
+  {
+    const double target = std::max(1.0, (double)total_w / n_cta);
+    int s = 0;
+    while (s < n_slices) {
+      int64_t w = 0;
+      int envs_seen = 0, last_env = -1;
+      while (s < n_slices) {
+        const int ev = slice_env[s];
+        if (ev != last_env) {
+          if (envs_seen == kPcgMaxEnvsPerCta) break;
+          envs_seen++;
+          last_env = ev;
+        }
+        w += slice_ptr[s + 1] - slice_ptr[s];
+        ++s;
+        if ((double)w >= target && (int)cs.size() < n_cta) break;
+      }
+      cs.push_back(s);
+    }
+  }
+  while ((int)cs.size() - 1 < n_cta) cs.push_back(n_slices);
+  if ((int)cs.size() - 1 > n_cta) {
+    return set_error(SDX_ERR_UNSUPPORTED, "too many small environments for %d persistent CTAs", n_cta);
+  }
+  std::vector<int> e0(n_cta), e1(n_cta), pbase(n_cta + 1, 0), ec0(n_envs, -1), ec1(n_envs, -1);
+  for (int k = 0; k < n_cta; ++k) {
+    if (cs[k + 1] > cs[k]) {
+      e0[k] = slice_env[cs[k]];
+      e1[k] = slice_env[cs[k + 1] - 1];
+      for (int ev = e0[k]; ev <= e1[k]; ++ev) {
+        if (ec0[ev] < 0) ec0[ev] = k;
+        ec1[ev] = k;
+      }
+    } else {
+      e0[k] = 0;
+      e1[k] = -1;
+    }
+    pbase[k + 1] = pbase[k] + std::max(0, e1[k] - e0[k] + 1);
+  }
+  for (int ev = 0; ev < n_envs; ++ev)
+    if (ec0[ev] < 0) {
+      ec0[ev] = 0;
+      ec1[ev] = -1;
+    }
+  SDX_TRY(upload(&P.cta_slice, cs));
+  SDX_TRY(upload(&P.cta_env0, e0));
+  SDX_TRY(upload(&P.cta_env1, e1));
+  SDX_TRY(upload(&P.cta_pbase, pbase));
+  SDX_TRY(upload(&P.env_cta0, ec0));
+  SDX_TRY(upload(&P.env_cta1, ec1));
+  SDX_TRY(dalloc(&P.part, (size_t)2 * std::max(1, pbase[n_cta]) * kPcgNq));
+  P.n_cta = n_cta;
+  P.threads = threads;
+  return SDX_OK;
+}
+
+static int alloc_work(PcgWork& W, int64_t n_rows, int n_envs) {
+  if (W.n_rows == n_rows && W.n_envs_alloc == n_envs) return SDX_OK;
+  W.release();
+  SDX_TRY(dalloc(&W.r, 3 * n_rows));
+  SDX_TRY(dalloc(&W.p, 3 * n_rows));
+  SDX_TRY(dalloc(&W.q, 3 * n_rows));
+  SDX_TRY(dalloc(&W.z, n_rows));
+  SDX_TRY(dalloc(&W.dinv, 9 * n_rows));
+  SDX_TRY(dalloc(&W.sync, 8));
+  SDX_TRY(dalloc(&W.out_iters, n_envs));
+  SDX_TRY(dalloc(&W.out_res, n_envs));
+  SDX_TRY(dalloc(&W.out_relres, n_envs));
+  SDX_TRY(dalloc(&W.out_conv, n_envs));
+  SDX_TRY(dalloc(&W.env_rel_tol, n_envs));
+  SDX_CUDA(cudaMemset(W.p, 0, sizeof(float) * 3 * n_rows));
+  SDX_CUDA(cudaMemset(W.q, 0, sizeof(float) * 3 * n_rows));
+  SDX_CUDA(cudaMemset(W.z, 0, sizeof(float4) * n_rows));
+  SDX_CUDA(cudaMemset(W.dinv, 0, sizeof(float) * 9 * n_rows));
+  W.n_rows = n_rows;
+  W.n_envs_alloc = n_envs;
+  return SDX_OK;
+}
+
+// Runs the persistent PCG on matrix A for the envs in env_mask (NULL = all), b -> x.
+static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_envs, PcgPartition& P,
+                   PcgWork& W, const double* b, double* x, const uint8_t* env_mask, int n_active,
+                   const sdx_linear_params& lp, bool zero_guess, const double* env_rel_tol) {
+  PcgArgs a;
+  memset(&a, 0, sizeof(a));
+  a.A = A;
+  a.n_envs = n_envs;
+  a.precond = lp.preconditioner;
+  a.diag_pos = diag_pos;
+  a.b = b;
+  a.x = x;
+  a.r = W.r;
+  a.p = W.p;
+  a.q = W.q;
+  a.z = W.z;
+  a.dinv = W.dinv;
+  a.cta_slice = P.cta_slice;
+  a.cta_env0 = P.cta_env0;
+  a.cta_env1 = P.cta_env1;
+  a.cta_pbase = P.cta_pbase;
+  a.env_cta0 = P.env_cta0;
+  a.env_cta1 = P.env_cta1;
+  a.part = P.part;
+  a.env_mask = env_mask;
+  a.rel_tol = lp.rel_tol;
+  a.abs_tol = lp.abs_tol;
+  a.rel_div_tol = lp.rel_div_tol;
+  a.max_iter = lp.max_iter;
+  a.polak_ribiere = lp.polak_ribiere;
+  a.replace_every = lp.replace_every > 0 ? lp.replace_every : 32;
+  a.zero_guess = zero_guess ? 1 : 0;
+  a.abort_spd = lp.abort_if_not_spd;
+  a.out_iters = W.out_iters;
+  a.out_res = W.out_res;
+  a.out_relres = W.out_relres;
+  a.out_conv = W.out_conv;
+  a.sync = W.sync;
+  a.env_rel_tol = env_rel_tol;
+  a.spin_limit = 1ll << 26;
+  unsigned init[8] = {0u, 0u, 0u, (unsigned)n_active, 0u, 0u, 0u, 0u};
+  SDX_CUDA(cudaMemcpyAsync(W.sync, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+  SDX_CUDA(cudaMemsetAsync(W.out_iters, 0, sizeof(int) * n_envs, c->stream));
+  SDX_CUDA(cudaMemsetAsync(W.out_conv, 0, sizeof(int) * n_envs, c->stream));
+  cudaError_t e = launch_pcg(a, P.n_cta, P.threads, c->stream);
+  c->launches++;
+  if (e != cudaSuccess) return set_error(SDX_ERR_CUDA, "PCG cooperative launch: %s", cudaGetErrorString(e));
+  unsigned flags[8];
+  SDX_CUDA(cudaMemcpyAsync(flags, W.sync, sizeof(flags), cudaMemcpyDeviceToHost, c->stream));
+  SDX_CUDA(cudaStreamSynchronize(c->stream));
+  if (flags[2] != 0u) return set_error(SDX_ERR_DEVICE_TIMEOUT, "PCG grid barrier timed out");
+  return SDX_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// C-ABI: misc
+
+extern "C" const char* sdx_last_error(void) { return g_last_error.c_str(); }
+extern "C" int sdx_version(void) { return 1; }
+
+extern "C" void sdx_default_linear_params(sdx_linear_params* p) {
+  p->rel_tol = 1e-6;
+  p->abs_tol = 1e-9;  // LinearSolverParams::absTol (linear_solver_params.h:370)
+  p->rel_div_tol = 1e10;
+  p->max_iter = 10000;
+  p->preconditioner = SDX_PREC_JACOBI;
+  p->abort_if_not_spd = 0;
+  p->polak_ribiere = 1;
+  p->replace_every = 32;
+}
+
+extern "C" void sdx_default_step_params(sdx_step_params* p) {
+  memset(p, 0, sizeof(*p));
+  p->dt = 1.0 / 240.0;
+  p->gravity[2] = -9.81;
+  p->psd_strategy = SDX_PSD_PROJECTION;
+  p->k_contact = 1e9;
+  p->t_half = 0.005;
+  p->thr = 0.001;
+  p->max_align = 0.0;
+  p->newton_max_iter = 50;
+  p->newton_rel_tol = 1e-6;
+  p->newton_abs_tol = 1e-3;
+  p->newton_rel_step_tol = 10.0 * 2.220446049250313e-16;
+  p->ls_max_iter = 4;
+  p->ls_alpha = 0.5;
+  p->ew_forcing = 0;
+  p->rel_div_tol = 1e4;
+  p->abs_div_tol = 1e9;
+  p->warm_start = SDX_WARM_ZERO;
+  sdx_default_linear_params(&p->linear);
+}
+
+extern "C" sdx_context* sdx_create(int device) {
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    set_error(SDX_ERR_CUDA, "no CUDA device: %s", cudaGetErrorString(e));
+    return nullptr;
+  }
+  if (device < 0 || device >= ndev) {
+    set_error(SDX_ERR_INVALID_ARGUMENT, "device %d out of range", device);
+    return nullptr;
+  }
+  if (cudaSetDevice(device) != cudaSuccess) {
+    set_error(SDX_ERR_CUDA, "cudaSetDevice failed");
+    return nullptr;
+  }
+  sdx_context* c = new sdx_context();
+  c->device = device;
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    set_error(SDX_ERR_CUDA, "stream creation failed");
+    return nullptr;
+  }
+  sdx_default_step_params(&c->params);
+  return c;
+}
+
+extern "C" int sdx_destroy(sdx_context* c) {
+  if (!c) return SDX_OK;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  release_topology(c);
+  release_solo(c);
+  cudaStreamDestroy(c->stream);
+  delete c;
+  return SDX_OK;
+}
+
+extern "C" int64_t sdx_kernel_launches(sdx_context* c) { return c ? c->launches : 0; }
+
+extern "C" int sdx_set_params(sdx_context* c, const sdx_step_params* p) {
+  if (!c || !p) return set_error(SDX_ERR_INVALID_ARGUMENT, "null argument");
+  if (!(p->dt > 0.0)) return set_error(SDX_ERR_INVALID_ARGUMENT, "dt must be positive");
+  if (p->linear.preconditioner < 0 || p->linear.preconditioner > 2)
+    return set_error(SDX_ERR_INVALID_ARGUMENT, "unknown preconditioner %d", p->linear.preconditioner);
+  c->params = *p;
+  return SDX_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// C-ABI: upload
+
+extern "C" int sdx_upload_bodies(sdx_context* c, int n_envs, const int64_t* node_off, const int64_t* tet_off,
+                                 const double* X, const int32_t* tets, const double* lambda, const double* mu,
+                                 const double* rho, const uint8_t* pin) {
+  if (!c || n_envs <= 0 || !node_off || !tet_off || !X || !tets || !lambda || !mu || !rho || !pin)
+    return set_error(SDX_ERR_INVALID_ARGUMENT, "null or empty argument to sdx_upload_bodies");
+  cudaSetDevice(c->device);
+  release_topology(c);
+  const int64_t N = node_off[n_envs], T = tet_off[n_envs];
+  if (node_off[0] != 0 || tet_off[0] != 0) return set_error(SDX_ERR_INVALID_ARGUMENT, "offsets must start at 0");
+  for (int e = 0; e < n_envs; ++e) {
+    if (node_off[e + 1] <= node_off[e] || tet_off[e + 1] < tet_off[e])
+      return set_error(SDX_ERR_INVALID_ARGUMENT, "env %d has no nodes or negative tet count", e);
+  }
+  for (int e = 0; e < n_envs; ++e)
+    for (int64_t t = tet_off[e]; t < tet_off[e + 1]; ++t)
+      for (int k = 0; k < 4; ++k) {
+        const int64_t nd = tets[4 * t + k];
+        if (nd < node_off[e] || nd >= node_off[e + 1])
+          return set_error(SDX_ERR_INVALID_ARGUMENT, "tet %lld references node %lld outside env %d",
+                           (long long)t, (long long)nd, e);
+      }
+  c->n_envs = n_envs;
+  c->n_nodes = N;
+  c->n_tets = T;
+  c->h_node_off.assign(node_off, node_off + n_envs + 1);
+  c->h_tet_off.assign(tet_off, tet_off + n_envs + 1);
+  // rows: per env padded to a multiple of 32
+  c->h_row_off.assign(n_envs + 1, 0);
+  for (int e = 0; e < n_envs; ++e) {
+    const int64_t n = node_off[e + 1] - node_off[e];
+    c->h_row_off[e + 1] = c->h_row_off[e] + ((n + kSlice - 1) / kSlice) * kSlice;
+  }
+  c->n_rows = c->h_row_off[n_envs];
+  if (c->n_rows >= (int64_t)1 << 31) return set_error(SDX_ERR_UNSUPPORTED, "more than 2^31 rows");
+  c->n_slices = (int)(c->n_rows / kSlice);
+  c->h_row_of_node.resize(N);
+  std::vector<int32_t> node_of_row(c->n_rows, -1);
+  for (int e = 0; e < n_envs; ++e)
+    for (int64_t i = node_off[e]; i < node_off[e + 1]; ++i) {
+      c->h_row_of_node[i] = (int32_t)(c->h_row_off[e] + (i - node_off[e]));
+      node_of_row[c->h_row_of_node[i]] = (int32_t)i;
+    }
+  c->h_slice_env.resize(c->n_slices);
+  for (int e = 0; e < n_envs; ++e)
+    for (int64_t s = c->h_row_off[e] / kSlice; s < c->h_row_off[e + 1] / kSlice; ++s) c->h_slice_env[s] = e;
+
+  // node -> incident tets
+  std::vector<int64_t> nt_ptr(N + 1, 0);
+  for (int64_t t = 0; t < T; ++t)
+    for (int k = 0; k < 4; ++k) nt_ptr[tets[4 * t + k] + 1]++;
+  for (int64_t i = 0; i < N; ++i) nt_ptr[i + 1] += nt_ptr[i];
+  std::vector<int32_t> nt(nt_ptr[N]);
+  {
+    std::vector<int64_t> fill(nt_ptr.begin(), nt_ptr.end() - 1);
+    for (int64_t t = 0; t < T; ++t)
+      for (int k = 0; k < 4; ++k) nt[fill[tets[4 * t + k]]++] = (int32_t)t;
+  }
+  // block pattern (sorted neighbour lists incl. the diagonal)
+  std::vector<int> deg(N);
+#pragma omp parallel
+  {
+    std::vector<int32_t> buf;
+#pragma omp for schedule(dynamic, 4096)
+    for (int64_t i = 0; i < N; ++i) {
+      buf.clear();
+      buf.push_back((int32_t)i);
+      for (int64_t k = nt_ptr[i]; k < nt_ptr[i + 1]; ++k)
+        for (int j = 0; j < 4; ++j) buf.push_back(tets[4 * (int64_t)nt[k] + j]);
+      std::sort(buf.begin(), buf.end());
+      deg[i] = (int)(std::unique(buf.begin(), buf.end()) - buf.begin());
+    }
+  }
+  c->h_prow.assign(N + 1, 0);
+  for (int64_t i = 0; i < N; ++i) c->h_prow[i + 1] = c->h_prow[i] + deg[i];
+  c->nnzb = c->h_prow[N];
+  c->h_pcol.resize(c->nnzb);
+#pragma omp parallel
+  {
+    std::vector<int32_t> buf;
+#pragma omp for schedule(dynamic, 4096)
+    for (int64_t i = 0; i < N; ++i) {
+      buf.clear();
+      buf.push_back((int32_t)i);
+      for (int64_t k = nt_ptr[i]; k < nt_ptr[i + 1]; ++k)
+        for (int j = 0; j < 4; ++j) buf.push_back(tets[4 * (int64_t)nt[k] + j]);
+      std::sort(buf.begin(), buf.end());
+      std::unique(buf.begin(), buf.end());
+      std::copy(buf.begin(), buf.begin() + deg[i], c->h_pcol.begin() + c->h_prow[i]);
+    }
+  }
+  // sliced-ELL layout
+  c->h_slice_ptr.assign(c->n_slices + 1, 0);
+  c->h_slice_w.assign(c->n_slices, 0);
+  for (int s = 0; s < c->n_slices; ++s) {
+    int w = 0;
+    for (int l = 0; l < kSlice; ++l) {
+      const int32_t nd = node_of_row[(int64_t)s * kSlice + l];
+      if (nd >= 0) w = std::max(w, deg[nd]);
+    }
+    c->h_slice_w[s] = w;
+    if ((int64_t)c->h_slice_ptr[s] + (int64_t)w * kSlice >= ((int64_t)1 << 31))
+      return set_error(SDX_ERR_UNSUPPORTED, "more than 2^31 block positions");
+    c->h_slice_ptr[s + 1] = c->h_slice_ptr[s] + w * kSlice;
+  }
+  c->nb_pad = c->h_slice_ptr[c->n_slices];
+  std::vector<int> hcol(c->nb_pad), hdiag(c->n_rows, -1);
+#pragma omp parallel for schedule(static)
+  for (int s = 0; s < c->n_slices; ++s) {
+    for (int l = 0; l < kSlice; ++l) {
+      const int64_t row = (int64_t)s * kSlice + l;
+      const int32_t nd = node_of_row[row];
+      const int len = nd >= 0 ? deg[nd] : 0;
+      for (int k = 0; k < c->h_slice_w[s]; ++k) {
+        const int p = c->h_slice_ptr[s] + k * kSlice + l;
+        if (k < len) {
+          const int32_t nb = c->h_pcol[c->h_prow[nd] + k];
+          hcol[p] = c->h_row_of_node[nb];
+          if (nb == nd) hdiag[row] = p;
+        } else {
+          hcol[p] = (int)(row | (int64_t)kPadBit);
+        }
+      }
+    }
+  }
+  // per tet: rows, rest data, scatter slots
+  std::vector<int4> htets(T);
+  std::vector<float4> hr[4];
+  std::vector<int4> hs[4];
+  for (int k = 0; k < 4; ++k) {
+    hr[k].resize(T);
+    hs[k].resize(T);
+  }
+  int bad_tet = -1;
+#pragma omp parallel for schedule(static)
+  for (int64_t t = 0; t < T; ++t) {
+    const int32_t* nd = tets + 4 * t;
+    htets[t] = make_int4(c->h_row_of_node[nd[0]], c->h_row_of_node[nd[1]], c->h_row_of_node[nd[2]],
+                         c->h_row_of_node[nd[3]]);
+    // rest data of a P1 tet with one quadrature point (finite_element.h:93-139)
+    const double* x0 = X + 3 * (int64_t)nd[0];
+    double D[9];
+    for (int k = 1; k <= 3; ++k) {
+      const double* xk = X + 3 * (int64_t)nd[k];
+      for (int r = 0; r < 3; ++r) D[r * 3 + (k - 1)] = xk[r] - x0[r];
+    }
+    const double det = D[0] * (D[4] * D[8] - D[5] * D[7]) - D[1] * (D[3] * D[8] - D[5] * D[6]) +
+                       D[2] * (D[3] * D[7] - D[4] * D[6]);
+    if (!(det > 0.0)) bad_tet = (int)t;
+    double cf[9];
+    cf[0] = D[4] * D[8] - D[5] * D[7];
+    cf[1] = D[5] * D[6] - D[3] * D[8];
+    cf[2] = D[3] * D[7] - D[4] * D[6];
+    cf[3] = D[2] * D[7] - D[1] * D[8];
+    cf[4] = D[0] * D[8] - D[2] * D[6];
+    cf[5] = D[1] * D[6] - D[0] * D[7];
+    cf[6] = D[1] * D[5] - D[2] * D[4];
+    cf[7] = D[2] * D[3] - D[0] * D[5];
+    cf[8] = D[0] * D[4] - D[1] * D[3];
+    double dN[12];
+    for (int f = 1; f <= 3; ++f)
+      for (int cc = 0; cc < 3; ++cc) dN[3 * f + cc] = cf[cc * 3 + (f - 1)] / det;
+    for (int cc = 0; cc < 3; ++cc) dN[cc] = -(dN[3 + cc] + dN[6 + cc] + dN[9 + cc]);
+    hr[0][t] = make_float4((float)dN[0], (float)dN[1], (float)dN[2], (float)dN[3]);
+    hr[1][t] = make_float4((float)dN[4], (float)dN[5], (float)dN[6], (float)dN[7]);
+    hr[2][t] = make_float4((float)dN[8], (float)dN[9], (float)dN[10], (float)dN[11]);
+    hr[3][t] = make_float4((float)(det / 6.0), (float)mu[t], (float)lambda[t], (float)rho[t]);
+    int sp[16];
+    for (int f = 0; f < 4; ++f)
+      for (int g = 0; g < 4; ++g) sp[f * 4 + g] = sell_pos(c, nd[f], nd[g]);
+    for (int k = 0; k < 4; ++k) hs[k][t] = make_int4(sp[4 * k], sp[4 * k + 1], sp[4 * k + 2], sp[4 * k + 3]);
+  }
+  if (bad_tet >= 0) return set_error(SDX_ERR_INVALID_ARGUMENT, "tet %d has non-positive rest volume", bad_tet);
+  for (int k = 0; k < 4; ++k)
+    for (int64_t t = 0; t < T; ++t) {
+      const int4 q = hs[k][t];
+      if (q.x < 0 || q.y < 0 || q.z < 0 || q.w < 0 || q.x >= c->nb_pad || q.y >= c->nb_pad || q.z >= c->nb_pad ||
+          q.w >= c->nb_pad)
+        return set_error(SDX_ERR_INVALID_ARGUMENT, "internal: tet %lld has no block slot", (long long)t);
+    }
+  // boundary faces (canonical order: owning tet, then local face) and their block slots
+  c->h_face_nodes.clear();
+  c->h_face_tet.clear();
+  c->h_face_area.clear();
+  {
+    std::vector<std::vector<int32_t>> fn(n_envs), ft(n_envs);
+    std::vector<std::vector<double>> fa(n_envs);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int e = 0; e < n_envs; ++e) boundary_faces_env(tet_off[e], tet_off[e + 1], tets, X, fn[e], ft[e], fa[e]);
+    for (int e = 0; e < n_envs; ++e) {
+      c->h_face_nodes.insert(c->h_face_nodes.end(), fn[e].begin(), fn[e].end());
+      c->h_face_tet.insert(c->h_face_tet.end(), ft[e].begin(), ft[e].end());
+      c->h_face_area.insert(c->h_face_area.end(), fa[e].begin(), fa[e].end());
+    }
+  }
+  c->n_faces = (int64_t)c->h_face_tet.size();
+  std::vector<int4> hfaces(c->n_faces);
+  std::vector<int> hfslots(9 * c->n_faces);
+  {
+    // env of each face from its owning tet
+    std::vector<int> tet_env_of_face(c->n_faces);
+    int e = 0;
+    for (int64_t f = 0; f < c->n_faces; ++f) {
+      while (c->h_face_tet[f] >= tet_off[e + 1]) ++e;
+      tet_env_of_face[f] = e;
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t f = 0; f < c->n_faces; ++f) {
+      const int32_t* fn = c->h_face_nodes.data() + 3 * f;
+      hfaces[f] = make_int4(c->h_row_of_node[fn[0]], c->h_row_of_node[fn[1]], c->h_row_of_node[fn[2]],
+                            tet_env_of_face[f]);
+      for (int k = 0; k < 3; ++k)
+        for (int l = 0; l < 3; ++l) hfslots[9 * f + 3 * k + l] = sell_pos(c, fn[k], fn[l]);
+    }
+  }
+  for (size_t i = 0; i < hfslots.size(); ++i)
+    if (hfslots[i] < 0 || hfslots[i] >= c->nb_pad)
+      return set_error(SDX_ERR_INVALID_ARGUMENT, "internal: face %zu has no block slot", i / 9);
+  // pins in row order, rest positions in row order
+  std::vector<uint8_t> hpin(c->n_rows, 0);
+  std::vector<double> hX(3 * c->n_rows, 0.0);
+  for (int64_t i = 0; i < N; ++i) {
+    hpin[c->h_row_of_node[i]] = pin[i] & 7;
+    for (int k = 0; k < 3; ++k) hX[3 * (int64_t)c->h_row_of_node[i] + k] = X[3 * i + k];
+  }
+  // device uploads
+  SDX_TRY(upload(&c->slice_ptr, c->h_slice_ptr));
+  SDX_TRY(upload(&c->slice_w, c->h_slice_w));
+  SDX_TRY(upload(&c->slice_env, c->h_slice_env));
+  SDX_TRY(upload(&c->col, hcol));
+  SDX_TRY(upload(&c->diag_pos, hdiag));
+  SDX_TRY(dalloc(&c->val, (size_t)9 * c->nb_pad));
+  SDX_TRY(dalloc(&c->mass, (size_t)c->nb_pad));
+  SDX_CUDA(cudaMemset(c->val, 0, sizeof(float) * 9 * (size_t)c->nb_pad));
+  SDX_CUDA(cudaMemset(c->mass, 0, sizeof(float) * (size_t)c->nb_pad));
+  SDX_TRY(upload(&c->tets, htets));
+  for (int k = 0; k < 4; ++k) {
+    SDX_TRY(upload(&c->rest[k], hr[k]));
+    SDX_TRY(upload(&c->slots[k], hs[k]));
+  }
+  SDX_TRY(upload(&c->pin, hpin));
+  SDX_TRY(upload(&c->X, hX));
+  SDX_TRY(upload(&c->faces, hfaces));
+  SDX_TRY(upload(&c->face_area, c->h_face_area));
+  SDX_TRY(upload(&c->face_slots, hfslots));
+  SDX_TRY(upload(&c->row_of_node, c->h_row_of_node));
+  const size_t n3 = (size_t)3 * c->n_rows;
+  for (double** pv : {&c->u, &c->v, &c->u0, &c->ut, &c->g, &c->dx, &c->ubase, &c->uscratch}) {
+    SDX_TRY(dalloc(pv, n3));
+    SDX_CUDA(cudaMemset(*pv, 0, sizeof(double) * n3));
+  }
+  SDX_TRY(dalloc(&c->staging, (size_t)3 * N));
+  SDX_TRY(dalloc(&c->env_norm, n_envs));
+  SDX_TRY(dalloc(&c->env_scale, n_envs));
+  SDX_TRY(dalloc(&c->env_obj, n_envs));
+  SDX_TRY(dalloc(&c->env_mask, n_envs));
+  SDX_TRY(dalloc(&c->env_pairs, n_envs));
+  SDX_TRY(dalloc(&c->pair_mask, 3 * c->n_faces));
+  SDX_CUDA(cudaMemset(c->pair_mask, 0, sizeof(unsigned) * 3 * std::max<int64_t>(1, c->n_faces)));
+  // no colliders until sdx_set_colliders
+  c->h_coll_off.assign(n_envs + 1, 0);
+  c->n_colliders = 0;
+  c->max_coll_per_env = 0;
+  SDX_TRY(upload(&c->coll_off, c->h_coll_off));
+  SDX_TRY(dalloc(&c->colliders, 11));
+  // mass couplings
+  const int4* sl[4] = {c->slots[0], c->slots[1], c->slots[2], c->slots[3]};
+  launch_mass_accum(T, sl, c->rest[3], c->mass, c->stream);
+  c->launches++;
+  // PCG partition and work
+  SDX_TRY(choose_partition(c, c->n_slices, c->h_slice_env, n_envs, c->h_slice_ptr, c->part, 0, 0));
+  SDX_TRY(alloc_work(c->work, c->n_rows, n_envs));
+  c->stats.assign(n_envs, sdx_env_stats{});
+  c->time = 0.0;
+  SDX_CUDA(cudaStreamSynchronize(c->stream));
+  c->uploaded = true;
+  return SDX_OK;
+}
+
+extern "C" int sdx_set_colliders(sdx_context* c, int n, const int32_t* env, const double* rows) {
+  if (!c || !c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
+  if (n < 0 || (n > 0 && (!env || !rows))) return set_error(SDX_ERR_INVALID_ARGUMENT, "bad collider arrays");
+  std::vector<int> off(c->n_envs + 1, 0);
+  for (int i = 0; i < n; ++i) {
+    if (env[i] < 0 || env[i] >= c->n_envs) return set_error(SDX_ERR_INVALID_ARGUMENT, "collider env out of range");
+    if (i > 0 && env[i] < env[i - 1]) return set_error(SDX_ERR_INVALID_ARGUMENT, "collider envs must be sorted");
+    const double ty = rows[11 * i];
+    if (ty != 0.0 && ty != 1.0) return set_error(SDX_ERR_INVALID_ARGUMENT, "unknown collider type");
+    off[env[i] + 1]++;
+  }
+  int mx = 0;
+  for (int e = 0; e < c->n_envs; ++e) {
+    mx = std::max(mx, off[e + 1]);
+    off[e + 1] += off[e];
+  }
+  if (mx > 32) return set_error(SDX_ERR_UNSUPPORTED, "at most 32 colliders per env");
+  dfree(c->coll_off);
+  dfree(c->colliders);
+  c->h_coll_off = off;
+  SDX_TRY(upload(&c->coll_off, off));
+  std::vector<double> h(rows, rows + 11 * (size_t)n);
+  if (h.empty()) h.assign(11, 0.0);
+  SDX_TRY(upload(&c->colliders, h));
+  c->n_colliders = n;
+  c->max_coll_per_env = mx;
+  return SDX_OK;
+}
+
+extern "C" int sdx_get_sizes(sdx_context* c, int64_t* n_nodes, int64_t* n_tets, int64_t* nnzb, int64_t* n_faces) {
+  if (!c || !c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
+  if (n_nodes) *n_nodes = c->n_nodes;
+  if (n_tets) *n_tets = c->n_tets;
+  if (nnzb) *nnzb = c->nnzb;
+  if (n_faces) *n_faces = c->n_faces;
+  return SDX_OK;
+}
+
+extern "C" int sdx_get_pattern(sdx_context* c, int64_t* row_ptr, int32_t* col) {
+  if (!c || !c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
+  if (row_ptr) std::copy(c->h_prow.begin(), c->h_prow.end(), row_ptr);
+  if (col) std::copy(c->h_pcol.begin(), c->h_pcol.end(), col);
+  return SDX_OK;
+}
+
+extern "C" int sdx_get_faces(sdx_context* c, int32_t* fn, int32_t* ft, double* fa) {
+  if (!c || !c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
+  if (fn) std::copy(c->h_face_nodes.begin(), c->h_face_nodes.end(), fn);
+  if (ft) std::copy(c->h_face_tet.begin(), c->h_face_tet.end(), ft);
+  if (fa) std::copy(c->h_face_area.begin(), c->h_face_area.end(), fa);
+  return SDX_OK;
+}
+
+extern "C" int sdx_set_state(sdx_context* c, const double* u, const double* v, double time) {
+  if (!c || !c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
+  cudaSetDevice(c->device);
+  if (u) SDX_TRY(h2d_rows(c, u, c->u));
+  if (v) SDX_TRY(h2d_rows(c, v, c->v));
+  c->time = time;
+  return SDX_OK;
+}
+
+extern "C" int sdx_get_state(sdx_context* c, double* u, double* v, double* time) {
+  if (!c || !c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
+  cudaSetDevice(c->device);
+  if (u) SDX_TRY(d2h_rows(c, c->u, u));
+  if (v) SDX_TRY(d2h_rows(c, c->v, v));
+  if (time) *time = c->time;
+  return SDX_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// assembly
+
+static Matrix ctx_matrix(sdx_context* c) {
+  Matrix A;
+  A.n_slices = c->n_slices;
+  A.slice_ptr = c->slice_ptr;
+  A.slice_w = c->slice_w;
+  A.slice_env = c->slice_env;
+  A.col = c->col;
+  A.val = c->val;
+  return A;
+}
+
+// Assembles into c->g / c->val / c->env_obj for the envs in mask (device array, NULL = all).
+static void assemble_dev(sdx_context* c, const double* u, const double* ut, double t, int flags,
+                         const uint8_t* mask, bool record_pairs) {
+  const sdx_step_params& p = c->params;
+  const double dtfi2 = 1.0 / (p.dt * p.dt);
+  if (flags & SDX_ASM_RES) {
+    launch_zero_rows(c->n_slices, c->slice_env, mask, c->g, c->stream);
+    c->launches++;
+  }
+  if (flags & SDX_ASM_HESS) {
+    launch_seed_hessian(ctx_matrix(c), c->mass, c->pin, mask, (float)dtfi2, c->stream);
+    c->launches++;
+  }
+  ElemArgs ea;
+  memset(&ea, 0, sizeof(ea));
+  ea.n_tets = c->n_tets;
+  ea.tets = c->tets;
+  ea.rest0 = c->rest[0];
+  ea.rest1 = c->rest[1];
+  ea.rest2 = c->rest[2];
+  ea.rest3 = c->rest[3];
+  ea.slots0 = c->slots[0];
+  ea.slots1 = c->slots[1];
+  ea.slots2 = c->slots[2];
+  ea.slots3 = c->slots[3];
+  ea.slice_env = c->slice_env;
+  ea.env_mask = mask;
+  ea.u = u;
+  ea.ut = ut;
+  ea.X = c->X;
+  ea.pin = c->pin;
+  ea.g = c->g;
+  ea.val = c->val;
+  ea.obj = c->env_obj;
+  ea.dtfi2 = dtfi2;
+  for (int k = 0; k < 3; ++k) ea.grav[k] = p.gravity[k];
+  ea.min_eig = 1.1920928955078125e-07f;  // kMinProjectedEigenvalue of the FP32 build
+  ea.psd = p.psd_strategy;
+  ea.flags = flags;
+  launch_element(ea, c->stream);
+  c->launches++;
+  if (c->n_colliders > 0 || record_pairs) {
+    ContactArgs ca;
+    memset(&ca, 0, sizeof(ca));
+    ca.n_samples = 3 * c->n_faces;
+    ca.faces = c->faces;
+    ca.face_area = c->face_area;
+    ca.face_slots = c->face_slots;
+    ca.colliders = c->colliders;
+    ca.coll_off = c->coll_off;
+    ca.env_mask = mask;
+    ca.u = u;
+    ca.X = c->X;
+    ca.pin = c->pin;
+    ca.g = c->g;
+    ca.val = c->val;
+    ca.obj = c->env_obj;
+    ca.pair_mask = record_pairs ? c->pair_mask : nullptr;
+    ca.n_pairs = c->env_pairs;
+    ca.t = t;
+    ca.k = p.k_contact;
+    ca.t_half = p.t_half;
+    ca.thr = p.thr;
+    ca.max_align = p.max_align;
+    ca.flags = flags;
+    launch_contact(ca, c->stream);
+    c->launches++;
+  }
+}
+
+extern "C" int sdx_assemble(sdx_context* c, const double* u, double t, int flags, double* obj, double* g,
+                            float* hess, int64_t* n_pairs) {
+  if (!c || !c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
+  cudaSetDevice(c->device);
+  const int64_t n3 = 3 * c->n_rows;
+  const double* ud = c->u;
+  if (u) {
+    SDX_CUDA(cudaMemsetAsync(c->uscratch, 0, sizeof(double) * n3, c->stream));
+    SDX_TRY(h2d_rows(c, u, c->uscratch));
+    ud = c->uscratch;
+  }
+  launch_pred(n3, c->u, c->v, c->params.dt, c->ut, c->u0, c->stream);
+  c->launches++;
+  SDX_CUDA(cudaMemsetAsync(c->env_obj, 0, sizeof(double) * c->n_envs, c->stream));
+  SDX_CUDA(cudaMemsetAsync(c->env_pairs, 0, sizeof(unsigned long long) * c->n_envs, c->stream));
+  assemble_dev(c, ud, c->ut, t, flags | SDX_ASM_RES | (hess ? SDX_ASM_HESS : 0), nullptr, true);
+  SDX_CUDA(cudaGetLastError());
+  if (obj) SDX_CUDA(cudaMemcpyAsync(obj, c->env_obj, sizeof(double) * c->n_envs, cudaMemcpyDeviceToHost, c->stream));
+  if (n_pairs) {
+    std::vector<unsigned long long> tmp(c->n_envs);
+    SDX_CUDA(cudaMemcpyAsync(tmp.data(), c->env_pairs, sizeof(unsigned long long) * c->n_envs,
+                             cudaMemcpyDeviceToHost, c->stream));
+    SDX_CUDA(cudaStreamSynchronize(c->stream));
+    for (int e = 0; e < c->n_envs; ++e) n_pairs[e] = (int64_t)tmp[e];
+  }
+  if (g) SDX_TRY(d2h_rows(c, c->g, g));
+  if (hess) {
+    std::vector<float> hv((size_t)9 * c->nb_pad);
+    SDX_CUDA(cudaMemcpyAsync(hv.data(), c->val, sizeof(float) * hv.size(), cudaMemcpyDeviceToHost, c->stream));
+    SDX_CUDA(cudaStreamSynchronize(c->stream));
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < c->n_nodes; ++i) {
+      const int64_t row = c->h_row_of_node[i];
+      const int s = (int)(row >> 5), l = (int)(row & 31);
+      for (int64_t b = c->h_prow[i]; b < c->h_prow[i + 1]; ++b) {
+        const int k = (int)(b - c->h_prow[i]);
+        const int64_t pos = c->h_slice_ptr[s] + k * kSlice + l;
+        for (int e = 0; e < 9; ++e) hess[9 * b + e] = hv[val_index(pos, e)];
+      }
+    }
+  }
+  SDX_CUDA(cudaStreamSynchronize(c->stream));
+  return SDX_OK;
+}
+
+extern "C" int sdx_get_contact_pairs(sdx_context* c, int64_t* pairs, int64_t cap, int64_t* n_pairs) {
+  if (!c || !c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
+  const int64_t ns = 3 * c->n_faces;
+  std::vector<unsigned> m(std::max<int64_t>(1, ns));
+  SDX_CUDA(cudaMemcpyAsync(m.data(), c->pair_mask, sizeof(unsigned) * ns, cudaMemcpyDeviceToHost, c->stream));
+  SDX_CUDA(cudaStreamSynchronize(c->stream));
+  // samples are env-contiguous; key = local sample index within the env * max colliders + local collider
+  int64_t n = 0;
+  int e = 0;
+  int64_t f_env0 = 0;
+  const int K = std::max(1, c->max_coll_per_env);
+  for (int64_t s = 0; s < ns; ++s) {
+    const int64_t f = s / 3;
+    while (c->h_face_tet[f] >= c->h_tet_off[e + 1]) {
+      ++e;
+      f_env0 = f;
+    }
+    unsigned bits = m[s];
+    while (bits) {
+      const int b = __builtin_ctz(bits);
+      bits &= bits - 1;
+      if (pairs && n < cap) pairs[n] = (s - 3 * f_env0) * K + b;
+      ++n;
+    }
+  }
+  if (n_pairs) *n_pairs = n;
+  return SDX_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Newton step (NewtonSolver<T>::Solve, newton_solver.cpp:603-876, batched over envs)
+
+static int env_dot_host(sdx_context* c, const double* a, const double* b, const uint8_t* mask,
+                        std::vector<double>& out) {
+  SDX_CUDA(cudaMemsetAsync(c->env_norm, 0, sizeof(double) * c->n_envs, c->stream));
+  launch_env_dot(c->n_slices, c->slice_env, mask, a, b, c->env_norm, c->stream);
+  c->launches++;
+  out.resize(c->n_envs);
+  SDX_CUDA(cudaMemcpyAsync(out.data(), c->env_norm, sizeof(double) * c->n_envs, cudaMemcpyDeviceToHost, c->stream));
+  SDX_CUDA(cudaStreamSynchronize(c->stream));
+  return SDX_OK;
+}
+
+static int upload_mask(sdx_context* c, const std::vector<uint8_t>& m) {
+  SDX_CUDA(cudaMemcpyAsync(c->env_mask, m.data(), m.size(), cudaMemcpyHostToDevice, c->stream));
+  return SDX_OK;
+}
+
+static int step_once(sdx_context* c) {
+  const sdx_step_params& p = c->params;
+  const int E = c->n_envs;
+  const int64_t n3 = 3 * c->n_rows;
+  const double t_end = c->time + p.dt;
+  launch_pred(n3, c->u, c->v, p.dt, c->ut, c->u0, c->stream);
+  c->launches++;
+  std::vector<int> status(E, 0), iters(E, 0), cg(E, 0), lsi(E, 0);
+  std::vector<double> res0(E, 0.0), res(E, 0.0), res_prev(E, 0.0), dxn(E, 0.0), eta(E, p.linear.rel_tol);
+  std::vector<uint8_t> mask(E, 1), lsmask(E, 0);
+  std::vector<double> nrm, scale(E, 1.0);
+  SDX_CUDA(cudaMemsetAsync(c->env_pairs, 0, sizeof(unsigned long long) * E, c->stream));
+  SDX_TRY(upload_mask(c, mask));
+  assemble_dev(c, c->u, c->ut, t_end, SDX_ASM_RES | SDX_ASM_HESS | SDX_ASM_PSD, c->env_mask, false);
+  SDX_TRY(env_dot_host(c, c->g, c->g, c->env_mask, nrm));
+  for (int e = 0; e < E; ++e) res[e] = std::sqrt(nrm[e]);
+  bool first_pass = true;
+  std::vector<double> unorm;
+  for (;;) {
+    // stop criteria in the reference order (newton_solver.cpp:303-313)
+    bool need_unorm = false;
+    for (int e = 0; e < E; ++e)
+      if (status[e] == 0 && iters[e] > 0) need_unorm = true;
+    if (need_unorm) SDX_TRY(env_dot_host(c, c->u, c->u, nullptr, unorm));
+    int n_active = 0;
+    for (int e = 0; e < E; ++e) {
+      mask[e] = 0;
+      if (status[e] != 0) continue;
+      if (iters[e] == 0) res0[e] = res[e];
+      if (res[e] <= p.newton_abs_tol || (iters[e] > 0 && res[e] <= p.newton_rel_tol * res0[e])) {
+        status[e] = 1;
+        continue;
+      }
+      if (iters[e] >= p.newton_max_iter) {
+        status[e] = 2;
+        continue;
+      }
+      if (iters[e] > 0 && dxn[e] <= p.newton_rel_step_tol * std::sqrt(unorm[e])) {
+        status[e] = 2;
+        continue;
+      }
+      if (p.ew_forcing == 2) {  // Eisenstat-Walker choice 2 (newton_solver.cpp:452-468)
+        const double kMax = 0.01, kSafe = 0.01, kMin = 100.0 * 2.220446049250313e-16;
+        if (iters[e] == 0) {
+          eta[e] = kMax;
+        } else {
+          const double al = 0.5 + 0.5 * std::sqrt(5.0), gam = 0.9;
+          const double safe = gam * std::pow(eta[e], al);
+          double v = gam * std::pow(res[e] / res_prev[e], al);
+          if (safe > kSafe) v = std::max(v, safe);
+          eta[e] = std::min(std::max(v, kMin), kMax);
+        }
+      }
+      res_prev[e] = res[e];
+      iters[e]++;
+      mask[e] = 1;
+      n_active++;
+    }
+    if (n_active == 0) break;
+    SDX_TRY(upload_mask(c, mask));
+    if (!first_pass) assemble_dev(c, c->u, c->ut, t_end, SDX_ASM_HESS | SDX_ASM_PSD, c->env_mask, false);
+    // linear solve H dx = g
+    const bool zero = p.warm_start == SDX_WARM_ZERO;
+    if (p.ew_forcing == 2)
+      SDX_CUDA(cudaMemcpyAsync(c->work.env_rel_tol, eta.data(), sizeof(double) * E, cudaMemcpyHostToDevice, c->stream));
+    SDX_TRY(run_pcg(c, ctx_matrix(c), c->diag_pos, E, c->part, c->work, c->g, c->dx, c->env_mask, n_active,
+                    p.linear, zero, p.ew_forcing == 2 ? c->work.env_rel_tol : nullptr));
+    std::vector<int> it_out(E);
+    SDX_CUDA(cudaMemcpy(it_out.data(), c->work.out_iters, sizeof(int) * E, cudaMemcpyDeviceToHost));
+    for (int e = 0; e < E; ++e)
+      if (mask[e]) cg[e] += it_out[e];
+    SDX_TRY(env_dot_host(c, c->dx, c->dx, c->env_mask, nrm));
+    for (int e = 0; e < E; ++e)
+      if (mask[e]) dxn[e] = std::sqrt(nrm[e]);
+    // ResidualNorm line search along -dx (line_search.h:300-336)
+    launch_copy_rows(c->n_slices, c->slice_env, c->env_mask, c->u, c->ubase, c->stream);
+    c->launches++;
+    lsmask = mask;
+    for (int e = 0; e < E; ++e) scale[e] = 1.0;
+    for (int it = 0; it < p.ls_max_iter; ++it) {
+      if (it > 0)
+        for (int e = 0; e < E; ++e)
+          if (lsmask[e]) scale[e] *= p.ls_alpha;
+      SDX_TRY(upload_mask(c, lsmask));
+      SDX_CUDA(cudaMemcpyAsync(c->env_scale, scale.data(), sizeof(double) * E, cudaMemcpyHostToDevice, c->stream));
+      launch_ls_candidate(c->n_slices, c->slice_env, c->env_mask, c->ubase, c->dx, c->env_scale, c->u, c->stream);
+      c->launches++;
+      SDX_CUDA(cudaMemsetAsync(c->env_pairs, 0, sizeof(unsigned long long) * E, c->stream));
+      assemble_dev(c, c->u, c->ut, t_end, SDX_ASM_RES, c->env_mask, false);
+      SDX_TRY(env_dot_host(c, c->g, c->g, c->env_mask, nrm));
+      int left = 0;
+      for (int e = 0; e < E; ++e) {
+        if (!lsmask[e]) continue;
+        lsi[e]++;
+        const double rn = std::sqrt(nrm[e]);
+        if (rn <= res[e]) {
+          lsmask[e] = 0;
+        } else {
+          left++;
+        }
+        res[e] = (rn <= res[e]) ? rn : res[e];
+        // keep the evaluated norm for explosion control of the final iterate
+        if (it == p.ls_max_iter - 1 && lsmask[e]) res[e] = rn;
+      }
+      if (left == 0) break;
+    }
+    // explosion control (newton_solver.cpp:841-874)
+    for (int e = 0; e < E; ++e) {
+      if (!mask[e]) continue;
+      if (res[e] > p.rel_div_tol * res0[e] || res[e] > p.abs_div_tol || !std::isfinite(res[e])) status[e] = 3;
+    }
+    first_pass = false;
+  }
+  launch_velocity(n3, c->u, c->u0, p.dt, c->v, c->stream);
+  c->launches++;
+  std::vector<unsigned long long> pairs(E);
+  SDX_CUDA(cudaMemcpyAsync(pairs.data(), c->env_pairs, sizeof(unsigned long long) * E, cudaMemcpyDeviceToHost, c->stream));
+  SDX_CUDA(cudaStreamSynchronize(c->stream));
+  for (int e = 0; e < E; ++e) {
+    sdx_env_stats& s = c->stats[e];
+    s.newton_iters = iters[e];
+    s.cg_iters = cg[e];
+    s.ls_iters = lsi[e];
+    s.convergence = status[e];
+    s.res_norm0 = res0[e];
+    s.res_norm = res[e];
+    s.n_contacts = (int64_t)pairs[e];
+  }
+  c->time = t_end;
+  return SDX_OK;
+}
+
+extern "C" int sdx_step(sdx_context* c, int n_steps) {
+  if (!c || !c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
+  if (n_steps < 0) return set_error(SDX_ERR_INVALID_ARGUMENT, "negative step count");
+  cudaSetDevice(c->device);
+  for (int k = 0; k < n_steps; ++k) SDX_TRY(step_once(c));
+  SDX_CUDA(cudaGetLastError());
+  return SDX_OK;
+}
+
+extern "C" int sdx_get_stats(sdx_context* c, sdx_env_stats* per_env) {
+  if (!c || !c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
+  if (per_env) std::copy(c->stats.begin(), c->stats.end(), per_env);
+  return SDX_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// SpMV benchmark on the context's matrix
+
+extern "C" int sdx_bench_spmv(sdx_context* c, int reps, double* ms, double* bytes) {
+  if (!c || !c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
+  cudaSetDevice(c->device);
+  float4* x = nullptr;
+  float* y = nullptr;
+  SDX_TRY(dalloc(&x, c->n_rows));
+  SDX_TRY(dalloc(&y, 3 * c->n_rows));
+  launch_pack_z(c->n_rows, c->u, x, c->stream);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  for (int i = 0; i < 3; ++i) launch_spmv(ctx_matrix(c), x, y, 256, c->stream);
+  cudaEventRecord(e0, c->stream);
+  for (int i = 0; i < reps; ++i) launch_spmv(ctx_matrix(c), x, y, 256, c->stream);
+  cudaEventRecord(e1, c->stream);
+  cudaEventSynchronize(e1);
+  float t = 0.0f;
+  cudaEventElapsedTime(&t, e0, e1);
+  c->launches += 3 + reps + 1;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  dfree(x);
+  dfree(y);
+  SDX_CUDA(cudaGetLastError());
+  if (ms) *ms = t / std::max(1, reps);
+  // algorithmic bytes: nnzb (9 values + 1 index) + row pointers + x read once + y written
+  if (bytes) *bytes = (double)c->nnzb * (9 * 4 + 4) + 4.0 * (c->n_nodes + 1) + 12.0 * c->n_nodes + 12.0 * c->n_nodes;
+  return SDX_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// standalone linear solve (LinearSolver<T>::Solve -> CudaIterativeSolve, linear_solver.h:614-662)
+
+extern "C" int sdx_pcg_solve_ctx(sdx_context* c, int n, int64_t nnzb, const int64_t* row_ptr, const int32_t* bcol,
+                                 const void* values, int value_type, const double* b, double* x, int hint,
+                                 const sdx_linear_params* lp, sdx_linear_status* status) {
+  if (!c || n <= 0 || nnzb <= 0 || !row_ptr || !bcol || !values || !b || !x || !lp || !status)
+    return set_error(SDX_ERR_INVALID_ARGUMENT, "null or empty argument to sdx_pcg_solve");
+  if (value_type != SDX_F32 && value_type != SDX_F64) return set_error(SDX_ERR_INVALID_ARGUMENT, "value_type");
+  if (lp->preconditioner < 0 || lp->preconditioner > 2) return set_error(SDX_ERR_INVALID_ARGUMENT, "preconditioner");
+  if (lp->max_iter <= 0) return set_error(SDX_ERR_INVALID_ARGUMENT, "max_iter must be positive");
+  if (row_ptr[0] != 0 || row_ptr[n] != nnzb) return set_error(SDX_ERR_INVALID_ARGUMENT, "row_ptr inconsistent with nnzb");
+  for (int i = 0; i < n; ++i) {
+    if (row_ptr[i + 1] < row_ptr[i]) return set_error(SDX_ERR_INVALID_ARGUMENT, "row_ptr not monotone");
+    for (int64_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
+      if (bcol[k] < 0 || bcol[k] >= n) return set_error(SDX_ERR_INVALID_ARGUMENT, "column index out of range");
+  }
+  cudaSetDevice(c->device);
+  const int rows = ((n + kSlice - 1) / kSlice) * kSlice;
+  const int ns = rows / kSlice;
+  std::vector<int> sp(ns + 1, 0), sw(ns, 0), se(ns, 0);
+  for (int s = 0; s < ns; ++s) {
+    int w = 0;
+    for (int l = 0; l < kSlice; ++l) {
+      const int r = s * kSlice + l;
+      if (r < n) w = std::max<int>(w, (int)(row_ptr[r + 1] - row_ptr[r]));
+    }
+    sw[s] = w;
+    if ((int64_t)sp[s] + (int64_t)w * kSlice >= ((int64_t)1 << 31)) return set_error(SDX_ERR_UNSUPPORTED, "matrix too large");
+    sp[s + 1] = sp[s] + w * kSlice;
+  }
+  const int64_t nbp = sp[ns];
+  if (c->solo_rows != rows || c->solo_nb != nbp) {
+    release_solo(c);
+    SDX_TRY(dalloc(&c->solo_slice_ptr, ns + 1));
+    SDX_TRY(dalloc(&c->solo_slice_w, ns));
+    SDX_TRY(dalloc(&c->solo_slice_env, ns));
+    SDX_TRY(dalloc(&c->solo_col, nbp));
+    SDX_TRY(dalloc(&c->solo_diag, rows));
+    SDX_TRY(dalloc(&c->solo_val, (size_t)9 * nbp));
+    SDX_TRY(dalloc(&c->solo_b, (size_t)3 * rows));
+    SDX_TRY(dalloc(&c->solo_x, (size_t)3 * rows));
+    SDX_TRY(choose_partition(c, ns, se, 1, sp, c->solo_part, 0, 0));
+    SDX_TRY(alloc_work(c->solo_work, rows, 1));
+    c->solo_rows = rows;
+    c->solo_nb = nbp;
+  }
+  SDX_CUDA(cudaMemcpyAsync(c->solo_slice_ptr, sp.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(c->solo_slice_w, sw.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(c->solo_slice_env, se.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, c->stream));
+  // upload BSR (FP32) and convert on device (the reference converts to cuSPARSE BSR, cuda_bsr_matrix.cu:22-63)
+  int64_t* drp = nullptr;
+  int32_t* dbc = nullptr;
+  float* dbv = nullptr;
+  SDX_TRY(dalloc(&drp, (size_t)rows + 1));
+  SDX_TRY(dalloc(&dbc, (size_t)nnzb));
+  SDX_TRY(dalloc(&dbv, (size_t)9 * nnzb));
+  std::vector<int64_t> rp(rows + 1);
+  for (int i = 0; i <= rows; ++i) rp[i] = row_ptr[std::min(i, n)];
+  SDX_CUDA(cudaMemcpyAsync(drp, rp.data(), sizeof(int64_t) * (rows + 1), cudaMemcpyHostToDevice, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(dbc, bcol, sizeof(int32_t) * nnzb, cudaMemcpyHostToDevice, c->stream));
+  std::vector<float> fv;
+  if (value_type == SDX_F64) {
+    fv.resize((size_t)9 * nnzb);
+    const double* dv = (const double*)values;
+    for (size_t i = 0; i < fv.size(); ++i) fv[i] = (float)dv[i];
+    SDX_CUDA(cudaMemcpyAsync(dbv, fv.data(), sizeof(float) * fv.size(), cudaMemcpyHostToDevice, c->stream));
+  } else {
+    SDX_CUDA(cudaMemcpyAsync(dbv, values, sizeof(float) * 9 * nnzb, cudaMemcpyHostToDevice, c->stream));
+  }
+  launch_bsr_to_sell(rows, drp, dbc, dbv, c->solo_slice_ptr, c->solo_col, c->solo_val, c->solo_diag, c->stream);
+  c->launches++;
+  std::vector<double> hb((size_t)3 * rows, 0.0), hx((size_t)3 * rows, 0.0);
+  std::copy(b, b + 3 * (size_t)n, hb.begin());
+  if (hint != SDX_GUESS_ZERO) std::copy(x, x + 3 * (size_t)n, hx.begin());
+  SDX_CUDA(cudaMemcpyAsync(c->solo_b, hb.data(), sizeof(double) * hb.size(), cudaMemcpyHostToDevice, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(c->solo_x, hx.data(), sizeof(double) * hx.size(), cudaMemcpyHostToDevice, c->stream));
+  Matrix A;
+  A.n_slices = ns;
+  A.slice_ptr = c->solo_slice_ptr;
+  A.slice_w = c->solo_slice_w;
+  A.slice_env = c->solo_slice_env;
+  A.col = c->solo_col;
+  A.val = c->solo_val;
+  int rc = run_pcg(c, A, c->solo_diag, 1, c->solo_part, c->solo_work, c->solo_b, c->solo_x, nullptr, 1, *lp,
+                   hint == SDX_GUESS_ZERO, nullptr);
+  dfree(drp);
+  dfree(dbc);
+  dfree(dbv);
+  if (rc != SDX_OK) return rc;
+  SDX_CUDA(cudaMemcpyAsync(hx.data(), c->solo_x, sizeof(double) * hx.size(), cudaMemcpyDeviceToHost, c->stream));
+  int it = 0, conv = 0;
+  double res = 0.0, rel = 0.0;
+  SDX_CUDA(cudaMemcpyAsync(&it, c->solo_work.out_iters, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(&conv, c->solo_work.out_conv, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(&res, c->solo_work.out_res, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(&rel, c->solo_work.out_relres, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  SDX_CUDA(cudaStreamSynchronize(c->stream));
+  std::copy(hx.begin(), hx.begin() + 3 * (size_t)n, x);
+  status->num_iter = it;
+  status->residual_norm = res;
+  status->relative_residual_norm = rel;
+  status->convergence = conv;
+  return SDX_OK;
+}
+
+extern "C" int sdx_pcg_solve(int n, int64_t nnzb, const int64_t* row_ptr, const int32_t* col, const void* values,
+                             int value_type, const double* b, double* x, int hint, const sdx_linear_params* lp,
+                             sdx_linear_status* status) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  sdx_context* c = sdx_create(dev);
+  if (!c) return SDX_ERR_CUDA;
+  int rc = sdx_pcg_solve_ctx(c, n, nnzb, row_ptr, col, values, value_type, b, x, hint, lp, status);
+  std::string err = g_last_error;
+  sdx_destroy(c);
+  g_last_error = err;
+  return rc;
+}

@@ -1,0 +1,148 @@
+// sdx_internal.cuh — kernel argument blocks and launch wrappers shared by the host runtime and the
+// kernels of libsdx_b200.so.
+//
+// HBM layout (all envs of a batch live in one set of arrays, CSR-of-environments):
+//   * rows: each env's nodes occupy a contiguous range of "rows" padded to a multiple of 32, so a
+//     32-row slice belongs to exactly one env. Vectors are indexed by row (3 components per row).
+//   * matrix: 3x3 sliced-ELL ("SELL-32 of 3x3 blocks"). Slice s covers rows [32s, 32s+32) and has
+//     width w_s = the longest block row in it. Block position p = slice_ptr[s] + 32k + lane holds the
+//     k-th block of row 32s+lane; its column is col[p] (padding: row | 0x80000000) and its 9 values
+//     are interleaved per (slice, k) group: val[(p - lane) * 9 + 32 e + lane], e = 3r + c. A warp
+//     reading one (slice, k) group loads 9 fully coalesced 128-byte lines.
+//   * per tet: int4 rows, 4 float4 rest records (dN 12, vol, mu, lambda, rho) stored as 4 separate
+//     float4 arrays (coalesced), 4 int4 records of the 16 block positions its 4x4 blocks scatter to.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sdx {
+
+constexpr int kSlice = 32;
+constexpr int kPadBit = 0x80000000;
+constexpr int kPcgMaxEnvsPerCta = 32;
+constexpr int kPcgNq = 3;
+
+__host__ __device__ __forceinline__ size_t val_index(int64_t p, int e) {
+  return (size_t)(p - (p & 31)) * 9 + (size_t)e * 32 + (size_t)(p & 31);
+}
+
+struct Matrix {
+  int n_slices;
+  const int* slice_ptr;  // n_slices + 1, in block positions
+  const int* slice_w;
+  const int* slice_env;
+  const int* col;
+  float* val;
+};
+
+struct ElemArgs {
+  int64_t n_tets;
+  const int4* tets;
+  const float4* rest0;
+  const float4* rest1;
+  const float4* rest2;
+  const float4* rest3;
+  const int4* slots0;
+  const int4* slots1;
+  const int4* slots2;
+  const int4* slots3;
+  const int* slice_env;
+  const uint8_t* env_mask;  // NULL = all
+  const double* u;
+  const double* ut;
+  const double* X;
+  const uint8_t* pin;
+  double* g;
+  float* val;
+  double* obj;  // per env
+  double dtfi2;
+  double grav[3];
+  float min_eig;
+  int psd;
+  int flags;
+};
+
+struct ContactArgs {
+  int64_t n_samples;
+  const int4* faces;  // 3 rows + env
+  const double* face_area;
+  const int* face_slots;  // 9 per face
+  const double* colliders;  // 11 per collider
+  const int* coll_off;      // per env
+  const uint8_t* env_mask;
+  const double* u;
+  const double* X;
+  const uint8_t* pin;
+  double* g;
+  float* val;
+  double* obj;
+  unsigned* pair_mask;      // per sample (NULL: not recorded)
+  unsigned long long* n_pairs;  // per env
+  double t, k, t_half, thr, max_align;
+  int flags;
+};
+
+struct PcgArgs {
+  Matrix A;
+  int n_envs;
+  int precond;  // 0 none, 1 Jacobi, 2 block Jacobi
+  const int* diag_pos;
+  const double* b;
+  double* x;
+  double* r;
+  float* p;
+  float* q;
+  float4* z;
+  float* dinv;  // 3 per row (Jacobi) or 9 per row (block Jacobi)
+  const int* cta_slice;
+  const int* cta_env0;
+  const int* cta_env1;
+  const int* cta_pbase;
+  const int* env_cta0;
+  const int* env_cta1;
+  double* part;
+  const uint8_t* env_mask;
+  const double* env_rel_tol;  // per-env relative tolerance (NULL: rel_tol)
+  double rel_tol, abs_tol, rel_div_tol;
+  int max_iter;
+  int polak_ribiere;
+  int replace_every;
+  int zero_guess;
+  int abort_spd;
+  int* out_iters;
+  double* out_res;
+  double* out_relres;
+  int* out_conv;
+  unsigned* sync;  // [0] barrier count, [1] barrier generation, [2] error, [3] active, [4] verify_iter
+  long long spin_limit;
+};
+
+// kernels launched by the host runtime (sdx_kernels.cu)
+void launch_mass_accum(int64_t n_tets, const int4* slots[4], const float4* rest3, float* mass,
+                       cudaStream_t st);
+void launch_seed_hessian(const Matrix& A, const float* mass, const uint8_t* pin, const uint8_t* env_mask,
+                         float mass_scale, cudaStream_t st);
+void launch_element(const ElemArgs& a, cudaStream_t st);
+void launch_contact(const ContactArgs& a, cudaStream_t st);
+void launch_env_dot(int n_slices, const int* slice_env, const uint8_t* env_mask, const double* a,
+                    const double* b, double* out, cudaStream_t st);
+void launch_zero_rows(int n_slices, const int* slice_env, const uint8_t* env_mask, double* v,
+                      cudaStream_t st);
+void launch_pred(int64_t n3, const double* u, const double* v, double dt, double* ut, double* u0,
+                 cudaStream_t st);
+void launch_ls_candidate(int n_slices, const int* slice_env, const uint8_t* env_mask,
+                         const double* ubase, const double* dx, const double* scale, double* u,
+                         cudaStream_t st);
+void launch_copy_rows(int n_slices, const int* slice_env, const uint8_t* env_mask, const double* src,
+                      double* dst, cudaStream_t st);
+void launch_velocity(int64_t n3, const double* u, const double* u0, double dt, double* v,
+                     cudaStream_t st);
+cudaError_t launch_pcg(const PcgArgs& a, int n_cta, int threads, cudaStream_t st);
+void launch_spmv(const Matrix& A, const float4* x, float* y, int threads, cudaStream_t st);
+void launch_bsr_to_sell(int n_rows, const int64_t* row_ptr, const int32_t* bcol, const float* bval,
+                        const int* slice_ptr, int* col, float* val, int* diag_pos, cudaStream_t st);
+void launch_pack_z(int64_t n_rows, const double* x, float4* z, cudaStream_t st);
+int pcg_shared_bytes(int threads);
+int pcg_max_ctas_per_sm(int threads);
+
+}  // namespace sdx

@@ -1,0 +1,908 @@
+// sdx_kernels.cu — sm_100a kernels of the implicit soft-body step.
+//
+// Element assembly follows fem::StressWork / GravityWork / InertiaWork
+// (mochi_core/include/mochi_core/element_operations/fem_stress.h:107-262, fem_gravity.h:44-128,
+// fem_inertia.h:55-137) with the DRes seeded by the scaled mass matrix
+// (mochi_physics/src/mochi_soft.cpp:249-262). Contact follows the penalty response
+// (mochi_core/include/mochi_core/contact/contact_utils.h:498-570) integrated by TractionWork
+// (fem_traction.h:58-178). The linear solve is the reference's left-preconditioned CG with the
+// residual-L2 stop test (mochi_core/include/mochi_core/linear_algebra/krylov/pcg.h:70-238), fused
+// into one persistent cooperative launch per solve.
+#include <cooperative_groups.h>
+
+#include "sdx_device.cuh"
+#include "sdx_internal.cuh"
+
+namespace sdx {
+
+// ------------------------------------------------------------------------------------------------
+// mass couplings and Hessian seeding
+
+__global__ void k_mass_accum(int64_t n_tets, const int4* __restrict__ s0, const int4* __restrict__ s1,
+                             const int4* __restrict__ s2, const int4* __restrict__ s3,
+                             const float4* __restrict__ rest3, float* mass) {
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_tets) return;
+  const float4 r3 = rest3[t];
+  const float m = r3.w * r3.x / 20.0f;  // rho * vol / 20: P1 consistent mass (Q4 exact)
+  const int4 sl[4] = {s0[t], s1[t], s2[t], s3[t]};
+  const int* sp = reinterpret_cast<const int*>(sl);
+#pragma unroll
+  for (int f = 0; f < 4; ++f)
+#pragma unroll
+    for (int g = 0; g < 4; ++g) atomicAdd(mass + sp[f * 4 + g], f == g ? 2.0f * m : m);
+}
+
+void launch_mass_accum(int64_t n_tets, const int4* slots[4], const float4* rest3, float* mass,
+                       cudaStream_t st) {
+  if (n_tets == 0) return;
+  const int th = 256;
+  k_mass_accum<<<(unsigned)((n_tets + th - 1) / th), th, 0, st>>>(n_tets, slots[0], slots[1], slots[2],
+                                                                   slots[3], rest3, mass);
+}
+
+// One warp per slice: DRes <- mass_scale * M with Dirichlet rows/cols (unit diagonal).
+__global__ void k_seed_hessian(Matrix A, const float* __restrict__ mass, const uint8_t* __restrict__ pin,
+                               const uint8_t* __restrict__ env_mask, float mass_scale) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= A.n_slices) return;
+  const int s = warp;
+  if (env_mask && !env_mask[A.slice_env[s]]) return;
+  const int row = s * kSlice + lane;
+  const int base = A.slice_ptr[s], w = A.slice_w[s];
+  const int pr = pin[row];
+  for (int k = 0; k < w; ++k) {
+    const int p = base + k * kSlice + lane;
+    const int cj = A.col[p];
+    float* vp = A.val + val_index(p, 0);
+    if (cj & kPadBit) {
+#pragma unroll
+      for (int e = 0; e < 9; ++e) vp[e * 32] = 0.0f;
+      continue;
+    }
+    const int pc = pin[cj];
+    const float m = mass[p] * mass_scale;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float v = (r == c) ? m : 0.0f;
+        if (((pr >> r) & 1) || ((pc >> c) & 1)) v = (cj == row && r == c) ? 1.0f : 0.0f;
+        vp[(r * 3 + c) * 32] = v;
+      }
+  }
+}
+
+void launch_seed_hessian(const Matrix& A, const float* mass, const uint8_t* pin, const uint8_t* env_mask,
+                         float mass_scale, cudaStream_t st) {
+  if (A.n_slices == 0) return;
+  const int th = 256;
+  const int64_t threads = (int64_t)A.n_slices * 32;
+  k_seed_hessian<<<(unsigned)((threads + th - 1) / th), th, 0, st>>>(A, mass, pin, env_mask, mass_scale);
+}
+
+// ------------------------------------------------------------------------------------------------
+// per-tet element kernel
+
+__device__ __forceinline__ void warp_env_add(double* obj, int env, double v) {
+  // aggregate lanes of the same env before one atomic
+  const unsigned mask = __activemask();
+  const unsigned same = __match_any_sync(mask, env);
+  const int leader = __ffs(same) - 1;
+  double s = 0.0;
+  for (unsigned m = same; m; m &= m - 1) {
+    const int l = __ffs(m) - 1;
+    s += __shfl_sync(mask, v, l);
+  }
+  if ((int)(threadIdx.x & 31) == leader) atomicAdd(obj + env, s);
+}
+
+__global__ void __launch_bounds__(128) k_element(ElemArgs a) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n_tets) return;
+  const int4 nd = a.tets[t];
+  const int env = a.slice_env[nd.x >> 5];
+  if (a.env_mask && !a.env_mask[env]) return;
+  const float4 R0 = a.rest0[t], R1 = a.rest1[t], R2 = a.rest2[t], R3 = a.rest3[t];
+  const float dN[12] = {R0.x, R0.y, R0.z, R0.w, R1.x, R1.y, R1.z, R1.w, R2.x, R2.y, R2.z, R2.w};
+  const float vol = R3.x, mu = R3.y, lam = R3.z, rho = R3.w;
+  const int rows[4] = {nd.x, nd.y, nd.z, nd.w};
+  double uf[4][3];
+#pragma unroll
+  for (int f = 0; f < 4; ++f)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) uf[f][r] = a.u[3 * (int64_t)rows[f] + r];
+  double F[9] = {1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0};
+#pragma unroll
+  for (int f = 0; f < 4; ++f)
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) F[r * 3 + c] = fma(uf[f][r], (double)dN[3 * f + c], F[r * 3 + c]);
+
+  const bool want_res = a.flags & 2, want_obj = a.flags & 1, want_hess = a.flags & 4;
+  if (want_res || want_obj) {
+    const SnhConsts kc = snh_consts((double)mu, (double)lam);
+    const double w = (double)vol;
+    const double m = (double)rho * w / 20.0;
+    double acc[4][3], asum[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int f = 0; f < 4; ++f)
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        acc[f][r] = uf[f][r] - a.ut[3 * (int64_t)rows[f] + r];
+        asum[r] += acc[f][r];
+      }
+    if (want_res) {
+      double P[9];
+      snh_pk1_f64(kc, F, P);
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        const int pf = a.pin[rows[f]];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) {
+          if ((pf >> r) & 1) continue;
+          double v = (P[r * 3 + 0] * dN[3 * f + 0] + P[r * 3 + 1] * dN[3 * f + 1] +
+                      P[r * 3 + 2] * dN[3 * f + 2]) * w;
+          v -= (double)rho * a.grav[r] * w * 0.25;
+          v += a.dtfi2 * m * (acc[f][r] + asum[r]);
+          atomicAdd(a.g + 3 * (int64_t)rows[f] + r, v);
+        }
+      }
+    }
+    if (want_obj) {
+      double xc[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+      for (int f = 0; f < 4; ++f)
+#pragma unroll
+        for (int r = 0; r < 3; ++r) xc[r] += 0.25 * (a.X[3 * (int64_t)rows[f] + r] + uf[f][r]);
+      double ein = 0.0;
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        double sq = 0.0;
+#pragma unroll
+        for (int f = 0; f < 4; ++f) sq += acc[f][r] * acc[f][r];
+        ein += m * (sq + asum[r] * asum[r]);
+      }
+      const double e = snh_energy_f64(kc, F) * w -
+                       (double)rho * w * (a.grav[0] * xc[0] + a.grav[1] * xc[1] + a.grav[2] * xc[2]) +
+                       0.5 * a.dtfi2 * ein;
+      warp_env_add(a.obj, env, e);
+    }
+  }
+
+  if (want_hess) {
+    float Ff[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Ff[i] = (float)F[i];
+    float C[81];
+    snh_tangent_f32(mu, lam, Ff, (a.flags & 8) != 0, a.psd, a.min_eig, C);
+    const int4 S0 = a.slots0[t], S1 = a.slots1[t], S2 = a.slots2[t], S3 = a.slots3[t];
+    const int slot[16] = {S0.x, S0.y, S0.z, S0.w, S1.x, S1.y, S1.z, S1.w,
+                          S2.x, S2.y, S2.z, S2.w, S3.x, S3.y, S3.z, S3.w};
+    int pins[4];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) pins[f] = a.pin[rows[f]];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        if ((pins[f] >> r) & 1) continue;
+        // Cf_r[c][l] = sum_j dN_f[j] C[(3r+j)][(3c+l)]  (fem_stress.h:218-241)
+        float Cf[9];
+#pragma unroll
+        for (int cl = 0; cl < 9; ++cl)
+          Cf[cl] = dN[3 * f + 0] * C[(3 * r + 0) * 9 + cl] + dN[3 * f + 1] * C[(3 * r + 1) * 9 + cl] +
+                   dN[3 * f + 2] * C[(3 * r + 2) * 9 + cl];
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+          const int p = slot[f * 4 + g];
+          float* vp = a.val + val_index(p, 3 * r);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            if ((pins[g] >> c) & 1) continue;
+            const float k = vol * (Cf[c * 3 + 0] * dN[3 * g + 0] + Cf[c * 3 + 1] * dN[3 * g + 1] +
+                                   Cf[c * 3 + 2] * dN[3 * g + 2]);
+            atomicAdd(vp + c * 32, k);
+          }
+        }
+      }
+    }
+  }
+}
+
+void launch_element(const ElemArgs& a, cudaStream_t st) {
+  if (a.n_tets == 0) return;
+  const int th = 128;
+  k_element<<<(unsigned)((a.n_tets + th - 1) / th), th, 0, st>>>(a);
+}
+
+// ------------------------------------------------------------------------------------------------
+// contact: one thread per boundary sample (face, quadrature point)
+
+__constant__ double c_face_w[3][3] = {{2.0 / 3.0, 1.0 / 6.0, 1.0 / 6.0},
+                                      {1.0 / 6.0, 2.0 / 3.0, 1.0 / 6.0},
+                                      {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0}};
+
+__global__ void __launch_bounds__(128) k_contact(ContactArgs a) {
+  const int64_t sidx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (sidx >= a.n_samples) return;
+  const int64_t f = sidx / 3;
+  const int q = (int)(sidx - 3 * f);
+  const int4 fr = a.faces[f];
+  const int env = fr.w;
+  unsigned bits = 0;
+  if (!a.env_mask || a.env_mask[env]) {
+    const int rows[3] = {fr.x, fr.y, fr.z};
+    double xn[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int r = 0; r < 3; ++r) xn[k][r] = a.X[3 * (int64_t)rows[k] + r] + a.u[3 * (int64_t)rows[k] + r];
+    double e1[3], e2[3], nrm[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      e1[r] = xn[1][r] - xn[0][r];
+      e2[r] = xn[2][r] - xn[0][r];
+    }
+    nrm[0] = e1[1] * e2[2] - e1[2] * e2[1];
+    nrm[1] = e1[2] * e2[0] - e1[0] * e2[2];
+    nrm[2] = e1[0] * e2[1] - e1[1] * e2[0];
+    const double nl = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+#pragma unroll
+    for (int r = 0; r < 3; ++r) nrm[r] = nl > 0.0 ? nrm[r] / nl : 0.0;
+    double xs[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      xs[r] = c_face_w[q][0] * xn[0][r] + c_face_w[q][1] * xn[1][r] + c_face_w[q][2] * xn[2][r];
+    const double wq = a.face_area[f] / 3.0;
+    const int c0 = a.coll_off[env], c1 = a.coll_off[env + 1];
+    double energy = 0.0;
+    for (int c = c0; c < c1; ++c) {
+      double d, gr[3];
+      collider_sdf(a.colliders + 11 * (int64_t)c, xs, a.t, d, gr);
+      if (!(d < a.thr)) continue;
+      const double align = gr[0] * nrm[0] + gr[1] * nrm[1] + gr[2] * nrm[2];
+      if (align > a.max_align) continue;
+      bits |= 1u << (c - c0);
+      double pv, dp, ddp;
+      polyrelu(-d, a.t_half, a.t_half - a.thr, pv, dp, ddp);
+      energy += 0.5 * a.k * pv * pv * wq;
+      const double fn = a.k * pv * dp;
+      if (a.flags & 2) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const int pk = a.pin[rows[k]];
+#pragma unroll
+          for (int r = 0; r < 3; ++r)
+            if (!((pk >> r) & 1)) atomicAdd(a.g + 3 * (int64_t)rows[k] + r, -fn * gr[r] * c_face_w[q][k] * wq);
+        }
+      }
+      if (a.flags & 4) {
+        const double dfn = -a.k * (dp * dp + pv * ddp);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const int pk = a.pin[rows[k]];
+#pragma unroll
+          for (int l = 0; l < 3; ++l) {
+            const int pl = a.pin[rows[l]];
+            const int p = a.face_slots[9 * f + 3 * k + l];
+            const double wkl = c_face_w[q][k] * c_face_w[q][l] * wq;
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+              for (int cc = 0; cc < 3; ++cc) {
+                if (((pk >> r) & 1) || ((pl >> cc) & 1)) continue;
+                atomicAdd(a.val + val_index(p, 3 * r + cc), (float)(-dfn * gr[r] * gr[cc] * wkl));
+              }
+          }
+        }
+      }
+    }
+    if (a.flags & 1) {
+      if (energy != 0.0) atomicAdd(a.obj + env, energy);
+    }
+    if (bits) atomicAdd(a.n_pairs + env, (unsigned long long)__popc(bits));
+  }
+  if (a.pair_mask) a.pair_mask[sidx] = bits;
+}
+
+void launch_contact(const ContactArgs& a, cudaStream_t st) {
+  if (a.n_samples == 0) return;
+  const int th = 128;
+  k_contact<<<(unsigned)((a.n_samples + th - 1) / th), th, 0, st>>>(a);
+}
+
+// ------------------------------------------------------------------------------------------------
+// per-env reductions and row-wise vector kernels (one warp per slice)
+
+__global__ void k_env_dot(int n_slices, const int* __restrict__ slice_env, const uint8_t* __restrict__ env_mask,
+                          const double* __restrict__ a, const double* __restrict__ b, double* out) {
+  __shared__ double sw[8];
+  __shared__ int se[8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int s = blockIdx.x * 8 + warp;
+  double v = 0.0;
+  int env = -1;
+  if (s < n_slices) {
+    env = slice_env[s];
+    if (!env_mask || env_mask[env]) {
+      const int64_t base = 3 * ((int64_t)s * kSlice + lane);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) v += a[base + k] * b[base + k];
+    } else {
+      env = -1;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (lane == 0) {
+    sw[warp] = v;
+    se[warp] = env;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double acc = 0.0;
+    int cur = -1;
+    for (int w = 0; w < 8; ++w) {
+      if (se[w] != cur) {
+        if (cur >= 0) atomicAdd(out + cur, acc);
+        cur = se[w];
+        acc = 0.0;
+      }
+      acc += sw[w];
+    }
+    if (cur >= 0) atomicAdd(out + cur, acc);
+  }
+}
+
+void launch_env_dot(int n_slices, const int* slice_env, const uint8_t* env_mask, const double* a,
+                    const double* b, double* out, cudaStream_t st) {
+  if (n_slices == 0) return;
+  k_env_dot<<<(n_slices + 7) / 8, 256, 0, st>>>(n_slices, slice_env, env_mask, a, b, out);
+}
+
+__global__ void k_zero_rows(int n_slices, const int* __restrict__ slice_env, const uint8_t* __restrict__ env_mask,
+                            double* v) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;  // component index
+  if (i >= (int64_t)n_slices * kSlice * 3) return;
+  const int s = (int)(i / (kSlice * 3));
+  if (env_mask && !env_mask[slice_env[s]]) return;
+  v[i] = 0.0;
+}
+
+void launch_zero_rows(int n_slices, const int* slice_env, const uint8_t* env_mask, double* v,
+                      cudaStream_t st) {
+  const int64_t n = (int64_t)n_slices * kSlice * 3;
+  if (n == 0) return;
+  k_zero_rows<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n_slices, slice_env, env_mask, v);
+}
+
+__global__ void k_pred(int64_t n3, const double* __restrict__ u, const double* __restrict__ v, double dt,
+                       double* ut, double* u0) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n3) return;
+  const double ui = u[i];
+  ut[i] = ui + dt * v[i];  // GatherPredTarget: x~ = x0 + dt v0 (batched_element_utils.h:90-123)
+  u0[i] = ui;
+}
+
+void launch_pred(int64_t n3, const double* u, const double* v, double dt, double* ut, double* u0,
+                 cudaStream_t st) {
+  if (n3 == 0) return;
+  k_pred<<<(unsigned)((n3 + 255) / 256), 256, 0, st>>>(n3, u, v, dt, ut, u0);
+}
+
+__global__ void k_ls_candidate(int n_slices, const int* __restrict__ slice_env,
+                               const uint8_t* __restrict__ env_mask, const double* __restrict__ ubase,
+                               const double* __restrict__ dx, const double* __restrict__ scale, double* u) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)n_slices * kSlice * 3) return;
+  const int env = slice_env[i / (kSlice * 3)];
+  if (env_mask && !env_mask[env]) return;
+  u[i] = ubase[i] - scale[env] * dx[i];
+}
+
+void launch_ls_candidate(int n_slices, const int* slice_env, const uint8_t* env_mask,
+                         const double* ubase, const double* dx, const double* scale, double* u,
+                         cudaStream_t st) {
+  const int64_t n = (int64_t)n_slices * kSlice * 3;
+  if (n == 0) return;
+  k_ls_candidate<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n_slices, slice_env, env_mask, ubase, dx,
+                                                               scale, u);
+}
+
+__global__ void k_copy_rows(int n_slices, const int* __restrict__ slice_env, const uint8_t* __restrict__ env_mask,
+                            const double* __restrict__ src, double* dst) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)n_slices * kSlice * 3) return;
+  if (env_mask && !env_mask[slice_env[i / (kSlice * 3)]]) return;
+  dst[i] = src[i];
+}
+
+void launch_copy_rows(int n_slices, const int* slice_env, const uint8_t* env_mask, const double* src,
+                      double* dst, cudaStream_t st) {
+  const int64_t n = (int64_t)n_slices * kSlice * 3;
+  if (n == 0) return;
+  k_copy_rows<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n_slices, slice_env, env_mask, src, dst);
+}
+
+__global__ void k_velocity(int64_t n3, const double* __restrict__ u, const double* __restrict__ u0, double dt,
+                           double* v) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n3) return;
+  v[i] = (u[i] - u0[i]) / dt;
+}
+
+void launch_velocity(int64_t n3, const double* u, const double* u0, double dt, double* v,
+                     cudaStream_t st) {
+  if (n3 == 0) return;
+  k_velocity<<<(unsigned)((n3 + 255) / 256), 256, 0, st>>>(n3, u, u0, dt, v);
+}
+
+__global__ void k_pack_z(int64_t n_rows, const double* __restrict__ x, float4* z) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_rows) return;
+  z[i] = make_float4((float)x[3 * i], (float)x[3 * i + 1], (float)x[3 * i + 2], 0.0f);
+}
+
+void launch_pack_z(int64_t n_rows, const double* x, float4* z, cudaStream_t st) {
+  if (n_rows == 0) return;
+  k_pack_z<<<(unsigned)((n_rows + 255) / 256), 256, 0, st>>>(n_rows, x, z);
+}
+
+// ------------------------------------------------------------------------------------------------
+// SELL-32 3x3 SpMV building block: acc = A_row . src (one warp per slice, lane = row)
+
+template <class Load>
+__device__ __forceinline__ void sell_row_product(const Matrix& A, int s, int lane, Load load, float& a0,
+                                                 float& a1, float& a2) {
+  const int base = A.slice_ptr[s], w = A.slice_w[s];
+  a0 = a1 = a2 = 0.0f;
+#pragma unroll 2
+  for (int k = 0; k < w; ++k) {
+    const int p = base + k * kSlice + lane;
+    const int j = __ldcs(A.col + p) & 0x7fffffff;
+    const float* vp = A.val + (size_t)(base + k * kSlice) * 9 + lane;
+    const float4 xj = load(j);
+    const float v0 = __ldcs(vp + 0 * 32), v1 = __ldcs(vp + 1 * 32), v2 = __ldcs(vp + 2 * 32);
+    const float v3 = __ldcs(vp + 3 * 32), v4 = __ldcs(vp + 4 * 32), v5 = __ldcs(vp + 5 * 32);
+    const float v6 = __ldcs(vp + 6 * 32), v7 = __ldcs(vp + 7 * 32), v8 = __ldcs(vp + 8 * 32);
+    a0 = fmaf(v0, xj.x, fmaf(v1, xj.y, fmaf(v2, xj.z, a0)));
+    a1 = fmaf(v3, xj.x, fmaf(v4, xj.y, fmaf(v5, xj.z, a1)));
+    a2 = fmaf(v6, xj.x, fmaf(v7, xj.y, fmaf(v8, xj.z, a2)));
+  }
+}
+
+__global__ void k_spmv(Matrix A, const float4* __restrict__ x, float* __restrict__ y) {
+  const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (s >= A.n_slices) return;
+  float a0, a1, a2;
+  sell_row_product(A, s, lane, [&](int j) { return __ldg(x + j); }, a0, a1, a2);
+  const int64_t row = (int64_t)s * kSlice + lane;
+  y[3 * row] = a0;
+  y[3 * row + 1] = a1;
+  y[3 * row + 2] = a2;
+}
+
+void launch_spmv(const Matrix& A, const float4* x, float* y, int threads, cudaStream_t st) {
+  if (A.n_slices == 0) return;
+  const int64_t t = (int64_t)A.n_slices * 32;
+  k_spmv<<<(unsigned)((t + threads - 1) / threads), threads, 0, st>>>(A, x, y);
+}
+
+// ------------------------------------------------------------------------------------------------
+// BSR (row-major 3x3 blocks, FP32) -> SELL-32. One thread per block row.
+
+__global__ void k_bsr_to_sell(int n_rows, const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ bcol,
+                              const float* __restrict__ bval, const int* __restrict__ slice_ptr, int* col,
+                              float* val, int* diag_pos) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= n_rows) return;
+  const int s = row >> 5, lane = row & 31;
+  const int base = slice_ptr[s];
+  const int w = (slice_ptr[s + 1] - base) / kSlice;
+  const int64_t b0 = row_ptr[row], len = row_ptr[row + 1] - b0;
+  diag_pos[row] = -1;
+  for (int k = 0; k < w; ++k) {
+    const int p = base + k * kSlice + lane;
+    if (k < len) {
+      const int j = bcol[b0 + k];
+      col[p] = j;
+      if (j == row) diag_pos[row] = p;
+#pragma unroll
+      for (int e = 0; e < 9; ++e) val[val_index(p, e)] = bval[9 * (b0 + k) + e];
+    } else {
+      col[p] = row | kPadBit;
+#pragma unroll
+      for (int e = 0; e < 9; ++e) val[val_index(p, e)] = 0.0f;
+    }
+  }
+}
+
+void launch_bsr_to_sell(int n_rows, const int64_t* row_ptr, const int32_t* bcol, const float* bval,
+                        const int* slice_ptr, int* col, float* val, int* diag_pos, cudaStream_t st) {
+  if (n_rows == 0) return;
+  k_bsr_to_sell<<<(n_rows + 127) / 128, 128, 0, st>>>(n_rows, row_ptr, bcol, bval, slice_ptr, col, val,
+                                                       diag_pos);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Persistent Jacobi-PCG (one cooperative launch per solve, every env of the batch at once).
+//
+// Per iteration two grid barriers:
+//   phase 1: p <- z + beta p, q <- A z + beta q (= A p by linearity), partial p.q
+//   phase 2: x += alpha p, r -= alpha q (FP64), z <- M^-1 r, partials r.r, r.z_old, r.z
+// Every `replace_every` iterations, and one iteration after an env's recurrence residual first meets
+// the tolerance, r is recomputed as b - A x with FP64 accumulation (extra barrier) and the stop test
+// uses that true residual. Per-env scalars are reduced deterministically: each CTA writes one partial
+// per (CTA, env) it covers and every CTA that needs an env's total sums that env's partials in a fixed
+// order, so all CTAs hold bit-identical alpha / beta / status for their envs.
+
+int pcg_shared_bytes(int threads);
+
+struct EnvState {
+  double rz, alpha, beta, conv_thr, div_thr, bb;
+  int status;  // 0 active, 1 converged, 2 stopped, 3 diverged, 4 not requested, 5 diverging
+  int first;
+};
+
+__device__ __forceinline__ bool grid_barrier(unsigned* sync, unsigned nblocks, long long spin_limit) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* vgen = sync + 1;
+    const unsigned gen = *vgen;
+    __threadfence();
+    const unsigned prev = atomicAdd(sync, 1u);
+    if (prev == nblocks - 1) {
+      atomicExch(sync, 0u);
+      __threadfence();
+      atomicAdd(sync + 1, 1u);
+    } else {
+      long long spins = 0;
+      while (*vgen == gen) {
+        if (++spins > spin_limit) {
+          atomicExch(sync + 2, 1u);  // device timeout: recorded, the kernel unwinds
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *((volatile unsigned*)(sync + 2)) == 0u;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__device__ __forceinline__ void prec_apply(const PcgArgs& a, int64_t row, const double r[3], float z[3]) {
+  if (a.precond == 1) {
+    const float* d = a.dinv + 3 * row;
+    z[0] = (float)(d[0] * r[0]);
+    z[1] = (float)(d[1] * r[1]);
+    z[2] = (float)(d[2] * r[2]);
+  } else if (a.precond == 2) {
+    const float* B = a.dinv + 9 * row;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) z[k] = (float)(B[3 * k] * r[0] + B[3 * k + 1] * r[1] + B[3 * k + 2] * r[2]);
+  } else {
+    z[0] = (float)r[0];
+    z[1] = (float)r[1];
+    z[2] = (float)r[2];
+  }
+}
+
+// r = b - A x with FP64 accumulation (FP32 matrix values, FP64 x gathered from L2)
+__device__ __forceinline__ void true_residual(const PcgArgs& a, int s, int lane, double r[3]) {
+  const int base = a.A.slice_ptr[s], w = a.A.slice_w[s];
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  for (int k = 0; k < w; ++k) {
+    const int p = base + k * kSlice + lane;
+    const int j = __ldcs(a.A.col + p) & 0x7fffffff;
+    const float* vp = a.A.val + (size_t)(base + k * kSlice) * 9 + lane;
+    const double x0 = __ldcg(a.x + 3 * (int64_t)j), x1 = __ldcg(a.x + 3 * (int64_t)j + 1),
+                 x2 = __ldcg(a.x + 3 * (int64_t)j + 2);
+    a0 += (double)vp[0] * x0 + (double)vp[32] * x1 + (double)vp[64] * x2;
+    a1 += (double)vp[96] * x0 + (double)vp[128] * x1 + (double)vp[160] * x2;
+    a2 += (double)vp[192] * x0 + (double)vp[224] * x1 + (double)vp[256] * x2;
+  }
+  const int64_t row = (int64_t)s * kSlice + lane;
+  r[0] = a.b[3 * row] - a0;
+  r[1] = a.b[3 * row + 1] - a1;
+  r[2] = a.b[3 * row + 2] - a2;
+}
+
+__global__ void k_pcg(PcgArgs a) {
+  extern __shared__ double wacc[];  // [nwarps][kPcgMaxEnvsPerCta][kPcgNq]
+  __shared__ EnvState st[kPcgMaxEnvsPerCta];
+  __shared__ double tot[kPcgMaxEnvsPerCta][kPcgNq];
+  __shared__ int s_exit, s_replace;
+  const int c = blockIdx.x;
+  const unsigned ncta = gridDim.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const int s0 = a.cta_slice[c], s1 = a.cta_slice[c + 1];
+  const int e0 = a.cta_env0[c];
+  const int ne = (s1 > s0) ? (a.cta_env1[c] - e0 + 1) : 0;
+
+  auto clear_acc = [&]() {
+    for (int i = threadIdx.x; i < nwarps * kPcgMaxEnvsPerCta * kPcgNq; i += blockDim.x) wacc[i] = 0.0;
+    __syncthreads();
+  };
+  auto add_acc = [&](int le, int k, double v) {
+    v = warp_sum(v);
+    if (lane == 0) wacc[(warp * kPcgMaxEnvsPerCta + le) * kPcgNq + k] += v;
+  };
+  // Partials of phase 1 live in buffer 1, those of phases 0 and 2 in buffer 0, so a CTA writing the
+  // next phase's partials never overwrites values another CTA is still reducing.
+  const size_t pstride = (size_t)a.cta_pbase[ncta] * kPcgNq;
+  auto flush_acc = [&](int nq, int buf) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < ne * nq; i += blockDim.x) {
+      const int le = i / nq, k = i % nq;
+      double v = 0.0;
+      for (int w = 0; w < nwarps; ++w) v += wacc[(w * kPcgMaxEnvsPerCta + le) * kPcgNq + k];
+      a.part[buf * pstride + (size_t)(a.cta_pbase[c] + le) * kPcgNq + k] = v;
+    }
+  };
+  auto reduce_tot = [&](int nq, int buf) {
+    for (int le = warp; le < ne; le += nwarps) {
+      const int e = e0 + le;
+      const int ca = a.env_cta0[e], cb = a.env_cta1[e];
+      for (int k = 0; k < nq; ++k) {
+        double v = 0.0;
+        for (int cc = ca + lane; cc <= cb; cc += 32)
+          v += __ldcg(a.part + buf * pstride + (size_t)(a.cta_pbase[cc] + e - a.cta_env0[cc]) * kPcgNq + k);
+        v = warp_sum(v);
+        if (lane == 0) tot[le][k] = v;
+      }
+    }
+    __syncthreads();
+  };
+  auto finish_env = [&](int le, int it, double rr) {
+    const int e = e0 + le;
+    if (a.env_cta0[e] == c) {
+      a.out_iters[e] = it;
+      a.out_res[e] = sqrt(fmax(rr, 0.0));
+      a.out_relres[e] = st[le].bb == 0.0 ? 0.0 : sqrt(fmax(rr, 0.0) / st[le].bb);
+      a.out_conv[e] = st[le].status;
+      atomicSub((int*)(a.sync + 3), 1);
+    }
+  };
+
+  for (int le = threadIdx.x; le < ne; le += blockDim.x) {
+    st[le].status = (a.env_mask && !a.env_mask[e0 + le]) ? 4 : 0;
+    st[le].first = 1;
+    st[le].beta = 0.0;
+  }
+  __syncthreads();
+
+  // ---- phase 0: r = b - A x0, z = M^-1 r, partials b.b, r.r, r.z ----
+  clear_acc();
+  for (int s = s0 + warp; s < s1; s += nwarps) {
+    const int le = a.A.slice_env[s] - e0;
+    if (st[le].status != 0) continue;
+    const int64_t row = (int64_t)s * kSlice + lane;
+    // preconditioner from the diagonal block (BlockJacobiPrec<1> / <3>, block_jacobi_prec.h:35-151)
+    const int dp = a.diag_pos[row];
+    if (a.precond == 1) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const float d = dp >= 0 ? a.A.val[val_index(dp, 4 * k)] : 0.0f;
+        a.dinv[3 * row + k] = d != 0.0f ? 1.0f / d : 0.0f;
+      }
+    } else if (a.precond == 2) {
+      float B[9];
+#pragma unroll
+      for (int e = 0; e < 9; ++e) B[e] = dp >= 0 ? a.A.val[val_index(dp, e)] : 0.0f;
+      float cof[9];
+      cof3(B, cof);
+      const float det = det3(B);
+      const float inv = det != 0.0f ? 1.0f / det : 0.0f;
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) a.dinv[9 * row + 3 * i + j] = cof[3 * j + i] * inv;
+    }
+    double r[3];
+    if (a.zero_guess) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        a.x[3 * row + k] = 0.0;
+        r[k] = a.b[3 * row + k];
+      }
+    }
+    if (!a.zero_guess) true_residual(a, s, lane, r);
+    float z[3];
+    prec_apply(a, row, r, z);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) a.r[3 * row + k] = r[k];
+    a.z[row] = make_float4(z[0], z[1], z[2], 0.0f);
+    const double b0 = a.b[3 * row], b1 = a.b[3 * row + 1], b2 = a.b[3 * row + 2];
+    add_acc(le, 0, b0 * b0 + b1 * b1 + b2 * b2);
+    add_acc(le, 1, r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    add_acc(le, 2, r[0] * z[0] + r[1] * z[1] + r[2] * z[2]);
+  }
+  flush_acc(3, 0);
+  if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
+  reduce_tot(3, 0);
+  for (int le = threadIdx.x; le < ne; le += blockDim.x) {
+    if (st[le].status != 0) continue;
+    const double bb = tot[le][0], rr = tot[le][1];
+    st[le].bb = bb;
+    const double rt = a.env_rel_tol ? a.env_rel_tol[e0 + le] : a.rel_tol;
+    st[le].conv_thr = fmax(a.abs_tol * a.abs_tol, (bb * rt) * rt);
+    st[le].div_thr = (bb * a.rel_div_tol) * a.rel_div_tol;
+    st[le].rz = tot[le][2];
+    if (!isfinite(rr) || rr > st[le].div_thr) {
+      st[le].status = 3;
+      finish_env(le, 0, rr);
+    } else if (rr <= st[le].conv_thr) {
+      st[le].status = 1;
+      finish_env(le, 0, rr);
+    }
+  }
+  __syncthreads();
+
+  for (int it = 1;; ++it) {
+    // ---- phase 1 ----
+    clear_acc();
+    for (int s = s0 + warp; s < s1; s += nwarps) {
+      const int le = a.A.slice_env[s] - e0;
+      if (st[le].status != 0) continue;
+      const int64_t row = (int64_t)s * kSlice + lane;
+      float a0, a1, a2;
+      sell_row_product(a.A, s, lane, [&](int j) { return __ldcg(a.z + j); }, a0, a1, a2);
+      const float4 zr = a.z[row];
+      float pn[3], qn[3];
+      if (st[le].first) {
+        pn[0] = zr.x;
+        pn[1] = zr.y;
+        pn[2] = zr.z;
+        qn[0] = a0;
+        qn[1] = a1;
+        qn[2] = a2;
+      } else {
+        const float beta = (float)st[le].beta;
+        pn[0] = fmaf(beta, a.p[3 * row], zr.x);
+        pn[1] = fmaf(beta, a.p[3 * row + 1], zr.y);
+        pn[2] = fmaf(beta, a.p[3 * row + 2], zr.z);
+        qn[0] = fmaf(beta, a.q[3 * row], a0);
+        qn[1] = fmaf(beta, a.q[3 * row + 1], a1);
+        qn[2] = fmaf(beta, a.q[3 * row + 2], a2);
+      }
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        a.p[3 * row + k] = pn[k];
+        a.q[3 * row + k] = qn[k];
+      }
+      add_acc(le, 0, (double)pn[0] * qn[0] + (double)pn[1] * qn[1] + (double)pn[2] * qn[2]);
+    }
+    flush_acc(1, 1);
+    if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
+    if (threadIdx.x == 0) {
+      s_exit = *((volatile int*)(a.sync + 3)) <= 0;
+      const int vi = *((volatile int*)(a.sync + 4));
+      s_replace = (vi == it - 1) || (a.replace_every > 0 && it % a.replace_every == 0);
+    }
+    reduce_tot(1, 1);
+    if (s_exit) break;
+    const bool replace = s_replace != 0;
+    for (int le = threadIdx.x; le < ne; le += blockDim.x) {
+      if (st[le].status != 0) continue;
+      const double pq = tot[le][0];
+      st[le].alpha = st[le].rz / pq;
+      // non-SPD abort (pcg.h:152-169): the env stops now, its exit is published in the post-barrier
+      // stage below so that every CTA reads the same active count after the next barrier
+      if (pq <= 0.0 && a.abort_spd) st[le].status = 5;
+    }
+    __syncthreads();
+
+    // ---- phase 2 ----
+    clear_acc();
+    for (int s = s0 + warp; s < s1; s += nwarps) {
+      const int le = a.A.slice_env[s] - e0;
+      if (st[le].status != 0) continue;
+      const int64_t row = (int64_t)s * kSlice + lane;
+      const double al = st[le].alpha;
+      double r[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        a.x[3 * row + k] += al * (double)a.p[3 * row + k];
+        r[k] = a.r[3 * row + k] - al * (double)a.q[3 * row + k];
+      }
+      if (replace) continue;
+      const float4 zo = a.z[row];
+      float z[3];
+      prec_apply(a, row, r, z);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) a.r[3 * row + k] = r[k];
+      a.z[row] = make_float4(z[0], z[1], z[2], 0.0f);
+      add_acc(le, 0, r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+      add_acc(le, 1, r[0] * zo.x + r[1] * zo.y + r[2] * zo.z);
+      add_acc(le, 2, r[0] * z[0] + r[1] * z[1] + r[2] * z[2]);
+    }
+    if (replace) {
+      if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
+      for (int s = s0 + warp; s < s1; s += nwarps) {
+        const int le = a.A.slice_env[s] - e0;
+        if (st[le].status != 0) continue;
+        const int64_t row = (int64_t)s * kSlice + lane;
+        double r[3];
+        true_residual(a, s, lane, r);
+        const float4 zo = a.z[row];
+        float z[3];
+        prec_apply(a, row, r, z);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) a.r[3 * row + k] = r[k];
+        a.z[row] = make_float4(z[0], z[1], z[2], 0.0f);
+        add_acc(le, 0, r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+        add_acc(le, 1, r[0] * zo.x + r[1] * zo.y + r[2] * zo.z);
+        add_acc(le, 2, r[0] * z[0] + r[1] * z[1] + r[2] * z[2]);
+      }
+    }
+    flush_acc(3, 0);
+    if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
+    reduce_tot(3, 0);
+    for (int le = threadIdx.x; le < ne; le += blockDim.x) {
+      if (st[le].status == 5) {
+        st[le].status = 3;
+        finish_env(le, it, 0.0);
+        continue;
+      }
+      if (st[le].status != 0) continue;
+      const double rr = tot[le][0], rzo = tot[le][1], rzn = tot[le][2];
+      if (!isfinite(rr) || rr > st[le].div_thr) {
+        st[le].status = 3;
+        finish_env(le, it, rr);
+        continue;
+      }
+      if (rr <= st[le].conv_thr) {
+        if (replace) {
+          st[le].status = 1;
+          finish_env(le, it, rr);
+          continue;
+        }
+        if (a.env_cta0[e0 + le] == c) atomicMax((int*)(a.sync + 4), it);
+      }
+      if (it >= a.max_iter) {
+        st[le].status = 2;
+        finish_env(le, it, rr);
+        continue;
+      }
+      if (rzn == 0.0) {
+        st[le].status = 3;
+        finish_env(le, it, rr);
+        continue;
+      }
+      const double bpr = (a.polak_ribiere && !st[le].first) ? rzo : 0.0;
+      st[le].beta = (rzn - bpr) / st[le].rz;
+      st[le].rz = rzn;
+      st[le].first = 0;
+    }
+    __syncthreads();
+  }
+}
+
+int pcg_max_ctas_per_sm(int threads) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pcg, threads, pcg_shared_bytes(threads)) != cudaSuccess) return 0;
+  return n;
+}
+
+int pcg_shared_bytes(int threads) { return (threads / 32) * kPcgMaxEnvsPerCta * kPcgNq * (int)sizeof(double); }
+
+cudaError_t launch_pcg(const PcgArgs& a, int n_cta, int threads, cudaStream_t st) {
+  PcgArgs args = a;
+  void* params[] = {&args};
+  return cudaLaunchCooperativeKernel((const void*)k_pcg, dim3(n_cta), dim3(threads), params,
+                                     (size_t)pcg_shared_bytes(threads), st);
+}
+
+}  // namespace sdx

@@ -1,0 +1,147 @@
+"""Batched soft-body world on the GPU: the reference's FEM-body and island-Newton boundary.
+
+A `SoftBodyWorld` holds many independent soft bodies (environments) in one device-resident batch and
+advances all of them with `step()`, the analogue of Scene::Step for soft actors
+(mochi_physics/src/mochi_scene.cpp:594 -> solver::StepIslandNewtonAsync, mochi_solve.cpp:1090; one
+island per env). `assemble()` exposes the FEM-body assembly (AssembleObjResDRes + MakeBatchedBodyOp +
+async contact, mochi_soft.cpp:202-474) for parity checks.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import capi
+from .scenes import Body, SceneConfig, concat_bodies
+
+
+class SoftBodyWorld:
+    def __init__(self, bodies: Sequence[Body], cfg: SceneConfig, device: int = 0, **overrides):
+        L = capi.lib()
+        self.bodies = list(bodies)
+        self.cfg = cfg
+        self._ctx = L.sdx_create(device)
+        if not self._ctx:
+            raise capi.SdxError(L.sdx_last_error().decode())
+        node_off, tet_off, X, tets = concat_bodies(self.bodies)
+        lam = np.concatenate([b.lame()[0] for b in self.bodies])
+        mu = np.concatenate([b.lame()[1] for b in self.bodies])
+        rho = np.concatenate([b.rho for b in self.bodies]).astype(np.float64)
+        pin = np.concatenate([b.pin for b in self.bodies]).astype(np.uint8)
+        self.node_off, self.tet_off = node_off, tet_off
+        self.n_envs = len(self.bodies)
+        self.n_nodes = int(node_off[-1])
+        capi.check(L.sdx_upload_bodies(self._ctx, self.n_envs, capi.ptr(node_off, capi._lp),
+                                       capi.ptr(tet_off, capi._lp), capi.ptr(np.ascontiguousarray(X)),
+                                       capi.ptr(np.ascontiguousarray(tets), capi._ip),
+                                       capi.ptr(np.ascontiguousarray(lam)), capi.ptr(np.ascontiguousarray(mu)),
+                                       capi.ptr(rho), capi.ptr(pin, capi._up)))
+        rows, envs = [], []
+        for e, b in enumerate(self.bodies):
+            for c in b.colliders:
+                rows.append(c.as_row())
+                envs.append(e)
+        self.n_colliders = len(rows)
+        if rows:
+            R = np.ascontiguousarray(np.stack(rows))
+            E = np.asarray(envs, np.int32)
+            capi.check(L.sdx_set_colliders(self._ctx, len(rows), capi.ptr(E, capi._ip), capi.ptr(R)))
+        self.params = capi.default_step_params()
+        self.params.dt = cfg.dt
+        for k in range(3):
+            self.params.gravity[k] = cfg.gravity[k]
+        self.params.k_contact, self.params.t_half = cfg.k_contact, cfg.t_half
+        self.params.thr, self.params.max_align = cfg.thr, cfg.max_align
+        for k, v in overrides.items():
+            if k.startswith("linear_"):
+                setattr(self.params.linear, k[len("linear_"):], v)
+            else:
+                setattr(self.params, k, v)
+        capi.check(L.sdx_set_params(self._ctx, C.byref(self.params)))
+        sizes = [C.c_int64() for _ in range(4)]
+        capi.check(L.sdx_get_sizes(self._ctx, *[C.byref(s) for s in sizes]))
+        self.n_tets, self.nnzb, self.n_faces = sizes[1].value, sizes[2].value, sizes[3].value
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            capi.lib().sdx_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        self.close()
+
+    def set_params(self, **kw):
+        for k, v in kw.items():
+            if k.startswith("linear_"):
+                setattr(self.params.linear, k[len("linear_"):], v)
+            else:
+                setattr(self.params, k, v)
+        capi.check(capi.lib().sdx_set_params(self._ctx, C.byref(self.params)))
+
+    # state -------------------------------------------------------------------------------------
+    def set_state(self, u: Optional[np.ndarray], v: Optional[np.ndarray], time: float = 0.0):
+        u = None if u is None else np.ascontiguousarray(u, np.float64).reshape(-1)
+        v = None if v is None else np.ascontiguousarray(v, np.float64).reshape(-1)
+        capi.check(capi.lib().sdx_set_state(self._ctx, capi.ptr(u), capi.ptr(v), time))
+
+    def get_state(self, u_out: Optional[np.ndarray] = None, v_out: Optional[np.ndarray] = None):
+        u = np.empty(3 * self.n_nodes) if u_out is None else u_out
+        v = np.empty(3 * self.n_nodes) if v_out is None else v_out
+        t = C.c_double()
+        capi.check(capi.lib().sdx_get_state(self._ctx, capi.ptr(u), capi.ptr(v), C.byref(t)))
+        return u, v, t.value
+
+    # stepping ------------------------------------------------------------------------------------
+    def step(self, n: int = 1):
+        capi.check(capi.lib().sdx_step(self._ctx, int(n)))
+
+    def stats(self):
+        arr = (capi.EnvStats * self.n_envs)()
+        capi.check(capi.lib().sdx_get_stats(self._ctx, arr))
+        return [dict(newton_iters=s.newton_iters, cg_iters=s.cg_iters, ls_iters=s.ls_iters,
+                     convergence=s.convergence, res_norm0=s.res_norm0, res_norm=s.res_norm,
+                     n_contacts=s.n_contacts) for s in arr]
+
+    def kernel_launches(self) -> int:
+        return int(capi.lib().sdx_kernel_launches(self._ctx))
+
+    # parity ----------------------------------------------------------------------------------------
+    def pattern(self):
+        rp = np.zeros(self.n_nodes + 1, np.int64)
+        col = np.zeros(self.nnzb, np.int32)
+        capi.check(capi.lib().sdx_get_pattern(self._ctx, capi.ptr(rp, capi._lp), capi.ptr(col, capi._ip)))
+        return rp, col
+
+    def faces(self):
+        fn = np.zeros(3 * self.n_faces, np.int32)
+        ft = np.zeros(self.n_faces, np.int32)
+        fa = np.zeros(self.n_faces)
+        capi.check(capi.lib().sdx_get_faces(self._ctx, capi.ptr(fn, capi._ip), capi.ptr(ft, capi._ip),
+                                            capi.ptr(fa)))
+        return fn, ft, fa
+
+    def assemble(self, u: Optional[np.ndarray] = None, t: float = 0.0, hess: bool = True, psd: bool = True,
+                 obj: bool = True):
+        flags = capi.SDX_ASM_RES | (capi.SDX_ASM_OBJ if obj else 0) | (capi.SDX_ASM_PSD if psd else 0)
+        o = np.zeros(self.n_envs)
+        g = np.zeros(3 * self.n_nodes)
+        H = np.zeros(9 * self.nnzb, np.float32) if hess else None
+        npairs = np.zeros(self.n_envs, np.int64)
+        uu = None if u is None else np.ascontiguousarray(u, np.float64).reshape(-1)
+        capi.check(capi.lib().sdx_assemble(self._ctx, capi.ptr(uu), t, flags, capi.ptr(o), capi.ptr(g),
+                                           capi.ptr(H, capi._fp), capi.ptr(npairs, capi._lp)))
+        return {"obj": o, "g": g, "H": None if H is None else H.reshape(-1, 3, 3), "n_pairs": npairs}
+
+    def contact_pairs(self) -> np.ndarray:
+        n = C.c_int64()
+        capi.check(capi.lib().sdx_get_contact_pairs(self._ctx, None, 0, C.byref(n)))
+        out = np.zeros(max(1, n.value), np.int64)
+        capi.check(capi.lib().sdx_get_contact_pairs(self._ctx, capi.ptr(out, capi._lp), out.size, C.byref(n)))
+        return out[: n.value]
+
+    def bench_spmv(self, reps: int = 20):
+        ms, by = C.c_double(), C.c_double()
+        capi.check(capi.lib().sdx_bench_spmv(self._ctx, reps, C.byref(ms), C.byref(by)))
+        return ms.value, by.value
