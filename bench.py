@@ -1,0 +1,306 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 implicit soft-body step (one JSON line on rank 0).
+
+Workload (default): the single large body with contact — a 64^3-cell tet grid (274,625 nodes,
+1,572,864 tets) of heterogeneous stable Neo-Hookean (E log-uniform [1e4, 1e6] Pa, nu = 0.45) pressed
+by 5 moving capsules (penalty stiffness 1e4, activation distance 1 mm), backward Euler dt = 1/240,
+Newton to rel 1e-6 with Jacobi-PCG at rel. residual 1e-6. A step is one backward-Euler step of every
+env of the batch. Inputs (matrix ~160 MB, tet data ~300 MB) exceed the 126 MB L2.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload cfg1|cfg0|cfg2]
+
+N > 1 runs one independent replica per GPU (the path shards by environment and has no exchange),
+launched by torchrun; timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "env-steps/sec at rel-res 1e-6: learned warm-start vs plain PCG; SpMV HBM GB/s"
+UNIT = "env-steps/s"
+
+
+def measured_peaks():
+    p = os.path.join(HERE, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary (profiles/traffic.txt)."""
+    p = os.path.join(HERE, "profiles", "traffic.txt")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            parts = line.split()
+            if len(parts) >= 2 and parts[0] == kernel:
+                try:
+                    return float(parts[1])
+                except ValueError:
+                    return None
+    return None
+
+
+def build_workload(name: str, seed: int = 0):
+    from project_superdex_b200 import scenes
+    if name == "cfg0":
+        return scenes.config0(seed), "single soft cube 10^3 cells (1,331 nodes, 6,000 tets), no contact"
+    if name == "cfg1":
+        return scenes.config1(seed), ("single body 64^3 cells (274,625 nodes, 1,572,864 tets), E log-uniform "
+                                      "[1e4,1e6], nu 0.45, 5 capsules r=4mm L=20mm at 0.05 m/s, k=1e4")
+    if name == "cfg2":
+        n = int(os.environ.get("SDX_CFG2_ENVS", "1024"))
+        return scenes.config2(seed, n_envs=n), f"{n} uneven bodies, cells/axis U{{8..40}}, 5 capsules + plane each"
+    raise ValueError(name)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        if not self.path or not os.path.exists(self.path):
+            return out
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                cols = [c.strip() for c in line.split(",")]
+                if len(cols) < 9:
+                    continue
+                try:
+                    sm.append(float(cols[1]))
+                    mx.append(float(cols[2]))
+                except ValueError:
+                    continue
+                for nme, v in zip(names, cols[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nme)
+        os.unlink(self.path)
+        if sm:
+            out["sm_mhz"] = statistics.median(sm)
+            out["sm_max_mhz"] = max(mx)
+        out["reasons"] = sorted(reasons)
+        out["samples"] = len(sm)
+        return out
+
+
+def cpu_oracle_sample(workload: str, seed: int = 0):
+    """The CPU restatement of the reference path (oracle/) on a bounded sample: one backward-Euler
+    step of the first env of the workload from rest, all host threads."""
+    from oracle import oracle as O
+    (bodies, cfg), _ = build_workload(workload, seed)
+    b = bodies[0]
+    s = O.Scene(b, cfg)
+    u = np.zeros(3 * b.n_nodes)
+    v = np.zeros_like(u)
+    prm = O.default_newton_params()
+    prm.abs_tol = 1e-9  # same Newton stopping test as the GPU arm: rel 1e-6
+    t0 = time.perf_counter()
+    u, v, st = s.step(u, v, cfg.dt, prm)
+    dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": UNIT, "cores": int(O.lib().or_num_threads()), "kind": "port",
+            "sample": (f"1 backward-Euler step of env 0 of {workload} from rest ({st.newton_iters} Newton "
+                       f"iterations, {st.cg_iters} CG iterations) in {dt:.2f} s")}
+
+
+def vector_bytes_per_node():
+    # algorithmic bytes per node per CG iteration of the fused PCG besides the matrix:
+    # phase 1: z own 12 + z gather 12 + p r/w 24 + q r/w 24; phase 2: x r/w 48 (FP64),
+    # r r/w 48 (FP64), p 12, q 12, dinv 12, z r/w 24
+    return 12 + 12 + 24 + 24 + 48 + 48 + 12 + 12 + 12 + 24
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from project_superdex_b200.soft_body import SoftBodyWorld
+    torch.cuda.set_device(local_rank)
+    (bodies, cfg), desc = build_workload(args.workload, seed=args.seed)
+    # Newton to rel 1e-6 (the absolute floor is only a guard for an exactly zero residual)
+    w = SoftBodyWorld(bodies, cfg, device=local_rank, warm_start=args.warm_start, newton_abs_tol=1e-9)
+    n_envs = w.n_envs
+    stream = torch.cuda.ExternalStream(w.stream_handle(), device=local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    w.step(args.warmup)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches0 = w.kernel_launches()
+    w.set_profiling(True)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        w.step(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    prof = w.profile()
+    w.set_profiling(False)
+    launches = w.kernel_launches() - launches0
+    stats = w.stats()
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n_envs * args.steps / (ms / 1000.0)
+
+    # roofline of the dominant kernel (the persistent PCG)
+    peak, peak_kind = measured_peaks()
+    bytes_iter = w.nnzb * 40 + 4 * (w.n_nodes + 1) + vector_bytes_per_node() * w.n_nodes
+    pcg_s = prof["pcg_ms"] / 1000.0
+    achieved = prof["pcg_iters"] * bytes_iter / pcg_s / 1e9 if pcg_s > 0 else None
+    traffic = ncu_traffic("k_pcg_per_iter")
+    roofline = {"bound": "hbm", "kernel": "k_pcg (persistent Jacobi-PCG)", "achieved": achieved,
+                "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                "peak_source": peak_kind, "traffic": traffic, "bytes_per_iter": bytes_iter,
+                "iters": prof["pcg_iters"], "share_of_step": prof["pcg_ms"] / ms}
+    # standalone SpMV on the last assembled matrix
+    spmv_ms, spmv_bytes = w.bench_spmv(reps=20)
+    spmv = {"achieved_gbs": spmv_bytes / (spmv_ms / 1000.0) / 1e9, "ms": spmv_ms, "bytes": spmv_bytes}
+    spmv["frac"] = spmv["achieved_gbs"] / peak
+
+    # end to end through the public API with pinned host buffers, copies inside the timed region
+    hu = torch.empty(3 * w.n_nodes, dtype=torch.float64, pin_memory=True).numpy()
+    hv = torch.empty(3 * w.n_nodes, dtype=torch.float64, pin_memory=True).numpy()
+    _, _, t_state = w.get_state(hu, hv)
+    e2e_steps = max(1, min(args.steps, 5))
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    t_wall = time.perf_counter()
+    for _ in range(e2e_steps):
+        w.set_state(hu, hv, t_state)
+        w.step(1)
+        _, _, t_state = w.get_state(hu, hv)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": world * n_envs * e2e_steps / (e2e_ms / 1000.0), "unit": UNIT,
+           "h2d_bytes_per_step": 2 * 3 * 8 * w.n_nodes, "d2h_bytes_per_step": 2 * 3 * 8 * w.n_nodes,
+           "steps": e2e_steps}
+    cg_per_step = sum(s["cg_iters"] for s in stats) / max(1, n_envs)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic (seeded tet grids, random materials and collider trajectories)",
+        "config": {"workload": f"{args.workload}: {desc}", "n_envs": n_envs, "n_nodes": w.n_nodes,
+                   "n_tets": w.n_tets, "nnzb": w.nnzb,
+                   "precision": "FP32 Hessian assembly + SpMV, FP64 residual / energy / CG dots / x,r",
+                   "warm_start": ["zero", "previous", "learned"][args.warm_start],
+                   "cg_rel_tol": 1e-6, "newton_rel_tol": 1e-6, "newton_abs_tol": 1e-9,
+                   "l2": "inputs larger than L2 (matrix + tet data > 126 MB)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "roofline": roofline, "spmv": spmv, "e2e": e2e, "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "solver": {"cg_iters_per_step": cg_per_step,
+                   "newton_iters_per_step": sum(s["newton_iters"] for s in stats) / max(1, n_envs),
+                   "profile_ms": {k: v for k, v in prof.items() if k.endswith("_ms")}},
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_oracle_sample(args.workload, args.seed)
+    w.close()
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2"])
+    ap.add_argument("--warm-start", type=int, default=0, dest="warm_start")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        # The reference's own implementation of this path is CPU code; its timed stand-in is the CPU
+        # restatement in oracle/ (the reference's full step needs its cmake build). Rank 0 only.
+        if rank != 0:
+            return 0
+        cb = cpu_oracle_sample(args.workload, args.seed)
+        line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / cb["value"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": {"workload": args.workload}, "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    line = run_ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -200,6 +200,26 @@ int sdx_bench_spmv(sdx_context* ctx, int reps, double* ms_per_spmv, double* byte
 /* Count of kernel launches issued by this context since creation (for launch accounting). */
 int64_t sdx_kernel_launches(sdx_context* ctx);
 
+/* The CUDA stream (cudaStream_t) all work of this context is issued on, for event timing by callers. */
+int sdx_get_stream(sdx_context* ctx, void** stream);
+
+/* Opt-in per-kernel device timing (CUDA events on the context stream around each launch). */
+typedef struct {
+  double pcg_ms;            /* persistent PCG launches */
+  int64_t pcg_launches;
+  int64_t pcg_iters;        /* sum over launches of the largest iteration count of the batch */
+  double asm_hess_ms;       /* element kernel launches that assemble the Hessian */
+  int64_t asm_hess_launches;
+  double asm_res_ms;        /* element kernel launches that assemble the residual only */
+  int64_t asm_res_launches;
+  double contact_ms;
+  int64_t contact_launches;
+  double seed_ms;           /* Hessian seeding with the scaled mass matrix */
+  int64_t seed_launches;
+} sdx_profile;
+int sdx_set_profiling(sdx_context* ctx, int enable);
+int sdx_get_profile(sdx_context* ctx, sdx_profile* out);
+
 #ifdef __cplusplus
 }
 #endif

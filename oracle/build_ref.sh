@@ -12,7 +12,7 @@ if [ ! -d "$M/mochi_core/include" ]; then
   exit 0
 fi
 mkdir -p "$HERE/_ref"
-"${REF_CXX:-/usr/bin/g++}" -std=c++20 -O2 -fPIC -shared -DMOCHI_USE_DOUBLE_PRECISION=1 \
+"${REF_CXX:-/usr/bin/g++}" -std=c++20 -O2 -w -fPIC -shared -DMOCHI_USE_DOUBLE_PRECISION=1 \
   -I"$M/mochi_core/include" -I"$M/third_party/eigen" \
   "$HERE/ref_shim.cpp" "$M/mochi_core/src/materials/batched_smith_neo_hookean.cpp" \
   -o "$HERE/_ref/libsdx_ref.so"

@@ -27,7 +27,8 @@ EXPORTED = [
     "sdx_pcg_solve", "sdx_pcg_solve_ctx", "sdx_create", "sdx_destroy", "sdx_upload_bodies",
     "sdx_set_colliders", "sdx_set_params", "sdx_set_state", "sdx_get_state", "sdx_get_sizes",
     "sdx_get_pattern", "sdx_get_faces", "sdx_assemble", "sdx_get_contact_pairs", "sdx_step",
-    "sdx_get_stats", "sdx_bench_spmv", "sdx_kernel_launches",
+    "sdx_get_stats", "sdx_bench_spmv", "sdx_kernel_launches", "sdx_get_stream",
+    "sdx_set_profiling", "sdx_get_profile",
 ]
 
 
@@ -60,6 +61,14 @@ class EnvStats(C.Structure):
     _fields_ = [("newton_iters", C.c_int), ("cg_iters", C.c_int), ("ls_iters", C.c_int),
                 ("convergence", C.c_int), ("res_norm0", C.c_double), ("res_norm", C.c_double),
                 ("n_contacts", C.c_int64)]
+
+
+class Profile(C.Structure):
+    _fields_ = [("pcg_ms", C.c_double), ("pcg_launches", C.c_int64), ("pcg_iters", C.c_int64),
+                ("asm_hess_ms", C.c_double), ("asm_hess_launches", C.c_int64),
+                ("asm_res_ms", C.c_double), ("asm_res_launches", C.c_int64),
+                ("contact_ms", C.c_double), ("contact_launches", C.c_int64),
+                ("seed_ms", C.c_double), ("seed_launches", C.c_int64)]
 
 
 _dp = C.POINTER(C.c_double)
@@ -110,6 +119,9 @@ def lib():
     L.sdx_bench_spmv.argtypes = [_vp, C.c_int, _dp, _dp]
     L.sdx_kernel_launches.argtypes = [_vp]
     L.sdx_kernel_launches.restype = C.c_int64
+    L.sdx_get_stream.argtypes = [_vp, C.POINTER(C.c_void_p)]
+    L.sdx_set_profiling.argtypes = [_vp, C.c_int]
+    L.sdx_get_profile.argtypes = [_vp, C.POINTER(Profile)]
     _lib = L
     return L
 

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -83,8 +84,10 @@ struct PcgPartition {
   int* cta_pbase = nullptr;
   int* env_cta0 = nullptr;
   int* env_cta1 = nullptr;
+  int* env_poff = nullptr;
   double* part = nullptr;
   void release() {
+    dfree(env_poff);
     dfree(cta_slice);
     dfree(cta_env0);
     dfree(cta_env1);
@@ -191,7 +194,75 @@ struct sdx_context {
   double *solo_b = nullptr, *solo_x = nullptr;
   PcgPartition solo_part;
   PcgWork solo_work;
+  // opt-in per-kernel timing: event pairs resolved lazily
+  bool profiling = false;
+  sdx_profile prof;
+  std::vector<cudaEvent_t> ev_pool;
+  struct Pending {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<Pending> pending;
 };
+
+enum { PROF_PCG = 0, PROF_HESS = 1, PROF_RES = 2, PROF_CONTACT = 3, PROF_SEED = 4 };
+
+static cudaEvent_t pool_event(sdx_context* c) {
+  if (!c->ev_pool.empty()) {
+    cudaEvent_t e = c->ev_pool.back();
+    c->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+static void prof_begin(sdx_context* c, cudaEvent_t* a) {
+  *a = nullptr;
+  if (!c->profiling) return;
+  *a = pool_event(c);
+  cudaEventRecord(*a, c->stream);
+}
+
+static void prof_end(sdx_context* c, int kind, cudaEvent_t a) {
+  if (!c->profiling || !a) return;
+  cudaEvent_t b = pool_event(c);
+  cudaEventRecord(b, c->stream);
+  c->pending.push_back({kind, a, b});
+}
+
+static void prof_resolve(sdx_context* c) {
+  for (auto& pd : c->pending) {
+    cudaEventSynchronize(pd.b);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, pd.a, pd.b);
+    switch (pd.kind) {
+      case PROF_PCG:
+        c->prof.pcg_ms += ms;
+        break;
+      case PROF_HESS:
+        c->prof.asm_hess_ms += ms;
+        c->prof.asm_hess_launches++;
+        break;
+      case PROF_RES:
+        c->prof.asm_res_ms += ms;
+        c->prof.asm_res_launches++;
+        break;
+      case PROF_CONTACT:
+        c->prof.contact_ms += ms;
+        c->prof.contact_launches++;
+        break;
+      case PROF_SEED:
+        c->prof.seed_ms += ms;
+        c->prof.seed_launches++;
+        break;
+    }
+    c->ev_pool.push_back(pd.a);
+    c->ev_pool.push_back(pd.b);
+  }
+  c->pending.clear();
+}
 
 static void release_topology(sdx_context* c) {
   dfree(c->slice_ptr);
@@ -371,11 +442,16 @@ static int choose_partition(sdx_context* c, int n_slices, const std::vector<int>
                             const std::vector<int>& slice_ptr, PcgPartition& P, int threads_req,
                             int ctas_per_sm_req) {
   P.release();
-  const int threads = threads_req > 0 ? threads_req : 256;
+  // launch shape: explicit request, else SDX_PCG_THREADS / SDX_PCG_CTAS_PER_SM, else 1024 x 1
+  if (threads_req <= 0 && getenv("SDX_PCG_THREADS")) threads_req = atoi(getenv("SDX_PCG_THREADS"));
+  if (ctas_per_sm_req <= 0 && getenv("SDX_PCG_CTAS_PER_SM")) ctas_per_sm_req = atoi(getenv("SDX_PCG_CTAS_PER_SM"));
+  if (threads_req > 0 && (threads_req % 32 != 0 || threads_req > 1024))
+    return set_error(SDX_ERR_INVALID_ARGUMENT, "PCG threads must be a multiple of 32 up to 1024");
+  const int threads = threads_req > 0 ? threads_req : 1024;
   const int max_active = pcg_max_ctas_per_sm(threads);
   if (max_active <= 0) return set_error(SDX_ERR_CUDA, "PCG kernel cannot be resident with %d threads", threads);
-  // cooperative launch: every CTA must be co-resident (default 2 CTAs per SM)
-  const int per_sm = std::min(max_active, ctas_per_sm_req > 0 ? ctas_per_sm_req : 2);
+  // cooperative launch: every CTA must be co-resident
+  const int per_sm = std::min(max_active, ctas_per_sm_req > 0 ? ctas_per_sm_req : 1);
   int n_cta = c->num_sms * per_sm;
   // each CTA may cover at most kPcgMaxEnvsPerCta envs; grow CTAs over weight-balanced slices
   const int64_t total_w = slice_ptr[n_slices];
@@ -430,7 +506,10 @@ static int choose_partition(sdx_context* c, int n_slices, const std::vector<int>
   SDX_TRY(upload(&P.cta_pbase, pbase));
   SDX_TRY(upload(&P.env_cta0, ec0));
   SDX_TRY(upload(&P.env_cta1, ec1));
-  SDX_TRY(dalloc(&P.part, (size_t)2 * std::max(1, pbase[n_cta]) * kPcgNq));
+  std::vector<int> poff(n_envs + 1, 0);
+  for (int ev = 0; ev < n_envs; ++ev) poff[ev + 1] = poff[ev] + std::max(0, ec1[ev] - ec0[ev] + 1);
+  SDX_TRY(upload(&P.env_poff, poff));
+  SDX_TRY(dalloc(&P.part, (size_t)2 * std::max(1, poff[n_envs]) * kPcgNq));
   P.n_cta = n_cta;
   P.threads = threads;
   return SDX_OK;
@@ -482,6 +561,7 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
   a.cta_pbase = P.cta_pbase;
   a.env_cta0 = P.env_cta0;
   a.env_cta1 = P.env_cta1;
+  a.env_poff = P.env_poff;
   a.part = P.part;
   a.env_mask = env_mask;
   a.rel_tol = lp.rel_tol;
@@ -503,13 +583,22 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
   SDX_CUDA(cudaMemcpyAsync(W.sync, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
   SDX_CUDA(cudaMemsetAsync(W.out_iters, 0, sizeof(int) * n_envs, c->stream));
   SDX_CUDA(cudaMemsetAsync(W.out_conv, 0, sizeof(int) * n_envs, c->stream));
+  cudaEvent_t ev;
+  prof_begin(c, &ev);
   cudaError_t e = launch_pcg(a, P.n_cta, P.threads, c->stream);
   c->launches++;
   if (e != cudaSuccess) return set_error(SDX_ERR_CUDA, "PCG cooperative launch: %s", cudaGetErrorString(e));
+  prof_end(c, PROF_PCG, ev);
   unsigned flags[8];
   SDX_CUDA(cudaMemcpyAsync(flags, W.sync, sizeof(flags), cudaMemcpyDeviceToHost, c->stream));
   SDX_CUDA(cudaStreamSynchronize(c->stream));
   if (flags[2] != 0u) return set_error(SDX_ERR_DEVICE_TIMEOUT, "PCG grid barrier timed out");
+  if (c->profiling) {
+    std::vector<int> its(n_envs);
+    SDX_CUDA(cudaMemcpy(its.data(), W.out_iters, sizeof(int) * n_envs, cudaMemcpyDeviceToHost));
+    c->prof.pcg_iters += *std::max_element(its.begin(), its.end());
+    c->prof.pcg_launches++;
+  }
   return SDX_OK;
 }
 
@@ -585,12 +674,35 @@ extern "C" int sdx_destroy(sdx_context* c) {
   cudaStreamSynchronize(c->stream);
   release_topology(c);
   release_solo(c);
+  prof_resolve(c);
+  for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   cudaStreamDestroy(c->stream);
   delete c;
   return SDX_OK;
 }
 
 extern "C" int64_t sdx_kernel_launches(sdx_context* c) { return c ? c->launches : 0; }
+
+extern "C" int sdx_get_stream(sdx_context* c, void** stream) {
+  if (!c || !stream) return set_error(SDX_ERR_INVALID_ARGUMENT, "null argument");
+  *stream = (void*)c->stream;
+  return SDX_OK;
+}
+
+extern "C" int sdx_set_profiling(sdx_context* c, int enable) {
+  if (!c) return set_error(SDX_ERR_INVALID_ARGUMENT, "null context");
+  prof_resolve(c);
+  c->profiling = enable != 0;
+  memset(&c->prof, 0, sizeof(c->prof));
+  return SDX_OK;
+}
+
+extern "C" int sdx_get_profile(sdx_context* c, sdx_profile* out) {
+  if (!c || !out) return set_error(SDX_ERR_INVALID_ARGUMENT, "null argument");
+  prof_resolve(c);
+  *out = c->prof;
+  return SDX_OK;
+}
 
 extern "C" int sdx_set_params(sdx_context* c, const sdx_step_params* p) {
   if (!c || !p) return set_error(SDX_ERR_INVALID_ARGUMENT, "null argument");
@@ -976,9 +1088,12 @@ static void assemble_dev(sdx_context* c, const double* u, const double* ut, doub
     launch_zero_rows(c->n_slices, c->slice_env, mask, c->g, c->stream);
     c->launches++;
   }
+  cudaEvent_t ev;
   if (flags & SDX_ASM_HESS) {
+    prof_begin(c, &ev);
     launch_seed_hessian(ctx_matrix(c), c->mass, c->pin, mask, (float)dtfi2, c->stream);
     c->launches++;
+    prof_end(c, PROF_SEED, ev);
   }
   ElemArgs ea;
   memset(&ea, 0, sizeof(ea));
@@ -1006,8 +1121,10 @@ static void assemble_dev(sdx_context* c, const double* u, const double* ut, doub
   ea.min_eig = 1.1920928955078125e-07f;  // kMinProjectedEigenvalue of the FP32 build
   ea.psd = p.psd_strategy;
   ea.flags = flags;
+  prof_begin(c, &ev);
   launch_element(ea, c->stream);
   c->launches++;
+  prof_end(c, (flags & SDX_ASM_HESS) ? PROF_HESS : PROF_RES, ev);
   if (c->n_colliders > 0 || record_pairs) {
     ContactArgs ca;
     memset(&ca, 0, sizeof(ca));
@@ -1032,8 +1149,10 @@ static void assemble_dev(sdx_context* c, const double* u, const double* ut, doub
     ca.thr = p.thr;
     ca.max_align = p.max_align;
     ca.flags = flags;
+    prof_begin(c, &ev);
     launch_contact(ca, c->stream);
     c->launches++;
+    prof_end(c, PROF_CONTACT, ev);
   }
 }
 

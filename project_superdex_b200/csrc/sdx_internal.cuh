@@ -6,9 +6,11 @@
 //     32-row slice belongs to exactly one env. Vectors are indexed by row (3 components per row).
 //   * matrix: 3x3 sliced-ELL ("SELL-32 of 3x3 blocks"). Slice s covers rows [32s, 32s+32) and has
 //     width w_s = the longest block row in it. Block position p = slice_ptr[s] + 32k + lane holds the
-//     k-th block of row 32s+lane; its column is col[p] (padding: row | 0x80000000) and its 9 values
-//     are interleaved per (slice, k) group: val[(p - lane) * 9 + 32 e + lane], e = 3r + c. A warp
-//     reading one (slice, k) group loads 9 fully coalesced 128-byte lines.
+//     k-th block of row 32s+lane; its column is col[p] (padding: row | 0x80000000). The 9 values of
+//     the 32 blocks of one (slice, k) group occupy 1152 contiguous bytes starting at G = (p - lane) * 9
+//     floats, split 4 + 4 + 1: entries e = 0..3 of lane l at G + 4l + e, entries 4..7 at
+//     G + 128 + 4l + (e - 4), entry 8 at G + 256 + l (e = 3r + c). A warp loads a group with two
+//     fully coalesced 128-bit loads and one 32-bit load per lane.
 //   * per tet: int4 rows, 4 float4 rest records (dN 12, vol, mu, lambda, rho) stored as 4 separate
 //     float4 arrays (coalesced), 4 int4 records of the 16 block positions its 4x4 blocks scatter to.
 #pragma once
@@ -23,7 +25,9 @@ constexpr int kPcgMaxEnvsPerCta = 32;
 constexpr int kPcgNq = 3;
 
 __host__ __device__ __forceinline__ size_t val_index(int64_t p, int e) {
-  return (size_t)(p - (p & 31)) * 9 + (size_t)e * 32 + (size_t)(p & 31);
+  const size_t g = (size_t)(p - (p & 31)) * 9;
+  const size_t l = (size_t)(p & 31);
+  return e < 4 ? g + 4 * l + e : (e < 8 ? g + 128 + 4 * l + (e - 4) : g + 256 + l);
 }
 
 struct Matrix {
@@ -100,6 +104,7 @@ struct PcgArgs {
   const int* cta_pbase;
   const int* env_cta0;
   const int* env_cta1;
+  const int* env_poff;  // partials of env e live at [env_poff[e], env_poff[e] + env_cta1[e] - env_cta0[e]]
   double* part;
   const uint8_t* env_mask;
   const double* env_rel_tol;  // per-env relative tolerance (NULL: rel_tol)

@@ -55,10 +55,9 @@ __global__ void k_seed_hessian(Matrix A, const float* __restrict__ mass, const u
   for (int k = 0; k < w; ++k) {
     const int p = base + k * kSlice + lane;
     const int cj = A.col[p];
-    float* vp = A.val + val_index(p, 0);
     if (cj & kPadBit) {
 #pragma unroll
-      for (int e = 0; e < 9; ++e) vp[e * 32] = 0.0f;
+      for (int e = 0; e < 9; ++e) A.val[val_index(p, e)] = 0.0f;
       continue;
     }
     const int pc = pin[cj];
@@ -69,7 +68,7 @@ __global__ void k_seed_hessian(Matrix A, const float* __restrict__ mass, const u
       for (int c = 0; c < 3; ++c) {
         float v = (r == c) ? m : 0.0f;
         if (((pr >> r) & 1) || ((pc >> c) & 1)) v = (cj == row && r == c) ? 1.0f : 0.0f;
-        vp[(r * 3 + c) * 32] = v;
+        A.val[val_index(p, r * 3 + c)] = v;
       }
   }
 }
@@ -198,13 +197,12 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
 #pragma unroll
         for (int g = 0; g < 4; ++g) {
           const int p = slot[f * 4 + g];
-          float* vp = a.val + val_index(p, 3 * r);
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
             if ((pins[g] >> c) & 1) continue;
             const float k = vol * (Cf[c * 3 + 0] * dN[3 * g + 0] + Cf[c * 3 + 1] * dN[3 * g + 1] +
                                    Cf[c * 3 + 2] * dN[3 * g + 2]);
-            atomicAdd(vp + c * 32, k);
+            atomicAdd(a.val + val_index(p, 3 * r + c), k);
           }
         }
       }
@@ -455,23 +453,53 @@ void launch_pack_z(int64_t n_rows, const double* x, float4* z, cudaStream_t st) 
 // ------------------------------------------------------------------------------------------------
 // SELL-32 3x3 SpMV building block: acc = A_row . src (one warp per slice, lane = row)
 
+// loads of one (slice, k) group for lane `lane`: 9 values (4 + 4 + 1 split, see val_index)
+__device__ __forceinline__ void load_block(const float* g, int lane, float v[9]) {
+  const float4 a = __ldcs(reinterpret_cast<const float4*>(g) + lane);
+  const float4 b = __ldcs(reinterpret_cast<const float4*>(g + 128) + lane);
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = a.z;
+  v[3] = a.w;
+  v[4] = b.x;
+  v[5] = b.y;
+  v[6] = b.z;
+  v[7] = b.w;
+  v[8] = __ldcs(g + 256 + lane);
+}
+
 template <class Load>
 __device__ __forceinline__ void sell_row_product(const Matrix& A, int s, int lane, Load load, float& a0,
                                                  float& a1, float& a2) {
   const int base = A.slice_ptr[s], w = A.slice_w[s];
   a0 = a1 = a2 = 0.0f;
-#pragma unroll 2
-  for (int k = 0; k < w; ++k) {
-    const int p = base + k * kSlice + lane;
-    const int j = __ldcs(A.col + p) & 0x7fffffff;
-    const float* vp = A.val + (size_t)(base + k * kSlice) * 9 + lane;
+  int k = 0;
+  // four groups per batch: all column, value and gather loads are issued before the FMAs
+  for (; k + 4 <= w; k += 4) {
+    int j[4];
+    float v[4][9];
+    float4 xj[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) j[u] = __ldcs(A.col + base + (k + u) * kSlice + lane) & 0x7fffffff;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) load_block(A.val + (size_t)(base + (k + u) * kSlice) * 9, lane, v[u]);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) xj[u] = load(j[u]);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      a0 = fmaf(v[u][0], xj[u].x, fmaf(v[u][1], xj[u].y, fmaf(v[u][2], xj[u].z, a0)));
+      a1 = fmaf(v[u][3], xj[u].x, fmaf(v[u][4], xj[u].y, fmaf(v[u][5], xj[u].z, a1)));
+      a2 = fmaf(v[u][6], xj[u].x, fmaf(v[u][7], xj[u].y, fmaf(v[u][8], xj[u].z, a2)));
+    }
+  }
+  for (; k < w; ++k) {
+    const int j = __ldcs(A.col + base + k * kSlice + lane) & 0x7fffffff;
+    float v[9];
+    load_block(A.val + (size_t)(base + k * kSlice) * 9, lane, v);
     const float4 xj = load(j);
-    const float v0 = __ldcs(vp + 0 * 32), v1 = __ldcs(vp + 1 * 32), v2 = __ldcs(vp + 2 * 32);
-    const float v3 = __ldcs(vp + 3 * 32), v4 = __ldcs(vp + 4 * 32), v5 = __ldcs(vp + 5 * 32);
-    const float v6 = __ldcs(vp + 6 * 32), v7 = __ldcs(vp + 7 * 32), v8 = __ldcs(vp + 8 * 32);
-    a0 = fmaf(v0, xj.x, fmaf(v1, xj.y, fmaf(v2, xj.z, a0)));
-    a1 = fmaf(v3, xj.x, fmaf(v4, xj.y, fmaf(v5, xj.z, a1)));
-    a2 = fmaf(v6, xj.x, fmaf(v7, xj.y, fmaf(v8, xj.z, a2)));
+    a0 = fmaf(v[0], xj.x, fmaf(v[1], xj.y, fmaf(v[2], xj.z, a0)));
+    a1 = fmaf(v[3], xj.x, fmaf(v[4], xj.y, fmaf(v[5], xj.z, a1)));
+    a2 = fmaf(v[6], xj.x, fmaf(v[7], xj.y, fmaf(v[8], xj.z, a2)));
   }
 }
 
@@ -606,12 +634,13 @@ __device__ __forceinline__ void true_residual(const PcgArgs& a, int s, int lane,
   for (int k = 0; k < w; ++k) {
     const int p = base + k * kSlice + lane;
     const int j = __ldcs(a.A.col + p) & 0x7fffffff;
-    const float* vp = a.A.val + (size_t)(base + k * kSlice) * 9 + lane;
+    float v[9];
+    load_block(a.A.val + (size_t)(base + k * kSlice) * 9, lane, v);
     const double x0 = __ldcg(a.x + 3 * (int64_t)j), x1 = __ldcg(a.x + 3 * (int64_t)j + 1),
                  x2 = __ldcg(a.x + 3 * (int64_t)j + 2);
-    a0 += (double)vp[0] * x0 + (double)vp[32] * x1 + (double)vp[64] * x2;
-    a1 += (double)vp[96] * x0 + (double)vp[128] * x1 + (double)vp[160] * x2;
-    a2 += (double)vp[192] * x0 + (double)vp[224] * x1 + (double)vp[256] * x2;
+    a0 += (double)v[0] * x0 + (double)v[1] * x1 + (double)v[2] * x2;
+    a1 += (double)v[3] * x0 + (double)v[4] * x1 + (double)v[5] * x2;
+    a2 += (double)v[6] * x0 + (double)v[7] * x1 + (double)v[8] * x2;
   }
   const int64_t row = (int64_t)s * kSlice + lane;
   r[0] = a.b[3 * row] - a0;
@@ -640,28 +669,37 @@ __global__ void k_pcg(PcgArgs a) {
     if (lane == 0) wacc[(warp * kPcgMaxEnvsPerCta + le) * kPcgNq + k] += v;
   };
   // Partials of phase 1 live in buffer 1, those of phases 0 and 2 in buffer 0, so a CTA writing the
-  // next phase's partials never overwrites values another CTA is still reducing.
-  const size_t pstride = (size_t)a.cta_pbase[ncta] * kPcgNq;
+  // next phase's partials never overwrites values another CTA is still reducing. The partials of one
+  // env are contiguous (one per covering CTA, in CTA order), so a reduction is a coalesced read.
+  const size_t pstride = (size_t)a.env_poff[a.n_envs] * kPcgNq;
   auto flush_acc = [&](int nq, int buf) {
     __syncthreads();
     for (int i = threadIdx.x; i < ne * nq; i += blockDim.x) {
       const int le = i / nq, k = i % nq;
       double v = 0.0;
       for (int w = 0; w < nwarps; ++w) v += wacc[(w * kPcgMaxEnvsPerCta + le) * kPcgNq + k];
-      a.part[buf * pstride + (size_t)(a.cta_pbase[c] + le) * kPcgNq + k] = v;
+      const int e = e0 + le;
+      a.part[buf * pstride + (size_t)(a.env_poff[e] + (c - a.env_cta0[e])) * kPcgNq + k] = v;
     }
   };
   auto reduce_tot = [&](int nq, int buf) {
-    for (int le = warp; le < ne; le += nwarps) {
+    // one warp per (env, quantity); fixed summation order, identical in every CTA
+    for (int i = warp; i < ne * nq; i += nwarps) {
+      const int le = i / nq, k = i % nq;
       const int e = e0 + le;
-      const int ca = a.env_cta0[e], cb = a.env_cta1[e];
-      for (int k = 0; k < nq; ++k) {
-        double v = 0.0;
-        for (int cc = ca + lane; cc <= cb; cc += 32)
-          v += __ldcg(a.part + buf * pstride + (size_t)(a.cta_pbase[cc] + e - a.cta_env0[cc]) * kPcgNq + k);
-        v = warp_sum(v);
-        if (lane == 0) tot[le][k] = v;
+      const int n = a.env_cta1[e] - a.env_cta0[e] + 1;
+      const double* src = a.part + buf * pstride + (size_t)a.env_poff[e] * kPcgNq + k;
+      double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+      int j = lane;
+      for (; j + 96 < n; j += 128) {
+        v0 += __ldcg(src + (size_t)j * kPcgNq);
+        v1 += __ldcg(src + (size_t)(j + 32) * kPcgNq);
+        v2 += __ldcg(src + (size_t)(j + 64) * kPcgNq);
+        v3 += __ldcg(src + (size_t)(j + 96) * kPcgNq);
       }
+      for (; j < n; j += 32) v0 += __ldcg(src + (size_t)j * kPcgNq);
+      const double v = warp_sum((v0 + v1) + (v2 + v3));
+      if (lane == 0) tot[le][k] = v;
     }
     __syncthreads();
   };

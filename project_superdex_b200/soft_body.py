@@ -141,6 +141,19 @@ class SoftBodyWorld:
         capi.check(capi.lib().sdx_get_contact_pairs(self._ctx, capi.ptr(out, capi._lp), out.size, C.byref(n)))
         return out[: n.value]
 
+    def stream_handle(self) -> int:
+        h = C.c_void_p()
+        capi.check(capi.lib().sdx_get_stream(self._ctx, C.byref(h)))
+        return int(h.value or 0)
+
+    def set_profiling(self, enable: bool = True):
+        capi.check(capi.lib().sdx_set_profiling(self._ctx, int(enable)))
+
+    def profile(self) -> dict:
+        p = capi.Profile()
+        capi.check(capi.lib().sdx_get_profile(self._ctx, C.byref(p)))
+        return {f: getattr(p, f) for f, _ in capi.Profile._fields_}
+
     def bench_spmv(self, reps: int = 20):
         ms, by = C.c_double(), C.c_double()
         capi.check(capi.lib().sdx_bench_spmv(self._ctx, reps, C.byref(ms), C.byref(by)))

@@ -1,0 +1,164 @@
+"""Generates the golden fixtures of this directory from the reference (run where the reference tree
+exists; the fixtures are committed, nothing reads the reference at test time).
+
+  * smith_nh_reference.json — the 5 Smith Neo-Hookean known-answer cases of the reference test suite
+    (mochi_core/test/data/material_test_data.h, smith_neo_hookean_test_data, E = 1, nu = 0.4), read
+    as text from the header.
+  * krylov_psd100.json — the reference's 100 x 100 SPD golden system (matrix, rhs, solution) from
+    mochi_core/test/data/krylov_solver_test_data.h, read as text.
+  * reference_vectors.json — outputs of the reference's own compiled code (oracle/_ref, built by
+    oracle/build_ref.sh from the reference sources) on seeded inputs: Smith NH with every PSD
+    strategy (projected tangents), PolyReLU, the penalty contact response, fem::StressWork on single
+    tets, and krylov::PCG iteration counts / solutions on the two golden systems.
+
+  python tests/golden/make_golden.py [--reference-root /path/to/reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+NUM = r"[-+]?(?:\d+\.\d*|\.\d+|\d+)(?:[eE][-+]?\d+)?"
+
+
+def parse_smith(path):
+    text = open(path).read()
+    start = text.index("namespace smith_neo_hookean_test_data")
+    end = text.index("} // namespace smith_neo_hookean_test_data")
+    block = text[start:end]
+    cases = []
+    for chunk in re.split(r"\bTestData\{", block)[1:]:
+        nums = [float(x) for x in re.findall(NUM + r"(?=_r)", chunk)]
+        assert len(nums) == 9 + 1 + 9 + 81, len(nums)
+        cases.append({"F": nums[0:9], "energy": nums[9], "pk1": nums[10:19], "tangent": nums[19:100]})
+    return {"youngs_modulus": 1.0, "poisson_ratio": 0.4, "source": "material_test_data.h smith block",
+            "cases": cases}
+
+
+def parse_array(text, name, kind=float):
+    m = re.search(name + r"\[\]\s*=\s*\{(.*?)\};", text, re.S)
+    vals = re.findall(NUM, m.group(1))
+    return [kind(v) for v in vals]
+
+
+def parse_krylov(path):
+    text = open(path).read()
+    rows = parse_array(text, "kPsdMatrixRows", int)
+    cols = parse_array(text, "kPsdMatrixCols", int)
+    vals = parse_array(text, "kPsdMatrixVals")
+    rhs = parse_array(text, "kPsdMatrixRhs")
+    out = parse_array(text, "kPsdMatrixOut")
+    assert len(rows) == len(cols) == len(vals) == 3718 and len(rhs) == len(out) == 100
+    return {"n": 100, "rows": rows, "cols": cols, "vals": vals, "rhs": rhs, "solution": out,
+            "source": "krylov_solver_test_data.h kPsdMatrix*"}
+
+
+def tridiag64():
+    n = 64
+    A = np.diag(np.full(n, 2.0)) - np.diag(np.ones(n - 1), 1) - np.diag(np.ones(n - 1), -1)
+    return A, np.ones(n)
+
+
+def reference_vectors():
+    from oracle import oracle as O
+    R = O.ref()
+    assert R is not None, "oracle/_ref/libsdx_ref.so missing: run oracle/build_ref.sh"
+    rng = np.random.default_rng(20261203)
+    out = {"smith": [], "polyrelu": [], "penalty": [], "stress_work": [], "pcg": []}
+    for i in range(48):
+        F = np.eye(3) + rng.normal(0, 0.35, (3, 3))
+        if i % 4 == 0:
+            F[:, 0] *= -1.0  # inverted element
+        mu, lam = float(rng.uniform(0.2, 3.0)), float(rng.uniform(0.5, 30.0))
+        for psd in (0, 1, 2, 3):
+            e, P, Cm = O.ref_smith_nh(mu, lam, F, project=psd != 0, psd=psd, oracle_kind=1)
+            out["smith"].append({"mu": mu, "lambda": lam, "F": F.reshape(-1).tolist(), "psd": psd,
+                                 "energy": e, "pk1": P.reshape(-1).tolist(), "tangent": Cm.reshape(-1).tolist()})
+    for x in np.linspace(-0.02, 0.02, 41):
+        f, df, ddf = O.polyrelu(float(x), 0.005, 0.004, use_ref=True)
+        out["polyrelu"].append({"x": float(x), "t": 0.005, "shift": 0.004, "f": f, "df": df, "ddf": ddf})
+    for i in range(40):
+        d = float(rng.uniform(-0.012, 0.003))
+        g = rng.normal(size=3)
+        g /= np.linalg.norm(g)
+        k = float(10 ** rng.uniform(3, 9))
+        e = np.zeros(1)
+        f = np.zeros(3)
+        df = np.zeros(6)
+        R.ref_penalty(d, O.ptr(g), k, 0.005, 0.001, O.ptr(e), O.ptr(f), O.ptr(df))
+        out["penalty"].append({"d": d, "grad": g.tolist(), "k": k, "t_half": 0.005, "thr": 0.001,
+                               "energy": float(e[0]), "force": f.tolist(), "dforce6": df.tolist()})
+    for i in range(24):
+        X = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], float) * 0.01 + rng.normal(0, 0.001, (4, 3))
+        D = np.stack([X[k] - X[0] for k in (1, 2, 3)], axis=1)
+        if np.linalg.det(D) < 0:
+            X[[1, 2]] = X[[2, 1]]
+        u = rng.normal(0, 0.003, (4, 3))
+        mu, lam = float(rng.uniform(1e3, 1e5)), float(rng.uniform(1e3, 1e6))
+        for proj in (0, 1):
+            e = np.zeros(1)
+            r = np.zeros(12)
+            K = np.zeros(144)
+            R.ref_stress_work(O.ptr(np.ascontiguousarray(X.reshape(-1))), O.ptr(np.ascontiguousarray(u.reshape(-1))),
+                              mu, lam, proj, 1, O.ptr(e), O.ptr(r), O.ptr(K))
+            out["stress_work"].append({"X": X.reshape(-1).tolist(), "u": u.reshape(-1).tolist(), "mu": mu,
+                                       "lambda": lam, "project": proj, "energy": float(e[0]),
+                                       "res": r.tolist(), "K": K.tolist()})
+    # krylov::PCG on the golden systems (residual-L2 stop test, Jacobi, Polak-Ribiere)
+    kr = parse_krylov(os.path.join(args_ns.mc, "test/data/krylov_solver_test_data.h"))
+    A100 = np.zeros((100, 100))
+    for r_, c_, v_ in zip(kr["rows"], kr["cols"], kr["vals"]):
+        A100[r_, c_] = v_
+    systems = {"psd100": (A100, np.array(kr["rhs"])), "tridiag64": tridiag64()}
+    for name, (A, b) in systems.items():
+        n = A.shape[0]
+        rp = np.zeros(n + 1, np.int64)
+        cols, vals = [], []
+        for i in range(n):
+            nz = np.nonzero(A[i])[0]
+            cols += nz.tolist()
+            vals += A[i, nz].tolist()
+            rp[i + 1] = len(cols)
+        cols = np.asarray(cols, np.int32)
+        vals = np.asarray(vals)
+        for rel in (1e-6, 1e-10):
+            for jac in (0, 1):
+                x = np.zeros(n)
+                rn, rr = np.zeros(1), np.zeros(1)
+                cv = C.c_int()
+                it = R.ref_pcg_csr(n, O.ptr(rp, O._lp), O.ptr(cols, O._ip), O.ptr(vals), O.ptr(b), O.ptr(x),
+                                   rel, 1e-30, 1e10, 10000, jac, 1, 1, O.ptr(rn), O.ptr(rr), C.byref(cv))
+                out["pcg"].append({"system": name, "rel_tol": rel, "jacobi": jac, "iters": int(it),
+                                   "convergence": int(cv.value), "res_norm": float(rn[0]),
+                                   "rel_res_norm": float(rr[0]), "x": x.tolist()})
+    out["source"] = "oracle/_ref/libsdx_ref.so (reference sources, FP64 build)"
+    return out
+
+
+def main():
+    global args_ns
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference-root", default="/root/reference")
+    args_ns = ap.parse_args()
+    args_ns.mc = os.path.join(args_ns.reference_root, "superdex_physics/libraries/mochi/mochi_core")
+    with open(os.path.join(HERE, "smith_nh_reference.json"), "w") as f:
+        json.dump(parse_smith(os.path.join(args_ns.mc, "test/data/material_test_data.h")), f)
+    with open(os.path.join(HERE, "krylov_psd100.json"), "w") as f:
+        json.dump(parse_krylov(os.path.join(args_ns.mc, "test/data/krylov_solver_test_data.h")), f)
+    with open(os.path.join(HERE, "reference_vectors.json"), "w") as f:
+        json.dump(reference_vectors(), f)
+    print("wrote fixtures to", HERE)
+
+
+if __name__ == "__main__":
+    main()

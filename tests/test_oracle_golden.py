@@ -1,0 +1,113 @@
+"""Pins the CPU oracle (oracle/sdx_oracle.c) to the reference: its golden vectors (read as text from the
+reference test data) and outputs of the reference's own compiled code (tests/golden/reference_vectors.json)."""
+import numpy as np
+import pytest
+
+from conftest import dense_from_coo, scalar_to_block
+
+
+def test_smith_nh_known_answers(oracle, golden):
+    """material_test_data.h smith_neo_hookean_test_data (E = 1, nu = 0.4), as batched_materials_test.cpp:413."""
+    g = golden("smith_nh_reference.json")
+    lam, mu = 1.0 * 0.4 / ((1 + 0.4) * (1 - 0.8)), 1.0 / (2 * 1.4)
+    assert len(g["cases"]) == 5
+    for c in g["cases"]:
+        e, P, C = oracle.smith_nh(mu, lam, np.array(c["F"]), project=False, psd=0)
+        # golden data carries 7 significant digits
+        assert e == pytest.approx(c["energy"], rel=2e-5, abs=1e-6)
+        np.testing.assert_allclose(P.reshape(-1), c["pk1"], rtol=2e-5, atol=2e-6)
+        np.testing.assert_allclose(C.reshape(-1), c["tangent"], rtol=2e-5, atol=2e-6)
+
+
+def test_smith_nh_all_psd_strategies_match_reference_code(oracle, golden):
+    v = golden("reference_vectors.json")
+    assert len(v["smith"]) == 192
+    for c in v["smith"]:
+        e, P, C = oracle.smith_nh(c["mu"], c["lambda"], np.array(c["F"]), project=c["psd"] != 0, psd=c["psd"])
+        scale = max(1.0, np.abs(c["tangent"]).max())
+        assert e == pytest.approx(c["energy"], rel=1e-11, abs=1e-11)
+        np.testing.assert_allclose(P.reshape(-1), c["pk1"], rtol=1e-11, atol=1e-11)
+        np.testing.assert_allclose(C.reshape(-1), c["tangent"], rtol=1e-9, atol=1e-10 * scale)
+
+
+def test_projected_tangent_is_psd(oracle, golden):
+    v = golden("reference_vectors.json")
+    for c in v["smith"]:
+        if c["psd"] in (1, 2):
+            _, _, C = oracle.smith_nh(c["mu"], c["lambda"], np.array(c["F"]), project=True, psd=c["psd"])
+            assert np.linalg.eigvalsh(0.5 * (C + C.T)).min() > -1e-9 * np.abs(C).max()
+
+
+def test_polyrelu_matches_reference(oracle, golden):
+    for c in golden("reference_vectors.json")["polyrelu"]:
+        f, df, ddf = oracle.polyrelu(c["x"], c["t"], c["shift"])
+        assert (f, df, ddf) == pytest.approx((c["f"], c["df"], c["ddf"]), rel=1e-14, abs=1e-16)
+
+
+def test_penalty_matches_reference(oracle, golden):
+    for c in golden("reference_vectors.json")["penalty"]:
+        e, f, df = oracle.penalty(c["d"], np.array(c["grad"]), c["k"], c["t_half"], c["thr"])
+        assert e == pytest.approx(c["energy"], rel=1e-12, abs=1e-300)
+        np.testing.assert_allclose(f, c["force"], rtol=1e-12, atol=1e-300)
+        d6 = [df[0, 0], df[1, 1], df[2, 2], df[0, 1], df[0, 2], df[1, 2]]
+        np.testing.assert_allclose(d6, c["dforce6"], rtol=1e-12, atol=1e-300)
+
+
+def test_stress_work_matches_reference(oracle, golden):
+    """Single-tet StressWork (fem_stress.h:107) through the oracle's assembly (no inertia/gravity)."""
+    from project_superdex_b200 import scenes
+    for c in golden("reference_vectors.json")["stress_work"]:
+        X = np.array(c["X"]).reshape(4, 3)
+        b = scenes.Body(X=X, tets=np.array([[0, 1, 2, 3]], np.int32), E=np.array([1.0]), nu=np.array([0.3]),
+                        rho=np.array([0.0]), pin=np.zeros(4, np.uint8), colliders=[])
+        s = oracle.Scene(b, scenes.SceneConfig(gravity=(0, 0, 0)))
+        s.mu[:] = c["mu"]
+        s.lam[:] = c["lambda"]
+        u = np.array(c["u"])
+        out = s.assemble(u, u, psd=bool(c["project"]))
+        K = oracle.bsr_to_dense(s.row_ptr, s.col, out["H"])
+        assert out["obj"] == pytest.approx(c["energy"], rel=1e-11)
+        np.testing.assert_allclose(out["g"], c["res"], rtol=1e-10, atol=1e-12 * np.abs(c["res"]).max())
+        np.testing.assert_allclose(K.reshape(-1), c["K"], rtol=1e-9, atol=1e-11 * np.abs(c["K"]).max())
+
+
+@pytest.mark.parametrize("system", ["psd100", "tridiag64"])
+def test_pcg_iteration_counts_match_reference(oracle, golden, system):
+    """krylov::PCG (pcg.h:70) on the reference's golden systems: identical iteration counts."""
+    kr = golden("krylov_psd100.json")
+    if system == "psd100":
+        A = dense_from_coo(100, kr["rows"], kr["cols"], kr["vals"])
+        b = np.array(kr["rhs"])
+        x_true = np.array(kr["solution"])
+    else:
+        A = np.diag(np.full(64, 2.0)) - np.diag(np.ones(63), 1) - np.diag(np.ones(63), -1)
+        b = np.ones(64)
+        x_true = np.array([(i + 1) * (64 - i) / 2.0 for i in range(64)])
+    n = A.shape[0]
+    rp, col, vals, bp = scalar_to_block(A, b)
+    for ref in [p for p in golden("reference_vectors.json")["pcg"] if p["system"] == system]:
+        # the oracle's Jacobi on the block embedding equals the reference's scalar Jacobi
+        x, st = oracle.pcg(rp, col, vals, bp, rel_tol=ref["rel_tol"], abs_tol=1e-30,
+                           precond=1 if ref["jacobi"] else 0)
+        assert st.num_iter == ref["iters"]
+        assert st.convergence == ref["convergence"]
+        np.testing.assert_allclose(x[:n], ref["x"], rtol=1e-9, atol=1e-9 * np.abs(ref["x"]).max())
+        if ref["rel_tol"] == 1e-10:
+            # golden solution of the test data (krylov_solver_test_data.h kPsdMatrixOut) within the
+            # reference test's own bound eps_f32 * n * cond (krylov_solver_test_helpers.h:34-38)
+            cond = 2.4104e05 if system == "psd100" else 1712.0
+            err = np.linalg.norm(x[:n] - x_true) / np.linalg.norm(x_true)
+            assert err < np.finfo(np.float32).eps * n * cond
+
+
+def test_pcg_stop_and_divergence_statuses(oracle):
+    A = np.diag(np.arange(1.0, 10.0))
+    rp, col, vals, bp = scalar_to_block(A, np.ones(9))
+    x, st = oracle.pcg(rp, col, vals, bp, rel_tol=1e-12, max_iter=2, precond=0)
+    assert st.convergence == 2 and st.num_iter == 2  # Stopped at maxIter
+    x, st = oracle.pcg(rp, col, vals, bp, rel_tol=1e-12, precond=1)
+    assert st.convergence == 1 and st.num_iter == 1  # Jacobi solves a diagonal system at once
+    Z = np.zeros((9, 9))
+    rp, col, vals, bp = scalar_to_block(Z + np.eye(9), np.zeros(9))
+    x, st = oracle.pcg(rp, col, vals, bp)
+    assert st.convergence == 1 and st.num_iter == 0  # b = 0: converged at iteration 0
