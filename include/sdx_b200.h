@@ -146,6 +146,24 @@ int sdx_pcg_solve_ctx(sdx_context* ctx, int block_rows, int64_t nnzb, const int6
                       double* x, int hint, const sdx_linear_params* params,
                       sdx_linear_status* status);
 
+/* No counterpart in the reference. A Jacobi-PCG solve for callers that cannot allocate GPU memory
+ * when they need the solve — an engine whose pool allocator owns all device memory and forbids
+ * cudaMalloc/cudaFree inside its step callbacks, or a real-time loop that must not take allocator
+ * locks. Same algorithm, parameters and status as sdx_pcg_solve, but every pointer is a DEVICE pointer
+ * owned by the caller (BSR with FP32 row-major 3x3 blocks, FP64 b and x) and nothing is allocated:
+ * the work vectors live in one fixed array inside the library, held by every GPU that loads it until
+ * the process exits. Limits: at most SDX_NOALLOC_MAX_BLOCK_ROWS block rows (larger systems return
+ * SDX_ERR_INVALID_ARGUMENT). All calls on a device share that array: calls whose GPU work overlaps
+ * (unordered streams or threads) race and must be serialized by the caller. The first call on a device
+ * performs a one-time set-up (it looks up the array's device address); make it before any stream
+ * capture. `stream` is a cudaStream_t (NULL: legacy default stream); the call returns after the solve
+ * has finished on that stream. */
+#define SDX_NOALLOC_MAX_BLOCK_ROWS 65536
+int sdx_pcg_solve_device_noalloc(int block_rows, int64_t nnzb, const int64_t* row_ptr, const int32_t* col,
+                                 const float* values, const double* b, double* x, int hint,
+                                 const sdx_linear_params* params, sdx_linear_status* status,
+                                 void* stream);
+
 /* ---- context / FEM bodies ----------------------------------------------------------------------- */
 
 sdx_context* sdx_create(int device);

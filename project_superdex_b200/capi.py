@@ -28,8 +28,9 @@ EXPORTED = [
     "sdx_set_colliders", "sdx_set_params", "sdx_set_state", "sdx_get_state", "sdx_get_sizes",
     "sdx_get_pattern", "sdx_get_faces", "sdx_assemble", "sdx_get_contact_pairs", "sdx_step",
     "sdx_get_stats", "sdx_bench_spmv", "sdx_kernel_launches", "sdx_get_stream",
-    "sdx_set_profiling", "sdx_get_profile",
+    "sdx_set_profiling", "sdx_get_profile", "sdx_pcg_solve_device_noalloc",
 ]
+SDX_NOALLOC_MAX_BLOCK_ROWS = 65536
 
 
 class LinearParams(C.Structure):
@@ -122,6 +123,8 @@ def lib():
     L.sdx_get_stream.argtypes = [_vp, C.POINTER(C.c_void_p)]
     L.sdx_set_profiling.argtypes = [_vp, C.c_int]
     L.sdx_get_profile.argtypes = [_vp, C.POINTER(Profile)]
+    L.sdx_pcg_solve_device_noalloc.argtypes = [C.c_int, C.c_int64, _vp, _vp, _vp, _vp, _vp, C.c_int,
+                                               C.POINTER(LinearParams), C.POINTER(LinearStatus), _vp]
     _lib = L
     return L
 

@@ -34,6 +34,14 @@ static int set_error(int code, const char* fmt, ...) {
   return code;
 }
 
+namespace sdx {
+// error text for entry points defined in other translation units (read back by sdx_last_error)
+int record_error(int code, const char* msg, const char* detail) {
+  g_last_error = detail ? std::string(msg) + ": " + detail : std::string(msg);
+  return code;
+}
+}  // namespace sdx
+
 #define SDX_CUDA(call)                                                                       \
   do {                                                                                       \
     cudaError_t _e = (call);                                                                 \
