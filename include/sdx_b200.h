@@ -212,6 +212,28 @@ int sdx_get_contact_pairs(sdx_context* ctx, int64_t* pairs, int64_t pairs_cap, i
 int sdx_step(sdx_context* ctx, int n_steps);
 int sdx_get_stats(sdx_context* ctx, sdx_env_stats* per_env);
 
+/* ---- learned CG warm start (no counterpart in the reference) -------------------------------------
+ * A per-vertex MLP (15 -> 128 -> 128 -> 128 -> 3, GELU; BF16 weights / activations, FP32 accumulate;
+ * forward on the tensor cores) maps 1-ring-averaged displacement, dt * velocity, the last two Newton
+ * updates and the Jacobi-preconditioned Newton gradient (all divided by the env's RMS of the latter)
+ * to the Newton update in the same units. With warm_start = SDX_WARM_LEARNED its prediction is the
+ * initial guess of every Newton linear solve; the converged residual still decides the solution. */
+#define SDX_MLP_PARAMS 37264
+int sdx_mlp_init(sdx_context* ctx, uint64_t seed);
+int sdx_mlp_set_params(sdx_context* ctx, const float* params, int n);
+int sdx_mlp_get_params(sdx_context* ctx, float* params, int n);
+/* Y (n x 3) = MLP(X (n x 16, column 15 ignored)); host arrays. */
+int sdx_mlp_forward(sdx_context* ctx, const float* X, int n, float* Y);
+/* Gradient of the mean-squared error against targets T (n x 3) w.r.t. all parameters, and the loss. */
+int sdx_mlp_gradients(sdx_context* ctx, const float* X, const float* T, int n, float* grad, double* loss);
+/* Adam (lr) over `epochs` shuffled passes of minibatches of `batch` samples; epoch_loss[epochs]. */
+int sdx_mlp_train(sdx_context* ctx, const float* X, const float* T, int64_t n, int batch, int epochs, float lr,
+                  uint64_t seed, double* epoch_loss);
+/* While stepping, record (features, normalized solution) of samples_per_solve random nodes of every
+ * Newton linear solve, up to `capacity` samples (0 disables). */
+int sdx_collect_training(sdx_context* ctx, int samples_per_solve, int64_t capacity, uint64_t seed);
+int sdx_get_training_data(sdx_context* ctx, float* X, float* T, int64_t cap, int64_t* n);
+
 /* Kernel-level entry points used by the benchmark: y = A x on the context's last assembled matrix
  * (device resident, FP32), repeated `reps` times; returns the average time per SpMV in ms. */
 int sdx_bench_spmv(sdx_context* ctx, int reps, double* ms_per_spmv, double* bytes_per_spmv);

@@ -28,8 +28,11 @@ EXPORTED = [
     "sdx_set_colliders", "sdx_set_params", "sdx_set_state", "sdx_get_state", "sdx_get_sizes",
     "sdx_get_pattern", "sdx_get_faces", "sdx_assemble", "sdx_get_contact_pairs", "sdx_step",
     "sdx_get_stats", "sdx_bench_spmv", "sdx_kernel_launches", "sdx_get_stream",
-    "sdx_set_profiling", "sdx_get_profile", "sdx_pcg_solve_device_noalloc",
+    "sdx_set_profiling", "sdx_get_profile", "sdx_pcg_solve_device_noalloc", "sdx_mlp_init",
+    "sdx_mlp_set_params", "sdx_mlp_get_params", "sdx_mlp_forward", "sdx_mlp_gradients", "sdx_mlp_train",
+    "sdx_collect_training", "sdx_get_training_data",
 ]
+SDX_MLP_PARAMS = 37264
 SDX_NOALLOC_MAX_BLOCK_ROWS = 65536
 
 
@@ -123,6 +126,15 @@ def lib():
     L.sdx_get_stream.argtypes = [_vp, C.POINTER(C.c_void_p)]
     L.sdx_set_profiling.argtypes = [_vp, C.c_int]
     L.sdx_get_profile.argtypes = [_vp, C.POINTER(Profile)]
+    _fp_ = C.POINTER(C.c_float)
+    L.sdx_mlp_init.argtypes = [_vp, C.c_uint64]
+    L.sdx_mlp_set_params.argtypes = [_vp, _fp_, C.c_int]
+    L.sdx_mlp_get_params.argtypes = [_vp, _fp_, C.c_int]
+    L.sdx_mlp_forward.argtypes = [_vp, _fp_, C.c_int, _fp_]
+    L.sdx_mlp_gradients.argtypes = [_vp, _fp_, _fp_, C.c_int, _fp_, _dp]
+    L.sdx_mlp_train.argtypes = [_vp, _fp_, _fp_, C.c_int64, C.c_int, C.c_int, C.c_float, C.c_uint64, _dp]
+    L.sdx_collect_training.argtypes = [_vp, C.c_int, C.c_int64, C.c_uint64]
+    L.sdx_get_training_data.argtypes = [_vp, _fp_, _fp_, C.c_int64, _lp]
     L.sdx_pcg_solve_device_noalloc.argtypes = [C.c_int, C.c_int64, _vp, _vp, _vp, _vp, _vp, C.c_int,
                                                C.POINTER(LinearParams), C.POINTER(LinearStatus), _vp]
     _lib = L

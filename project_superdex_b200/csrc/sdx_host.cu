@@ -16,6 +16,8 @@
 
 #include "../../include/sdx_b200.h"
 #include "sdx_internal.cuh"
+#include "sdx_mlp.cuh"
+#include <random>
 
 using namespace sdx;
 
@@ -202,6 +204,20 @@ struct sdx_context {
   double *solo_b = nullptr, *solo_x = nullptr;
   PcgPartition solo_part;
   PcgWork solo_work;
+  // learned warm start (per-vertex MLP)
+  MlpParams mlp;
+  MlpWork mlpw;
+  int* mlp_error = nullptr;
+  double* mlp_loss = nullptr;
+  float *feat_raw = nullptr, *feat_X = nullptr, *feat_Y = nullptr;
+  double *feat_sumsq = nullptr, *dx_prev1 = nullptr, *dx_prev2 = nullptr;
+  int* env_rows = nullptr;
+  // training-data capture from the plain solver
+  int collect_per_solve = 0;
+  int64_t ds_cap = 0, ds_n = 0;
+  float *ds_X = nullptr, *ds_T = nullptr;
+  int* ds_idx = nullptr;
+  std::mt19937_64 ds_rng{0};
   // opt-in per-kernel timing: event pairs resolved lazily
   bool profiling = false;
   sdx_profile prof;
@@ -310,7 +326,37 @@ static void release_topology(sdx_context* c) {
   dfree(c->pair_mask);
   c->part.release();
   c->work.release();
+  dfree(c->feat_raw);
+  dfree(c->feat_X);
+  dfree(c->feat_Y);
+  dfree(c->feat_sumsq);
+  dfree(c->dx_prev1);
+  dfree(c->dx_prev2);
+  dfree(c->env_rows);
+  dfree(c->ds_X);
+  dfree(c->ds_T);
+  dfree(c->ds_idx);
+  c->ds_cap = c->ds_n = 0;
+  c->collect_per_solve = 0;
   c->uploaded = false;
+}
+
+static void release_mlp_work(MlpWork& W) {
+  for (float** p : {&W.Y, &W.Z, &W.H1, &W.H2, &W.H3, &W.G1, &W.G2, &W.G3, &W.dY, &W.dA, &W.dB, &W.Xb}) dfree(*p);
+  W.cap = 0;
+}
+
+static void release_mlp(sdx_context* c) {
+  dfree(c->mlp.p);
+  dfree(c->mlp.g);
+  dfree(c->mlp.m);
+  dfree(c->mlp.v);
+  dfree(c->mlp.pr);
+  dfree(c->mlp.pb);
+  dfree(c->mlp.mask);
+  release_mlp_work(c->mlpw);
+  dfree(c->mlp_error);
+  dfree(c->mlp_loss);
 }
 
 static void release_solo(sdx_context* c) {
@@ -349,6 +395,20 @@ __global__ void k_gather_rows(int64_t n_nodes, const int* __restrict__ row_of_no
   dst[3 * i] = src[3 * r];
   dst[3 * i + 1] = src[3 * r + 1];
   dst[3 * i + 2] = src[3 * r + 2];
+}
+
+__global__ void k_gather_float_rows(const int* __restrict__ idx, int n, const float* __restrict__ src, int width,
+                                    float* dst) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)n * width) return;
+  const int r = (int)(i / width), k = (int)(i % width);
+  dst[i] = src[(int64_t)idx[r] * width + k];
+}
+
+static void launch_gather_rows(const int* idx, int n, const float* src, int width, float* dst, cudaStream_t st) {
+  if (n <= 0) return;
+  const int64_t t = (int64_t)n * width;
+  k_gather_float_rows<<<(unsigned)((t + 255) / 256), 256, 0, st>>>(idx, n, src, width, dst);
 }
 
 static int h2d_rows(sdx_context* c, const double* host, double* dev_rows) {
@@ -549,7 +609,8 @@ static int alloc_work(PcgWork& W, int64_t n_rows, int n_envs) {
 // Runs the persistent PCG on matrix A for the envs in env_mask (NULL = all), b -> x.
 static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_envs, PcgPartition& P,
                    PcgWork& W, const double* b, double* x, const uint8_t* env_mask, int n_active,
-                   const sdx_linear_params& lp, bool zero_guess, const double* env_rel_tol) {
+                   const sdx_linear_params& lp, bool zero_guess, const double* env_rel_tol,
+                   bool scale_guess = false) {
   PcgArgs a;
   memset(&a, 0, sizeof(a));
   a.A = A;
@@ -579,6 +640,7 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
   a.polak_ribiere = lp.polak_ribiere;
   a.replace_every = lp.replace_every > 0 ? lp.replace_every : 32;
   a.zero_guess = zero_guess ? 1 : 0;
+  a.scale_guess = scale_guess ? 1 : 0;
   a.abort_spd = lp.abort_if_not_spd;
   a.out_iters = W.out_iters;
   a.out_res = W.out_res;
@@ -682,6 +744,7 @@ extern "C" int sdx_destroy(sdx_context* c) {
   cudaStreamSynchronize(c->stream);
   release_topology(c);
   release_solo(c);
+  release_mlp(c);
   prof_resolve(c);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   cudaStreamDestroy(c->stream);
@@ -975,6 +1038,20 @@ extern "C" int sdx_upload_bodies(sdx_context* c, int n_envs, const int64_t* node
     SDX_CUDA(cudaMemset(*pv, 0, sizeof(double) * n3));
   }
   SDX_TRY(dalloc(&c->staging, (size_t)3 * N));
+  // learned warm start buffers (features, predictions, Newton-update history)
+  SDX_TRY(dalloc(&c->feat_raw, (size_t)16 * c->n_rows));
+  SDX_TRY(dalloc(&c->feat_X, (size_t)16 * c->n_rows));
+  SDX_TRY(dalloc(&c->feat_Y, (size_t)3 * c->n_rows));
+  SDX_TRY(dalloc(&c->feat_sumsq, (size_t)5 * n_envs));
+  for (double** pv : {&c->dx_prev1, &c->dx_prev2}) {
+    SDX_TRY(dalloc(pv, n3));
+    SDX_CUDA(cudaMemset(*pv, 0, sizeof(double) * n3));
+  }
+  {
+    std::vector<int> er(n_envs);
+    for (int e = 0; e < n_envs; ++e) er[e] = (int)(node_off[e + 1] - node_off[e]);
+    SDX_TRY(upload(&c->env_rows, er));
+  }
   SDX_TRY(dalloc(&c->env_norm, n_envs));
   SDX_TRY(dalloc(&c->env_scale, n_envs));
   SDX_TRY(dalloc(&c->env_obj, n_envs));
@@ -1257,6 +1334,40 @@ static int upload_mask(sdx_context* c, const std::vector<uint8_t>& m) {
   return SDX_OK;
 }
 
+static int mlp_check_error(sdx_context* c);
+static void launch_gather_rows(const int* idx, int n, const float* src, int width, float* dst, cudaStream_t st);
+
+// Appends samples (features before the solve, solution / env scale) of random nodes of the active envs.
+static int capture_samples(sdx_context* c, const std::vector<uint8_t>& mask) {
+  launch_targets(c->n_rows, c->slice_env, c->dx, c->env_norm, c->env_rows, c->feat_Y, c->stream);
+  c->launches++;
+  std::vector<int64_t> pref(1, 0);
+  std::vector<int> envs;
+  for (int e = 0; e < c->n_envs; ++e)
+    if (mask[e]) {
+      envs.push_back(e);
+      pref.push_back(pref.back() + (c->h_node_off[e + 1] - c->h_node_off[e]));
+    }
+  const int64_t total = pref.back();
+  const int k = (int)std::min<int64_t>(c->collect_per_solve, c->ds_cap - c->ds_n);
+  if (total == 0 || k <= 0) return SDX_OK;
+  std::vector<int> idx(k);
+  std::uniform_int_distribution<int64_t> U(0, total - 1);
+  for (int i = 0; i < k; ++i) {
+    const int64_t q = U(c->ds_rng);
+    const int j = (int)(std::upper_bound(pref.begin(), pref.end(), q) - pref.begin()) - 1;
+    const int e = envs[j];
+    idx[i] = c->h_row_of_node[c->h_node_off[e] + (q - pref[j])];
+  }
+  SDX_CUDA(cudaMemcpyAsync(c->ds_idx, idx.data(), sizeof(int) * k, cudaMemcpyHostToDevice, c->stream));
+  launch_gather_rows(c->ds_idx, k, c->feat_X, 16, c->ds_X + (size_t)c->ds_n * 16, c->stream);
+  launch_gather_rows(c->ds_idx, k, c->feat_Y, 3, c->ds_T + (size_t)c->ds_n * 3, c->stream);
+  c->launches += 2;
+  SDX_CUDA(cudaStreamSynchronize(c->stream));
+  c->ds_n += k;
+  return SDX_OK;
+}
+
 static int step_once(sdx_context* c) {
   const sdx_step_params& p = c->params;
   const int E = c->n_envs;
@@ -1318,16 +1429,42 @@ static int step_once(sdx_context* c) {
     if (n_active == 0) break;
     SDX_TRY(upload_mask(c, mask));
     if (!first_pass) assemble_dev(c, c->u, c->ut, t_end, SDX_ASM_HESS | SDX_ASM_PSD, c->env_mask, false);
-    // linear solve H dx = g
+    // linear solve H dx = g, warm started from zero, the previous dx, or the learned prediction
+    const bool learned = p.warm_start == SDX_WARM_LEARNED;
+    const bool collect = c->collect_per_solve > 0 && c->ds_n < c->ds_cap;
+    if (learned && !c->mlp.p) return set_error(SDX_ERR_NOT_READY, "learned warm start needs MLP parameters");
+    if (learned || collect) {
+      launch_features(ctx_matrix(c), c->n_rows, c->env_mask, c->u, c->v, p.dt, c->dx_prev1, c->dx_prev2, c->g,
+                      c->diag_pos, c->pin, c->env_rows, c->feat_raw, c->feat_sumsq, E, c->feat_X, c->stream);
+      c->launches += 3;
+    }
+    if (learned) {
+      if (launch_mlp_forward(mlp_forward_args(c->mlp, c->feat_X, (int)c->n_rows, c->feat_Y, nullptr, c->mlp_error),
+                             c->num_sms, c->stream) != 0)
+        return set_error(SDX_ERR_CUDA, "MLP forward launch failed");
+      launch_warm_start(c->n_rows, c->slice_env, c->env_mask, c->feat_Y, c->pin, c->diag_pos, c->dx, c->stream);
+      c->launches += 2;
+    }
     const bool zero = p.warm_start == SDX_WARM_ZERO;
     if (p.ew_forcing == 2)
       SDX_CUDA(cudaMemcpyAsync(c->work.env_rel_tol, eta.data(), sizeof(double) * E, cudaMemcpyHostToDevice, c->stream));
     SDX_TRY(run_pcg(c, ctx_matrix(c), c->diag_pos, E, c->part, c->work, c->g, c->dx, c->env_mask, n_active,
-                    p.linear, zero, p.ew_forcing == 2 ? c->work.env_rel_tol : nullptr));
+                    p.linear, zero, p.ew_forcing == 2 ? c->work.env_rel_tol : nullptr, /*scale_guess*/ !zero));
     std::vector<int> it_out(E);
     SDX_CUDA(cudaMemcpy(it_out.data(), c->work.out_iters, sizeof(int) * E, cudaMemcpyDeviceToHost));
     for (int e = 0; e < E; ++e)
       if (mask[e]) cg[e] += it_out[e];
+    if (learned) SDX_TRY(mlp_check_error(c));
+    if (collect) {
+      SDX_CUDA(cudaMemsetAsync(c->env_norm, 0, sizeof(double) * E, c->stream));
+      launch_env_dot(c->n_slices, c->slice_env, c->env_mask, c->dx, c->dx, c->env_norm, c->stream);
+      c->launches++;
+      SDX_TRY(capture_samples(c, mask));
+    }
+    // Newton-update history for the learned features
+    launch_copy_rows(c->n_slices, c->slice_env, c->env_mask, c->dx_prev1, c->dx_prev2, c->stream);
+    launch_copy_rows(c->n_slices, c->slice_env, c->env_mask, c->dx, c->dx_prev1, c->stream);
+    c->launches += 2;
     SDX_TRY(env_dot_host(c, c->dx, c->dx, c->env_mask, nrm));
     for (int e = 0; e < E; ++e)
       if (mask[e]) dxn[e] = std::sqrt(nrm[e]);
@@ -1555,4 +1692,223 @@ extern "C" int sdx_pcg_solve(int n, int64_t nnzb, const int64_t* row_ptr, const 
   sdx_destroy(c);
   g_last_error = err;
   return rc;
+}
+
+// ------------------------------------------------------------------------------------------------
+// learned warm start: MLP parameters, training and data capture
+
+static int mlp_ensure(sdx_context* c) {
+  if (c->mlp.p) return SDX_OK;
+  SDX_TRY(dalloc(&c->mlp.p, kMlpParams));
+  SDX_TRY(dalloc(&c->mlp.g, kMlpParams));
+  SDX_TRY(dalloc(&c->mlp.m, kMlpParams));
+  SDX_TRY(dalloc(&c->mlp.v, kMlpParams));
+  SDX_TRY(dalloc(&c->mlp.pr, kMlpParams));
+  SDX_TRY(dalloc(&c->mlp.pb, kMlpParams));
+  SDX_TRY(dalloc(&c->mlp.mask, kMlpParams));
+  SDX_TRY(dalloc(&c->mlp_error, 1));
+  SDX_TRY(dalloc(&c->mlp_loss, 1));
+  SDX_CUDA(cudaMemset(c->mlp.p, 0, sizeof(float) * kMlpParams));
+  SDX_CUDA(cudaMemset(c->mlp.m, 0, sizeof(float) * kMlpParams));
+  SDX_CUDA(cudaMemset(c->mlp.v, 0, sizeof(float) * kMlpParams));
+  SDX_CUDA(cudaMemset(c->mlp_error, 0, sizeof(int)));
+  // trainable entries: everything except the zero pad input (W1 column 15) and unused outputs (rows 3..15)
+  std::vector<uint8_t> mask(kMlpParams, 1);
+  for (int o = 0; o < 128; ++o) mask[kOffW1 + o * 16 + 15] = 0;
+  for (int o = 3; o < 16; ++o) {
+    for (int i = 0; i < 128; ++i) mask[kOffW4 + o * 128 + i] = 0;
+    mask[kOffB4 + o] = 0;
+  }
+  SDX_CUDA(cudaMemcpy(c->mlp.mask, mask.data(), kMlpParams, cudaMemcpyHostToDevice));
+  c->mlp.step = 0;
+  return SDX_OK;
+}
+
+static int mlp_work_ensure(sdx_context* c, int n) {
+  MlpWork& W = c->mlpw;
+  if (W.cap >= n) return SDX_OK;
+  release_mlp_work(W);
+  const size_t nh = (size_t)n * 128;
+  SDX_TRY(dalloc(&W.Y, (size_t)n * 3));
+  SDX_TRY(dalloc(&W.Z, 3 * nh));
+  for (float** p : {&W.H1, &W.H2, &W.H3, &W.G1, &W.G2, &W.G3, &W.dA, &W.dB}) SDX_TRY(dalloc(p, nh));
+  SDX_TRY(dalloc(&W.dY, (size_t)n * 3));
+  SDX_TRY(dalloc(&W.Xb, (size_t)n * 16));
+  W.cap = n;
+  return SDX_OK;
+}
+
+static int mlp_check_error(sdx_context* c) {
+  int err = 0;
+  SDX_CUDA(cudaMemcpyAsync(&err, c->mlp_error, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  SDX_CUDA(cudaStreamSynchronize(c->stream));
+  if (err) return set_error(SDX_ERR_DEVICE_TIMEOUT, "MLP tensor-core wait timed out");
+  return SDX_OK;
+}
+
+extern "C" int sdx_mlp_set_params(sdx_context* c, const float* params, int n) {
+  if (!c || !params || n != kMlpParams) return set_error(SDX_ERR_INVALID_ARGUMENT, "expected %d parameters", kMlpParams);
+  cudaSetDevice(c->device);
+  SDX_TRY(mlp_ensure(c));
+  std::vector<float> h(params, params + n);
+  for (int o = 0; o < 128; ++o) h[kOffW1 + o * 16 + 15] = 0.0f;
+  for (int o = 3; o < 16; ++o) {
+    for (int i = 0; i < 128; ++i) h[kOffW4 + o * 128 + i] = 0.0f;
+    h[kOffB4 + o] = 0.0f;
+  }
+  SDX_CUDA(cudaMemcpy(c->mlp.p, h.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+  SDX_CUDA(cudaMemset(c->mlp.m, 0, sizeof(float) * kMlpParams));
+  SDX_CUDA(cudaMemset(c->mlp.v, 0, sizeof(float) * kMlpParams));
+  c->mlp.step = 0;
+  mlp_sync_bf16(c->mlp, c->stream);
+  c->launches++;
+  SDX_CUDA(cudaStreamSynchronize(c->stream));
+  return SDX_OK;
+}
+
+extern "C" int sdx_mlp_get_params(sdx_context* c, float* params, int n) {
+  if (!c || !params || n != kMlpParams) return set_error(SDX_ERR_INVALID_ARGUMENT, "expected %d parameters", kMlpParams);
+  if (!c->mlp.p) return set_error(SDX_ERR_NOT_READY, "MLP parameters not set");
+  SDX_CUDA(cudaMemcpy(params, c->mlp.p, sizeof(float) * n, cudaMemcpyDeviceToHost));
+  return SDX_OK;
+}
+
+extern "C" int sdx_mlp_init(sdx_context* c, uint64_t seed) {
+  if (!c) return set_error(SDX_ERR_INVALID_ARGUMENT, "null context");
+  // He-uniform hidden layers, small output layer
+  std::mt19937_64 rng(seed);
+  std::vector<float> h(kMlpParams, 0.0f);
+  auto fill = [&](int off, int rows, int cols, int fan_in, float gain) {
+    std::uniform_real_distribution<float> U(-1.0f, 1.0f);
+    const float a = gain * std::sqrt(3.0f / (float)fan_in);
+    for (int r = 0; r < rows; ++r)
+      for (int k = 0; k < cols; ++k) h[off + r * cols + k] = a * U(rng);
+  };
+  fill(kOffW1, 128, 16, 15, 1.41421356f);
+  fill(kOffW2, 128, 128, 128, 1.41421356f);
+  fill(kOffW3, 128, 128, 128, 1.41421356f);
+  fill(kOffW4, 3, 128, 128, 0.1f);
+  return sdx_mlp_set_params(c, h.data(), kMlpParams);
+}
+
+extern "C" int sdx_mlp_forward(sdx_context* c, const float* X, int n, float* Y) {
+  if (!c || !X || !Y || n <= 0) return set_error(SDX_ERR_INVALID_ARGUMENT, "bad arguments");
+  if (!c->mlp.p) return set_error(SDX_ERR_NOT_READY, "MLP parameters not set");
+  cudaSetDevice(c->device);
+  SDX_TRY(mlp_work_ensure(c, n));
+  float* dX = nullptr;
+  SDX_TRY(dalloc(&dX, (size_t)n * 16));
+  SDX_CUDA(cudaMemcpyAsync(dX, X, sizeof(float) * 16 * n, cudaMemcpyHostToDevice, c->stream));
+  int rc = launch_mlp_forward(mlp_forward_args(c->mlp, dX, n, c->mlpw.Y, nullptr, c->mlp_error), c->num_sms, c->stream);
+  c->launches++;
+  if (rc != 0) {
+    dfree(dX);
+    return set_error(SDX_ERR_CUDA, "MLP forward launch failed");
+  }
+  SDX_CUDA(cudaMemcpyAsync(Y, c->mlpw.Y, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, c->stream));
+  int r2 = mlp_check_error(c);
+  dfree(dX);
+  return r2;
+}
+
+extern "C" int sdx_mlp_gradients(sdx_context* c, const float* X, const float* T, int n, float* grad, double* loss) {
+  if (!c || !X || !T || n <= 0) return set_error(SDX_ERR_INVALID_ARGUMENT, "bad arguments");
+  if (!c->mlp.p) return set_error(SDX_ERR_NOT_READY, "MLP parameters not set");
+  cudaSetDevice(c->device);
+  SDX_TRY(mlp_work_ensure(c, n));
+  float *dX = nullptr, *dT = nullptr;
+  SDX_TRY(dalloc(&dX, (size_t)n * 16));
+  SDX_TRY(dalloc(&dT, (size_t)n * 3));
+  SDX_CUDA(cudaMemcpyAsync(dX, X, sizeof(float) * 16 * n, cudaMemcpyHostToDevice, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(dT, T, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+  int rc = mlp_gradients(c->mlp, c->mlpw, dX, dT, n, c->num_sms, c->mlp_loss, c->mlp_error, c->stream);
+  c->launches += 24;
+  if (rc == 0) {
+    if (grad) cudaMemcpyAsync(grad, c->mlp.g, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost, c->stream);
+    if (loss) cudaMemcpyAsync(loss, c->mlp_loss, sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  }
+  int r2 = mlp_check_error(c);
+  dfree(dX);
+  dfree(dT);
+  if (rc != 0) return set_error(SDX_ERR_CUDA, "MLP gradient launch failed");
+  return r2;
+}
+
+extern "C" int sdx_mlp_train(sdx_context* c, const float* X, const float* T, int64_t n, int batch, int epochs,
+                             float lr, uint64_t seed, double* epoch_loss) {
+  if (!c || !X || !T || n <= 0 || batch <= 0 || epochs <= 0)
+    return set_error(SDX_ERR_INVALID_ARGUMENT, "bad arguments");
+  if (!c->mlp.p) return set_error(SDX_ERR_NOT_READY, "MLP parameters not set");
+  cudaSetDevice(c->device);
+  if (batch > n) batch = (int)n;
+  SDX_TRY(mlp_work_ensure(c, batch));
+  float *dX = nullptr, *dT = nullptr, *bX = nullptr, *bT = nullptr;
+  SDX_TRY(dalloc(&dX, (size_t)n * 16));
+  SDX_TRY(dalloc(&dT, (size_t)n * 3));
+  SDX_TRY(dalloc(&bX, (size_t)batch * 16));
+  SDX_TRY(dalloc(&bT, (size_t)batch * 3));
+  SDX_CUDA(cudaMemcpyAsync(dX, X, sizeof(float) * 16 * n, cudaMemcpyHostToDevice, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(dT, T, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+  std::mt19937_64 rng(seed);
+  std::vector<int64_t> perm(n);
+  std::iota(perm.begin(), perm.end(), 0);
+  const int64_t steps_per_epoch = n / batch;
+  std::vector<int> bidx(batch);
+  int* didx = nullptr;
+  SDX_TRY(dalloc(&didx, batch));
+  int rc = 0;
+  for (int ep = 0; ep < epochs && rc == 0; ++ep) {
+    std::shuffle(perm.begin(), perm.end(), rng);
+    double acc = 0.0;
+    for (int64_t s = 0; s < steps_per_epoch && rc == 0; ++s) {
+      for (int i = 0; i < batch; ++i) bidx[i] = (int)perm[s * batch + i];
+      SDX_CUDA(cudaMemcpyAsync(didx, bidx.data(), sizeof(int) * batch, cudaMemcpyHostToDevice, c->stream));
+      launch_gather_rows(didx, batch, dX, 16, bX, c->stream);
+      launch_gather_rows(didx, batch, dT, 3, bT, c->stream);
+      rc = mlp_gradients(c->mlp, c->mlpw, bX, bT, batch, c->num_sms, c->mlp_loss, c->mlp_error, c->stream);
+      mlp_adam(c->mlp, lr, ++c->mlp.step, c->stream);
+      c->launches += 28;
+      double l = 0.0;
+      SDX_CUDA(cudaMemcpyAsync(&l, c->mlp_loss, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      SDX_CUDA(cudaStreamSynchronize(c->stream));
+      acc += l;
+    }
+    if (epoch_loss) epoch_loss[ep] = acc / std::max<int64_t>(1, steps_per_epoch);
+  }
+  int r2 = mlp_check_error(c);
+  dfree(dX);
+  dfree(dT);
+  dfree(bX);
+  dfree(bT);
+  dfree(didx);
+  if (rc != 0) return set_error(SDX_ERR_CUDA, "MLP training launch failed");
+  return r2;
+}
+
+extern "C" int sdx_collect_training(sdx_context* c, int samples_per_solve, int64_t capacity, uint64_t seed) {
+  if (!c || !c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
+  if (samples_per_solve < 0 || capacity < 0) return set_error(SDX_ERR_INVALID_ARGUMENT, "negative size");
+  cudaSetDevice(c->device);
+  dfree(c->ds_X);
+  dfree(c->ds_T);
+  dfree(c->ds_idx);
+  c->ds_n = 0;
+  c->ds_cap = capacity;
+  c->collect_per_solve = samples_per_solve;
+  c->ds_rng.seed(seed);
+  if (samples_per_solve > 0 && capacity > 0) {
+    SDX_TRY(dalloc(&c->ds_X, (size_t)capacity * 16));
+    SDX_TRY(dalloc(&c->ds_T, (size_t)capacity * 3));
+    SDX_TRY(dalloc(&c->ds_idx, samples_per_solve));
+  }
+  return SDX_OK;
+}
+
+extern "C" int sdx_get_training_data(sdx_context* c, float* X, float* T, int64_t cap, int64_t* n) {
+  if (!c) return set_error(SDX_ERR_INVALID_ARGUMENT, "null context");
+  const int64_t m = std::min(cap, c->ds_n);
+  if (m > 0 && X) SDX_CUDA(cudaMemcpy(X, c->ds_X, sizeof(float) * 16 * m, cudaMemcpyDeviceToHost));
+  if (m > 0 && T) SDX_CUDA(cudaMemcpy(T, c->ds_T, sizeof(float) * 3 * m, cudaMemcpyDeviceToHost));
+  if (n) *n = c->ds_n;
+  return SDX_OK;
 }

@@ -113,6 +113,7 @@ struct PcgArgs {
   int polak_ribiere;
   int replace_every;
   int zero_guess;
+  int scale_guess;  // non-zero guess: replace x0 by alpha x0, alpha = (x0.b)/(x0.A x0) (energy-optimal)
   int abort_spd;
   int* out_iters;
   double* out_res;

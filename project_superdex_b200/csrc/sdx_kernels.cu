@@ -722,6 +722,39 @@ __global__ void k_pcg(PcgArgs a) {
   __syncthreads();
 
   // ---- phase 0: r = b - A x0, z = M^-1 r, partials b.b, r.r, r.z ----
+  const bool scaled = !a.zero_guess && a.scale_guess;
+  if (scaled) {
+    // energy-optimal scaling of the guess: alpha = (x0.b) / (x0.A x0), A x0 = b - r0; the scaled start
+    // alpha x0 never has a larger A-norm error than the zero start
+    clear_acc();
+    for (int s = s0 + warp; s < s1; s += nwarps) {
+      const int le = a.A.slice_env[s] - e0;
+      if (st[le].status != 0) continue;
+      const int64_t row = (int64_t)s * kSlice + lane;
+      double r[3];
+      true_residual(a, s, lane, r);
+      double xb = 0.0, xr = 0.0, bb = 0.0;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        a.r[3 * row + k] = r[k];
+        const double xk = a.x[3 * row + k], bk = a.b[3 * row + k];
+        xb += xk * bk;
+        xr += xk * r[k];
+        bb += bk * bk;
+      }
+      add_acc(le, 0, bb);
+      add_acc(le, 1, xb);
+      add_acc(le, 2, xr);
+    }
+    flush_acc(3, 1);
+    if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
+    reduce_tot(3, 1);
+    for (int le = threadIdx.x; le < ne; le += blockDim.x) {
+      const double xb = tot[le][1], xax = tot[le][1] - tot[le][2];
+      st[le].alpha = (xax > 0.0 && xb > 0.0 && isfinite(xb / xax)) ? xb / xax : 0.0;
+    }
+    __syncthreads();
+  }
   clear_acc();
   for (int s = s0 + warp; s < s1; s += nwarps) {
     const int le = a.A.slice_env[s] - e0;
@@ -756,7 +789,15 @@ __global__ void k_pcg(PcgArgs a) {
         r[k] = a.b[3 * row + k];
       }
     }
-    if (!a.zero_guess) true_residual(a, s, lane, r);
+    if (!a.zero_guess && !scaled) true_residual(a, s, lane, r);
+    if (scaled) {
+      const double al = st[le].alpha;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        a.x[3 * row + k] *= al;
+        r[k] = (1.0 - al) * a.b[3 * row + k] + al * a.r[3 * row + k];
+      }
+    }
     float z[3];
     prec_apply(a, row, r, z);
 #pragma unroll

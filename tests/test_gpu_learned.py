@@ -1,0 +1,85 @@
+"""The learned CG warm start on the GPU: the tensor-core forward and the backward kernels against the
+CPU restatement (oracle/mlp_oracle.py), training reduces the loss, and a learned warm start changes only
+the iteration count, never the converged Newton state."""
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as MO
+from project_superdex_b200 import capi, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mlp():
+    from project_superdex_b200.learned import Mlp
+    ctx = capi.lib().sdx_create(0)
+    m = Mlp(ctx)
+    m.init(7)
+    yield m
+    capi.lib().sdx_destroy(ctx)
+
+
+@pytest.mark.parametrize("n", [1, 127, 128, 300, 5000])
+def test_tensor_core_forward_matches_restatement(mlp, n):
+    rng = np.random.default_rng(n)
+    X = rng.normal(size=(n, 16)).astype(np.float32)
+    X[:, 15] = 0.0
+    Y = mlp.forward(X)
+    Yo = MO.forward(mlp.get_params(), X)
+    # BF16 activations: a few BF16 ulps of the output scale
+    assert np.abs(Y - Yo).max() <= 2e-3 * max(1.0, np.abs(Yo).max())
+
+
+def test_gradients_match_restatement(mlp):
+    rng = np.random.default_rng(1)
+    X = rng.normal(size=(777, 16)).astype(np.float32)
+    X[:, 15] = 0.0
+    T = rng.normal(size=(777, 3)).astype(np.float32)
+    loss, g = mlp.gradients(X, T)
+    lo, go = MO.loss_and_grad(mlp.get_params(), X, T)
+    assert loss == pytest.approx(lo, rel=1e-4)
+    assert np.abs(g - go).max() <= 1e-3 * np.abs(go).max()
+    for name in ("W1", "W2", "W3", "W4", "b1", "b4"):
+        o, shape = MO.OFF[name]
+        sl = slice(o, o + int(np.prod(shape)))
+        assert np.linalg.norm(g[sl] - go[sl]) <= 1e-3 * max(np.linalg.norm(go[sl]), 1e-12)
+
+
+def test_training_reduces_loss(mlp):
+    rng = np.random.default_rng(2)
+    X = rng.normal(size=(20000, 16)).astype(np.float32)
+    X[:, 15] = 0.0
+    T = np.stack([np.tanh(X[:, 0] - X[:, 12]), X[:, 3] * 0.5, np.sin(X[:, 13])], axis=1).astype(np.float32)
+    losses = mlp.train(X, T, batch=2048, epochs=15, lr=1e-3)
+    assert losses[-1] < 0.2 * losses[0]
+
+
+def test_learned_warm_start_keeps_the_converged_state():
+    from project_superdex_b200.learned import Mlp, collect
+    from project_superdex_b200.soft_body import SoftBodyWorld
+    rng = np.random.default_rng(3)
+    b = scenes.grid_body(8, 8, 8, 0.1 / 8, rng=rng, nu=0.45)
+    b.E = np.exp(rng.uniform(np.log(1e4), np.log(1e6), size=b.n_tets))
+    b.colliders = scenes._fingertips(rng, (0, 0), (0.1, 0.1), 0.1)
+    cfg = scenes.SceneConfig(k_contact=1e4)
+    w = SoftBodyWorld([b], cfg, newton_abs_tol=1e-9)
+    X, T = collect(w, 12, 1000, 20000, seed=1)
+    assert X.shape[0] > 5000 and np.all(np.isfinite(X)) and np.all(np.isfinite(T))
+    m = Mlp(w._ctx)
+    m.init(5)
+    losses = m.train(X, T, batch=2048, epochs=10)
+    assert losses[-1] < losses[0]
+    params = m.get_params()
+    states = {}
+    for ws in (capi.SDX_WARM_ZERO, capi.SDX_WARM_LEARNED):
+        w2 = SoftBodyWorld([b], cfg, newton_abs_tol=1e-9)
+        if ws == capi.SDX_WARM_LEARNED:
+            Mlp(w2._ctx).set_params(params)
+        w2.set_params(warm_start=ws)
+        w2.step(4)
+        states[ws] = (w2.get_state()[0], w2.stats()[0])
+    u0, s0 = states[capi.SDX_WARM_ZERO]
+    u1, s1 = states[capi.SDX_WARM_LEARNED]
+    assert s1["convergence"] == s0["convergence"] == 1
+    assert np.abs(u1 - u0).max() <= 1e-5 * 0.1  # vertex error <= 1e-5 of the body size
