@@ -110,6 +110,11 @@ struct PcgPartition {
 
 struct PcgWork {
   int64_t n_rows = 0;
+  // one arena for the vectors every CG iteration touches (so one L2 access-policy window covers them)
+  char* arena = nullptr;
+  size_t arena_bytes = 0;
+  double* hot_b = nullptr;  // Newton gradient (the CG right-hand side), when carved for a context
+  double* hot_x = nullptr;  // Newton update (the CG solution)
   double* r = nullptr;
   float* p = nullptr;
   float* q = nullptr;
@@ -123,11 +128,12 @@ struct PcgWork {
   double* env_rel_tol = nullptr;
   int n_envs_alloc = 0;
   void release() {
-    dfree(r);
-    dfree(p);
-    dfree(q);
-    dfree(z);
-    dfree(dinv);
+    dfree(arena);
+    arena_bytes = 0;
+    hot_b = hot_x = nullptr;
+    r = nullptr;
+    p = q = dinv = nullptr;
+    z = nullptr;
     dfree(sync);
     dfree(out_iters);
     dfree(out_res);
@@ -218,6 +224,7 @@ struct sdx_context {
   float *ds_X = nullptr, *ds_T = nullptr;
   int* ds_idx = nullptr;
   std::mt19937_64 ds_rng{0};
+  bool l2_persist = false;
   // opt-in per-kernel timing: event pairs resolved lazily
   bool profiling = false;
   sdx_profile prof;
@@ -313,8 +320,7 @@ static void release_topology(sdx_context* c) {
   dfree(c->v);
   dfree(c->u0);
   dfree(c->ut);
-  dfree(c->g);
-  dfree(c->dx);
+  c->g = c->dx = nullptr;  // carved from the PCG work arena
   dfree(c->ubase);
   dfree(c->uscratch);
   dfree(c->staging);
@@ -583,24 +589,37 @@ static int choose_partition(sdx_context* c, int n_slices, const std::vector<int>
   return SDX_OK;
 }
 
-static int alloc_work(PcgWork& W, int64_t n_rows, int n_envs) {
-  if (W.n_rows == n_rows && W.n_envs_alloc == n_envs) return SDX_OK;
+static int alloc_work(PcgWork& W, int64_t n_rows, int n_envs, bool newton_vectors = false) {
+  if (W.n_rows == n_rows && W.n_envs_alloc == n_envs && (W.hot_b != nullptr) == newton_vectors) return SDX_OK;
   W.release();
-  SDX_TRY(dalloc(&W.r, 3 * n_rows));
-  SDX_TRY(dalloc(&W.p, 3 * n_rows));
-  SDX_TRY(dalloc(&W.q, 3 * n_rows));
-  SDX_TRY(dalloc(&W.z, n_rows));
-  SDX_TRY(dalloc(&W.dinv, 9 * n_rows));
+  auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t d3 = al(sizeof(double) * 3 * n_rows), f3 = al(sizeof(float) * 3 * n_rows),
+               f4 = al(sizeof(float4) * n_rows), f9 = al(sizeof(float) * 9 * n_rows);
+  W.arena_bytes = d3 * (newton_vectors ? 3 : 1) + 2 * f3 + f4 + f9;
+  SDX_TRY(dalloc(&W.arena, W.arena_bytes));
+  char* q = W.arena;
+  W.r = (double*)q;
+  q += d3;
+  if (newton_vectors) {
+    W.hot_b = (double*)q;
+    q += d3;
+    W.hot_x = (double*)q;
+    q += d3;
+  }
+  W.p = (float*)q;
+  q += f3;
+  W.q = (float*)q;
+  q += f3;
+  W.z = (float4*)q;
+  q += f4;
+  W.dinv = (float*)q;
+  SDX_CUDA(cudaMemset(W.arena, 0, W.arena_bytes));
   SDX_TRY(dalloc(&W.sync, 8));
   SDX_TRY(dalloc(&W.out_iters, n_envs));
   SDX_TRY(dalloc(&W.out_res, n_envs));
   SDX_TRY(dalloc(&W.out_relres, n_envs));
   SDX_TRY(dalloc(&W.out_conv, n_envs));
   SDX_TRY(dalloc(&W.env_rel_tol, n_envs));
-  SDX_CUDA(cudaMemset(W.p, 0, sizeof(float) * 3 * n_rows));
-  SDX_CUDA(cudaMemset(W.q, 0, sizeof(float) * 3 * n_rows));
-  SDX_CUDA(cudaMemset(W.z, 0, sizeof(float4) * n_rows));
-  SDX_CUDA(cudaMemset(W.dinv, 0, sizeof(float) * 9 * n_rows));
   W.n_rows = n_rows;
   W.n_envs_alloc = n_envs;
   return SDX_OK;
@@ -747,6 +766,10 @@ extern "C" int sdx_destroy(sdx_context* c) {
   release_mlp(c);
   prof_resolve(c);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+  if (c->l2_persist) {
+    cudaCtxResetPersistingL2Cache();
+    cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
+  }
   cudaStreamDestroy(c->stream);
   delete c;
   return SDX_OK;
@@ -786,6 +809,34 @@ extern "C" int sdx_set_params(sdx_context* c, const sdx_step_params* p) {
 
 // ------------------------------------------------------------------------------------------------
 // C-ABI: upload
+
+// Keeps the CG working vectors resident in L2 while the matrix streams through it: an access-policy
+// window on the context stream marks the vector arena persisting (process-local: the persisting carve-out
+// is a per-context limit that ends with the process). SDX_L2_PERSIST=0 disables it.
+static int set_l2_persistence(sdx_context* c) {
+  const char* env = getenv("SDX_L2_PERSIST");
+  if (env && atoi(env) == 0) return SDX_OK;
+  int max_persist = 0;
+  if (cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, c->device) != cudaSuccess ||
+      max_persist <= 0)
+    return SDX_OK;
+  int max_window = 0;
+  cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, c->device);
+  const size_t bytes = std::min<size_t>(c->work.arena_bytes, (size_t)std::max(0, max_window));
+  if (bytes == 0) return SDX_OK;
+  const size_t carve = std::min<size_t>(bytes, (size_t)max_persist);
+  SDX_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, carve));
+  cudaStreamAttrValue attr;
+  memset(&attr, 0, sizeof(attr));
+  attr.accessPolicyWindow.base_ptr = c->work.arena;
+  attr.accessPolicyWindow.num_bytes = bytes;
+  attr.accessPolicyWindow.hitRatio = (float)std::min(1.0, (double)carve / (double)bytes);
+  attr.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+  attr.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+  SDX_CUDA(cudaStreamSetAttribute(c->stream, cudaStreamAttributeAccessPolicyWindow, &attr));
+  c->l2_persist = true;
+  return SDX_OK;
+}
 
 extern "C" int sdx_upload_bodies(sdx_context* c, int n_envs, const int64_t* node_off, const int64_t* tet_off,
                                  const double* X, const int32_t* tets, const double* lambda, const double* mu,
@@ -1033,7 +1084,7 @@ extern "C" int sdx_upload_bodies(sdx_context* c, int n_envs, const int64_t* node
   SDX_TRY(upload(&c->face_slots, hfslots));
   SDX_TRY(upload(&c->row_of_node, c->h_row_of_node));
   const size_t n3 = (size_t)3 * c->n_rows;
-  for (double** pv : {&c->u, &c->v, &c->u0, &c->ut, &c->g, &c->dx, &c->ubase, &c->uscratch}) {
+  for (double** pv : {&c->u, &c->v, &c->u0, &c->ut, &c->ubase, &c->uscratch}) {
     SDX_TRY(dalloc(pv, n3));
     SDX_CUDA(cudaMemset(*pv, 0, sizeof(double) * n3));
   }
@@ -1071,7 +1122,10 @@ extern "C" int sdx_upload_bodies(sdx_context* c, int n_envs, const int64_t* node
   c->launches++;
   // PCG partition and work
   SDX_TRY(choose_partition(c, c->n_slices, c->h_slice_env, n_envs, c->h_slice_ptr, c->part, 0, 0));
-  SDX_TRY(alloc_work(c->work, c->n_rows, n_envs));
+  SDX_TRY(alloc_work(c->work, c->n_rows, n_envs, /*newton_vectors*/ true));
+  c->g = c->work.hot_b;
+  c->dx = c->work.hot_x;
+  SDX_TRY(set_l2_persistence(c));
   c->stats.assign(n_envs, sdx_env_stats{});
   c->time = 0.0;
   SDX_CUDA(cudaStreamSynchronize(c->stream));
@@ -1555,9 +1609,9 @@ extern "C" int sdx_bench_spmv(sdx_context* c, int reps, double* ms, double* byte
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  for (int i = 0; i < 3; ++i) launch_spmv(ctx_matrix(c), x, y, 256, c->stream);
+  for (int i = 0; i < 3; ++i) launch_spmv(ctx_matrix(c), x, y, 128, c->stream);
   cudaEventRecord(e0, c->stream);
-  for (int i = 0; i < reps; ++i) launch_spmv(ctx_matrix(c), x, y, 256, c->stream);
+  for (int i = 0; i < reps; ++i) launch_spmv(ctx_matrix(c), x, y, 128, c->stream);
   cudaEventRecord(e1, c->stream);
   cudaEventSynchronize(e1);
   float t = 0.0f;

@@ -468,6 +468,7 @@ __device__ __forceinline__ void load_block(const float* g, int lane, float v[9])
   v[8] = __ldcs(g + 256 + lane);
 }
 
+// Batched: the column, value and gather loads of 4 groups are issued before their FMAs (fits 64 registers).
 template <class Load>
 __device__ __forceinline__ void sell_row_product(const Matrix& A, int s, int lane, Load load, float& a0,
                                                  float& a1, float& a2) {
@@ -503,12 +504,64 @@ __device__ __forceinline__ void sell_row_product(const Matrix& A, int s, int lan
   }
 }
 
+// loads of 4 consecutive (slice, k) groups starting at k (groups past the row width load group k with
+// zero weight, so the batch needs no branch)
+__device__ __forceinline__ void load_batch(const Matrix& A, int base, int k, int w, int lane, int row, int j[4],
+                                           float v[4][9]) {
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const bool ok = k + u < w;
+    const int kk = ok ? k + u : k;
+    j[u] = ok ? (__ldcs(A.col + base + kk * kSlice + lane) & 0x7fffffff) : row;
+    load_block(A.val + (size_t)(base + kk * kSlice) * 9, lane, v[u]);
+    if (!ok) {
+#pragma unroll
+      for (int e = 0; e < 9; ++e) v[u][e] = 0.0f;
+    }
+  }
+}
+
+// Software-pipelined: the columns and values of the next batch of 4 groups are in flight while the
+// current batch gathers its x entries, so the matrix stream does not stall on the gather latency.
+template <class Load>
+__device__ __forceinline__ void sell_row_product_pipe(const Matrix& A, int s, int lane, Load load, float& a0,
+                                                      float& a1, float& a2) {
+  const int base = A.slice_ptr[s], w = A.slice_w[s];
+  const int row = s * kSlice + lane;
+  a0 = a1 = a2 = 0.0f;
+  if (w <= 0) return;
+  int j0[4], j1[4];
+  float v0[4][9], v1[4][9];
+  load_batch(A, base, 0, w, lane, row, j0, v0);
+  for (int k = 0; k < w; k += 4) {
+    const bool more = k + 4 < w;
+    if (more) load_batch(A, base, k + 4, w, lane, row, j1, v1);
+    float4 xj[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) xj[u] = load(j0[u]);
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      a0 = fmaf(v0[u][0], xj[u].x, fmaf(v0[u][1], xj[u].y, fmaf(v0[u][2], xj[u].z, a0)));
+      a1 = fmaf(v0[u][3], xj[u].x, fmaf(v0[u][4], xj[u].y, fmaf(v0[u][5], xj[u].z, a1)));
+      a2 = fmaf(v0[u][6], xj[u].x, fmaf(v0[u][7], xj[u].y, fmaf(v0[u][8], xj[u].z, a2)));
+    }
+    if (more) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        j0[u] = j1[u];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) v0[u][e] = v1[u][e];
+      }
+    }
+  }
+}
+
 __global__ void k_spmv(Matrix A, const float4* __restrict__ x, float* __restrict__ y) {
   const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (s >= A.n_slices) return;
   float a0, a1, a2;
-  sell_row_product(A, s, lane, [&](int j) { return __ldg(x + j); }, a0, a1, a2);
+  sell_row_product_pipe(A, s, lane, [&](int j) { return __ldg(x + j); }, a0, a1, a2);
   const int64_t row = (int64_t)s * kSlice + lane;
   y[3 * row] = a0;
   y[3 * row + 1] = a1;
@@ -648,7 +701,10 @@ __device__ __forceinline__ void true_residual(const PcgArgs& a, int s, int lane,
   r[2] = a.b[3 * row + 2] - a2;
 }
 
-__global__ void k_pcg(PcgArgs a) {
+// kPipe: SpMV phase with the software-pipelined row product (128 registers, so at most 512 threads per
+// SM); otherwise the batched product that fits 64 registers at 1024 threads.
+template <bool kPipe>
+__global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
   extern __shared__ double wacc[];  // [nwarps][kPcgMaxEnvsPerCta][kPcgNq]
   __shared__ EnvState st[kPcgMaxEnvsPerCta];
   __shared__ double tot[kPcgMaxEnvsPerCta][kPcgNq];
@@ -837,7 +893,10 @@ __global__ void k_pcg(PcgArgs a) {
       if (st[le].status != 0) continue;
       const int64_t row = (int64_t)s * kSlice + lane;
       float a0, a1, a2;
-      sell_row_product(a.A, s, lane, [&](int j) { return __ldcg(a.z + j); }, a0, a1, a2);
+      if constexpr (kPipe)
+        sell_row_product_pipe(a.A, s, lane, [&](int j) { return __ldcg(a.z + j); }, a0, a1, a2);
+      else
+        sell_row_product(a.A, s, lane, [&](int j) { return __ldcg(a.z + j); }, a0, a1, a2);
       const float4 zr = a.z[row];
       float pn[3], qn[3];
       if (st[le].first) {
@@ -969,10 +1028,22 @@ __global__ void k_pcg(PcgArgs a) {
   }
 }
 
+// The pipelined variant runs at 512 threads per CTA or fewer (SDX_PCG_PIPE=0 selects the batched one).
+static bool pcg_pipelined(int threads) {
+  static const int pipe = [] {
+    const char* e = getenv("SDX_PCG_PIPE");
+    return e ? atoi(e) : 1;
+  }();
+  return pipe != 0 && threads <= 512;
+}
+
 int pcg_max_ctas_per_sm(int threads) {
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pcg, threads, pcg_shared_bytes(threads)) != cudaSuccess) return 0;
-  return n;
+  const cudaError_t e =
+      pcg_pipelined(threads)
+          ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pcg<true>, threads, pcg_shared_bytes(threads))
+          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pcg<false>, threads, pcg_shared_bytes(threads));
+  return e == cudaSuccess ? n : 0;
 }
 
 int pcg_shared_bytes(int threads) { return (threads / 32) * kPcgMaxEnvsPerCta * kPcgNq * (int)sizeof(double); }
@@ -980,8 +1051,10 @@ int pcg_shared_bytes(int threads) { return (threads / 32) * kPcgMaxEnvsPerCta * 
 cudaError_t launch_pcg(const PcgArgs& a, int n_cta, int threads, cudaStream_t st) {
   PcgArgs args = a;
   void* params[] = {&args};
-  return cudaLaunchCooperativeKernel((const void*)k_pcg, dim3(n_cta), dim3(threads), params,
+  const void* fn = pcg_pipelined(threads) ? (const void*)k_pcg<true> : (const void*)k_pcg<false>;
+  return cudaLaunchCooperativeKernel(fn, dim3(n_cta), dim3(threads), params,
                                      (size_t)pcg_shared_bytes(threads), st);
 }
 
 }  // namespace sdx
+

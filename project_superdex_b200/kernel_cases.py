@@ -1,0 +1,79 @@
+"""Fixed-length launches of the hot kernels, sized for profiler captures.
+
+    python -m project_superdex_b200.kernel_cases pcg --iters 100
+        one backward-Euler step limited to one Newton iteration whose persistent PCG launch runs exactly
+        `iters` CG iterations (the tolerance is unreachable), after one untimed warm-up step;
+    python -m project_superdex_b200.kernel_cases element
+        one full assembly (energy, residual, PSD-projected Hessian) of the current state;
+    python -m project_superdex_b200.kernel_cases spmv --reps 3
+        `reps` standalone SpMVs of the last assembled matrix.
+
+The workload is the single-body 64^3-cell grid (274,625 nodes, 1,572,864 tets, 5 capsules) unless
+`--cells` says otherwise. One JSON line reports the sizes and the algorithmic bytes of one launch (or one
+CG iteration), so that DRAM counters from a capture divide into per-unit traffic. Only the measured
+launches run between cudaProfilerStart and cudaProfilerStop (capture with `ncu --profile-from-start off`).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+from . import scenes
+from .soft_body import SoftBodyWorld
+
+
+def pcg_bytes_per_iter(nnzb: int, n_rows: int) -> int:
+    """Algorithmic HBM bytes of one fused Jacobi-PCG iteration: the matrix once (36 B values + 4 B column
+    per 3x3 block), the slice pointers, and per row 228 B of vector traffic (phase 1: own z 12 + gathered
+    z 12 + p and q read/write 48; phase 2: FP64 x and r read/write 96, p 12, q 12, Jacobi diagonal 12,
+    z read/write 24)."""
+    return nnzb * 40 + 4 * (n_rows + 1) + 228 * n_rows
+
+
+def element_bytes(n_tets: int, n_nodes: int, nnzb: int) -> int:
+    """Algorithmic HBM bytes of one assembly launch: per tet its 4 row indices 16 B, rest data 64 B and
+    16 block positions 64 B; per node u and the inertia target (FP64, 48 B) read and the FP64 gradient
+    read/modified/written (48 B); the Hessian values written once (36 B per block)."""
+    return n_tets * (16 + 64 + 64) + n_nodes * (48 + 48) + nnzb * 36
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("case", choices=["pcg", "element", "spmv"])
+    ap.add_argument("--cells", type=int, default=64)
+    ap.add_argument("--iters", type=int, default=100)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--seed", type=int, default=0)
+    args = ap.parse_args(argv)
+    bodies, cfg = scenes.config1(args.seed, n=args.cells)
+    w = SoftBodyWorld(bodies, cfg, newton_abs_tol=1e-9)
+    w.step(1)  # warm-up: assembles a contact state and the matrix
+    import torch
+    torch.cuda.synchronize()
+    out = {"case": args.case, "cells": args.cells, "n_nodes": w.n_nodes, "n_tets": w.n_tets, "nnzb": w.nnzb}
+    if args.case == "pcg":
+        w.set_params(newton_max_iter=1, linear_max_iter=args.iters, linear_rel_tol=1e-30, linear_abs_tol=0.0)
+        torch.cuda.profiler.start()
+        w.step(1)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        st = w.stats()[0]
+        out.update(cg_iters=st["cg_iters"], bytes_per_iter=pcg_bytes_per_iter(w.nnzb, w.n_nodes))
+    elif args.case == "element":
+        torch.cuda.profiler.start()
+        w.assemble(hess=True, psd=True, obj=True)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        out.update(bytes_per_launch=element_bytes(w.n_tets, w.n_nodes, w.nnzb))
+    else:
+        torch.cuda.profiler.start()
+        ms, by = w.bench_spmv(reps=args.reps)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        out.update(ms=ms, bytes_per_launch=by)
+    w.close()
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()
