@@ -8,6 +8,17 @@ Newton to rel 1e-6 with Jacobi-PCG at rel. residual 1e-6. A step is one backward
 env of the batch. Inputs (matrix ~160 MB, tet data ~300 MB) exceed the 126 MB L2.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload cfg1|cfg0|cfg2]
+                  [--arms plain_fp64,fused_zero,learned]
+
+Three solver arms on the same GPU and the same seeded workload, each a full Newton step:
+  plain_fp64  the reference's CUDA PCG path restated (FP64 3x3 BSR with cuSPARSE bsrmv, cuBLAS vector
+              operations, CUDA-graph bursts of 8 iterations with a host convergence check, one env after
+              the other), zero initial guess;
+  fused_zero  this library's persistent batched PCG (FP32 matrix / SpMV, FP64 x, r and reductions),
+              zero initial guess (the reference's Newton behaviour);
+  learned     the same with the learned warm start (per-vertex MLP trained first, on the GPU, from
+              plain-solver episodes of held-out seeds).
+The headline `value` is the last arm (learned); `arms` gives each and the ratios.
 
 N > 1 runs one independent replica per GPU (the path shards by environment and has no exchange),
 launched by torchrun; timing is the max over ranks.
@@ -155,18 +166,36 @@ def vector_bytes_per_node():
     return 12 + 12 + 24 + 24 + 48 + 48 + 12 + 12 + 12 + 24
 
 
-def run_ours(args, rank, world, local_rank):
-    import torch
+def train_warm_start(args, local_rank):
+    """Train the warm-start MLP on the GPU from plain-solver episodes of held-out seeds of the same
+    workload (never the evaluated seed). Returns (params, info)."""
+    from project_superdex_b200.learned import Mlp, collect
     from project_superdex_b200.soft_body import SoftBodyWorld
-    torch.cuda.set_device(local_rank)
-    (bodies, cfg), desc = build_workload(args.workload, seed=args.seed)
-    # Newton to rel 1e-6 (the absolute floor is only a guard for an exactly zero residual)
-    w = SoftBodyWorld(bodies, cfg, device=local_rank, warm_start=args.warm_start, newton_abs_tol=1e-9)
-    n_envs = w.n_envs
-    stream = torch.cuda.ExternalStream(w.stream_handle(), device=local_rank)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
+    t0 = time.perf_counter()
+    Xs, Ts = [], []
+    for k in range(args.train_episodes):
+        (bodies, cfg), _ = build_workload(args.workload, seed=args.seed + 1000 + k)
+        tw = SoftBodyWorld(bodies, cfg, device=local_rank, newton_abs_tol=1e-9)
+        X, T = collect(tw, args.train_steps, samples_per_solve=65536, capacity=1 << 20, seed=k)
+        Xs.append(X)
+        Ts.append(T)
+        if k < args.train_episodes - 1:
+            tw.close()
+    X, T = np.concatenate(Xs), np.concatenate(Ts)
+    m = Mlp(tw._ctx)
+    m.init(args.seed)
+    losses = m.train(X, T, batch=4096, epochs=args.train_epochs, lr=1e-3, seed=args.seed)
+    params = m.get_params()
+    tw.close()
+    return params, {"episodes": args.train_episodes, "steps_per_episode": args.train_steps,
+                    "samples": int(X.shape[0]), "epochs": args.train_epochs, "loss_first": float(losses[0]),
+                    "loss_last": float(losses[-1]), "seconds": time.perf_counter() - t0,
+                    "seeds": f"{args.seed + 1000}..{args.seed + 999 + args.train_episodes} (held out)"}
+
+
+def time_arm(w, args, stream, local_rank, dist, world):
+    """W untimed steps, then exactly K steps between CUDA events on the library stream."""
+    import torch
     w.step(args.warmup)
     torch.cuda.synchronize()
     if dist:
@@ -190,14 +219,56 @@ def run_ours(args, rank, world, local_rank):
         t = torch.tensor([ms], device=f"cuda:{local_rank}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    value = world * n_envs * args.steps / (ms / 1000.0)
+    n_envs = w.n_envs
+    # over the K timed steps: one PCG launch per Newton iteration (all envs together), and per launch the
+    # iterations of its slowest env
+    return {"value": world * n_envs * args.steps / (ms / 1000.0), "ms": ms, "prof": prof, "launches": launches,
+            "clocks": clk.summary(),
+            "cg_iters_per_step": prof["pcg_iters"] / args.steps,
+            "newton_iters_per_step": prof["pcg_launches"] / args.steps,
+            "last_step_cg_iters_mean_env": sum(s["cg_iters"] for s in stats) / max(1, n_envs)}
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from project_superdex_b200 import capi
+    from project_superdex_b200.learned import Mlp
+    from project_superdex_b200.soft_body import SoftBodyWorld
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    arms = [a for a in args.arms.split(",") if a]
+    params, train_info = (None, None)
+    if "learned" in arms:
+        params, train_info = train_warm_start(args, local_rank)
+    (bodies, cfg), desc = build_workload(args.workload, seed=args.seed)
+    results = {}
+    w = None
+    for arm in arms:
+        if w is not None:
+            w.close()
+        # Newton to rel 1e-6 (the absolute floor is only a guard for an exactly zero residual)
+        w = SoftBodyWorld(bodies, cfg, device=local_rank, newton_abs_tol=1e-9)
+        if arm == "learned":
+            Mlp(w._ctx).set_params(params)
+        w.set_params(warm_start=capi.SDX_WARM_LEARNED if arm == "learned" else capi.SDX_WARM_ZERO,
+                     linear_solver_impl=(capi.SDX_SOLVER_PLAIN_FP64 if arm == "plain_fp64"
+                                         else capi.SDX_SOLVER_FUSED))
+        stream = torch.cuda.ExternalStream(w.stream_handle(), device=local_rank)
+        results[arm] = time_arm(w, args, stream, local_rank, dist, world)
+    head = results[arms[-1]]  # the headline arm is the last one (learned by default); w is its world
+    n_envs = w.n_envs
+    ms, prof = head["ms"], head["prof"]
 
     # roofline of the dominant kernel (the persistent PCG)
     peak, peak_kind = measured_peaks()
+    # algorithmic bytes: per env, its CG iterations x (40 B per block + 4 B per row pointer + 228 B per
+    # row), summed by the library over the timed launches (envs of a batch converge at different counts)
     bytes_iter = w.nnzb * 40 + 4 * (w.n_nodes + 1) + vector_bytes_per_node() * w.n_nodes
     pcg_s = prof["pcg_ms"] / 1000.0
-    achieved = prof["pcg_iters"] * bytes_iter / pcg_s / 1e9 if pcg_s > 0 else None
-    traffic = ncu_traffic("k_pcg_per_iter")
+    achieved = prof["pcg_bytes"] / pcg_s / 1e9 if pcg_s > 0 else None
+    traffic = ncu_traffic("k_pcg_per_iter") if args.workload == "cfg1" else None
     roofline = {"bound": "hbm", "kernel": "k_pcg (persistent Jacobi-PCG)", "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                 "peak_source": peak_kind, "traffic": traffic, "bytes_per_iter": bytes_iter,
@@ -208,6 +279,7 @@ def run_ours(args, rank, world, local_rank):
     spmv["frac"] = spmv["achieved_gbs"] / peak
 
     # end to end through the public API with pinned host buffers, copies inside the timed region
+    stream = torch.cuda.ExternalStream(w.stream_handle(), device=local_rank)
     hu = torch.empty(3 * w.n_nodes, dtype=torch.float64, pin_memory=True).numpy()
     hv = torch.empty(3 * w.n_nodes, dtype=torch.float64, pin_memory=True).numpy()
     _, _, t_state = w.get_state(hu, hv)
@@ -216,7 +288,6 @@ def run_ours(args, rank, world, local_rank):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    t_wall = time.perf_counter()
     for _ in range(e2e_steps):
         w.set_state(hu, hv, t_state)
         w.step(1)
@@ -230,24 +301,35 @@ def run_ours(args, rank, world, local_rank):
         e2e_ms = float(t.item())
     e2e = {"value": world * n_envs * e2e_steps / (e2e_ms / 1000.0), "unit": UNIT,
            "h2d_bytes_per_step": 2 * 3 * 8 * w.n_nodes, "d2h_bytes_per_step": 2 * 3 * 8 * w.n_nodes,
-           "steps": e2e_steps}
-    cg_per_step = sum(s["cg_iters"] for s in stats) / max(1, n_envs)
+           "steps": e2e_steps, "warm_start": arms[-1]}
+    arm_summary = {a: {"value": r["value"], "ms_per_step": r["ms"] / args.steps,
+                       "cg_iters_per_step": r["cg_iters_per_step"],
+                       "newton_iters_per_step": r["newton_iters_per_step"]} for a, r in results.items()}
+    for base in ("plain_fp64", "fused_zero"):
+        if base in results and "learned" in results:
+            arm_summary[f"learned_over_{base}"] = results["learned"]["value"] / results[base]["value"]
+            arm_summary[f"cg_iters_learned_over_{base}"] = (results["learned"]["cg_iters_per_step"]
+                                                            / results[base]["cg_iters_per_step"])
+    reasons = sorted(set().union(*[set(r["clocks"].get("reasons", [])) for r in results.values()]))
+    clocks = dict(head["clocks"])
+    clocks["reasons_all_arms"] = reasons
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic (seeded tet grids, random materials and collider trajectories)",
         "config": {"workload": f"{args.workload}: {desc}", "n_envs": n_envs, "n_nodes": w.n_nodes,
                    "n_tets": w.n_tets, "nnzb": w.nnzb,
                    "precision": "FP32 Hessian assembly + SpMV, FP64 residual / energy / CG dots / x,r",
-                   "warm_start": ["zero", "previous", "learned"][args.warm_start],
+                   "warm_start": arms[-1], "arms": arms,
                    "cg_rel_tol": 1e-6, "newton_rel_tol": 1e-6, "newton_abs_tol": 1e-9,
                    "l2": "inputs larger than L2 (matrix + tet data > 126 MB)",
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
-        "roofline": roofline, "spmv": spmv, "e2e": e2e, "gpu_launches": launches,
-        "clocks": clk.summary(),
-        "solver": {"cg_iters_per_step": cg_per_step,
-                   "newton_iters_per_step": sum(s["newton_iters"] for s in stats) / max(1, n_envs),
+        "arms": arm_summary, "training": train_info,
+        "roofline": roofline, "spmv": spmv, "e2e": e2e, "gpu_launches": head["launches"],
+        "clocks": clocks,
+        "solver": {"cg_iters_per_step": head["cg_iters_per_step"],
+                   "newton_iters_per_step": head["newton_iters_per_step"],
                    "profile_ms": {k: v for k, v in prof.items() if k.endswith("_ms")}},
     }
     if rank == 0 and not args.no_cpu_baseline:
@@ -263,7 +345,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2"])
-    ap.add_argument("--warm-start", type=int, default=0, dest="warm_start")
+    ap.add_argument("--arms", default="plain_fp64,fused_zero,learned",
+                    help="comma list of solver arms to time, headline last: plain_fp64 (the reference's CUDA "
+                         "PCG path restated: FP64 BSR, cuSPARSE/cuBLAS, zero start), fused_zero (this "
+                         "library's PCG, zero start), learned (this library's PCG, learned warm start)")
+    ap.add_argument("--train-episodes", type=int, default=2, dest="train_episodes")
+    ap.add_argument("--train-steps", type=int, default=8, dest="train_steps")
+    ap.add_argument("--train-epochs", type=int, default=8, dest="train_epochs")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -82,7 +82,16 @@ typedef struct {
   int abort_if_not_spd; /* stop with DIVERGED on p.Ap <= 0 */
   int polak_ribiere;    /* 1: Polak-Ribiere beta (reference default) */
   int replace_every;    /* FP64 true-residual replacement period in iterations (0: default 32) */
+  int solver_impl;      /* SDX_SOLVER_* (used by sdx_step; the sdx_pcg_solve* entry points are fused) */
 } sdx_linear_params;
+
+/* Linear solver implementations behind sdx_step. FUSED: this library's persistent, batched Jacobi-PCG
+ * (FP32 matrix and SpMV, FP64 x, r and reductions). PLAIN_FP64: the reference's CUDA solver path
+ * (krylov::CudaPCG, cuda_pcg.cpp:243-525) restated as the same-GPU comparison arm — FP64 3x3 BSR with
+ * cuSPARSE bsrmv, cuBLAS vector operations, CUDA-graph bursts of 8 iterations with a host convergence
+ * check after each, one env after the other; Jacobi or no preconditioner. */
+#define SDX_SOLVER_FUSED 0
+#define SDX_SOLVER_PLAIN_FP64 1
 
 /* Mirrors LinearSolverStatus (krylov_solver.h:85-116). */
 typedef struct {
@@ -256,6 +265,8 @@ typedef struct {
   int64_t contact_launches;
   double seed_ms;           /* Hessian seeding with the scaled mass matrix */
   int64_t seed_launches;
+  double pcg_bytes;         /* algorithmic HBM bytes of the PCG launches: per env, its CG iterations x
+                               (40 B per block + 4 B per row pointer + 228 B per row) */
 } sdx_profile;
 int sdx_set_profiling(sdx_context* ctx, int enable);
 int sdx_get_profile(sdx_context* ctx, sdx_profile* out);

@@ -20,6 +20,7 @@ SDX_F32, SDX_F64 = 0, 1
 SDX_PREC_NONE, SDX_PREC_JACOBI, SDX_PREC_BLOCK_JACOBI = 0, 1, 2
 SDX_WARM_ZERO, SDX_WARM_PREVIOUS, SDX_WARM_LEARNED = 0, 1, 2
 SDX_LINEAR_CONVERGED, SDX_LINEAR_STOPPED, SDX_LINEAR_DIVERGED = 1, 2, 3
+SDX_SOLVER_FUSED, SDX_SOLVER_PLAIN_FP64 = 0, 1
 
 # every entry point include/sdx_b200.h declares
 EXPORTED = [
@@ -41,7 +42,7 @@ class LinearParams(C.Structure):
 
     _fields_ = [("rel_tol", C.c_double), ("abs_tol", C.c_double), ("rel_div_tol", C.c_double),
                 ("max_iter", C.c_int), ("preconditioner", C.c_int), ("abort_if_not_spd", C.c_int),
-                ("polak_ribiere", C.c_int), ("replace_every", C.c_int)]
+                ("polak_ribiere", C.c_int), ("replace_every", C.c_int), ("solver_impl", C.c_int)]
 
 
 class LinearStatus(C.Structure):
@@ -72,7 +73,7 @@ class Profile(C.Structure):
                 ("asm_hess_ms", C.c_double), ("asm_hess_launches", C.c_int64),
                 ("asm_res_ms", C.c_double), ("asm_res_launches", C.c_int64),
                 ("contact_ms", C.c_double), ("contact_launches", C.c_int64),
-                ("seed_ms", C.c_double), ("seed_launches", C.c_int64)]
+                ("seed_ms", C.c_double), ("seed_launches", C.c_int64), ("pcg_bytes", C.c_double)]
 
 
 _dp = C.POINTER(C.c_double)

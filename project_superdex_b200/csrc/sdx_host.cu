@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <numeric>
 #include <string>
 #include <vector>
@@ -17,6 +18,7 @@
 #include "../../include/sdx_b200.h"
 #include "sdx_internal.cuh"
 #include "sdx_mlp.cuh"
+#include "sdx_plain.cuh"
 #include <random>
 
 using namespace sdx;
@@ -161,6 +163,7 @@ struct sdx_context {
   // host topology
   std::vector<int64_t> h_node_off, h_tet_off, h_row_off;
   std::vector<int32_t> h_row_of_node;
+  std::vector<double> h_env_pcg_bytes;  // algorithmic bytes of one CG iteration of each env
   std::vector<int64_t> h_prow;  // user pattern row_ptr
   std::vector<int32_t> h_pcol;  // user pattern columns (user node ids)
   std::vector<int> h_slice_ptr, h_slice_w, h_slice_env;
@@ -225,6 +228,7 @@ struct sdx_context {
   int* ds_idx = nullptr;
   std::mt19937_64 ds_rng{0};
   bool l2_persist = false;
+  std::unique_ptr<PlainSolver> plain;  // the plain FP64 comparison solver, built on first use
   // opt-in per-kernel timing: event pairs resolved lazily
   bool profiling = false;
   sdx_profile prof;
@@ -296,6 +300,7 @@ static void prof_resolve(sdx_context* c) {
 }
 
 static void release_topology(sdx_context* c) {
+  c->plain.reset();
   dfree(c->slice_ptr);
   dfree(c->slice_w);
   dfree(c->slice_env);
@@ -687,6 +692,8 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
     SDX_CUDA(cudaMemcpy(its.data(), W.out_iters, sizeof(int) * n_envs, cudaMemcpyDeviceToHost));
     c->prof.pcg_iters += *std::max_element(its.begin(), its.end());
     c->prof.pcg_launches++;
+    if (A.val == c->val && (int)c->h_env_pcg_bytes.size() == n_envs)
+      for (int e = 0; e < n_envs; ++e) c->prof.pcg_bytes += its[e] * c->h_env_pcg_bytes[e];
   }
   return SDX_OK;
 }
@@ -706,6 +713,7 @@ extern "C" void sdx_default_linear_params(sdx_linear_params* p) {
   p->abort_if_not_spd = 0;
   p->polak_ribiere = 1;
   p->replace_every = 32;
+  p->solver_impl = SDX_SOLVER_FUSED;
 }
 
 extern "C" void sdx_default_step_params(sdx_step_params* p) {
@@ -913,6 +921,12 @@ extern "C" int sdx_upload_bodies(sdx_context* c, int n_envs, const int64_t* node
   c->h_prow.assign(N + 1, 0);
   for (int64_t i = 0; i < N; ++i) c->h_prow[i + 1] = c->h_prow[i] + deg[i];
   c->nnzb = c->h_prow[N];
+  c->h_env_pcg_bytes.assign(n_envs, 0.0);
+  for (int e = 0; e < n_envs; ++e) {
+    const int64_t n_e = node_off[e + 1] - node_off[e];
+    const int64_t b_e = c->h_prow[node_off[e + 1]] - c->h_prow[node_off[e]];
+    c->h_env_pcg_bytes[e] = 40.0 * (double)b_e + 4.0 * (double)(n_e + 1) + 228.0 * (double)n_e;
+  }
   c->h_pcol.resize(c->nnzb);
 #pragma omp parallel
   {
@@ -1422,6 +1436,39 @@ static int capture_samples(sdx_context* c, const std::vector<uint8_t>& mask) {
   return SDX_OK;
 }
 
+// The plain FP64 comparison solver (sdx_plain.cu) on the envs in mask: builds its FP64 BSR structure on
+// first use, converts the assembled values, and solves env after env into c->dx.
+static int run_plain(sdx_context* c, const std::vector<uint8_t>& mask, const sdx_linear_params& lp, bool zero,
+                     std::vector<int>& it_out) {
+  if (!c->plain) {
+    PlainTopology t;
+    t.n_envs = c->n_envs;
+    t.row_off = c->h_row_off;
+    t.node_off = c->h_node_off;
+    t.prow = c->h_prow.data();
+    t.pcol = c->h_pcol.data();
+    t.row_of_node = c->h_row_of_node.data();
+    t.slice_ptr = c->h_slice_ptr.data();
+    auto ps = std::make_unique<PlainSolver>();
+    const int rc = ps->build(t);
+    if (rc != 0) return set_error(rc == -1 ? SDX_ERR_OUT_OF_MEMORY : SDX_ERR_CUDA, "plain solver set-up failed (%d)", rc);
+    c->plain = std::move(ps);
+  }
+  if (lp.preconditioner == SDX_PREC_BLOCK_JACOBI)
+    return set_error(SDX_ERR_UNSUPPORTED, "the plain FP64 solver supports the Jacobi and no preconditioner");
+  cudaEvent_t ev;
+  prof_begin(c, &ev);
+  std::vector<int> conv;
+  const int rc = c->plain->solve(c->val, c->g, c->dx, mask.data(), lp, zero, c->stream, it_out, conv);
+  prof_end(c, PROF_PCG, ev);
+  if (rc != 0) return set_error(SDX_ERR_CUDA, "plain solver failed (%d)", rc);
+  if (c->profiling) {
+    c->prof.pcg_iters += *std::max_element(it_out.begin(), it_out.end());
+    c->prof.pcg_launches++;
+  }
+  return SDX_OK;
+}
+
 static int step_once(sdx_context* c) {
   const sdx_step_params& p = c->params;
   const int E = c->n_envs;
@@ -1502,10 +1549,14 @@ static int step_once(sdx_context* c) {
     const bool zero = p.warm_start == SDX_WARM_ZERO;
     if (p.ew_forcing == 2)
       SDX_CUDA(cudaMemcpyAsync(c->work.env_rel_tol, eta.data(), sizeof(double) * E, cudaMemcpyHostToDevice, c->stream));
-    SDX_TRY(run_pcg(c, ctx_matrix(c), c->diag_pos, E, c->part, c->work, c->g, c->dx, c->env_mask, n_active,
-                    p.linear, zero, p.ew_forcing == 2 ? c->work.env_rel_tol : nullptr, /*scale_guess*/ !zero));
     std::vector<int> it_out(E);
-    SDX_CUDA(cudaMemcpy(it_out.data(), c->work.out_iters, sizeof(int) * E, cudaMemcpyDeviceToHost));
+    if (p.linear.solver_impl == SDX_SOLVER_PLAIN_FP64) {
+      SDX_TRY(run_plain(c, mask, p.linear, zero, it_out));
+    } else {
+      SDX_TRY(run_pcg(c, ctx_matrix(c), c->diag_pos, E, c->part, c->work, c->g, c->dx, c->env_mask, n_active,
+                      p.linear, zero, p.ew_forcing == 2 ? c->work.env_rel_tol : nullptr, /*scale_guess*/ !zero));
+      SDX_CUDA(cudaMemcpy(it_out.data(), c->work.out_iters, sizeof(int) * E, cudaMemcpyDeviceToHost));
+    }
     for (int e = 0; e < E; ++e)
       if (mask[e]) cg[e] += it_out[e];
     if (learned) SDX_TRY(mlp_check_error(c));

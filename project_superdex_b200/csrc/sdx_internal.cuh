@@ -22,7 +22,7 @@ namespace sdx {
 constexpr int kSlice = 32;
 constexpr int kPadBit = 0x80000000;
 constexpr int kPcgMaxEnvsPerCta = 32;
-constexpr int kPcgNq = 3;  // partial sums per (CTA, env) and phase
+constexpr int kPcgNq = 5;  // partial sums per (CTA, env) and phase
 
 __host__ __device__ __forceinline__ size_t val_index(int64_t p, int e) {
   const size_t g = (size_t)(p - (p & 31)) * 9;

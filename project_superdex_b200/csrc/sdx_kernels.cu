@@ -781,7 +781,9 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
   const bool scaled = !a.zero_guess && a.scale_guess;
   if (scaled) {
     // energy-optimal scaling of the guess: alpha = (x0.b) / (x0.A x0), A x0 = b - r0; the scaled start
-    // alpha x0 never has a larger A-norm error than the zero start
+    // alpha x0 never has a larger A-norm error than the zero start. The guess is kept only if it also
+    // lowers the residual the stop test measures: ||b - alpha A x0||^2 = (1-alpha)^2 b.b
+    // + 2 alpha (1-alpha) b.r0 + alpha^2 r0.r0 < b.b; otherwise the env falls back to the zero start.
     clear_acc();
     for (int s = s0 + warp; s < s1; s += nwarps) {
       const int le = a.A.slice_env[s] - e0;
@@ -789,7 +791,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
       const int64_t row = (int64_t)s * kSlice + lane;
       double r[3];
       true_residual(a, s, lane, r);
-      double xb = 0.0, xr = 0.0, bb = 0.0;
+      double xb = 0.0, xr = 0.0, bb = 0.0, br = 0.0, rr = 0.0;
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         a.r[3 * row + k] = r[k];
@@ -797,17 +799,24 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
         xb += xk * bk;
         xr += xk * r[k];
         bb += bk * bk;
+        br += bk * r[k];
+        rr += r[k] * r[k];
       }
       add_acc(le, 0, bb);
       add_acc(le, 1, xb);
       add_acc(le, 2, xr);
+      add_acc(le, 3, br);
+      add_acc(le, 4, rr);
     }
-    flush_acc(3, 1);
+    flush_acc(5, 1);
     if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
-    reduce_tot(3, 1);
+    reduce_tot(5, 1);
     for (int le = threadIdx.x; le < ne; le += blockDim.x) {
-      const double xb = tot[le][1], xax = tot[le][1] - tot[le][2];
-      st[le].alpha = (xax > 0.0 && xb > 0.0 && isfinite(xb / xax)) ? xb / xax : 0.0;
+      const double bb = tot[le][0], xb = tot[le][1], xax = tot[le][1] - tot[le][2];
+      double al = (xax > 0.0 && xb > 0.0 && isfinite(xb / xax)) ? xb / xax : 0.0;
+      const double ra = (1.0 - al) * (1.0 - al) * bb + 2.0 * al * (1.0 - al) * tot[le][3] + al * al * tot[le][4];
+      if (!(ra < bb)) al = 0.0;
+      st[le].alpha = al;
     }
     __syncthreads();
   }
