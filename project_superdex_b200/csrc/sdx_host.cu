@@ -521,12 +521,13 @@ static int choose_partition(sdx_context* c, int n_slices, const std::vector<int>
                             const std::vector<int>& slice_ptr, PcgPartition& P, int threads_req,
                             int ctas_per_sm_req) {
   P.release();
-  // launch shape: explicit request, else SDX_PCG_THREADS / SDX_PCG_CTAS_PER_SM, else 1024 x 1
+  // launch shape: explicit request, else SDX_PCG_THREADS / SDX_PCG_CTAS_PER_SM, else 512 x 1 (the
+  // software-pipelined SpMV variant, 128 registers per thread)
   if (threads_req <= 0 && getenv("SDX_PCG_THREADS")) threads_req = atoi(getenv("SDX_PCG_THREADS"));
   if (ctas_per_sm_req <= 0 && getenv("SDX_PCG_CTAS_PER_SM")) ctas_per_sm_req = atoi(getenv("SDX_PCG_CTAS_PER_SM"));
   if (threads_req > 0 && (threads_req % 32 != 0 || threads_req > 1024))
     return set_error(SDX_ERR_INVALID_ARGUMENT, "PCG threads must be a multiple of 32 up to 1024");
-  const int threads = threads_req > 0 ? threads_req : 1024;
+  const int threads = threads_req > 0 ? threads_req : 512;
   const int max_active = pcg_max_ctas_per_sm(threads);
   if (max_active <= 0) return set_error(SDX_ERR_CUDA, "PCG kernel cannot be resident with %d threads", threads);
   // cooperative launch: every CTA must be co-resident

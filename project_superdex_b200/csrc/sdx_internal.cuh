@@ -119,7 +119,7 @@ struct PcgArgs {
   double* out_res;
   double* out_relres;
   int* out_conv;
-  unsigned* sync;  // [0] barrier count, [1] barrier generation, [2] error, [3] active, [4] verify_iter
+  unsigned* sync;  // [0] barrier arrivals (monotonic), [1] unused, [2] error, [3] active, [4] verify_iter
   long long spin_limit;
 };
 

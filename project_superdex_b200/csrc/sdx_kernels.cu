@@ -630,28 +630,33 @@ struct EnvState {
   int first;
 };
 
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid barrier on a monotonically increasing arrival counter (sync[0], zero at launch): the k-th barrier
+// of a launch completes when the counter reaches k * nblocks. One atomic per CTA and no reset, so the
+// last arrival releases every waiting CTA within one L2 round trip. The spin is bounded: on timeout
+// sync[2] is set and every CTA unwinds.
 __device__ __forceinline__ bool grid_barrier(unsigned* sync, unsigned nblocks, long long spin_limit) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile unsigned* vgen = sync + 1;
-    const unsigned gen = *vgen;
-    __threadfence();
-    const unsigned prev = atomicAdd(sync, 1u);
-    if (prev == nblocks - 1) {
-      atomicExch(sync, 0u);
-      __threadfence();
-      atomicAdd(sync + 1, 1u);
-    } else {
-      long long spins = 0;
-      while (*vgen == gen) {
-        if (++spins > spin_limit) {
-          atomicExch(sync + 2, 1u);  // device timeout: recorded, the kernel unwinds
-          break;
-        }
-        __nanosleep(32);
+    // release: this CTA's writes (ordered before thread 0 by the CTA barrier) become visible with the
+    // arrival; acquire: the poll that sees the last arrival orders every later load of the CTA after all
+    // CTAs' pre-barrier writes (the CTA barrier below extends it to the other threads)
+    unsigned prev;
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], 1;" : "=r"(prev) : "l"(sync) : "memory");
+    const unsigned target = (prev / nblocks + 1u) * nblocks;
+    long long spins = 0;
+    while ((int)(ld_acquire_gpu(sync) - target) < 0) {
+      if (++spins > spin_limit) {
+        atomicExch(sync + 2, 1u);  // device timeout: recorded, the kernel unwinds
+        break;
       }
+      __nanosleep(32);
     }
-    __threadfence();
   }
   __syncthreads();
   return *((volatile unsigned*)(sync + 2)) == 0u;
@@ -767,6 +772,28 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
       a.out_relres[e] = st[le].bb == 0.0 ? 0.0 : sqrt(fmax(rr, 0.0) / st[le].bb);
       a.out_conv[e] = st[le].status;
       atomicSub((int*)(a.sync + 3), 1);
+    }
+  };
+
+  // A CTA whose slices all belong to one env keeps its dot-product partials in registers through a
+  // phase and reduces them across the warp once, at the end (acc_end); otherwise every slice adds its
+  // warp sum to the shared per-(warp, env) slots directly.
+  const bool single_env = ne == 1;
+  double acc[3] = {0.0, 0.0, 0.0};
+  auto acc_add = [&](int le, int k, double v) {
+    if (single_env)
+      acc[k] += v;
+    else
+      add_acc(le, k, v);
+  };
+  auto acc_end = [&](int nq) {  // nq is 1 or 3; constant indices keep acc[] in registers
+    if (!single_env) return;
+    add_acc(0, 0, acc[0]);
+    acc[0] = 0.0;
+    if (nq > 1) {
+      add_acc(0, 1, acc[1]);
+      add_acc(0, 2, acc[2]);
+      acc[1] = acc[2] = 0.0;
     }
   };
 
@@ -901,36 +928,41 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
       const int le = a.A.slice_env[s] - e0;
       if (st[le].status != 0) continue;
       const int64_t row = (int64_t)s * kSlice + lane;
-      float a0, a1, a2;
-      if constexpr (kPipe)
-        sell_row_product_pipe(a.A, s, lane, [&](int j) { return __ldcg(a.z + j); }, a0, a1, a2);
-      else
-        sell_row_product(a.A, s, lane, [&](int j) { return __ldcg(a.z + j); }, a0, a1, a2);
+      // own-row operands are loaded before the row product so that their latency overlaps it
+      const bool first = st[le].first != 0;
       const float4 zr = a.z[row];
-      float pn[3], qn[3];
-      if (st[le].first) {
-        pn[0] = zr.x;
-        pn[1] = zr.y;
-        pn[2] = zr.z;
-        qn[0] = a0;
-        qn[1] = a1;
-        qn[2] = a2;
-      } else {
-        const float beta = (float)st[le].beta;
-        pn[0] = fmaf(beta, a.p[3 * row], zr.x);
-        pn[1] = fmaf(beta, a.p[3 * row + 1], zr.y);
-        pn[2] = fmaf(beta, a.p[3 * row + 2], zr.z);
-        qn[0] = fmaf(beta, a.q[3 * row], a0);
-        qn[1] = fmaf(beta, a.q[3 * row + 1], a1);
-        qn[2] = fmaf(beta, a.q[3 * row + 2], a2);
+      float po[3] = {0.0f, 0.0f, 0.0f}, qo[3] = {0.0f, 0.0f, 0.0f};
+      if (!first) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          po[k] = a.p[3 * row + k];
+          qo[k] = a.q[3 * row + k];
+        }
       }
+      float a0, a1, a2;
+      // z gathers are weak L1-cacheable loads: z was last written before the grid barrier, whose acquire
+      // fence (thread 0, then __syncthreads) orders every thread of the CTA after those writes, as with
+      // cooperative-groups grid.sync(); neighbour rows of the same slice then hit in L1
+      if constexpr (kPipe)
+        sell_row_product_pipe(a.A, s, lane, [&](int j) { return a.z[j]; }, a0, a1, a2);
+      else
+        sell_row_product(a.A, s, lane, [&](int j) { return a.z[j]; }, a0, a1, a2);
+      const float beta = first ? 0.0f : (float)st[le].beta;
+      float pn[3], qn[3];
+      pn[0] = fmaf(beta, po[0], zr.x);
+      pn[1] = fmaf(beta, po[1], zr.y);
+      pn[2] = fmaf(beta, po[2], zr.z);
+      qn[0] = fmaf(beta, qo[0], a0);
+      qn[1] = fmaf(beta, qo[1], a1);
+      qn[2] = fmaf(beta, qo[2], a2);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         a.p[3 * row + k] = pn[k];
         a.q[3 * row + k] = qn[k];
       }
-      add_acc(le, 0, (double)pn[0] * qn[0] + (double)pn[1] * qn[1] + (double)pn[2] * qn[2]);
+      acc_add(le, 0, (double)pn[0] * qn[0] + (double)pn[1] * qn[1] + (double)pn[2] * qn[2]);
     }
+    acc_end(1);
     flush_acc(1, 1);
     if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
     if (threadIdx.x == 0) {
@@ -957,24 +989,42 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
       const int le = a.A.slice_env[s] - e0;
       if (st[le].status != 0) continue;
       const int64_t row = (int64_t)s * kSlice + lane;
+      // every operand load is issued before the first store (the row update is latency bound, operands
+      // in L2)
+      double xo[3], ro[3];
+      float pp[3], qq[3], dd[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        xo[k] = a.x[3 * row + k];
+        pp[k] = a.p[3 * row + k];
+        ro[k] = a.r[3 * row + k];
+        qq[k] = a.q[3 * row + k];
+        dd[k] = (!replace && a.precond == 1) ? a.dinv[3 * row + k] : 1.0f;
+      }
+      const float4 zo = replace ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : a.z[row];
       const double al = st[le].alpha;
       double r[3];
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        a.x[3 * row + k] += al * (double)a.p[3 * row + k];
-        r[k] = a.r[3 * row + k] - al * (double)a.q[3 * row + k];
+        a.x[3 * row + k] = xo[k] + al * (double)pp[k];
+        r[k] = ro[k] - al * (double)qq[k];
       }
       if (replace) continue;
-      const float4 zo = a.z[row];
       float z[3];
-      prec_apply(a, row, r, z);
+      if (a.precond == 1) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) z[k] = (float)(dd[k] * r[k]);
+      } else {
+        prec_apply(a, row, r, z);
+      }
 #pragma unroll
       for (int k = 0; k < 3; ++k) a.r[3 * row + k] = r[k];
       a.z[row] = make_float4(z[0], z[1], z[2], 0.0f);
-      add_acc(le, 0, r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-      add_acc(le, 1, r[0] * zo.x + r[1] * zo.y + r[2] * zo.z);
-      add_acc(le, 2, r[0] * z[0] + r[1] * z[1] + r[2] * z[2]);
+      acc_add(le, 0, r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+      acc_add(le, 1, r[0] * zo.x + r[1] * zo.y + r[2] * zo.z);
+      acc_add(le, 2, r[0] * z[0] + r[1] * z[1] + r[2] * z[2]);
     }
+    acc_end(3);
     if (replace) {
       if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
       for (int s = s0 + warp; s < s1; s += nwarps) {
@@ -989,10 +1039,11 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) a.r[3 * row + k] = r[k];
         a.z[row] = make_float4(z[0], z[1], z[2], 0.0f);
-        add_acc(le, 0, r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-        add_acc(le, 1, r[0] * zo.x + r[1] * zo.y + r[2] * zo.z);
-        add_acc(le, 2, r[0] * z[0] + r[1] * z[1] + r[2] * z[2]);
+        acc_add(le, 0, r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+        acc_add(le, 1, r[0] * zo.x + r[1] * zo.y + r[2] * zo.z);
+        acc_add(le, 2, r[0] * z[0] + r[1] * z[1] + r[2] * z[2]);
       }
+      acc_end(3);
     }
     flush_acc(3, 0);
     if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
