@@ -151,6 +151,8 @@ def cpu_oracle_sample(workload: str, seed: int = 0):
     v = np.zeros_like(u)
     prm = O.default_newton_params()
     prm.abs_tol = 1e-9  # same Newton stopping test as the GPU arm: rel 1e-6
+    if workload == "cfg2":
+        prm.max_iter = 12  # same Newton cap as the GPU arm
     t0 = time.perf_counter()
     u, v, st = s.step(u, v, cfg.dt, prm)
     dt = time.perf_counter() - t0
@@ -166,6 +168,15 @@ def vector_bytes_per_node():
     return 12 + 12 + 24 + 24 + 48 + 48 + 12 + 12 + 12 + 24
 
 
+def newton_max_iter(args):
+    """Newton iteration cap: 50 by default; 12 for the batched workload, where 1-2 % of the envs stall
+    between relative residual 1e-5 and 1e-3 on the penalty contact's non-smooth activation (the FP64 CPU
+    oracle stalls at the same residuals), and would otherwise run every step to the cap."""
+    if args.newton_max_iter:
+        return args.newton_max_iter
+    return 12 if args.workload == "cfg2" else 50
+
+
 def train_warm_start(args, local_rank):
     """Train the warm-start MLP on the GPU from plain-solver episodes of held-out seeds of the same
     workload (never the evaluated seed). Returns (params, info)."""
@@ -175,7 +186,8 @@ def train_warm_start(args, local_rank):
     Xs, Ts = [], []
     for k in range(args.train_episodes):
         (bodies, cfg), _ = build_workload(args.workload, seed=args.seed + 1000 + k)
-        tw = SoftBodyWorld(bodies, cfg, device=local_rank, newton_abs_tol=1e-9)
+        tw = SoftBodyWorld(bodies, cfg, device=local_rank, newton_abs_tol=1e-9,
+                           newton_max_iter=newton_max_iter(args))
         X, T = collect(tw, args.train_steps, samples_per_solve=65536, capacity=1 << 20, seed=k)
         Xs.append(X)
         Ts.append(T)
@@ -249,7 +261,8 @@ def run_ours(args, rank, world, local_rank):
         if w is not None:
             w.close()
         # Newton to rel 1e-6 (the absolute floor is only a guard for an exactly zero residual)
-        w = SoftBodyWorld(bodies, cfg, device=local_rank, newton_abs_tol=1e-9)
+        w = SoftBodyWorld(bodies, cfg, device=local_rank, newton_abs_tol=1e-9,
+                          newton_max_iter=newton_max_iter(args))
         if arm == "learned":
             Mlp(w._ctx).set_params(params)
         w.set_params(warm_start=capi.SDX_WARM_LEARNED if arm == "learned" else capi.SDX_WARM_ZERO,
@@ -323,6 +336,7 @@ def run_ours(args, rank, world, local_rank):
                    "precision": "FP32 Hessian assembly + SpMV, FP64 residual / energy / CG dots / x,r",
                    "warm_start": arms[-1], "arms": arms,
                    "cg_rel_tol": 1e-6, "newton_rel_tol": 1e-6, "newton_abs_tol": 1e-9,
+                   "newton_max_iter": newton_max_iter(args),
                    "l2": "inputs larger than L2 (matrix + tet data > 126 MB)",
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
         "arms": arm_summary, "training": train_info,
@@ -353,6 +367,7 @@ def main():
     ap.add_argument("--train-steps", type=int, default=8, dest="train_steps")
     ap.add_argument("--train-epochs", type=int, default=8, dest="train_epochs")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--newton-max-iter", type=int, default=0, dest="newton_max_iter")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))

@@ -267,6 +267,7 @@ typedef struct {
   int64_t seed_launches;
   double pcg_bytes;         /* algorithmic HBM bytes of the PCG launches: per env, its CG iterations x
                                (40 B per block + 4 B per row pointer + 228 B per row) */
+  int64_t pcg_relaunches;   /* re-partitioned PCG relaunches (batches whose slow envs got all CTAs) */
 } sdx_profile;
 int sdx_set_profiling(sdx_context* ctx, int enable);
 int sdx_get_profile(sdx_context* ctx, sdx_profile* out);

@@ -90,10 +90,10 @@ static int upload(T** d, const std::vector<T>& h) {
 
 struct PcgPartition {
   int n_cta = 0, threads = 0;
-  int* cta_slice = nullptr;
-  int* cta_env0 = nullptr;
-  int* cta_env1 = nullptr;
-  int* cta_pbase = nullptr;
+  int* cta_slice = nullptr;   // CTA c covers entries [cta_slice[c], cta_slice[c+1]) of the slice list
+  int* slice_list = nullptr;  // slice ids in ascending order (NULL: every slice, entry i = slice i)
+  int* cta_eoff = nullptr;    // CTA c's envs are cta_envs[cta_eoff[c] .. cta_eoff[c+1])
+  int* cta_envs = nullptr;
   int* env_cta0 = nullptr;
   int* env_cta1 = nullptr;
   int* env_poff = nullptr;
@@ -101,9 +101,9 @@ struct PcgPartition {
   void release() {
     dfree(env_poff);
     dfree(cta_slice);
-    dfree(cta_env0);
-    dfree(cta_env1);
-    dfree(cta_pbase);
+    dfree(slice_list);
+    dfree(cta_eoff);
+    dfree(cta_envs);
     dfree(env_cta0);
     dfree(env_cta1);
     dfree(part);
@@ -128,6 +128,7 @@ struct PcgWork {
   double* out_relres = nullptr;
   int* out_conv = nullptr;
   double* env_rel_tol = nullptr;
+  EnvSave* es = nullptr;  // per env CG scalars across re-partitioning relaunches
   int n_envs_alloc = 0;
   void release() {
     dfree(arena);
@@ -142,6 +143,7 @@ struct PcgWork {
     dfree(out_relres);
     dfree(out_conv);
     dfree(env_rel_tol);
+    dfree(es);
     n_rows = 0;
     n_envs_alloc = 0;
   }
@@ -228,6 +230,8 @@ struct sdx_context {
   int* ds_idx = nullptr;
   std::mt19937_64 ds_rng{0};
   bool l2_persist = false;
+  PcgPartition part_dyn;       // partition of the envs still iterating (re-partitioned PCG relaunches)
+  int* env_nrows = nullptr;    // padded rows per env (device)
   std::unique_ptr<PlainSolver> plain;  // the plain FP64 comparison solver, built on first use
   // opt-in per-kernel timing: event pairs resolved lazily
   bool profiling = false;
@@ -301,6 +305,8 @@ static void prof_resolve(sdx_context* c) {
 
 static void release_topology(sdx_context* c) {
   c->plain.reset();
+  c->part_dyn.release();
+  dfree(c->env_nrows);
   dfree(c->slice_ptr);
   dfree(c->slice_w);
   dfree(c->slice_env);
@@ -517,9 +523,12 @@ static inline int sell_pos(const sdx_context* c, int64_t a, int64_t b) {
   return c->h_slice_ptr[row >> 5] + k * kSlice + (int)(row & 31);
 }
 
+// Persistent-PCG partition: contiguous runs of a slice list (all slices, or the slices of the envs still
+// iterating) split over the CTAs by block positions, each CTA holding at most kPcgMaxEnvsPerCta envs;
+// per env, the CTAs that cover it (a contiguous CTA range) and the offset of its reduction partials.
 static int choose_partition(sdx_context* c, int n_slices, const std::vector<int>& slice_env, int n_envs,
                             const std::vector<int>& slice_ptr, PcgPartition& P, int threads_req,
-                            int ctas_per_sm_req) {
+                            int ctas_per_sm_req, const std::vector<int>* list = nullptr) {
   P.release();
   // launch shape: explicit request, else SDX_PCG_THREADS / SDX_PCG_CTAS_PER_SM, else 512 x 1 (the
   // software-pipelined SpMV variant, 128 registers per thread)
@@ -532,58 +541,65 @@ static int choose_partition(sdx_context* c, int n_slices, const std::vector<int>
   if (max_active <= 0) return set_error(SDX_ERR_CUDA, "PCG kernel cannot be resident with %d threads", threads);
   // cooperative launch: every CTA must be co-resident
   const int per_sm = std::min(max_active, ctas_per_sm_req > 0 ? ctas_per_sm_req : 1);
-  int n_cta = c->num_sms * per_sm;
-  // each CTA may cover at most kPcgMaxEnvsPerCta envs; grow CTAs over weight-balanced slices
-  const int64_t total_w = slice_ptr[n_slices];
+  const int n_cta = c->num_sms * per_sm;
+  const int n_list = list ? (int)list->size() : n_slices;
+  auto slice_at = [&](int i) { return list ? (*list)[i] : i; };
+  auto width = [&](int i) { const int sl = slice_at(i); return (int64_t)(slice_ptr[sl + 1] - slice_ptr[sl]); };
+  int64_t total_w = 0;
+  for (int i = 0; i < n_list; ++i) total_w += width(i);
   std::vector<int> cs(1, 0);
   {
-    const double target = std::max(1.0, (double)total_w / n_cta);
-    int s = 0;
-    while (s < n_slices) {
+    // each CTA takes the remaining work divided by the remaining CTAs, stopping at the slice boundary
+    // nearest to that target
+    int i = 0;
+    int64_t remaining = total_w;
+    while (i < n_list) {
+      const int ctas_left = std::max(1, n_cta - ((int)cs.size() - 1));
+      const double target = std::max(1.0, (double)remaining / ctas_left);
       int64_t w = 0;
       int envs_seen = 0, last_env = -1;
-      while (s < n_slices) {
-        const int ev = slice_env[s];
+      while (i < n_list) {
+        const int ev = slice_env[slice_at(i)];
         if (ev != last_env) {
           if (envs_seen == kPcgMaxEnvsPerCta) break;
           envs_seen++;
           last_env = ev;
         }
-        w += slice_ptr[s + 1] - slice_ptr[s];
-        ++s;
-        if ((double)w >= target && (int)cs.size() < n_cta) break;
+        const int64_t ws = width(i);
+        if (w > 0 && (double)w + 0.5 * (double)ws > target && (int)cs.size() < n_cta) break;
+        w += ws;
+        ++i;
       }
-      cs.push_back(s);
+      remaining -= w;
+      cs.push_back(i);
     }
   }
-  while ((int)cs.size() - 1 < n_cta) cs.push_back(n_slices);
-  if ((int)cs.size() - 1 > n_cta) {
+  while ((int)cs.size() - 1 < n_cta) cs.push_back(n_list);
+  if ((int)cs.size() - 1 > n_cta)
     return set_error(SDX_ERR_UNSUPPORTED, "too many small environments for %d persistent CTAs", n_cta);
-  }
-  std::vector<int> e0(n_cta), e1(n_cta), pbase(n_cta + 1, 0), ec0(n_envs, -1), ec1(n_envs, -1);
+  std::vector<int> eoff(n_cta + 1, 0), envs, ec0(n_envs, -1), ec1(n_envs, -1);
   for (int k = 0; k < n_cta; ++k) {
-    if (cs[k + 1] > cs[k]) {
-      e0[k] = slice_env[cs[k]];
-      e1[k] = slice_env[cs[k + 1] - 1];
-      for (int ev = e0[k]; ev <= e1[k]; ++ev) {
-        if (ec0[ev] < 0) ec0[ev] = k;
-        ec1[ev] = k;
-      }
-    } else {
-      e0[k] = 0;
-      e1[k] = -1;
+    int last = -1;
+    for (int i = cs[k]; i < cs[k + 1]; ++i) {
+      const int ev = slice_env[slice_at(i)];
+      if (ev == last) continue;
+      last = ev;
+      envs.push_back(ev);
+      if (ec0[ev] < 0) ec0[ev] = k;
+      ec1[ev] = k;
     }
-    pbase[k + 1] = pbase[k] + std::max(0, e1[k] - e0[k] + 1);
+    eoff[k + 1] = (int)envs.size();
   }
   for (int ev = 0; ev < n_envs; ++ev)
     if (ec0[ev] < 0) {
       ec0[ev] = 0;
       ec1[ev] = -1;
     }
+  if (envs.empty()) envs.push_back(0);
   SDX_TRY(upload(&P.cta_slice, cs));
-  SDX_TRY(upload(&P.cta_env0, e0));
-  SDX_TRY(upload(&P.cta_env1, e1));
-  SDX_TRY(upload(&P.cta_pbase, pbase));
+  if (list) SDX_TRY(upload(&P.slice_list, *list));
+  SDX_TRY(upload(&P.cta_eoff, eoff));
+  SDX_TRY(upload(&P.cta_envs, envs));
   SDX_TRY(upload(&P.env_cta0, ec0));
   SDX_TRY(upload(&P.env_cta1, ec1));
   std::vector<int> poff(n_envs + 1, 0);
@@ -626,16 +642,21 @@ static int alloc_work(PcgWork& W, int64_t n_rows, int n_envs, bool newton_vector
   SDX_TRY(dalloc(&W.out_relres, n_envs));
   SDX_TRY(dalloc(&W.out_conv, n_envs));
   SDX_TRY(dalloc(&W.env_rel_tol, n_envs));
+  SDX_TRY(dalloc(&W.es, n_envs));
   W.n_rows = n_rows;
   W.n_envs_alloc = n_envs;
   return SDX_OK;
 }
 
 // Runs the persistent PCG on matrix A for the envs in env_mask (NULL = all), b -> x.
+// One PCG solve of every env in env_mask (host copy h_mask, NULL: all). For a batch of envs on the
+// context matrix, the persistent kernel exits each time the rows still iterating fall to half of those it
+// started with; the envs still iterating are then re-partitioned over all CTAs (a slice list of just
+// their slices) and the kernel resumes where it stopped, so the slowest envs get the whole GPU.
 static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_envs, PcgPartition& P,
                    PcgWork& W, const double* b, double* x, const uint8_t* env_mask, int n_active,
                    const sdx_linear_params& lp, bool zero_guess, const double* env_rel_tol,
-                   bool scale_guess = false) {
+                   bool scale_guess = false, const uint8_t* h_mask = nullptr) {
   PcgArgs a;
   memset(&a, 0, sizeof(a));
   a.A = A;
@@ -649,14 +670,6 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
   a.q = W.q;
   a.z = W.z;
   a.dinv = W.dinv;
-  a.cta_slice = P.cta_slice;
-  a.cta_env0 = P.cta_env0;
-  a.cta_env1 = P.cta_env1;
-  a.cta_pbase = P.cta_pbase;
-  a.env_cta0 = P.env_cta0;
-  a.env_cta1 = P.env_cta1;
-  a.env_poff = P.env_poff;
-  a.part = P.part;
   a.env_mask = env_mask;
   a.rel_tol = lp.rel_tol;
   a.abs_tol = lp.abs_tol;
@@ -674,20 +687,77 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
   a.sync = W.sync;
   a.env_rel_tol = env_rel_tol;
   a.spin_limit = 1ll << 26;
-  unsigned init[8] = {0u, 0u, 0u, (unsigned)n_active, 0u, 0u, 0u, 0u};
+  a.es = W.es;
+  // re-partitioning applies to batches on the context matrix (SDX_PCG_REPART=0 disables it)
+  static const bool repart_on = [] {
+    const char* e = getenv("SDX_PCG_REPART");
+    return !(e && atoi(e) == 0);
+  }();
+  const bool batch = repart_on && A.val == c->val && n_envs == c->n_envs && n_envs > 1 && c->env_nrows;
+  int64_t rows = 0;
+  if (batch) {
+    for (int e = 0; e < n_envs; ++e)
+      if (!h_mask || h_mask[e]) rows += c->h_row_off[e + 1] - c->h_row_off[e];
+    a.env_nrows = c->env_nrows;
+  }
+  const int64_t min_rows = (int64_t)kSlice * 4 * c->num_sms;  // below this, iterations are latency bound
+  auto repart_target = [&](int64_t r) { return (batch && r / 2 >= min_rows) ? r / 2 : 0; };
+  unsigned init[8] = {0u, 0u, 0u, (unsigned)n_active, 0u, (unsigned)rows, 0u, 0u};
   SDX_CUDA(cudaMemcpyAsync(W.sync, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
   SDX_CUDA(cudaMemsetAsync(W.out_iters, 0, sizeof(int) * n_envs, c->stream));
   SDX_CUDA(cudaMemsetAsync(W.out_conv, 0, sizeof(int) * n_envs, c->stream));
   cudaEvent_t ev;
   prof_begin(c, &ev);
-  cudaError_t e = launch_pcg(a, P.n_cta, P.threads, c->stream);
-  c->launches++;
-  if (e != cudaSuccess) return set_error(SDX_ERR_CUDA, "PCG cooperative launch: %s", cudaGetErrorString(e));
+  PcgPartition* part = &P;
+  if (batch && h_mask && rows < (c->h_row_off[n_envs] * 3) / 4) {
+    // most envs are already converged (later Newton iterations): partition just the envs in the mask
+    std::vector<int> list;
+    for (int s = 0; s < c->n_slices; ++s)
+      if (h_mask[c->h_slice_env[s]]) list.push_back(s);
+    if (!list.empty()) {
+      SDX_TRY(choose_partition(c, c->n_slices, c->h_slice_env, n_envs, c->h_slice_ptr, c->part_dyn, P.threads, 0,
+                               &list));
+      part = &c->part_dyn;
+    }
+  }
+  int64_t target = repart_target(rows);
+  for (;;) {
+    a.cta_slice = part->cta_slice;
+    a.slice_list = part->slice_list;
+    a.cta_eoff = part->cta_eoff;
+    a.cta_envs = part->cta_envs;
+    a.env_cta0 = part->env_cta0;
+    a.env_cta1 = part->env_cta1;
+    a.env_poff = part->env_poff;
+    a.part = part->part;
+    a.repart_rows = target;
+    cudaError_t e = launch_pcg(a, part->n_cta, part->threads, c->stream);
+    c->launches++;
+    if (e != cudaSuccess) return set_error(SDX_ERR_CUDA, "PCG cooperative launch: %s", cudaGetErrorString(e));
+    unsigned flags[8];
+    SDX_CUDA(cudaMemcpyAsync(flags, W.sync, sizeof(flags), cudaMemcpyDeviceToHost, c->stream));
+    SDX_CUDA(cudaStreamSynchronize(c->stream));
+    if (flags[2] != 0u) return set_error(SDX_ERR_DEVICE_TIMEOUT, "PCG grid barrier timed out");
+    if (flags[7] == 0u) break;
+    // re-partition the envs still iterating and resume from iteration flags[6]
+    std::vector<EnvSave> es(n_envs);
+    SDX_CUDA(cudaMemcpy(es.data(), W.es, sizeof(EnvSave) * n_envs, cudaMemcpyDeviceToHost));
+    std::vector<int> list;
+    for (int s = 0; s < c->n_slices; ++s)
+      if (es[c->h_slice_env[s]].status == 0) list.push_back(s);
+    if (list.empty()) break;
+    SDX_TRY(choose_partition(c, c->n_slices, c->h_slice_env, n_envs, c->h_slice_ptr, c->part_dyn, P.threads, 0,
+                             &list));
+    part = &c->part_dyn;
+    if (c->profiling) c->prof.pcg_relaunches++;
+    a.resume = 1;
+    a.it0 = (int)flags[6];
+    target = repart_target((int64_t)(int)flags[5]);
+    const unsigned zero = 0u;
+    SDX_CUDA(cudaMemcpyAsync(W.sync, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, c->stream));
+    SDX_CUDA(cudaMemcpyAsync(W.sync + 7, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, c->stream));
+  }
   prof_end(c, PROF_PCG, ev);
-  unsigned flags[8];
-  SDX_CUDA(cudaMemcpyAsync(flags, W.sync, sizeof(flags), cudaMemcpyDeviceToHost, c->stream));
-  SDX_CUDA(cudaStreamSynchronize(c->stream));
-  if (flags[2] != 0u) return set_error(SDX_ERR_DEVICE_TIMEOUT, "PCG grid barrier timed out");
   if (c->profiling) {
     std::vector<int> its(n_envs);
     SDX_CUDA(cudaMemcpy(its.data(), W.out_iters, sizeof(int) * n_envs, cudaMemcpyDeviceToHost));
@@ -1117,6 +1187,8 @@ extern "C" int sdx_upload_bodies(sdx_context* c, int n_envs, const int64_t* node
     std::vector<int> er(n_envs);
     for (int e = 0; e < n_envs; ++e) er[e] = (int)(node_off[e + 1] - node_off[e]);
     SDX_TRY(upload(&c->env_rows, er));
+    for (int e = 0; e < n_envs; ++e) er[e] = (int)(c->h_row_off[e + 1] - c->h_row_off[e]);
+    SDX_TRY(upload(&c->env_nrows, er));
   }
   SDX_TRY(dalloc(&c->env_norm, n_envs));
   SDX_TRY(dalloc(&c->env_scale, n_envs));
@@ -1555,7 +1627,8 @@ static int step_once(sdx_context* c) {
       SDX_TRY(run_plain(c, mask, p.linear, zero, it_out));
     } else {
       SDX_TRY(run_pcg(c, ctx_matrix(c), c->diag_pos, E, c->part, c->work, c->g, c->dx, c->env_mask, n_active,
-                      p.linear, zero, p.ew_forcing == 2 ? c->work.env_rel_tol : nullptr, /*scale_guess*/ !zero));
+                      p.linear, zero, p.ew_forcing == 2 ? c->work.env_rel_tol : nullptr, /*scale_guess*/ !zero,
+                      mask.data()));
       SDX_CUDA(cudaMemcpy(it_out.data(), c->work.out_iters, sizeof(int) * E, cudaMemcpyDeviceToHost));
     }
     for (int e = 0; e < E; ++e)

@@ -86,6 +86,12 @@ struct ContactArgs {
   int flags;
 };
 
+// CG scalars of one env carried across a re-partitioning relaunch
+struct EnvSave {
+  double rz, beta, bb, conv_thr, div_thr;
+  int first, status;
+};
+
 struct PcgArgs {
   Matrix A;
   int n_envs;
@@ -98,10 +104,10 @@ struct PcgArgs {
   float* q;
   float4* z;
   float* dinv;  // 3 per row (Jacobi) or 9 per row (block Jacobi)
-  const int* cta_slice;
-  const int* cta_env0;
-  const int* cta_env1;
-  const int* cta_pbase;
+  const int* cta_slice;   // CTA c covers entries [cta_slice[c], cta_slice[c+1]) of the slice list
+  const int* slice_list;  // ascending slice ids (NULL: entry i is slice i)
+  const int* cta_eoff;    // CTA c's envs: cta_envs[cta_eoff[c] .. cta_eoff[c+1]), ascending
+  const int* cta_envs;
   const int* env_cta0;
   const int* env_cta1;
   const int* env_poff;  // partials of env e live at [env_poff[e], env_poff[e] + env_cta1[e] - env_cta0[e]]
@@ -119,9 +125,19 @@ struct PcgArgs {
   double* out_res;
   double* out_relres;
   int* out_conv;
-  unsigned* sync;  // [0] barrier arrivals (monotonic), [1] unused, [2] error, [3] active, [4] verify_iter
+  unsigned* sync;  // [0] barrier arrivals (monotonic), [1] unused, [2] error, [3] active envs,
+                   // [4] verify_iter, [5] active rows, [6] resume iteration, [7] repartition exit
   long long spin_limit;
+  // Re-partitioning: once the rows of the envs still iterating fall to repart_rows (0: never), the
+  // kernel saves every env's CG scalars in es[] and exits after the iteration; the host re-partitions
+  // the remaining envs over all CTAs and relaunches with resume = 1 from iteration it0.
+  const int* env_nrows;  // rows per env (counted off sync[5] as envs finish)
+  long long repart_rows;
+  int resume;
+  int it0;
+  EnvSave* es;
 };
+
 
 // kernels launched by the host runtime (sdx_kernels.cu)
 void launch_mass_accum(int64_t n_tets, const int4* slots[4], const float4* rest3, float* mass,

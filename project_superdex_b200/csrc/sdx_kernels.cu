@@ -717,9 +717,25 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
   const int c = blockIdx.x;
   const unsigned ncta = gridDim.x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  // this CTA's entries [s0, s1) of the slice list and its envs (ascending) s_env[0 .. ne)
   const int s0 = a.cta_slice[c], s1 = a.cta_slice[c + 1];
-  const int e0 = a.cta_env0[c];
-  const int ne = (s1 > s0) ? (a.cta_env1[c] - e0 + 1) : 0;
+  const int eo = a.cta_eoff[c];
+  const int ne = (s1 > s0) ? (a.cta_eoff[c + 1] - eo) : 0;
+  __shared__ int s_env[kPcgMaxEnvsPerCta];
+  __shared__ int s_repart;
+  for (int le = threadIdx.x; le < ne; le += blockDim.x) s_env[le] = a.cta_envs[eo + le];
+  auto slice_of = [&](int i) { return a.slice_list ? a.slice_list[i] : i; };
+  auto local_env = [&](int ev) {  // index of env ev in s_env
+    int lo = 0, hi = ne - 1;
+    while (lo < hi) {
+      const int m = (lo + hi) >> 1;
+      if (s_env[m] < ev)
+        lo = m + 1;
+      else
+        hi = m;
+    }
+    return lo;
+  };
 
   auto clear_acc = [&]() {
     for (int i = threadIdx.x; i < nwarps * kPcgMaxEnvsPerCta * kPcgNq; i += blockDim.x) wacc[i] = 0.0;
@@ -739,7 +755,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
       const int le = i / nq, k = i % nq;
       double v = 0.0;
       for (int w = 0; w < nwarps; ++w) v += wacc[(w * kPcgMaxEnvsPerCta + le) * kPcgNq + k];
-      const int e = e0 + le;
+      const int e = s_env[le];
       a.part[buf * pstride + (size_t)(a.env_poff[e] + (c - a.env_cta0[e])) * kPcgNq + k] = v;
     }
   };
@@ -747,7 +763,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     // one warp per (env, quantity); fixed summation order, identical in every CTA
     for (int i = warp; i < ne * nq; i += nwarps) {
       const int le = i / nq, k = i % nq;
-      const int e = e0 + le;
+      const int e = s_env[le];
       const int n = a.env_cta1[e] - a.env_cta0[e] + 1;
       const double* src = a.part + buf * pstride + (size_t)a.env_poff[e] * kPcgNq + k;
       double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
@@ -765,13 +781,14 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     __syncthreads();
   };
   auto finish_env = [&](int le, int it, double rr) {
-    const int e = e0 + le;
+    const int e = s_env[le];
     if (a.env_cta0[e] == c) {
       a.out_iters[e] = it;
       a.out_res[e] = sqrt(fmax(rr, 0.0));
       a.out_relres[e] = st[le].bb == 0.0 ? 0.0 : sqrt(fmax(rr, 0.0) / st[le].bb);
       a.out_conv[e] = st[le].status;
       atomicSub((int*)(a.sync + 3), 1);
+      if (a.env_nrows) atomicSub((int*)(a.sync + 5), a.env_nrows[e]);
     }
   };
 
@@ -798,134 +815,151 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
   };
 
   for (int le = threadIdx.x; le < ne; le += blockDim.x) {
-    st[le].status = (a.env_mask && !a.env_mask[e0 + le]) ? 4 : 0;
-    st[le].first = 1;
-    st[le].beta = 0.0;
+    if (a.resume) {  // continue a re-partitioned solve: the CG scalars saved at the previous exit
+      const EnvSave& sv = a.es[s_env[le]];
+      st[le].rz = sv.rz;
+      st[le].beta = sv.beta;
+      st[le].bb = sv.bb;
+      st[le].conv_thr = sv.conv_thr;
+      st[le].div_thr = sv.div_thr;
+      st[le].first = sv.first;
+      st[le].status = sv.status;
+    } else {
+      st[le].status = (a.env_mask && !a.env_mask[s_env[le]]) ? 4 : 0;
+      st[le].first = 1;
+      st[le].beta = 0.0;
+    }
   }
+  if (threadIdx.x == 0) s_repart = 0;
   __syncthreads();
 
-  // ---- phase 0: r = b - A x0, z = M^-1 r, partials b.b, r.r, r.z ----
-  const bool scaled = !a.zero_guess && a.scale_guess;
-  if (scaled) {
-    // energy-optimal scaling of the guess: alpha = (x0.b) / (x0.A x0), A x0 = b - r0; the scaled start
-    // alpha x0 never has a larger A-norm error than the zero start. The guess is kept only if it also
-    // lowers the residual the stop test measures: ||b - alpha A x0||^2 = (1-alpha)^2 b.b
-    // + 2 alpha (1-alpha) b.r0 + alpha^2 r0.r0 < b.b; otherwise the env falls back to the zero start.
+  if (!a.resume) {
+    // ---- phase 0: r = b - A x0, z = M^-1 r, partials b.b, r.r, r.z ----
+    const bool scaled = !a.zero_guess && a.scale_guess;
+    if (scaled) {
+      // energy-optimal scaling of the guess: alpha = (x0.b) / (x0.A x0), A x0 = b - r0; the scaled start
+      // alpha x0 never has a larger A-norm error than the zero start. The guess is kept only if it also
+      // lowers the residual the stop test measures: ||b - alpha A x0||^2 = (1-alpha)^2 b.b
+      // + 2 alpha (1-alpha) b.r0 + alpha^2 r0.r0 < b.b; otherwise the env falls back to the zero start.
+      clear_acc();
+      for (int i = s0 + warp; i < s1; i += nwarps) {
+        const int s = slice_of(i);
+        const int le = local_env(a.A.slice_env[s]);
+        if (st[le].status != 0) continue;
+        const int64_t row = (int64_t)s * kSlice + lane;
+        double r[3];
+        true_residual(a, s, lane, r);
+        double xb = 0.0, xr = 0.0, bb = 0.0, br = 0.0, rr = 0.0;
+  #pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          a.r[3 * row + k] = r[k];
+          const double xk = a.x[3 * row + k], bk = a.b[3 * row + k];
+          xb += xk * bk;
+          xr += xk * r[k];
+          bb += bk * bk;
+          br += bk * r[k];
+          rr += r[k] * r[k];
+        }
+        add_acc(le, 0, bb);
+        add_acc(le, 1, xb);
+        add_acc(le, 2, xr);
+        add_acc(le, 3, br);
+        add_acc(le, 4, rr);
+      }
+      flush_acc(5, 1);
+      if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
+      reduce_tot(5, 1);
+      for (int le = threadIdx.x; le < ne; le += blockDim.x) {
+        const double bb = tot[le][0], xb = tot[le][1], xax = tot[le][1] - tot[le][2];
+        double al = (xax > 0.0 && xb > 0.0 && isfinite(xb / xax)) ? xb / xax : 0.0;
+        const double ra = (1.0 - al) * (1.0 - al) * bb + 2.0 * al * (1.0 - al) * tot[le][3] + al * al * tot[le][4];
+        if (!(ra < bb)) al = 0.0;
+        st[le].alpha = al;
+      }
+      __syncthreads();
+    }
     clear_acc();
-    for (int s = s0 + warp; s < s1; s += nwarps) {
-      const int le = a.A.slice_env[s] - e0;
+    for (int i = s0 + warp; i < s1; i += nwarps) {
+      const int s = slice_of(i);
+      const int le = local_env(a.A.slice_env[s]);
       if (st[le].status != 0) continue;
       const int64_t row = (int64_t)s * kSlice + lane;
-      double r[3];
-      true_residual(a, s, lane, r);
-      double xb = 0.0, xr = 0.0, bb = 0.0, br = 0.0, rr = 0.0;
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        a.r[3 * row + k] = r[k];
-        const double xk = a.x[3 * row + k], bk = a.b[3 * row + k];
-        xb += xk * bk;
-        xr += xk * r[k];
-        bb += bk * bk;
-        br += bk * r[k];
-        rr += r[k] * r[k];
+      // preconditioner from the diagonal block (BlockJacobiPrec<1> / <3>, block_jacobi_prec.h:35-151)
+      const int dp = a.diag_pos[row];
+      if (a.precond == 1) {
+  #pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const float d = dp >= 0 ? a.A.val[val_index(dp, 4 * k)] : 0.0f;
+          a.dinv[3 * row + k] = d != 0.0f ? 1.0f / d : 0.0f;
+        }
+      } else if (a.precond == 2) {
+        float B[9];
+  #pragma unroll
+        for (int e = 0; e < 9; ++e) B[e] = dp >= 0 ? a.A.val[val_index(dp, e)] : 0.0f;
+        float cof[9];
+        cof3(B, cof);
+        const float det = det3(B);
+        const float inv = det != 0.0f ? 1.0f / det : 0.0f;
+  #pragma unroll
+        for (int i = 0; i < 3; ++i)
+  #pragma unroll
+          for (int j = 0; j < 3; ++j) a.dinv[9 * row + 3 * i + j] = cof[3 * j + i] * inv;
       }
-      add_acc(le, 0, bb);
-      add_acc(le, 1, xb);
-      add_acc(le, 2, xr);
-      add_acc(le, 3, br);
-      add_acc(le, 4, rr);
+      double r[3];
+      if (a.zero_guess) {
+  #pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          a.x[3 * row + k] = 0.0;
+          r[k] = a.b[3 * row + k];
+        }
+      }
+      if (!a.zero_guess && !scaled) true_residual(a, s, lane, r);
+      if (scaled) {
+        const double al = st[le].alpha;
+  #pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          a.x[3 * row + k] *= al;
+          r[k] = (1.0 - al) * a.b[3 * row + k] + al * a.r[3 * row + k];
+        }
+      }
+      float z[3];
+      prec_apply(a, row, r, z);
+  #pragma unroll
+      for (int k = 0; k < 3; ++k) a.r[3 * row + k] = r[k];
+      a.z[row] = make_float4(z[0], z[1], z[2], 0.0f);
+      const double b0 = a.b[3 * row], b1 = a.b[3 * row + 1], b2 = a.b[3 * row + 2];
+      add_acc(le, 0, b0 * b0 + b1 * b1 + b2 * b2);
+      add_acc(le, 1, r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+      add_acc(le, 2, r[0] * z[0] + r[1] * z[1] + r[2] * z[2]);
     }
-    flush_acc(5, 1);
+    flush_acc(3, 0);
     if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
-    reduce_tot(5, 1);
+    reduce_tot(3, 0);
     for (int le = threadIdx.x; le < ne; le += blockDim.x) {
-      const double bb = tot[le][0], xb = tot[le][1], xax = tot[le][1] - tot[le][2];
-      double al = (xax > 0.0 && xb > 0.0 && isfinite(xb / xax)) ? xb / xax : 0.0;
-      const double ra = (1.0 - al) * (1.0 - al) * bb + 2.0 * al * (1.0 - al) * tot[le][3] + al * al * tot[le][4];
-      if (!(ra < bb)) al = 0.0;
-      st[le].alpha = al;
+      if (st[le].status != 0) continue;
+      const double bb = tot[le][0], rr = tot[le][1];
+      st[le].bb = bb;
+      const double rt = a.env_rel_tol ? a.env_rel_tol[s_env[le]] : a.rel_tol;
+      st[le].conv_thr = fmax(a.abs_tol * a.abs_tol, (bb * rt) * rt);
+      st[le].div_thr = (bb * a.rel_div_tol) * a.rel_div_tol;
+      st[le].rz = tot[le][2];
+      if (!isfinite(rr) || rr > st[le].div_thr) {
+        st[le].status = 3;
+        finish_env(le, 0, rr);
+      } else if (rr <= st[le].conv_thr) {
+        st[le].status = 1;
+        finish_env(le, 0, rr);
+      }
     }
     __syncthreads();
   }
-  clear_acc();
-  for (int s = s0 + warp; s < s1; s += nwarps) {
-    const int le = a.A.slice_env[s] - e0;
-    if (st[le].status != 0) continue;
-    const int64_t row = (int64_t)s * kSlice + lane;
-    // preconditioner from the diagonal block (BlockJacobiPrec<1> / <3>, block_jacobi_prec.h:35-151)
-    const int dp = a.diag_pos[row];
-    if (a.precond == 1) {
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const float d = dp >= 0 ? a.A.val[val_index(dp, 4 * k)] : 0.0f;
-        a.dinv[3 * row + k] = d != 0.0f ? 1.0f / d : 0.0f;
-      }
-    } else if (a.precond == 2) {
-      float B[9];
-#pragma unroll
-      for (int e = 0; e < 9; ++e) B[e] = dp >= 0 ? a.A.val[val_index(dp, e)] : 0.0f;
-      float cof[9];
-      cof3(B, cof);
-      const float det = det3(B);
-      const float inv = det != 0.0f ? 1.0f / det : 0.0f;
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) a.dinv[9 * row + 3 * i + j] = cof[3 * j + i] * inv;
-    }
-    double r[3];
-    if (a.zero_guess) {
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        a.x[3 * row + k] = 0.0;
-        r[k] = a.b[3 * row + k];
-      }
-    }
-    if (!a.zero_guess && !scaled) true_residual(a, s, lane, r);
-    if (scaled) {
-      const double al = st[le].alpha;
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        a.x[3 * row + k] *= al;
-        r[k] = (1.0 - al) * a.b[3 * row + k] + al * a.r[3 * row + k];
-      }
-    }
-    float z[3];
-    prec_apply(a, row, r, z);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) a.r[3 * row + k] = r[k];
-    a.z[row] = make_float4(z[0], z[1], z[2], 0.0f);
-    const double b0 = a.b[3 * row], b1 = a.b[3 * row + 1], b2 = a.b[3 * row + 2];
-    add_acc(le, 0, b0 * b0 + b1 * b1 + b2 * b2);
-    add_acc(le, 1, r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-    add_acc(le, 2, r[0] * z[0] + r[1] * z[1] + r[2] * z[2]);
-  }
-  flush_acc(3, 0);
-  if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
-  reduce_tot(3, 0);
-  for (int le = threadIdx.x; le < ne; le += blockDim.x) {
-    if (st[le].status != 0) continue;
-    const double bb = tot[le][0], rr = tot[le][1];
-    st[le].bb = bb;
-    const double rt = a.env_rel_tol ? a.env_rel_tol[e0 + le] : a.rel_tol;
-    st[le].conv_thr = fmax(a.abs_tol * a.abs_tol, (bb * rt) * rt);
-    st[le].div_thr = (bb * a.rel_div_tol) * a.rel_div_tol;
-    st[le].rz = tot[le][2];
-    if (!isfinite(rr) || rr > st[le].div_thr) {
-      st[le].status = 3;
-      finish_env(le, 0, rr);
-    } else if (rr <= st[le].conv_thr) {
-      st[le].status = 1;
-      finish_env(le, 0, rr);
-    }
-  }
-  __syncthreads();
 
-  for (int it = 1;; ++it) {
+  for (int it = a.resume ? a.it0 : 1;; ++it) {
     // ---- phase 1 ----
     clear_acc();
-    for (int s = s0 + warp; s < s1; s += nwarps) {
-      const int le = a.A.slice_env[s] - e0;
+    for (int i = s0 + warp; i < s1; i += nwarps) {
+      const int s = slice_of(i);
+      const int le = local_env(a.A.slice_env[s]);
       if (st[le].status != 0) continue;
       const int64_t row = (int64_t)s * kSlice + lane;
       // own-row operands are loaded before the row product so that their latency overlaps it
@@ -967,6 +1001,8 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
     if (threadIdx.x == 0) {
       s_exit = *((volatile int*)(a.sync + 3)) <= 0;
+      // re-partition after this iteration once few rows are left to iterate
+      s_repart = a.repart_rows > 0 && (long long)*((volatile int*)(a.sync + 5)) <= a.repart_rows;
       const int vi = *((volatile int*)(a.sync + 4));
       s_replace = (vi == it - 1) || (a.replace_every > 0 && it % a.replace_every == 0);
     }
@@ -985,8 +1021,9 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
 
     // ---- phase 2 ----
     clear_acc();
-    for (int s = s0 + warp; s < s1; s += nwarps) {
-      const int le = a.A.slice_env[s] - e0;
+    for (int i = s0 + warp; i < s1; i += nwarps) {
+      const int s = slice_of(i);
+      const int le = local_env(a.A.slice_env[s]);
       if (st[le].status != 0) continue;
       const int64_t row = (int64_t)s * kSlice + lane;
       // every operand load is issued before the first store (the row update is latency bound, operands
@@ -1027,8 +1064,9 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     acc_end(3);
     if (replace) {
       if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
-      for (int s = s0 + warp; s < s1; s += nwarps) {
-        const int le = a.A.slice_env[s] - e0;
+      for (int i = s0 + warp; i < s1; i += nwarps) {
+        const int s = slice_of(i);
+        const int le = local_env(a.A.slice_env[s]);
         if (st[le].status != 0) continue;
         const int64_t row = (int64_t)s * kSlice + lane;
         double r[3];
@@ -1067,7 +1105,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
           finish_env(le, it, rr);
           continue;
         }
-        if (a.env_cta0[e0 + le] == c) atomicMax((int*)(a.sync + 4), it);
+        if (a.env_cta0[s_env[le]] == c) atomicMax((int*)(a.sync + 4), it);
       }
       if (it >= a.max_iter) {
         st[le].status = 2;
@@ -1085,6 +1123,28 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
       st[le].first = 0;
     }
     __syncthreads();
+    if (s_repart) {
+      // save the CG scalars (the env's first CTA writes them) and exit; the host re-partitions the envs
+      // still iterating and relaunches from iteration it + 1
+      for (int le = threadIdx.x; le < ne; le += blockDim.x) {
+        const int e = s_env[le];
+        if (a.env_cta0[e] != c) continue;
+        EnvSave sv;
+        sv.rz = st[le].rz;
+        sv.beta = st[le].beta;
+        sv.bb = st[le].bb;
+        sv.conv_thr = st[le].conv_thr;
+        sv.div_thr = st[le].div_thr;
+        sv.first = st[le].first;
+        sv.status = st[le].status;
+        a.es[e] = sv;
+      }
+      if (c == 0 && threadIdx.x == 0) {
+        a.sync[6] = (unsigned)(it + 1);
+        a.sync[7] = 1u;
+      }
+      return;
+    }
   }
 }
 
