@@ -649,9 +649,12 @@ static int alloc_work(PcgWork& W, int64_t n_rows, int n_envs, bool newton_vector
 }
 
 // Runs the persistent PCG on matrix A for the envs in env_mask (NULL = all), b -> x.
+// share of the rows still iterating at which a batched PCG launch re-partitions
+constexpr double kPcgRepartRatio = 0.5;
+
 // One PCG solve of every env in env_mask (host copy h_mask, NULL: all). For a batch of envs on the
-// context matrix, the persistent kernel exits each time the rows still iterating fall to half of those it
-// started with; the envs still iterating are then re-partitioned over all CTAs (a slice list of just
+// context matrix, the persistent kernel exits each time the rows still iterating fall to a share
+// (kPcgRepartRatio) of those it started with; the envs still iterating are then re-partitioned over all CTAs (a slice list of just
 // their slices) and the kernel resumes where it stopped, so the slowest envs get the whole GPU.
 static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_envs, PcgPartition& P,
                    PcgWork& W, const double* b, double* x, const uint8_t* env_mask, int n_active,
@@ -701,7 +704,15 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
     a.env_nrows = c->env_nrows;
   }
   const int64_t min_rows = (int64_t)kSlice * 4 * c->num_sms;  // below this, iterations are latency bound
-  auto repart_target = [&](int64_t r) { return (batch && r / 2 >= min_rows) ? r / 2 : 0; };
+  static const double repart_ratio = [] {
+    const char* e = getenv("SDX_PCG_REPART_RATIO");
+    const double v = e ? atof(e) : kPcgRepartRatio;
+    return v > 0.0 && v < 1.0 ? v : kPcgRepartRatio;
+  }();
+  auto repart_target = [&](int64_t r) {
+    const int64_t t = (int64_t)(repart_ratio * (double)r);
+    return (batch && t >= min_rows) ? t : (int64_t)0;
+  };
   unsigned init[8] = {0u, 0u, 0u, (unsigned)n_active, 0u, (unsigned)rows, 0u, 0u};
   SDX_CUDA(cudaMemcpyAsync(W.sync, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
   SDX_CUDA(cudaMemsetAsync(W.out_iters, 0, sizeof(int) * n_envs, c->stream));

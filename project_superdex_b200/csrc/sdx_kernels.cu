@@ -760,11 +760,24 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     }
   };
   auto reduce_tot = [&](int nq, int buf) {
-    // one warp per (env, quantity); fixed summation order, identical in every CTA
+    // fixed summation order, identical in every CTA. Envs spread over at most 8 CTAs: one thread per
+    // (env, quantity) sums the partials in CTA order (one load round for all of this CTA's envs) ...
+    for (int i = threadIdx.x; i < ne * nq; i += blockDim.x) {
+      const int le = i / nq, k = i % nq;
+      const int e = s_env[le];
+      const int n = a.env_cta1[e] - a.env_cta0[e] + 1;
+      if (n > 8) continue;
+      const double* src = a.part + buf * pstride + (size_t)a.env_poff[e] * kPcgNq + k;
+      double v = 0.0;
+      for (int j = 0; j < n; ++j) v += __ldcg(src + (size_t)j * kPcgNq);
+      tot[le][k] = v;
+    }
+    // ... wider envs: one warp per (env, quantity)
     for (int i = warp; i < ne * nq; i += nwarps) {
       const int le = i / nq, k = i % nq;
       const int e = s_env[le];
       const int n = a.env_cta1[e] - a.env_cta0[e] + 1;
+      if (n <= 8) continue;
       const double* src = a.part + buf * pstride + (size_t)a.env_poff[e] * kPcgNq + k;
       double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
       int j = lane;
@@ -792,26 +805,33 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     }
   };
 
-  // A CTA whose slices all belong to one env keeps its dot-product partials in registers through a
-  // phase and reduces them across the warp once, at the end (acc_end); otherwise every slice adds its
-  // warp sum to the shared per-(warp, env) slots directly.
-  const bool single_env = ne == 1;
+  // Dot-product partials stay in registers while a warp's consecutive slices belong to one env (its
+  // slices ascend, so the env changes rarely); the warp sums them into the shared per-(warp, env) slots
+  // only when the env changes and at the end of the phase (acc_end). acc_le is uniform in the warp.
   double acc[3] = {0.0, 0.0, 0.0};
+  int acc_le = -1;
+  auto acc_flush = [&]() {
+    if (acc_le < 0) return;
+    add_acc(acc_le, 0, acc[0]);
+    add_acc(acc_le, 1, acc[1]);
+    add_acc(acc_le, 2, acc[2]);
+    acc[0] = acc[1] = acc[2] = 0.0;
+  };
   auto acc_add = [&](int le, int k, double v) {
-    if (single_env)
-      acc[k] += v;
-    else
-      add_acc(le, k, v);
+    if (le != acc_le) {
+      acc_flush();
+      acc_le = le;
+    }
+    acc[k] += v;
   };
   auto acc_end = [&](int nq) {  // nq is 1 or 3; constant indices keep acc[] in registers
-    if (!single_env) return;
-    add_acc(0, 0, acc[0]);
-    acc[0] = 0.0;
-    if (nq > 1) {
-      add_acc(0, 1, acc[1]);
-      add_acc(0, 2, acc[2]);
-      acc[1] = acc[2] = 0.0;
+    if (nq == 1) {
+      if (acc_le >= 0) add_acc(acc_le, 0, acc[0]);
+      acc[0] = 0.0;
+    } else {
+      acc_flush();
     }
+    acc_le = -1;
   };
 
   for (int le = threadIdx.x; le < ne; le += blockDim.x) {
