@@ -75,6 +75,9 @@ def build_workload(name: str, seed: int = 0):
     if name == "cfg1":
         return scenes.config1(seed), ("single body 64^3 cells (274,625 nodes, 1,572,864 tets), E log-uniform "
                                       "[1e4,1e6], nu 0.45, 5 capsules r=4mm L=20mm at 0.05 m/s, k=1e4")
+    if name == "cfg4":
+        return scenes.config4(seed), ("stiff heterogeneous body 96^3 cells (912,673 nodes, 5,308,416 tets), nu 0.49, "
+                                      "E log-uniform [1e4,1e7] with 10 inclusions x100, 2 closing planes + 5 capsules")
     if name == "cfg2":
         n = int(os.environ.get("SDX_CFG2_ENVS", "1024"))
         return scenes.config2(seed, n_envs=n), f"{n} uneven bodies, cells/axis U{{8..40}}, 5 capsules + plane each"
@@ -242,6 +245,8 @@ def time_arm(w, args, stream, local_rank, dist, world):
 
 
 def run_ours(args, rank, world, local_rank):
+    # the PCG launch shape is picked by the library's autotuner on each world's first Newton solve
+    os.environ.setdefault("SDX_PCG_AUTOTUNE", "1")
     import torch
     from project_superdex_b200 import capi
     from project_superdex_b200.learned import Mlp
@@ -338,6 +343,7 @@ def run_ours(args, rank, world, local_rank):
                    "cg_rel_tol": 1e-6, "newton_rel_tol": 1e-6, "newton_abs_tol": 1e-9,
                    "newton_max_iter": newton_max_iter(args),
                    "l2": "inputs larger than L2 (matrix + tet data > 126 MB)",
+                   "pcg_threads_autotuned": int(prof.get("pcg_threads", 0)),
                    "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
         "arms": arm_summary, "training": train_info,
         "roofline": roofline, "spmv": spmv, "e2e": e2e, "gpu_launches": head["launches"],
@@ -358,7 +364,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2"])
+    ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg4"])
     ap.add_argument("--arms", default="plain_fp64,fused_zero,learned",
                     help="comma list of solver arms to time, headline last: plain_fp64 (the reference's CUDA "
                          "PCG path restated: FP64 BSR, cuSPARSE/cuBLAS, zero start), fused_zero (this "

@@ -268,6 +268,7 @@ typedef struct {
   double pcg_bytes;         /* algorithmic HBM bytes of the PCG launches: per env, its CG iterations x
                                (40 B per block + 4 B per row pointer + 228 B per row) */
   int64_t pcg_relaunches;   /* re-partitioned PCG relaunches (batches whose slow envs got all CTAs) */
+  int64_t pcg_threads;      /* threads per CTA of the PCG launch shape in use (autotuned or default) */
 } sdx_profile;
 int sdx_set_profiling(sdx_context* ctx, int enable);
 int sdx_get_profile(sdx_context* ctx, sdx_profile* out);

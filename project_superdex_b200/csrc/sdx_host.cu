@@ -231,6 +231,8 @@ struct sdx_context {
   std::mt19937_64 ds_rng{0};
   bool l2_persist = false;
   PcgPartition part_dyn;       // partition of the envs still iterating (re-partitioned PCG relaunches)
+  bool pcg_tuned = false;      // the PCG launch shape was picked by autotune_pcg for this batch
+  int pcg_threads = 0;         // threads per CTA of the context's PCG partition
   int* env_nrows = nullptr;    // padded rows per env (device)
   std::unique_ptr<PlainSolver> plain;  // the plain FP64 comparison solver, built on first use
   // opt-in per-kernel timing: event pairs resolved lazily
@@ -885,6 +887,7 @@ extern "C" int sdx_get_profile(sdx_context* c, sdx_profile* out) {
   if (!c || !out) return set_error(SDX_ERR_INVALID_ARGUMENT, "null argument");
   prof_resolve(c);
   *out = c->prof;
+  out->pcg_threads = c->pcg_threads;
   return SDX_OK;
 }
 
@@ -1220,6 +1223,8 @@ extern "C" int sdx_upload_bodies(sdx_context* c, int n_envs, const int64_t* node
   c->launches++;
   // PCG partition and work
   SDX_TRY(choose_partition(c, c->n_slices, c->h_slice_env, n_envs, c->h_slice_ptr, c->part, 0, 0));
+  c->pcg_threads = c->part.threads;
+  c->pcg_tuned = false;
   SDX_TRY(alloc_work(c->work, c->n_rows, n_envs, /*newton_vectors*/ true));
   c->g = c->work.hot_b;
   c->dx = c->work.hot_x;
@@ -1553,6 +1558,64 @@ static int run_plain(sdx_context* c, const std::vector<uint8_t>& mask, const sdx
   return SDX_OK;
 }
 
+// Launch-shape autotuner for the persistent PCG (SDX_PCG_AUTOTUNE=1): on the first Newton solve of an
+// uploaded batch, each candidate shape runs a fixed 24-iteration solve of the real system (right-hand
+// side g, solution into a scratch vector, statistics off) and the fastest per iteration becomes the
+// context's partition. Candidates: 512 threads with the software-pipelined SpMV (128 registers),
+// 1024 / 768 threads with the batched SpMV (64 / 80 registers), 384 pipelined.
+static int autotune_pcg(sdx_context* c, const sdx_linear_params& lp) {
+  c->pcg_tuned = true;
+  const char* env = getenv("SDX_PCG_AUTOTUNE");
+  if (!(env && atoi(env) != 0) || getenv("SDX_PCG_THREADS")) return SDX_OK;
+  const bool prof = c->profiling;
+  c->profiling = false;
+  sdx_linear_params tl = lp;
+  tl.max_iter = 24;
+  tl.rel_tol = 0.0;
+  tl.abs_tol = 0.0;
+  const int cand[4] = {512, 1024, 768, 384};
+  double best_us = 1e30;
+  int best = c->pcg_threads > 0 ? c->pcg_threads : 512;
+  cudaEvent_t e0, e1;
+  SDX_CUDA(cudaEventCreate(&e0));
+  SDX_CUDA(cudaEventCreate(&e1));
+  for (int t : cand) {
+    PcgPartition P;
+    if (choose_partition(c, c->n_slices, c->h_slice_env, c->n_envs, c->h_slice_ptr, P, t, 1) != SDX_OK) {
+      P.release();
+      continue;
+    }
+    double us = 0.0;
+    for (int rep = 0; rep < 2; ++rep) {  // first run warms up, second is timed
+      SDX_CUDA(cudaEventRecord(e0, c->stream));
+      const int rc = run_pcg(c, ctx_matrix(c), c->diag_pos, c->n_envs, P, c->work, c->g, c->uscratch, nullptr,
+                             c->n_envs, tl, /*zero_guess*/ true, nullptr);
+      SDX_CUDA(cudaEventRecord(e1, c->stream));
+      SDX_CUDA(cudaEventSynchronize(e1));
+      if (rc != SDX_OK) {
+        us = 1e30;
+        break;
+      }
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      us = 1e3 * ms;
+    }
+    P.release();
+    if (us < best_us) {
+      best_us = us;
+      best = t;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->profiling = prof;
+  if (best != c->pcg_threads) {
+    SDX_TRY(choose_partition(c, c->n_slices, c->h_slice_env, c->n_envs, c->h_slice_ptr, c->part, best, 1));
+    c->pcg_threads = best;
+  }
+  return SDX_OK;
+}
+
 static int step_once(sdx_context* c) {
   const sdx_step_params& p = c->params;
   const int E = c->n_envs;
@@ -1634,6 +1697,7 @@ static int step_once(sdx_context* c) {
     if (p.ew_forcing == 2)
       SDX_CUDA(cudaMemcpyAsync(c->work.env_rel_tol, eta.data(), sizeof(double) * E, cudaMemcpyHostToDevice, c->stream));
     std::vector<int> it_out(E);
+    if (!c->pcg_tuned && p.linear.solver_impl != SDX_SOLVER_PLAIN_FP64) SDX_TRY(autotune_pcg(c, p.linear));
     if (p.linear.solver_impl == SDX_SOLVER_PLAIN_FP64) {
       SDX_TRY(run_plain(c, mask, p.linear, zero, it_out));
     } else {

@@ -88,3 +88,16 @@ def test_solver_variants_reach_same_state(oracle, mode):
     size = 0.1
     tol = 1e-5 * size if mode == "previous" else 1e-4 * size  # EW2 loosens the linear solves
     assert np.abs(ug - states[0][0]).max() <= tol
+
+
+def test_autotuned_launch_shape_reaches_same_state(oracle, monkeypatch):
+    """SDX_PCG_AUTOTUNE=1 times the candidate PCG launch shapes on the first Newton solve and keeps the
+    fastest; the step still matches the oracle."""
+    from project_superdex_b200.soft_body import SoftBodyWorld
+    monkeypatch.setenv("SDX_PCG_AUTOTUNE", "1")
+    monkeypatch.delenv("SDX_PCG_THREADS", raising=False)
+    bodies, cfg = scenes.config0()
+    w, ug, vg, states, hist = _run(oracle, bodies, cfg, 2)
+    w.set_profiling(True)
+    assert w.profile()["pcg_threads"] in (384, 512, 768, 1024)
+    _check(bodies, ug, states, hist)
