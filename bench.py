@@ -10,14 +10,16 @@ env of the batch. Inputs (matrix ~160 MB, tet data ~300 MB) exceed the 126 MB L2
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload cfg1|cfg0|cfg2]
                   [--arms plain_fp64,fused_zero,learned]
 
-Three solver arms on the same GPU and the same seeded workload, each a full Newton step:
+Four solver arms on the same GPU and the same seeded workload, each a full Newton step:
   plain_fp64  the reference's CUDA PCG path restated (FP64 3x3 BSR with cuSPARSE bsrmv, cuBLAS vector
               operations, CUDA-graph bursts of 8 iterations with a host convergence check, one env after
               the other), zero initial guess;
   fused_zero  this library's persistent batched PCG (FP32 matrix / SpMV, FP64 x, r and reductions),
               zero initial guess (the reference's Newton behaviour);
-  learned     the same with the learned warm start (per-vertex MLP trained first, on the GPU, from
-              plain-solver episodes of held-out seeds).
+  temporal    the same, started from the previous step's Newton update at the same Newton iteration
+              (energy-optimal scaling; zero when it would raise the residual);
+  learned     the same, started by a Galerkin step on span{temporal guess, MLP correction} (per-vertex
+              MLP trained first, on the GPU, from plain-solver episodes of held-out seeds).
 The headline `value` is the last arm (learned); `arms` gives each and the ratios.
 
 N > 1 runs one independent replica per GPU (the path shards by environment and has no exchange),
@@ -270,7 +272,8 @@ def run_ours(args, rank, world, local_rank):
                           newton_max_iter=newton_max_iter(args))
         if arm == "learned":
             Mlp(w._ctx).set_params(params)
-        w.set_params(warm_start=capi.SDX_WARM_LEARNED if arm == "learned" else capi.SDX_WARM_ZERO,
+        w.set_params(warm_start={"learned": capi.SDX_WARM_LEARNED, "temporal": capi.SDX_WARM_TEMPORAL}.get(
+                         arm, capi.SDX_WARM_ZERO),
                      linear_solver_impl=(capi.SDX_SOLVER_PLAIN_FP64 if arm == "plain_fp64"
                                          else capi.SDX_SOLVER_FUSED))
         stream = torch.cuda.ExternalStream(w.stream_handle(), device=local_rank)
@@ -323,7 +326,7 @@ def run_ours(args, rank, world, local_rank):
     arm_summary = {a: {"value": r["value"], "ms_per_step": r["ms"] / args.steps,
                        "cg_iters_per_step": r["cg_iters_per_step"],
                        "newton_iters_per_step": r["newton_iters_per_step"]} for a, r in results.items()}
-    for base in ("plain_fp64", "fused_zero"):
+    for base in ("plain_fp64", "fused_zero", "temporal"):
         if base in results and "learned" in results:
             arm_summary[f"learned_over_{base}"] = results["learned"]["value"] / results[base]["value"]
             arm_summary[f"cg_iters_learned_over_{base}"] = (results["learned"]["cg_iters_per_step"]
@@ -365,10 +368,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg4"])
-    ap.add_argument("--arms", default="plain_fp64,fused_zero,learned",
+    ap.add_argument("--arms", default="plain_fp64,fused_zero,temporal,learned",
                     help="comma list of solver arms to time, headline last: plain_fp64 (the reference's CUDA "
                          "PCG path restated: FP64 BSR, cuSPARSE/cuBLAS, zero start), fused_zero (this "
-                         "library's PCG, zero start), learned (this library's PCG, learned warm start)")
+                         "library's PCG, zero start), temporal (start from the previous step's update at the "
+                         "same Newton iteration), learned (temporal guess + learned correction, Galerkin)")
     ap.add_argument("--train-episodes", type=int, default=2, dest="train_episodes")
     ap.add_argument("--train-steps", type=int, default=8, dest="train_steps")
     ap.add_argument("--train-epochs", type=int, default=8, dest="train_epochs")

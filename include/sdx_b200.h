@@ -71,6 +71,7 @@ extern "C" {
 #define SDX_WARM_ZERO 0     /* reference behaviour: dx0 = 0 (newton_solver.cpp:746) */
 #define SDX_WARM_PREVIOUS 1 /* dx0 = the previous solve's dx of the same env */
 #define SDX_WARM_LEARNED 2  /* dx0 = per-vertex MLP prediction (sdx_mlp_*) */
+#define SDX_WARM_TEMPORAL 3 /* dx0 = the previous step's dx of the same Newton iteration (first 4) */
 
 /* Mirrors KrylovSolverParams (krylov_solver.h:43-82). Only the residual-L2 norm is supported. */
 typedef struct {
@@ -223,8 +224,9 @@ int sdx_get_stats(sdx_context* ctx, sdx_env_stats* per_env);
 
 /* ---- learned CG warm start (no counterpart in the reference) -------------------------------------
  * A per-vertex MLP (15 -> 128 -> 128 -> 128 -> 3, GELU; BF16 weights / activations, FP32 accumulate;
- * forward on the tensor cores) maps 1-ring-averaged displacement, dt * velocity, the last two Newton
- * updates and the Jacobi-preconditioned Newton gradient (all divided by the env's RMS of the latter)
+ * forward on the tensor cores) maps 1-ring-averaged displacement, dt * velocity, the last Newton
+ * update, the previous step's update at the same Newton iteration and the Jacobi-preconditioned Newton
+ * gradient (each group divided by the env's RMS of it)
  * to the Newton update in the same units. With warm_start = SDX_WARM_LEARNED its prediction is the
  * initial guess of every Newton linear solve; the converged residual still decides the solution. */
 #define SDX_MLP_PARAMS 37264

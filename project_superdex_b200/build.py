@@ -34,7 +34,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return LIB
     srcs = [os.path.join(CSRC, s) for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--extended-lambda", "-shared",
-           "-Xcompiler", "-fPIC,-fopenmp", "-ccbin", "/usr/bin/g++", "-o", LIB + ".tmp", *srcs, "-lgomp", "-lcusparse", "-lcublas"]
+           "-Xcompiler", "-fPIC,-fopenmp", "-ccbin", "/usr/bin/g++", "-o", LIB + ".tmp", *srcs, "-lgomp", "-lcusparse", "-lcublas", "-Xlinker", "--no-undefined"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd), file=sys.stderr)

@@ -18,7 +18,7 @@ SDX_ASM_OBJ, SDX_ASM_RES, SDX_ASM_HESS, SDX_ASM_PSD = 1, 2, 4, 8
 SDX_GUESS_UNKNOWN, SDX_GUESS_ZERO = 0, 1
 SDX_F32, SDX_F64 = 0, 1
 SDX_PREC_NONE, SDX_PREC_JACOBI, SDX_PREC_BLOCK_JACOBI = 0, 1, 2
-SDX_WARM_ZERO, SDX_WARM_PREVIOUS, SDX_WARM_LEARNED = 0, 1, 2
+SDX_WARM_ZERO, SDX_WARM_PREVIOUS, SDX_WARM_LEARNED, SDX_WARM_TEMPORAL = 0, 1, 2, 3
 SDX_LINEAR_CONVERGED, SDX_LINEAR_STOPPED, SDX_LINEAR_DIVERGED = 1, 2, 3
 SDX_SOLVER_FUSED, SDX_SOLVER_PLAIN_FP64 = 0, 1
 

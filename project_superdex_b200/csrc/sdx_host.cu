@@ -197,6 +197,7 @@ struct sdx_context {
          *ubase = nullptr, *uscratch = nullptr, *staging = nullptr;
   // per env
   double* env_norm = nullptr;
+  double* env_hnorm = nullptr;  // |h|^2 per env of the temporal guess h (learned warm start)
   double* env_scale = nullptr;
   double* env_obj = nullptr;
   uint8_t* env_mask = nullptr;
@@ -232,6 +233,10 @@ struct sdx_context {
   bool l2_persist = false;
   PcgPartition part_dyn;       // partition of the envs still iterating (re-partitioned PCG relaunches)
   bool pcg_tuned = false;      // the PCG launch shape was picked by autotune_pcg for this batch
+  // temporal warm start: the Newton updates of the previous step, per Newton iteration (first kHist)
+  static constexpr int kHist = 4;
+  double* dx_hist = nullptr;
+  bool hist_valid[kHist] = {false, false, false, false};
   int pcg_threads = 0;         // threads per CTA of the context's PCG partition
   int* env_nrows = nullptr;    // padded rows per env (device)
   std::unique_ptr<PlainSolver> plain;  // the plain FP64 comparison solver, built on first use
@@ -309,6 +314,8 @@ static void release_topology(sdx_context* c) {
   c->plain.reset();
   c->part_dyn.release();
   dfree(c->env_nrows);
+  dfree(c->dx_hist);
+  for (bool& h : c->hist_valid) h = false;
   dfree(c->slice_ptr);
   dfree(c->slice_w);
   dfree(c->slice_env);
@@ -338,6 +345,7 @@ static void release_topology(sdx_context* c) {
   dfree(c->uscratch);
   dfree(c->staging);
   dfree(c->env_norm);
+  dfree(c->env_hnorm);
   dfree(c->env_scale);
   dfree(c->env_obj);
   dfree(c->env_mask);
@@ -661,7 +669,7 @@ constexpr double kPcgRepartRatio = 0.5;
 static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_envs, PcgPartition& P,
                    PcgWork& W, const double* b, double* x, const uint8_t* env_mask, int n_active,
                    const sdx_linear_params& lp, bool zero_guess, const double* env_rel_tol,
-                   bool scale_guess = false, const uint8_t* h_mask = nullptr) {
+                   bool scale_guess = false, const uint8_t* h_mask = nullptr, const double* x2 = nullptr) {
   PcgArgs a;
   memset(&a, 0, sizeof(a));
   a.A = A;
@@ -670,6 +678,7 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
   a.diag_pos = diag_pos;
   a.b = b;
   a.x = x;
+  a.x2 = x2;
   a.r = W.r;
   a.p = W.p;
   a.q = W.q;
@@ -1205,6 +1214,7 @@ extern "C" int sdx_upload_bodies(sdx_context* c, int n_envs, const int64_t* node
     SDX_TRY(upload(&c->env_nrows, er));
   }
   SDX_TRY(dalloc(&c->env_norm, n_envs));
+  SDX_TRY(dalloc(&c->env_hnorm, n_envs));
   SDX_TRY(dalloc(&c->env_scale, n_envs));
   SDX_TRY(dalloc(&c->env_obj, n_envs));
   SDX_TRY(dalloc(&c->env_mask, n_envs));
@@ -1496,7 +1506,8 @@ static void launch_gather_rows(const int* idx, int n, const float* src, int widt
 
 // Appends samples (features before the solve, solution / env scale) of random nodes of the active envs.
 static int capture_samples(sdx_context* c, const std::vector<uint8_t>& mask) {
-  launch_targets(c->n_rows, c->slice_env, c->dx, c->env_norm, c->env_rows, c->feat_Y, c->stream);
+  launch_targets(c->n_rows, c->slice_env, c->dx, c->env_norm, c->dx_prev2, c->env_hnorm, c->env_rows, c->feat_Y,
+                 c->stream);
   c->launches++;
   std::vector<int64_t> pref(1, 0);
   std::vector<int> envs;
@@ -1633,6 +1644,7 @@ static int step_once(sdx_context* c) {
   SDX_TRY(env_dot_host(c, c->g, c->g, c->env_mask, nrm));
   for (int e = 0; e < E; ++e) res[e] = std::sqrt(nrm[e]);
   bool first_pass = true;
+  int pass = 0;  // Newton passes of this step (every env still iterating is at the same pass)
   std::vector<double> unorm;
   for (;;) {
     // stop criteria in the reference order (newton_solver.cpp:303-313)
@@ -1677,11 +1689,26 @@ static int step_once(sdx_context* c) {
     if (n_active == 0) break;
     SDX_TRY(upload_mask(c, mask));
     if (!first_pass) assemble_dev(c, c->u, c->ut, t_end, SDX_ASM_HESS | SDX_ASM_PSD, c->env_mask, false);
+    // the launch-shape autotuner (opt-in) runs on the first solve, before any start vector is written
+    if (!c->pcg_tuned && p.linear.solver_impl != SDX_SOLVER_PLAIN_FP64) SDX_TRY(autotune_pcg(c, p.linear));
     // linear solve H dx = g, warm started from zero, the previous dx, or the learned prediction
     const bool learned = p.warm_start == SDX_WARM_LEARNED;
     const bool collect = c->collect_per_solve > 0 && c->ds_n < c->ds_cap;
     if (learned && !c->mlp.p) return set_error(SDX_ERR_NOT_READY, "learned warm start needs MLP parameters");
+    // per-Newton-iteration history of the previous step's updates: the temporal warm start, and the
+    // third feature group of the learned one (dx_prev2 holds the same-iteration update of the previous
+    // step, zero when there is none)
+    const bool keep_hist = (p.warm_start == SDX_WARM_TEMPORAL || learned || collect) && pass < sdx_context::kHist;
+    if (keep_hist && !c->dx_hist) SDX_TRY(dalloc(&c->dx_hist, (size_t)sdx_context::kHist * n3));
     if (learned || collect) {
+      if (keep_hist && c->hist_valid[pass])
+        launch_copy_rows(c->n_slices, c->slice_env, c->env_mask, c->dx_hist + (size_t)pass * n3, c->dx_prev2,
+                         c->stream);
+      else
+        SDX_CUDA(cudaMemsetAsync(c->dx_prev2, 0, sizeof(double) * n3, c->stream));
+      SDX_CUDA(cudaMemsetAsync(c->env_hnorm, 0, sizeof(double) * E, c->stream));
+      launch_env_dot(c->n_slices, c->slice_env, c->env_mask, c->dx_prev2, c->dx_prev2, c->env_hnorm, c->stream);
+      c->launches += 2;
       launch_features(ctx_matrix(c), c->n_rows, c->env_mask, c->u, c->v, p.dt, c->dx_prev1, c->dx_prev2, c->g,
                       c->diag_pos, c->pin, c->env_rows, c->feat_raw, c->feat_sumsq, E, c->feat_X, c->stream);
       c->launches += 3;
@@ -1690,20 +1717,26 @@ static int step_once(sdx_context* c) {
       if (launch_mlp_forward(mlp_forward_args(c->mlp, c->feat_X, (int)c->n_rows, c->feat_Y, nullptr, c->mlp_error),
                              c->num_sms, c->stream) != 0)
         return set_error(SDX_ERR_CUDA, "MLP forward launch failed");
-      launch_warm_start(c->n_rows, c->slice_env, c->env_mask, c->feat_Y, c->pin, c->diag_pos, c->dx, c->stream);
+      launch_warm_start(c->n_rows, c->slice_env, c->env_mask, c->feat_Y, c->pin, c->diag_pos, c->dx_prev2,
+                        c->env_hnorm, c->env_rows, c->dx, c->uscratch, c->stream);
       c->launches += 2;
     }
-    const bool zero = p.warm_start == SDX_WARM_ZERO;
+    const bool temporal = p.warm_start == SDX_WARM_TEMPORAL && pass < sdx_context::kHist;
+    if (temporal && c->hist_valid[pass]) {
+      launch_copy_rows(c->n_slices, c->slice_env, c->env_mask, c->dx_hist + (size_t)pass * n3, c->dx, c->stream);
+      c->launches++;
+    }
+    const bool zero = p.warm_start == SDX_WARM_ZERO || (p.warm_start == SDX_WARM_TEMPORAL &&
+                                                        !(temporal && c->hist_valid[pass]));
     if (p.ew_forcing == 2)
       SDX_CUDA(cudaMemcpyAsync(c->work.env_rel_tol, eta.data(), sizeof(double) * E, cudaMemcpyHostToDevice, c->stream));
     std::vector<int> it_out(E);
-    if (!c->pcg_tuned && p.linear.solver_impl != SDX_SOLVER_PLAIN_FP64) SDX_TRY(autotune_pcg(c, p.linear));
     if (p.linear.solver_impl == SDX_SOLVER_PLAIN_FP64) {
       SDX_TRY(run_plain(c, mask, p.linear, zero, it_out));
     } else {
       SDX_TRY(run_pcg(c, ctx_matrix(c), c->diag_pos, E, c->part, c->work, c->g, c->dx, c->env_mask, n_active,
                       p.linear, zero, p.ew_forcing == 2 ? c->work.env_rel_tol : nullptr, /*scale_guess*/ !zero,
-                      mask.data()));
+                      mask.data(), learned ? c->uscratch : nullptr));
       SDX_CUDA(cudaMemcpy(it_out.data(), c->work.out_iters, sizeof(int) * E, cudaMemcpyDeviceToHost));
     }
     for (int e = 0; e < E; ++e)
@@ -1715,10 +1748,15 @@ static int step_once(sdx_context* c) {
       c->launches++;
       SDX_TRY(capture_samples(c, mask));
     }
-    // Newton-update history for the learned features
-    launch_copy_rows(c->n_slices, c->slice_env, c->env_mask, c->dx_prev1, c->dx_prev2, c->stream);
+    if (keep_hist) {
+      launch_copy_rows(c->n_slices, c->slice_env, c->env_mask, c->dx, c->dx_hist + (size_t)pass * n3, c->stream);
+      c->launches++;
+      c->hist_valid[pass] = true;
+    }
+    ++pass;
+    // last Newton update, for the learned features
     launch_copy_rows(c->n_slices, c->slice_env, c->env_mask, c->dx, c->dx_prev1, c->stream);
-    c->launches += 2;
+    c->launches++;
     SDX_TRY(env_dot_host(c, c->dx, c->dx, c->env_mask, nrm));
     for (int e = 0; e < E; ++e)
       if (mask[e]) dxn[e] = std::sqrt(nrm[e]);

@@ -22,7 +22,7 @@ namespace sdx {
 constexpr int kSlice = 32;
 constexpr int kPadBit = 0x80000000;
 constexpr int kPcgMaxEnvsPerCta = 32;
-constexpr int kPcgNq = 5;  // partial sums per (CTA, env) and phase
+constexpr int kPcgNq = 11;  // partial sums per (CTA, env) and phase (11: the two-vector start)
 
 __host__ __device__ __forceinline__ size_t val_index(int64_t p, int e) {
   const size_t g = (size_t)(p - (p & 31)) * 9;
@@ -99,6 +99,7 @@ struct PcgArgs {
   const int* diag_pos;
   const double* b;
   double* x;
+  const double* x2;  // second start vector (learned correction): Galerkin start on span{x, x2} (NULL: none)
   double* r;
   float* p;
   float* q;

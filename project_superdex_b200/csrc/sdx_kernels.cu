@@ -685,6 +685,26 @@ __device__ __forceinline__ void prec_apply(const PcgArgs& a, int64_t row, const 
   }
 }
 
+// y = A v for the 32 rows of slice s, FP64 accumulation (FP32 matrix values, FP64 v gathered from L2)
+__device__ __forceinline__ void spmv_f64(const PcgArgs& a, int s, int lane, const double* v_, double y[3]) {
+  const int base = a.A.slice_ptr[s], w = a.A.slice_w[s];
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  for (int k = 0; k < w; ++k) {
+    const int p = base + k * kSlice + lane;
+    const int j = __ldcs(a.A.col + p) & 0x7fffffff;
+    float v[9];
+    load_block(a.A.val + (size_t)(base + k * kSlice) * 9, lane, v);
+    const double x0 = __ldcg(v_ + 3 * (int64_t)j), x1 = __ldcg(v_ + 3 * (int64_t)j + 1),
+                 x2 = __ldcg(v_ + 3 * (int64_t)j + 2);
+    a0 += (double)v[0] * x0 + (double)v[1] * x1 + (double)v[2] * x2;
+    a1 += (double)v[3] * x0 + (double)v[4] * x1 + (double)v[5] * x2;
+    a2 += (double)v[6] * x0 + (double)v[7] * x1 + (double)v[8] * x2;
+  }
+  y[0] = a0;
+  y[1] = a1;
+  y[2] = a2;
+}
+
 // r = b - A x with FP64 accumulation (FP32 matrix values, FP64 x gathered from L2)
 __device__ __forceinline__ void true_residual(const PcgArgs& a, int s, int lane, double r[3]) {
   const int base = a.A.slice_ptr[s], w = a.A.slice_w[s];
@@ -856,7 +876,81 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
   if (!a.resume) {
     // ---- phase 0: r = b - A x0, z = M^-1 r, partials b.b, r.r, r.z ----
     const bool scaled = !a.zero_guess && a.scale_guess;
-    if (scaled) {
+    const bool two = scaled && a.x2 != nullptr;
+    if (two) {
+      // Galerkin start on span{x, x2} (the temporal guess and the learned correction): with Ah = A x,
+      // Ay = A x2, the coefficients (ca, cb) minimise the A-norm error, i.e. solve
+      // [x.Ah x.Ay; x.Ay x2.Ay] (ca, cb) = (x.b, x2.b). Among that pair and the one-vector optima, the
+      // env keeps the one with the smallest A-norm error whose residual ||b - ca Ah - cb Ay|| is below
+      // ||b|| (the measure of the stop test); failing all, the zero start.
+      clear_acc();
+      for (int i = s0 + warp; i < s1; i += nwarps) {
+        const int s = slice_of(i);
+        const int le = local_env(a.A.slice_env[s]);
+        if (st[le].status != 0) continue;
+        const int64_t row = (int64_t)s * kSlice + lane;
+        double ah[3], ay[3];
+        spmv_f64(a, s, lane, a.x, ah);
+        spmv_f64(a, s, lane, a.x2, ay);
+        double q[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const double h = a.x[3 * row + k], y = a.x2[3 * row + k], bk = a.b[3 * row + k];
+          q[0] += bk * bk;
+          q[1] += h * bk;
+          q[2] += y * bk;
+          q[3] += h * ah[k];
+          q[4] += h * ay[k];
+          q[5] += y * ay[k];
+          q[6] += bk * ah[k];
+          q[7] += bk * ay[k];
+          q[8] += ah[k] * ah[k];
+          q[9] += ah[k] * ay[k];
+          q[10] += ay[k] * ay[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 11; ++k) add_acc(le, k, q[k]);
+      }
+      flush_acc(11, 1);
+      if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
+      reduce_tot(11, 1);
+      for (int le = threadIdx.x; le < ne; le += blockDim.x) {
+        const double* t = tot[le];
+        const double bb = t[0];
+        auto res2 = [&](double ca, double cb) {
+          return bb - 2.0 * (ca * t[6] + cb * t[7]) + ca * ca * t[8] + 2.0 * ca * cb * t[9] + cb * cb * t[10];
+        };
+        double best_gain = 0.0, ba = 0.0, bc = 0.0;
+        auto consider = [&](double ca, double cb) {
+          const double gain = ca * t[1] + cb * t[2];  // A-norm error reduction at a Galerkin optimum
+          if (isfinite(gain) && gain > best_gain && res2(ca, cb) < bb) {
+            best_gain = gain;
+            ba = ca;
+            bc = cb;
+          }
+        };
+        const double det = t[3] * t[5] - t[4] * t[4];
+        if (t[3] > 0.0 && t[5] > 0.0 && det > 1e-12 * t[3] * t[5])
+          consider((t[1] * t[5] - t[2] * t[4]) / det, (t[3] * t[2] - t[4] * t[1]) / det);
+        if (t[3] > 0.0) consider(t[1] / t[3], 0.0);
+        if (t[5] > 0.0) consider(0.0, t[2] / t[5]);
+        st[le].alpha = ba;
+        st[le].beta = bc;
+      }
+      __syncthreads();
+      for (int i = s0 + warp; i < s1; i += nwarps) {
+        const int s = slice_of(i);
+        const int le = local_env(a.A.slice_env[s]);
+        if (st[le].status != 0) continue;
+        const int64_t row = (int64_t)s * kSlice + lane;
+        const double ca = st[le].alpha, cb = st[le].beta;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) a.x[3 * row + k] = ca * a.x[3 * row + k] + cb * a.x2[3 * row + k];
+      }
+      for (int le = threadIdx.x; le < ne; le += blockDim.x) st[le].beta = 0.0;
+      // the residual pass below gathers neighbouring rows of the combined x
+      if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
+    } else if (scaled) {
       // energy-optimal scaling of the guess: alpha = (x0.b) / (x0.A x0), A x0 = b - r0; the scaled start
       // alpha x0 never has a larger A-norm error than the zero start. The guess is kept only if it also
       // lowers the residual the stop test measures: ||b - alpha A x0||^2 = (1-alpha)^2 b.b
@@ -933,8 +1027,8 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
           r[k] = a.b[3 * row + k];
         }
       }
-      if (!a.zero_guess && !scaled) true_residual(a, s, lane, r);
-      if (scaled) {
+      if (!a.zero_guess && (!scaled || two)) true_residual(a, s, lane, r);
+      if (scaled && !two) {
         const double al = st[le].alpha;
   #pragma unroll
         for (int k = 0; k < 3; ++k) {
@@ -1179,6 +1273,8 @@ static bool pcg_pipelined(int threads) {
 
 int pcg_max_ctas_per_sm(int threads) {
   int n = 0;
+  for (const void* fn : {(const void*)k_pcg<true>, (const void*)k_pcg<false>})
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, pcg_shared_bytes(1024));
   const cudaError_t e =
       pcg_pipelined(threads)
           ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pcg<true>, threads, pcg_shared_bytes(threads))

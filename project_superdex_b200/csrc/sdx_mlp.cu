@@ -443,7 +443,8 @@ void mlp_adam(const MlpParams& P, float lr, int step, cudaStream_t st) {
 // ------------------------------------------------------------------------------------------------
 // features and warm start (one thread per row)
 
-// raw per-row quantities: u, dt v, dx_{k-1}, dx_{k-2}, D^-1 g (Jacobi-preconditioned Newton gradient)
+// raw per-row quantities: u, dt v, the last Newton update dx1, the previous step's update at the same
+// Newton iteration dx2 (zero when there is none), D^-1 g (Jacobi-preconditioned Newton gradient)
 __global__ void k_feature_raw(int64_t n_rows, const double* __restrict__ u, const double* __restrict__ v, double dt,
                               const double* __restrict__ dx1, const double* __restrict__ dx2,
                               const double* __restrict__ g, const float* __restrict__ val,
@@ -517,21 +518,28 @@ __global__ void k_feature_ring(Matrix A, const uint8_t* __restrict__ env_mask, c
 }
 
 // dx0 = MLP(X) on free DoFs of active envs (its scale is set by the solver's energy-optimal scaling)
+// Start vectors of the learned warm start: x = h / RMS_env(h), the temporal guess (the previous step's
+// update at the same Newton iteration, zero when there is none), and x2 = Y, the network's correction;
+// the PCG combines them by a Galerkin step on span{x, x2}. Pinned and padding DoFs are zero.
 __global__ void k_warm_start(int64_t n_rows, const int* __restrict__ slice_env, const uint8_t* __restrict__ env_mask,
                              const float* __restrict__ Y, const uint8_t* __restrict__ pin,
-                             const int* __restrict__ diag_pos, double* dx) {
+                             const int* __restrict__ diag_pos, const double* __restrict__ h,
+                             const double* __restrict__ h2, const int* __restrict__ env_rows, double* dx,
+                             double* x2) {
   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n_rows) return;
   const int e = slice_env[r >> 5];
   if (env_mask && !env_mask[e]) return;
+  const double hr = sqrt(h2[e] / fmax(1.0, 3.0 * (double)env_rows[e]));
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const bool free = diag_pos[r] >= 0 && !((pin[r] >> k) & 1);
     const double y = (double)Y[3 * r + k];
-    dx[3 * r + k] = (free && isfinite(y)) ? y : 0.0;
+    const double t = hr > 0.0 ? h[3 * r + k] / hr : 0.0;
+    dx[3 * r + k] = (free && isfinite(t)) ? t : 0.0;
+    x2[3 * r + k] = (free && isfinite(y)) ? y : 0.0;
   }
 }
-
 void launch_features(const Matrix& A, int64_t n_rows, const uint8_t* env_mask, const double* u, const double* v,
                      double dt, const double* dx1, const double* dx2, const double* g, const int* diag_pos,
                      const uint8_t* pin, const int* env_rows, float* raw, double* sumsq, int n_envs, float* X,
@@ -544,28 +552,33 @@ void launch_features(const Matrix& A, int64_t n_rows, const uint8_t* env_mask, c
   k_feature_scale<<<(unsigned)((t + 255) / 256), 256, 0, st>>>(A.n_slices, A.slice_env, env_mask, raw, sumsq);
   k_feature_ring<<<(unsigned)((t + 255) / 256), 256, 0, st>>>(A, env_mask, raw, sumsq, env_rows, X);
 }
-
 void launch_warm_start(int64_t n_rows, const int* slice_env, const uint8_t* env_mask, const float* Y,
-                       const uint8_t* pin, const int* diag_pos, double* dx, cudaStream_t st) {
+                       const uint8_t* pin, const int* diag_pos, const double* h, const double* h2,
+                       const int* env_rows, double* dx, double* x2, cudaStream_t st) {
   if (n_rows == 0) return;
-  k_warm_start<<<(unsigned)((n_rows + 255) / 256), 256, 0, st>>>(n_rows, slice_env, env_mask, Y, pin, diag_pos, dx);
+  k_warm_start<<<(unsigned)((n_rows + 255) / 256), 256, 0, st>>>(n_rows, slice_env, env_mask, Y, pin, diag_pos, h,
+                                                                   h2, env_rows, dx, x2);
 }
 
-// training targets: T[row] = dx / RMS_env(dx) (the shape of the update; dx2 holds |dx|^2 per env)
+// training targets: the shape of the update relative to the temporal guess h,
+// T[row] = dx / RMS_env(dx) - h / RMS_env(h) (the second term is zero without a guess); dx2 and h2 hold
+// |dx|^2 and |h|^2 per env
 __global__ void k_targets(int64_t n_rows, const int* __restrict__ slice_env, const double* __restrict__ dx,
-                          const double* __restrict__ dx2, const int* __restrict__ env_rows, float* T) {
+                          const double* __restrict__ dx2, const double* __restrict__ h,
+                          const double* __restrict__ h2, const int* __restrict__ env_rows, float* T) {
   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n_rows) return;
   const int e = slice_env[r >> 5];
-  const double rms = sqrt(dx2[e] / fmax(1.0, 3.0 * (double)env_rows[e]));
+  const double n3 = fmax(1.0, 3.0 * (double)env_rows[e]);
+  const double rms = sqrt(dx2[e] / n3), hr = sqrt(h2[e] / n3);
 #pragma unroll
-  for (int k = 0; k < 3; ++k) T[3 * r + k] = rms > 0.0 ? (float)(dx[3 * r + k] / rms) : 0.0f;
+  for (int k = 0; k < 3; ++k)
+    T[3 * r + k] = rms > 0.0 ? (float)(dx[3 * r + k] / rms - (hr > 0.0 ? h[3 * r + k] / hr : 0.0)) : 0.0f;
 }
-
-void launch_targets(int64_t n_rows, const int* slice_env, const double* dx, const double* dx2, const int* env_rows,
-                    float* T, cudaStream_t st) {
+void launch_targets(int64_t n_rows, const int* slice_env, const double* dx, const double* dx2, const double* h,
+                    const double* h2, const int* env_rows, float* T, cudaStream_t st) {
   if (n_rows == 0) return;
-  k_targets<<<(unsigned)((n_rows + 255) / 256), 256, 0, st>>>(n_rows, slice_env, dx, dx2, env_rows, T);
+  k_targets<<<(unsigned)((n_rows + 255) / 256), 256, 0, st>>>(n_rows, slice_env, dx, dx2, h, h2, env_rows, T);
 }
 
 }  // namespace sdx

@@ -59,8 +59,9 @@ void launch_features(const Matrix& A, int64_t n_rows, const uint8_t* env_mask, c
                      const uint8_t* pin, const int* env_rows, float* raw, double* sumsq, int n_envs, float* X,
                      cudaStream_t st);
 void launch_warm_start(int64_t n_rows, const int* slice_env, const uint8_t* env_mask, const float* Y,
-                       const uint8_t* pin, const int* diag_pos, double* dx, cudaStream_t st);
-void launch_targets(int64_t n_rows, const int* slice_env, const double* dx, const double* dx2, const int* env_rows,
-                    float* T, cudaStream_t st);
+                       const uint8_t* pin, const int* diag_pos, const double* h, const double* h2,
+                       const int* env_rows, double* dx, double* x2, cudaStream_t st);
+void launch_targets(int64_t n_rows, const int* slice_env, const double* dx, const double* dx2, const double* h,
+                    const double* h2, const int* env_rows, float* T, cudaStream_t st);
 
 }  // namespace sdx

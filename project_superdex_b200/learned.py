@@ -1,8 +1,9 @@
 """Learned CG warm start: data generation from the plain solver, GPU training, evaluation.
 
 The network (sdx_mlp.cu) maps per-vertex, 1-ring-averaged features — displacement, dt * velocity, the last
-two Newton updates and the Jacobi-preconditioned Newton gradient, all divided by the env's RMS of the
-latter — to the Newton update in the same units. Training pairs are (features before a Newton linear
+Newton update, the previous step's update at the same Newton iteration (the temporal warm start) and the
+Jacobi-preconditioned Newton gradient, each group divided by the env's RMS of it — to the Newton update
+in the same units. Training pairs are (features before a Newton linear
 solve, its converged solution) recorded while the plain solver (zero initial guess, the reference's
 behaviour at mochi_core/src/solvers/newton_solver.cpp:746) steps seeded episodes. The prediction is only
 ever an initial guess: every solve still runs to the same residual tolerance.

@@ -83,3 +83,45 @@ def test_learned_warm_start_keeps_the_converged_state():
     u1, s1 = states[capi.SDX_WARM_LEARNED]
     assert s1["convergence"] == s0["convergence"] == 1
     assert np.abs(u1 - u0).max() <= 1e-5 * 0.1  # vertex error <= 1e-5 of the body size
+
+
+def test_learned_start_gains_over_the_plain_start():
+    """What the trained network gains: CG iterations of 8 steps of a body pressed by a capsule, from the
+    zero start (the reference's behaviour), the temporal start (previous step's update at the same Newton
+    iteration) and the learned start (Galerkin step on the temporal guess and the network's correction,
+    trained on another seed of the same scene)."""
+    from project_superdex_b200.learned import Mlp, collect
+    from project_superdex_b200.soft_body import SoftBodyWorld
+
+    def scene(seed):
+        rng = np.random.default_rng(seed)
+        b = scenes.grid_body(16, 16, 12, 0.1 / 16, rng=rng, nu=0.45)
+        b.E = np.exp(rng.uniform(np.log(1e4), np.log(1e6), size=b.n_tets))
+        b.colliders = scenes._fingertips(rng, (0, 0), (0.1, 0.1), 0.075)
+        return [b], scenes.SceneConfig(k_contact=1e4)
+
+    bodies, cfg = scene(11)
+    tw = SoftBodyWorld(bodies, cfg, newton_abs_tol=1e-9)
+    X, T = collect(tw, 10, 4000, 200000, seed=2)
+    m = Mlp(tw._ctx)
+    m.init(3)
+    m.train(X, T, batch=2048, epochs=12)
+    params = m.get_params()
+    bodies, cfg = scene(12)
+    cg = {}
+    for ws in (capi.SDX_WARM_ZERO, capi.SDX_WARM_TEMPORAL, capi.SDX_WARM_LEARNED):
+        w = SoftBodyWorld(bodies, cfg, newton_abs_tol=1e-9)
+        if ws == capi.SDX_WARM_LEARNED:
+            Mlp(w._ctx).set_params(params)
+        w.set_params(warm_start=ws)
+        total = 0
+        for _ in range(8):
+            w.step(1)
+            st = w.stats()[0]
+            assert st["convergence"] == 1
+            total += st["cg_iters"]
+        cg[ws] = total
+    zero, temporal, learned = cg[capi.SDX_WARM_ZERO], cg[capi.SDX_WARM_TEMPORAL], cg[capi.SDX_WARM_LEARNED]
+    print("CG iterations over 8 steps: zero %d, temporal %d, learned %d" % (zero, temporal, learned))
+    assert learned < zero
+    assert learned <= 1.05 * temporal
