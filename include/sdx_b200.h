@@ -193,6 +193,15 @@ int sdx_upload_bodies(sdx_context* ctx, int n_envs, const int64_t* node_offsets,
  * non-decreasing. */
 int sdx_set_colliders(sdx_context* ctx, int n_colliders, const int32_t* env, const double* rows);
 
+/* Soft material of each env, values as SoftMaterialType (mochi_core/.../materials/material_types.h:
+ * 148-172): the constitutive response of BatchedSmithNeoHookean (batched_smith_neo_hookean.cpp:29),
+ * BatchedStVenantKirchhoff (batched_st_venant_kirchhoff.cpp:29) or BatchedLinearElastic
+ * (batched_linear_elastic.cpp:27) with the body's per-tet Lame parameters. Default: all Neo-Hookean. */
+#define SDX_MAT_NEO_HOOKEAN 0
+#define SDX_MAT_ST_VENANT_KIRCHHOFF 1
+#define SDX_MAT_LINEAR_ELASTIC 2
+int sdx_set_materials(sdx_context* ctx, int n_envs, const int32_t* material);
+
 int sdx_set_params(sdx_context* ctx, const sdx_step_params* params);
 
 /* State in user node order (3 doubles per node): displacement u and velocity v. */

@@ -42,7 +42,7 @@ class OrScene(C.Structure):
         ("min_eig", C.c_double),
         ("n_colliders", C.c_int), ("colliders", C.POINTER(OrCollider)),
         ("k_contact", C.c_double), ("t_half", C.c_double), ("thr", C.c_double),
-        ("max_align", C.c_double),
+        ("max_align", C.c_double), ("material", C.c_int),
     ]
 
 
@@ -81,6 +81,8 @@ def lib():
             build()
         L = C.CDLL(LIB_PATH)
         L.or_smith_nh.argtypes = [C.c_double, C.c_double, _dp, C.c_int, C.c_int, C.c_double, _dp, _dp, _dp]
+        L.or_material.argtypes = [C.c_int, C.c_double, C.c_double, _dp, C.c_int, C.c_int, C.c_double, _dp, _dp,
+                                  _dp]
         L.or_polyrelu.argtypes = [C.c_double] * 3 + [_dp] * 3
         L.or_penalty.argtypes = [C.c_double, _dp, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp]
         L.or_pattern_nnzb.argtypes = [C.c_int, C.c_int, _ip]
@@ -110,6 +112,7 @@ def ref():
     if _ref is None and os.path.exists(REF_PATH):
         R = C.CDLL(REF_PATH)
         R.ref_smith_nh.argtypes = [C.c_double, C.c_double, _dp, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp]
+        R.ref_material.argtypes = [C.c_int, C.c_double, C.c_double, _dp, C.c_int, C.c_int, _dp, _dp, _dp]
         R.ref_polyrelu.argtypes = [C.c_double] * 3 + [_dp] * 3
         R.ref_penalty.argtypes = [C.c_double, _dp, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp]
         R.ref_stress_work.argtypes = [_dp, _dp, C.c_double, C.c_double, C.c_int, C.c_int, _dp, _dp, _dp]
@@ -134,6 +137,26 @@ def smith_nh(mu, lam, F, project=False, psd=1, min_eig=np.finfo(np.float64).eps)
     P = np.zeros(9)
     Cm = np.zeros(81)
     lib().or_smith_nh(mu, lam, ptr(F), int(project), psd, min_eig, ptr(e), ptr(P), ptr(Cm))
+    return e[0], P.reshape(3, 3), Cm.reshape(9, 9)
+
+
+def material(kind, mu, lam, F, project=False, psd=1, min_eig=np.finfo(np.float64).eps):
+    """or_material: kind 0 Smith Neo-Hookean, 1 St. Venant-Kirchhoff, 2 linear elastic."""
+    F = np.ascontiguousarray(F, np.float64).reshape(9)
+    e = np.zeros(1)
+    P = np.zeros(9)
+    Cm = np.zeros(81)
+    lib().or_material(int(kind), mu, lam, ptr(F), int(project), psd, min_eig, ptr(e), ptr(P), ptr(Cm))
+    return e[0], P.reshape(3, 3), Cm.reshape(9, 9)
+
+
+def ref_material(kind, mu, lam, F, project=False, psd=1):
+    """The reference's own StVK (kind 1) / linear-elastic (kind 2) response."""
+    F = np.ascontiguousarray(F, np.float64).reshape(9)
+    e = np.zeros(1)
+    P = np.zeros(9)
+    Cm = np.zeros(81)
+    ref().ref_material(int(kind), mu, lam, ptr(F), int(project), psd, ptr(e), ptr(P), ptr(Cm))
     return e[0], P.reshape(3, 3), Cm.reshape(9, 9)
 
 
@@ -212,6 +235,7 @@ class Scene:
         s.dN, s.vol = ptr(self.dN), ptr(self.vol)
         s.row_ptr, s.col, s.nnzb = ptr(self.row_ptr, _lp), ptr(self.col, _ip), nnzb
         s.mass = ptr(self.mass)
+        s.material = int(getattr(body, "material", 0))
         for k in range(3):
             s.gravity[k] = cfg.gravity[k]
         s.dt = cfg.dt

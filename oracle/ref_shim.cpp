@@ -10,7 +10,9 @@
 #include <mochi_core/elements/tetrahedral/finite_element.h>
 #include <mochi_core/linear_algebra/krylov/pcg.h>
 #include <mochi_core/linear_algebra/matrix.h>
+#include <mochi_core/materials/batched_linear_elastic.h>
 #include <mochi_core/materials/batched_smith_neo_hookean.h>
+#include <mochi_core/materials/batched_st_venant_kirchhoff.h>
 #include <mochi_core/solvers/krylov_solver.h>
 #include <mochi_core/utils/activations.h>
 
@@ -52,6 +54,36 @@ void ref_smith_nh(double mu, double lambda, const double* F9, int project, int p
   NdArray<BatchReal3x3<1>, 3, 3> C{};
   materials::BatchedSmithNeoHookeanConstitutiveResponse<1>(
       p, F, &e, &pk1, &C, project != 0, static_cast<materials::MaterialPsdOracle>(oracle));
+  if (energy) *energy = Get0(e);
+  if (P9)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) P9[i * 3 + j] = Get0(pk1[i][j]);
+  if (C81)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        for (int k = 0; k < 3; ++k)
+          for (int l = 0; l < 3; ++l) C81[(i * 3 + j) * 9 + k * 3 + l] = Get0(C[i][j][k][l]);
+}
+
+// BatchedStVenantKirchhoffConstitutiveResponse<1> (mochi_core/src/materials/batched_st_venant_kirchhoff.cpp:29)
+// and BatchedLinearElasticConstitutiveResponse<1> (batched_linear_elastic.cpp:27); material 1 / 2 as in
+// SoftMaterialType.
+void ref_material(int material, double mu, double lambda, const double* F9, int project, int psd_strategy,
+                  double* energy, double* P9, double* C81) {
+  materials::BatchLameParams<1> p;
+  p.mu = BatchReal<1>{mu};
+  p.lambda = BatchReal<1>{lambda};
+  p.psdStrategy = ToStrategy(psd_strategy);
+  BatchReal3x3<1> F{};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) F[i][j] = BatchReal<1>{F9[i * 3 + j]};
+  BatchDouble<1> e{};
+  BatchReal3x3<1> pk1{};
+  NdArray<BatchReal3x3<1>, 3, 3> C{};
+  if (material == 1)
+    materials::BatchedStVenantKirchhoffConstitutiveResponse<1>(p, F, &e, &pk1, &C, project != 0);
+  else
+    materials::BatchedLinearElasticConstitutiveResponse<1>(p, F, &e, &pk1, &C, project != 0);
   if (energy) *energy = Get0(e);
   if (P9)
     for (int i = 0; i < 3; ++i)

@@ -173,6 +173,113 @@ void or_smith_nh(double mu, double lambda, const double F[9], int project, int p
   }
 }
 
+/* Clamp the 9 eigenvalues of a symmetric tangent: max(l, eps) (Projection) or max(|l|, eps). */
+static void or_project_tangent(double C[81], int abs_eig, double min_eig) {
+  double A[81], V[81], lam[9];
+  memcpy(A, C, sizeof(A));
+  jacobi_eig(9, A, V);
+  for (int i = 0; i < 9; ++i) {
+    double l = A[i * 9 + i];
+    if (abs_eig) l = fabs(l);
+    lam[i] = l > min_eig ? l : min_eig;
+  }
+  for (int a = 0; a < 9; ++a)
+    for (int b = 0; b < 9; ++b) {
+      double s = 0.0;
+      for (int i = 0; i < 9; ++i) s += V[a * 9 + i] * lam[i] * V[b * 9 + i];
+      C[a * 9 + b] = s;
+    }
+}
+
+void or_stvk(double mu, double lambda, const double F[9], int project, int psd_strategy, double min_eig,
+             double* energy, double P[9], double C[81]) {
+  /* Green strain, batched_st_venant_kirchhoff.cpp:53-63 */
+  double G[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double g = 0.0;
+      for (int k = 0; k < 3; ++k) g += F[k * 3 + i] * F[k * 3 + j];
+      G[i * 3 + j] = 0.5 * (g - (i == j ? 1.0 : 0.0));
+    }
+  double trG = G[0] + G[4] + G[8];
+  if (energy) {
+    double n2 = 0.0;
+    for (int i = 0; i < 9; ++i) n2 += G[i] * G[i];
+    *energy = mu * n2 + 0.5 * lambda * trG * trG;
+  }
+  if (P) {
+    double S[9];
+    for (int i = 0; i < 9; ++i) S[i] = 2.0 * mu * G[i];
+    for (int i = 0; i < 3; ++i) S[i * 4] += lambda * trG;
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) {
+        double v = 0.0;
+        for (int m = 0; m < 3; ++m) v += F[r * 3 + m] * S[m * 3 + c];
+        P[r * 3 + c] = v;
+      }
+  }
+  if (!C) return;
+  const int eigen = project && (psd_strategy == OR_PSD_PROJECTION || psd_strategy == OR_PSD_ABS_EIGEN);
+  if (project && psd_strategy == OR_PSD_FAST) { /* :158-169 */
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) G[i * 3 + j] = (i == j) ? (G[i * 4] > 0.0 ? G[i * 4] : 0.0) : 0.0;
+    trG = G[0] + G[4] + G[8];
+  }
+  double S[9], FFt[9];
+  for (int i = 0; i < 9; ++i) S[i] = 2.0 * mu * G[i];
+  for (int i = 0; i < 3; ++i) S[i * 4] += lambda * trG;
+  for (int r = 0; r < 3; ++r)
+    for (int i = 0; i < 3; ++i) {
+      double v = 0.0;
+      for (int k = 0; k < 3; ++k) v += F[r * 3 + k] * F[i * 3 + k];
+      FFt[r * 3 + i] = v;
+    }
+  /* dP_rc/dF_ij = delta_ri S_jc + mu F_rj F_ic + mu delta_jc (F F^T)_ri + lambda F_ij F_rc (:171-197) */
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c)
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          double v = mu * F[r * 3 + j] * F[i * 3 + c] + lambda * F[i * 3 + j] * F[r * 3 + c];
+          if (r == i) v += S[j * 3 + c];
+          if (j == c) v += mu * FFt[r * 3 + i];
+          C[(r * 3 + c) * 9 + (i * 3 + j)] = v;
+        }
+  if (eigen) or_project_tangent(C, psd_strategy == OR_PSD_ABS_EIGEN, min_eig); /* :96-154 */
+}
+
+void or_linear_elastic(double mu, double lambda, const double F[9], double* energy, double P[9], double C[81]) {
+  double e[9];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) e[r * 3 + c] = 0.5 * (F[r * 3 + c] + F[c * 3 + r]) - (r == c ? 1.0 : 0.0);
+  const double tr = e[0] + e[4] + e[8];
+  if (energy) {
+    double n2 = 0.0;
+    for (int i = 0; i < 9; ++i) n2 += e[i] * e[i];
+    *energy = mu * n2 + 0.5 * lambda * tr * tr;
+  }
+  if (P) {
+    for (int i = 0; i < 9; ++i) P[i] = 2.0 * mu * e[i];
+    for (int i = 0; i < 3; ++i) P[i * 4] += lambda * tr;
+  }
+  if (C) /* dP_rc/dF_ij = mu (d_ri d_cj + d_ci d_rj) + lambda d_rc d_ij (:72-94) */
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c)
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j)
+            C[(r * 3 + c) * 9 + (i * 3 + j)] =
+                mu * ((r == i && c == j) + (c == i && r == j)) + lambda * (r == c && i == j);
+}
+
+void or_material(int material, double mu, double lambda, const double F[9], int project, int psd_strategy,
+                 double min_eig, double* energy, double P[9], double C[81]) {
+  if (material == OR_MAT_STVK)
+    or_stvk(mu, lambda, F, project, psd_strategy, min_eig, energy, P, C);
+  else if (material == OR_MAT_LINEAR)
+    or_linear_elastic(mu, lambda, F, energy, P, C);
+  else
+    or_smith_nh(mu, lambda, F, project, psd_strategy, min_eig, energy, P, C);
+}
+
 /* ------------------------------------------------------------------------------------------- */
 /* contact                                                                                      */
 
@@ -505,7 +612,7 @@ int64_t or_assemble(const or_scene* s, const double* u, const double* ut, double
         for (int c = 0; c < 3; ++c) F[r * 3 + c] += uf[r] * dN[3 * f + c];
     }
     double Psi, P[9], C[81];
-    or_smith_nh(s->mu[e], s->lambda[e], F, project, s->psd_strategy, s->min_eig,
+    or_material(s->material, s->mu[e], s->lambda[e], F, project, s->psd_strategy, s->min_eig,
                 want_obj ? &Psi : NULL, want_res ? P : NULL, want_hess ? C : NULL);
     const double rho = s->rho[e];
     /* inertia acceleration a_f = u_f - ut_f, consistent mass M_fg = rho w (1 + d_fg) / 20 */

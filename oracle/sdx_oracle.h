@@ -36,6 +36,26 @@ enum { OR_PSD_NONE = 0, OR_PSD_PROJECTION = 1, OR_PSD_ABS_EIGEN = 2, OR_PSD_FAST
 void or_smith_nh(double mu, double lambda, const double F[9], int project, int psd_strategy,
                  double min_eig, double* energy, double P[9], double C[81]);
 
+/* Soft materials, same values as SoftMaterialType (mochi_core/.../materials/material_types.h:148-172). */
+enum { OR_MAT_NEO_HOOKEAN = 0, OR_MAT_STVK = 1, OR_MAT_LINEAR = 2 };
+
+/* St. Venant-Kirchhoff: psi = mu |G|^2 + lambda/2 tr(G)^2 with G = (F^T F - I)/2; P = F S,
+ * S = 2 mu G + lambda tr(G) I. Follows mochi_core/src/materials/batched_st_venant_kirchhoff.cpp:29-203:
+ * Projection / AbsEigenProjection clamp the 9 tangent eigenvalues (always: no definiteness test); Fast
+ * keeps only the non-negative stretches of G (no shear) inside the tangent's S. Same layout as
+ * or_smith_nh. */
+void or_stvk(double mu, double lambda, const double F[9], int project, int psd_strategy, double min_eig,
+             double* energy, double P[9], double C[81]);
+
+/* Linear elasticity: eps = (F + F^T)/2 - I, psi = mu eps:eps + lambda/2 tr(eps)^2,
+ * P = 2 mu eps + lambda tr(eps) I, constant PSD tangent (no projection).
+ * mochi_core/src/materials/batched_linear_elastic.cpp:25-97. */
+void or_linear_elastic(double mu, double lambda, const double F[9], double* energy, double P[9], double C[81]);
+
+/* Dispatch on OR_MAT_*. */
+void or_material(int material, double mu, double lambda, const double F[9], int project, int psd_strategy,
+                 double min_eig, double* energy, double P[9], double C[81]);
+
 /* (E, nu) -> (lambda, mu). mochi_core/.../materials/material_utils.h:331-339. */
 void or_lame(double E, double nu, double* lambda, double* mu);
 
@@ -104,6 +124,8 @@ typedef struct {
   int n_colliders;
   const or_collider* colliders;
   double k_contact, t_half, thr, max_align;
+  /* material (OR_MAT_*) of every tet of the body */
+  int material;
 } or_scene;
 
 /* Consistent P1 mass coupling per block (Q4 quadrature, exact for P1): m_ij = sum_t rho V (1+d_ij)/20.

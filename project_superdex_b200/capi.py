@@ -21,12 +21,13 @@ SDX_PREC_NONE, SDX_PREC_JACOBI, SDX_PREC_BLOCK_JACOBI = 0, 1, 2
 SDX_WARM_ZERO, SDX_WARM_PREVIOUS, SDX_WARM_LEARNED, SDX_WARM_TEMPORAL = 0, 1, 2, 3
 SDX_LINEAR_CONVERGED, SDX_LINEAR_STOPPED, SDX_LINEAR_DIVERGED = 1, 2, 3
 SDX_SOLVER_FUSED, SDX_SOLVER_PLAIN_FP64 = 0, 1
+SDX_MAT_NEO_HOOKEAN, SDX_MAT_ST_VENANT_KIRCHHOFF, SDX_MAT_LINEAR_ELASTIC = 0, 1, 2
 
 # every entry point include/sdx_b200.h declares
 EXPORTED = [
     "sdx_last_error", "sdx_version", "sdx_default_step_params", "sdx_default_linear_params",
     "sdx_pcg_solve", "sdx_pcg_solve_ctx", "sdx_create", "sdx_destroy", "sdx_upload_bodies",
-    "sdx_set_colliders", "sdx_set_params", "sdx_set_state", "sdx_get_state", "sdx_get_sizes",
+    "sdx_set_colliders", "sdx_set_materials", "sdx_set_params", "sdx_set_state", "sdx_get_state", "sdx_get_sizes",
     "sdx_get_pattern", "sdx_get_faces", "sdx_assemble", "sdx_get_contact_pairs", "sdx_step",
     "sdx_get_stats", "sdx_bench_spmv", "sdx_kernel_launches", "sdx_get_stream",
     "sdx_set_profiling", "sdx_get_profile", "sdx_pcg_solve_device_noalloc", "sdx_mlp_init",
@@ -112,6 +113,7 @@ def lib():
     L.sdx_destroy.argtypes = [_vp]
     L.sdx_upload_bodies.argtypes = [_vp, C.c_int, _lp, _lp, _dp, _ip, _dp, _dp, _dp, _up]
     L.sdx_set_colliders.argtypes = [_vp, C.c_int, _ip, _dp]
+    L.sdx_set_materials.argtypes = [_vp, C.c_int, _ip]
     L.sdx_set_params.argtypes = [_vp, C.POINTER(StepParams)]
     L.sdx_set_state.argtypes = [_vp, _dp, _dp, C.c_double]
     L.sdx_get_state.argtypes = [_vp, _dp, _dp, _dp]

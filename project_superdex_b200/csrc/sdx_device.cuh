@@ -225,6 +225,60 @@ __device__ __forceinline__ void svd3_rv(const float F[9], float U[9], float s[3]
 }
 
 // ------------------------------------------------------------------------------------------------
+// Projected tangent of an isotropic energy from its analytic eigensystem (Smith et al. 2018; Kim and
+// Eberle, "Analytic Eigensystems for Isotropic Distortion Energies"): F = U diag(s) V^T; the 9 modes are
+// the 3 scaling modes U diag(q_i) V^T (q_i the eigenvectors of the 3x3 scaling matrix A), the twists
+// (u_j v_k^T - u_k v_j^T)/sqrt(2) and the flips (u_j v_k^T + u_k v_j^T)/sqrt(2) for the pairs
+// (j,k) = (1,2), (0,2), (0,1). Eigenvalues are clamped at min_eig (psd 1) or |l| then min_eig (psd 2).
+
+__device__ __forceinline__ void modal_tangent_f32(const float U[9], const float V[9], const float A[9],
+                                                  const float tw[3], const float fl[3], int psd, float min_eig,
+                                                  float C[81]) {
+  float wa[3], Va[9];
+  sym_eig3(A, wa, Va);
+  float lam[9] = {wa[0], wa[1], wa[2], tw[0], tw[1], tw[2], fl[0], fl[1], fl[2]};
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    float l = (psd == 2) ? fabsf(lam[i]) : lam[i];
+    lam[i] = fmaxf(l, min_eig);
+  }
+  float M[9][9];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        M[i][r * 3 + c] = U[r * 3 + 0] * Va[0 * 3 + i] * V[c * 3 + 0] + U[r * 3 + 1] * Va[1 * 3 + i] * V[c * 3 + 1] +
+                          U[r * 3 + 2] * Va[2 * 3 + i] * V[c * 3 + 2];
+  const float rs2 = 0.70710678118654752f;
+#pragma unroll
+  for (int n = 0; n < 3; ++n) {
+    const int j = (n == 0) ? 1 : 0;
+    const int k = (n == 2) ? 1 : 2;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float a = U[r * 3 + j] * V[c * 3 + k];
+        const float b = U[r * 3 + k] * V[c * 3 + j];
+        M[3 + n][r * 3 + c] = (a - b) * rs2;
+        M[6 + n][r * 3 + c] = (a + b) * rs2;
+      }
+  }
+#pragma unroll
+  for (int a = 0; a < 9; ++a)
+#pragma unroll
+    for (int b = a; b < 9; ++b) {
+      float v = 0.0f;
+#pragma unroll
+      for (int i = 0; i < 9; ++i) v = fmaf(lam[i] * M[i][a], M[i][b], v);
+      C[a * 9 + b] = v;
+      C[b * 9 + a] = v;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
 // FP32 tangent dP/dF (9x9, symmetric, full storage C[a*9+b]) with the reference's PSD handling.
 // psd: 0 none, 1 projection (max(l, eps)), 2 |l| projection, 3 fast (drop d2J when indefinite).
 
@@ -268,13 +322,13 @@ __device__ __forceinline__ void snh_tangent_f32(float mu, float lambda, const fl
     svd3_rv(F, U, s, V);
     const float coeff0 = muHat - muHat * IcPlus1Inv;
     const float coeff1 = lambdaHat * Jma;
-    float lam[9];
-    lam[3] = coeff1 * s[0] + coeff0;  // twist, pair (1,2)
-    lam[4] = coeff1 * s[1] + coeff0;  // twist, pair (0,2)
-    lam[5] = coeff1 * s[2] + coeff0;  // twist, pair (0,1)
-    lam[6] = -coeff1 * s[0] + coeff0; // flip
-    lam[7] = -coeff1 * s[1] + coeff0;
-    lam[8] = -coeff1 * s[2] + coeff0;
+    float tw[3], fl[3];
+    tw[0] = coeff1 * s[0] + coeff0;  // twist, pair (1,2)
+    tw[1] = coeff1 * s[1] + coeff0;  // twist, pair (0,2)
+    tw[2] = coeff1 * s[2] + coeff0;  // twist, pair (0,1)
+    fl[0] = -coeff1 * s[0] + coeff0; // flip
+    fl[1] = -coeff1 * s[1] + coeff0;
+    fl[2] = -coeff1 * s[2] + coeff0;
     const float Ic2inv = IcPlus1Inv * IcPlus1Inv;
     const float mu2 = 2.0f * muHat;
     const float J2al = (2.0f * J - alpha) * lambdaHat;
@@ -286,52 +340,7 @@ __device__ __forceinline__ void snh_tangent_f32(float mu, float lambda, const fl
     A[1] = A[3] = J2al * s[2] + mu2 * s[0] * s[1] * Ic2inv;
     A[2] = A[6] = J2al * s[1] + mu2 * s[0] * s[2] * Ic2inv;
     A[5] = A[7] = J2al * s[0] + mu2 * s[1] * s[2] * Ic2inv;
-    float wa[3], Va[9];
-    sym_eig3(A, wa, Va);
-    lam[0] = wa[0];
-    lam[1] = wa[1];
-    lam[2] = wa[2];
-#pragma unroll
-    for (int i = 0; i < 9; ++i) {
-      float l = (psd == 2) ? fabsf(lam[i]) : lam[i];
-      lam[i] = fmaxf(l, min_eig);
-    }
-    // modes as 9-vectors: Q_i = U diag(a_i) V^T, T_n / L_n = (u_j v_k^T -/+ u_k v_j^T) / sqrt(2)
-    float M[9][9];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-      for (int r = 0; r < 3; ++r)
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-          M[i][r * 3 + c] = U[r * 3 + 0] * Va[0 * 3 + i] * V[c * 3 + 0] +
-                            U[r * 3 + 1] * Va[1 * 3 + i] * V[c * 3 + 1] +
-                            U[r * 3 + 2] * Va[2 * 3 + i] * V[c * 3 + 2];
-    const float rs2 = 0.70710678118654752f;
-#pragma unroll
-    for (int n = 0; n < 3; ++n) {
-      const int j = (n == 0) ? 1 : 0;
-      const int k = (n == 2) ? 1 : 2;
-#pragma unroll
-      for (int r = 0; r < 3; ++r)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const float a = U[r * 3 + j] * V[c * 3 + k];
-          const float b = U[r * 3 + k] * V[c * 3 + j];
-          M[3 + n][r * 3 + c] = (a - b) * rs2;
-          M[6 + n][r * 3 + c] = (a + b) * rs2;
-        }
-    }
-#pragma unroll
-    for (int a = 0; a < 9; ++a)
-#pragma unroll
-      for (int b = a; b < 9; ++b) {
-        float v = 0.0f;
-#pragma unroll
-        for (int i = 0; i < 9; ++i) v = fmaf(lam[i] * M[i][a], M[i][b], v);
-        C[a * 9 + b] = v;
-        C[b * 9 + a] = v;
-      }
+    modal_tangent_f32(U, V, A, tw, fl, psd, min_eig, C);
     return;
   }
 
@@ -349,6 +358,139 @@ __device__ __forceinline__ void snh_tangent_f32(float mu, float lambda, const fl
       C[a * 9 + b] = v;
       C[b * 9 + a] = v;
     }
+}
+
+// ------------------------------------------------------------------------------------------------
+// St. Venant-Kirchhoff (mochi_core/src/materials/batched_st_venant_kirchhoff.cpp:29-203) and linear
+// elasticity (batched_linear_elastic.cpp:25-97): FP64 energy and PK1, FP32 tangent.
+
+__device__ __forceinline__ void stvk_green(const double F[9], double G[9]) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      G[i * 3 + j] = 0.5 * (F[i] * F[j] + F[3 + i] * F[3 + j] + F[6 + i] * F[6 + j] - (i == j ? 1.0 : 0.0));
+}
+
+// psi = mu |G|^2 + lambda/2 tr(G)^2 ; P = F (2 mu G + lambda tr(G) I)
+__device__ __forceinline__ void stvk_energy_pk1_f64(double mu, double lambda, const double F[9], double* energy,
+                                                    double P[9]) {
+  double G[9];
+  stvk_green(F, G);
+  const double trG = G[0] + G[4] + G[8];
+  if (energy) {
+    double n2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) n2 += G[i] * G[i];
+    *energy = mu * n2 + 0.5 * lambda * trG * trG;
+  }
+  if (P) {
+    double S[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) S[i] = 2.0 * mu * G[i] + ((i % 4 == 0) ? lambda * trG : 0.0);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        P[r * 3 + c] = F[r * 3 + 0] * S[c] + F[r * 3 + 1] * S[3 + c] + F[r * 3 + 2] * S[6 + c];
+  }
+}
+
+__device__ __forceinline__ void stvk_tangent_f32(float mu, float lambda, const float F[9], int project, int psd,
+                                                 float min_eig, float C[81]) {
+  if (project && (psd == 1 || psd == 2)) {
+    // eigensystem (batched_st_venant_kirchhoff.cpp:96-154): base = -mu + lambda (I2 - 3) / 2
+    float U[9], s[3], V[9];
+    svd3_rv(F, U, s, V);
+    const float s0 = s[0] * s[0], s1 = s[1] * s[1], s2 = s[2] * s[2];
+    const float base = -mu + 0.5f * lambda * (s0 + s1 + s2 - 3.0f);
+    float tw[3], fl[3];
+    tw[0] = base + mu * (s1 + s2 - s[1] * s[2]);
+    tw[1] = base + mu * (s0 + s2 - s[0] * s[2]);
+    tw[2] = base + mu * (s0 + s1 - s[0] * s[1]);
+    fl[0] = base + mu * (s1 + s2 + s[1] * s[2]);
+    fl[1] = base + mu * (s0 + s2 + s[0] * s[2]);
+    fl[2] = base + mu * (s0 + s1 + s[0] * s[1]);
+    const float dc = lambda + 3.0f * mu;
+    float A[9];
+    A[0] = base + dc * s0;
+    A[4] = base + dc * s1;
+    A[8] = base + dc * s2;
+    A[1] = A[3] = lambda * s[0] * s[1];
+    A[2] = A[6] = lambda * s[0] * s[2];
+    A[5] = A[7] = lambda * s[1] * s[2];
+    modal_tangent_f32(U, V, A, tw, fl, psd, min_eig, C);
+    return;
+  }
+  // direct tangent dP_rc/dF_ij = delta_ri S_jc + mu F_rj F_ic + mu delta_jc (F F^T)_ri + lambda F_ij F_rc
+  // (:156-197); Fast (psd 3) keeps only the non-negative stretches of G inside S
+  float G[9];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      G[i * 3 + j] = 0.5f * (F[i] * F[j] + F[3 + i] * F[3 + j] + F[6 + i] * F[6 + j] - (i == j ? 1.0f : 0.0f));
+  if (project && psd == 3) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) G[i] = (i % 4 == 0) ? fmaxf(G[i], 0.0f) : 0.0f;
+  }
+  const float trG = G[0] + G[4] + G[8];
+  float S[9], FFt[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) S[i] = 2.0f * mu * G[i] + ((i % 4 == 0) ? lambda * trG : 0.0f);
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      FFt[r * 3 + i] = F[r * 3 + 0] * F[i * 3 + 0] + F[r * 3 + 1] * F[i * 3 + 1] + F[r * 3 + 2] * F[i * 3 + 2];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          float v = mu * F[r * 3 + j] * F[i * 3 + c] + lambda * F[i * 3 + j] * F[r * 3 + c];
+          if (r == i) v += S[j * 3 + c];
+          if (j == c) v += mu * FFt[r * 3 + i];
+          C[(r * 3 + c) * 9 + (i * 3 + j)] = v;
+        }
+}
+
+// eps = (F + F^T)/2 - I ; psi = mu eps:eps + lambda/2 tr(eps)^2 ; P = 2 mu eps + lambda tr(eps) I
+__device__ __forceinline__ void linear_energy_pk1_f64(double mu, double lambda, const double F[9], double* energy,
+                                                      double P[9]) {
+  double e[9];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) e[r * 3 + c] = 0.5 * (F[r * 3 + c] + F[c * 3 + r]) - (r == c ? 1.0 : 0.0);
+  const double tr = e[0] + e[4] + e[8];
+  if (energy) {
+    double n2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) n2 += e[i] * e[i];
+    *energy = mu * n2 + 0.5 * lambda * tr * tr;
+  }
+  if (P) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) P[i] = 2.0 * mu * e[i] + ((i % 4 == 0) ? lambda * tr : 0.0);
+  }
+}
+
+// constant, PSD: dP_rc/dF_ij = mu (d_ri d_cj + d_ci d_rj) + lambda d_rc d_ij
+__device__ __forceinline__ void linear_tangent_f32(float mu, float lambda, float C[81]) {
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          C[(r * 3 + c) * 9 + (i * 3 + j)] = mu * (float)((r == i && c == j) + (c == i && r == j)) +
+                                             lambda * (float)(r == c && i == j);
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -201,6 +201,7 @@ struct sdx_context {
   double* env_scale = nullptr;
   double* env_obj = nullptr;
   uint8_t* env_mask = nullptr;
+  uint8_t* env_material = nullptr;  // SDX_MAT_* per env (zero: Smith Neo-Hookean)
   unsigned long long* env_pairs = nullptr;
   unsigned* pair_mask = nullptr;
   std::vector<sdx_env_stats> stats;
@@ -349,6 +350,7 @@ static void release_topology(sdx_context* c) {
   dfree(c->env_scale);
   dfree(c->env_obj);
   dfree(c->env_mask);
+  dfree(c->env_material);
   dfree(c->env_pairs);
   dfree(c->pair_mask);
   c->part.release();
@@ -1218,6 +1220,8 @@ extern "C" int sdx_upload_bodies(sdx_context* c, int n_envs, const int64_t* node
   SDX_TRY(dalloc(&c->env_scale, n_envs));
   SDX_TRY(dalloc(&c->env_obj, n_envs));
   SDX_TRY(dalloc(&c->env_mask, n_envs));
+  SDX_TRY(dalloc(&c->env_material, n_envs));
+  SDX_CUDA(cudaMemset(c->env_material, 0, n_envs));
   SDX_TRY(dalloc(&c->env_pairs, n_envs));
   SDX_TRY(dalloc(&c->pair_mask, 3 * c->n_faces));
   SDX_CUDA(cudaMemset(c->pair_mask, 0, sizeof(unsigned) * 3 * std::max<int64_t>(1, c->n_faces)));
@@ -1243,6 +1247,21 @@ extern "C" int sdx_upload_bodies(sdx_context* c, int n_envs, const int64_t* node
   c->time = 0.0;
   SDX_CUDA(cudaStreamSynchronize(c->stream));
   c->uploaded = true;
+  return SDX_OK;
+}
+
+extern "C" int sdx_set_materials(sdx_context* c, int n_envs, const int32_t* material) {
+  if (!c || !material) return set_error(SDX_ERR_INVALID_ARGUMENT, "null argument");
+  if (!c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
+  if (n_envs != c->n_envs) return set_error(SDX_ERR_INVALID_ARGUMENT, "expected %d materials", c->n_envs);
+  std::vector<uint8_t> m(n_envs);
+  for (int e = 0; e < n_envs; ++e) {
+    if (material[e] < SDX_MAT_NEO_HOOKEAN || material[e] > SDX_MAT_LINEAR_ELASTIC)
+      return set_error(SDX_ERR_INVALID_ARGUMENT, "env %d: unknown material %d", e, material[e]);
+    m[e] = (uint8_t)material[e];
+  }
+  cudaSetDevice(c->device);
+  SDX_CUDA(cudaMemcpy(c->env_material, m.data(), n_envs, cudaMemcpyHostToDevice));
   return SDX_OK;
 }
 
@@ -1361,6 +1380,7 @@ static void assemble_dev(sdx_context* c, const double* u, const double* ut, doub
   ea.slots3 = c->slots[3];
   ea.slice_env = c->slice_env;
   ea.env_mask = mask;
+  ea.env_material = c->env_material;
   ea.u = u;
   ea.ut = ut;
   ea.X = c->X;

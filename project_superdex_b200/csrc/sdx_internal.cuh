@@ -51,7 +51,8 @@ struct ElemArgs {
   const int4* slots2;
   const int4* slots3;
   const int* slice_env;
-  const uint8_t* env_mask;  // NULL = all
+  const uint8_t* env_mask;      // NULL = all
+  const uint8_t* env_material;  // per env: 0 Smith Neo-Hookean, 1 St. Venant-Kirchhoff, 2 linear (NULL: 0)
   const double* u;
   const double* ut;
   const double* X;

@@ -103,6 +103,7 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
   const int4 nd = a.tets[t];
   const int env = a.slice_env[nd.x >> 5];
   if (a.env_mask && !a.env_mask[env]) return;
+  const int mat = a.env_material ? a.env_material[env] : 0;
   const float4 R0 = a.rest0[t], R1 = a.rest1[t], R2 = a.rest2[t], R3 = a.rest3[t];
   const float dN[12] = {R0.x, R0.y, R0.z, R0.w, R1.x, R1.y, R1.z, R1.w, R2.x, R2.y, R2.z, R2.w};
   const float vol = R3.x, mu = R3.y, lam = R3.z, rho = R3.w;
@@ -135,7 +136,12 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
       }
     if (want_res) {
       double P[9];
-      snh_pk1_f64(kc, F, P);
+      if (mat == 1)
+        stvk_energy_pk1_f64((double)mu, (double)lam, F, nullptr, P);
+      else if (mat == 2)
+        linear_energy_pk1_f64((double)mu, (double)lam, F, nullptr, P);
+      else
+        snh_pk1_f64(kc, F, P);
 #pragma unroll
       for (int f = 0; f < 4; ++f) {
         const int pf = a.pin[rows[f]];
@@ -164,7 +170,14 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
         for (int f = 0; f < 4; ++f) sq += acc[f][r] * acc[f][r];
         ein += m * (sq + asum[r] * asum[r]);
       }
-      const double e = snh_energy_f64(kc, F) * w -
+      double psi;
+      if (mat == 1)
+        stvk_energy_pk1_f64((double)mu, (double)lam, F, &psi, nullptr);
+      else if (mat == 2)
+        linear_energy_pk1_f64((double)mu, (double)lam, F, &psi, nullptr);
+      else
+        psi = snh_energy_f64(kc, F);
+      const double e = psi * w -
                        (double)rho * w * (a.grav[0] * xc[0] + a.grav[1] * xc[1] + a.grav[2] * xc[2]) +
                        0.5 * a.dtfi2 * ein;
       warp_env_add(a.obj, env, e);
@@ -176,7 +189,12 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
 #pragma unroll
     for (int i = 0; i < 9; ++i) Ff[i] = (float)F[i];
     float C[81];
-    snh_tangent_f32(mu, lam, Ff, (a.flags & 8) != 0, a.psd, a.min_eig, C);
+    if (mat == 1)
+      stvk_tangent_f32(mu, lam, Ff, (a.flags & 8) != 0, a.psd, a.min_eig, C);
+    else if (mat == 2)
+      linear_tangent_f32(mu, lam, C);
+    else
+      snh_tangent_f32(mu, lam, Ff, (a.flags & 8) != 0, a.psd, a.min_eig, C);
     const int4 S0 = a.slots0[t], S1 = a.slots1[t], S2 = a.slots2[t], S3 = a.slots3[t];
     const int slot[16] = {S0.x, S0.y, S0.z, S0.w, S1.x, S1.y, S1.z, S1.w,
                           S2.x, S2.y, S2.z, S2.w, S3.x, S3.y, S3.z, S3.w};

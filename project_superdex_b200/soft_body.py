@@ -44,6 +44,9 @@ class SoftBodyWorld:
                 rows.append(c.as_row())
                 envs.append(e)
         self.n_colliders = len(rows)
+        mats = np.asarray([int(getattr(b, "material", 0)) for b in self.bodies], np.int32)
+        if np.any(mats != 0):
+            capi.check(L.sdx_set_materials(self._ctx, self.n_envs, capi.ptr(mats, capi._ip)))
         if rows:
             R = np.ascontiguousarray(np.stack(rows))
             E = np.asarray(envs, np.int32)

@@ -4,11 +4,14 @@ exists; the fixtures are committed, nothing reads the reference at test time).
   * smith_nh_reference.json — the 5 Smith Neo-Hookean known-answer cases of the reference test suite
     (mochi_core/test/data/material_test_data.h, smith_neo_hookean_test_data, E = 1, nu = 0.4), read
     as text from the header.
+  * stvk_reference.json — the 6 St. Venant-Kirchhoff known-answer cases of the same header
+    (st_venant_kirchhoff_test_data, E = 1, nu = 0.4).
   * krylov_psd100.json — the reference's 100 x 100 SPD golden system (matrix, rhs, solution) from
     mochi_core/test/data/krylov_solver_test_data.h, read as text.
   * reference_vectors.json — outputs of the reference's own compiled code (oracle/_ref, built by
     oracle/build_ref.sh from the reference sources) on seeded inputs: Smith NH with every PSD
-    strategy (projected tangents), PolyReLU, the penalty contact response, fem::StressWork on single
+    strategy (projected tangents), St. Venant-Kirchhoff and linear elasticity with every PSD strategy,
+    PolyReLU, the penalty contact response, fem::StressWork on single
     tets, and krylov::PCG iteration counts / solutions on the two golden systems.
 
   python tests/golden/make_golden.py [--reference-root /path/to/reference]
@@ -45,6 +48,22 @@ def parse_smith(path):
             "cases": cases}
 
 
+def parse_stvk(path):
+    """The St. Venant-Kirchhoff known-answer cases (st_venant_kirchhoff_test_data, E = 1, nu = 0.4)."""
+    text = open(path).read()
+    start = text.index("namespace st_venant_kirchhoff_test_data")
+    end = text.index("} // namespace st_venant_kirchhoff_test_data")
+    block = text[start:end]
+    cases = []
+    for chunk in re.split(r"\bTestData\{", block)[1:]:
+        nums = [float(x) for x in re.findall(NUM + r"(?=_r)", chunk)]
+        energy = float(re.search(r"\.strainEnergy\s*=\s*(" + NUM + ")", chunk).group(1))
+        assert len(nums) == 9 + 9 + 81, len(nums)
+        cases.append({"F": nums[0:9], "energy": energy, "pk1": nums[9:18], "tangent": nums[18:99]})
+    return {"youngs_modulus": 1.0, "poisson_ratio": 0.4, "source": "material_test_data.h st_venant_kirchhoff block",
+            "cases": cases}
+
+
 def parse_array(text, name, kind=float):
     m = re.search(name + r"\[\]\s*=\s*\{(.*?)\};", text, re.S)
     vals = re.findall(NUM, m.group(1))
@@ -74,7 +93,7 @@ def reference_vectors():
     R = O.ref()
     assert R is not None, "oracle/_ref/libsdx_ref.so missing: run oracle/build_ref.sh"
     rng = np.random.default_rng(20261203)
-    out = {"smith": [], "polyrelu": [], "penalty": [], "stress_work": [], "pcg": []}
+    out = {"smith": [], "polyrelu": [], "penalty": [], "stress_work": [], "pcg": [], "materials": []}
     for i in range(48):
         F = np.eye(3) + rng.normal(0, 0.35, (3, 3))
         if i % 4 == 0:
@@ -141,6 +160,19 @@ def reference_vectors():
                 out["pcg"].append({"system": name, "rel_tol": rel, "jacobi": jac, "iters": int(it),
                                    "convergence": int(cv.value), "res_norm": float(rn[0]),
                                    "rel_res_norm": float(rr[0]), "x": x.tolist()})
+    # St. Venant-Kirchhoff (1) and linear elasticity (2), every PSD strategy, inverted cases included
+    rng = np.random.default_rng(7)
+    for kind in (1, 2):
+        for t in range(12):
+            F = np.eye(3) + rng.normal(0.0, 0.35, (3, 3))
+            if t % 3 == 0:
+                F[:, 0] *= -0.6
+            mu, lam = float(rng.uniform(0.2, 2.0)), float(rng.uniform(0.5, 5.0))
+            for psd in (0, 1, 2, 3):
+                e, P, Cm = O.ref_material(kind, mu, lam, F, project=psd != 0, psd=psd)
+                out["materials"].append({"kind": kind, "mu": mu, "lambda": lam, "F": F.reshape(-1).tolist(),
+                                         "psd": psd, "energy": e, "pk1": P.reshape(-1).tolist(),
+                                         "tangent": Cm.reshape(-1).tolist()})
     out["source"] = "oracle/_ref/libsdx_ref.so (reference sources, FP64 build)"
     return out
 
@@ -153,6 +185,8 @@ def main():
     args_ns.mc = os.path.join(args_ns.reference_root, "superdex_physics/libraries/mochi/mochi_core")
     with open(os.path.join(HERE, "smith_nh_reference.json"), "w") as f:
         json.dump(parse_smith(os.path.join(args_ns.mc, "test/data/material_test_data.h")), f)
+    with open(os.path.join(HERE, "stvk_reference.json"), "w") as f:
+        json.dump(parse_stvk(os.path.join(args_ns.mc, "test/data/material_test_data.h")), f)
     with open(os.path.join(HERE, "krylov_psd100.json"), "w") as f:
         json.dump(parse_krylov(os.path.join(args_ns.mc, "test/data/krylov_solver_test_data.h")), f)
     with open(os.path.join(HERE, "reference_vectors.json"), "w") as f:

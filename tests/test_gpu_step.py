@@ -101,3 +101,12 @@ def test_autotuned_launch_shape_reaches_same_state(oracle, monkeypatch):
     w.set_profiling(True)
     assert w.profile()["pcg_threads"] in (384, 512, 768, 1024)
     _check(bodies, ug, states, hist)
+
+
+@pytest.mark.parametrize("material", [1, 2])
+def test_other_materials_steps_match_oracle(oracle, material):
+    """Newton steps of a St. Venant-Kirchhoff / linear-elastic body against the oracle."""
+    bodies, cfg = scenes.config0()
+    bodies[0].material = material
+    w, ug, vg, states, hist = _run(oracle, bodies, cfg, 3)
+    _check(bodies, ug, states, hist, newton_exact=False)

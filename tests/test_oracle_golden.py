@@ -19,6 +19,32 @@ def test_smith_nh_known_answers(oracle, golden):
         np.testing.assert_allclose(C.reshape(-1), c["tangent"], rtol=2e-5, atol=2e-6)
 
 
+def test_stvk_known_answers(oracle, golden):
+    """material_test_data.h st_venant_kirchhoff_test_data (E = 1, nu = 0.4), as batched_materials_test.cpp:240."""
+    g = golden("stvk_reference.json")
+    lam, mu = 1.0 * 0.4 / ((1 + 0.4) * (1 - 0.8)), 1.0 / (2 * 1.4)
+    assert len(g["cases"]) == 6
+    for c in g["cases"]:
+        e, P, C = oracle.material(1, mu, lam, np.array(c["F"]), project=False, psd=0)
+        assert e == pytest.approx(c["energy"], rel=2e-5, abs=1e-6)
+        np.testing.assert_allclose(P.reshape(-1), c["pk1"], rtol=2e-5, atol=2e-6)
+        np.testing.assert_allclose(C.reshape(-1), c["tangent"], rtol=2e-5, atol=2e-6)
+
+
+def test_stvk_and_linear_elastic_match_reference_code(oracle, golden):
+    """St. Venant-Kirchhoff and linear elasticity with every PSD strategy against the reference's own
+    compiled translation units (batched_st_venant_kirchhoff.cpp, batched_linear_elastic.cpp)."""
+    v = golden("reference_vectors.json")
+    assert len(v["materials"]) == 96
+    for c in v["materials"]:
+        e, P, C = oracle.material(c["kind"], c["mu"], c["lambda"], np.array(c["F"]), project=c["psd"] != 0,
+                                  psd=c["psd"])
+        scale = max(1.0, np.abs(c["tangent"]).max())
+        assert e == pytest.approx(c["energy"], rel=1e-11, abs=1e-11)
+        np.testing.assert_allclose(P.reshape(-1), c["pk1"], rtol=1e-11, atol=1e-11)
+        np.testing.assert_allclose(C.reshape(-1), c["tangent"], rtol=1e-9, atol=1e-10 * scale)
+
+
 def test_smith_nh_all_psd_strategies_match_reference_code(oracle, golden):
     v = golden("reference_vectors.json")
     assert len(v["smith"]) == 192
