@@ -120,6 +120,9 @@ typedef struct {
   double rel_div_tol, abs_div_tol;
   int warm_start;              /* SDX_WARM_* */
   sdx_linear_params linear;
+  double mass_damping;         /* Rayleigh mass damping coefficient alpha [1/s] (massDampingCoefficient):
+                                  adds alpha/dt * M (u - u_stage) to the residual and alpha/dt * M to the
+                                  Hessian (ComputeSoftDampingScales, mochi_physics/src/mochi_soft.h:274-290) */
 } sdx_step_params;
 
 /* Per-env statistics of the last step (StageSolverStats, mochi_physics/src/mochi_solve.cpp:1144). */

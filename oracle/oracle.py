@@ -42,7 +42,8 @@ class OrScene(C.Structure):
         ("min_eig", C.c_double),
         ("n_colliders", C.c_int), ("colliders", C.POINTER(OrCollider)),
         ("k_contact", C.c_double), ("t_half", C.c_double), ("thr", C.c_double),
-        ("max_align", C.c_double), ("material", C.c_int),
+        ("max_align", C.c_double), ("material", C.c_int), ("mass_damping", C.c_double),
+        ("u_stage", _dp),
     ]
 
 
@@ -236,6 +237,7 @@ class Scene:
         s.row_ptr, s.col, s.nnzb = ptr(self.row_ptr, _lp), ptr(self.col, _ip), nnzb
         s.mass = ptr(self.mass)
         s.material = int(getattr(body, "material", 0))
+        s.mass_damping = float(getattr(cfg, "mass_damping", 0.0))
         for k in range(3):
             s.gravity[k] = cfg.gravity[k]
         s.dt = cfg.dt
@@ -249,10 +251,12 @@ class Scene:
         self.nnzb = nnzb
         self.n_faces = nf
 
-    def assemble(self, u, ut, t=0.0, obj=True, res=True, hess=True, psd=True, pairs=False):
+    def assemble(self, u, ut, t=0.0, obj=True, res=True, hess=True, psd=True, pairs=False, u_stage=None):
         N = self.body.n_nodes
         u = np.ascontiguousarray(u, np.float64).reshape(-1)
         ut = np.ascontiguousarray(ut, np.float64).reshape(-1)
+        us = None if u_stage is None else np.ascontiguousarray(u_stage, np.float64).reshape(-1)
+        self.s.u_stage = ptr(us) if us is not None else None
         flags = (1 if obj else 0) | (2 if res else 0) | (4 if hess else 0) | (8 if psd else 0)
         o = np.zeros(1)
         g = np.zeros(3 * N)

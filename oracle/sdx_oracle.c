@@ -585,14 +585,15 @@ int64_t or_assemble(const or_scene* s, const double* u, const double* ut, double
             want_hess = flags & OR_ASM_HESS;
   const int project = (flags & OR_ASM_PSD) != 0;
   const double dt = s->dt, dtfi2 = 1.0 / (dt * dt);
+  const double dmp = s->mass_damping > 0.0 ? s->mass_damping / dt : 0.0; /* massDampingScale */
   double energy = 0.0;
   const int64_t N = s->n_nodes;
   if (want_res) memset(g, 0, sizeof(double) * 3 * (size_t)N);
   if (want_hess) {
-    /* DRes <- massScale * M (mochi_physics/src/mochi_soft.cpp:249-262), massScale = 1/dt^2. */
+    /* DRes <- massScale * M (mochi_physics/src/mochi_soft.cpp:249-262), massScale = 1/dt^2 + alpha/dt. */
     for (int64_t b = 0; b < s->nnzb; ++b) {
       double* blk = H + 9 * b;
-      double m = s->mass[b] * dtfi2;
+      double m = s->mass[b] * (dtfi2 + dmp);
       for (int k = 0; k < 9; ++k) blk[k] = 0.0;
       blk[0] = blk[4] = blk[8] = m;
     }
@@ -617,10 +618,13 @@ int64_t or_assemble(const or_scene* s, const double* u, const double* ut, double
     const double rho = s->rho[e];
     /* inertia acceleration a_f = u_f - ut_f, consistent mass M_fg = rho w (1 + d_fg) / 20 */
     double a[4][3], asum[3] = {0, 0, 0};
+    double dd[4][3], dsum[3] = {0, 0, 0}; /* mass damping: u - u_stage */
     for (int f = 0; f < 4; ++f)
       for (int r = 0; r < 3; ++r) {
         a[f][r] = u[3 * (int64_t)nd[f] + r] - ut[3 * (int64_t)nd[f] + r];
         asum[r] += a[f][r];
+        dd[f][r] = (dmp > 0.0 && s->u_stage) ? u[3 * (int64_t)nd[f] + r] - s->u_stage[3 * (int64_t)nd[f] + r] : 0.0;
+        dsum[r] += dd[f][r];
       }
     const double m = rho * w / 20.0;
     if (want_obj) {
@@ -628,15 +632,19 @@ int64_t or_assemble(const or_scene* s, const double* u, const double* ut, double
       for (int f = 0; f < 4; ++f)
         for (int r = 0; r < 3; ++r)
           xc[r] += 0.25 * (s->X[3 * (int64_t)nd[f] + r] + u[3 * (int64_t)nd[f] + r]);
-      double ein = 0.0;
+      double ein = 0.0, edm = 0.0;
       for (int r = 0; r < 3; ++r) {
-        double sq = 0.0;
-        for (int f = 0; f < 4; ++f) sq += a[f][r] * a[f][r];
+        double sq = 0.0, sd = 0.0;
+        for (int f = 0; f < 4; ++f) {
+          sq += a[f][r] * a[f][r];
+          sd += dd[f][r] * dd[f][r];
+        }
         ein += m * (sq + asum[r] * asum[r]);
+        edm += m * (sd + dsum[r] * dsum[r]);
       }
       energy += Psi * w - rho * w * (s->gravity[0] * xc[0] + s->gravity[1] * xc[1] +
                                      s->gravity[2] * xc[2]) +
-                0.5 * dtfi2 * ein;
+                0.5 * dtfi2 * ein + 0.5 * dmp * edm;
     }
     if (want_res) {
       for (int f = 0; f < 4; ++f)
@@ -646,6 +654,7 @@ int64_t or_assemble(const or_scene* s, const double* u, const double* ut, double
                      w;
           v -= rho * s->gravity[r] * w * 0.25;
           v += dtfi2 * m * (a[f][r] + asum[r]);
+          v += dmp * m * (dd[f][r] + dsum[r]);
           atomic_add(&g[3 * (int64_t)nd[f] + r], v);
         }
     }
@@ -919,16 +928,19 @@ void or_default_newton_params(or_newton_params* p) {
 
 static double norm2(int64_t n, const double* a) { return sqrt(dotv(n, a, a)); }
 
-or_newton_status or_step(const or_scene* s, double* u, double* v, double t,
+or_newton_status or_step(const or_scene* s_in, double* u, double* v, double t,
                          const or_newton_params* prm, const double* warm) {
-  const int64_t m = 3 * (int64_t)s->n_nodes;
+  const int64_t m = 3 * (int64_t)s_in->n_nodes;
   double* u0 = (double*)malloc(sizeof(double) * (size_t)m);
   double* ut = (double*)malloc(sizeof(double) * (size_t)m);
   double* g = (double*)malloc(sizeof(double) * (size_t)m);
   double* dx = (double*)malloc(sizeof(double) * (size_t)m);
   double* ubase = (double*)malloc(sizeof(double) * (size_t)m);
-  double* H = (double*)malloc(sizeof(double) * 9 * (size_t)s->nnzb);
+  double* H = (double*)malloc(sizeof(double) * 9 * (size_t)s_in->nnzb);
   memcpy(u0, u, sizeof(double) * (size_t)m);
+  or_scene sl = *s_in; /* the stage-start displacement of mass damping is this step's start */
+  sl.u_stage = u0;
+  const or_scene* s = &sl;
   /* x~ = x0 + dt v0 (GatherPredTarget, batched_element_utils.h:90-123) */
   for (int64_t i = 0; i < m; ++i) ut[i] = u0[i] + s->dt * v[i];
   or_newton_status st;

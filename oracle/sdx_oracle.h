@@ -126,6 +126,10 @@ typedef struct {
   double k_contact, t_half, thr, max_align;
   /* material (OR_MAT_*) of every tet of the body */
   int material;
+  /* Rayleigh mass damping alpha [1/s] about the stage-start displacement u_stage (3N; or_step sets it;
+   * NULL: the inertia-free terms are skipped) — mochi_physics/src/mochi_soft.h:274-290, 408-420 */
+  double mass_damping;
+  const double* u_stage;
 } or_scene;
 
 /* Consistent P1 mass coupling per block (Q4 quadrature, exact for P1): m_ij = sum_t rho V (1+d_ij)/20.

@@ -905,6 +905,7 @@ extern "C" int sdx_get_profile(sdx_context* c, sdx_profile* out) {
 extern "C" int sdx_set_params(sdx_context* c, const sdx_step_params* p) {
   if (!c || !p) return set_error(SDX_ERR_INVALID_ARGUMENT, "null argument");
   if (!(p->dt > 0.0)) return set_error(SDX_ERR_INVALID_ARGUMENT, "dt must be positive");
+  if (!(p->mass_damping >= 0.0)) return set_error(SDX_ERR_INVALID_ARGUMENT, "mass_damping must be >= 0");
   if (p->linear.preconditioner < 0 || p->linear.preconditioner > 2)
     return set_error(SDX_ERR_INVALID_ARGUMENT, "unknown preconditioner %d", p->linear.preconditioner);
   c->params = *p;
@@ -1362,7 +1363,9 @@ static void assemble_dev(sdx_context* c, const double* u, const double* ut, doub
   cudaEvent_t ev;
   if (flags & SDX_ASM_HESS) {
     prof_begin(c, &ev);
-    launch_seed_hessian(ctx_matrix(c), c->mass, c->pin, mask, (float)dtfi2, c->stream);
+    // massScale = 1/dt^2 + alpha/dt (ComputeSoftDampingScales, mochi_physics/src/mochi_soft.h:274-290)
+    const double mdamp = p.mass_damping > 0.0 ? p.mass_damping / p.dt : 0.0;
+    launch_seed_hessian(ctx_matrix(c), c->mass, c->pin, mask, (float)(dtfi2 + mdamp), c->stream);
     c->launches++;
     prof_end(c, PROF_SEED, ev);
   }
@@ -1383,6 +1386,8 @@ static void assemble_dev(sdx_context* c, const double* u, const double* ut, doub
   ea.env_material = c->env_material;
   ea.u = u;
   ea.ut = ut;
+  ea.u0 = c->u0;
+  ea.mdamp = p.mass_damping > 0.0 ? p.mass_damping / p.dt : 0.0;
   ea.X = c->X;
   ea.pin = c->pin;
   ea.g = c->g;

@@ -55,12 +55,14 @@ struct ElemArgs {
   const uint8_t* env_material;  // per env: 0 Smith Neo-Hookean, 1 St. Venant-Kirchhoff, 2 linear (NULL: 0)
   const double* u;
   const double* ut;
+  const double* u0;  // stage-start displacement (mass damping)
   const double* X;
   const uint8_t* pin;
   double* g;
   float* val;
   double* obj;  // per env
   double dtfi2;
+  double mdamp;  // mass damping scale alpha / dt (0: none)
   double grav[3];
   float min_eig;
   int psd;

@@ -127,12 +127,17 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
     const double w = (double)vol;
     const double m = (double)rho * w / 20.0;
     double acc[4][3], asum[3] = {0.0, 0.0, 0.0};
+    // mass damping (mochi_physics/src/mochi_soft.h:408-420): InertiaWork with scale alpha/dt about the
+    // stage-start displacement
+    double dmp[4][3], dsum[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int f = 0; f < 4; ++f)
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
         acc[f][r] = uf[f][r] - a.ut[3 * (int64_t)rows[f] + r];
         asum[r] += acc[f][r];
+        dmp[f][r] = a.mdamp > 0.0 ? uf[f][r] - a.u0[3 * (int64_t)rows[f] + r] : 0.0;
+        dsum[r] += dmp[f][r];
       }
     if (want_res) {
       double P[9];
@@ -152,6 +157,7 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
                       P[r * 3 + 2] * dN[3 * f + 2]) * w;
           v -= (double)rho * a.grav[r] * w * 0.25;
           v += a.dtfi2 * m * (acc[f][r] + asum[r]);
+          v += a.mdamp * m * (dmp[f][r] + dsum[r]);
           atomicAdd(a.g + 3 * (int64_t)rows[f] + r, v);
         }
       }
@@ -162,13 +168,17 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
       for (int f = 0; f < 4; ++f)
 #pragma unroll
         for (int r = 0; r < 3; ++r) xc[r] += 0.25 * (a.X[3 * (int64_t)rows[f] + r] + uf[f][r]);
-      double ein = 0.0;
+      double ein = 0.0, edm = 0.0;
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
-        double sq = 0.0;
+        double sq = 0.0, sd = 0.0;
 #pragma unroll
-        for (int f = 0; f < 4; ++f) sq += acc[f][r] * acc[f][r];
+        for (int f = 0; f < 4; ++f) {
+          sq += acc[f][r] * acc[f][r];
+          sd += dmp[f][r] * dmp[f][r];
+        }
         ein += m * (sq + asum[r] * asum[r]);
+        edm += m * (sd + dsum[r] * dsum[r]);
       }
       double psi;
       if (mat == 1)
@@ -179,7 +189,7 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
         psi = snh_energy_f64(kc, F);
       const double e = psi * w -
                        (double)rho * w * (a.grav[0] * xc[0] + a.grav[1] * xc[1] + a.grav[2] * xc[2]) +
-                       0.5 * a.dtfi2 * ein;
+                       0.5 * a.dtfi2 * ein + 0.5 * a.mdamp * edm;
       warp_env_add(a.obj, env, e);
     }
   }

@@ -78,6 +78,7 @@ class SceneConfig:
     thr: float = 0.001            # penaltyThresholdDefault (contact_params.h:123)
     max_align: float = 0.0        # maxAlignmentNormals
     steps: int = 100
+    mass_damping: float = 0.0     # Rayleigh massDampingCoefficient alpha [1/s]
 
 
 # Freudenthal split of a hex into 6 tets: paths 0 -> 7 through the corner cube.

@@ -57,6 +57,7 @@ class SoftBodyWorld:
             self.params.gravity[k] = cfg.gravity[k]
         self.params.k_contact, self.params.t_half = cfg.k_contact, cfg.t_half
         self.params.thr, self.params.max_align = cfg.thr, cfg.max_align
+        self.params.mass_damping = float(getattr(cfg, "mass_damping", 0.0))
         for k, v in overrides.items():
             if k.startswith("linear_"):
                 setattr(self.params.linear, k[len("linear_"):], v)

@@ -120,3 +120,24 @@ def test_other_materials_assembly_matches_oracle(oracle, material, psd):
     H_scale = np.abs(a_or["H"]).max()
     np.testing.assert_allclose(a_gpu["H"], a_or["H"], rtol=0, atol=2e-5 * H_scale)
     assert a_gpu["obj"][0] == pytest.approx(a_or["obj"], rel=1e-6)
+
+
+def test_mass_damping_assembly_matches_oracle(oracle):
+    """Rayleigh mass damping about the state's displacement (the stage start) with an StVK body."""
+    b = _body(21)
+    b.material = 1
+    cfg = scenes.SceneConfig(k_contact=1e6, mass_damping=4.0)
+    w, s = _pair(oracle, b, cfg, 1)
+    rng = np.random.default_rng(321)
+    free = (b.pin == 0).repeat(3)
+    us = rng.normal(0, 5e-4, 3 * b.n_nodes) * free
+    u = us + rng.normal(0, 1e-3, 3 * b.n_nodes) * free
+    v = rng.normal(0, 2e-2, 3 * b.n_nodes) * free
+    w.set_state(us, v, 0.0)
+    a_gpu = w.assemble(u, t=0.01, psd=True)
+    a_or = s.assemble(u, us + cfg.dt * v, t=0.01, psd=True, u_stage=us)
+    g_scale = np.abs(a_or["g"]).max()
+    np.testing.assert_allclose(a_gpu["g"], a_or["g"], rtol=0, atol=1e-6 * g_scale)
+    H_scale = np.abs(a_or["H"]).max()
+    np.testing.assert_allclose(a_gpu["H"], a_or["H"], rtol=0, atol=2e-5 * H_scale)
+    assert a_gpu["obj"][0] == pytest.approx(a_or["obj"], rel=1e-6)

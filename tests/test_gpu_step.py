@@ -110,3 +110,10 @@ def test_other_materials_steps_match_oracle(oracle, material):
     bodies[0].material = material
     w, ug, vg, states, hist = _run(oracle, bodies, cfg, 3)
     _check(bodies, ug, states, hist, newton_exact=False)
+
+
+def test_mass_damped_steps_match_oracle(oracle):
+    bodies, cfg = scenes.config0()
+    cfg.mass_damping = 5.0
+    w, ug, vg, states, hist = _run(oracle, bodies, cfg, 3)
+    _check(bodies, ug, states, hist, newton_exact=False)
