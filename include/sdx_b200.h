@@ -123,6 +123,11 @@ typedef struct {
   double mass_damping;         /* Rayleigh mass damping coefficient alpha [1/s] (massDampingCoefficient):
                                   adds alpha/dt * M (u - u_stage) to the residual and alpha/dt * M to the
                                   Hessian (ComputeSoftDampingScales, mochi_physics/src/mochi_soft.h:274-290) */
+  double stiffness_damping;    /* Rayleigh stiffness damping coefficient beta [s] (stiffnessDampingCoefficient):
+                                  viscous stress kappa C0 (E(F) - E(F_stage)), kappa = beta / dt
+                                  (fem::StressDampingWork, fem_stress_damping.h:29-501) */
+  int stiffness_damping_geometric; /* stiffnessDampingIncludeGeometricTerm: add the viscous-stress term to
+                                      the Hessian (PSD-projected with the material's projection) */
 } sdx_step_params;
 
 /* Per-env statistics of the last step (StageSolverStats, mochi_physics/src/mochi_solve.cpp:1144). */

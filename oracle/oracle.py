@@ -43,7 +43,7 @@ class OrScene(C.Structure):
         ("n_colliders", C.c_int), ("colliders", C.POINTER(OrCollider)),
         ("k_contact", C.c_double), ("t_half", C.c_double), ("thr", C.c_double),
         ("max_align", C.c_double), ("material", C.c_int), ("mass_damping", C.c_double),
-        ("u_stage", _dp),
+        ("u_stage", _dp), ("stiffness_damping", C.c_double), ("stiffness_damping_geometric", C.c_int),
     ]
 
 
@@ -84,6 +84,8 @@ def lib():
         L.or_smith_nh.argtypes = [C.c_double, C.c_double, _dp, C.c_int, C.c_int, C.c_double, _dp, _dp, _dp]
         L.or_material.argtypes = [C.c_int, C.c_double, C.c_double, _dp, C.c_int, C.c_int, C.c_double, _dp, _dp,
                                   _dp]
+        L.or_stress_damping.argtypes = [_dp, C.c_double, _dp, _dp, C.c_double, C.c_double, C.c_double, C.c_int,
+                                        C.c_int, _dp, _dp, _dp]
         L.or_polyrelu.argtypes = [C.c_double] * 3 + [_dp] * 3
         L.or_penalty.argtypes = [C.c_double, _dp, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp]
         L.or_pattern_nnzb.argtypes = [C.c_int, C.c_int, _ip]
@@ -114,6 +116,9 @@ def ref():
         R = C.CDLL(REF_PATH)
         R.ref_smith_nh.argtypes = [C.c_double, C.c_double, _dp, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp]
         R.ref_material.argtypes = [C.c_int, C.c_double, C.c_double, _dp, C.c_int, C.c_int, _dp, _dp, _dp]
+        R.ref_stress_damping.argtypes = [_dp, _dp, _dp, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, _dp,
+                                         _dp, _dp]
+        R.ref_reference_stiffness.argtypes = [C.c_int, C.c_double, C.c_double, _dp]
         R.ref_polyrelu.argtypes = [C.c_double] * 3 + [_dp] * 3
         R.ref_penalty.argtypes = [C.c_double, _dp, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp]
         R.ref_stress_work.argtypes = [_dp, _dp, C.c_double, C.c_double, C.c_int, C.c_int, _dp, _dp, _dp]
@@ -238,6 +243,8 @@ class Scene:
         s.mass = ptr(self.mass)
         s.material = int(getattr(body, "material", 0))
         s.mass_damping = float(getattr(cfg, "mass_damping", 0.0))
+        s.stiffness_damping = float(getattr(cfg, "stiffness_damping", 0.0))
+        s.stiffness_damping_geometric = int(bool(getattr(cfg, "stiffness_damping_geometric", False)))
         for k in range(3):
             s.gravity[k] = cfg.gravity[k]
         s.dt = cfg.dt

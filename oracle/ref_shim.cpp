@@ -7,6 +7,8 @@
 #include <mochi_core/contact/contact_params.h>
 #include <mochi_core/contact/contact_utils.h>
 #include <mochi_core/element_operations/fem_stress.h>
+#include <mochi_core/element_operations/fem_stress_damping.h>
+#include <mochi_core/materials/reference_material_stiffness.h>
 #include <mochi_core/elements/tetrahedral/finite_element.h>
 #include <mochi_core/linear_algebra/krylov/pcg.h>
 #include <mochi_core/linear_algebra/matrix.h>
@@ -93,6 +95,61 @@ void ref_material(int material, double mu, double lambda, const double* F9, int 
       for (int j = 0; j < 3; ++j)
         for (int k = 0; k < 3; ++k)
           for (int l = 0; l < 3; ++l) C81[(i * 3 + j) * 9 + k * 3 + l] = Get0(C[i][j][k][l]);
+}
+
+// fem::StressDampingWork<1> on one P1 tet (mochi_core/.../element_operations/fem_stress_damping.h:29-501),
+// isotropic reference stiffness C0 = (lambda0, mu0) in Voigt form, stiffness damping factor kappa.
+void ref_stress_damping(const double* X12, const double* u12, const double* uss12, double kappa,
+                        double lambda0, double mu0, int geometric, int project, double* energy,
+                        double* res12, double* K144) {
+  Real3 coords[4];
+  for (int i = 0; i < 4; ++i) coords[i] = Real3{X12[3 * i], X12[3 * i + 1], X12[3 * i + 2]};
+  Int4 conn[1] = {Int4{0, 1, 2, 3}};
+  using Elem = tetrahedral::Pk3DElement<1, 1>;
+  Elem elem(0, Span<Real3 const>(coords, 4), Span<Int4 const>(conn, 1));
+  NdArray<int, 1> idx{0};
+  fem::BatchElementVector<1, Elem> disp{}, ss{};
+  for (int i = 0; i < 12; ++i) {
+    disp[i] = BatchReal<1>{u12[i]};
+    ss[i] = BatchReal<1>{uss12[i]};
+  }
+  NdArray<BatchReal<1>, 6, 6> c0{};
+  for (int a = 0; a < 6; ++a)
+    for (int b = 0; b < 6; ++b) {
+      double v = 0.0;
+      if (a < 3 && b < 3) v = lambda0 + (a == b ? 2.0 * mu0 : 0.0);
+      if (a >= 3 && a == b) v = mu0;
+      c0[a][b] = BatchReal<1>{v};
+    }
+  BatchDouble<1> e{0.0};
+  fem::BatchElementVector<1, Elem> res{};
+  fem::BatchElementMatrix<1, Elem> K{};
+  fem::StressDampingWork<1>(idx, Span<Elem const>(&elem, 1), disp, ss, &e, &res, &K, project != 0,
+                            geometric != 0, kappa, c0, /*materialIsIsotropic*/ true);
+  *energy = Get0(e);
+  for (int i = 0; i < 12; ++i) res12[i] = Get0(res[i]);
+  for (int i = 0; i < 144; ++i) K144[i] = Get0(K[i]);
+}
+
+// ComputeReferenceMaterialStiffnessVoigt<1> (mochi_core/.../materials/reference_material_stiffness.h:67)
+// of material 0 (Smith Neo-Hookean), 1 (StVK) or 2 (linear elastic).
+void ref_reference_stiffness(int material, double mu, double lambda, double* c0v36) {
+  auto response = [&](NdArray<int, 1> const&, auto const& F, auto* en, auto* pk1, auto* tan, bool psd) {
+    materials::BatchLameParams<1> p;
+    p.mu = BatchReal<1>{mu};
+    p.lambda = BatchReal<1>{lambda};
+    p.psdStrategy = MaterialPsdStrategy::None;
+    if (material == 1)
+      materials::BatchedStVenantKirchhoffConstitutiveResponse<1>(p, F, en, pk1, tan, psd);
+    else if (material == 2)
+      materials::BatchedLinearElasticConstitutiveResponse<1>(p, F, en, pk1, tan, psd);
+    else
+      materials::BatchedSmithNeoHookeanConstitutiveResponse<1>(p, F, en, pk1, tan, psd,
+                                                               materials::MaterialPsdOracle::Correct);
+  };
+  auto c0 = materials::ComputeReferenceMaterialStiffnessVoigt<1>(NdArray<int, 1>{0}, response);
+  for (int a = 0; a < 6; ++a)
+    for (int b = 0; b < 6; ++b) c0v36[a * 6 + b] = Get0(c0[a][b]);
 }
 
 // PolyReLU (mochi_core/include/mochi_core/utils/activations.h:113).

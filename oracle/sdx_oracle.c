@@ -270,6 +270,89 @@ void or_linear_elastic(double mu, double lambda, const double F[9], double* ener
                 mu * ((r == i && c == j) + (c == i && r == j)) + lambda * (r == c && i == j);
 }
 
+/* symmetric 3x3 projected to eigenvalues >= DBL_EPSILON unless its leading minors prove it SPD
+ * (BatchedProjectSymPsd, mochi_core/.../utils/decomposition_utils_inl.h:1558) */
+static void or_project_sym3(double S[9]) {
+  const double m1 = S[0], m2 = S[0] * S[4] - S[1] * S[1];
+  const double m3 = S[0] * (S[4] * S[8] - S[5] * S[5]) - S[1] * (S[1] * S[8] - S[5] * S[2]) +
+                    S[2] * (S[1] * S[5] - S[4] * S[2]);
+  if (m1 > 0.0 && m2 > 0.0 && m3 > 0.0) return;
+  double A[9], V[9];
+  memcpy(A, S, sizeof(A));
+  jacobi_eig(3, A, V);
+  double l[3];
+  for (int i = 0; i < 3; ++i) l[i] = A[i * 4] > DBL_EPSILON ? A[i * 4] : DBL_EPSILON;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) S[a * 3 + b] = V[a * 3 + 0] * l[0] * V[b * 3 + 0] + V[a * 3 + 1] * l[1] * V[b * 3 + 1] +
+                                               V[a * 3 + 2] * l[2] * V[b * 3 + 2];
+}
+
+void or_stress_damping(const double dN[12], double vol, const double u[12], const double uss[12], double kappa,
+                       double lambda, double mu, int geometric, int project, double* energy, double res[12],
+                       double K[144]) {
+  static const int vi[6] = {0, 1, 2, 1, 0, 0}, vj[6] = {0, 1, 2, 2, 2, 1};
+  double F[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, Fs[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  for (int f = 0; f < 4; ++f)
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) {
+        F[r * 3 + c] += u[3 * f + r] * dN[3 * f + c];
+        Fs[r * 3 + c] += uss[3 * f + r] * dN[3 * f + c];
+      }
+  double dE[6], Sv[6];
+  for (int a = 0; a < 6; ++a) {
+    double acc = 0.0;
+    for (int p = 0; p < 3; ++p) acc += F[p * 3 + vi[a]] * F[p * 3 + vj[a]] - Fs[p * 3 + vi[a]] * Fs[p * 3 + vj[a]];
+    dE[a] = a < 3 ? 0.5 * acc : acc; /* engineering shear */
+  }
+  const double tr = dE[0] + dE[1] + dE[2];
+  for (int a = 0; a < 3; ++a) Sv[a] = kappa * lambda * tr + 2.0 * kappa * mu * dE[a];
+  for (int a = 3; a < 6; ++a) Sv[a] = kappa * mu * dE[a];
+  double S[9] = {Sv[0], Sv[5], Sv[4], Sv[5], Sv[1], Sv[3], Sv[4], Sv[3], Sv[2]};
+  if (energy) {
+    double psi = 0.0;
+    for (int a = 0; a < 6; ++a) psi += Sv[a] * dE[a];
+    *energy = 0.5 * psi * vol;
+  }
+  if (res) {
+    for (int f = 0; f < 4; ++f)
+      for (int i = 0; i < 3; ++i) {
+        double acc = 0.0;
+        for (int c = 0; c < 3; ++c) {
+          double pic = 0.0;
+          for (int k = 0; k < 3; ++k) pic += F[i * 3 + k] * S[k * 3 + c];
+          acc += pic * dN[3 * f + c];
+        }
+        res[3 * f + i] = vol * acc;
+      }
+  }
+  if (!K) return;
+  if (geometric && project) or_project_sym3(S);
+  double FFt[9], a[4][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double v = 0.0;
+      for (int k = 0; k < 3; ++k) v += F[i * 3 + k] * F[j * 3 + k];
+      FFt[i * 3 + j] = v;
+    }
+  for (int f = 0; f < 4; ++f)
+    for (int i = 0; i < 3; ++i)
+      a[f][i] = F[i * 3 + 0] * dN[3 * f + 0] + F[i * 3 + 1] * dN[3 * f + 1] + F[i * 3 + 2] * dN[3 * f + 2];
+  for (int f = 0; f < 4; ++f)
+    for (int g = 0; g < 4; ++g) {
+      const double dd = dN[3 * f] * dN[3 * g] + dN[3 * f + 1] * dN[3 * g + 1] + dN[3 * f + 2] * dN[3 * g + 2];
+      double geo = 0.0;
+      if (geometric)
+        for (int k = 0; k < 3; ++k)
+          for (int l = 0; l < 3; ++l) geo += dN[3 * f + k] * S[k * 3 + l] * dN[3 * g + l];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          double v = kappa * lambda * a[f][i] * a[g][j] + kappa * mu * (FFt[i * 3 + j] * dd + a[g][i] * a[f][j]);
+          if (i == j) v += geo;
+          K[(3 * f + i) * 12 + 3 * g + j] = vol * v;
+        }
+    }
+}
+
 void or_material(int material, double mu, double lambda, const double F[9], int project, int psd_strategy,
                  double min_eig, double* energy, double P[9], double C[81]) {
   if (material == OR_MAT_STVK)
@@ -658,6 +741,26 @@ int64_t or_assemble(const or_scene* s, const double* u, const double* ut, double
           atomic_add(&g[3 * (int64_t)nd[f] + r], v);
         }
     }
+    /* Rayleigh stiffness damping (mochi_physics/src/mochi_soft.h:420-440): viscous stress about the
+     * stage-start displacement, reference stiffness = the rest tangent = (lambda, mu) for these
+     * isotropic materials */
+    double dres[12], dK[144];
+    const int sdamp = s->stiffness_damping > 0.0 && s->u_stage != NULL;
+    if (sdamp) {
+      double ue[12], us[12], de = 0.0;
+      for (int f = 0; f < 4; ++f)
+        for (int r = 0; r < 3; ++r) {
+          ue[3 * f + r] = u[3 * (int64_t)nd[f] + r];
+          us[3 * f + r] = s->u_stage[3 * (int64_t)nd[f] + r];
+        }
+      or_stress_damping(dN, w, ue, us, s->stiffness_damping / dt, s->lambda[e], s->mu[e],
+                        s->stiffness_damping_geometric, project, want_obj ? &de : NULL, want_res ? dres : NULL,
+                        want_hess ? dK : NULL);
+      energy += de;
+      if (want_res)
+        for (int f = 0; f < 4; ++f)
+          for (int r = 0; r < 3; ++r) atomic_add(&g[3 * (int64_t)nd[f] + r], dres[3 * f + r]);
+    }
     if (want_hess) {
       for (int f = 0; f < 4; ++f)
         for (int gg = 0; gg < 4; ++gg) {
@@ -669,7 +772,9 @@ int64_t or_assemble(const or_scene* s, const double* u, const double* ut, double
               for (int j = 0; j < 3; ++j)
                 for (int l = 0; l < 3; ++l)
                   k += dN[3 * f + j] * C[(r * 3 + j) * 9 + (c * 3 + l)] * dN[3 * gg + l];
-              atomic_add(&blk[r * 3 + c], k * w);
+              k *= w;
+              if (sdamp) k += dK[(3 * f + r) * 12 + 3 * gg + c];
+              atomic_add(&blk[r * 3 + c], k);
             }
         }
     }

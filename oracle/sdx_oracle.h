@@ -56,6 +56,17 @@ void or_linear_elastic(double mu, double lambda, const double F[9], double* ener
 void or_material(int material, double mu, double lambda, const double F[9], int project, int psd_strategy,
                  double min_eig, double* energy, double P[9], double C[81]);
 
+/* Rayleigh stiffness damping of one P1 tet (viscous stress), isotropic reference stiffness (lambda, mu):
+ * dE = E(F) - E(F_stage) (Green strains, Voigt with engineering shear), S = kappa (lambda tr(dE) I +
+ * 2 mu dE), energy 1/2 S : dE vol, residual (F S) dN vol, Hessian the Gauss-Newton part
+ * kappa B^T C0 B plus, if geometric, the (PSD-projected when project) S term.
+ * Follows mochi_core/.../element_operations/fem_stress_damping.h:29-501 (isotropic path); kappa is the
+ * damping coefficient / dt. dN: 4x3 shape-function gradients; u, uss: 12 displacements. res: 12, K: 144
+ * (row (f,i), column (g,j)); any output may be NULL. */
+void or_stress_damping(const double dN[12], double vol, const double u[12], const double uss[12], double kappa,
+                       double lambda, double mu, int geometric, int project, double* energy, double res[12],
+                       double K[144]);
+
 /* (E, nu) -> (lambda, mu). mochi_core/.../materials/material_utils.h:331-339. */
 void or_lame(double E, double nu, double* lambda, double* mu);
 
@@ -130,6 +141,10 @@ typedef struct {
    * NULL: the inertia-free terms are skipped) — mochi_physics/src/mochi_soft.h:274-290, 408-420 */
   double mass_damping;
   const double* u_stage;
+  /* Rayleigh stiffness damping coefficient beta [s] (stiffnessDampingCoefficient; kappa = beta / dt)
+   * and its geometric term (stiffnessDampingIncludeGeometricTerm) */
+  double stiffness_damping;
+  int stiffness_damping_geometric;
 } or_scene;
 
 /* Consistent P1 mass coupling per block (Q4 quadrature, exact for P1): m_ij = sum_t rho V (1+d_ij)/20.

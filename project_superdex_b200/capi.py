@@ -61,7 +61,8 @@ class StepParams(C.Structure):
                 ("newton_rel_step_tol", C.c_double), ("ls_max_iter", C.c_int),
                 ("ls_alpha", C.c_double), ("ew_forcing", C.c_int), ("rel_div_tol", C.c_double),
                 ("abs_div_tol", C.c_double), ("warm_start", C.c_int), ("linear", LinearParams),
-                ("mass_damping", C.c_double)]
+                ("mass_damping", C.c_double), ("stiffness_damping", C.c_double),
+                ("stiffness_damping_geometric", C.c_int)]
 
 
 class EnvStats(C.Structure):

@@ -494,6 +494,44 @@ __device__ __forceinline__ void linear_tangent_f32(float mu, float lambda, float
 }
 
 // ------------------------------------------------------------------------------------------------
+// Rayleigh stiffness damping (viscous stress), fem_stress_damping.h:29-501, isotropic reference stiffness:
+// dE = E(F) - E(F_stage) in Voigt order [00, 11, 22, 12, 02, 01] with engineering shear,
+// Sv = kappa lambda tr(dE) + 2 kappa mu dE (normal), kappa mu dE (shear).
+
+__device__ __forceinline__ void visc_stress_f64(const double F[9], const double Fs[9], double kl, double km,
+                                                double dE[6], double Sv[6]) {
+  constexpr int vi[6] = {0, 1, 2, 1, 0, 0}, vj[6] = {0, 1, 2, 2, 2, 1};
+#pragma unroll
+  for (int a = 0; a < 6; ++a) {
+    double acc = 0.0;
+#pragma unroll
+    for (int p = 0; p < 3; ++p) acc += F[p * 3 + vi[a]] * F[p * 3 + vj[a]] - Fs[p * 3 + vi[a]] * Fs[p * 3 + vj[a]];
+    dE[a] = a < 3 ? 0.5 * acc : acc;
+  }
+  const double tr = dE[0] + dE[1] + dE[2];
+#pragma unroll
+  for (int a = 0; a < 6; ++a) Sv[a] = a < 3 ? kl * tr + 2.0 * km * dE[a] : km * dE[a];
+}
+
+// symmetric 3x3 to eigenvalues >= FLT_EPSILON unless the leading minors prove it SPD
+// (BatchedProjectSymPsd, decomposition_utils_inl.h:1558)
+__device__ __forceinline__ void project_sym3_f32(float S[9]) {
+  const float m1 = S[0], m2 = S[0] * S[4] - S[1] * S[1];
+  const float m3 = S[0] * (S[4] * S[8] - S[5] * S[5]) - S[1] * (S[1] * S[8] - S[5] * S[2]) +
+                   S[2] * (S[1] * S[5] - S[4] * S[2]);
+  if (m1 > 0.0f && m2 > 0.0f && m3 > 0.0f) return;
+  float w[3], V[9];
+  sym_eig3(S, w, V);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) w[i] = fmaxf(w[i], 1.1920928955078125e-07f);
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int b = 0; b < 3; ++b)
+      S[a * 3 + b] = V[a * 3 + 0] * w[0] * V[b * 3 + 0] + V[a * 3 + 1] * w[1] * V[b * 3 + 1] + V[a * 3 + 2] * w[2] * V[b * 3 + 2];
+}
+
+// ------------------------------------------------------------------------------------------------
 // contact helpers (FP64): PolyReLU and the analytic collider SDFs
 
 // activations.h:113-130

@@ -906,6 +906,8 @@ extern "C" int sdx_set_params(sdx_context* c, const sdx_step_params* p) {
   if (!c || !p) return set_error(SDX_ERR_INVALID_ARGUMENT, "null argument");
   if (!(p->dt > 0.0)) return set_error(SDX_ERR_INVALID_ARGUMENT, "dt must be positive");
   if (!(p->mass_damping >= 0.0)) return set_error(SDX_ERR_INVALID_ARGUMENT, "mass_damping must be >= 0");
+  if (!(p->stiffness_damping >= 0.0))
+    return set_error(SDX_ERR_INVALID_ARGUMENT, "stiffness_damping must be >= 0");
   if (p->linear.preconditioner < 0 || p->linear.preconditioner > 2)
     return set_error(SDX_ERR_INVALID_ARGUMENT, "unknown preconditioner %d", p->linear.preconditioner);
   c->params = *p;
@@ -1388,6 +1390,8 @@ static void assemble_dev(sdx_context* c, const double* u, const double* ut, doub
   ea.ut = ut;
   ea.u0 = c->u0;
   ea.mdamp = p.mass_damping > 0.0 ? p.mass_damping / p.dt : 0.0;
+  ea.kdamp = p.stiffness_damping > 0.0 ? p.stiffness_damping / p.dt : 0.0;
+  ea.kdamp_geo = p.stiffness_damping_geometric;
   ea.X = c->X;
   ea.pin = c->pin;
   ea.g = c->g;

@@ -63,6 +63,8 @@ struct ElemArgs {
   double* obj;  // per env
   double dtfi2;
   double mdamp;  // mass damping scale alpha / dt (0: none)
+  double kdamp;  // stiffness damping factor kappa = beta / dt (0: none)
+  int kdamp_geo; // include the geometric (stress) term of the stiffness damping Hessian
   double grav[3];
   float min_eig;
   int psd;

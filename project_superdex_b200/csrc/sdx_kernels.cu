@@ -122,6 +122,21 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
       for (int c = 0; c < 3; ++c) F[r * 3 + c] = fma(uf[f][r], (double)dN[3 * f + c], F[r * 3 + c]);
 
   const bool want_res = a.flags & 2, want_obj = a.flags & 1, want_hess = a.flags & 4;
+  // Rayleigh stiffness damping: viscous stress about the stage-start displacement
+  // (fem_stress_damping.h:29-501; reference stiffness = the tet's lambda, mu)
+  double Sv[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, dE[6];
+  if (a.kdamp > 0.0) {
+    double Fs[9] = {1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0};
+#pragma unroll
+    for (int f = 0; f < 4; ++f)
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        const double us = a.u0[3 * (int64_t)rows[f] + r];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) Fs[r * 3 + c] = fma(us, (double)dN[3 * f + c], Fs[r * 3 + c]);
+      }
+    visc_stress_f64(F, Fs, a.kdamp * (double)lam, a.kdamp * (double)mu, dE, Sv);
+  }
   if (want_res || want_obj) {
     const SnhConsts kc = snh_consts((double)mu, (double)lam);
     const double w = (double)vol;
@@ -147,6 +162,14 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
         linear_energy_pk1_f64((double)mu, (double)lam, F, nullptr, P);
       else
         snh_pk1_f64(kc, F, P);
+      if (a.kdamp > 0.0) {  // + F S_visc
+        const double S[9] = {Sv[0], Sv[5], Sv[4], Sv[5], Sv[1], Sv[3], Sv[4], Sv[3], Sv[2]};
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            P[r * 3 + c] += F[r * 3 + 0] * S[c] + F[r * 3 + 1] * S[3 + c] + F[r * 3 + 2] * S[6 + c];
+      }
 #pragma unroll
       for (int f = 0; f < 4; ++f) {
         const int pf = a.pin[rows[f]];
@@ -187,6 +210,8 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
         linear_energy_pk1_f64((double)mu, (double)lam, F, &psi, nullptr);
       else
         psi = snh_energy_f64(kc, F);
+      if (a.kdamp > 0.0) psi += 0.5 * (Sv[0] * dE[0] + Sv[1] * dE[1] + Sv[2] * dE[2] + Sv[3] * dE[3] +
+                                       Sv[4] * dE[4] + Sv[5] * dE[5]);
       const double e = psi * w -
                        (double)rho * w * (a.grav[0] * xc[0] + a.grav[1] * xc[1] + a.grav[2] * xc[2]) +
                        0.5 * a.dtfi2 * ein + 0.5 * a.mdamp * edm;
@@ -211,6 +236,28 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
     int pins[4];
 #pragma unroll
     for (int f = 0; f < 4; ++f) pins[f] = a.pin[rows[f]];
+    // stiffness damping: Gauss-Newton part kappa B^T C0 B and the (projected) geometric part
+    const bool kd = a.kdamp > 0.0;
+    float aF[4][3], FFt[9], Sg[9];
+    const float kl = (float)(a.kdamp * (double)lam), km = (float)(a.kdamp * (double)mu);
+    if (kd) {
+#pragma unroll
+      for (int f = 0; f < 4; ++f)
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+          aF[f][i] = Ff[i * 3 + 0] * dN[3 * f + 0] + Ff[i * 3 + 1] * dN[3 * f + 1] + Ff[i * 3 + 2] * dN[3 * f + 2];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          FFt[i * 3 + j] = Ff[i * 3 + 0] * Ff[j * 3 + 0] + Ff[i * 3 + 1] * Ff[j * 3 + 1] + Ff[i * 3 + 2] * Ff[j * 3 + 2];
+      const float s6[6] = {(float)Sv[0], (float)Sv[1], (float)Sv[2], (float)Sv[3], (float)Sv[4], (float)Sv[5]};
+      Sg[0] = s6[0]; Sg[4] = s6[1]; Sg[8] = s6[2];
+      Sg[5] = Sg[7] = s6[3];
+      Sg[2] = Sg[6] = s6[4];
+      Sg[1] = Sg[3] = s6[5];
+      if (a.kdamp_geo && (a.flags & 8)) project_sym3_f32(Sg);
+    }
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
 #pragma unroll
@@ -228,8 +275,21 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
             if ((pins[g] >> c) & 1) continue;
-            const float k = vol * (Cf[c * 3 + 0] * dN[3 * g + 0] + Cf[c * 3 + 1] * dN[3 * g + 1] +
-                                   Cf[c * 3 + 2] * dN[3 * g + 2]);
+            float k = vol * (Cf[c * 3 + 0] * dN[3 * g + 0] + Cf[c * 3 + 1] * dN[3 * g + 1] +
+                             Cf[c * 3 + 2] * dN[3 * g + 2]);
+            if (kd) {
+              const float dd = dN[3 * f] * dN[3 * g] + dN[3 * f + 1] * dN[3 * g + 1] + dN[3 * f + 2] * dN[3 * g + 2];
+              float v = kl * aF[f][r] * aF[g][c] + km * (FFt[r * 3 + c] * dd + aF[g][r] * aF[f][c]);
+              if (a.kdamp_geo && r == c) {
+                float geo = 0.0f;
+#pragma unroll
+                for (int kk = 0; kk < 3; ++kk)
+                  geo += dN[3 * f + kk] * (Sg[kk * 3 + 0] * dN[3 * g + 0] + Sg[kk * 3 + 1] * dN[3 * g + 1] +
+                                           Sg[kk * 3 + 2] * dN[3 * g + 2]);
+                v += geo;
+              }
+              k += vol * v;
+            }
             atomicAdd(a.val + val_index(p, 3 * r + c), k);
           }
         }

@@ -79,6 +79,8 @@ class SceneConfig:
     max_align: float = 0.0        # maxAlignmentNormals
     steps: int = 100
     mass_damping: float = 0.0     # Rayleigh massDampingCoefficient alpha [1/s]
+    stiffness_damping: float = 0.0  # Rayleigh stiffnessDampingCoefficient beta [s]
+    stiffness_damping_geometric: bool = False  # stiffnessDampingIncludeGeometricTerm
 
 
 # Freudenthal split of a hex into 6 tets: paths 0 -> 7 through the corner cube.

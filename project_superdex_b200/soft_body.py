@@ -58,6 +58,8 @@ class SoftBodyWorld:
         self.params.k_contact, self.params.t_half = cfg.k_contact, cfg.t_half
         self.params.thr, self.params.max_align = cfg.thr, cfg.max_align
         self.params.mass_damping = float(getattr(cfg, "mass_damping", 0.0))
+        self.params.stiffness_damping = float(getattr(cfg, "stiffness_damping", 0.0))
+        self.params.stiffness_damping_geometric = int(bool(getattr(cfg, "stiffness_damping_geometric", False)))
         for k, v in overrides.items():
             if k.startswith("linear_"):
                 setattr(self.params.linear, k[len("linear_"):], v)

@@ -11,7 +11,7 @@ exists; the fixtures are committed, nothing reads the reference at test time).
   * reference_vectors.json — outputs of the reference's own compiled code (oracle/_ref, built by
     oracle/build_ref.sh from the reference sources) on seeded inputs: Smith NH with every PSD
     strategy (projected tangents), St. Venant-Kirchhoff and linear elasticity with every PSD strategy,
-    PolyReLU, the penalty contact response, fem::StressWork on single
+    fem::StressDampingWork (Rayleigh stiffness damping) on single tets, PolyReLU, the penalty contact response, fem::StressWork on single
     tets, and krylov::PCG iteration counts / solutions on the two golden systems.
 
   python tests/golden/make_golden.py [--reference-root /path/to/reference]
@@ -93,7 +93,8 @@ def reference_vectors():
     R = O.ref()
     assert R is not None, "oracle/_ref/libsdx_ref.so missing: run oracle/build_ref.sh"
     rng = np.random.default_rng(20261203)
-    out = {"smith": [], "polyrelu": [], "penalty": [], "stress_work": [], "pcg": [], "materials": []}
+    out = {"smith": [], "polyrelu": [], "penalty": [], "stress_work": [], "pcg": [], "materials": [],
+           "stress_damping": []}
     for i in range(48):
         F = np.eye(3) + rng.normal(0, 0.35, (3, 3))
         if i % 4 == 0:
@@ -173,6 +174,27 @@ def reference_vectors():
                 out["materials"].append({"kind": kind, "mu": mu, "lambda": lam, "F": F.reshape(-1).tolist(),
                                          "psd": psd, "energy": e, "pk1": P.reshape(-1).tolist(),
                                          "tangent": Cm.reshape(-1).tolist()})
+    # fem::StressDampingWork (Rayleigh stiffness damping) on single tets, with / without the geometric
+    # term and its projection
+    R = O.ref()
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    rng = np.random.default_rng(11)
+    for t in range(16):
+        X = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], float) * 0.01 + rng.normal(0, 0.001, (4, 3))
+        if np.linalg.det(np.stack([X[1] - X[0], X[2] - X[0], X[3] - X[0]], 1)) < 0:
+            X[[1, 2]] = X[[2, 1]]
+        u = rng.normal(0, 0.002, 12)
+        uss = u + rng.normal(0, 0.001, 12)
+        kappa, lam, mu = float(rng.uniform(0.05, 2.0)), float(rng.uniform(1e4, 1e5)), float(rng.uniform(3e3, 3e4))
+        geo, proj = t % 2, (t // 2) % 2
+        e = np.zeros(1)
+        r = np.zeros(12)
+        K = np.zeros(144)
+        Xf = np.ascontiguousarray(X.reshape(-1))
+        R.ref_stress_damping(dp(Xf), dp(u), dp(uss), kappa, lam, mu, geo, proj, dp(e), dp(r), dp(K))
+        out["stress_damping"].append({"X": Xf.tolist(), "u": u.tolist(), "uss": uss.tolist(), "kappa": kappa,
+                                      "lambda": lam, "mu": mu, "geometric": geo, "project": proj,
+                                      "energy": float(e[0]), "res": r.tolist(), "K": K.tolist()})
     out["source"] = "oracle/_ref/libsdx_ref.so (reference sources, FP64 build)"
     return out
 

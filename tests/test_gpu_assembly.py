@@ -141,3 +141,26 @@ def test_mass_damping_assembly_matches_oracle(oracle):
     H_scale = np.abs(a_or["H"]).max()
     np.testing.assert_allclose(a_gpu["H"], a_or["H"], rtol=0, atol=2e-5 * H_scale)
     assert a_gpu["obj"][0] == pytest.approx(a_or["obj"], rel=1e-6)
+
+
+@pytest.mark.parametrize("geometric,psd", [(False, 1), (True, 0), (True, 1)])
+def test_stiffness_damping_assembly_matches_oracle(oracle, geometric, psd):
+    """Rayleigh stiffness damping (viscous stress about the stage start), with and without its geometric
+    Hessian term and its projection."""
+    b = _body(31)
+    cfg = scenes.SceneConfig(k_contact=1e6, mass_damping=2.0, stiffness_damping=0.01,
+                             stiffness_damping_geometric=geometric)
+    w, s = _pair(oracle, b, cfg, psd)
+    rng = np.random.default_rng(431 + psd)
+    free = (b.pin == 0).repeat(3)
+    us = rng.normal(0, 5e-4, 3 * b.n_nodes) * free
+    u = us + rng.normal(0, 1e-3, 3 * b.n_nodes) * free
+    v = rng.normal(0, 2e-2, 3 * b.n_nodes) * free
+    w.set_state(us, v, 0.0)
+    a_gpu = w.assemble(u, t=0.01, psd=psd != 0)
+    a_or = s.assemble(u, us + cfg.dt * v, t=0.01, psd=psd != 0, u_stage=us)
+    g_scale = np.abs(a_or["g"]).max()
+    np.testing.assert_allclose(a_gpu["g"], a_or["g"], rtol=0, atol=1e-6 * g_scale)
+    H_scale = np.abs(a_or["H"]).max()
+    np.testing.assert_allclose(a_gpu["H"], a_or["H"], rtol=0, atol=2e-5 * H_scale)
+    assert a_gpu["obj"][0] == pytest.approx(a_or["obj"], rel=1e-6)

@@ -117,3 +117,11 @@ def test_mass_damped_steps_match_oracle(oracle):
     cfg.mass_damping = 5.0
     w, ug, vg, states, hist = _run(oracle, bodies, cfg, 3)
     _check(bodies, ug, states, hist, newton_exact=False)
+
+
+def test_stiffness_damped_steps_match_oracle(oracle):
+    bodies, cfg = scenes.config0()
+    cfg.stiffness_damping = 0.005
+    cfg.stiffness_damping_geometric = True
+    w, ug, vg, states, hist = _run(oracle, bodies, cfg, 3)
+    _check(bodies, ug, states, hist, newton_exact=False)

@@ -89,12 +89,14 @@ def test_contact_pairs_sorted_unique(oracle):
 
 @pytest.mark.parametrize("material", [0, 1, 2])
 def test_damped_materials_match_finite_differences(oracle, material):
-    """Energy -> gradient -> Hessian consistency with Rayleigh mass damping (about a stage-start
-    displacement) for each soft material."""
+    """Energy -> gradient -> Hessian consistency with Rayleigh mass and stiffness damping (about a
+    stage-start displacement; the stiffness-damping Hessian with its geometric term is exact) for each
+    soft material."""
     rng = np.random.default_rng(9 + material)
     b = scenes.grid_body(3, 3, 3, 0.01, rng=rng, E=2e4, nu=0.4)
     b.material = material
-    cfg = scenes.SceneConfig(k_contact=1e6, mass_damping=3.0)
+    cfg = scenes.SceneConfig(k_contact=1e6, mass_damping=3.0, stiffness_damping=0.02,
+                             stiffness_damping_geometric=True)
     s = oracle.Scene(b, cfg, psd_strategy=0)
     free = (b.pin == 0).repeat(3)
     u = rng.normal(0, 4e-4, 3 * b.n_nodes) * free

@@ -137,3 +137,24 @@ def test_pcg_stop_and_divergence_statuses(oracle):
     rp, col, vals, bp = scalar_to_block(Z + np.eye(9), np.zeros(9))
     x, st = oracle.pcg(rp, col, vals, bp)
     assert st.convergence == 1 and st.num_iter == 0  # b = 0: converged at iteration 0
+
+
+def test_stiffness_damping_matches_reference_code(oracle, golden):
+    """The oracle's viscous-stress damping against fem::StressDampingWork compiled from the reference."""
+    import ctypes as C
+    L = oracle.lib()
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    v = golden("reference_vectors.json")
+    assert len(v["stress_damping"]) == 16
+    for c in v["stress_damping"]:
+        X = np.array(c["X"])
+        tets = np.arange(4, dtype=np.int32)
+        dN = np.zeros(12)
+        vol = np.zeros(1)
+        L.or_rest_data(1, tets.ctypes.data_as(C.POINTER(C.c_int32)), dp(X), dp(dN), dp(vol))
+        e, r, K = np.zeros(1), np.zeros(12), np.zeros(144)
+        L.or_stress_damping(dp(dN), vol[0], dp(np.array(c["u"])), dp(np.array(c["uss"])), c["kappa"], c["lambda"],
+                            c["mu"], c["geometric"], c["project"], dp(e), dp(r), dp(K))
+        assert e[0] == pytest.approx(c["energy"], rel=1e-11, abs=1e-18)
+        np.testing.assert_allclose(r, c["res"], rtol=1e-10, atol=1e-12 * np.abs(c["res"]).max())
+        np.testing.assert_allclose(K, c["K"], rtol=1e-10, atol=1e-12 * np.abs(c["K"]).max())
