@@ -94,6 +94,10 @@ typedef struct {
 #define SDX_SOLVER_FUSED 0
 #define SDX_SOLVER_PLAIN_FP64 1
 
+/* Coulomb friction smoothing (CoulombFrictionModel, contact_params.h:307-327) */
+#define SDX_FRICTION_C1 0
+#define SDX_FRICTION_CINF 1
+
 /* Mirrors LinearSolverStatus (krylov_solver.h:85-116). */
 typedef struct {
   int num_iter;
@@ -128,6 +132,23 @@ typedef struct {
                                   (fem::StressDampingWork, fem_stress_damping.h:29-501) */
   int stiffness_damping_geometric; /* stiffnessDampingIncludeGeometricTerm: add the viscous-stress term to
                                       the Hessian (PSD-projected with the material's projection) */
+  /* Contact dissipation (ComputeBatchContactDissipationForceDForce, contact_utils.h:627-960): Coulomb and
+   * viscous friction and normal viscous damping of each contact sample, driven by the sample's
+   * displacement relative to the collider over the step and by the normal force at the stage start
+   * (ContactParams, contact_params.h:150-230; ContactEvalConfig, contact_utils.h:459-490). */
+  double friction_coulomb;         /* coulombFrictionCoefficient (the reference's default is 0.5; 0 here) */
+  double friction_falloff_vel;     /* frictionFalloffVel [m/s] (default 0.01) */
+  double friction_viscous;         /* viscousFrictionCoefficient [s/m] (default 0) */
+  double contact_normal_damping;   /* normalViscousDampingCoefficient [s/m] (default 0) */
+  int friction_model;              /* SDX_FRICTION_* (CoulombFrictionModel, default C1) */
+  int friction_fitted_hessian;     /* fittedSaturationHessian.contactFriction (default 1) */
+  int friction_fade;               /* fadeFriction (default 1) */
+  int friction_collider_normal;    /* frictionWithColliderNormal (default 1) */
+  int contact_explicit_normals;    /* explicitNormals (default 0): alignment, friction plane and the
+                                      dissipation's normal force from the stage start; pairs in contact at
+                                      the stage start stay in the contact set */
+  int contact_implicit_normal_force; /* implicitNormalForceForDissipation (default 0; not together with
+                                        explicit normals) */
 } sdx_step_params;
 
 /* Per-env statistics of the last step (StageSolverStats, mochi_physics/src/mochi_solve.cpp:1144). */

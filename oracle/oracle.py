@@ -44,7 +44,32 @@ class OrScene(C.Structure):
         ("k_contact", C.c_double), ("t_half", C.c_double), ("thr", C.c_double),
         ("max_align", C.c_double), ("material", C.c_int), ("mass_damping", C.c_double),
         ("u_stage", _dp), ("stiffness_damping", C.c_double), ("stiffness_damping_geometric", C.c_int),
+        ("coulomb", C.c_double), ("falloff_vel", C.c_double), ("viscous", C.c_double),
+        ("normal_damping", C.c_double), ("collider_normal", C.c_int), ("explicit_normals", C.c_int),
+        ("fade", C.c_int), ("implicit_normal_force", C.c_int), ("fitted", C.c_int), ("friction_model", C.c_int),
     ]
+
+
+class OrContactParams(C.Structure):
+    _fields_ = [("k", C.c_double), ("t_half", C.c_double), ("thr", C.c_double), ("max_align", C.c_double),
+                ("coulomb", C.c_double), ("falloff_vel", C.c_double), ("viscous", C.c_double),
+                ("normal_damping", C.c_double), ("collider_normal", C.c_int), ("explicit_normals", C.c_int),
+                ("fade", C.c_int), ("implicit_normal_force", C.c_int), ("fitted", C.c_int), ("model", C.c_int)]
+
+
+CONTACT_DEFAULTS = dict(k=1e4, t_half=5e-3, thr=1e-3, max_align=0.0, coulomb=0.5, falloff_vel=0.01, viscous=0.0,
+                        normal_damping=0.0, collider_normal=1, explicit_normals=0, fade=1, implicit_normal_force=0,
+                        fitted=1, model=0)
+
+
+def contact_params(**kw):
+    """OrContactParams from the reference's defaults (ContactParams, ContactEvalConfig) overridden by kw."""
+    v = dict(CONTACT_DEFAULTS)
+    for k_, x in kw.items():
+        if k_ not in v:
+            raise KeyError(k_)
+        v[k_] = x
+    return OrContactParams(**v)
 
 
 class OrPcgParams(C.Structure):
@@ -88,6 +113,8 @@ def lib():
                                         C.c_int, _dp, _dp, _dp]
         L.or_polyrelu.argtypes = [C.c_double] * 3 + [_dp] * 3
         L.or_penalty.argtypes = [C.c_double, _dp, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp]
+        L.or_collision_response.argtypes = [C.POINTER(OrContactParams), C.c_double, _dp, C.c_double, _dp, _dp, _dp,
+                                            _dp, C.c_double, C.c_int, _dp, _dp, _dp]
         L.or_pattern_nnzb.argtypes = [C.c_int, C.c_int, _ip]
         L.or_pattern_nnzb.restype = C.c_int64
         L.or_pattern_fill.argtypes = [C.c_int, C.c_int, _ip, _lp, _ip]
@@ -121,6 +148,8 @@ def ref():
         R.ref_reference_stiffness.argtypes = [C.c_int, C.c_double, C.c_double, _dp]
         R.ref_polyrelu.argtypes = [C.c_double] * 3 + [_dp] * 3
         R.ref_penalty.argtypes = [C.c_double, _dp, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp]
+        R.ref_collision_response.argtypes = ([C.c_double, _dp, C.c_double, _dp, _dp, _dp, _dp] + [C.c_double] * 8 +
+                                             [C.c_int] * 7 + [C.c_double, C.c_int, _dp, _dp, _dp])
         R.ref_stress_work.argtypes = [_dp, _dp, C.c_double, C.c_double, C.c_int, C.c_int, _dp, _dp, _dp]
         R.ref_pcg_csr.argtypes = [C.c_int, _lp, _ip, _dp, _dp, _dp, C.c_double, C.c_double, C.c_double,
                                   C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, C.POINTER(C.c_int)]
@@ -181,6 +210,27 @@ def penalty(d, grad, k, t_half, thr):
     f = np.zeros(3)
     df = np.zeros(9)
     lib().or_penalty(d, ptr(g), k, t_half, thr, ptr(e), ptr(f), ptr(df))
+    return e[0], f, df.reshape(3, 3)
+
+
+def collision_response(prm, d, grad, d_ss, grad_ss, n_col, pos, pos_ss, dt, unit_grad=True, use_ref=False):
+    """Energy, force (3) and dforce (3x3) of one contact sample (or_collision_response; with use_ref the
+    reference's own ComputeBatchCollisionForceDForce). n_col None: colliding normals not valid."""
+    a = [np.ascontiguousarray(v, np.float64) for v in (grad, grad_ss, n_col if n_col is not None else np.zeros(3),
+                                                       pos, pos_ss)]
+    e = np.zeros(1)
+    f = np.zeros(3)
+    df = np.zeros(9)
+    if use_ref:
+        ref().ref_collision_response(d, ptr(a[0]), d_ss, ptr(a[1]), ptr(a[2]), ptr(a[3]), ptr(a[4]), prm.k,
+                                     prm.t_half, prm.thr, prm.max_align, prm.coulomb, prm.falloff_vel, prm.viscous,
+                                     prm.normal_damping, prm.collider_normal, int(n_col is not None),
+                                     prm.explicit_normals, prm.fade, prm.implicit_normal_force, prm.fitted,
+                                     prm.model, dt, int(unit_grad), ptr(e), ptr(f), ptr(df))
+    else:
+        lib().or_collision_response(C.byref(prm), d, ptr(a[0]), d_ss, ptr(a[1]),
+                                    ptr(a[2]) if n_col is not None else None, ptr(a[3]), ptr(a[4]), dt,
+                                    int(unit_grad), ptr(e), ptr(f), ptr(df))
     return e[0], f, df.reshape(3, 3)
 
 
@@ -253,6 +303,16 @@ class Scene:
         s.n_colliders = len(body.colliders)
         s.colliders = C.cast(self.colliders, C.POINTER(OrCollider))
         s.k_contact, s.t_half, s.thr, s.max_align = cfg.k_contact, cfg.t_half, cfg.thr, cfg.max_align
+        s.coulomb = float(getattr(cfg, "friction_coulomb", 0.0))
+        s.falloff_vel = float(getattr(cfg, "friction_falloff_vel", 0.01))
+        s.viscous = float(getattr(cfg, "friction_viscous", 0.0))
+        s.normal_damping = float(getattr(cfg, "contact_normal_damping", 0.0))
+        s.collider_normal = int(bool(getattr(cfg, "friction_collider_normal", True)))
+        s.explicit_normals = int(bool(getattr(cfg, "contact_explicit_normals", False)))
+        s.fade = int(bool(getattr(cfg, "friction_fade", True)))
+        s.implicit_normal_force = int(bool(getattr(cfg, "contact_implicit_normal_force", False)))
+        s.fitted = int(bool(getattr(cfg, "friction_fitted_hessian", True)))
+        s.friction_model = int(getattr(cfg, "friction_model", 0))
         self.s = s
         L.or_mass_blocks(C.byref(s), ptr(self.mass))
         self.nnzb = nnzb

@@ -181,6 +181,58 @@ void ref_penalty(double d, const double* grad3, double k, double t_half, double 
   for (int i = 0; i < 6; ++i) dforce6[i] = Get0(df[i]);
 }
 
+// ComputeBatchCollisionForceDForce<1, GradTarget::Current> (mochi_core/include/mochi_core/contact/
+// contact_utils.h:1003-1230): the penalty response plus Coulomb / viscous friction and normal viscous
+// damping (ComputeBatchContactDissipationForceDForce, contact_utils.h:627-960) of one sample, every
+// vector in the collider frame. d, grad: implicit SDF value and gradient; d_ss, grad_ss: stage-start
+// ones (read only with explicit normals); n_col: the colliding surface normal; p, p_ss: the sample's
+// current and stage-start positions. model: 0 C1Regularized, 1 CinfRegularized. dforce9 row-major.
+void ref_collision_response(double d, const double* grad3, double d_ss, const double* grad_ss3,
+                            const double* n_col3, const double* p3, const double* p_ss3, double k,
+                            double t_half, double thr, double max_align, double coulomb,
+                            double falloff_vel, double viscous, double normal_damping,
+                            int collider_normal, int valid_colliding_normals, int explicit_normals,
+                            int fade, int implicit_normal_force, int fitted, int model, double dt,
+                            int unit_grad, double* energy, double* force3, double* dforce9) {
+  ContactParams params;
+  params.penaltyCoefficient = k;
+  params.penaltySmoothingHalfDistance = t_half;
+  params.penaltyThresholdDefault = thr;
+  params.penaltyThresholdExtraPadding = 0;
+  params.maxAlignmentNormals = max_align;
+  params.coulombFrictionCoefficient = coulomb;
+  params.frictionFalloffVel = falloff_vel;
+  params.viscousFrictionCoefficient = viscous;
+  params.normalViscousDampingCoefficient = normal_damping;
+  params.frictionWithColliderNormal = collider_normal != 0;
+  ContactEvalConfig config{};
+  config.addPadding = false;
+  config.validCollidingNormals = valid_colliding_normals != 0;
+  config.explicitNormals = explicit_normals != 0;
+  config.fadeFriction = fade != 0;
+  config.implicitNormalForceForDissipation = implicit_normal_force != 0;
+  config.useFittedHessian = fitted != 0;
+  config.frictionModel = model == 1 ? CoulombFrictionModel::CinfRegularized : CoulombFrictionModel::C1Regularized;
+  double e[1] = {0.0};
+  Real3 f[1];
+  VMatrix3x3r df[1];
+  real dist[1] = {d}, dist_ss[1] = {d_ss};
+  Real3 g[1] = {Real3{grad3[0], grad3[1], grad3[2]}};
+  Real3 g_ss[1] = {Real3{grad_ss3[0], grad_ss3[1], grad_ss3[2]}};
+  Real3 nc[1] = {Real3{n_col3[0], n_col3[1], n_col3[2]}};
+  Real3 pc[1] = {Real3{p3[0], p3[1], p3[2]}};
+  Real3 pss[1] = {Real3{p_ss3[0], p_ss3[1], p_ss3[2]}};
+  ComputeBatchCollisionForceDForce<1, GradTarget::Current>(
+      Span<double>(e, 1), Span<Real3>(f, 1), Span<VMatrix3x3r>(df, 1), Span<real const>(dist, 1),
+      Span<Real3 const>(g, 1), Span<real const>(dist_ss, 1), Span<Real3 const>(g_ss, 1),
+      Span<Real3 const>(nc, 1), Span<Real3 const>(pc, 1), Span<Real3 const>(pss, 1), params, config, dt,
+      true, true, true, unit_grad != 0);
+  *energy = e[0];
+  for (int i = 0; i < 3; ++i) force3[i] = f[0][i];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) dforce9[3 * i + j] = df[0][i][j];
+}
+
 // fem::StressWork<1> over one Pk3DElement<1,1> built from rest coordinates (mochi_core/include/
 // mochi_core/element_operations/fem_stress.h:107), Smith Neo-Hookean response, PSD oracle Correct.
 // X12 = 4 rest nodes, u12 = 4 nodal displacements. res12 / K144 are overwritten.

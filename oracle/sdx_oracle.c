@@ -400,6 +400,140 @@ void or_penalty(double d, const double grad[3], double k, double t_half, double 
       for (int j = 0; j < 3; ++j) dforce[i * 3 + j] = dfn * grad[i] * grad[j];
 }
 
+/* Coulomb smoothing of the tangential displacement x >= 0 over the width t: value f, derivatives df,
+ * ddf and df/x (finite at x = 0).
+ * model 0, the C1 step of Incremental Potential Contact (Li et al. 2020): df rises as 2x/t - x^2/t^2
+ * on [0, t) and is 1 above (mochi_core/.../utils/activations.h:150-168);
+ * model 1, the C-infinity regularization f = sqrt(x^2 + t^2/4) - t/2 with t clamped to the machine
+ * epsilon (activations.h:188-207). */
+static void or_friction_smoother(int model, double x, double t, double* f, double* df, double* ddf,
+                                 double* dfx) {
+  if (model == 1) {
+    const double e = t > DBL_EPSILON ? t : DBL_EPSILON;
+    const double e2 = 0.25 * e * e;
+    const double sq = sqrt(x * x + e2);
+    *f = sq - 0.5 * e;
+    *dfx = 1.0 / sq;
+    *df = x / sq;
+    *ddf = e2 / (sq * sq * sq);
+    return;
+  }
+  const double r = x / t;
+  if (x >= t) {
+    *f = x - t / 3.0;
+    *ddf = 0.0;
+    *dfx = x == 0.0 ? 0.0 : 1.0 / x;
+    *df = 1.0;
+    return;
+  }
+  *f = x * r * (1.0 - r / 3.0);
+  *ddf = 2.0 * (1.0 - r) / t;
+  *dfx = (2.0 - r) / t;
+  *df = x * *dfx;
+}
+
+static double dot3(const double a[3], const double b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+void or_collision_response(const or_contact_params* p, double d, const double grad[3], double d_ss,
+                           const double grad_ss[3], const double n_col[3], const double pos[3],
+                           const double pos_ss[3], double dt, int unit_grad, double* energy,
+                           double force[3], double dforce[9]) {
+  /* normals: the collider's (SDF gradient, stage-start with explicit normals) and the colliding
+   * surface's; contact is masked when they are more aligned than max_align, and the dissipation's
+   * normal force fades with the alignment (contact_utils.h:1058-1095) */
+  const double* nc = p->explicit_normals ? grad_ss : grad;
+  const int valid = n_col != NULL;
+  const double align = valid ? dot3(nc, n_col) : -1.0;
+  const int on = align <= p->max_align;
+  const double afac = (p->fade && valid && p->max_align > -1.0) ? (p->max_align - align) / (p->max_align + 1.0)
+                                                               : 1.0;
+  /* penalty with the current distance and gradient (contact_utils.h:498-570) */
+  double pv, dp, ddp;
+  or_polyrelu(-d, p->t_half, p->t_half - p->thr, &pv, &dp, &ddp);
+  if (!on) pv = dp = ddp = 0.0;
+  double E = 0.5 * p->k * pv * pv;
+  const double fn = p->k * pv * dp, dfn = -p->k * (dp * dp + pv * ddp);
+  double F[3], D[9];
+  for (int i = 0; i < 3; ++i) {
+    F[i] = fn * grad[i];
+    for (int j = 0; j < 3; ++j) D[3 * i + j] = dfn * grad[i] * grad[j];
+  }
+  const int diss = p->coulomb > 0.0 || p->viscous > 0.0 || p->normal_damping > 0.0;
+  if (diss) {
+    /* the dissipation's normal force: current (implicit) or at the stage-start distance, exact with
+     * explicit normals, else estimated along the current gradient (contact_utils.h:1133-1175) */
+    double fP;
+    double prel[3];
+    for (int i = 0; i < 3; ++i) prel[i] = pos[i] - pos_ss[i];
+    if (p->implicit_normal_force) {
+      fP = afac * fn;
+    } else {
+      const double dss = p->explicit_normals ? d_ss : d - dot3(grad, prel);
+      double q, dq, ddq;
+      or_polyrelu(-dss, p->t_half, p->t_half - p->thr, &q, &dq, &ddq);
+      if (!on) q = dq = 0.0;
+      fP = afac * p->k * q * dq;
+    }
+    /* friction plane normal (contact_utils.h:643-690) */
+    double n[3];
+    if (p->collider_normal || !valid) {
+      for (int i = 0; i < 3; ++i) n[i] = nc[i];
+      if (!unit_grad) {
+        const double nl = sqrt(dot3(n, n));
+        for (int i = 0; i < 3; ++i) n[i] /= nl;
+        if (nl < 100.0 * 1e-6)
+          for (int i = 0; i < 3; ++i) n[i] = valid ? -n_col[i] : 0.0;
+      }
+    } else {
+      for (int i = 0; i < 3; ++i) n[i] = -n_col[i];
+    }
+    const double pn = dot3(prel, n);
+    double pt[3];
+    for (int i = 0; i < 3; ++i) pt[i] = prel[i] - pn * n[i];
+    const double tn = sqrt(dot3(pt, pt));
+    /* dforce = eigP (I - n n^T) + eigN n n^T [+ (eigT - eigP) t t^T]; energy = fP * factor
+     * (contact_utils.h:700-960, GradTarget::Current) */
+    double ef = 0.0, eigP = 0.0, eigN = 0.0, eigDT = 0.0, tg[3] = {0.0, 0.0, 0.0};
+    if (p->coulomb > 0.0) {
+      double f, df, ddf, dfx;
+      or_friction_smoother(p->model, tn, p->falloff_vel * dt, &f, &df, &ddf, &dfx);
+      ef = p->coulomb * f;
+      const double c = p->coulomb * fP * dfx;
+      for (int i = 0; i < 3; ++i) F[i] -= c * pt[i];
+      eigP = -c;
+      if (!p->fitted) {
+        const double eigT = -p->coulomb * fP * ddf;
+        const double inv = 1.0 / (tn + DBL_MIN);
+        for (int i = 0; i < 3; ++i) tg[i] = pt[i] * inv;
+        eigDT = tn > 1e-11 ? eigT - eigP : 0.0;
+      }
+    }
+    if (p->viscous > 0.0) {
+      const double cv = p->viscous / dt;
+      ef += 0.5 * cv * tn * tn;
+      for (int i = 0; i < 3; ++i) F[i] -= cv * fP * pt[i];
+      eigP -= cv * fP;
+    }
+    if (p->normal_damping > 0.0) {
+      const double cn = p->normal_damping / dt;
+      ef += 0.5 * cn * pn * pn;
+      for (int i = 0; i < 3; ++i) F[i] -= cn * fP * pn * n[i];
+      eigN = -cn * fP;
+    }
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        D[3 * i + j] += (i == j ? eigP : 0.0) + (eigN - eigP) * n[i] * n[j];
+        if (!p->fitted && p->coulomb > 0.0) D[3 * i + j] += eigDT * tg[i] * tg[j];
+      }
+    E += fP * ef;
+  }
+  if (energy) *energy = E;
+  if (force)
+    for (int i = 0; i < 3; ++i) force[i] = F[i];
+  if (dforce)
+    for (int i = 0; i < 9; ++i) dforce[i] = D[i];
+}
+
 /* Signed distance and gradient of a collider at time t. Plane: d = n.x - (o + (n.v) t).
  * Capsule: distance to the moving segment a(t) b(t) minus the radius (closed form). */
 static void collider_sdf(const or_collider* c, const double x[3], double t, double* d,
@@ -662,6 +796,20 @@ static int cmp_i64(const void* a, const void* b) {
   return (x > y) - (x < y);
 }
 
+/* Unit normal (x1 - x0) x (x2 - x0) of a deformed boundary face (zero for a degenerate face). */
+static void face_normal(double xn[3][3], double nrm[3]) {
+  double e1[3], e2[3];
+  for (int r = 0; r < 3; ++r) {
+    e1[r] = xn[1][r] - xn[0][r];
+    e2[r] = xn[2][r] - xn[0][r];
+  }
+  nrm[0] = e1[1] * e2[2] - e1[2] * e2[1];
+  nrm[1] = e1[2] * e2[0] - e1[0] * e2[2];
+  nrm[2] = e1[0] * e2[1] - e1[1] * e2[0];
+  const double nl = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+  for (int r = 0; r < 3; ++r) nrm[r] = nl > 0.0 ? nrm[r] / nl : 0.0;
+}
+
 int64_t or_assemble(const or_scene* s, const double* u, const double* ut, double t, int flags,
                     double* obj, double* g, double* H, int64_t* pair_out) {
   const int want_obj = flags & OR_ASM_OBJ, want_res = flags & OR_ASM_RES,
@@ -780,40 +928,68 @@ int64_t or_assemble(const or_scene* s, const double* u, const double* ut, double
     }
   }
 
-  /* Contact: boundary samples (P1Q3 trace elements) against kinematic colliders, penalty response
-   * (contact_utils.h:498-570) integrated by TractionWork (fem_traction.h:58-178). */
+  /* Contact: boundary samples (P1Q3 trace elements) against kinematic colliders (rigid translations
+   * with velocity vel), the penalty response with Coulomb / viscous friction and normal damping
+   * (or_collision_response), integrated by TractionWork (fem_traction.h:58-178). The stage start is
+   * u_stage at time t - dt (NULL: the current displacement). The contact set is the samples closer than
+   * thr, plus with explicit normals those closer than thr at the stage start, which enter with d = thr
+   * and the stage-start gradient (mochi_physics/src/mochi_stage_start_contact.cpp:205-318). */
   int64_t n_pairs = 0;
   int64_t cap = pair_out ? 3 * (int64_t)s->n_faces * (s->n_colliders > 0 ? s->n_colliders : 1) : 0;
   int64_t* pairs = pair_out ? (int64_t*)malloc(sizeof(int64_t) * (size_t)(cap ? cap : 1)) : NULL;
   if (s->n_colliders > 0) {
+    or_contact_params cp;
+    cp.k = s->k_contact;
+    cp.t_half = s->t_half;
+    cp.thr = s->thr;
+    cp.max_align = s->max_align;
+    cp.coulomb = s->coulomb;
+    cp.falloff_vel = s->falloff_vel;
+    cp.viscous = s->viscous;
+    cp.normal_damping = s->normal_damping;
+    cp.collider_normal = s->collider_normal;
+    cp.explicit_normals = s->explicit_normals;
+    cp.fade = s->fade;
+    cp.implicit_normal_force = s->implicit_normal_force;
+    cp.fitted = s->fitted;
+    cp.model = s->friction_model;
+    const int diss = cp.coulomb > 0.0 || cp.viscous > 0.0 || cp.normal_damping > 0.0;
+    const int need_ss = diss || cp.explicit_normals;
+    const double* us = s->u_stage ? s->u_stage : u;
+    const double t0 = t - s->dt;
 #pragma omp parallel for schedule(static) reduction(+ : energy)
     for (int64_t f = 0; f < s->n_faces; ++f) {
       const int32_t* fn = s->face_nodes + 3 * f;
-      double xn[3][3];
+      double xn[3][3], xn0[3][3], nrm[3], nrm0[3];
       for (int k = 0; k < 3; ++k)
-        for (int r = 0; r < 3; ++r)
+        for (int r = 0; r < 3; ++r) {
           xn[k][r] = s->X[3 * (int64_t)fn[k] + r] + u[3 * (int64_t)fn[k] + r];
-      double e1[3], e2[3], nrm[3];
-      for (int r = 0; r < 3; ++r) {
-        e1[r] = xn[1][r] - xn[0][r];
-        e2[r] = xn[2][r] - xn[0][r];
-      }
-      nrm[0] = e1[1] * e2[2] - e1[2] * e2[1];
-      nrm[1] = e1[2] * e2[0] - e1[0] * e2[2];
-      nrm[2] = e1[0] * e2[1] - e1[1] * e2[0];
-      double nl = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
-      for (int r = 0; r < 3; ++r) nrm[r] = nl > 0.0 ? nrm[r] / nl : 0.0;
+          xn0[k][r] = s->X[3 * (int64_t)fn[k] + r] + us[3 * (int64_t)fn[k] + r];
+        }
+      face_normal(xn, nrm);
+      face_normal(xn0, nrm0);
       const double wq = s->face_area[f] / 3.0;
       for (int q = 0; q < 3; ++q) {
-        double xs[3];
-        for (int r = 0; r < 3; ++r)
+        double xs[3], xs0[3];
+        for (int r = 0; r < 3; ++r) {
           xs[r] = kFaceW[q][0] * xn[0][r] + kFaceW[q][1] * xn[1][r] + kFaceW[q][2] * xn[2][r];
+          xs0[r] = kFaceW[q][0] * xn0[0][r] + kFaceW[q][1] * xn0[1][r] + kFaceW[q][2] * xn0[2][r];
+        }
         for (int c = 0; c < s->n_colliders; ++c) {
-          double d, gr[3];
-          collider_sdf(&s->colliders[c], xs, t, &d, gr);
-          if (!(d < s->thr)) continue;
-          double align = gr[0] * nrm[0] + gr[1] * nrm[1] + gr[2] * nrm[2];
-          if (align > s->max_align) continue; /* contact_utils.h:1094-1099 */
+          const or_collider* col = &s->colliders[c];
+          double d, gr[3], d0 = 0.0, gr0[3] = {0.0, 0.0, 0.0};
+          collider_sdf(col, xs, t, &d, gr);
+          if (need_ss) collider_sdf(col, xs0, t0, &d0, gr0);
+          const int cur = d < s->thr;
+          const int ss = cp.explicit_normals && d0 < s->thr;
+          if (!cur && !ss) continue;
+          if (!cur) { /* in contact at the stage start only */
+            d = s->thr;
+            for (int r = 0; r < 3; ++r) gr[r] = gr0[r];
+          }
+          const double* ncol = cp.explicit_normals ? nrm0 : nrm;
+          const double* nc = cp.explicit_normals ? gr0 : gr;
+          if (nc[0] * ncol[0] + nc[1] * ncol[1] + nc[2] * ncol[2] > s->max_align) continue; /* masked */
           if (pairs) {
             int64_t slot;
 #pragma omp atomic capture
@@ -823,8 +999,14 @@ int64_t or_assemble(const or_scene* s, const double* u, const double* ut, double
 #pragma omp atomic
             n_pairs++;
           }
+          /* sample positions in the collider frame, now and at the stage start */
+          double pos[3], pos0[3];
+          for (int r = 0; r < 3; ++r) {
+            pos[r] = xs[r] - col->vel[r] * t;
+            pos0[r] = xs0[r] - col->vel[r] * t0;
+          }
           double E, force[3], dforce[9];
-          or_penalty(d, gr, s->k_contact, s->t_half, s->thr, &E, force, dforce);
+          or_collision_response(&cp, d, gr, d0, gr0, ncol, pos, pos0, s->dt, 1, &E, force, dforce);
           if (want_obj) energy += E * wq;
           if (want_res)
             for (int k = 0; k < 3; ++k)

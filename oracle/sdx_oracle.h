@@ -78,6 +78,32 @@ void or_polyrelu(double x, double t, double shift, double* f, double* df, double
 void or_penalty(double d, const double grad[3], double k, double t_half, double thr,
                 double* energy, double force[3], double dforce[9]);
 
+/* Contact response parameters (ContactParams, ContactEvalConfig; mochi_core/.../contact/
+ * contact_params.h:80-260, contact_utils.h:459-490). */
+typedef struct {
+  double k, t_half, thr, max_align;       /* penalty stiffness, smoothing half distance, threshold,
+                                             maxAlignmentNormals */
+  double coulomb, falloff_vel;            /* coulombFrictionCoefficient, frictionFalloffVel [m/s] */
+  double viscous, normal_damping;         /* viscousFrictionCoefficient, normalViscousDampingCoefficient [s/m] */
+  int collider_normal;                    /* frictionWithColliderNormal */
+  int explicit_normals;                   /* explicitNormals */
+  int fade;                               /* fadeFriction */
+  int implicit_normal_force;              /* implicitNormalForceForDissipation */
+  int fitted;                             /* fittedSaturationHessian.contactFriction */
+  int model;                              /* CoulombFrictionModel: 0 C1Regularized, 1 CinfRegularized */
+} or_contact_params;
+
+/* Contact response of one sample in the collider frame: penalty plus Coulomb / viscous friction and
+ * normal viscous damping, GradTarget::Current. mochi_core/.../contact/contact_utils.h:1003-1230
+ * (ComputeBatchCollisionForceDForce) and 627-960 (ComputeBatchContactDissipationForceDForce).
+ * d, grad: current SDF value and gradient; d_ss, grad_ss: at the stage start (read with explicit
+ * normals); n_col: colliding surface normal (NULL: not valid); pos, pos_ss: current and stage-start
+ * sample positions; dt: the stage's dtFactor. dforce (row-major) is d force / d pos. */
+void or_collision_response(const or_contact_params* p, double d, const double grad[3], double d_ss,
+                           const double grad_ss[3], const double n_col[3], const double pos[3],
+                           const double pos_ss[3], double dt, int unit_grad, double* energy,
+                           double force[3], double dforce[9]);
+
 /* ---- mesh / pattern ---------------------------------------------------------------- */
 
 /* Number of nonzero 3x3 blocks of the node-node adjacency induced by the tets (diagonal included). */
@@ -145,6 +171,9 @@ typedef struct {
    * and its geometric term (stiffnessDampingIncludeGeometricTerm) */
   double stiffness_damping;
   int stiffness_damping_geometric;
+  /* contact dissipation and evaluation settings (or_contact_params; k, t_half, thr, max_align above) */
+  double coulomb, falloff_vel, viscous, normal_damping;
+  int collider_normal, explicit_normals, fade, implicit_normal_force, fitted, friction_model;
 } or_scene;
 
 /* Consistent P1 mass coupling per block (Q4 quadrature, exact for P1): m_ij = sum_t rho V (1+d_ij)/20.

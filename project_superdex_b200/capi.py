@@ -62,7 +62,12 @@ class StepParams(C.Structure):
                 ("ls_alpha", C.c_double), ("ew_forcing", C.c_int), ("rel_div_tol", C.c_double),
                 ("abs_div_tol", C.c_double), ("warm_start", C.c_int), ("linear", LinearParams),
                 ("mass_damping", C.c_double), ("stiffness_damping", C.c_double),
-                ("stiffness_damping_geometric", C.c_int)]
+                ("stiffness_damping_geometric", C.c_int), ("friction_coulomb", C.c_double),
+                ("friction_falloff_vel", C.c_double), ("friction_viscous", C.c_double),
+                ("contact_normal_damping", C.c_double), ("friction_model", C.c_int),
+                ("friction_fitted_hessian", C.c_int), ("friction_fade", C.c_int),
+                ("friction_collider_normal", C.c_int), ("contact_explicit_normals", C.c_int),
+                ("contact_implicit_normal_force", C.c_int)]
 
 
 class EnvStats(C.Structure):

@@ -553,6 +553,88 @@ __device__ __forceinline__ void polyrelu(double x, double t, double shift, doubl
   ddf = fmax(ddfv, 0.0);
 }
 
+// Coulomb smoothing of the tangential displacement x >= 0 over the width t: value f, f'' and f'/x.
+// cinf = false: the C1 step of Incremental Potential Contact (Li et al. 2020), f' = 2x/t - x^2/t^2 on
+// [0, t), 1 above (activations.h:150-168); cinf = true: f = sqrt(x^2 + t^2/4) - t/2 with t clamped to the
+// FP64 machine epsilon (activations.h:188-207).
+__device__ __forceinline__ void friction_smoother(bool cinf, double x, double t, double& f, double& ddf,
+                                                  double& dfx) {
+  if (cinf) {
+    const double e = fmax(t, 2.220446049250313e-16);
+    const double e2 = 0.25 * e * e;
+    const double sq = sqrt(x * x + e2);
+    f = sq - 0.5 * e;
+    dfx = 1.0 / sq;
+    ddf = e2 / (sq * sq * sq);
+    return;
+  }
+  if (x >= t) {
+    f = x - t / 3.0;
+    ddf = 0.0;
+    dfx = x == 0.0 ? 0.0 : 1.0 / x;
+    return;
+  }
+  const double r = x / t;
+  f = x * r * (1.0 - r / 3.0);
+  ddf = 2.0 * (1.0 - r) / t;
+  dfx = (2.0 - r) / t;
+}
+
+// Dissipative part of one unmasked contact sample (ComputeBatchContactDissipationForceDForce,
+// contact_utils.h:627-960, GradTarget::Current): Coulomb / viscous friction in the plane normal to n and
+// normal viscous damping, scaled by the normal force fP, for the displacement prel relative to the
+// collider. Adds to the energy E, the force F and the symmetric dforce D (xx, yy, zz, xy, xz, yz).
+__device__ __forceinline__ void dissipation_response(double coulomb, double falloff, double viscous,
+                                                     double ndamp, bool fitted, bool cinf, double fP,
+                                                     const double n[3], const double prel[3], double& E,
+                                                     double F[3], double D[6]) {
+  const double pn = prel[0] * n[0] + prel[1] * n[1] + prel[2] * n[2];
+  double pt[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) pt[i] = prel[i] - pn * n[i];
+  const double tn = sqrt(pt[0] * pt[0] + pt[1] * pt[1] + pt[2] * pt[2]);
+  double ef = 0.0, eigP = 0.0, eigN = 0.0, eigDT = 0.0;
+  if (coulomb > 0.0) {
+    double f, ddf, dfx;
+    friction_smoother(cinf, tn, falloff, f, ddf, dfx);
+    ef = coulomb * f;
+    const double c = coulomb * fP * dfx;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) F[i] -= c * pt[i];
+    eigP = -c;
+    if (!fitted && tn > 1e-11) eigDT = -coulomb * fP * ddf - eigP;
+  }
+  if (viscous > 0.0) {
+    ef += 0.5 * viscous * tn * tn;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) F[i] -= viscous * fP * pt[i];
+    eigP -= viscous * fP;
+  }
+  if (ndamp > 0.0) {
+    ef += 0.5 * ndamp * pn * pn;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) F[i] -= ndamp * fP * pn * n[i];
+    eigN = -ndamp * fP;
+  }
+  const double dn = eigN - eigP;
+  D[0] += eigP + dn * n[0] * n[0];
+  D[1] += eigP + dn * n[1] * n[1];
+  D[2] += eigP + dn * n[2] * n[2];
+  D[3] += dn * n[0] * n[1];
+  D[4] += dn * n[0] * n[2];
+  D[5] += dn * n[1] * n[2];
+  if (eigDT != 0.0) {
+    const double inv = 1.0 / (tn + 2.2250738585072014e-308), w = eigDT * inv * inv;
+    D[0] += w * pt[0] * pt[0];
+    D[1] += w * pt[1] * pt[1];
+    D[2] += w * pt[2] * pt[2];
+    D[3] += w * pt[0] * pt[1];
+    D[4] += w * pt[0] * pt[2];
+    D[5] += w * pt[1] * pt[2];
+  }
+  E += fP * ef;
+}
+
 // collider row: (type, p[6], radius, vel[3])
 __device__ __forceinline__ void collider_sdf(const double* c, const double x[3], double t, double& d,
                                              double g[3]) {

@@ -831,6 +831,11 @@ extern "C" void sdx_default_step_params(sdx_step_params* p) {
   p->abs_div_tol = 1e9;
   p->warm_start = SDX_WARM_ZERO;
   sdx_default_linear_params(&p->linear);
+  p->friction_falloff_vel = 0.01;
+  p->friction_model = SDX_FRICTION_C1;
+  p->friction_fitted_hessian = 1;
+  p->friction_fade = 1;
+  p->friction_collider_normal = 1;
 }
 
 extern "C" sdx_context* sdx_create(int device) {
@@ -910,6 +915,18 @@ extern "C" int sdx_set_params(sdx_context* c, const sdx_step_params* p) {
     return set_error(SDX_ERR_INVALID_ARGUMENT, "stiffness_damping must be >= 0");
   if (p->linear.preconditioner < 0 || p->linear.preconditioner > 2)
     return set_error(SDX_ERR_INVALID_ARGUMENT, "unknown preconditioner %d", p->linear.preconditioner);
+  // contact dissipation (the reference asserts the same ranges, contact_utils.h:635-640, 1040-1048)
+  if (!(p->friction_coulomb >= 0.0) || !(p->friction_viscous >= 0.0) || !(p->contact_normal_damping >= 0.0))
+    return set_error(SDX_ERR_INVALID_ARGUMENT, "friction and damping coefficients must be >= 0");
+  if (!(p->friction_falloff_vel >= 0.0))
+    return set_error(SDX_ERR_INVALID_ARGUMENT, "friction_falloff_vel must be >= 0");
+  if (p->friction_model != SDX_FRICTION_C1 && p->friction_model != SDX_FRICTION_CINF)
+    return set_error(SDX_ERR_INVALID_ARGUMENT, "unknown friction model %d", p->friction_model);
+  if (p->contact_explicit_normals && p->contact_implicit_normal_force)
+    return set_error(SDX_ERR_INVALID_ARGUMENT,
+                     "implicit normal force for dissipation is not supported with explicit normals");
+  if (!(p->max_align >= -1.0 && p->max_align <= 1.0))
+    return set_error(SDX_ERR_INVALID_ARGUMENT, "max_align must be in [-1, 1]");
   c->params = *p;
   return SDX_OK;
 }
@@ -1430,6 +1447,17 @@ static void assemble_dev(sdx_context* c, const double* u, const double* ut, doub
     ca.thr = p.thr;
     ca.max_align = p.max_align;
     ca.flags = flags;
+    ca.u0 = c->u0;
+    ca.t0 = t - p.dt;
+    ca.coulomb = p.friction_coulomb;
+    ca.falloff = p.friction_falloff_vel * p.dt;
+    ca.viscous = p.friction_viscous / p.dt;
+    ca.normal_damping = p.contact_normal_damping / p.dt;
+    ca.cflags = (p.friction_collider_normal ? kContactColliderNormal : 0) |
+                (p.contact_explicit_normals ? kContactExplicit : 0) | (p.friction_fade ? kContactFade : 0) |
+                (p.contact_implicit_normal_force ? kContactImplicitFn : 0) |
+                (p.friction_fitted_hessian ? kContactFitted : 0) |
+                (p.friction_model == SDX_FRICTION_CINF ? kContactCinf : 0);
     prof_begin(c, &ev);
     launch_contact(ca, c->stream);
     c->launches++;

@@ -89,7 +89,22 @@ struct ContactArgs {
   unsigned long long* n_pairs;  // per env
   double t, k, t_half, thr, max_align;
   int flags;
+  // contact dissipation and evaluation settings (ContactParams, ContactEvalConfig)
+  const double* u0;   // stage-start displacement (time t0); read when dissipative or explicit normals
+  double t0;          // stage-start time
+  double coulomb;     // coulombFrictionCoefficient
+  double falloff;     // frictionFalloffVel * dt: the smoothing width in displacement
+  double viscous, normal_damping;  // viscousFrictionCoefficient / dt, normalViscousDampingCoefficient / dt
+  int cflags;         // kContact* bits
 };
+
+// ContactArgs::cflags
+constexpr int kContactColliderNormal = 1;  // frictionWithColliderNormal
+constexpr int kContactExplicit = 2;        // explicitNormals
+constexpr int kContactFade = 4;            // fadeFriction
+constexpr int kContactImplicitFn = 8;      // implicitNormalForceForDissipation
+constexpr int kContactFitted = 16;         // fittedSaturationHessian.contactFriction
+constexpr int kContactCinf = 32;           // CoulombFrictionModel::CinfRegularized
 
 // CG scalars of one env carried across a re-partitioning relaunch
 struct EnvSave {

@@ -311,6 +311,27 @@ __constant__ double c_face_w[3][3] = {{2.0 / 3.0, 1.0 / 6.0, 1.0 / 6.0},
                                       {1.0 / 6.0, 2.0 / 3.0, 1.0 / 6.0},
                                       {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0}};
 
+__device__ __forceinline__ void face_normal(const double xn[3][3], double nrm[3]) {
+  double e1[3], e2[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    e1[r] = xn[1][r] - xn[0][r];
+    e2[r] = xn[2][r] - xn[0][r];
+  }
+  nrm[0] = e1[1] * e2[2] - e1[2] * e2[1];
+  nrm[1] = e1[2] * e2[0] - e1[0] * e2[2];
+  nrm[2] = e1[0] * e2[1] - e1[1] * e2[0];
+  const double nl = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+#pragma unroll
+  for (int r = 0; r < 3; ++r) nrm[r] = nl > 0.0 ? nrm[r] / nl : 0.0;
+}
+
+// Per (sample, collider) pair: the penalty response (contact_utils.h:498-570) with the alignment mask
+// and, when dissipative, Coulomb / viscous friction and normal damping driven by the sample's displacement
+// relative to the collider since the stage start (u0 at t0) and by the normal force at the stage-start
+// distance (contact_utils.h:1003-1230). Colliders are rigid translations, so the collider frame is the
+// world frame moved by vel t. With explicit normals the alignment, the friction plane and the normal
+// force come from the stage start, and pairs in contact only at the stage start enter with d = thr.
 __global__ void __launch_bounds__(128) k_contact(ContactArgs a) {
   const int64_t sidx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (sidx >= a.n_samples) return;
@@ -321,52 +342,103 @@ __global__ void __launch_bounds__(128) k_contact(ContactArgs a) {
   unsigned bits = 0;
   if (!a.env_mask || a.env_mask[env]) {
     const int rows[3] = {fr.x, fr.y, fr.z};
-    double xn[3][3];
+    const bool diss = a.coulomb > 0.0 || a.viscous > 0.0 || a.normal_damping > 0.0;
+    const bool expl = (a.cflags & kContactExplicit) != 0;
+    const bool need_ss = (diss || expl) && a.u0 != nullptr;
+    double xn[3][3], xs[3], nrm[3], xs0[3], nrm0[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k)
 #pragma unroll
       for (int r = 0; r < 3; ++r) xn[k][r] = a.X[3 * (int64_t)rows[k] + r] + a.u[3 * (int64_t)rows[k] + r];
-    double e1[3], e2[3], nrm[3];
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-      e1[r] = xn[1][r] - xn[0][r];
-      e2[r] = xn[2][r] - xn[0][r];
-    }
-    nrm[0] = e1[1] * e2[2] - e1[2] * e2[1];
-    nrm[1] = e1[2] * e2[0] - e1[0] * e2[2];
-    nrm[2] = e1[0] * e2[1] - e1[1] * e2[0];
-    const double nl = sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
-#pragma unroll
-    for (int r = 0; r < 3; ++r) nrm[r] = nl > 0.0 ? nrm[r] / nl : 0.0;
-    double xs[3];
+    face_normal(xn, nrm);
 #pragma unroll
     for (int r = 0; r < 3; ++r)
       xs[r] = c_face_w[q][0] * xn[0][r] + c_face_w[q][1] * xn[1][r] + c_face_w[q][2] * xn[2][r];
+    if (need_ss) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int r = 0; r < 3; ++r) xn[k][r] = a.X[3 * (int64_t)rows[k] + r] + a.u0[3 * (int64_t)rows[k] + r];
+      face_normal(xn, nrm0);
+#pragma unroll
+      for (int r = 0; r < 3; ++r)
+        xs0[r] = c_face_w[q][0] * xn[0][r] + c_face_w[q][1] * xn[1][r] + c_face_w[q][2] * xn[2][r];
+    } else {
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        nrm0[r] = nrm[r];
+        xs0[r] = xs[r];
+      }
+    }
     const double wq = a.face_area[f] / 3.0;
     const int c0 = a.coll_off[env], c1 = a.coll_off[env + 1];
     double energy = 0.0;
     for (int c = c0; c < c1; ++c) {
-      double d, gr[3];
-      collider_sdf(a.colliders + 11 * (int64_t)c, xs, a.t, d, gr);
-      if (!(d < a.thr)) continue;
-      const double align = gr[0] * nrm[0] + gr[1] * nrm[1] + gr[2] * nrm[2];
-      if (align > a.max_align) continue;
+      const double* crow = a.colliders + 11 * (int64_t)c;
+      double d, gr[3], d0 = 0.0, gr0[3] = {0.0, 0.0, 0.0};
+      collider_sdf(crow, xs, a.t, d, gr);
+      if (need_ss) collider_sdf(crow, xs0, a.t0, d0, gr0);
+      const bool cur = d < a.thr;
+      if (!cur && !(expl && d0 < a.thr)) continue;
+      if (!cur) {  // in contact at the stage start only
+        d = a.thr;
+#pragma unroll
+        for (int r = 0; r < 3; ++r) gr[r] = gr0[r];
+      }
+      const double* nc = expl ? gr0 : gr;
+      const double* ncol = expl ? nrm0 : nrm;
+      const double align = nc[0] * ncol[0] + nc[1] * ncol[1] + nc[2] * ncol[2];
+      if (align > a.max_align) continue;  // masked: no energy, force or dforce
       bits |= 1u << (c - c0);
       double pv, dp, ddp;
       polyrelu(-d, a.t_half, a.t_half - a.thr, pv, dp, ddp);
-      energy += 0.5 * a.k * pv * pv * wq;
-      const double fn = a.k * pv * dp;
+      double E = 0.5 * a.k * pv * pv;
+      const double fn = a.k * pv * dp, dfn = -a.k * (dp * dp + pv * ddp);
+      double F[3], D[6];
+#pragma unroll
+      for (int r = 0; r < 3; ++r) F[r] = fn * gr[r];
+      D[0] = dfn * gr[0] * gr[0];
+      D[1] = dfn * gr[1] * gr[1];
+      D[2] = dfn * gr[2] * gr[2];
+      D[3] = dfn * gr[0] * gr[1];
+      D[4] = dfn * gr[0] * gr[2];
+      D[5] = dfn * gr[1] * gr[2];
+      if (diss) {
+        const double afac = ((a.cflags & kContactFade) && a.max_align > -1.0)
+                                ? (a.max_align - align) / (a.max_align + 1.0)
+                                : 1.0;
+        double prel[3];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) prel[r] = (xs[r] - crow[8 + r] * a.t) - (xs0[r] - crow[8 + r] * a.t0);
+        double fP;
+        if (a.cflags & kContactImplicitFn) {
+          fP = afac * fn;
+        } else {
+          const double dss = expl ? d0 : d - (gr[0] * prel[0] + gr[1] * prel[1] + gr[2] * prel[2]);
+          double qv, dq, ddq;
+          polyrelu(-dss, a.t_half, a.t_half - a.thr, qv, dq, ddq);
+          fP = afac * a.k * qv * dq;
+        }
+        // the collider's normal (unit SDF gradient) or the colliding surface's, flipped
+        double n[3];
+#pragma unroll
+        for (int r = 0; r < 3; ++r) n[r] = (a.cflags & kContactColliderNormal) ? nc[r] : -ncol[r];
+        dissipation_response(a.coulomb, a.falloff, a.viscous, a.normal_damping, (a.cflags & kContactFitted) != 0,
+                             (a.cflags & kContactCinf) != 0, fP, n, prel, E, F, D);
+      }
+      energy += E * wq;
       if (a.flags & 2) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
           const int pk = a.pin[rows[k]];
 #pragma unroll
           for (int r = 0; r < 3; ++r)
-            if (!((pk >> r) & 1)) atomicAdd(a.g + 3 * (int64_t)rows[k] + r, -fn * gr[r] * c_face_w[q][k] * wq);
+            if (!((pk >> r) & 1)) atomicAdd(a.g + 3 * (int64_t)rows[k] + r, -F[r] * c_face_w[q][k] * wq);
         }
       }
       if (a.flags & 4) {
-        const double dfn = -a.k * (dp * dp + pv * ddp);
+        // symmetric index of (r, cc) in D
+        constexpr int kSym[9] = {0, 3, 4, 3, 1, 5, 4, 5, 2};
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
           const int pk = a.pin[rows[k]];
@@ -380,7 +452,7 @@ __global__ void __launch_bounds__(128) k_contact(ContactArgs a) {
 #pragma unroll
               for (int cc = 0; cc < 3; ++cc) {
                 if (((pk >> r) & 1) || ((pl >> cc) & 1)) continue;
-                atomicAdd(a.val + val_index(p, 3 * r + cc), (float)(-dfn * gr[r] * gr[cc] * wkl));
+                atomicAdd(a.val + val_index(p, 3 * r + cc), (float)(-D[kSym[3 * r + cc]] * wkl));
               }
           }
         }

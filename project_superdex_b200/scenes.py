@@ -81,6 +81,18 @@ class SceneConfig:
     mass_damping: float = 0.0     # Rayleigh massDampingCoefficient alpha [1/s]
     stiffness_damping: float = 0.0  # Rayleigh stiffnessDampingCoefficient beta [s]
     stiffness_damping_geometric: bool = False  # stiffnessDampingIncludeGeometricTerm
+    # contact dissipation (ContactParams / ContactEvalConfig); the reference's default Coulomb coefficient
+    # is 0.5, the workloads here are frictionless unless they say otherwise
+    friction_coulomb: float = 0.0
+    friction_falloff_vel: float = 0.01
+    friction_viscous: float = 0.0
+    contact_normal_damping: float = 0.0
+    friction_model: int = 0          # 0 C1Regularized, 1 CinfRegularized
+    friction_fitted_hessian: bool = True
+    friction_fade: bool = True
+    friction_collider_normal: bool = True
+    contact_explicit_normals: bool = False
+    contact_implicit_normal_force: bool = False
 
 
 # Freudenthal split of a hex into 6 tets: paths 0 -> 7 through the corner cube.

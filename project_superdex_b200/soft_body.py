@@ -60,6 +60,13 @@ class SoftBodyWorld:
         self.params.mass_damping = float(getattr(cfg, "mass_damping", 0.0))
         self.params.stiffness_damping = float(getattr(cfg, "stiffness_damping", 0.0))
         self.params.stiffness_damping_geometric = int(bool(getattr(cfg, "stiffness_damping_geometric", False)))
+        for name in ("friction_coulomb", "friction_falloff_vel", "friction_viscous", "contact_normal_damping"):
+            if hasattr(cfg, name):
+                setattr(self.params, name, float(getattr(cfg, name)))
+        for name in ("friction_model", "friction_fitted_hessian", "friction_fade", "friction_collider_normal",
+                     "contact_explicit_normals", "contact_implicit_normal_force"):
+            if hasattr(cfg, name):
+                setattr(self.params, name, int(getattr(cfg, name)))
         for k, v in overrides.items():
             if k.startswith("linear_"):
                 setattr(self.params.linear, k[len("linear_"):], v)

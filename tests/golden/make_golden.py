@@ -94,7 +94,7 @@ def reference_vectors():
     assert R is not None, "oracle/_ref/libsdx_ref.so missing: run oracle/build_ref.sh"
     rng = np.random.default_rng(20261203)
     out = {"smith": [], "polyrelu": [], "penalty": [], "stress_work": [], "pcg": [], "materials": [],
-           "stress_damping": []}
+           "stress_damping": [], "collision": []}
     for i in range(48):
         F = np.eye(3) + rng.normal(0, 0.35, (3, 3))
         if i % 4 == 0:
@@ -195,6 +195,38 @@ def reference_vectors():
         out["stress_damping"].append({"X": Xf.tolist(), "u": u.tolist(), "uss": uss.tolist(), "kappa": kappa,
                                       "lambda": lam, "mu": mu, "geometric": geo, "project": proj,
                                       "energy": float(e[0]), "res": r.tolist(), "K": K.tolist()})
+    # ComputeBatchCollisionForceDForce<1, GradTarget::Current>: penalty + Coulomb / viscous friction + normal
+    # damping over random option sets, distances across the threshold and displacements across the
+    # Coulomb smoothing width (frictionFalloffVel * dt = 4.2e-5 m at the defaults)
+    for i in range(128):
+        kw = dict(coulomb=float(rng.choice([0.0, 0.5, 0.9])), viscous=float(rng.choice([0.0, 0.4])),
+                  normal_damping=float(rng.choice([0.0, 0.3])), collider_normal=int(rng.integers(2)),
+                  explicit_normals=int(rng.integers(2)), fade=int(rng.integers(2)), fitted=int(rng.integers(2)),
+                  model=int(rng.integers(2)), max_align=float(rng.choice([0.0, -0.3, 0.5, -1.0])),
+                  falloff_vel=float(rng.choice([0.01, 0.1, 0.0])), k=float(10 ** rng.uniform(3, 9)))
+        kw["implicit_normal_force"] = 0 if kw["explicit_normals"] else int(rng.integers(2))
+        if kw["falloff_vel"] == 0.0 and kw["model"] == 0 and i % 2:
+            kw["falloff_vel"] = 0.01
+        prm = O.contact_params(**kw)
+        g = rng.normal(size=3)
+        g /= np.linalg.norm(g)
+        gs = g + 0.1 * rng.normal(size=3)
+        gs /= np.linalg.norm(gs)
+        nc = -g + 0.5 * rng.normal(size=3)
+        nc /= np.linalg.norm(nc)
+        d, dss = float(rng.uniform(-0.008, 0.002)), float(rng.uniform(-0.008, 0.002))
+        pos = rng.normal(size=3) * 0.01
+        step = rng.normal(size=3) * float(rng.choice([1e-6, 1e-5, 1e-4, 1e-3]))
+        if i % 16 == 0:
+            step = g * 1e-4  # along the normal: no tangential displacement
+        pss = pos - step
+        valid = i % 5 != 0
+        dt = 1.0 / 240.0
+        e, f, df = O.collision_response(prm, d, g, dss, gs, nc if valid else None, pos, pss, dt, use_ref=True)
+        out["collision"].append({"params": kw, "d": d, "grad": g.tolist(), "d_ss": dss, "grad_ss": gs.tolist(),
+                                 "n_col": nc.tolist() if valid else None, "pos": pos.tolist(),
+                                 "pos_ss": pss.tolist(), "dt": dt, "energy": float(e), "force": f.tolist(),
+                                 "dforce": df.reshape(-1).tolist()})
     out["source"] = "oracle/_ref/libsdx_ref.so (reference sources, FP64 build)"
     return out
 

@@ -164,3 +164,46 @@ def test_stiffness_damping_assembly_matches_oracle(oracle, geometric, psd):
     H_scale = np.abs(a_or["H"]).max()
     np.testing.assert_allclose(a_gpu["H"], a_or["H"], rtol=0, atol=2e-5 * H_scale)
     assert a_gpu["obj"][0] == pytest.approx(a_or["obj"], rel=1e-6)
+
+
+_FRICTION_CASES = [
+    dict(friction_coulomb=0.5),  # the reference's friction defaults: C1, fitted Hessian, fading, collider normal
+    dict(friction_coulomb=0.8, friction_model=1, friction_fitted_hessian=False, friction_viscous=0.3,
+         contact_normal_damping=0.2),
+    dict(friction_coulomb=0.5, contact_explicit_normals=True, friction_fitted_hessian=False,
+         contact_normal_damping=0.1),
+    dict(friction_coulomb=0.4, friction_viscous=0.2, contact_implicit_normal_force=True,
+         friction_collider_normal=False, friction_fade=False),
+]
+
+
+@pytest.mark.parametrize("case", range(len(_FRICTION_CASES)))
+def test_friction_assembly_matches_oracle(oracle, case):
+    """Contact with Coulomb / viscous friction and normal damping (ComputeBatchCollisionForceDForce):
+    capsules pressing and sliding on the top and a plane on the side, the stage start at the state."""
+    b = _body(41 + case)
+    top = b.X[:, 2].max()
+    b.colliders[0] = scenes.capsule((0.012, 0.02, top + 0.0025), (0.032, 0.03, top + 0.0025), 0.004,
+                                    (0.08, 0.03, -0.05))
+    cfg = scenes.SceneConfig(k_contact=1e9, **_FRICTION_CASES[case])
+    w, s = _pair(oracle, b, cfg, 1)
+    rng = np.random.default_rng(500 + case)
+    free = (b.pin == 0).repeat(3)
+    us = rng.normal(0, 3e-4, 3 * b.n_nodes) * free
+    u = us + rng.normal(0, 1e-4, 3 * b.n_nodes) * free
+    v = rng.normal(0, 2e-2, 3 * b.n_nodes) * free
+    w.set_state(us, v, 0.0)
+    t = 0.01
+    a_gpu = w.assemble(u, t=t, psd=True)
+    a_or = s.assemble(u, us + cfg.dt * v, t=t, psd=True, u_stage=us, pairs=True)
+    s0 = oracle.Scene(b, scenes.SceneConfig(k_contact=1e9, contact_explicit_normals=cfg.contact_explicit_normals),
+                      psd_strategy=1, min_eig=float(np.finfo(np.float32).eps))
+    g0 = s0.assemble(u, us + cfg.dt * v, t=t, psd=True, u_stage=us)["g"]
+    g_scale = np.abs(a_or["g"]).max()
+    assert np.abs(a_or["g"] - g0).max() > 0.005 * g_scale  # the dissipative terms: 5000x the tolerance below
+    np.testing.assert_allclose(a_gpu["g"], a_or["g"], rtol=0, atol=1e-6 * g_scale)
+    H_scale = np.abs(a_or["H"]).max()
+    np.testing.assert_allclose(a_gpu["H"], a_or["H"], rtol=0, atol=2e-5 * H_scale)
+    assert a_gpu["obj"][0] == pytest.approx(a_or["obj"], rel=1e-6)
+    assert a_gpu["n_pairs"][0] == a_or["n_pairs"] > 0
+    assert np.array_equal(w.contact_pairs(), a_or["pairs"])

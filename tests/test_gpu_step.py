@@ -125,3 +125,30 @@ def test_stiffness_damped_steps_match_oracle(oracle):
     cfg.stiffness_damping_geometric = True
     w, ug, vg, states, hist = _run(oracle, bodies, cfg, 3)
     _check(bodies, ug, states, hist, newton_exact=False)
+
+
+@pytest.mark.parametrize("opts", [
+    dict(friction_coulomb=0.5),
+    dict(friction_coulomb=0.6, friction_model=1, friction_viscous=0.2, contact_normal_damping=0.1,
+         contact_explicit_normals=True, friction_fitted_hessian=False),
+])
+def test_friction_steps_match_oracle(oracle, opts):
+    """Newton steps with a capsule pressing into the top and sliding along it, Coulomb friction (and
+    viscous friction, normal damping, explicit normals), against the oracle; friction moves the surface
+    well beyond the parity tolerance."""
+    rng = np.random.default_rng(4)
+    b = scenes.grid_body(6, 6, 5, 0.01, rng=rng, E=1e5, nu=0.45)
+    b.colliders = [scenes.capsule((0.02, 0.03, 0.0532), (0.04, 0.03, 0.0532), 0.004, (0.15, 0.0, -0.1))]
+    cfg = scenes.SceneConfig(k_contact=1e8, **opts)
+    w, ug, vg, states, hist = _run(oracle, [b], cfg, 3, newton_abs_tol=1e-9)
+    _check([b], ug, states, hist, newton_exact=False)
+    assert hist[-1][0][0]["n_contacts"] > 0
+    # the same steps without dissipation end elsewhere
+    s0 = oracle.Scene(b, scenes.SceneConfig(k_contact=1e8, contact_explicit_normals=cfg.contact_explicit_normals),
+                      min_eig=float(np.finfo(np.float32).eps))
+    p = oracle.default_newton_params()
+    p.abs_tol = 1e-9
+    u, v = np.zeros(3 * b.n_nodes), np.zeros(3 * b.n_nodes)
+    for k in range(3):
+        u, v, _ = s0.step(u, v, (k + 1) * cfg.dt, p)
+    assert np.abs(u - states[0][0]).max() > 20 * 1e-5 * 0.06

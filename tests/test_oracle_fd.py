@@ -114,3 +114,77 @@ def test_damped_materials_match_finite_differences(oracle, material):
         assert (ep - em) / (2 * h) == pytest.approx(g[i], rel=1e-4, abs=1e-6 * np.abs(g).max())
         col = (s.assemble(up, ut, hess=False, u_stage=us)["g"] - s.assemble(um, ut, hess=False, u_stage=us)["g"]) / (2 * h)
         np.testing.assert_allclose(col[free], H[free, i], rtol=1e-4, atol=1e-4 * np.abs(H[:, i]).max())
+
+
+@pytest.mark.parametrize("model", [0, 1])
+def test_friction_response_is_the_derivative_of_its_energy(oracle, model):
+    """With explicit normals the dissipation's normal force and friction plane are fixed by the stage
+    start, so the dissipative force is minus the gradient of its energy in the sample position and, with
+    the exact (unfitted) Coulomb Hessian, dforce is the force's derivative (contact_utils.h:700-960)."""
+    rng = np.random.default_rng(11 + model)
+    width = 0.01 / 240.0  # frictionFalloffVel * dt
+    kw = dict(k=1e5, coulomb=0.6, viscous=0.2, normal_damping=0.3, explicit_normals=1, fitted=0, model=model)
+    prm = oracle.contact_params(**kw)
+    pen = oracle.contact_params(**{**kw, "coulomb": 0.0, "viscous": 0.0, "normal_damping": 0.0})
+    dt = 1.0 / 240.0
+    for trial in range(16):
+        g = rng.normal(size=3)
+        g /= np.linalg.norm(g)
+        gs = g + 0.05 * rng.normal(size=3)
+        gs /= np.linalg.norm(gs)
+        nc = -gs + 0.2 * rng.normal(size=3)
+        nc /= np.linalg.norm(nc)
+        d, dss = -0.002, float(rng.uniform(-0.004, 0.0))
+        pss = rng.normal(size=3) * 0.01
+        step = rng.normal(size=3) * width * float(rng.choice([0.2, 0.6, 3.0, 30.0]))
+        pos = pss + step
+        e0, f0, d0 = oracle.collision_response(pen, d, g, dss, gs, nc, pos, pss, dt)
+        e, f, D = oracle.collision_response(prm, d, g, dss, gs, nc, pos, pss, dt)
+        fd, Dd = f - f0, D - d0
+        h = 1e-4 * np.linalg.norm(step)
+        for i in range(3):
+            dp = np.zeros(3)
+            dp[i] = h
+            ep, fp, _ = oracle.collision_response(prm, d, g, dss, gs, nc, pos + dp, pss, dt)
+            em, fm, _ = oracle.collision_response(prm, d, g, dss, gs, nc, pos - dp, pss, dt)
+            assert -(ep - em) / (2 * h) == pytest.approx(fd[i], rel=1e-5, abs=1e-7 * np.abs(fd).max())
+            np.testing.assert_allclose((fp - fm) / (2 * h), Dd[:, i], rtol=1e-4, atol=1e-5 * np.abs(Dd).max())
+
+
+def test_friction_with_explicit_normals_is_a_gradient_system(oracle):
+    """Assembled over a body with a plane pressing on its top and sliding along it: with explicit normals
+    the contact residual is the exact gradient of the contact merit (ExperimentalEvalParams::
+    explicitNormals, eval_params.h:73-85), and with the unfitted Coulomb Hessian and a flat collider the
+    Hessian is its exact derivative."""
+    rng = np.random.default_rng(7)
+    n = 3
+    b = scenes.grid_body(n, n, n, 0.01, rng=rng, E=2e4, nu=0.4)
+    top = n * 0.01
+    b.colliders = [scenes.plane((0, 0, -1), -(top - 0.0015), (0.05, 0.02, 0.0))]
+    kw = dict(friction_coulomb=0.6, friction_viscous=0.1, contact_normal_damping=0.05, contact_explicit_normals=True,
+              friction_fitted_hessian=False)
+    cfg = scenes.SceneConfig(k_contact=1e9, **kw)  # the reference's default penalty stiffness
+    s = oracle.Scene(b, cfg, psd_strategy=0)
+    free = (b.pin == 0).repeat(3)
+    us = rng.normal(0, 1e-4, 3 * b.n_nodes) * free
+    u = us + rng.normal(0, 6e-5, 3 * b.n_nodes) * free
+    ut = us.copy()
+    t = 0.02
+    out = s.assemble(u, ut, t=t, psd=False, u_stage=us)
+    assert out["n_pairs"] > 0
+    s0 = oracle.Scene(b, scenes.SceneConfig(k_contact=1e9, contact_explicit_normals=True), psd_strategy=0)
+    g0 = s0.assemble(u, ut, t=t, psd=False, u_stage=us)["g"]
+    assert np.abs(out["g"] - g0).max() > 0.2 * np.abs(out["g"]).max()  # the dissipative terms matter here
+    g, H = out["g"], oracle.bsr_to_dense(s.row_ptr, s.col, out["H"])
+    h = 1e-8
+    top_nodes = np.nonzero(np.abs(b.X[:, 2] - top) < 1e-9)[0]
+    idx = [3 * i + r for i in top_nodes[:: max(1, top_nodes.size // 6)] for r in range(3)]
+    for i in idx:
+        up, um = u.copy(), u.copy()
+        up[i] += h
+        um[i] -= h
+        ap = s.assemble(up, ut, t=t, hess=False, u_stage=us)
+        am = s.assemble(um, ut, t=t, hess=False, u_stage=us)
+        assert (ap["obj"] - am["obj"]) / (2 * h) == pytest.approx(g[i], rel=1e-5, abs=1e-7 * np.abs(g).max())
+        col = (ap["g"] - am["g"]) / (2 * h)
+        np.testing.assert_allclose(col[free], H[free, i], rtol=1e-4, atol=1e-5 * np.abs(H[:, i]).max())

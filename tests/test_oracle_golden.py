@@ -158,3 +158,25 @@ def test_stiffness_damping_matches_reference_code(oracle, golden):
         assert e[0] == pytest.approx(c["energy"], rel=1e-11, abs=1e-18)
         np.testing.assert_allclose(r, c["res"], rtol=1e-10, atol=1e-12 * np.abs(c["res"]).max())
         np.testing.assert_allclose(K, c["K"], rtol=1e-10, atol=1e-12 * np.abs(c["K"]).max())
+
+
+def test_collision_response_matches_reference_code(oracle, golden):
+    """or_collision_response (penalty + Coulomb / viscous friction + normal viscous damping) against the
+    reference's ComputeBatchCollisionForceDForce<1, GradTarget::Current> compiled from its sources, over
+    random option sets (friction model, fitted Hessian, explicit normals, implicit normal force, fading,
+    friction normal, invalid colliding normals)."""
+    v = golden("reference_vectors.json")["collision"]
+    assert len(v) == 128
+    n_diss = 0
+    for c in v:
+        prm = oracle.contact_params(**c["params"])
+        e, f, df = oracle.collision_response(prm, c["d"], c["grad"], c["d_ss"], c["grad_ss"], c["n_col"], c["pos"],
+                                             c["pos_ss"], c["dt"])
+        fs = max(np.abs(c["force"]).max(), 1e-300)
+        ds = max(np.abs(c["dforce"]).max(), 1e-300)
+        assert e == pytest.approx(c["energy"], rel=1e-12, abs=1e-300)
+        np.testing.assert_allclose(f, c["force"], rtol=1e-12, atol=1e-13 * fs)
+        np.testing.assert_allclose(df.reshape(-1), c["dforce"], rtol=1e-12, atol=1e-13 * ds)
+        p = c["params"]
+        n_diss += (p["coulomb"] > 0 or p["viscous"] > 0 or p["normal_damping"] > 0) and c["energy"] > 0
+    assert n_diss >= 40  # the set exercises the dissipative terms, not only the penalty
