@@ -237,6 +237,30 @@ int sdx_set_params(sdx_context* ctx, const sdx_step_params* params);
 int sdx_set_state(sdx_context* ctx, const double* u, const double* v, double time);
 int sdx_get_state(sdx_context* ctx, double* u, double* v, double* time);
 
+/* Masked state write (SceneBatchExecutorV2::WriteState, mochi_physics/pybind/src/scene_batch_executor_v2.cpp:
+ * 459-540): in user node order, DoF i of u / v is written where its mask byte is nonzero (a NULL mask
+ * writes every DoF; NULL values leave the vector as it is). The host buffers may be reused on return. */
+int sdx_write_state_masked(sdx_context* ctx, const double* u, const double* v, const uint8_t* u_mask,
+                           const uint8_t* v_mask);
+
+/* State snapshots (Scene::CaptureState / RestoreState / ReleaseState / ReleaseAllStates / IsEqualState /
+ * CaptureStateToBytes / RestoreStateFromBytes, mochi_physics/include/mochi_physics/cpp_api/mochi_scene.h:
+ * 79-93; mochi_physics/src/mochi_scene.cpp:739-840). A snapshot holds everything a later step reads: the
+ * displacement, velocity and clock, the warm-start vectors of the last solves and the temporal history,
+ * and the per-env statistics; stepping on from a restored snapshot repeats the original steps (up to the
+ * rounding order of the assembly's atomic accumulation). Handles refer to device-resident copies (no host round trip; captures are ordered on the
+ * context's stream). env_mask (n_envs bytes, NULL: all) restores only the selected envs and keeps the
+ * clock. A handle of another context, or one already released, is refused by sdx_restore_state;
+ * releasing an unknown handle is a no-op. The bytes format is little-endian, versioned, carries a
+ * fingerprint of the uploaded bodies and a checksum; out = NULL asks for the size. */
+int sdx_capture_state(sdx_context* ctx, uint64_t* handle);
+int sdx_restore_state(sdx_context* ctx, uint64_t handle, int release_immediately, const uint8_t* env_mask);
+int sdx_release_state(sdx_context* ctx, uint64_t handle);
+int sdx_release_all_states(sdx_context* ctx);
+int sdx_is_equal_state(sdx_context* ctx, uint64_t a, uint64_t b, int* equal);
+int sdx_capture_state_to_bytes(sdx_context* ctx, uint8_t* out, int64_t capacity, int64_t* size);
+int sdx_restore_state_from_bytes(sdx_context* ctx, const uint8_t* data, int64_t size);
+
 /* Sizes of the uploaded problem. */
 int sdx_get_sizes(sdx_context* ctx, int64_t* n_nodes, int64_t* n_tets, int64_t* nnzb,
                   int64_t* n_faces);

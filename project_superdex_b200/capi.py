@@ -32,7 +32,9 @@ EXPORTED = [
     "sdx_get_stats", "sdx_bench_spmv", "sdx_kernel_launches", "sdx_get_stream",
     "sdx_set_profiling", "sdx_get_profile", "sdx_pcg_solve_device_noalloc", "sdx_mlp_init",
     "sdx_mlp_set_params", "sdx_mlp_get_params", "sdx_mlp_forward", "sdx_mlp_gradients", "sdx_mlp_train",
-    "sdx_collect_training", "sdx_get_training_data",
+    "sdx_collect_training", "sdx_get_training_data", "sdx_write_state_masked", "sdx_capture_state",
+    "sdx_restore_state", "sdx_release_state", "sdx_release_all_states", "sdx_is_equal_state",
+    "sdx_capture_state_to_bytes", "sdx_restore_state_from_bytes",
 ]
 SDX_MLP_PARAMS = 37264
 SDX_NOALLOC_MAX_BLOCK_ROWS = 65536
@@ -124,6 +126,14 @@ def lib():
     L.sdx_set_params.argtypes = [_vp, C.POINTER(StepParams)]
     L.sdx_set_state.argtypes = [_vp, _dp, _dp, C.c_double]
     L.sdx_get_state.argtypes = [_vp, _dp, _dp, _dp]
+    L.sdx_write_state_masked.argtypes = [_vp, _dp, _dp, _up, _up]
+    L.sdx_capture_state.argtypes = [_vp, C.POINTER(C.c_uint64)]
+    L.sdx_restore_state.argtypes = [_vp, C.c_uint64, C.c_int, _up]
+    L.sdx_release_state.argtypes = [_vp, C.c_uint64]
+    L.sdx_release_all_states.argtypes = [_vp]
+    L.sdx_is_equal_state.argtypes = [_vp, C.c_uint64, C.c_uint64, C.POINTER(C.c_int)]
+    L.sdx_capture_state_to_bytes.argtypes = [_vp, C.c_void_p, C.c_int64, _lp]
+    L.sdx_restore_state_from_bytes.argtypes = [_vp, C.c_void_p, C.c_int64]
     L.sdx_get_sizes.argtypes = [_vp, _lp, _lp, _lp, _lp]
     L.sdx_get_pattern.argtypes = [_vp, _lp, _ip]
     L.sdx_get_faces.argtypes = [_vp, _ip, _ip, _dp]

@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <numeric>
 #include <string>
@@ -149,6 +150,18 @@ struct PcgWork {
   }
 };
 
+// One captured state: every vector a later step reads (displacement, velocity, the warm-start vectors
+// of the last solve and the temporal history), in the context's row layout, plus the clock, the
+// history flags and the per-env statistics.
+struct Snapshot {
+  double* buf = nullptr;  // kSnapVectors x 3 n_rows
+  double time = 0.0;
+  unsigned hist_valid = 0;  // bit k: temporal history entry k is valid
+  std::vector<sdx_env_stats> stats;
+};
+constexpr int kSnapHist = 4;                 // == sdx_context::kHist
+constexpr int kSnapVectors = 5 + kSnapHist;  // u, v, dx, dx_prev1, dx_prev2, dx_hist[kHist]
+
 struct sdx_context {
   int device = 0;
   int num_sms = 0;
@@ -241,6 +254,15 @@ struct sdx_context {
   int pcg_threads = 0;         // threads per CTA of the context's PCG partition
   int* env_nrows = nullptr;    // padded rows per env (device)
   std::unique_ptr<PlainSolver> plain;  // the plain FP64 comparison solver, built on first use
+  // state snapshots (device-resident), keyed by handle
+  std::map<uint64_t, Snapshot> snaps;
+  uint64_t snap_next = 1;
+  uint64_t snap_tag = 0;       // per-context bits of every handle, so a handle of another context is refused
+  uint8_t* snap_mask = nullptr;    // per-env restore mask (device)
+  uint8_t* staging_mask = nullptr; // per-DoF write mask (device, 3 per node)
+  std::vector<double*> snap_pool;  // released snapshot buffers kept for the next capture
+  unsigned long long* snap_flag = nullptr;  // device word of sdx_is_equal_state
+  uint64_t fingerprint = 0;        // FNV-1a of the uploaded bodies (offsets, rest positions, tets)
   // opt-in per-kernel timing: event pairs resolved lazily
   bool profiling = false;
   sdx_profile prof;
@@ -337,6 +359,14 @@ static void release_topology(sdx_context* c) {
   dfree(c->row_of_node);
   dfree(c->coll_off);
   dfree(c->colliders);
+  if (!c->snaps.empty() || !c->snap_pool.empty()) cudaStreamSynchronize(c->stream);
+  for (auto& kv : c->snaps) dfree(kv.second.buf);
+  c->snaps.clear();
+  for (double*& b : c->snap_pool) dfree(b);
+  c->snap_pool.clear();
+  dfree(c->snap_flag);
+  dfree(c->snap_mask);
+  dfree(c->staging_mask);
   dfree(c->u);
   dfree(c->v);
   dfree(c->u0);
@@ -986,6 +1016,19 @@ extern "C" int sdx_upload_bodies(sdx_context* c, int n_envs, const int64_t* node
   c->n_envs = n_envs;
   c->n_nodes = N;
   c->n_tets = T;
+  {
+    uint64_t h = 1469598103934665603ull;  // FNV-1a 64
+    auto mix = [&](const void* p, size_t n) {
+      const unsigned char* b = (const unsigned char*)p;
+      for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+    };
+    mix(&n_envs, sizeof(n_envs));
+    mix(node_off, sizeof(int64_t) * (n_envs + 1));
+    mix(tet_off, sizeof(int64_t) * (n_envs + 1));
+    mix(X, sizeof(double) * 3 * N);
+    mix(tets, sizeof(int32_t) * 4 * T);
+    c->fingerprint = h;
+  }
   c->h_node_off.assign(node_off, node_off + n_envs + 1);
   c->h_tet_off.assign(tet_off, tet_off + n_envs + 1);
   // rows: per env padded to a multiple of 32
@@ -1353,6 +1396,339 @@ extern "C" int sdx_get_state(sdx_context* c, double* u, double* v, double* time)
   if (u) SDX_TRY(d2h_rows(c, c->u, u));
   if (v) SDX_TRY(d2h_rows(c, c->v, v));
   if (time) *time = c->time;
+  return SDX_OK;
+}
+
+// ------------------------------------------------------------------------------------------------
+// C-ABI: masked state writes and state snapshots
+
+__global__ void k_masked_scatter_rows(int64_t n_nodes, const int* __restrict__ row_of_node,
+                                      const double* __restrict__ src, const uint8_t* __restrict__ mask, double* dst) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_nodes) return;
+  const int64_t r = row_of_node[i];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+    if (mask[3 * i + k]) dst[3 * r + k] = src[3 * i + k];
+}
+
+// counts the 8-byte words in which a and b differ
+__global__ void k_words_differ(int64_t n, const unsigned long long* __restrict__ a,
+                               const unsigned long long* __restrict__ b, unsigned long long* count) {
+  unsigned long long local = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    local += a[i] != b[i];
+  if (local) atomicAdd(count, local);
+}
+
+extern "C" int sdx_write_state_masked(sdx_context* c, const double* u, const double* v, const uint8_t* u_mask,
+                                      const uint8_t* v_mask) {
+  if (!c || !c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
+  cudaSetDevice(c->device);
+  const size_t n3 = (size_t)3 * c->n_nodes;
+  const double* vals[2] = {u, v};
+  const uint8_t* masks[2] = {u_mask, v_mask};
+  double* dst[2] = {c->u, c->v};
+  for (int k = 0; k < 2; ++k) {
+    if (!vals[k]) continue;
+    if (!masks[k]) {
+      SDX_TRY(h2d_rows(c, vals[k], dst[k]));
+      continue;
+    }
+    if (!c->staging_mask) SDX_TRY(dalloc(&c->staging_mask, n3));
+    SDX_CUDA(cudaMemcpyAsync(c->staging, vals[k], sizeof(double) * n3, cudaMemcpyHostToDevice, c->stream));
+    SDX_CUDA(cudaMemcpyAsync(c->staging_mask, masks[k], n3, cudaMemcpyHostToDevice, c->stream));
+    k_masked_scatter_rows<<<(unsigned)((c->n_nodes + 255) / 256), 256, 0, c->stream>>>(
+        c->n_nodes, c->row_of_node, c->staging, c->staging_mask, dst[k]);
+    c->launches++;
+  }
+  SDX_CUDA(cudaStreamSynchronize(c->stream));  // the host buffers may be reused when this returns
+  return SDX_OK;
+}
+
+// The k-th captured vector of the live state (nullptr: not allocated).
+static double* snap_vector(sdx_context* c, int k) {
+  const size_t n3 = (size_t)3 * c->n_rows;
+  switch (k) {
+    case 0: return c->u;
+    case 1: return c->v;
+    case 2: return c->dx;
+    case 3: return c->dx_prev1;
+    case 4: return c->dx_prev2;
+    default: return c->dx_hist ? c->dx_hist + (size_t)(k - 5) * n3 : nullptr;
+  }
+}
+
+static unsigned hist_bits(const sdx_context* c) {
+  unsigned b = 0;
+  for (int k = 0; k < sdx_context::kHist; ++k)
+    if (c->hist_valid[k] && c->dx_hist) b |= 1u << k;
+  return b;
+}
+
+static_assert(kSnapHist == sdx_context::kHist, "snapshot history length");
+
+extern "C" int sdx_capture_state(sdx_context* c, uint64_t* handle) {
+  if (!c || !c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
+  if (!handle) return set_error(SDX_ERR_INVALID_ARGUMENT, "null handle");
+  cudaSetDevice(c->device);
+  const size_t n3 = (size_t)3 * c->n_rows;
+  Snapshot sn;
+  if (!c->snap_pool.empty()) {
+    sn.buf = c->snap_pool.back();
+    c->snap_pool.pop_back();
+  } else {
+    SDX_TRY(dalloc(&sn.buf, (size_t)kSnapVectors * n3));
+  }
+  // device-to-device copies on the context stream: ordered before every later step, no host round trip
+  for (int k = 0; k < kSnapVectors; ++k) {
+    const double* src = snap_vector(c, k);
+    if (src)
+      SDX_CUDA(cudaMemcpyAsync(sn.buf + k * n3, src, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->stream));
+    else
+      SDX_CUDA(cudaMemsetAsync(sn.buf + k * n3, 0, sizeof(double) * n3, c->stream));
+  }
+  sn.time = c->time;
+  sn.hist_valid = hist_bits(c);
+  sn.stats = c->stats;
+  if (c->snap_tag == 0) c->snap_tag = (((uint64_t)(uintptr_t)c * 0x9E3779B97F4A7C15ull) | (1ull << 63)) & ~0xFFFFFFFFFFull;
+  const uint64_t h = c->snap_tag | (c->snap_next++ & 0xFFFFFFFFFFull);
+  c->snaps[h] = std::move(sn);
+  *handle = h;
+  return SDX_OK;
+}
+
+extern "C" int sdx_release_state(sdx_context* c, uint64_t handle) {
+  if (!c) return set_error(SDX_ERR_INVALID_ARGUMENT, "null context");
+  auto it = c->snaps.find(handle);
+  if (it == c->snaps.end()) return SDX_OK;  // redundant releases are ignored
+  // kept for the next capture (stream-ordered reuse, no cudaFree on the hot path)
+  if (c->snap_pool.size() < 4) {
+    c->snap_pool.push_back(it->second.buf);
+  } else {
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    dfree(it->second.buf);
+  }
+  c->snaps.erase(it);
+  return SDX_OK;
+}
+
+extern "C" int sdx_release_all_states(sdx_context* c) {
+  if (!c) return set_error(SDX_ERR_INVALID_ARGUMENT, "null context");
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  for (auto& kv : c->snaps) dfree(kv.second.buf);
+  c->snaps.clear();
+  for (double*& b : c->snap_pool) dfree(b);
+  c->snap_pool.clear();
+  return SDX_OK;
+}
+
+extern "C" int sdx_restore_state(sdx_context* c, uint64_t handle, int release_immediately, const uint8_t* env_mask) {
+  if (!c || !c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
+  auto it = c->snaps.find(handle);
+  if (it == c->snaps.end()) return set_error(SDX_ERR_INVALID_ARGUMENT, "invalid state handle");
+  cudaSetDevice(c->device);
+  const Snapshot& sn = it->second;
+  const size_t n3 = (size_t)3 * c->n_rows;
+  if (sn.hist_valid && !c->dx_hist) {
+    SDX_TRY(dalloc(&c->dx_hist, (size_t)sdx_context::kHist * n3));
+    SDX_CUDA(cudaMemsetAsync(c->dx_hist, 0, sizeof(double) * sdx_context::kHist * n3, c->stream));
+  }
+  if (!env_mask) {
+    for (int k = 0; k < kSnapVectors; ++k) {
+      double* dst = snap_vector(c, k);
+      if (dst)
+        SDX_CUDA(cudaMemcpyAsync(dst, sn.buf + k * n3, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c->stream));
+    }
+    c->time = sn.time;
+    for (int k = 0; k < sdx_context::kHist; ++k) c->hist_valid[k] = (sn.hist_valid >> k) & 1u;
+    c->stats = sn.stats;
+  } else {
+    // the rows of the selected envs only; the clock is shared by all envs and stays
+    if (!c->snap_mask) SDX_TRY(dalloc(&c->snap_mask, c->n_envs));
+    SDX_CUDA(cudaMemcpyAsync(c->snap_mask, env_mask, c->n_envs, cudaMemcpyHostToDevice, c->stream));
+    for (int k = 0; k < kSnapVectors; ++k) {
+      double* dst = snap_vector(c, k);
+      if (dst) {
+        launch_copy_rows(c->n_slices, c->slice_env, c->snap_mask, sn.buf + k * n3, dst, c->stream);
+        c->launches++;
+      }
+    }
+    for (int k = 0; k < sdx_context::kHist; ++k) c->hist_valid[k] = c->hist_valid[k] && ((sn.hist_valid >> k) & 1u);
+    for (int e = 0; e < c->n_envs; ++e)
+      if (env_mask[e] && e < (int)sn.stats.size() && e < (int)c->stats.size()) c->stats[e] = sn.stats[e];
+    SDX_CUDA(cudaStreamSynchronize(c->stream));  // env_mask is a host buffer the caller may reuse
+  }
+  if (release_immediately) SDX_TRY(sdx_release_state(c, handle));
+  return SDX_OK;
+}
+
+extern "C" int sdx_is_equal_state(sdx_context* c, uint64_t a, uint64_t b, int* equal) {
+  if (!c || !equal) return set_error(SDX_ERR_INVALID_ARGUMENT, "null argument");
+  auto ia = c->snaps.find(a), ib = c->snaps.find(b);
+  if (ia == c->snaps.end() || ib == c->snaps.end()) {
+    *equal = 0;
+    return SDX_OK;  // an unknown handle is not equal to anything (the reference returns false)
+  }
+  const Snapshot &sa = ia->second, &sb = ib->second;
+  bool eq = sa.time == sb.time && sa.hist_valid == sb.hist_valid && sa.stats.size() == sb.stats.size();
+  for (size_t e = 0; eq && e < sa.stats.size(); ++e) {
+    const sdx_env_stats &x = sa.stats[e], &y = sb.stats[e];
+    eq = x.newton_iters == y.newton_iters && x.cg_iters == y.cg_iters && x.ls_iters == y.ls_iters &&
+         x.convergence == y.convergence && x.n_contacts == y.n_contacts &&
+         memcmp(&x.res_norm0, &y.res_norm0, sizeof(double)) == 0 && memcmp(&x.res_norm, &y.res_norm, sizeof(double)) == 0;
+  }
+  if (eq) {
+    cudaSetDevice(c->device);
+    if (!c->snap_flag) SDX_TRY(dalloc(&c->snap_flag, 1));
+    SDX_CUDA(cudaMemsetAsync(c->snap_flag, 0, sizeof(unsigned long long), c->stream));
+    const int64_t words = (int64_t)kSnapVectors * 3 * c->n_rows;
+    k_words_differ<<<c->num_sms * 4, 256, 0, c->stream>>>(words, (const unsigned long long*)sa.buf,
+                                                          (const unsigned long long*)sb.buf, c->snap_flag);
+    c->launches++;
+    unsigned long long diff = 0;
+    SDX_CUDA(cudaMemcpyAsync(&diff, c->snap_flag, sizeof(diff), cudaMemcpyDeviceToHost, c->stream));
+    SDX_CUDA(cudaStreamSynchronize(c->stream));
+    eq = diff == 0;
+  }
+  *equal = eq ? 1 : 0;
+  return SDX_OK;
+}
+
+// Bytes format (little-endian): magic "SDXSNAP1", u32 version 1, u32 vector count, u64 fingerprint of the
+// uploaded bodies, i64 nodes, i32 envs, u32 history flags, f64 time; then each vector as 3 doubles per
+// node in node order (u, v, the last solve's update, the two previous Newton updates, the temporal
+// history); then per env i32 newton_iters, cg_iters, ls_iters, convergence, f64 res_norm0, res_norm,
+// i64 n_contacts; then the u64 FNV-1a of all preceding bytes.
+static constexpr char kSnapMagic[8] = {'S', 'D', 'X', 'S', 'N', 'A', 'P', '1'};
+static constexpr size_t kSnapHeader = 8 + 4 + 4 + 8 + 8 + 4 + 4 + 8;
+static constexpr size_t kSnapEnvStats = 4 * 4 + 8 + 8 + 8;
+
+static uint64_t fnv1a(const uint8_t* p, size_t n) {
+  uint64_t h = 1469598103934665603ull;
+  for (size_t i = 0; i < n; ++i) h = (h ^ p[i]) * 1099511628211ull;
+  return h;
+}
+
+static size_t snap_bytes(const sdx_context* c) {
+  return kSnapHeader + (size_t)kSnapVectors * 3 * sizeof(double) * c->n_nodes + kSnapEnvStats * c->n_envs + 8;
+}
+
+extern "C" int sdx_capture_state_to_bytes(sdx_context* c, uint8_t* out, int64_t capacity, int64_t* size) {
+  if (!c || !c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
+  if (!size) return set_error(SDX_ERR_INVALID_ARGUMENT, "null size");
+  const size_t need = snap_bytes(c);
+  *size = (int64_t)need;
+  if (!out) return SDX_OK;
+  if (capacity < (int64_t)need) return set_error(SDX_ERR_INVALID_ARGUMENT, "buffer of %lld bytes, %lld needed",
+                                                 (long long)capacity, (long long)need);
+  cudaSetDevice(c->device);
+  uint8_t* q = out;
+  auto put = [&](const void* p, size_t n) {
+    memcpy(q, p, n);
+    q += n;
+  };
+  const uint32_t version = 1, nvec = kSnapVectors, hist = hist_bits(c);
+  const int64_t nn = c->n_nodes;
+  const int32_t ne = c->n_envs;
+  put(kSnapMagic, 8);
+  put(&version, 4);
+  put(&nvec, 4);
+  put(&c->fingerprint, 8);
+  put(&nn, 8);
+  put(&ne, 4);
+  put(&hist, 4);
+  put(&c->time, 8);
+  const size_t vb = sizeof(double) * 3 * c->n_nodes;
+  std::vector<double> zeros;
+  for (int k = 0; k < kSnapVectors; ++k) {
+    const double* src = snap_vector(c, k);
+    if (src) {
+      SDX_TRY(d2h_rows(c, src, (double*)(void*)q));  // byte copy: q need not be 8-byte aligned
+    } else {
+      memset(q, 0, vb);
+    }
+    q += vb;
+  }
+  for (int e = 0; e < c->n_envs; ++e) {
+    sdx_env_stats st{};
+    if (e < (int)c->stats.size()) st = c->stats[e];
+    const int32_t iv[4] = {st.newton_iters, st.cg_iters, st.ls_iters, st.convergence};
+    put(iv, sizeof(iv));
+    put(&st.res_norm0, 8);
+    put(&st.res_norm, 8);
+    const int64_t nc = st.n_contacts;
+    put(&nc, 8);
+  }
+  const uint64_t h = fnv1a(out, (size_t)(q - out));
+  put(&h, 8);
+  return SDX_OK;
+}
+
+extern "C" int sdx_restore_state_from_bytes(sdx_context* c, const uint8_t* data, int64_t size) {
+  if (!c || !c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
+  if (!data) return set_error(SDX_ERR_INVALID_ARGUMENT, "null data");
+  const size_t need = snap_bytes(c);
+  if (size < (int64_t)kSnapHeader || memcmp(data, kSnapMagic, 8) != 0)
+    return set_error(SDX_ERR_INVALID_ARGUMENT, "not a state snapshot");
+  uint32_t version, nvec, hist;
+  uint64_t fp, h;
+  int64_t nn;
+  int32_t ne;
+  double time;
+  const uint8_t* q = data + 8;
+  auto get = [&](void* p, size_t n) {
+    memcpy(p, q, n);
+    q += n;
+  };
+  get(&version, 4);
+  get(&nvec, 4);
+  get(&fp, 8);
+  get(&nn, 8);
+  get(&ne, 4);
+  get(&hist, 4);
+  get(&time, 8);
+  if (version != 1 || nvec != (uint32_t)kSnapVectors)
+    return set_error(SDX_ERR_INVALID_ARGUMENT, "unsupported snapshot version %u", version);
+  if (fp != c->fingerprint || nn != c->n_nodes || ne != c->n_envs)
+    return set_error(SDX_ERR_INVALID_ARGUMENT, "snapshot of different bodies");
+  if (size != (int64_t)need) return set_error(SDX_ERR_INVALID_ARGUMENT, "snapshot of %lld bytes, %lld expected",
+                                              (long long)size, (long long)need);
+  memcpy(&h, data + need - 8, 8);
+  if (h != fnv1a(data, need - 8)) return set_error(SDX_ERR_INVALID_ARGUMENT, "snapshot checksum mismatch");
+  cudaSetDevice(c->device);
+  const size_t n3 = (size_t)3 * c->n_rows, vb = sizeof(double) * 3 * c->n_nodes;
+  if (hist && !c->dx_hist) {
+    SDX_TRY(dalloc(&c->dx_hist, (size_t)sdx_context::kHist * n3));
+    SDX_CUDA(cudaMemsetAsync(c->dx_hist, 0, sizeof(double) * sdx_context::kHist * n3, c->stream));
+  }
+  for (int k = 0; k < kSnapVectors; ++k) {
+    double* dst = snap_vector(c, k);
+    if (dst) {
+      SDX_TRY(h2d_rows(c, (const double*)(const void*)q, dst));
+      SDX_CUDA(cudaStreamSynchronize(c->stream));  // the staging buffer is reused by the next vector
+    }
+    q += vb;
+  }
+  c->stats.assign(c->n_envs, sdx_env_stats{});
+  for (int e = 0; e < c->n_envs; ++e) {
+    int32_t iv[4];
+    get(iv, sizeof(iv));
+    sdx_env_stats& st = c->stats[e];
+    st.newton_iters = iv[0];
+    st.cg_iters = iv[1];
+    st.ls_iters = iv[2];
+    st.convergence = iv[3];
+    get(&st.res_norm0, 8);
+    get(&st.res_norm, 8);
+    int64_t nc;
+    get(&nc, 8);
+    st.n_contacts = nc;
+  }
+  c->time = time;
+  for (int k = 0; k < sdx_context::kHist; ++k) c->hist_valid[k] = (hist >> k) & 1u;
   return SDX_OK;
 }
 

@@ -106,6 +106,59 @@ class SoftBodyWorld:
         capi.check(capi.lib().sdx_get_state(self._ctx, capi.ptr(u), capi.ptr(v), C.byref(t)))
         return u, v, t.value
 
+    def write_state(self, qpos: Optional[np.ndarray] = None, qvel: Optional[np.ndarray] = None,
+                    qpos_write_mask: Optional[np.ndarray] = None, qvel_write_mask: Optional[np.ndarray] = None):
+        """Masked write of displacement (qpos) and velocity (qvel) DoFs in node order: DoF i is written where
+        its mask is nonzero, every DoF when the mask is None (SceneBatchExecutorV2.write_state)."""
+        n3 = 3 * self.n_nodes
+
+        def vec(a, dt):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dt).reshape(-1)
+            if a.size != n3:
+                raise ValueError(f"expected {n3} DoFs, got {a.size}")
+            return a
+        u, v = vec(qpos, np.float64), vec(qvel, np.float64)
+        mu, mv = vec(qpos_write_mask, np.uint8), vec(qvel_write_mask, np.uint8)
+        capi.check(capi.lib().sdx_write_state_masked(self._ctx, capi.ptr(u), capi.ptr(v), capi.ptr(mu, capi._up),
+                                                     capi.ptr(mv, capi._up)))
+
+    # state snapshots (Scene.capture_state / restore_state / ... of the reference) ---------------------
+    def capture_state(self) -> int:
+        h = C.c_uint64()
+        capi.check(capi.lib().sdx_capture_state(self._ctx, C.byref(h)))
+        return h.value
+
+    def restore_state(self, handle: int, release_immediately: bool = False, env_mask: Optional[np.ndarray] = None):
+        m = None if env_mask is None else np.ascontiguousarray(env_mask, np.uint8).reshape(-1)
+        if m is not None and m.size != self.n_envs:
+            raise ValueError(f"env_mask needs {self.n_envs} entries")
+        capi.check(capi.lib().sdx_restore_state(self._ctx, int(handle), int(bool(release_immediately)),
+                                                capi.ptr(m, capi._up)))
+
+    def release_state(self, handle: int):
+        capi.check(capi.lib().sdx_release_state(self._ctx, int(handle)))
+
+    def release_all_states(self):
+        capi.check(capi.lib().sdx_release_all_states(self._ctx))
+
+    def is_equal_state(self, a: int, b: int) -> bool:
+        eq = C.c_int()
+        capi.check(capi.lib().sdx_is_equal_state(self._ctx, int(a), int(b), C.byref(eq)))
+        return bool(eq.value)
+
+    def capture_state_to_bytes(self) -> bytes:
+        n = C.c_int64()
+        capi.check(capi.lib().sdx_capture_state_to_bytes(self._ctx, None, 0, C.byref(n)))
+        buf = (C.c_uint8 * n.value)()
+        capi.check(capi.lib().sdx_capture_state_to_bytes(self._ctx, buf, n.value, C.byref(n)))
+        return bytes(buf)
+
+    def restore_state_from_bytes(self, data: bytes):
+        b = (C.c_uint8 * len(data)).from_buffer_copy(data)
+        capi.check(capi.lib().sdx_restore_state_from_bytes(self._ctx, b, len(data)))
+
     # stepping ------------------------------------------------------------------------------------
     def step(self, n: int = 1):
         capi.check(capi.lib().sdx_step(self._ctx, int(n)))
