@@ -229,6 +229,7 @@ int sdx_set_colliders(sdx_context* ctx, int n_colliders, const int32_t* env, con
 #define SDX_MAT_NEO_HOOKEAN 0
 #define SDX_MAT_ST_VENANT_KIRCHHOFF 1
 #define SDX_MAT_LINEAR_ELASTIC 2
+#define SDX_MAT_ARAP 5  /* BatchedArap (batched_arap.cpp:29), stiffness = the tet's mu; not with SDX_PSD_FAST */
 int sdx_set_materials(sdx_context* ctx, int n_envs, const int32_t* material);
 
 int sdx_set_params(sdx_context* ctx, const sdx_step_params* params);

@@ -1,6 +1,6 @@
 #!/usr/bin/env bash
 # Builds oracle/_ref/libsdx_ref.so from the REFERENCE's own sources (read in place, never copied):
-# the Smith Neo-Hookean, St. Venant-Kirchhoff and linear-elastic translation units plus the header-only StressWork, PCG, PolyReLU and penalty
+# the Smith Neo-Hookean, St. Venant-Kirchhoff, linear-elastic and ARAP translation units plus the header-only StressWork, PCG, PolyReLU and penalty
 # contact code, in the reference's FP64 mode, behind the C shim oracle/ref_shim.cpp.
 # Runs only where the reference tree exists; the GPU box uses the prebuilt .so.
 set -euo pipefail
@@ -17,5 +17,6 @@ mkdir -p "$HERE/_ref"
   "$HERE/ref_shim.cpp" "$M/mochi_core/src/materials/batched_smith_neo_hookean.cpp" \
   "$M/mochi_core/src/materials/batched_st_venant_kirchhoff.cpp" \
   "$M/mochi_core/src/materials/batched_linear_elastic.cpp" \
+  "$M/mochi_core/src/materials/batched_arap.cpp" \
   -o "$HERE/_ref/libsdx_ref.so"
 echo "built $HERE/_ref/libsdx_ref.so"

@@ -176,7 +176,7 @@ def smith_nh(mu, lam, F, project=False, psd=1, min_eig=np.finfo(np.float64).eps)
 
 
 def material(kind, mu, lam, F, project=False, psd=1, min_eig=np.finfo(np.float64).eps):
-    """or_material: kind 0 Smith Neo-Hookean, 1 St. Venant-Kirchhoff, 2 linear elastic."""
+    """or_material: kind 0 Smith Neo-Hookean, 1 St. Venant-Kirchhoff, 2 linear elastic, 5 ARAP (stiffness mu)."""
     F = np.ascontiguousarray(F, np.float64).reshape(9)
     e = np.zeros(1)
     P = np.zeros(9)
@@ -186,7 +186,7 @@ def material(kind, mu, lam, F, project=False, psd=1, min_eig=np.finfo(np.float64
 
 
 def ref_material(kind, mu, lam, F, project=False, psd=1):
-    """The reference's own StVK (kind 1) / linear-elastic (kind 2) response."""
+    """The reference's own StVK (kind 1) / linear-elastic (kind 2) / ARAP (kind 5) response."""
     F = np.ascontiguousarray(F, np.float64).reshape(9)
     e = np.zeros(1)
     P = np.zeros(9)

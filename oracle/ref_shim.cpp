@@ -12,6 +12,7 @@
 #include <mochi_core/elements/tetrahedral/finite_element.h>
 #include <mochi_core/linear_algebra/krylov/pcg.h>
 #include <mochi_core/linear_algebra/matrix.h>
+#include <mochi_core/materials/batched_arap.h>
 #include <mochi_core/materials/batched_linear_elastic.h>
 #include <mochi_core/materials/batched_smith_neo_hookean.h>
 #include <mochi_core/materials/batched_st_venant_kirchhoff.h>
@@ -67,8 +68,9 @@ void ref_smith_nh(double mu, double lambda, const double* F9, int project, int p
           for (int l = 0; l < 3; ++l) C81[(i * 3 + j) * 9 + k * 3 + l] = Get0(C[i][j][k][l]);
 }
 
-// BatchedStVenantKirchhoffConstitutiveResponse<1> (mochi_core/src/materials/batched_st_venant_kirchhoff.cpp:29)
-// and BatchedLinearElasticConstitutiveResponse<1> (batched_linear_elastic.cpp:27); material 1 / 2 as in
+// BatchedStVenantKirchhoffConstitutiveResponse<1> (mochi_core/src/materials/batched_st_venant_kirchhoff.cpp:29),
+// BatchedLinearElasticConstitutiveResponse<1> (batched_linear_elastic.cpp:27) and
+// BatchedArapConstitutiveResponse<1> (batched_arap.cpp:29, stiffness = mu); material 1 / 2 / 5 as in
 // SoftMaterialType.
 void ref_material(int material, double mu, double lambda, const double* F9, int project, int psd_strategy,
                   double* energy, double* P9, double* C81) {
@@ -82,10 +84,16 @@ void ref_material(int material, double mu, double lambda, const double* F9, int 
   BatchDouble<1> e{};
   BatchReal3x3<1> pk1{};
   NdArray<BatchReal3x3<1>, 3, 3> C{};
-  if (material == 1)
+  if (material == 1) {
     materials::BatchedStVenantKirchhoffConstitutiveResponse<1>(p, F, &e, &pk1, &C, project != 0);
-  else
+  } else if (material == 5) {
+    materials::BatchArapParams<1> a;
+    a.stiffness = BatchReal<1>{mu};
+    a.psdStrategy = ToStrategy(psd_strategy);
+    materials::BatchedArapConstitutiveResponse<1>(a, F, &e, &pk1, &C, project != 0);
+  } else {
     materials::BatchedLinearElasticConstitutiveResponse<1>(p, F, &e, &pk1, &C, project != 0);
+  }
   if (energy) *energy = Get0(e);
   if (P9)
     for (int i = 0; i < 3; ++i)
@@ -139,9 +147,14 @@ void ref_reference_stiffness(int material, double mu, double lambda, double* c0v
     p.mu = BatchReal<1>{mu};
     p.lambda = BatchReal<1>{lambda};
     p.psdStrategy = MaterialPsdStrategy::None;
-    if (material == 1)
+    if (material == 1) {
       materials::BatchedStVenantKirchhoffConstitutiveResponse<1>(p, F, en, pk1, tan, psd);
-    else if (material == 2)
+    } else if (material == 5) {
+      materials::BatchArapParams<1> a;
+      a.stiffness = BatchReal<1>{mu};
+      a.psdStrategy = MaterialPsdStrategy::None;
+      materials::BatchedArapConstitutiveResponse<1>(a, F, en, pk1, tan, psd);
+    } else if (material == 2)
       materials::BatchedLinearElasticConstitutiveResponse<1>(p, F, en, pk1, tan, psd);
     else
       materials::BatchedSmithNeoHookeanConstitutiveResponse<1>(p, F, en, pk1, tan, psd,

@@ -353,12 +353,95 @@ void or_stress_damping(const double dN[12], double vol, const double u[12], cons
     }
 }
 
+/* Rotation-variant SVD F = U diag(s) V^T with det U = det V = +1 and s[2] < 0 iff det F < 0 (the
+ * convention of BatchedRotationVariantSvd3x3, mochi_core/.../utils/decomposition_utils.h): V from the
+ * eigenvectors of F^T F by decreasing eigenvalue, U from F V (normalised, Gram-Schmidt, u2 = u0 x u1),
+ * s_k = u_k . F v_k. */
+static void or_svd_rv(const double F[9], double U[9], double s[3], double V[9]) {
+  double S[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double v = 0.0;
+      for (int k = 0; k < 3; ++k) v += F[k * 3 + i] * F[k * 3 + j];
+      S[i * 3 + j] = v;
+    }
+  jacobi_eig(3, S, V);
+  int ord[3] = {0, 1, 2};
+  for (int a = 0; a < 3; ++a)
+    for (int b = a + 1; b < 3; ++b)
+      if (S[ord[b] * 4] > S[ord[a] * 4]) {
+        int t = ord[a];
+        ord[a] = ord[b];
+        ord[b] = t;
+      }
+  double Vs[9];
+  for (int r = 0; r < 3; ++r)
+    for (int k = 0; k < 3; ++k) Vs[r * 3 + k] = V[r * 3 + ord[k]];
+  if (det3(Vs) < 0.0)
+    for (int r = 0; r < 3; ++r) Vs[r * 3 + 2] = -Vs[r * 3 + 2];
+  memcpy(V, Vs, sizeof(Vs));
+  double fv[3][3];
+  for (int k = 0; k < 3; ++k)
+    for (int r = 0; r < 3; ++r) fv[k][r] = F[r * 3] * V[k] + F[r * 3 + 1] * V[3 + k] + F[r * 3 + 2] * V[6 + k];
+  double u[3][3];
+  const double n0 = sqrt(fv[0][0] * fv[0][0] + fv[0][1] * fv[0][1] + fv[0][2] * fv[0][2]);
+  for (int r = 0; r < 3; ++r) u[0][r] = n0 > 0.0 ? fv[0][r] / n0 : (r == 0 ? 1.0 : 0.0);
+  const double d01 = u[0][0] * fv[1][0] + u[0][1] * fv[1][1] + u[0][2] * fv[1][2];
+  for (int r = 0; r < 3; ++r) u[1][r] = fv[1][r] - d01 * u[0][r];
+  double n1 = sqrt(u[1][0] * u[1][0] + u[1][1] * u[1][1] + u[1][2] * u[1][2]);
+  if (n1 <= 1e-12 * (n0 > 0.0 ? n0 : 1.0)) { /* rank < 2: any unit vector orthogonal to u0 */
+    double a[3] = {fabs(u[0][0]) < 0.9 ? 1.0 : 0.0, fabs(u[0][0]) < 0.9 ? 0.0 : 1.0, 0.0};
+    const double dd = a[0] * u[0][0] + a[1] * u[0][1] + a[2] * u[0][2];
+    for (int r = 0; r < 3; ++r) u[1][r] = a[r] - dd * u[0][r];
+    n1 = sqrt(u[1][0] * u[1][0] + u[1][1] * u[1][1] + u[1][2] * u[1][2]);
+  }
+  for (int r = 0; r < 3; ++r) u[1][r] /= n1;
+  u[2][0] = u[0][1] * u[1][2] - u[0][2] * u[1][1];
+  u[2][1] = u[0][2] * u[1][0] - u[0][0] * u[1][2];
+  u[2][2] = u[0][0] * u[1][1] - u[0][1] * u[1][0];
+  for (int k = 0; k < 3; ++k) {
+    for (int r = 0; r < 3; ++r) U[r * 3 + k] = u[k][r];
+    s[k] = u[k][0] * fv[k][0] + u[k][1] * fv[k][1] + u[k][2] * fv[k][2];
+  }
+}
+
+void or_arap(double mu, const double F[9], int project, int psd_strategy, double min_eig, double* energy,
+             double P[9], double C[81]) {
+  /* batched_arap.cpp:29-136: energy 1/2 mu |s - 1|^2, PK1 mu (F - U V^T), tangent the exact Hessian
+   * mu I - sum_n mu / (s_j + s_k) T_n (x) T_n over the twist modes T_n = u_k v_j^T - u_j v_k^T; the six
+   * other eigenvalues are mu, so clamping the 9x9 spectrum equals the reference's twist-only clamp. */
+  double U[9], s[3], V[9];
+  or_svd_rv(F, U, s, V);
+  if (energy) *energy = 0.5 * mu * ((s[0] - 1.0) * (s[0] - 1.0) + (s[1] - 1.0) * (s[1] - 1.0) +
+                                    (s[2] - 1.0) * (s[2] - 1.0));
+  if (P)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        P[i * 3 + j] = mu * (F[i * 3 + j] - (U[i * 3] * V[j * 3] + U[i * 3 + 1] * V[j * 3 + 1] + U[i * 3 + 2] * V[j * 3 + 2]));
+  if (!C) return;
+  memset(C, 0, sizeof(double) * 81);
+  for (int a = 0; a < 9; ++a) C[a * 9 + a] = mu;
+  static const int pj[3] = {1, 0, 0}, pk[3] = {2, 2, 1};
+  for (int n = 0; n < 3; ++n) {
+    const int j = pj[n], k = pk[n];
+    const double lam = -mu / (s[j] + s[k]);
+    double T[9];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) T[r * 3 + c] = U[r * 3 + k] * V[c * 3 + j] - U[r * 3 + j] * V[c * 3 + k];
+    for (int a = 0; a < 9; ++a)
+      for (int b = 0; b < 9; ++b) C[a * 9 + b] += lam * T[a] * T[b];
+  }
+  if (project && psd_strategy != OR_PSD_NONE) or_project_tangent(C, psd_strategy == OR_PSD_ABS_EIGEN, min_eig);
+}
+
 void or_material(int material, double mu, double lambda, const double F[9], int project, int psd_strategy,
                  double min_eig, double* energy, double P[9], double C[81]) {
   if (material == OR_MAT_STVK)
     or_stvk(mu, lambda, F, project, psd_strategy, min_eig, energy, P, C);
   else if (material == OR_MAT_LINEAR)
     or_linear_elastic(mu, lambda, F, energy, P, C);
+  else if (material == OR_MAT_ARAP)
+    or_arap(mu, F, project, psd_strategy, min_eig, energy, P, C);
   else
     or_smith_nh(mu, lambda, F, project, psd_strategy, min_eig, energy, P, C);
 }
@@ -901,7 +984,11 @@ int64_t or_assemble(const or_scene* s, const double* u, const double* ut, double
           ue[3 * f + r] = u[3 * (int64_t)nd[f] + r];
           us[3 * f + r] = s->u_stage[3 * (int64_t)nd[f] + r];
         }
-      or_stress_damping(dN, w, ue, us, s->stiffness_damping / dt, s->lambda[e], s->mu[e],
+      /* the reference stiffness (ComputeReferenceMaterialStiffnessVoigt): the tet's (lambda, mu), for
+       * ARAP (0, mu / 2) */
+      const double l0 = s->material == OR_MAT_ARAP ? 0.0 : s->lambda[e];
+      const double m0 = s->material == OR_MAT_ARAP ? 0.5 * s->mu[e] : s->mu[e];
+      or_stress_damping(dN, w, ue, us, s->stiffness_damping / dt, l0, m0,
                         s->stiffness_damping_geometric, project, want_obj ? &de : NULL, want_res ? dres : NULL,
                         want_hess ? dK : NULL);
       energy += de;

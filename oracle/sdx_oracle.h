@@ -37,7 +37,7 @@ void or_smith_nh(double mu, double lambda, const double F[9], int project, int p
                  double min_eig, double* energy, double P[9], double C[81]);
 
 /* Soft materials, same values as SoftMaterialType (mochi_core/.../materials/material_types.h:148-172). */
-enum { OR_MAT_NEO_HOOKEAN = 0, OR_MAT_STVK = 1, OR_MAT_LINEAR = 2 };
+enum { OR_MAT_NEO_HOOKEAN = 0, OR_MAT_STVK = 1, OR_MAT_LINEAR = 2, OR_MAT_ARAP = 5 };
 
 /* St. Venant-Kirchhoff: psi = mu |G|^2 + lambda/2 tr(G)^2 with G = (F^T F - I)/2; P = F S,
  * S = 2 mu G + lambda tr(G) I. Follows mochi_core/src/materials/batched_st_venant_kirchhoff.cpp:29-203:
@@ -52,7 +52,13 @@ void or_stvk(double mu, double lambda, const double F[9], int project, int psd_s
  * mochi_core/src/materials/batched_linear_elastic.cpp:25-97. */
 void or_linear_elastic(double mu, double lambda, const double F[9], double* energy, double P[9], double C[81]);
 
-/* Dispatch on OR_MAT_*. */
+/* As-rigid-as-possible material with stiffness mu (mochi_core/src/materials/batched_arap.cpp:29-136):
+ * energy 1/2 mu |sigma - 1|^2 over the rotation-variant singular values, PK1 mu (F - U V^T), tangent with
+ * the twist-mode eigenvalues clamped under projection. */
+void or_arap(double mu, const double F[9], int project, int psd_strategy, double min_eig, double* energy,
+             double P[9], double C[81]);
+
+/* Dispatch on OR_MAT_* (ARAP takes mu as its stiffness). */
 void or_material(int material, double mu, double lambda, const double F[9], int project, int psd_strategy,
                  double min_eig, double* energy, double P[9], double C[81]);
 

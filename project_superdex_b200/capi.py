@@ -21,7 +21,7 @@ SDX_PREC_NONE, SDX_PREC_JACOBI, SDX_PREC_BLOCK_JACOBI = 0, 1, 2
 SDX_WARM_ZERO, SDX_WARM_PREVIOUS, SDX_WARM_LEARNED, SDX_WARM_TEMPORAL = 0, 1, 2, 3
 SDX_LINEAR_CONVERGED, SDX_LINEAR_STOPPED, SDX_LINEAR_DIVERGED = 1, 2, 3
 SDX_SOLVER_FUSED, SDX_SOLVER_PLAIN_FP64 = 0, 1
-SDX_MAT_NEO_HOOKEAN, SDX_MAT_ST_VENANT_KIRCHHOFF, SDX_MAT_LINEAR_ELASTIC = 0, 1, 2
+SDX_MAT_NEO_HOOKEAN, SDX_MAT_ST_VENANT_KIRCHHOFF, SDX_MAT_LINEAR_ELASTIC, SDX_MAT_ARAP = 0, 1, 2, 5
 
 # every entry point include/sdx_b200.h declares
 EXPORTED = [

@@ -480,6 +480,154 @@ __device__ __forceinline__ void linear_energy_pk1_f64(double mu, double lambda, 
 }
 
 // constant, PSD: dP_rc/dF_ij = mu (d_ri d_cj + d_ci d_rj) + lambda d_rc d_ij
+// ------------------------------------------------------------------------------------------------
+// As-rigid-as-possible (batched_arap.cpp:29-136): energy 1/2 mu |s - 1|^2 over the rotation-variant
+// singular values, PK1 mu (F - U V^T), tangent mu I + sum_n l_n T_n (x) T_n over the twist modes
+// T_n = u_k v_j^T - u_j v_k^T with l_n = -mu / (s_j + s_k) (the exact Hessian), the twist eigenvalues
+// mu + 2 l_n clamped under projection (the other six are mu).
+
+// FP64 symmetric 3x3 eigen-decomposition and rotation-variant SVD: the constructions of sym_eig3 /
+// svd3_rv in double precision.
+__device__ __forceinline__ void jacobi_rot_f64(double A[9], double V[9], int p, int q) {
+  const double apq = A[p * 3 + q];
+  if (fabs(apq) < 1e-300) return;
+  const double theta = (A[q * 3 + q] - A[p * 3 + p]) / (2.0 * apq);
+  const double t = copysign(1.0, theta) / (fabs(theta) + sqrt(fma(theta, theta, 1.0)));
+  const double c = 1.0 / sqrt(fma(t, t, 1.0));
+  const double s = t * c;
+  for (int k = 0; k < 3; ++k) {
+    const double akp = A[k * 3 + p], akq = A[k * 3 + q];
+    A[k * 3 + p] = c * akp - s * akq;
+    A[k * 3 + q] = s * akp + c * akq;
+  }
+  for (int k = 0; k < 3; ++k) {
+    const double apk = A[p * 3 + k], aqk = A[q * 3 + k];
+    A[p * 3 + k] = c * apk - s * aqk;
+    A[q * 3 + k] = s * apk + c * aqk;
+  }
+  for (int k = 0; k < 3; ++k) {
+    const double vkp = V[k * 3 + p], vkq = V[k * 3 + q];
+    V[k * 3 + p] = c * vkp - s * vkq;
+    V[k * 3 + q] = s * vkp + c * vkq;
+  }
+}
+
+__device__ __forceinline__ void svd3_rv_f64(const double F[9], double U[9], double s[3], double V[9]) {
+  double A[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      A[i * 3 + j] = F[i] * F[j] + F[3 + i] * F[3 + j] + F[6 + i] * F[6 + j];
+  for (int i = 0; i < 9; ++i) V[i] = (i % 4 == 0) ? 1.0 : 0.0;
+  for (int sweep = 0; sweep < 16; ++sweep) {
+    const double off = A[1] * A[1] + A[2] * A[2] + A[5] * A[5];
+    const double dg = A[0] * A[0] + A[4] * A[4] + A[8] * A[8];
+    if (off <= 1e-32 * dg) break;
+    jacobi_rot_f64(A, V, 0, 1);
+    jacobi_rot_f64(A, V, 0, 2);
+    jacobi_rot_f64(A, V, 1, 2);
+  }
+  double w[3] = {A[0], A[4], A[8]};
+  // descending eigenvalues, V columns alongside
+  for (int a = 0; a < 2; ++a)
+    for (int b = a + 1; b < 3; ++b)
+      if (w[a] < w[b]) {
+        const double tw = w[a];
+        w[a] = w[b];
+        w[b] = tw;
+        for (int r = 0; r < 3; ++r) {
+          const double tv = V[r * 3 + a];
+          V[r * 3 + a] = V[r * 3 + b];
+          V[r * 3 + b] = tv;
+        }
+      }
+  if (det3(V) < 0.0) {
+    V[2] = -V[2];
+    V[5] = -V[5];
+    V[8] = -V[8];
+  }
+  double fv[3][3];
+  for (int k = 0; k < 3; ++k)
+    for (int r = 0; r < 3; ++r)
+      fv[k][r] = F[r * 3 + 0] * V[0 * 3 + k] + F[r * 3 + 1] * V[1 * 3 + k] + F[r * 3 + 2] * V[2 * 3 + k];
+  double u0[3], u1[3], u2[3];
+  const double n0 = sqrt(fv[0][0] * fv[0][0] + fv[0][1] * fv[0][1] + fv[0][2] * fv[0][2]);
+  for (int r = 0; r < 3; ++r) u0[r] = n0 > 0.0 ? fv[0][r] / n0 : (r == 0 ? 1.0 : 0.0);
+  const double d01 = u0[0] * fv[1][0] + u0[1] * fv[1][1] + u0[2] * fv[1][2];
+  for (int r = 0; r < 3; ++r) u1[r] = fv[1][r] - d01 * u0[r];
+  double n1 = sqrt(u1[0] * u1[0] + u1[1] * u1[1] + u1[2] * u1[2]);
+  if (!(n1 > 1e-12 * fmax(n0, 1e-300))) {  // rank < 2: any unit vector orthogonal to u0
+    const double a0 = fabs(u0[0]) < 0.9 ? 1.0 : 0.0, a1 = 1.0 - a0;
+    const double dd = a0 * u0[0] + a1 * u0[1];
+    u1[0] = a0 - dd * u0[0];
+    u1[1] = a1 - dd * u0[1];
+    u1[2] = -dd * u0[2];
+    n1 = sqrt(u1[0] * u1[0] + u1[1] * u1[1] + u1[2] * u1[2]);
+  }
+  for (int r = 0; r < 3; ++r) u1[r] /= n1;
+  u2[0] = u0[1] * u1[2] - u0[2] * u1[1];
+  u2[1] = u0[2] * u1[0] - u0[0] * u1[2];
+  u2[2] = u0[0] * u1[1] - u0[1] * u1[0];
+  for (int r = 0; r < 3; ++r) {
+    U[r * 3 + 0] = u0[r];
+    U[r * 3 + 1] = u1[r];
+    U[r * 3 + 2] = u2[r];
+  }
+  s[0] = u0[0] * fv[0][0] + u0[1] * fv[0][1] + u0[2] * fv[0][2];
+  s[1] = u1[0] * fv[1][0] + u1[1] * fv[1][1] + u1[2] * fv[1][2];
+  s[2] = u2[0] * fv[2][0] + u2[1] * fv[2][1] + u2[2] * fv[2][2];
+}
+
+__device__ __forceinline__ void arap_energy_pk1_f64(double mu, const double F[9], double* psi, double P[9]) {
+  double U[9], s[3], V[9];
+  svd3_rv_f64(F, U, s, V);
+  if (psi) *psi = 0.5 * mu * ((s[0] - 1.0) * (s[0] - 1.0) + (s[1] - 1.0) * (s[1] - 1.0) + (s[2] - 1.0) * (s[2] - 1.0));
+  if (P) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        P[i * 3 + j] = mu * (F[i * 3 + j] - (U[i * 3] * V[j * 3] + U[i * 3 + 1] * V[j * 3 + 1] + U[i * 3 + 2] * V[j * 3 + 2]));
+  }
+}
+
+__device__ __forceinline__ void arap_tangent_f32(float mu, const float F[9], int project, int psd, float min_eig,
+                                                 float C[81]) {
+  float U[9], s[3], V[9];
+  svd3_rv(F, U, s, V);
+  float lam[3];
+#pragma unroll
+  for (int n = 0; n < 3; ++n) {
+    const int j = (n == 0) ? 1 : 0;
+    const int k = (n == 2) ? 1 : 2;
+    float l = -mu / (s[j] + s[k]);
+    if (project && psd != 0) {
+      const float e = 2.0f * l + mu;
+      l = 0.5f * (fmaxf(psd == 2 ? fabsf(e) : e, min_eig) - mu);
+    }
+    lam[n] = l;
+  }
+  float T[3][9];
+#pragma unroll
+  for (int n = 0; n < 3; ++n) {
+    const int j = (n == 0) ? 1 : 0;
+    const int k = (n == 2) ? 1 : 2;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) T[n][r * 3 + c] = U[r * 3 + k] * V[c * 3 + j] - U[r * 3 + j] * V[c * 3 + k];
+  }
+#pragma unroll
+  for (int a = 0; a < 9; ++a)
+#pragma unroll
+    for (int b = a; b < 9; ++b) {
+      float v = (a == b) ? mu : 0.0f;
+#pragma unroll
+      for (int n = 0; n < 3; ++n) v = fmaf(lam[n] * T[n][a], T[n][b], v);
+      C[a * 9 + b] = v;
+      C[b * 9 + a] = v;
+    }
+}
+
 __device__ __forceinline__ void linear_tangent_f32(float mu, float lambda, float C[81]) {
 #pragma unroll
   for (int r = 0; r < 3; ++r)

@@ -215,6 +215,7 @@ struct sdx_context {
   double* env_obj = nullptr;
   uint8_t* env_mask = nullptr;
   uint8_t* env_material = nullptr;  // SDX_MAT_* per env (zero: Smith Neo-Hookean)
+  bool has_arap = false;            // some env uses SDX_MAT_ARAP
   unsigned long long* env_pairs = nullptr;
   unsigned* pair_mask = nullptr;
   std::vector<sdx_env_stats> stats;
@@ -398,6 +399,7 @@ static void release_topology(sdx_context* c) {
   c->ds_cap = c->ds_n = 0;
   c->collect_per_solve = 0;
   c->uploaded = false;
+  c->has_arap = false;
 }
 
 static void release_mlp_work(MlpWork& W) {
@@ -957,6 +959,8 @@ extern "C" int sdx_set_params(sdx_context* c, const sdx_step_params* p) {
                      "implicit normal force for dissipation is not supported with explicit normals");
   if (!(p->max_align >= -1.0 && p->max_align <= 1.0))
     return set_error(SDX_ERR_INVALID_ARGUMENT, "max_align must be in [-1, 1]");
+  if (c->has_arap && p->psd_strategy == SDX_PSD_FAST)
+    return set_error(SDX_ERR_INVALID_ARGUMENT, "ARAP does not support the Fast PSD strategy");
   c->params = *p;
   return SDX_OK;
 }
@@ -1318,13 +1322,21 @@ extern "C" int sdx_set_materials(sdx_context* c, int n_envs, const int32_t* mate
   if (!c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
   if (n_envs != c->n_envs) return set_error(SDX_ERR_INVALID_ARGUMENT, "expected %d materials", c->n_envs);
   std::vector<uint8_t> m(n_envs);
+  bool arap = false;
   for (int e = 0; e < n_envs; ++e) {
-    if (material[e] < SDX_MAT_NEO_HOOKEAN || material[e] > SDX_MAT_LINEAR_ELASTIC)
-      return set_error(SDX_ERR_INVALID_ARGUMENT, "env %d: unknown material %d", e, material[e]);
-    m[e] = (uint8_t)material[e];
+    const int k = material[e];
+    if (k != SDX_MAT_NEO_HOOKEAN && k != SDX_MAT_ST_VENANT_KIRCHHOFF && k != SDX_MAT_LINEAR_ELASTIC &&
+        k != SDX_MAT_ARAP)
+      return set_error(SDX_ERR_INVALID_ARGUMENT, "env %d: unknown material %d", e, k);
+    m[e] = (uint8_t)k;
+    arap = arap || k == SDX_MAT_ARAP;
   }
+  // ARAP supports the None, Projection and AbsEigenProjection strategies (batched_arap.h:37-40)
+  if (arap && c->params.psd_strategy == SDX_PSD_FAST)
+    return set_error(SDX_ERR_INVALID_ARGUMENT, "ARAP does not support the Fast PSD strategy");
   cudaSetDevice(c->device);
   SDX_CUDA(cudaMemcpy(c->env_material, m.data(), n_envs, cudaMemcpyHostToDevice));
+  c->has_arap = arap;
   return SDX_OK;
 }
 
@@ -1795,6 +1807,7 @@ static void assemble_dev(sdx_context* c, const double* u, const double* ut, doub
   ea.min_eig = 1.1920928955078125e-07f;  // kMinProjectedEigenvalue of the FP32 build
   ea.psd = p.psd_strategy;
   ea.flags = flags;
+  ea.has_arap = c->has_arap ? 1 : 0;
   prof_begin(c, &ev);
   launch_element(ea, c->stream);
   c->launches++;

@@ -69,6 +69,7 @@ struct ElemArgs {
   float min_eig;
   int psd;
   int flags;
+  int has_arap;  // some env uses ARAP (launch the variant that evaluates it)
 };
 
 struct ContactArgs {

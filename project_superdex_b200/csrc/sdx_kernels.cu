@@ -97,6 +97,9 @@ __device__ __forceinline__ void warp_env_add(double* obj, int env, double v) {
   if ((int)(threadIdx.x & 31) == leader) atomicAdd(obj + env, s);
 }
 
+// kArap: the variant that also evaluates ARAP envs (SVD-based, more registers); launched only when some
+// env uses ARAP, so the other materials keep the lean variant.
+template <bool kArap>
 __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= a.n_tets) return;
@@ -135,7 +138,10 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) Fs[r * 3 + c] = fma(us, (double)dN[3 * f + c], Fs[r * 3 + c]);
       }
-    visc_stress_f64(F, Fs, a.kdamp * (double)lam, a.kdamp * (double)mu, dE, Sv);
+    // reference stiffness (ComputeReferenceMaterialStiffnessVoigt): (lambda, mu), for ARAP (0, mu / 2)
+    const bool arap = kArap && mat == 5;
+    const double l0 = arap ? 0.0 : (double)lam, m0 = arap ? 0.5 * (double)mu : (double)mu;
+    visc_stress_f64(F, Fs, a.kdamp * l0, a.kdamp * m0, dE, Sv);
   }
   if (want_res || want_obj) {
     const SnhConsts kc = snh_consts((double)mu, (double)lam);
@@ -160,6 +166,8 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
         stvk_energy_pk1_f64((double)mu, (double)lam, F, nullptr, P);
       else if (mat == 2)
         linear_energy_pk1_f64((double)mu, (double)lam, F, nullptr, P);
+      else if (kArap && mat == 5)
+        arap_energy_pk1_f64((double)mu, F, nullptr, P);
       else
         snh_pk1_f64(kc, F, P);
       if (a.kdamp > 0.0) {  // + F S_visc
@@ -208,6 +216,8 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
         stvk_energy_pk1_f64((double)mu, (double)lam, F, &psi, nullptr);
       else if (mat == 2)
         linear_energy_pk1_f64((double)mu, (double)lam, F, &psi, nullptr);
+      else if (kArap && mat == 5)
+        arap_energy_pk1_f64((double)mu, F, &psi, nullptr);
       else
         psi = snh_energy_f64(kc, F);
       if (a.kdamp > 0.0) psi += 0.5 * (Sv[0] * dE[0] + Sv[1] * dE[1] + Sv[2] * dE[2] + Sv[3] * dE[3] +
@@ -228,6 +238,8 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
       stvk_tangent_f32(mu, lam, Ff, (a.flags & 8) != 0, a.psd, a.min_eig, C);
     else if (mat == 2)
       linear_tangent_f32(mu, lam, C);
+    else if (kArap && mat == 5)
+      arap_tangent_f32(mu, Ff, (a.flags & 8) != 0, a.psd, a.min_eig, C);
     else
       snh_tangent_f32(mu, lam, Ff, (a.flags & 8) != 0, a.psd, a.min_eig, C);
     const int4 S0 = a.slots0[t], S1 = a.slots1[t], S2 = a.slots2[t], S3 = a.slots3[t];
@@ -239,7 +251,9 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
     // stiffness damping: Gauss-Newton part kappa B^T C0 B and the (projected) geometric part
     const bool kd = a.kdamp > 0.0;
     float aF[4][3], FFt[9], Sg[9];
-    const float kl = (float)(a.kdamp * (double)lam), km = (float)(a.kdamp * (double)mu);
+    const bool arap_h = kArap && mat == 5;
+    const float kl = arap_h ? 0.0f : (float)(a.kdamp * (double)lam);
+    const float km = (float)(a.kdamp * (arap_h ? 0.5 * (double)mu : (double)mu));
     if (kd) {
 #pragma unroll
       for (int f = 0; f < 4; ++f)
@@ -301,7 +315,10 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
 void launch_element(const ElemArgs& a, cudaStream_t st) {
   if (a.n_tets == 0) return;
   const int th = 128;
-  k_element<<<(unsigned)((a.n_tets + th - 1) / th), th, 0, st>>>(a);
+  if (a.has_arap)
+    k_element<true><<<(unsigned)((a.n_tets + th - 1) / th), th, 0, st>>>(a);
+  else
+    k_element<false><<<(unsigned)((a.n_tets + th - 1) / th), th, 0, st>>>(a);
 }
 
 // ------------------------------------------------------------------------------------------------

@@ -50,7 +50,8 @@ class Body:
     pin: np.ndarray        # (N,) uint8, bit c set -> DoF c pinned
     colliders: List[Collider]
     cells: tuple = (0, 0, 0)
-    material: int = 0      # SoftMaterialType: 0 Neo-Hookean (Smith), 1 St. Venant-Kirchhoff, 2 linear elastic
+    material: int = 0      # SoftMaterialType: 0 Neo-Hookean (Smith), 1 St. Venant-Kirchhoff, 2 linear elastic,
+                           # 5 ARAP (stiffness = the tet's mu)
 
     @property
     def n_nodes(self) -> int:

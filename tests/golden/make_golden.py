@@ -94,7 +94,7 @@ def reference_vectors():
     assert R is not None, "oracle/_ref/libsdx_ref.so missing: run oracle/build_ref.sh"
     rng = np.random.default_rng(20261203)
     out = {"smith": [], "polyrelu": [], "penalty": [], "stress_work": [], "pcg": [], "materials": [],
-           "stress_damping": [], "collision": []}
+           "stress_damping": [], "collision": [], "arap": [], "reference_stiffness": []}
     for i in range(48):
         F = np.eye(3) + rng.normal(0, 0.35, (3, 3))
         if i % 4 == 0:
@@ -227,6 +227,21 @@ def reference_vectors():
                                  "n_col": nc.tolist() if valid else None, "pos": pos.tolist(),
                                  "pos_ss": pss.tolist(), "dt": dt, "energy": float(e), "force": f.tolist(),
                                  "dforce": df.reshape(-1).tolist()})
+    # BatchedArapConstitutiveResponse (stiffness = mu) with None / Projection / AbsEigenProjection, inverted
+    # elements included, and the rest stiffness ComputeReferenceMaterialStiffnessVoigt gives each material
+    for i in range(32):
+        F = np.eye(3) + rng.normal(0, 0.35, (3, 3))
+        if i % 4 == 0:
+            F[:, 0] *= -1.0
+        mu = float(rng.uniform(0.2, 3.0))
+        for psd in (0, 1, 2):
+            e, P, Cm = O.ref_material(5, mu, 0.0, F, project=psd != 0, psd=psd)
+            out["arap"].append({"mu": mu, "F": F.reshape(-1).tolist(), "psd": psd, "energy": e,
+                                "pk1": P.reshape(-1).tolist(), "tangent": Cm.reshape(-1).tolist()})
+    for kind in (0, 1, 2, 5):
+        c0 = np.zeros(36)
+        R.ref_reference_stiffness(kind, 1000.0, 3000.0, O.ptr(c0))
+        out["reference_stiffness"].append({"kind": kind, "mu": 1000.0, "lambda": 3000.0, "c0": c0.tolist()})
     out["source"] = "oracle/_ref/libsdx_ref.so (reference sources, FP64 build)"
     return out
 

@@ -100,10 +100,11 @@ def test_batched_uneven_envs_match_per_env_oracle(oracle):
         off += u.size
 
 
-@pytest.mark.parametrize("material,psd", [(1, 0), (1, 1), (1, 2), (1, 3), (2, 1)])
+@pytest.mark.parametrize("material,psd", [(1, 0), (1, 1), (1, 2), (1, 3), (2, 1), (5, 0), (5, 1), (5, 2)])
 def test_other_materials_assembly_matches_oracle(oracle, material, psd):
     """St. Venant-Kirchhoff (every PSD strategy, eigensystem projection on the GPU, 9x9 eigen-solve in the
-    oracle) and linear elasticity, with contact."""
+    oracle), linear elasticity and ARAP (FP64 SVD for energy and stress, twist-mode clamp on the GPU),
+    with contact."""
     b = _body(10 + material)
     b.material = material
     cfg = scenes.SceneConfig(k_contact=1e6)
@@ -207,3 +208,30 @@ def test_friction_assembly_matches_oracle(oracle, case):
     assert a_gpu["obj"][0] == pytest.approx(a_or["obj"], rel=1e-6)
     assert a_gpu["n_pairs"][0] == a_or["n_pairs"] > 0
     assert np.array_equal(w.contact_pairs(), a_or["pairs"])
+
+
+def test_arap_with_stiffness_damping_and_mixed_envs_matches_oracle(oracle):
+    """A batch mixing ARAP and Neo-Hookean envs (the ARAP-capable element kernel), with Rayleigh stiffness
+    damping, whose reference stiffness for ARAP is (0, mu / 2)."""
+    from project_superdex_b200.soft_body import SoftBodyWorld
+    bodies = [_body(60), _body(61, n=4)]
+    bodies[0].material = 5
+    cfg = scenes.SceneConfig(k_contact=1e6, stiffness_damping=0.01, stiffness_damping_geometric=True)
+    w = SoftBodyWorld(bodies, cfg, psd_strategy=1)
+    rng = np.random.default_rng(700)
+    us_all, u_all, v_all, g_or, obj_or = [], [], [], [], []
+    for b in bodies:
+        free = (b.pin == 0).repeat(3)
+        us = rng.normal(0, 5e-4, 3 * b.n_nodes) * free
+        u = us + rng.normal(0, 1e-3, 3 * b.n_nodes) * free
+        v = rng.normal(0, 2e-2, 3 * b.n_nodes) * free
+        s = oracle.Scene(b, cfg, psd_strategy=1, min_eig=float(np.finfo(np.float32).eps))
+        a = s.assemble(u, us + cfg.dt * v, t=0.01, psd=True, u_stage=us)
+        us_all.append(us), u_all.append(u), v_all.append(v), g_or.append(a["g"]), obj_or.append(a["obj"])
+    w.set_state(np.concatenate(us_all), np.concatenate(v_all), 0.0)
+    a_gpu = w.assemble(np.concatenate(u_all), t=0.01, psd=True)
+    g = np.concatenate(g_or)
+    np.testing.assert_allclose(a_gpu["g"], g, rtol=0, atol=1e-6 * np.abs(g).max())
+    np.testing.assert_allclose(a_gpu["obj"], obj_or, rtol=1e-6)
+    with pytest.raises(Exception, match="Fast"):
+        w.set_params(psd_strategy=3)

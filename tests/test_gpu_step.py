@@ -103,9 +103,9 @@ def test_autotuned_launch_shape_reaches_same_state(oracle, monkeypatch):
     _check(bodies, ug, states, hist)
 
 
-@pytest.mark.parametrize("material", [1, 2])
+@pytest.mark.parametrize("material", [1, 2, 5])
 def test_other_materials_steps_match_oracle(oracle, material):
-    """Newton steps of a St. Venant-Kirchhoff / linear-elastic body against the oracle."""
+    """Newton steps of a St. Venant-Kirchhoff / linear-elastic / ARAP body against the oracle."""
     bodies, cfg = scenes.config0()
     bodies[0].material = material
     w, ug, vg, states, hist = _run(oracle, bodies, cfg, 3)

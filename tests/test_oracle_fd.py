@@ -87,7 +87,7 @@ def test_contact_pairs_sorted_unique(oracle):
     assert np.all(pr % len(b.colliders) < len(b.colliders))
 
 
-@pytest.mark.parametrize("material", [0, 1, 2])
+@pytest.mark.parametrize("material", [0, 1, 2, 5])
 def test_damped_materials_match_finite_differences(oracle, material):
     """Energy -> gradient -> Hessian consistency with Rayleigh mass and stiffness damping (about a
     stage-start displacement; the stiffness-damping Hessian with its geometric term is exact) for each

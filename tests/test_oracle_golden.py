@@ -180,3 +180,29 @@ def test_collision_response_matches_reference_code(oracle, golden):
         p = c["params"]
         n_diss += (p["coulomb"] > 0 or p["viscous"] > 0 or p["normal_damping"] > 0) and c["energy"] > 0
     assert n_diss >= 40  # the set exercises the dissipative terms, not only the penalty
+
+
+def test_arap_matches_reference_code(oracle, golden):
+    """The oracle's ARAP (own rotation-variant SVD, exact Hessian, spectral clamp) against the reference's
+    BatchedArapConstitutiveResponse compiled from batched_arap.cpp, inverted elements and every PSD strategy
+    it supports."""
+    v = golden("reference_vectors.json")["arap"]
+    assert len(v) == 96
+    for c in v:
+        e, P, C = oracle.material(5, c["mu"], 0.0, np.array(c["F"]), project=c["psd"] != 0, psd=c["psd"])
+        scale = max(1.0, np.abs(c["tangent"]).max())
+        assert e == pytest.approx(c["energy"], rel=1e-11, abs=1e-12)
+        np.testing.assert_allclose(P.reshape(-1), c["pk1"], rtol=1e-10, atol=1e-11)
+        np.testing.assert_allclose(C.reshape(-1), c["tangent"], rtol=1e-9, atol=1e-10 * scale)
+
+
+def test_reference_stiffness_of_each_material(golden):
+    """The rest stiffness the Rayleigh stiffness damping uses (ComputeReferenceMaterialStiffnessVoigt) is the
+    isotropic (lambda, mu) for Neo-Hookean, StVK and linear elasticity and (0, mu / 2) for ARAP."""
+    for c in golden("reference_vectors.json")["reference_stiffness"]:
+        lam0, mu0 = (0.0, 0.5 * c["mu"]) if c["kind"] == 5 else (c["lambda"], c["mu"])
+        want = np.zeros((6, 6))
+        want[:3, :3] = lam0
+        want[np.arange(3), np.arange(3)] += 2 * mu0
+        want[np.arange(3, 6), np.arange(3, 6)] = mu0
+        np.testing.assert_allclose(np.array(c["c0"]).reshape(6, 6), want, rtol=1e-9, atol=1e-9 * c["lambda"])
