@@ -813,11 +813,18 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
   return v;
 }
 
+__device__ __forceinline__ unsigned ld_relaxed_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
 // Grid barrier on a monotonically increasing arrival counter (sync[0], zero at launch): the k-th barrier
 // of a launch completes when the counter reaches k * nblocks. One atomic per CTA and no reset, so the
 // last arrival releases every waiting CTA within one L2 round trip. The spin is bounded: on timeout
 // sync[2] is set and every CTA unwinds.
 __device__ __forceinline__ bool grid_barrier(unsigned* sync, unsigned nblocks, long long spin_limit) {
+  __shared__ unsigned s_bar_err;
   __syncthreads();
   if (threadIdx.x == 0) {
     // release: this CTA's writes (ordered before thread 0 by the CTA barrier) become visible with the
@@ -827,16 +834,23 @@ __device__ __forceinline__ bool grid_barrier(unsigned* sync, unsigned nblocks, l
     asm volatile("atom.add.release.gpu.global.u32 %0, [%1], 1;" : "=r"(prev) : "l"(sync) : "memory");
     const unsigned target = (prev / nblocks + 1u) * nblocks;
     long long spins = 0;
-    while ((int)(ld_acquire_gpu(sync) - target) < 0) {
+    unsigned err;
+    for (;;) {
+      // the error word is read beside each poll (a relaxed load issued first, so both are in flight at
+      // once): a CTA that timed out stops arriving, so the others time out at a later barrier at worst
+      err = ld_relaxed_gpu(sync + 2);
+      if ((int)(ld_acquire_gpu(sync) - target) >= 0) break;
       if (++spins > spin_limit) {
         atomicExch(sync + 2, 1u);  // device timeout: recorded, the kernel unwinds
+        err = 1u;
         break;
       }
       __nanosleep(32);
     }
+    s_bar_err = err;
   }
   __syncthreads();
-  return *((volatile unsigned*)(sync + 2)) == 0u;
+  return s_bar_err == 0u;
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -934,8 +948,12 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     return lo;
   };
 
-  auto clear_acc = [&]() {
-    for (int i = threadIdx.x; i < nwarps * kPcgMaxEnvsPerCta * kPcgNq; i += blockDim.x) wacc[i] = 0.0;
+  auto clear_acc = [&]() {  // the slots of this CTA's envs only
+    const int per_warp = ne * kPcgNq;
+    for (int i = threadIdx.x; i < nwarps * per_warp; i += blockDim.x) {
+      const int w = i / per_warp, j = i - w * per_warp;
+      wacc[w * kPcgMaxEnvsPerCta * kPcgNq + j] = 0.0;
+    }
     __syncthreads();
   };
   auto add_acc = [&](int le, int k, double v) {
@@ -1290,7 +1308,8 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     acc_end(1);
     flush_acc(1, 1);
     if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
-    if (threadIdx.x == 0) {
+    // the last thread reads the run flags while the others load the partials: both round trips overlap
+    if (threadIdx.x == blockDim.x - 1) {
       s_exit = *((volatile int*)(a.sync + 3)) <= 0;
       // re-partition after this iteration once few rows are left to iterate
       s_repart = a.repart_rows > 0 && (long long)*((volatile int*)(a.sync + 5)) <= a.repart_rows;
