@@ -337,6 +337,10 @@ typedef struct {
 } sdx_profile;
 int sdx_set_profiling(sdx_context* ctx, int enable);
 int sdx_get_profile(sdx_context* ctx, sdx_profile* out);
+/* Per-CTA phase times of the persistent PCG while profiling (no reference counterpart): 4 values per CTA,
+ * nanoseconds summed since profiling was enabled: SpMV phase, wait at the barrier after it, update phase,
+ * wait at the barrier after it. */
+int sdx_get_pcg_cta_profile(sdx_context* ctx, int n_cta, double* out);
 
 #ifdef __cplusplus
 }

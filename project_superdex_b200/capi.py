@@ -34,7 +34,7 @@ EXPORTED = [
     "sdx_mlp_set_params", "sdx_mlp_get_params", "sdx_mlp_forward", "sdx_mlp_gradients", "sdx_mlp_train",
     "sdx_collect_training", "sdx_get_training_data", "sdx_write_state_masked", "sdx_capture_state",
     "sdx_restore_state", "sdx_release_state", "sdx_release_all_states", "sdx_is_equal_state",
-    "sdx_capture_state_to_bytes", "sdx_restore_state_from_bytes",
+    "sdx_capture_state_to_bytes", "sdx_restore_state_from_bytes", "sdx_get_pcg_cta_profile",
 ]
 SDX_MLP_PARAMS = 37264
 SDX_NOALLOC_MAX_BLOCK_ROWS = 65536
@@ -127,6 +127,7 @@ def lib():
     L.sdx_set_state.argtypes = [_vp, _dp, _dp, C.c_double]
     L.sdx_get_state.argtypes = [_vp, _dp, _dp, _dp]
     L.sdx_write_state_masked.argtypes = [_vp, _dp, _dp, _up, _up]
+    L.sdx_get_pcg_cta_profile.argtypes = [_vp, C.c_int, _dp]
     L.sdx_capture_state.argtypes = [_vp, C.POINTER(C.c_uint64)]
     L.sdx_restore_state.argtypes = [_vp, C.c_uint64, C.c_int, _up]
     L.sdx_release_state.argtypes = [_vp, C.c_uint64]

@@ -267,6 +267,8 @@ struct sdx_context {
   // opt-in per-kernel timing: event pairs resolved lazily
   bool profiling = false;
   sdx_profile prof;
+  unsigned long long* cta_ns = nullptr;  // per-CTA PCG phase times while profiling (4 per CTA)
+  int cta_ns_n = 0;
   std::vector<cudaEvent_t> ev_pool;
   struct Pending {
     int kind;
@@ -787,6 +789,7 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
     a.env_poff = part->env_poff;
     a.part = part->part;
     a.repart_rows = target;
+    a.cta_ns = (c->profiling && part->n_cta <= c->cta_ns_n) ? c->cta_ns : nullptr;
     cudaError_t e = launch_pcg(a, part->n_cta, part->threads, c->stream);
     c->launches++;
     if (e != cudaSuccess) return set_error(SDX_ERR_CUDA, "PCG cooperative launch: %s", cudaGetErrorString(e));
@@ -906,6 +909,7 @@ extern "C" int sdx_destroy(sdx_context* c) {
   release_mlp(c);
   prof_resolve(c);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+  dfree(c->cta_ns);
   if (c->l2_persist) {
     cudaCtxResetPersistingL2Cache();
     cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, 0);
@@ -928,6 +932,28 @@ extern "C" int sdx_set_profiling(sdx_context* c, int enable) {
   prof_resolve(c);
   c->profiling = enable != 0;
   memset(&c->prof, 0, sizeof(c->prof));
+  if (c->profiling) {  // per-CTA PCG phase times, zeroed at each enable
+    cudaSetDevice(c->device);
+    const int n = 4 * std::max(1, c->num_sms * 8);
+    if (!c->cta_ns) {
+      SDX_TRY(dalloc(&c->cta_ns, n));
+      c->cta_ns_n = n / 4;
+    }
+    SDX_CUDA(cudaMemsetAsync(c->cta_ns, 0, sizeof(unsigned long long) * n, c->stream));
+  }
+  return SDX_OK;
+}
+
+extern "C" int sdx_get_pcg_cta_profile(sdx_context* c, int n_cta, double* out) {
+  if (!c || !out || n_cta <= 0) return set_error(SDX_ERR_INVALID_ARGUMENT, "null or empty argument");
+  if (!c->cta_ns) return set_error(SDX_ERR_NOT_READY, "profiling was never enabled");
+  if (n_cta > c->cta_ns_n) return set_error(SDX_ERR_INVALID_ARGUMENT, "at most %d CTAs", c->cta_ns_n);
+  cudaSetDevice(c->device);
+  std::vector<unsigned long long> h((size_t)4 * n_cta);
+  SDX_CUDA(cudaMemcpyAsync(h.data(), c->cta_ns, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost,
+                           c->stream));
+  SDX_CUDA(cudaStreamSynchronize(c->stream));
+  for (size_t i = 0; i < h.size(); ++i) out[i] = (double)h[i];
   return SDX_OK;
 }
 

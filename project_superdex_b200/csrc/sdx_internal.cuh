@@ -158,6 +158,9 @@ struct PcgArgs {
   int resume;
   int it0;
   EnvSave* es;
+  // per-CTA phase timing (profiling; NULL: off), nanoseconds accumulated over the launch's iterations:
+  // [4 c + 0] SpMV phase, [4 c + 1] wait at the barrier after it, [4 c + 2] update phase, [4 c + 3] wait
+  unsigned long long* cta_ns;
 };
 
 

@@ -813,6 +813,12 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
   return v;
 }
 
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 __device__ __forceinline__ unsigned ld_relaxed_gpu(const unsigned* p) {
   unsigned v;
   asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -1263,6 +1269,24 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     __syncthreads();
   }
 
+  // per-CTA phase timing (thread 0, when profiling): a phase's mark follows flush_acc, whose CTA barrier
+  // has seen every warp finish the phase
+  const bool timing = a.cta_ns != nullptr;
+  __shared__ unsigned long long t_ph[5];  // 4 phase sums and the last mark (shared: no registers held)
+  if (timing && threadIdx.x == 0)
+    for (int k = 0; k < 5; ++k) t_ph[k] = 0ull;
+  auto mark = [&](int k) {
+    if (timing && threadIdx.x == 0) {
+      const unsigned long long t = global_ns();
+      if (k >= 0) t_ph[k] += t - t_ph[4];
+      t_ph[4] = t;
+    }
+  };
+  auto mark_out = [&]() {
+    if (timing && threadIdx.x == 0)
+      for (int k = 0; k < 4; ++k) atomicAdd(a.cta_ns + 4 * c + k, t_ph[k]);
+  };
+  mark(-1);
   for (int it = a.resume ? a.it0 : 1;; ++it) {
     // ---- phase 1 ----
     clear_acc();
@@ -1307,7 +1331,9 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     }
     acc_end(1);
     flush_acc(1, 1);
+    mark(0);
     if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
+    mark(1);
     // the last thread reads the run flags while the others load the partials: both round trips overlap
     if (threadIdx.x == blockDim.x - 1) {
       s_exit = *((volatile int*)(a.sync + 3)) <= 0;
@@ -1317,7 +1343,10 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
       s_replace = (vi == it - 1) || (a.replace_every > 0 && it % a.replace_every == 0);
     }
     reduce_tot(1, 1);
-    if (s_exit) break;
+    if (s_exit) {
+      mark_out();
+      break;
+    }
     const bool replace = s_replace != 0;
     for (int le = threadIdx.x; le < ne; le += blockDim.x) {
       if (st[le].status != 0) continue;
@@ -1394,7 +1423,9 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
       acc_end(3);
     }
     flush_acc(3, 0);
+    mark(2);
     if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
+    mark(3);
     reduce_tot(3, 0);
     for (int le = threadIdx.x; le < ne; le += blockDim.x) {
       if (st[le].status == 5) {
@@ -1453,6 +1484,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
         a.sync[6] = (unsigned)(it + 1);
         a.sync[7] = 1u;
       }
+      mark_out();
       return;
     }
   }

@@ -47,6 +47,8 @@ def main(argv=None):
     ap.add_argument("--iters", type=int, default=100)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cta-profile", default=None,
+                    help="pcg: also time each CTA's phases over two launches and save them to this .npy")
     args = ap.parse_args(argv)
     if args.workload == "batch":
         bodies, cfg = scenes.config2(args.seed)
@@ -71,6 +73,24 @@ def main(argv=None):
         us = prof["pcg_ms"] * 1e3 / max(1, prof["pcg_iters"])
         out.update(cg_iters=st["cg_iters"], bytes_per_iter=bpi, us_per_iter=us,
                    algorithmic_tbs=bpi / (us * 1e-6) / 1e12)
+        if args.cta_profile:
+            import numpy as np
+            n_cta = torch.cuda.get_device_properties(0).multi_processor_count
+            runs = []
+            for _ in range(2):  # two launches: is the per-CTA spread systematic?
+                w.set_profiling(True)
+                w.step(1)
+                torch.cuda.synchronize()
+                runs.append(w.pcg_cta_profile(n_cta) / max(1, w.profile()["pcg_iters"]) * 1e-3)  # us / iter
+            prof2 = np.stack(runs)
+            np.save(args.cta_profile, prof2)
+            spmv = prof2[:, :, 0]
+            out.update(cta_spmv_us_mean=float(spmv.mean()), cta_spmv_us_min=float(spmv.min()),
+                       cta_spmv_us_max=float(spmv.max()),
+                       cta_spmv_run_corr=float(np.corrcoef(spmv[0], spmv[1])[0, 1]),
+                       cta_wait1_us_mean=float(prof2[:, :, 1].mean()),
+                       cta_update_us_mean=float(prof2[:, :, 2].mean()),
+                       cta_wait2_us_mean=float(prof2[:, :, 3].mean()))
     elif args.case == "element":
         torch.cuda.profiler.start()
         w.assemble(hess=True, psd=True, obj=True)
