@@ -335,11 +335,12 @@ typedef struct {
   int64_t pcg_relaunches;   /* re-partitioned PCG relaunches (batches whose slow envs got all CTAs) */
   int64_t pcg_threads;      /* threads per CTA of the PCG launch shape in use (autotuned or default) */
 } sdx_profile;
+/* enable: 0 off, 1 per-kernel event timing, 2 also the per-CTA PCG phase timers (sdx_get_pcg_cta_profile) */
 int sdx_set_profiling(sdx_context* ctx, int enable);
 int sdx_get_profile(sdx_context* ctx, sdx_profile* out);
-/* Per-CTA phase times of the persistent PCG while profiling (no reference counterpart): 4 values per CTA,
- * nanoseconds summed since profiling was enabled: SpMV phase, wait at the barrier after it, update phase,
- * wait at the barrier after it. */
+/* Per-CTA phase times of the persistent PCG (no reference counterpart), recorded while profiling at level 2
+ * (sdx_set_profiling(ctx, 2)): 4 values per CTA, SM clock cycles summed since then: SpMV phase, wait at the
+ * barrier after it, update phase, wait at the barrier after it. */
 int sdx_get_pcg_cta_profile(sdx_context* ctx, int n_cta, double* out);
 
 #ifdef __cplusplus

@@ -267,8 +267,9 @@ struct sdx_context {
   // opt-in per-kernel timing: event pairs resolved lazily
   bool profiling = false;
   sdx_profile prof;
-  unsigned long long* cta_ns = nullptr;  // per-CTA PCG phase times while profiling (4 per CTA)
+  unsigned long long* cta_ns = nullptr;  // per-CTA PCG phase cycles while profiling at level 2 (4 per CTA)
   int cta_ns_n = 0;
+  bool cta_timers = false;
   std::vector<cudaEvent_t> ev_pool;
   struct Pending {
     int kind;
@@ -789,7 +790,7 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
     a.env_poff = part->env_poff;
     a.part = part->part;
     a.repart_rows = target;
-    a.cta_ns = (c->profiling && part->n_cta <= c->cta_ns_n) ? c->cta_ns : nullptr;
+    a.cta_ns = (c->profiling && c->cta_timers && part->n_cta <= c->cta_ns_n) ? c->cta_ns : nullptr;
     cudaError_t e = launch_pcg(a, part->n_cta, part->threads, c->stream);
     c->launches++;
     if (e != cudaSuccess) return set_error(SDX_ERR_CUDA, "PCG cooperative launch: %s", cudaGetErrorString(e));
@@ -931,8 +932,9 @@ extern "C" int sdx_set_profiling(sdx_context* c, int enable) {
   if (!c) return set_error(SDX_ERR_INVALID_ARGUMENT, "null context");
   prof_resolve(c);
   c->profiling = enable != 0;
+  c->cta_timers = (enable & 2) != 0;
   memset(&c->prof, 0, sizeof(c->prof));
-  if (c->profiling) {  // per-CTA PCG phase times, zeroed at each enable
+  if (c->cta_timers) {  // per-CTA PCG phase cycles, zeroed at each enable
     cudaSetDevice(c->device);
     const int n = 4 * std::max(1, c->num_sms * 8);
     if (!c->cta_ns) {
@@ -946,7 +948,7 @@ extern "C" int sdx_set_profiling(sdx_context* c, int enable) {
 
 extern "C" int sdx_get_pcg_cta_profile(sdx_context* c, int n_cta, double* out) {
   if (!c || !out || n_cta <= 0) return set_error(SDX_ERR_INVALID_ARGUMENT, "null or empty argument");
-  if (!c->cta_ns) return set_error(SDX_ERR_NOT_READY, "profiling was never enabled");
+  if (!c->cta_ns) return set_error(SDX_ERR_NOT_READY, "per-CTA timers were never enabled (profiling level 2)");
   if (n_cta > c->cta_ns_n) return set_error(SDX_ERR_INVALID_ARGUMENT, "at most %d CTAs", c->cta_ns_n);
   cudaSetDevice(c->device);
   std::vector<unsigned long long> h((size_t)4 * n_cta);

@@ -158,7 +158,7 @@ struct PcgArgs {
   int resume;
   int it0;
   EnvSave* es;
-  // per-CTA phase timing (profiling; NULL: off), nanoseconds accumulated over the launch's iterations:
+  // per-CTA phase timing (NULL: off), SM clock cycles accumulated over the launch's iterations:
   // [4 c + 0] SpMV phase, [4 c + 1] wait at the barrier after it, [4 c + 2] update phase, [4 c + 3] wait
   unsigned long long* cta_ns;
 };

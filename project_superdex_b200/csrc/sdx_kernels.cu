@@ -813,12 +813,6 @@ __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
   return v;
 }
 
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
 __device__ __forceinline__ unsigned ld_relaxed_gpu(const unsigned* p) {
   unsigned v;
   asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -925,7 +919,9 @@ __device__ __forceinline__ void true_residual(const PcgArgs& a, int s, int lane,
 
 // kPipe: SpMV phase with the software-pipelined row product (128 registers, so at most 512 threads per
 // SM); otherwise the batched product that fits 64 registers at 1024 threads.
-template <bool kPipe>
+// kTimed: the variant with the per-CTA phase timers (launched only when they are asked for, so that the
+// default variant's code is exactly the untimed one)
+template <bool kPipe, bool kTimed>
 __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
   extern __shared__ double wacc[];  // [nwarps][kPcgMaxEnvsPerCta][kPcgNq]
   __shared__ EnvState st[kPcgMaxEnvsPerCta];
@@ -1269,22 +1265,28 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     __syncthreads();
   }
 
-  // per-CTA phase timing (thread 0, when profiling): a phase's mark follows flush_acc, whose CTA barrier
-  // has seen every warp finish the phase
-  const bool timing = a.cta_ns != nullptr;
-  __shared__ unsigned long long t_ph[5];  // 4 phase sums and the last mark (shared: no registers held)
-  if (timing && threadIdx.x == 0)
-    for (int k = 0; k < 5; ++k) t_ph[k] = 0ull;
+  // per-CTA phase timing (thread 0, when asked for): a phase's mark follows flush_acc, whose CTA barrier
+  // has seen every warp finish the phase. The SM cycle counter: a %globaltimer read just before each
+  // barrier arrival delayed the arrival measurably (about 3 us per iteration)
+  __shared__ unsigned long long t_ph[kTimed ? 5 : 1];  // 4 phase sums and the last mark
+  if constexpr (kTimed) {
+    if (threadIdx.x == 0)
+      for (int k = 0; k < 5; ++k) t_ph[k] = 0ull;
+  }
   auto mark = [&](int k) {
-    if (timing && threadIdx.x == 0) {
-      const unsigned long long t = global_ns();
-      if (k >= 0) t_ph[k] += t - t_ph[4];
-      t_ph[4] = t;
+    if constexpr (kTimed) {
+      if (threadIdx.x == 0) {
+        const unsigned long long t = (unsigned long long)clock64();
+        if (k >= 0) t_ph[k] += t - t_ph[4];
+        t_ph[4] = t;
+      }
     }
   };
   auto mark_out = [&]() {
-    if (timing && threadIdx.x == 0)
-      for (int k = 0; k < 4; ++k) atomicAdd(a.cta_ns + 4 * c + k, t_ph[k]);
+    if constexpr (kTimed) {
+      if (threadIdx.x == 0)
+        for (int k = 0; k < 4; ++k) atomicAdd(a.cta_ns + 4 * c + k, t_ph[k]);
+    }
   };
   mark(-1);
   for (int it = a.resume ? a.it0 : 1;; ++it) {
@@ -1340,7 +1342,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
       // re-partition after this iteration once few rows are left to iterate
       s_repart = a.repart_rows > 0 && (long long)*((volatile int*)(a.sync + 5)) <= a.repart_rows;
       const int vi = *((volatile int*)(a.sync + 4));
-      s_replace = (vi == it - 1) || (a.replace_every > 0 && it % a.replace_every == 0);
+      s_replace = (vi > 0 && vi == it - 1) || (a.replace_every > 0 && it % a.replace_every == 0);
     }
     reduce_tot(1, 1);
     if (s_exit) {
@@ -1501,12 +1503,13 @@ static bool pcg_pipelined(int threads) {
 
 int pcg_max_ctas_per_sm(int threads) {
   int n = 0;
-  for (const void* fn : {(const void*)k_pcg<true>, (const void*)k_pcg<false>})
+  for (const void* fn : {(const void*)k_pcg<true, false>, (const void*)k_pcg<false, false>,
+                         (const void*)k_pcg<true, true>, (const void*)k_pcg<false, true>})
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, pcg_shared_bytes(1024));
   const cudaError_t e =
       pcg_pipelined(threads)
-          ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pcg<true>, threads, pcg_shared_bytes(threads))
-          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pcg<false>, threads, pcg_shared_bytes(threads));
+          ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pcg<true, false>, threads, pcg_shared_bytes(threads))
+          : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pcg<false, false>, threads, pcg_shared_bytes(threads));
   return e == cudaSuccess ? n : 0;
 }
 
@@ -1515,7 +1518,10 @@ int pcg_shared_bytes(int threads) { return (threads / 32) * kPcgMaxEnvsPerCta * 
 cudaError_t launch_pcg(const PcgArgs& a, int n_cta, int threads, cudaStream_t st) {
   PcgArgs args = a;
   void* params[] = {&args};
-  const void* fn = pcg_pipelined(threads) ? (const void*)k_pcg<true> : (const void*)k_pcg<false>;
+  const bool timed = a.cta_ns != nullptr;
+  const void* fn = pcg_pipelined(threads)
+                       ? (timed ? (const void*)k_pcg<true, true> : (const void*)k_pcg<true, false>)
+                       : (timed ? (const void*)k_pcg<false, true> : (const void*)k_pcg<false, false>);
   return cudaLaunchCooperativeKernel(fn, dim3(n_cta), dim3(threads), params,
                                      (size_t)pcg_shared_bytes(threads), st);
 }

@@ -78,10 +78,14 @@ def main(argv=None):
             n_cta = torch.cuda.get_device_properties(0).multi_processor_count
             runs = []
             for _ in range(2):  # two launches: is the per-CTA spread systematic?
-                w.set_profiling(True)
+                w.set_profiling(True, cta=True)
                 w.step(1)
                 torch.cuda.synchronize()
-                runs.append(w.pcg_cta_profile(n_cta) / max(1, w.profile()["pcg_iters"]) * 1e-3)  # us / iter
+                pr = w.profile()
+                cyc = w.pcg_cta_profile(n_cta)
+                # cycles -> us: each CTA's four phases add up to the launch's event-timed iteration
+                us_it = pr["pcg_ms"] * 1e3 / max(1, pr["pcg_iters"])
+                runs.append(cyc / cyc.sum(axis=1, keepdims=True) * us_it)
             prof2 = np.stack(runs)
             np.save(args.cta_profile, prof2)
             spmv = prof2[:, :, 0]

@@ -213,14 +213,15 @@ class SoftBodyWorld:
         return int(h.value or 0)
 
     def pcg_cta_profile(self, n_cta: int) -> np.ndarray:
-        """Per-CTA PCG phase times [n_cta, 4] in ns since profiling was enabled (SpMV phase, barrier wait,
-        update phase, barrier wait)."""
+        """Per-CTA PCG phase times [n_cta, 4] in SM clock cycles since profiling was enabled with cta=True
+        (SpMV phase, barrier wait, update phase, barrier wait)."""
         out = np.zeros(4 * int(n_cta))
         capi.check(capi.lib().sdx_get_pcg_cta_profile(self._ctx, int(n_cta), capi.ptr(out)))
         return out.reshape(int(n_cta), 4)
 
-    def set_profiling(self, enable: bool = True):
-        capi.check(capi.lib().sdx_set_profiling(self._ctx, int(enable)))
+    def set_profiling(self, enable: bool = True, cta: bool = False):
+        """Per-kernel event timing; with cta=True also the per-CTA PCG phase timers."""
+        capi.check(capi.lib().sdx_set_profiling(self._ctx, (2 if cta else 1) if enable else 0))
 
     def profile(self) -> dict:
         p = capi.Profile()
