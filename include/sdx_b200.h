@@ -334,6 +334,8 @@ typedef struct {
                                (40 B per block + 4 B per row pointer + 228 B per row) */
   int64_t pcg_relaunches;   /* re-partitioned PCG relaunches (batches whose slow envs got all CTAs) */
   int64_t pcg_threads;      /* threads per CTA of the PCG launch shape in use (autotuned or default) */
+  double warm_ms;           /* learned warm start: features, MLP inference and the start-vector kernel */
+  int64_t warm_launches;
 } sdx_profile;
 /* enable: 0 off, 1 per-kernel event timing, 2 also the per-CTA PCG phase timers (sdx_get_pcg_cta_profile) */
 int sdx_set_profiling(sdx_context* ctx, int enable);

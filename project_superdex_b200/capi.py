@@ -84,7 +84,8 @@ class Profile(C.Structure):
                 ("asm_res_ms", C.c_double), ("asm_res_launches", C.c_int64),
                 ("contact_ms", C.c_double), ("contact_launches", C.c_int64),
                 ("seed_ms", C.c_double), ("seed_launches", C.c_int64), ("pcg_bytes", C.c_double),
-                ("pcg_relaunches", C.c_int64), ("pcg_threads", C.c_int64)]
+                ("pcg_relaunches", C.c_int64), ("pcg_threads", C.c_int64), ("warm_ms", C.c_double),
+                ("warm_launches", C.c_int64)]
 
 
 _dp = C.POINTER(C.c_double)

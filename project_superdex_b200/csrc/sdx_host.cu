@@ -278,7 +278,7 @@ struct sdx_context {
   std::vector<Pending> pending;
 };
 
-enum { PROF_PCG = 0, PROF_HESS = 1, PROF_RES = 2, PROF_CONTACT = 3, PROF_SEED = 4 };
+enum { PROF_PCG = 0, PROF_HESS = 1, PROF_RES = 2, PROF_CONTACT = 3, PROF_SEED = 4, PROF_WARM = 5 };
 
 static cudaEvent_t pool_event(sdx_context* c) {
   if (!c->ev_pool.empty()) {
@@ -329,6 +329,10 @@ static void prof_resolve(sdx_context* c) {
       case PROF_SEED:
         c->prof.seed_ms += ms;
         c->prof.seed_launches++;
+        break;
+      case PROF_WARM:
+        c->prof.warm_ms += ms;
+        c->prof.warm_launches++;
         break;
     }
     c->ev_pool.push_back(pd.a);
@@ -2174,6 +2178,8 @@ static int step_once(sdx_context* c) {
     // step, zero when there is none)
     const bool keep_hist = (p.warm_start == SDX_WARM_TEMPORAL || learned || collect) && pass < sdx_context::kHist;
     if (keep_hist && !c->dx_hist) SDX_TRY(dalloc(&c->dx_hist, (size_t)sdx_context::kHist * n3));
+    cudaEvent_t ev_warm;
+    if (learned || collect) prof_begin(c, &ev_warm);
     if (learned || collect) {
       if (keep_hist && c->hist_valid[pass])
         launch_copy_rows(c->n_slices, c->slice_env, c->env_mask, c->dx_hist + (size_t)pass * n3, c->dx_prev2,
@@ -2195,6 +2201,7 @@ static int step_once(sdx_context* c) {
                         c->env_hnorm, c->env_rows, c->dx, c->uscratch, c->stream);
       c->launches += 2;
     }
+    if (learned || collect) prof_end(c, PROF_WARM, ev_warm);
     const bool temporal = p.warm_start == SDX_WARM_TEMPORAL && pass < sdx_context::kHist;
     if (temporal && c->hist_valid[pass]) {
       launch_copy_rows(c->n_slices, c->slice_env, c->env_mask, c->dx_hist + (size_t)pass * n3, c->dx, c->stream);
