@@ -126,9 +126,14 @@ __device__ __forceinline__ void load_weight(const __nv_bfloat16* __restrict__ W,
   }
 }
 
-__global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpForwardArgs a) {
+// 256 threads: warps w and w + 4 read the same TMEM lane quadrant (vertices 32 (w % 4) ..) and split the
+// 128 accumulator columns of the bias + GELU epilogue between them
+constexpr int kMlpThreads = 256;
+
+__global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_forward(MlpForwardArgs a) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int tid = threadIdx.x, warp = tid >> 5;
+  const int lrow = tid & (kTile - 1), half = tid / kTile;  // tile row (TMEM lane) and column half
   const uint32_t base = smem_u32(smem);
   const uint32_t mbar = base + kSBar;
   uint32_t* tmem_holder = reinterpret_cast<uint32_t*>(smem + kSTmem);
@@ -148,15 +153,15 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpForwardArgs a) {
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_holder;
-  const uint32_t my_lanes = tmem + ((uint32_t)(warp * 32) << 16);
+  const uint32_t my_lanes = tmem + ((uint32_t)((warp & 3) * 32) << 16);
   uint32_t phase = 0;
   bool ok = true;
 
   const int n_tiles = (a.n + kTile - 1) / kTile;
   for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
-    const int row = tile * kTile + tid;  // this thread's vertex (TMEM lane tid)
-    // input tile: 16 features -> bf16
-    {
+    const int row = tile * kTile + lrow;  // this thread's vertex (TMEM lane lrow)
+    // input tile: 16 features -> bf16 (first column half)
+    if (half == 0) {
       float x[16];
       if (row < a.n) {
 #pragma unroll
@@ -176,7 +181,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpForwardArgs a) {
         __align__(16) __nv_bfloat16 h[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) h[i] = __float2bfloat16(x[kc * 8 + i]);
-        *reinterpret_cast<uint4*>(smem + kSX + core_off(tid, kc * 8, 16)) = *reinterpret_cast<uint4*>(h);
+        *reinterpret_cast<uint4*>(smem + kSX + core_off(lrow, kc * 8, 16)) = *reinterpret_cast<uint4*>(h);
       }
     }
     for (int layer = 0; layer < 4 && ok; ++layer) {
@@ -208,7 +213,7 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpForwardArgs a) {
         const float* bias = layer == 0 ? a.b1 : layer == 1 ? a.b2 : a.b3;
         float* zout = a.Z ? a.Z + (size_t)layer * a.n * 128 : nullptr;
 #pragma unroll 1
-        for (int c0 = 0; c0 < 128; c0 += 16) {
+        for (int c0 = half * 64; c0 < half * 64 + 64; c0 += 16) {
           float acc[16];
           tmem_ld16(my_lanes + c0, acc);
           __align__(16) __nv_bfloat16 h[16];
@@ -218,10 +223,10 @@ __global__ void __launch_bounds__(128, 1) k_mlp_forward(MlpForwardArgs a) {
             if (zout && row < a.n) zout[(size_t)row * 128 + c0 + i] = z;
             h[i] = __float2bfloat16(gelu(z));
           }
-          *reinterpret_cast<uint4*>(smem + kSH + core_off(tid, c0, 128)) = *reinterpret_cast<uint4*>(h);
-          *reinterpret_cast<uint4*>(smem + kSH + core_off(tid, c0 + 8, 128)) = *reinterpret_cast<uint4*>(h + 8);
+          *reinterpret_cast<uint4*>(smem + kSH + core_off(lrow, c0, 128)) = *reinterpret_cast<uint4*>(h);
+          *reinterpret_cast<uint4*>(smem + kSH + core_off(lrow, c0 + 8, 128)) = *reinterpret_cast<uint4*>(h + 8);
         }
-      } else {
+      } else if (half == 0) {  // warp-uniform: the output columns are read by the first four warps
         float acc[16];
         tmem_ld16(my_lanes, acc);
         if (row < a.n) {
@@ -248,7 +253,7 @@ int launch_mlp_forward(const MlpForwardArgs& a, int num_sms, cudaStream_t st) {
   if (a.n <= 0) return 0;
   const int tiles = (a.n + kTile - 1) / kTile;
   const int grid = tiles < num_sms ? tiles : num_sms;
-  k_mlp_forward<<<grid, 128, kSmemBytes, st>>>(a);
+  k_mlp_forward<<<grid, kMlpThreads, kSmemBytes, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -452,7 +457,7 @@ __global__ void k_feature_raw(int64_t n_rows, const double* __restrict__ u, cons
   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n_rows) return;
   const int dp = diag_pos[r];
-  float* o = raw + 16 * r;
+  float o[16];
 #pragma unroll
   for (int k = 0; k < 3; ++k) {
     const float d = dp >= 0 ? val[val_index(dp, 4 * k)] : 0.0f;
@@ -464,24 +469,46 @@ __global__ void k_feature_raw(int64_t n_rows, const double* __restrict__ u, cons
     o[12 + k] = (free && d != 0.0f) ? (float)(g[3 * r + k] / d) : 0.0f;
   }
   o[15] = 0.0f;
+  float4* out = reinterpret_cast<float4*>(raw + 16 * r);  // 64-byte records
+#pragma unroll
+  for (int q = 0; q < 4; ++q) out[q] = make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
 }
 
-// per-env sums of squares of the 5 feature groups (u, dt v, dx_{k-1}, dx_{k-2}, D^-1 g)
-__global__ void k_feature_scale(int n_slices, const int* __restrict__ slice_env, const uint8_t* __restrict__ env_mask,
-                                const float* __restrict__ raw, double* sumsq) {
-  const int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+// per-env sums of squares of the 5 feature groups (u, dt v, dx_{k-1}, dx_{k-2}, D^-1 g). Each warp walks a
+// contiguous run of slices and keeps lane-local sums while the env stays the same (slices are env-ordered),
+// so the atomics are one per warp and env run instead of one per slice.
+__global__ void k_feature_scale(int n_slices, int per_warp, const int* __restrict__ slice_env,
+                                const uint8_t* __restrict__ env_mask, const float* __restrict__ raw, double* sumsq) {
+  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (s >= n_slices) return;
-  const int e = slice_env[s];
-  if (env_mask && !env_mask[e]) return;
-  const float* o = raw + 16 * ((int64_t)s * 32 + lane);
+  const int s0 = wid * per_warp, s1 = min(n_slices, s0 + per_warp);
+  double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  int cur = -1;
+  auto flush = [&]() {
 #pragma unroll
-  for (int grp = 0; grp < 5; ++grp) {
-    double v = (double)o[3 * grp] * o[3 * grp] + (double)o[3 * grp + 1] * o[3 * grp + 1] +
-               (double)o[3 * grp + 2] * o[3 * grp + 2];
-    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-    if (lane == 0) atomicAdd(sumsq + 5 * e + grp, v);
+    for (int grp = 0; grp < 5; ++grp) {
+      double v = acc[grp];
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      if (lane == 0 && cur >= 0) atomicAdd(sumsq + 5 * cur + grp, v);
+      acc[grp] = 0.0;
+    }
+  };
+  for (int s = s0; s < s1; ++s) {
+    const int e = slice_env[s];
+    if (e != cur) {
+      flush();
+      cur = e;
+    }
+    if (env_mask && !env_mask[e]) continue;
+    const float4* o = reinterpret_cast<const float4*>(raw + 16 * ((int64_t)s * 32 + lane));
+    const float4 a = o[0], b = o[1], c = o[2], d = o[3];
+    const float f[16] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w, d.x, d.y, d.z, d.w};
+#pragma unroll
+    for (int grp = 0; grp < 5; ++grp)
+      acc[grp] += (double)f[3 * grp] * f[3 * grp] + (double)f[3 * grp + 1] * f[3 * grp + 1] +
+                  (double)f[3 * grp + 2] * f[3 * grp + 2];
   }
+  flush();
 }
 
 // X[row] = 1-ring average of each raw group / that group's RMS over the env (inputs of order one)
@@ -500,13 +527,15 @@ __global__ void k_feature_ring(Matrix A, const uint8_t* __restrict__ env_mask, c
   for (int k = 0; k < w; ++k) {
     const int cj = A.col[base + k * 32 + lane];
     if (cj & kPadBit) continue;
-    const float* o = raw + 16 * (int64_t)cj;
+    const float4* o = reinterpret_cast<const float4*>(raw + 16 * (int64_t)cj);  // one 64-byte record
+    const float4 a = o[0], b = o[1], c = o[2], d = o[3];
+    const float f[15] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w, d.x, d.y, d.z};
 #pragma unroll
-    for (int i = 0; i < 15; ++i) acc[i] += o[i];
+    for (int i = 0; i < 15; ++i) acc[i] += f[i];
     ++cnt;
   }
   const bool active = !env_mask || env_mask[e];
-  float* x = X + 16 * row;
+  float x[16];
 #pragma unroll
   for (int grp = 0; grp < 5; ++grp) {
     const double rms = sqrt(sumsq[5 * e + grp] / fmax(1.0, (double)env_rows[e]));
@@ -515,6 +544,9 @@ __global__ void k_feature_ring(Matrix A, const uint8_t* __restrict__ env_mask, c
     for (int i = 0; i < 3; ++i) x[3 * grp + i] = acc[3 * grp + i] * inv;
   }
   x[15] = 0.0f;
+  float4* xo = reinterpret_cast<float4*>(X + 16 * row);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) xo[q] = make_float4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
 }
 
 // dx0 = MLP(X) on free DoFs of active envs (its scale is set by the solver's energy-optimal scaling)
@@ -549,7 +581,14 @@ void launch_features(const Matrix& A, int64_t n_rows, const uint8_t* env_mask, c
                                                                    pin, raw);
   cudaMemsetAsync(sumsq, 0, sizeof(double) * 5 * n_envs, st);
   const int64_t t = (int64_t)A.n_slices * 32;
-  k_feature_scale<<<(unsigned)((t + 255) / 256), 256, 0, st>>>(A.n_slices, A.slice_env, env_mask, raw, sumsq);
+  {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int warps = 8 * sms;  // one 256-thread block per SM
+    const int per_warp = (A.n_slices + warps - 1) / warps;
+    k_feature_scale<<<(unsigned)sms, 256, 0, st>>>(A.n_slices, per_warp, A.slice_env, env_mask, raw, sumsq);
+  }
   k_feature_ring<<<(unsigned)((t + 255) / 256), 256, 0, st>>>(A, env_mask, raw, sumsq, env_rows, X);
 }
 void launch_warm_start(int64_t n_rows, const int* slice_env, const uint8_t* env_mask, const float* Y,
