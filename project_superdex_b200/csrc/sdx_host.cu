@@ -131,7 +131,9 @@ struct PcgWork {
   double* env_rel_tol = nullptr;
   EnvSave* es = nullptr;  // per env CG scalars across re-partitioning relaunches
   int n_envs_alloc = 0;
+  double* gal = nullptr;  // A x2 of the Galerkin start (allocated on first use)
   void release() {
+    dfree(gal);
     dfree(arena);
     arena_bytes = 0;
     hot_b = hot_x = nullptr;
@@ -720,6 +722,10 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
   a.b = b;
   a.x = x;
   a.x2 = x2;
+  if (x2) {
+    if (!W.gal) SDX_TRY(dalloc(&W.gal, (size_t)3 * W.n_rows));
+    a.gal = W.gal;
+  }
   a.r = W.r;
   a.p = W.p;
   a.q = W.q;

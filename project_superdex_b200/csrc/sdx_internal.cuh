@@ -121,6 +121,7 @@ struct PcgArgs {
   const double* b;
   double* x;
   const double* x2;  // second start vector (learned correction): Galerkin start on span{x, x2} (NULL: none)
+  double* gal;       // 3 per row: A x2 kept by the Galerkin start (needed with x2)
   double* r;
   float* p;
   float* q;

@@ -877,44 +877,74 @@ __device__ __forceinline__ void prec_apply(const PcgArgs& a, int64_t row, const 
 }
 
 // y = A v for the 32 rows of slice s, FP64 accumulation (FP32 matrix values, FP64 v gathered from L2)
-__device__ __forceinline__ void spmv_f64(const PcgArgs& a, int s, int lane, const double* v_, double y[3]) {
-  const int base = a.A.slice_ptr[s], w = a.A.slice_w[s];
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-  for (int k = 0; k < w; ++k) {
-    const int p = base + k * kSlice + lane;
-    const int j = __ldcs(a.A.col + p) & 0x7fffffff;
-    float v[9];
-    load_block(a.A.val + (size_t)(base + k * kSlice) * 9, lane, v);
-    const double x0 = __ldcg(v_ + 3 * (int64_t)j), x1 = __ldcg(v_ + 3 * (int64_t)j + 1),
-                 x2 = __ldcg(v_ + 3 * (int64_t)j + 2);
-    a0 += (double)v[0] * x0 + (double)v[1] * x1 + (double)v[2] * x2;
-    a1 += (double)v[3] * x0 + (double)v[4] * x1 + (double)v[5] * x2;
-    a2 += (double)v[6] * x0 + (double)v[7] * x1 + (double)v[8] * x2;
+// y = A v (and y2 = A v2 with kVec = 2) for one slice row: FP32 blocks times FP64 gathers, accumulated in
+// FP64 in ascending block order. The column, value and gather loads of kBatch consecutive groups are issued
+// before their FMAs (the loop was latency bound one group at a time).
+template <int kBatch, int kVec>
+__device__ __forceinline__ void spmv_f64_rows(const Matrix& A, int s, int lane, const double* __restrict__ v1,
+                                              const double* __restrict__ v2, double y1[3], double y2[3]) {
+  const int base = A.slice_ptr[s], w = A.slice_w[s];
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0;
+  auto acc = [&](const float v[9], const double x[3], const double z[3]) {
+    a0 += (double)v[0] * x[0] + (double)v[1] * x[1] + (double)v[2] * x[2];
+    a1 += (double)v[3] * x[0] + (double)v[4] * x[1] + (double)v[5] * x[2];
+    a2 += (double)v[6] * x[0] + (double)v[7] * x[1] + (double)v[8] * x[2];
+    if constexpr (kVec == 2) {
+      b0 += (double)v[0] * z[0] + (double)v[1] * z[1] + (double)v[2] * z[2];
+      b1 += (double)v[3] * z[0] + (double)v[4] * z[1] + (double)v[5] * z[2];
+      b2 += (double)v[6] * z[0] + (double)v[7] * z[1] + (double)v[8] * z[2];
+    }
+  };
+  int k = 0;
+  for (; k + kBatch <= w; k += kBatch) {
+    int j[kBatch];
+    float v[kBatch][9];
+    double x[kBatch][3], z[kBatch][3];
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) j[u] = __ldcs(A.col + base + (k + u) * kSlice + lane) & 0x7fffffff;
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) load_block(A.val + (size_t)(base + (k + u) * kSlice) * 9, lane, v[u]);
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        x[u][c] = __ldcg(v1 + 3 * (int64_t)j[u] + c);
+        if constexpr (kVec == 2) z[u][c] = __ldcg(v2 + 3 * (int64_t)j[u] + c);
+      }
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) acc(v[u], x[u], z[u]);
   }
-  y[0] = a0;
-  y[1] = a1;
-  y[2] = a2;
+  for (; k < w; ++k) {
+    const int j = __ldcs(A.col + base + k * kSlice + lane) & 0x7fffffff;
+    float v[9];
+    load_block(A.val + (size_t)(base + k * kSlice) * 9, lane, v);
+    double x[3], z[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      x[c] = __ldcg(v1 + 3 * (int64_t)j + c);
+      if constexpr (kVec == 2) z[c] = __ldcg(v2 + 3 * (int64_t)j + c);
+    }
+    acc(v, x, z);
+  }
+  y1[0] = a0;
+  y1[1] = a1;
+  y1[2] = a2;
+  if constexpr (kVec == 2) {
+    y2[0] = b0;
+    y2[1] = b1;
+    y2[2] = b2;
+  }
 }
 
 // r = b - A x with FP64 accumulation (FP32 matrix values, FP64 x gathered from L2)
+template <int kBatch>
 __device__ __forceinline__ void true_residual(const PcgArgs& a, int s, int lane, double r[3]) {
-  const int base = a.A.slice_ptr[s], w = a.A.slice_w[s];
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-  for (int k = 0; k < w; ++k) {
-    const int p = base + k * kSlice + lane;
-    const int j = __ldcs(a.A.col + p) & 0x7fffffff;
-    float v[9];
-    load_block(a.A.val + (size_t)(base + k * kSlice) * 9, lane, v);
-    const double x0 = __ldcg(a.x + 3 * (int64_t)j), x1 = __ldcg(a.x + 3 * (int64_t)j + 1),
-                 x2 = __ldcg(a.x + 3 * (int64_t)j + 2);
-    a0 += (double)v[0] * x0 + (double)v[1] * x1 + (double)v[2] * x2;
-    a1 += (double)v[3] * x0 + (double)v[4] * x1 + (double)v[5] * x2;
-    a2 += (double)v[6] * x0 + (double)v[7] * x1 + (double)v[8] * x2;
-  }
+  double ax[3];
+  spmv_f64_rows<kBatch, 1>(a.A, s, lane, a.x, nullptr, ax, nullptr);
   const int64_t row = (int64_t)s * kSlice + lane;
-  r[0] = a.b[3 * row] - a0;
-  r[1] = a.b[3 * row + 1] - a1;
-  r[2] = a.b[3 * row + 2] - a2;
+  r[0] = a.b[3 * row] - ax[0];
+  r[1] = a.b[3 * row + 1] - ax[1];
+  r[2] = a.b[3 * row + 2] - ax[2];
 }
 
 // kPipe: SpMV phase with the software-pipelined row product (128 registers, so at most 512 threads per
@@ -925,6 +955,7 @@ template <bool kPipe, bool kTimed>
 __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
   extern __shared__ double wacc[];  // [nwarps][kPcgMaxEnvsPerCta][kPcgNq]
   __shared__ EnvState st[kPcgMaxEnvsPerCta];
+  constexpr int kB64 = kPipe ? 4 : 2;  // groups per batch of the FP64 SpMVs (register budget of the variant)
   __shared__ double tot[kPcgMaxEnvsPerCta][kPcgNq];
   __shared__ int s_exit, s_replace;
   const int c = blockIdx.x;
@@ -1087,8 +1118,13 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
         if (st[le].status != 0) continue;
         const int64_t row = (int64_t)s * kSlice + lane;
         double ah[3], ay[3];
-        spmv_f64(a, s, lane, a.x, ah);
-        spmv_f64(a, s, lane, a.x2, ay);
+        spmv_f64_rows<kB64, 2>(a.A, s, lane, a.x, a.x2, ah, ay);  // one pass over the matrix for both
+        // kept for the residual of the combination (r is not gathered in this pass)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          a.r[3 * row + k] = ah[k];
+          a.gal[3 * row + k] = ay[k];
+        }
         double q[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
@@ -1141,12 +1177,17 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
         if (st[le].status != 0) continue;
         const int64_t row = (int64_t)s * kSlice + lane;
         const double ca = st[le].alpha, cb = st[le].beta;
+        // x = ca h + cb y and its residual b - ca A h - cb A y from the kept products: row-local, so the
+        // pass below needs neither a barrier nor another SpMV
 #pragma unroll
-        for (int k = 0; k < 3; ++k) a.x[3 * row + k] = ca * a.x[3 * row + k] + cb * a.x2[3 * row + k];
+        for (int k = 0; k < 3; ++k) {
+          a.x[3 * row + k] = ca * a.x[3 * row + k] + cb * a.x2[3 * row + k];
+          a.r[3 * row + k] = a.b[3 * row + k] - ca * a.r[3 * row + k] - cb * a.gal[3 * row + k];
+        }
       }
+      __syncthreads();
       for (int le = threadIdx.x; le < ne; le += blockDim.x) st[le].beta = 0.0;
-      // the residual pass below gathers neighbouring rows of the combined x
-      if (!grid_barrier(a.sync, ncta, a.spin_limit)) return;
+      __syncthreads();
     } else if (scaled) {
       // energy-optimal scaling of the guess: alpha = (x0.b) / (x0.A x0), A x0 = b - r0; the scaled start
       // alpha x0 never has a larger A-norm error than the zero start. The guess is kept only if it also
@@ -1159,7 +1200,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
         if (st[le].status != 0) continue;
         const int64_t row = (int64_t)s * kSlice + lane;
         double r[3];
-        true_residual(a, s, lane, r);
+        true_residual<kB64>(a, s, lane, r);
         double xb = 0.0, xr = 0.0, bb = 0.0, br = 0.0, rr = 0.0;
   #pragma unroll
         for (int k = 0; k < 3; ++k) {
@@ -1224,7 +1265,11 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
           r[k] = a.b[3 * row + k];
         }
       }
-      if (!a.zero_guess && (!scaled || two)) true_residual(a, s, lane, r);
+      if (!a.zero_guess && !scaled) true_residual<kB64>(a, s, lane, r);
+      if (two) {
+  #pragma unroll
+        for (int k = 0; k < 3; ++k) r[k] = a.r[3 * row + k];
+      }
       if (scaled && !two) {
         const double al = st[le].alpha;
   #pragma unroll
@@ -1411,7 +1456,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
         if (st[le].status != 0) continue;
         const int64_t row = (int64_t)s * kSlice + lane;
         double r[3];
-        true_residual(a, s, lane, r);
+        true_residual<kB64>(a, s, lane, r);
         const float4 zo = a.z[row];
         float z[3];
         prec_apply(a, row, r, z);
