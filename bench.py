@@ -7,8 +7,13 @@ by 5 moving capsules (penalty stiffness 1e4, activation distance 1 mm), backward
 Newton to rel 1e-6 with Jacobi-PCG at rel. residual 1e-6. A step is one backward-Euler step of every
 env of the batch. Inputs (matrix ~160 MB, tet data ~300 MB) exceed the 126 MB L2.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload cfg1|cfg0|cfg2]
-                  [--arms plain_fp64,fused_zero,learned]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload cfg1|cfg0|cfg2|cfg3|cfg4] [--arms plain_fp64,fused_zero,temporal,learned]
+
+`--workload cfg3` is the learned warm start's own protocol on the batched distribution: the MLP is trained
+on plain-solver episodes of 50 seeds (episodes of 16 uneven bodies, cells/axis U{8..40}, 5 capsules and a
+ground plane each; Adam, lr 1e-3), then each arm is timed on 20 held-out seeded episodes and the line
+aggregates them (env-steps over the summed timed seconds, CG iterations per step).
 
 Four solver arms on the same GPU and the same seeded workload, each a full Newton step:
   plain_fp64  the reference's CUDA PCG path restated (FP64 3x3 BSR with cuSPARSE bsrmv, cuBLAS vector
@@ -80,6 +85,10 @@ def build_workload(name: str, seed: int = 0):
     if name == "cfg4":
         return scenes.config4(seed), ("stiff heterogeneous body 96^3 cells (912,673 nodes, 5,308,416 tets), nu 0.49, "
                                       "E log-uniform [1e4,1e7] with 10 inclusions x100, 2 closing planes + 5 capsules")
+    if name == "cfg3":
+        n = int(os.environ.get("SDX_CFG3_ENVS", "16"))
+        return scenes.config2(seed, n_envs=n), (f"learned warm start on the batched distribution: an episode is {n} "
+                                                "uneven bodies, cells/axis U{8..40}, 5 capsules + plane each")
     if name == "cfg2":
         n = int(os.environ.get("SDX_CFG2_ENVS", "1024"))
         return scenes.config2(seed, n_envs=n), f"{n} uneven bodies, cells/axis U{{8..40}}, 5 capsules + plane each"
@@ -157,7 +166,7 @@ def cpu_oracle_sample(workload: str, seed: int = 0, steps: int = 1, warmup: int 
     v = np.zeros_like(u)
     prm = O.default_newton_params()
     prm.abs_tol = 1e-9  # same Newton stopping test as the GPU arm: rel 1e-6
-    if workload == "cfg2":
+    if workload in ("cfg2", "cfg3"):
         prm.max_iter = 12  # same Newton cap as the GPU arm
     t = 0.0
     for _ in range(warmup):
@@ -189,7 +198,7 @@ def newton_max_iter(args):
     oracle stalls at the same residuals), and would otherwise run every step to the cap."""
     if args.newton_max_iter:
         return args.newton_max_iter
-    return 12 if args.workload == "cfg2" else 50
+    return 12 if args.workload in ("cfg2", "cfg3") else 50
 
 
 def train_warm_start(args, local_rank):
@@ -199,11 +208,15 @@ def train_warm_start(args, local_rank):
     from project_superdex_b200.soft_body import SoftBodyWorld
     t0 = time.perf_counter()
     Xs, Ts = [], []
+    # the training set is capped at train_samples vertices, spread evenly over the episodes (cfg3's 50
+    # episodes take a few thousand vertices from each Newton solve; cfg1's two take the first 1 M each)
+    cap = max(4096, args.train_samples // args.train_episodes)
+    per_solve = 65536 if args.workload != "cfg3" else max(1024, min(65536, cap // (4 * args.train_steps)))
     for k in range(args.train_episodes):
         (bodies, cfg), _ = build_workload(args.workload, seed=args.seed + 1000 + k)
         tw = SoftBodyWorld(bodies, cfg, device=local_rank, newton_abs_tol=1e-9,
                            newton_max_iter=newton_max_iter(args))
-        X, T = collect(tw, args.train_steps, samples_per_solve=65536, capacity=1 << 20, seed=k)
+        X, T = collect(tw, args.train_steps, samples_per_solve=per_solve, capacity=cap, seed=k)
         Xs.append(X)
         Ts.append(T)
         if k < args.train_episodes - 1:
@@ -250,10 +263,32 @@ def time_arm(w, args, stream, local_rank, dist, world):
     # over the K timed steps: one PCG launch per Newton iteration (all envs together), and per launch the
     # iterations of its slowest env
     return {"value": world * n_envs * args.steps / (ms / 1000.0), "ms": ms, "prof": prof, "launches": launches,
-            "clocks": clk.summary(),
+            "clocks": clk.summary(), "env_steps": world * n_envs * args.steps, "steps": args.steps,
             "cg_iters_per_step": prof["pcg_iters"] / args.steps,
             "newton_iters_per_step": prof["pcg_launches"] / args.steps,
-            "last_step_cg_iters_mean_env": sum(s["cg_iters"] for s in stats) / max(1, n_envs)}
+            "last_step_cg_iters_mean_env": [sum(s["cg_iters"] for s in stats) / max(1, n_envs)]}
+
+
+def merge_runs(a, b):
+    """One arm timed on several episodes: sums of env-steps, time, launches and the solver profile."""
+    out = dict(b)
+    out["env_steps"] = a["env_steps"] + b["env_steps"]
+    out["steps"] = a["steps"] + b["steps"]
+    out["ms"] = a["ms"] + b["ms"]
+    out["launches"] = a["launches"] + b["launches"]
+    out["last_step_cg_iters_mean_env"] = a["last_step_cg_iters_mean_env"] + b["last_step_cg_iters_mean_env"]
+    out["value"] = out["env_steps"] / (out["ms"] / 1000.0)
+    out["prof"] = {k: (a["prof"].get(k, 0) + v if k != "pcg_threads" else v) for k, v in b["prof"].items()}
+    out["cg_iters_per_step"] = out["prof"]["pcg_iters"] / out["steps"]
+    out["newton_iters_per_step"] = out["prof"]["pcg_launches"] / out["steps"]
+    ca, cb = a["clocks"], b["clocks"]
+    sm = [x for x in (ca.get("sm_mhz"), cb.get("sm_mhz")) if x is not None]
+    out["clocks"] = {"sm_mhz": statistics.median(sm) if sm else None,
+                     "sm_max_mhz": max([x for x in (ca.get("sm_max_mhz"), cb.get("sm_max_mhz")) if x is not None],
+                                       default=None),
+                     "reasons": sorted(set(ca.get("reasons", [])) | set(cb.get("reasons", []))),
+                     "samples": ca.get("samples", 0) + cb.get("samples", 0)}
+    return out
 
 
 def run_ours(args, rank, world, local_rank):
@@ -271,23 +306,27 @@ def run_ours(args, rank, world, local_rank):
     params, train_info = (None, None)
     if "learned" in arms:
         params, train_info = train_warm_start(args, local_rank)
-    (bodies, cfg), desc = build_workload(args.workload, seed=args.seed)
+    # cfg3: every arm on each held-out episode (seeds args.seed.., training used args.seed + 1000..)
+    seeds = [args.seed + i for i in range(args.eval_episodes)] if args.workload == "cfg3" else [args.seed]
     results = {}
     w = None
-    for arm in arms:
-        if w is not None:
-            w.close()
-        # Newton to rel 1e-6 (the absolute floor is only a guard for an exactly zero residual)
-        w = SoftBodyWorld(bodies, cfg, device=local_rank, newton_abs_tol=1e-9,
-                          newton_max_iter=newton_max_iter(args))
-        if arm == "learned":
-            Mlp(w._ctx).set_params(params)
-        w.set_params(warm_start={"learned": capi.SDX_WARM_LEARNED, "temporal": capi.SDX_WARM_TEMPORAL}.get(
-                         arm, capi.SDX_WARM_ZERO),
-                     linear_solver_impl=(capi.SDX_SOLVER_PLAIN_FP64 if arm == "plain_fp64"
-                                         else capi.SDX_SOLVER_FUSED))
-        stream = torch.cuda.ExternalStream(w.stream_handle(), device=local_rank)
-        results[arm] = time_arm(w, args, stream, local_rank, dist, world)
+    for seed in seeds:
+        (bodies, cfg), desc = build_workload(args.workload, seed=seed)
+        for arm in arms:
+            if w is not None:
+                w.close()
+            # Newton to rel 1e-6 (the absolute floor is only a guard for an exactly zero residual)
+            w = SoftBodyWorld(bodies, cfg, device=local_rank, newton_abs_tol=1e-9,
+                              newton_max_iter=newton_max_iter(args))
+            if arm == "learned":
+                Mlp(w._ctx).set_params(params)
+            w.set_params(warm_start={"learned": capi.SDX_WARM_LEARNED, "temporal": capi.SDX_WARM_TEMPORAL}.get(
+                             arm, capi.SDX_WARM_ZERO),
+                         linear_solver_impl=(capi.SDX_SOLVER_PLAIN_FP64 if arm == "plain_fp64"
+                                             else capi.SDX_SOLVER_FUSED))
+            stream = torch.cuda.ExternalStream(w.stream_handle(), device=local_rank)
+            r = time_arm(w, args, stream, local_rank, dist, world)
+            results[arm] = merge_runs(results[arm], r) if arm in results else r
     head = results[arms[-1]]  # the headline arm is the last one (learned by default); w is its world
     n_envs = w.n_envs
     ms, prof = head["ms"], head["prof"]
@@ -339,9 +378,13 @@ def run_ours(args, rank, world, local_rank):
            "note": "the steps after the timed ones, continuing the trajectory",
            "cg_iters_per_step": eprof["pcg_iters"] / e2e_steps,
            "newton_iters_per_step": eprof["pcg_launches"] / e2e_steps}
-    arm_summary = {a: {"value": r["value"], "ms_per_step": r["ms"] / args.steps,
+    arm_summary = {a: {"value": r["value"], "ms_per_step": r["ms"] / r["steps"],
                        "cg_iters_per_step": r["cg_iters_per_step"],
-                       "newton_iters_per_step": r["newton_iters_per_step"]} for a, r in results.items()}
+                       "newton_iters_per_step": r["newton_iters_per_step"],
+                       # each env's own CG iterations in the last timed step (a launch runs until its
+                       # slowest env converges; cg_iters_per_step counts those launch-level iterations)
+                       "cg_iters_per_env_last_step": float(np.mean(r["last_step_cg_iters_mean_env"]))}
+                   for a, r in results.items()}
     for base in ("plain_fp64", "fused_zero", "temporal"):
         if base in results and "learned" in results:
             arm_summary[f"learned_over_{base}"] = results["learned"]["value"] / results[base]["value"]
@@ -352,7 +395,7 @@ def run_ours(args, rank, world, local_rank):
     clocks["reasons_all_arms"] = reasons
     line = {
         "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": ms / head["steps"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic (seeded tet grids, random materials and collider trajectories)",
         "config": {"workload": f"{args.workload}: {desc}", "n_envs": n_envs, "n_nodes": w.n_nodes,
@@ -363,7 +406,8 @@ def run_ours(args, rank, world, local_rank):
                    "newton_max_iter": newton_max_iter(args),
                    "l2": "inputs larger than L2 (matrix + tet data > 126 MB)",
                    "pcg_threads_autotuned": int(prof.get("pcg_threads", 0)),
-                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                   "episodes": len(seeds), "seeds": f"{seeds[0]}..{seeds[-1]}"},
         "arms": arm_summary, "training": train_info,
         "roofline": roofline, "spmv": spmv, "e2e": e2e, "gpu_launches": head["launches"],
         "clocks": clocks,
@@ -383,19 +427,33 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg4"])
-    ap.add_argument("--arms", default="plain_fp64,fused_zero,temporal,learned",
+    ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4"])
+    ap.add_argument("--arms", default=None,
                     help="comma list of solver arms to time, headline last: plain_fp64 (the reference's CUDA "
                          "PCG path restated: FP64 BSR, cuSPARSE/cuBLAS, zero start), fused_zero (this "
                          "library's PCG, zero start), temporal (start from the previous step's update at the "
-                         "same Newton iteration), learned (temporal guess + learned correction, Galerkin)")
-    ap.add_argument("--train-episodes", type=int, default=2, dest="train_episodes")
-    ap.add_argument("--train-steps", type=int, default=8, dest="train_steps")
+                         "same Newton iteration), learned (temporal guess + learned correction, Galerkin); "
+                         "default plain_fp64,fused_zero,temporal,learned (cfg3: fused_zero,temporal,learned)")
+    ap.add_argument("--train-episodes", type=int, default=None, dest="train_episodes",
+                    help="plain-solver training episodes (default 2; cfg3: 50)")
+    ap.add_argument("--train-steps", type=int, default=None, dest="train_steps",
+                    help="steps per training episode (default 8; cfg3: 2)")
     ap.add_argument("--train-epochs", type=int, default=8, dest="train_epochs")
+    ap.add_argument("--train-samples", type=int, default=1 << 21, dest="train_samples",
+                    help="training vertices kept over all episodes")
+    ap.add_argument("--eval-episodes", type=int, default=20, dest="eval_episodes",
+                    help="cfg3: held-out episodes each arm is timed on")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--newton-max-iter", type=int, default=0, dest="newton_max_iter")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    cfg3 = args.workload == "cfg3"
+    if args.arms is None:
+        args.arms = "fused_zero,temporal,learned" if cfg3 else "plain_fp64,fused_zero,temporal,learned"
+    if args.train_episodes is None:
+        args.train_episodes = 50 if cfg3 else 2
+    if args.train_steps is None:
+        args.train_steps = 2 if cfg3 else 8
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
