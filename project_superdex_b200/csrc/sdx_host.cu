@@ -91,6 +91,7 @@ static int upload(T** d, const std::vector<T>& h) {
 
 struct PcgPartition {
   int n_cta = 0, threads = 0;
+  int max_envs = kPcgMaxEnvsPerCta;  // the most envs one CTA covers
   int* cta_slice = nullptr;   // CTA c covers entries [cta_slice[c], cta_slice[c+1]) of the slice list
   int* slice_list = nullptr;  // slice ids in ascending order (NULL: every slice, entry i = slice i)
   int* cta_eoff = nullptr;    // CTA c's envs are cta_envs[cta_eoff[c] .. cta_eoff[c+1])
@@ -643,6 +644,8 @@ static int choose_partition(sdx_context* c, int n_slices, const std::vector<int>
     }
     eoff[k + 1] = (int)envs.size();
   }
+  P.max_envs = 1;
+  for (int k = 0; k < n_cta; ++k) P.max_envs = std::max(P.max_envs, eoff[k + 1] - eoff[k]);
   for (int ev = 0; ev < n_envs; ++ev)
     if (ec0[ev] < 0) {
       ec0[ev] = 0;
@@ -800,6 +803,7 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
     a.env_poff = part->env_poff;
     a.part = part->part;
     a.repart_rows = target;
+    a.wstride = part->max_envs;
     a.cta_ns = (c->profiling && c->cta_timers && part->n_cta <= c->cta_ns_n) ? c->cta_ns : nullptr;
     cudaError_t e = launch_pcg(a, part->n_cta, part->threads, c->stream);
     c->launches++;

@@ -162,6 +162,10 @@ struct PcgArgs {
   // per-CTA phase timing (NULL: off), SM clock cycles accumulated over the launch's iterations:
   // [4 c + 0] SpMV phase, [4 c + 1] wait at the barrier after it, [4 c + 2] update phase, [4 c + 3] wait
   unsigned long long* cta_ns;
+  // slots per warp in the shared partial sums: the most envs any CTA of the partition covers (0: the
+  // maximum, kPcgMaxEnvsPerCta). A single-env partition keeps 1 slot, so the CTA's shared memory stays
+  // small and the L1 share of the SM's unified memory, which the SpMV's z gathers use, stays large.
+  int wstride;
 };
 
 
@@ -190,7 +194,7 @@ void launch_spmv(const Matrix& A, const float4* x, float* y, int threads, cudaSt
 void launch_bsr_to_sell(int n_rows, const int64_t* row_ptr, const int32_t* bcol, const float* bval,
                         const int* slice_ptr, int* col, float* val, int* diag_pos, cudaStream_t st);
 void launch_pack_z(int64_t n_rows, const double* x, float4* z, cudaStream_t st);
-int pcg_shared_bytes(int threads);
+int pcg_shared_bytes(int threads, int wstride = kPcgMaxEnvsPerCta);
 int pcg_max_ctas_per_sm(int threads);
 
 }  // namespace sdx

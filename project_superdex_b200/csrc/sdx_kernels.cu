@@ -799,7 +799,6 @@ void launch_bsr_to_sell(int n_rows, const int64_t* row_ptr, const int32_t* bcol,
 // per (CTA, env) it covers and every CTA that needs an env's total sums that env's partials in a fixed
 // order, so all CTAs hold bit-identical alpha / beta / status for their envs.
 
-int pcg_shared_bytes(int threads);
 
 struct EnvState {
   double rz, alpha, beta, conv_thr, div_thr, bb;
@@ -953,7 +952,7 @@ __device__ __forceinline__ void true_residual(const PcgArgs& a, int s, int lane,
 // default variant's code is exactly the untimed one)
 template <bool kPipe, bool kTimed>
 __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
-  extern __shared__ double wacc[];  // [nwarps][kPcgMaxEnvsPerCta][kPcgNq]
+  extern __shared__ double wacc[];  // [nwarps][a.wstride][kPcgNq]
   __shared__ EnvState st[kPcgMaxEnvsPerCta];
   constexpr int kB64 = kPipe ? 4 : 2;  // groups per batch of the FP64 SpMVs (register budget of the variant)
   __shared__ double tot[kPcgMaxEnvsPerCta][kPcgNq];
@@ -981,17 +980,18 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     return lo;
   };
 
+  const int ws = a.wstride;
   auto clear_acc = [&]() {  // the slots of this CTA's envs only
     const int per_warp = ne * kPcgNq;
     for (int i = threadIdx.x; i < nwarps * per_warp; i += blockDim.x) {
       const int w = i / per_warp, j = i - w * per_warp;
-      wacc[w * kPcgMaxEnvsPerCta * kPcgNq + j] = 0.0;
+      wacc[w * ws * kPcgNq + j] = 0.0;
     }
     __syncthreads();
   };
   auto add_acc = [&](int le, int k, double v) {
     v = warp_sum(v);
-    if (lane == 0) wacc[(warp * kPcgMaxEnvsPerCta + le) * kPcgNq + k] += v;
+    if (lane == 0) wacc[(warp * ws + le) * kPcgNq + k] += v;
   };
   // Partials of phase 1 live in buffer 1, those of phases 0 and 2 in buffer 0, so a CTA writing the
   // next phase's partials never overwrites values another CTA is still reducing. The partials of one
@@ -1002,7 +1002,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     for (int i = threadIdx.x; i < ne * nq; i += blockDim.x) {
       const int le = i / nq, k = i % nq;
       double v = 0.0;
-      for (int w = 0; w < nwarps; ++w) v += wacc[(w * kPcgMaxEnvsPerCta + le) * kPcgNq + k];
+      for (int w = 0; w < nwarps; ++w) v += wacc[(w * ws + le) * kPcgNq + k];
       const int e = s_env[le];
       a.part[buf * pstride + (size_t)(a.env_poff[e] + (c - a.env_cta0[e])) * kPcgNq + k] = v;
     }
@@ -1558,17 +1558,18 @@ int pcg_max_ctas_per_sm(int threads) {
   return e == cudaSuccess ? n : 0;
 }
 
-int pcg_shared_bytes(int threads) { return (threads / 32) * kPcgMaxEnvsPerCta * kPcgNq * (int)sizeof(double); }
+int pcg_shared_bytes(int threads, int wstride) { return (threads / 32) * wstride * kPcgNq * (int)sizeof(double); }
 
 cudaError_t launch_pcg(const PcgArgs& a, int n_cta, int threads, cudaStream_t st) {
   PcgArgs args = a;
+  args.wstride = (a.wstride > 0 && a.wstride < kPcgMaxEnvsPerCta) ? a.wstride : kPcgMaxEnvsPerCta;
   void* params[] = {&args};
   const bool timed = a.cta_ns != nullptr;
   const void* fn = pcg_pipelined(threads)
                        ? (timed ? (const void*)k_pcg<true, true> : (const void*)k_pcg<true, false>)
                        : (timed ? (const void*)k_pcg<false, true> : (const void*)k_pcg<false, false>);
   return cudaLaunchCooperativeKernel(fn, dim3(n_cta), dim3(threads), params,
-                                     (size_t)pcg_shared_bytes(threads), st);
+                                     (size_t)pcg_shared_bytes(threads, args.wstride), st);
 }
 
 }  // namespace sdx
