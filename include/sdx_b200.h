@@ -336,10 +336,18 @@ typedef struct {
   int64_t pcg_threads;      /* threads per CTA of the PCG launch shape in use (autotuned or default) */
   double warm_ms;           /* learned warm start: features, MLP inference and the start-vector kernel */
   int64_t warm_launches;
+  int64_t pcg_cluster_solves; /* PCG solves that ran on the cluster kernel (a batch of small envs, one
+                                 thread-block cluster per env at a time) instead of the grid kernel */
 } sdx_profile;
 /* enable: 0 off, 1 per-kernel event timing, 2 also the per-CTA PCG phase timers (sdx_get_pcg_cta_profile) */
 int sdx_set_profiling(sdx_context* ctx, int enable);
 int sdx_get_profile(sdx_context* ctx, sdx_profile* out);
+
+/* Launch shape the cluster PCG uses on the current device for a queue of n_envs envs: how many
+   thread-block clusters of how many CTAs (one 512-thread CTA per SM). No reference counterpart (the
+   reference solves one env at a time). SDX_ERR_UNSUPPORTED when no cluster shape fits; batches then stay
+   on the grid kernel. */
+int sdx_pcg_cluster_shape(int n_envs, int* n_clusters, int* cluster_size);
 /* Per-CTA phase times of the persistent PCG (no reference counterpart), recorded while profiling at level 2
  * (sdx_set_profiling(ctx, 2)): 4 values per CTA, SM clock cycles summed since then: SpMV phase, wait at the
  * barrier after it, update phase, wait at the barrier after it. */

@@ -35,6 +35,7 @@ EXPORTED = [
     "sdx_collect_training", "sdx_get_training_data", "sdx_write_state_masked", "sdx_capture_state",
     "sdx_restore_state", "sdx_release_state", "sdx_release_all_states", "sdx_is_equal_state",
     "sdx_capture_state_to_bytes", "sdx_restore_state_from_bytes", "sdx_get_pcg_cta_profile",
+    "sdx_pcg_cluster_shape",
 ]
 SDX_MLP_PARAMS = 37264
 SDX_NOALLOC_MAX_BLOCK_ROWS = 65536
@@ -85,7 +86,7 @@ class Profile(C.Structure):
                 ("contact_ms", C.c_double), ("contact_launches", C.c_int64),
                 ("seed_ms", C.c_double), ("seed_launches", C.c_int64), ("pcg_bytes", C.c_double),
                 ("pcg_relaunches", C.c_int64), ("pcg_threads", C.c_int64), ("warm_ms", C.c_double),
-                ("warm_launches", C.c_int64)]
+                ("warm_launches", C.c_int64), ("pcg_cluster_solves", C.c_int64)]
 
 
 _dp = C.POINTER(C.c_double)
@@ -149,6 +150,7 @@ def lib():
     L.sdx_get_stream.argtypes = [_vp, C.POINTER(C.c_void_p)]
     L.sdx_set_profiling.argtypes = [_vp, C.c_int]
     L.sdx_get_profile.argtypes = [_vp, C.POINTER(Profile)]
+    L.sdx_pcg_cluster_shape.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     _fp_ = C.POINTER(C.c_float)
     L.sdx_mlp_init.argtypes = [_vp, C.c_uint64]
     L.sdx_mlp_set_params.argtypes = [_vp, _fp_, C.c_int]
@@ -183,3 +185,11 @@ def default_linear_params() -> LinearParams:
     p = LinearParams()
     lib().sdx_default_linear_params(C.byref(p))
     return p
+
+
+def pcg_cluster_shape(n_envs: int):
+    """(clusters, CTAs per cluster) the cluster PCG uses for a queue of n_envs envs on the current device;
+    raises SdxError when no cluster shape fits."""
+    n, size = C.c_int(), C.c_int()
+    check(lib().sdx_pcg_cluster_shape(int(n_envs), C.byref(n), C.byref(size)))
+    return n.value, size.value

@@ -257,6 +257,8 @@ struct sdx_context {
   bool hist_valid[kHist] = {false, false, false, false};
   int pcg_threads = 0;         // threads per CTA of the context's PCG partition
   int* env_nrows = nullptr;    // padded rows per env (device)
+  int* env_soff = nullptr;     // per env, its first slice (device, n_envs + 1): the cluster PCG's env ranges
+  int* cl_envs = nullptr;      // the cluster PCG's env queue (device, n_envs)
   std::unique_ptr<PlainSolver> plain;  // the plain FP64 comparison solver, built on first use
   // state snapshots (device-resident), keyed by handle
   std::map<uint64_t, Snapshot> snaps;
@@ -348,6 +350,8 @@ static void release_topology(sdx_context* c) {
   c->plain.reset();
   c->part_dyn.release();
   dfree(c->env_nrows);
+  dfree(c->env_soff);
+  dfree(c->cl_envs);
   dfree(c->dx_hist);
   for (bool& h : c->hist_valid) h = false;
   dfree(c->slice_ptr);
@@ -780,6 +784,69 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
   SDX_CUDA(cudaMemsetAsync(W.out_conv, 0, sizeof(int) * n_envs, c->stream));
   cudaEvent_t ev;
   prof_begin(c, &ev);
+  auto finish = [&]() -> int {
+    prof_end(c, PROF_PCG, ev);
+    if (c->profiling) {
+      std::vector<int> its(n_envs);
+      SDX_CUDA(cudaMemcpy(its.data(), W.out_iters, sizeof(int) * n_envs, cudaMemcpyDeviceToHost));
+      for (int e = 0; e < n_envs; ++e)
+        if (h_mask && !h_mask[e]) its[e] = 0;  // the envs this solve was asked for
+      c->prof.pcg_iters += *std::max_element(its.begin(), its.end());
+      c->prof.pcg_launches++;
+      if (A.val == c->val && (int)c->h_env_pcg_bytes.size() == n_envs)
+        for (int e = 0; e < n_envs; ++e) c->prof.pcg_bytes += its[e] * c->h_env_pcg_bytes[e];
+    }
+    return SDX_OK;
+  };
+  // Batches of small envs go to the cluster PCG (one thread-block cluster per env at a time, envs taken
+  // largest first from a queue, no grid-wide lockstep) when every active env has at most kClusterMaxRows
+  // rows and either the queue is long (at least kClusterQueueFactor envs per co-resident cluster, so the
+  // clusters stay busy until the last few envs) or only a few latency-bound envs are left (at most
+  // kClusterTailEnvs envs of at most kClusterLatencyRows rows). Not for the two-vector (learned) start.
+  // SDX_PCG_CLUSTER=0 keeps every solve on the grid kernel; SDX_PCG_CLUSTER_QUEUE and
+  // SDX_PCG_CLUSTER_TAIL override the two thresholds.
+  if (batch && !x2) {
+    const char* ce = getenv("SDX_PCG_CLUSTER");
+    std::vector<int> list;
+    int64_t max_rows = 0;
+    for (int e = 0; e < n_envs; ++e)
+      if (!h_mask || h_mask[e]) {
+        list.push_back(e);
+        max_rows = std::max<int64_t>(max_rows, c->h_row_off[e + 1] - c->h_row_off[e]);
+      }
+    const ClusterShape shape = (ce && atoi(ce) == 0) ? ClusterShape{0, 0, 0} : pcg_cluster_shape((int)list.size());
+    const char* qf = getenv("SDX_PCG_CLUSTER_QUEUE");
+    const char* tl = getenv("SDX_PCG_CLUSTER_TAIL");
+    const int queue_factor = qf ? atoi(qf) : kClusterQueueFactor, tail_envs = tl ? atoi(tl) : kClusterTailEnvs;
+    const int n_list = (int)list.size();
+    const bool long_queue = queue_factor > 0 && n_list >= queue_factor * shape.n_clusters;
+    const bool tail = n_list <= tail_envs && max_rows <= kClusterLatencyRows;
+    if (shape.n_clusters > 0 && n_list > 0 && max_rows <= kClusterMaxRows && (long_queue || tail)) {
+      std::stable_sort(list.begin(), list.end(), [&](int x, int y) {
+        return c->h_row_off[x + 1] - c->h_row_off[x] > c->h_row_off[y + 1] - c->h_row_off[y];
+      });
+      if (!c->env_soff) {
+        std::vector<int> so(n_envs + 1);
+        for (int e = 0; e <= n_envs; ++e) so[e] = (int)(c->h_row_off[e] / kSlice);
+        SDX_TRY(upload(&c->env_soff, so));
+        SDX_TRY(dalloc(&c->cl_envs, n_envs));
+      }
+      SDX_CUDA(cudaMemcpyAsync(c->cl_envs, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice,
+                               c->stream));
+      a.cl_envs = c->cl_envs;
+      a.cl_n = (int)list.size();
+      a.env_soff = c->env_soff;
+      cudaError_t e = launch_pcg_cluster(a, shape, c->stream);
+      c->launches++;
+      if (e != cudaSuccess) return set_error(SDX_ERR_CUDA, "PCG cluster launch: %s", cudaGetErrorString(e));
+      unsigned flags[8];
+      SDX_CUDA(cudaMemcpyAsync(flags, W.sync, sizeof(flags), cudaMemcpyDeviceToHost, c->stream));
+      SDX_CUDA(cudaStreamSynchronize(c->stream));
+      if (flags[2] != 0u) return set_error(SDX_ERR_DEVICE_TIMEOUT, "PCG cluster barrier timed out");
+      if (c->profiling) c->prof.pcg_cluster_solves++;
+      return finish();
+    }
+  }
   PcgPartition* part = &P;
   if (batch && h_mask && rows < (c->h_row_off[n_envs] * 3) / 4) {
     // most envs are already converged (later Newton iterations): partition just the envs in the mask
@@ -831,16 +898,7 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
     SDX_CUDA(cudaMemcpyAsync(W.sync, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, c->stream));
     SDX_CUDA(cudaMemcpyAsync(W.sync + 7, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, c->stream));
   }
-  prof_end(c, PROF_PCG, ev);
-  if (c->profiling) {
-    std::vector<int> its(n_envs);
-    SDX_CUDA(cudaMemcpy(its.data(), W.out_iters, sizeof(int) * n_envs, cudaMemcpyDeviceToHost));
-    c->prof.pcg_iters += *std::max_element(its.begin(), its.end());
-    c->prof.pcg_launches++;
-    if (A.val == c->val && (int)c->h_env_pcg_bytes.size() == n_envs)
-      for (int e = 0; e < n_envs; ++e) c->prof.pcg_bytes += its[e] * c->h_env_pcg_bytes[e];
-  }
-  return SDX_OK;
+  return finish();
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -970,6 +1028,19 @@ extern "C" int sdx_get_pcg_cta_profile(sdx_context* c, int n_cta, double* out) {
                            c->stream));
   SDX_CUDA(cudaStreamSynchronize(c->stream));
   for (size_t i = 0; i < h.size(); ++i) out[i] = (double)h[i];
+  return SDX_OK;
+}
+
+extern "C" int sdx_pcg_cluster_shape(int n_envs, int* n_clusters, int* cluster_size) {
+  if (!n_clusters || !cluster_size || n_envs <= 0) return set_error(SDX_ERR_INVALID_ARGUMENT, "null or empty argument");
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return set_error(SDX_ERR_CUDA, "no CUDA device");
+  const ClusterShape s = pcg_cluster_shape(n_envs);
+  *n_clusters = s.n_clusters;
+  *cluster_size = s.size;
+  if (s.n_clusters == 0)
+    return set_error(SDX_ERR_UNSUPPORTED, "no cluster shape fits (last occupancy query: %s)",
+                     cudaGetErrorString((cudaError_t)s.last_error));
   return SDX_OK;
 }
 

@@ -22,6 +22,13 @@ namespace sdx {
 constexpr int kSlice = 32;
 constexpr int kPadBit = 0x80000000;
 constexpr int kPcgMaxEnvsPerCta = 32;
+// cluster PCG: the largest env it takes (rows); the queue length, in envs per co-resident cluster, from
+// which it runs a whole batch; the envs (at most kClusterTailEnvs, each at most kClusterLatencyRows rows)
+// it takes at the end of a batch's Newton iterations, where the grid kernel is latency bound
+constexpr int64_t kClusterMaxRows = 131072;
+constexpr int kClusterQueueFactor = 4;
+constexpr int kClusterTailEnvs = 4;
+constexpr int64_t kClusterLatencyRows = 32768;
 constexpr int kPcgNq = 11;  // partial sums per (CTA, env) and phase (11: the two-vector start)
 
 __host__ __device__ __forceinline__ size_t val_index(int64_t p, int e) {
@@ -166,6 +173,16 @@ struct PcgArgs {
   // maximum, kPcgMaxEnvsPerCta). A single-env partition keeps 1 slot, so the CTA's shared memory stays
   // small and the L1 share of the SM's unified memory, which the SpMV's z gathers use, stays large.
   int wstride;
+  // cluster PCG (k_pcg_cluster): the envs to solve, largest first (taken in order through sync[1]), and
+  // each env's slice range [env_soff[e], env_soff[e + 1])
+  const int* cl_envs;
+  int cl_n;
+  const int* env_soff;
+};
+
+struct ClusterShape {
+  int n_clusters, size;
+  int last_error;  // cudaError_t of the last failed occupancy query (0: none)
 };
 
 
@@ -190,6 +207,8 @@ void launch_copy_rows(int n_slices, const int* slice_env, const uint8_t* env_mas
 void launch_velocity(int64_t n3, const double* u, const double* u0, double dt, double* v,
                      cudaStream_t st);
 cudaError_t launch_pcg(const PcgArgs& a, int n_cta, int threads, cudaStream_t st);
+ClusterShape pcg_cluster_shape(int n_envs);
+cudaError_t launch_pcg_cluster(const PcgArgs& a, ClusterShape shape, cudaStream_t st);
 void launch_spmv(const Matrix& A, const float4* x, float* y, int threads, cudaStream_t st);
 void launch_bsr_to_sell(int n_rows, const int64_t* row_ptr, const int32_t* bcol, const float* bval,
                         const int* slice_ptr, int* col, float* val, int* diag_pos, cudaStream_t st);

@@ -8,6 +8,7 @@
 // (fem_traction.h:58-178). The linear solve is the reference's left-preconditioned CG with the
 // residual-L2 stop test (mochi_core/include/mochi_core/linear_algebra/krylov/pcg.h:70-238), fused
 // into one persistent cooperative launch per solve.
+#include <array>
 #include <cooperative_groups.h>
 
 #include "sdx_device.cuh"
@@ -1537,6 +1538,378 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
   }
 }
 
+// ------------------------------------------------------------------------------------------------
+// Cluster PCG for batches of small envs. The grid kernel above iterates every env of a batch in lockstep
+// with grid-wide barriers, so once most envs have converged each iteration costs the grid barrier's
+// latency (~11 us) for a few thousand rows. Here a thread-block cluster solves one env at a time and
+// takes the next env from a queue (largest first) when it finishes: the clusters never wait on each other,
+// and the reductions and barriers inside a cluster go through distributed shared memory (a counter in
+// CTA 0's shared memory, polled with cluster-scope acquire loads; partial sums read from every CTA's
+// shared memory in rank order, so every CTA holds bit-identical scalars and takes the same branches).
+// Same recurrence, stop tests, FP64 residual replacement and verification iteration as k_pcg, per env.
+// Every wait is bounded: a timeout records the error word and the kernel unwinds to its final cluster
+// barrier, which every CTA reaches exactly once.
+
+constexpr int kClNq = 5;
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_size() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+// address of this CTA's shared variable p in the shared memory of cluster CTA `rank`
+__device__ __forceinline__ uint32_t cluster_map(const void* p, uint32_t rank) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;"
+               : "=r"(r)
+               : "r"((uint32_t)__cvta_generic_to_shared(p)), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ double cluster_ld_f64(uint32_t addr) {
+  double v;
+  asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(addr) : "memory");
+  return v;
+}
+__device__ __forceinline__ int cluster_ld_s32(uint32_t addr) {
+  int v;
+  asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(v) : "r"(addr) : "memory");
+  return v;
+}
+__device__ __forceinline__ void cluster_hw_sync() {
+  asm volatile("barrier.cluster.arrive.aligned;\n\tbarrier.cluster.wait.aligned;" ::: "memory");
+}
+
+// Software cluster barrier (every thread of every CTA calls it): arrivals counted on CTA 0's shared
+// counter with a cluster-scope release, the poll acquires. false when the wait gave up (error recorded).
+__device__ __forceinline__ bool cluster_sync(uint32_t cnt, unsigned n, long long limit, unsigned* err, int* s_ok) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned prev;
+    asm volatile("atom.release.cluster.shared::cluster.add.u32 %0, [%1], 1;" : "=r"(prev) : "r"(cnt) : "memory");
+    const unsigned target = (prev / n + 1u) * n;
+    long long spins = 0;
+    int ok = 1;
+    for (;;) {
+      unsigned v;
+      asm volatile("ld.acquire.cluster.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(cnt) : "memory");
+      if ((int)(v - target) >= 0) break;
+      if (++spins > limit) {
+        atomicExch(err, 1u);
+        ok = 0;
+        break;
+      }
+    }
+    *s_ok = ok;
+  }
+  __syncthreads();
+  return *s_ok != 0;
+}
+
+__global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
+  __shared__ double wq[16][kClNq];     // per-warp partial sums
+  __shared__ double s_part[2][kClNq];  // this CTA's partials, two buffers (consecutive reductions)
+  __shared__ double s_tot[kClNq];
+  __shared__ unsigned s_cnt;           // the cluster barrier counter (used in CTA 0)
+  __shared__ int s_env, s_ok;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const uint32_t rank = cluster_rank(), csize = cluster_size();
+  if (threadIdx.x == 0) s_cnt = 0u;
+  cluster_hw_sync();  // every CTA's shared memory is live before any remote access
+  const uint32_t cnt = cluster_map(&s_cnt, 0);
+  const uint32_t env0 = cluster_map(&s_env, 0);
+  unsigned* const err = a.sync + 2;
+  int rb = 0;  // partial buffer of the next reduction (the same sequence in every CTA)
+  bool fail = false;
+
+  auto acc_reset = [&]() {
+    for (int i = threadIdx.x; i < nwarps * kClNq; i += blockDim.x) (&wq[0][0])[i] = 0.0;
+    __syncthreads();
+  };
+  auto acc_add = [&](int k, double v) {
+    v = warp_sum(v);
+    if (lane == 0) wq[warp][k] += v;
+  };
+  // publish this CTA's partials, synchronise the cluster, sum all CTAs' partials in rank order
+  auto reduce = [&](int nq) {
+    __syncthreads();
+    if (threadIdx.x < nq) {
+      double v = 0.0;
+      for (int w = 0; w < nwarps; ++w) v += wq[w][threadIdx.x];
+      s_part[rb][threadIdx.x] = v;
+    }
+    if (!cluster_sync(cnt, csize, a.spin_limit, err, &s_ok)) return false;
+    if (threadIdx.x < nq) {
+      double v = 0.0;
+      for (uint32_t r = 0; r < csize; ++r) v += cluster_ld_f64(cluster_map(&s_part[rb][threadIdx.x], r));
+      s_tot[threadIdx.x] = v;
+    }
+    rb ^= 1;
+    __syncthreads();
+    return true;
+  };
+
+  for (;;) {
+    // ---- next env from the queue (CTA 0 takes it, every CTA reads it from CTA 0) ----
+    if (rank == 0 && threadIdx.x == 0) {
+      const int h = (int)atomicAdd(a.sync + 1, 1u);
+      s_env = h < a.cl_n ? a.cl_envs[h] : -1;
+    }
+    if (!cluster_sync(cnt, csize, a.spin_limit, err, &s_ok)) break;
+    const int e = cluster_ld_s32(env0);
+    if (e < 0) break;
+    const int sa = a.env_soff[e], ns = a.env_soff[e + 1] - sa;
+    const int c0 = sa + (int)((int64_t)ns * rank / csize), c1 = sa + (int)((int64_t)ns * (rank + 1) / csize);
+
+    // ---- phase 0: diagonal, start vector, r0, z0 ----
+    const bool scaled = !a.zero_guess && a.scale_guess;
+    double al0 = 0.0;
+    if (scaled) {
+      acc_reset();
+      for (int s = c0 + warp; s < c1; s += nwarps) {
+        const int64_t row = (int64_t)s * kSlice + lane;
+        double r[3];
+        true_residual<4>(a, s, lane, r);
+        double xb = 0.0, xr = 0.0, bb = 0.0, br = 0.0, rr = 0.0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          a.r[3 * row + k] = r[k];
+          const double xk = a.x[3 * row + k], bk = a.b[3 * row + k];
+          xb += xk * bk;
+          xr += xk * r[k];
+          bb += bk * bk;
+          br += bk * r[k];
+          rr += r[k] * r[k];
+        }
+        acc_add(0, bb);
+        acc_add(1, xb);
+        acc_add(2, xr);
+        acc_add(3, br);
+        acc_add(4, rr);
+      }
+      if (!reduce(5)) {
+        fail = true;
+        break;
+      }
+      const double bb = s_tot[0], xb = s_tot[1], xax = s_tot[1] - s_tot[2];
+      al0 = (xax > 0.0 && xb > 0.0 && isfinite(xb / xax)) ? xb / xax : 0.0;
+      const double ra = (1.0 - al0) * (1.0 - al0) * bb + 2.0 * al0 * (1.0 - al0) * s_tot[3] + al0 * al0 * s_tot[4];
+      if (!(ra < bb)) al0 = 0.0;
+    }
+    acc_reset();
+    for (int s = c0 + warp; s < c1; s += nwarps) {
+      const int64_t row = (int64_t)s * kSlice + lane;
+      const int dp = a.diag_pos[row];
+      if (a.precond == 1) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const float d = dp >= 0 ? a.A.val[val_index(dp, 4 * k)] : 0.0f;
+          a.dinv[3 * row + k] = d != 0.0f ? 1.0f / d : 0.0f;
+        }
+      } else if (a.precond == 2) {
+        float B[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) B[q] = dp >= 0 ? a.A.val[val_index(dp, q)] : 0.0f;
+        float cof[9];
+        cof3(B, cof);
+        const float det = det3(B);
+        const float inv = det != 0.0f ? 1.0f / det : 0.0f;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) a.dinv[9 * row + 3 * i + j] = cof[3 * j + i] * inv;
+      }
+      double r[3];
+      if (a.zero_guess) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          a.x[3 * row + k] = 0.0;
+          r[k] = a.b[3 * row + k];
+        }
+      } else if (scaled) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          a.x[3 * row + k] *= al0;
+          r[k] = (1.0 - al0) * a.b[3 * row + k] + al0 * a.r[3 * row + k];
+        }
+      } else {
+        true_residual<4>(a, s, lane, r);
+      }
+      float z[3];
+      prec_apply(a, row, r, z);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) a.r[3 * row + k] = r[k];
+      a.z[row] = make_float4(z[0], z[1], z[2], 0.0f);
+      const double b0 = a.b[3 * row], b1 = a.b[3 * row + 1], b2 = a.b[3 * row + 2];
+      acc_add(0, b0 * b0 + b1 * b1 + b2 * b2);
+      acc_add(1, r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+      acc_add(2, r[0] * z[0] + r[1] * z[1] + r[2] * z[2]);
+    }
+    if (!reduce(3)) {
+      fail = true;
+      break;
+    }
+    const double bb = s_tot[0];
+    const double rt = a.env_rel_tol ? a.env_rel_tol[e] : a.rel_tol;
+    const double conv_thr = fmax(a.abs_tol * a.abs_tol, (bb * rt) * rt);
+    const double div_thr = (bb * a.rel_div_tol) * a.rel_div_tol;
+    double rz = s_tot[2], rr = s_tot[1], beta = 0.0;
+    int status = 0, it_done = 0, verify_it = 0;
+    bool first = true;
+    if (!isfinite(rr) || rr > div_thr)
+      status = 3;
+    else if (rr <= conv_thr)
+      status = 1;
+
+    // ---- iterations ----
+    for (int it = 1; status == 0; ++it) {
+      // phase 1: p = z + beta p, q = A z + beta q, p.q
+      acc_reset();
+      for (int s = c0 + warp; s < c1; s += nwarps) {
+        const int64_t row = (int64_t)s * kSlice + lane;
+        const float4 zr = a.z[row];
+        float po[3] = {0.0f, 0.0f, 0.0f}, qo[3] = {0.0f, 0.0f, 0.0f};
+        if (!first) {
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            po[k] = a.p[3 * row + k];
+            qo[k] = a.q[3 * row + k];
+          }
+        }
+        float a0, a1, a2;
+        sell_row_product_pipe(a.A, s, lane, [&](int j) { return a.z[j]; }, a0, a1, a2);
+        const float fb = first ? 0.0f : (float)beta;
+        float pn[3], qn[3];
+        pn[0] = fmaf(fb, po[0], zr.x);
+        pn[1] = fmaf(fb, po[1], zr.y);
+        pn[2] = fmaf(fb, po[2], zr.z);
+        qn[0] = fmaf(fb, qo[0], a0);
+        qn[1] = fmaf(fb, qo[1], a1);
+        qn[2] = fmaf(fb, qo[2], a2);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          a.p[3 * row + k] = pn[k];
+          a.q[3 * row + k] = qn[k];
+        }
+        acc_add(0, (double)pn[0] * qn[0] + (double)pn[1] * qn[1] + (double)pn[2] * qn[2]);
+      }
+      if (!reduce(1)) {
+        fail = true;
+        break;
+      }
+      const double pq = s_tot[0];
+      const double al = rz / pq;
+      if (pq <= 0.0 && a.abort_spd) {  // non-SPD abort (pcg.h:152-169): x keeps the previous iterate
+        it_done = it;
+        status = 3;
+        rr = 0.0;
+        break;
+      }
+      const bool replace = (verify_it > 0 && verify_it == it - 1) || (a.replace_every > 0 && it % a.replace_every == 0);
+      // phase 2: x += alpha p, r -= alpha q, z = M^-1 r, r.r, r.z_old, r.z
+      acc_reset();
+      for (int s = c0 + warp; s < c1; s += nwarps) {
+        const int64_t row = (int64_t)s * kSlice + lane;
+        double xo[3], ro[3];
+        float pp[3], qq[3], dd[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          xo[k] = a.x[3 * row + k];
+          pp[k] = a.p[3 * row + k];
+          ro[k] = a.r[3 * row + k];
+          qq[k] = a.q[3 * row + k];
+          dd[k] = (!replace && a.precond == 1) ? a.dinv[3 * row + k] : 1.0f;
+        }
+        const float4 zo = replace ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : a.z[row];
+        double r[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          a.x[3 * row + k] = xo[k] + al * (double)pp[k];
+          r[k] = ro[k] - al * (double)qq[k];
+        }
+        if (replace) continue;
+        float z[3];
+        if (a.precond == 1) {
+#pragma unroll
+          for (int k = 0; k < 3; ++k) z[k] = (float)(dd[k] * r[k]);
+        } else {
+          prec_apply(a, row, r, z);
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) a.r[3 * row + k] = r[k];
+        a.z[row] = make_float4(z[0], z[1], z[2], 0.0f);
+        acc_add(0, r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+        acc_add(1, r[0] * zo.x + r[1] * zo.y + r[2] * zo.z);
+        acc_add(2, r[0] * z[0] + r[1] * z[1] + r[2] * z[2]);
+      }
+      if (replace) {
+        // true residual in FP64 (needs the neighbours' x updates)
+        if (!cluster_sync(cnt, csize, a.spin_limit, err, &s_ok)) {
+          fail = true;
+          break;
+        }
+        for (int s = c0 + warp; s < c1; s += nwarps) {
+          const int64_t row = (int64_t)s * kSlice + lane;
+          double r[3];
+          true_residual<4>(a, s, lane, r);
+          const float4 zo = a.z[row];
+          float z[3];
+          prec_apply(a, row, r, z);
+#pragma unroll
+          for (int k = 0; k < 3; ++k) a.r[3 * row + k] = r[k];
+          a.z[row] = make_float4(z[0], z[1], z[2], 0.0f);
+          acc_add(0, r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+          acc_add(1, r[0] * zo.x + r[1] * zo.y + r[2] * zo.z);
+          acc_add(2, r[0] * z[0] + r[1] * z[1] + r[2] * z[2]);
+        }
+      }
+      if (!reduce(3)) {
+        fail = true;
+        break;
+      }
+      it_done = it;
+      rr = s_tot[0];
+      const double rzo = s_tot[1], rzn = s_tot[2];
+      if (!isfinite(rr) || rr > div_thr) {
+        status = 3;
+        break;
+      }
+      if (rr <= conv_thr) {
+        if (replace) {
+          status = 1;
+          break;
+        }
+        verify_it = it;
+      }
+      if (it >= a.max_iter) {
+        status = 2;
+        break;
+      }
+      if (rzn == 0.0) {
+        status = 3;
+        break;
+      }
+      const double bpr = (a.polak_ribiere && !first) ? rzo : 0.0;
+      beta = (rzn - bpr) / rz;
+      rz = rzn;
+      first = false;
+    }
+    if (fail) break;
+    if (rank == 0 && threadIdx.x == 0) {
+      a.out_iters[e] = it_done;
+      a.out_res[e] = sqrt(fmax(rr, 0.0));
+      a.out_relres[e] = bb == 0.0 ? 0.0 : sqrt(fmax(rr, 0.0) / bb);
+      a.out_conv[e] = status;
+    }
+  }
+  (void)fail;
+  cluster_hw_sync();  // no CTA leaves while another may still read its shared memory
+}
+
 // The pipelined variant runs at 512 threads per CTA or fewer (SDX_PCG_PIPE=0 selects the batched one).
 static bool pcg_pipelined(int threads) {
   static const int pipe = [] {
@@ -1559,6 +1932,76 @@ int pcg_max_ctas_per_sm(int threads) {
 }
 
 int pcg_shared_bytes(int threads, int wstride) { return (threads / 32) * wstride * kPcgNq * (int)sizeof(double); }
+
+// Cluster shapes for k_pcg_cluster (one 512-thread CTA per SM): how many clusters of 16, 8, 4 and 2 CTAs
+// are co-resident on this device (occupancy queries, once).
+static const int kClSizes[4] = {16, 8, 4, 2};
+static const int* pcg_cluster_counts(int* last_error) {
+  static int err = 0;
+  static const std::array<int, 4> counts = [] {
+    std::array<int, 4> n{0, 0, 0, 0};
+    cudaFuncSetAttribute(k_pcg_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    for (int i = 0; i < 4; ++i) {
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = kClSizes[i];
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3(kClSizes[i]);
+      cfg.blockDim = dim3(512);
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      const cudaError_t e = cudaOccupancyMaxActiveClusters(&n[i], k_pcg_cluster, &cfg);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        n[i] = 0;
+        err = (int)e;
+      }
+    }
+    return n;
+  }();
+  if (last_error) *last_error = err;
+  return counts.data();
+}
+
+// The shape for a queue of n_envs envs: the cluster size that keeps the most SMs busy with min(n_envs,
+// co-resident clusters) clusters, ties to the smaller clusters (more envs in flight, so one slow env holds
+// up fewer SMs at the end). SDX_PCG_CLUSTER_SIZE=16/8/4/2 forces a size.
+ClusterShape pcg_cluster_shape(int n_envs) {
+  int err = 0;
+  const int* counts = pcg_cluster_counts(&err);
+  const char* force = getenv("SDX_PCG_CLUSTER_SIZE");
+  const int want = force ? atoi(force) : 0;
+  ClusterShape best{0, 0, err};
+  int best_busy = 0;
+  for (int i = 0; i < 4; ++i) {
+    const int cs = kClSizes[i], n = std::min(counts[i], std::max(1, n_envs));
+    if (counts[i] <= 0 || (want > 0 && cs != want)) continue;
+    const int busy = n * cs;
+    if (busy > best_busy || (busy == best_busy && cs < best.size)) {
+      best_busy = busy;
+      best = ClusterShape{n, cs, err};
+    }
+  }
+  return best;
+}
+
+cudaError_t launch_pcg_cluster(const PcgArgs& a, ClusterShape shape, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = shape.size;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3(shape.n_clusters * shape.size);
+  cfg.blockDim = dim3(512);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_pcg_cluster, a);
+}
 
 cudaError_t launch_pcg(const PcgArgs& a, int n_cta, int threads, cudaStream_t st) {
   PcgArgs args = a;

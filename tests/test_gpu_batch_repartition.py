@@ -1,7 +1,10 @@
-"""Batched envs whose CG solves end at very different iteration counts: once half of the rows have
-converged, the persistent PCG saves its per-env CG scalars, re-partitions the envs still iterating over
-all CTAs and resumes. A batched step must agree with each env stepped on its own (a single env is never
-re-partitioned), and the re-partitioning must have happened."""
+"""Batched envs whose CG solves end at very different iteration counts.
+
+The grid kernel: once half of the rows have converged, the persistent PCG saves its per-env CG scalars,
+re-partitions the envs still iterating over all CTAs and resumes. The cluster kernel (the default for
+batches of small envs): one thread-block cluster per env at a time, envs taken largest first from a
+queue. Either way a batched step must agree with each env stepped on its own (a single env always runs
+on the grid kernel, never re-partitioned), and the path under test must have run."""
 import numpy as np
 import pytest
 
@@ -20,7 +23,7 @@ def _bodies():
     return out
 
 
-def test_repartitioned_batch_matches_single_env_steps():
+def _check_against_single_env_steps(cluster: bool):
     from project_superdex_b200.soft_body import SoftBodyWorld
     bodies = _bodies()
     cfg = scenes.SceneConfig()
@@ -28,7 +31,10 @@ def test_repartitioned_batch_matches_single_env_steps():
     w.set_profiling(True)
     w.step(2)
     prof = w.profile()
-    assert prof["pcg_relaunches"] > 0
+    if cluster:
+        assert prof["pcg_cluster_solves"] == prof["pcg_launches"] > 0
+    else:
+        assert prof["pcg_relaunches"] > 0 and prof["pcg_cluster_solves"] == 0
     ub = w.get_state()[0]
     stats = w.stats()
     off = 0
@@ -45,3 +51,42 @@ def test_repartitioned_batch_matches_single_env_steps():
             (e, stats[e]["cg_iters"], s1["cg_iters"])
         off += 3 * b.n_nodes
         w1.close()
+
+
+def test_repartitioned_batch_matches_single_env_steps(monkeypatch):
+    monkeypatch.setenv("SDX_PCG_CLUSTER", "0")
+    _check_against_single_env_steps(cluster=False)
+
+
+def test_cluster_batch_matches_single_env_steps(monkeypatch):
+    monkeypatch.delenv("SDX_PCG_CLUSTER", raising=False)
+    monkeypatch.setenv("SDX_PCG_CLUSTER_QUEUE", "1")  # every solve of the batch on the cluster kernel
+    _check_against_single_env_steps(cluster=True)
+
+
+def test_cluster_and_grid_kernels_agree_on_a_contact_batch(monkeypatch):
+    """Uneven bodies pressed by capsules (active contact, temporal warm start): the cluster kernel and the
+    grid kernel reach the same states and the same per-env iteration counts within the CG tolerance."""
+    from project_superdex_b200 import capi
+    from project_superdex_b200.soft_body import SoftBodyWorld
+    bodies, cfg = scenes.config2(7, n_envs=12, lo=8, hi=14)
+    out = {}
+    monkeypatch.setenv("SDX_PCG_CLUSTER_QUEUE", "1")
+    for mode in ("0", "1"):
+        monkeypatch.setenv("SDX_PCG_CLUSTER", mode)
+        w = SoftBodyWorld(bodies, cfg, newton_abs_tol=1e-9, newton_max_iter=12)
+        w.set_params(warm_start=capi.SDX_WARM_TEMPORAL)
+        w.set_profiling(True)
+        w.step(3)
+        out[mode] = (w.get_state()[0], w.stats(), w.profile())
+        w.close()
+    assert out["1"][2]["pcg_cluster_solves"] > 0 and out["0"][2]["pcg_cluster_solves"] == 0
+    size = max(np.ptp(b.X, axis=0).max() for b in bodies)
+    assert np.abs(out["1"][0] - out["0"][0]).max() <= 1e-5 * size
+    assert max(s["n_contacts"] for s in out["1"][1]) > 0
+    # the grid kernel runs an FP64 replacement iteration for every env whenever one env verifies its
+    # convergence, the cluster kernel per env: iteration counts differ by a few per cent
+    for sa, sb in zip(out["0"][1], out["1"][1]):
+        assert sa["convergence"] == sb["convergence"]
+        assert abs(sa["newton_iters"] - sb["newton_iters"]) <= 1
+        assert abs(sa["cg_iters"] - sb["cg_iters"]) <= max(6, int(0.15 * sa["cg_iters"]))
