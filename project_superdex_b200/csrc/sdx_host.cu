@@ -883,9 +883,12 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
     // re-partition the envs still iterating and resume from iteration flags[6]
     std::vector<EnvSave> es(n_envs);
     SDX_CUDA(cudaMemcpy(es.data(), W.es, sizeof(EnvSave) * n_envs, cudaMemcpyDeviceToHost));
+    // the envs of this solve still iterating (es[] of envs outside the solve holds an older solve's state)
     std::vector<int> list;
-    for (int s = 0; s < c->n_slices; ++s)
-      if (es[c->h_slice_env[s]].status == 0) list.push_back(s);
+    for (int s = 0; s < c->n_slices; ++s) {
+      const int e = c->h_slice_env[s];
+      if ((!h_mask || h_mask[e]) && es[e].status == 0) list.push_back(s);
+    }
     if (list.empty()) break;
     SDX_TRY(choose_partition(c, c->n_slices, c->h_slice_env, n_envs, c->h_slice_ptr, c->part_dyn, P.threads, 0,
                              &list));
