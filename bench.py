@@ -413,6 +413,7 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clocks,
         "solver": {"cg_iters_per_step": head["cg_iters_per_step"],
                    "newton_iters_per_step": head["newton_iters_per_step"],
+                   "pcg_cluster_solves": int(prof.get("pcg_cluster_solves", 0)),
                    "profile_ms": {k: v for k, v in prof.items() if k.endswith("_ms")}},
     }
     if rank == 0 and not args.no_cpu_baseline:
