@@ -803,8 +803,8 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
   // rows and either the queue is long (at least kClusterQueueFactor envs per co-resident cluster, so the
   // clusters stay busy until the last few envs) or only a few latency-bound envs are left (at most
   // kClusterTailEnvs envs of at most kClusterLatencyRows rows). Not for the two-vector (learned) start.
-  // SDX_PCG_CLUSTER=0 keeps every solve on the grid kernel; SDX_PCG_CLUSTER_QUEUE and
-  // SDX_PCG_CLUSTER_TAIL override the two thresholds.
+  // SDX_PCG_CLUSTER=0 keeps every solve on the grid kernel; SDX_PCG_CLUSTER_QUEUE, SDX_PCG_CLUSTER_TAIL
+  // and SDX_PCG_CLUSTER_TAIL_ROWS override the thresholds.
   if (batch && !x2) {
     const char* ce = getenv("SDX_PCG_CLUSTER");
     std::vector<int> list;
@@ -820,7 +820,9 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
     const int queue_factor = qf ? atoi(qf) : kClusterQueueFactor, tail_envs = tl ? atoi(tl) : kClusterTailEnvs;
     const int n_list = (int)list.size();
     const bool long_queue = queue_factor > 0 && n_list >= queue_factor * shape.n_clusters;
-    const bool tail = n_list <= tail_envs && max_rows <= kClusterLatencyRows;
+    const char* tr = getenv("SDX_PCG_CLUSTER_TAIL_ROWS");
+    const int64_t tail_rows = tr ? atoll(tr) : kClusterLatencyRows;
+    const bool tail = n_list <= tail_envs && max_rows <= tail_rows;
     if (shape.n_clusters > 0 && n_list > 0 && max_rows <= kClusterMaxRows && (long_queue || tail)) {
       std::stable_sort(list.begin(), list.end(), [&](int x, int y) {
         return c->h_row_off[x + 1] - c->h_row_off[x] > c->h_row_off[y + 1] - c->h_row_off[y];

@@ -1614,8 +1614,9 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
   __shared__ double wq[16][kClNq];     // per-warp partial sums
   __shared__ double s_part[2][kClNq];  // this CTA's partials, two buffers (consecutive reductions)
   __shared__ double s_tot[kClNq];
+  __shared__ double s_gather[16][kClNq];  // every CTA's partials, gathered in one round of remote loads
   __shared__ unsigned s_cnt;           // the cluster barrier counter (used in CTA 0)
-  __shared__ int s_env, s_ok;
+  __shared__ int s_env, s_env_here, s_ok;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   const uint32_t rank = cluster_rank(), csize = cluster_size();
   if (threadIdx.x == 0) s_cnt = 0u;
@@ -1634,7 +1635,8 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
     v = warp_sum(v);
     if (lane == 0) wq[warp][k] += v;
   };
-  // publish this CTA's partials, synchronise the cluster, sum all CTAs' partials in rank order
+  // publish this CTA's partials, synchronise the cluster, gather all CTAs' partials (one remote load per
+  // thread, all in flight at once) and sum them in rank order
   auto reduce = [&](int nq) {
     __syncthreads();
     if (threadIdx.x < nq) {
@@ -1643,9 +1645,14 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
       s_part[rb][threadIdx.x] = v;
     }
     if (!cluster_sync(cnt, csize, a.spin_limit, err, &s_ok)) return false;
+    if (threadIdx.x < (int)csize * nq) {
+      const int r = threadIdx.x / nq, k = threadIdx.x - r * nq;
+      s_gather[r][k] = cluster_ld_f64(cluster_map(&s_part[rb][k], (uint32_t)r));
+    }
+    __syncthreads();
     if (threadIdx.x < nq) {
       double v = 0.0;
-      for (uint32_t r = 0; r < csize; ++r) v += cluster_ld_f64(cluster_map(&s_part[rb][threadIdx.x], r));
+      for (uint32_t r = 0; r < csize; ++r) v += s_gather[r][threadIdx.x];
       s_tot[threadIdx.x] = v;
     }
     rb ^= 1;
@@ -1660,7 +1667,9 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
       s_env = h < a.cl_n ? a.cl_envs[h] : -1;
     }
     if (!cluster_sync(cnt, csize, a.spin_limit, err, &s_ok)) break;
-    const int e = cluster_ld_s32(env0);
+    if (threadIdx.x == 0) s_env_here = cluster_ld_s32(env0);
+    __syncthreads();
+    const int e = s_env_here;
     if (e < 0) break;
     const int sa = a.env_soff[e], ns = a.env_soff[e + 1] - sa;
     const int c0 = sa + (int)((int64_t)ns * rank / csize), c1 = sa + (int)((int64_t)ns * (rank + 1) / csize);
