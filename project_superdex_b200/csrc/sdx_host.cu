@@ -802,10 +802,10 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
   // largest first from a queue, no grid-wide lockstep) when every active env has at most kClusterMaxRows
   // rows and either the queue is long (at least kClusterQueueFactor envs per co-resident cluster, so the
   // clusters stay busy until the last few envs) or only a few latency-bound envs are left (at most
-  // kClusterTailEnvs envs of at most kClusterLatencyRows rows). Not for the two-vector (learned) start.
+  // kClusterTailEnvs envs of at most kClusterLatencyRows rows).
   // SDX_PCG_CLUSTER=0 keeps every solve on the grid kernel; SDX_PCG_CLUSTER_QUEUE, SDX_PCG_CLUSTER_TAIL
   // and SDX_PCG_CLUSTER_TAIL_ROWS override the thresholds.
-  if (batch && !x2) {
+  if (batch) {
     const char* ce = getenv("SDX_PCG_CLUSTER");
     std::vector<int> list;
     int64_t max_rows = 0;

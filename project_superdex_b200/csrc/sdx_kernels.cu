@@ -1550,7 +1550,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
 // Every wait is bounded: a timeout records the error word and the kernel unwinds to its final cluster
 // barrier, which every CTA reaches exactly once.
 
-constexpr int kClNq = 5;
+constexpr int kClNq = 11;
 
 __device__ __forceinline__ uint32_t cluster_rank() {
   uint32_t r;
@@ -1676,8 +1676,69 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
 
     // ---- phase 0: diagonal, start vector, r0, z0 ----
     const bool scaled = !a.zero_guess && a.scale_guess;
+    const bool two = scaled && a.x2 != nullptr;
     double al0 = 0.0;
-    if (scaled) {
+    if (two) {
+      // Galerkin start on span{x, x2}, as in k_pcg: A h and A y in one FP64 pass, 11 reduced quantities,
+      // the best of the pair and the one-vector optima whose residual is below ||b||, else the zero start
+      acc_reset();
+      for (int s = c0 + warp; s < c1; s += nwarps) {
+        const int64_t row = (int64_t)s * kSlice + lane;
+        double ah[3], ay[3];
+        spmv_f64_rows<4, 2>(a.A, s, lane, a.x, a.x2, ah, ay);
+        double q[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          a.r[3 * row + k] = ah[k];
+          a.gal[3 * row + k] = ay[k];
+          const double h = a.x[3 * row + k], y = a.x2[3 * row + k], bk = a.b[3 * row + k];
+          q[0] += bk * bk;
+          q[1] += h * bk;
+          q[2] += y * bk;
+          q[3] += h * ah[k];
+          q[4] += h * ay[k];
+          q[5] += y * ay[k];
+          q[6] += bk * ah[k];
+          q[7] += bk * ay[k];
+          q[8] += ah[k] * ah[k];
+          q[9] += ah[k] * ay[k];
+          q[10] += ay[k] * ay[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 11; ++k) acc_add(k, q[k]);
+      }
+      if (!reduce(11)) {
+        fail = true;
+        break;
+      }
+      const double* t = s_tot;
+      const double bb0 = t[0];
+      auto res2 = [&](double ca, double cb) {
+        return bb0 - 2.0 * (ca * t[6] + cb * t[7]) + ca * ca * t[8] + 2.0 * ca * cb * t[9] + cb * cb * t[10];
+      };
+      double best_gain = 0.0, ca = 0.0, cb = 0.0;
+      auto consider = [&](double xa, double xb) {
+        const double gain = xa * t[1] + xb * t[2];
+        if (isfinite(gain) && gain > best_gain && res2(xa, xb) < bb0) {
+          best_gain = gain;
+          ca = xa;
+          cb = xb;
+        }
+      };
+      const double det = t[3] * t[5] - t[4] * t[4];
+      if (t[3] > 0.0 && t[5] > 0.0 && det > 1e-12 * t[3] * t[5])
+        consider((t[1] * t[5] - t[2] * t[4]) / det, (t[3] * t[2] - t[4] * t[1]) / det);
+      if (t[3] > 0.0) consider(t[1] / t[3], 0.0);
+      if (t[5] > 0.0) consider(0.0, t[2] / t[5]);
+      for (int s = c0 + warp; s < c1; s += nwarps) {
+        const int64_t row = (int64_t)s * kSlice + lane;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          a.x[3 * row + k] = ca * a.x[3 * row + k] + cb * a.x2[3 * row + k];
+          a.r[3 * row + k] = a.b[3 * row + k] - ca * a.r[3 * row + k] - cb * a.gal[3 * row + k];
+        }
+      }
+    } else if (scaled) {
       acc_reset();
       for (int s = c0 + warp; s < c1; s += nwarps) {
         const int64_t row = (int64_t)s * kSlice + lane;
@@ -1739,6 +1800,9 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
           a.x[3 * row + k] = 0.0;
           r[k] = a.b[3 * row + k];
         }
+      } else if (two) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) r[k] = a.r[3 * row + k];  // this row's, written by this warp above
       } else if (scaled) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) {

@@ -64,10 +64,13 @@ def test_cluster_batch_matches_single_env_steps(monkeypatch):
     _check_against_single_env_steps(cluster=True)
 
 
-def test_cluster_and_grid_kernels_agree_on_a_contact_batch(monkeypatch):
-    """Uneven bodies pressed by capsules (active contact, temporal warm start): the cluster kernel and the
-    grid kernel reach the same states and the same per-env iteration counts within the CG tolerance."""
+@pytest.mark.parametrize("warm", ["temporal", "learned"])
+def test_cluster_and_grid_kernels_agree_on_a_contact_batch(monkeypatch, warm):
+    """Uneven bodies pressed by capsules (active contact; temporal warm start, or the learned one's
+    two-vector Galerkin start with an untrained network): the cluster kernel and the grid kernel reach
+    the same states and the same per-env iteration counts within the CG tolerance."""
     from project_superdex_b200 import capi
+    from project_superdex_b200.learned import Mlp
     from project_superdex_b200.soft_body import SoftBodyWorld
     bodies, cfg = scenes.config2(7, n_envs=12, lo=8, hi=14)
     out = {}
@@ -75,7 +78,10 @@ def test_cluster_and_grid_kernels_agree_on_a_contact_batch(monkeypatch):
     for mode in ("0", "1"):
         monkeypatch.setenv("SDX_PCG_CLUSTER", mode)
         w = SoftBodyWorld(bodies, cfg, newton_abs_tol=1e-9, newton_max_iter=12)
-        w.set_params(warm_start=capi.SDX_WARM_TEMPORAL)
+        if warm == "learned":
+            m = Mlp(w._ctx)
+            m.init(3)
+        w.set_params(warm_start=capi.SDX_WARM_TEMPORAL if warm == "temporal" else capi.SDX_WARM_LEARNED)
         w.set_profiling(True)
         w.step(3)
         out[mode] = (w.get_state()[0], w.stats(), w.profile())
