@@ -24,11 +24,14 @@ constexpr int kPadBit = 0x80000000;
 constexpr int kPcgMaxEnvsPerCta = 32;
 // cluster PCG: the largest env it takes (rows); the queue length, in envs per co-resident cluster, from
 // which it runs a whole batch; the envs (at most kClusterTailEnvs, each at most kClusterLatencyRows rows)
-// it takes at the end of a batch's Newton iterations, where the grid kernel is latency bound
+// it takes at the end of a batch's Newton iterations. Per CG iteration on two-env batches the cluster
+// kernel measured 9.0 us against the grid kernel's 11.9 us at 2,197 rows per env, but 15.3 against 12.2
+// at 9,261 and 24.7 against 13.9 at 24,389 (the grid kernel spreads a small env over every SM), so the
+// tail rule is kept to tiny envs.
 constexpr int64_t kClusterMaxRows = 131072;
 constexpr int kClusterQueueFactor = 4;
 constexpr int kClusterTailEnvs = 4;
-constexpr int64_t kClusterLatencyRows = 32768;
+constexpr int64_t kClusterLatencyRows = 4096;
 constexpr int kPcgNq = 11;  // partial sums per (CTA, env) and phase (11: the two-vector start)
 
 __host__ __device__ __forceinline__ size_t val_index(int64_t p, int e) {
