@@ -339,7 +339,9 @@ def run_ours(args, rank, world, local_rank):
     pcg_s = prof["pcg_ms"] / 1000.0
     achieved = prof["pcg_bytes"] / pcg_s / 1e9 if pcg_s > 0 else None
     traffic = ncu_traffic("k_pcg_per_iter") if args.workload == "cfg1" else None
-    roofline = {"bound": "hbm", "kernel": "k_pcg (persistent Jacobi-PCG)", "achieved": achieved,
+    pcg_kernel = ("k_pcg (persistent Jacobi-PCG) and k_pcg_cluster (one cluster per env), every PCG solve"
+                  if prof.get("pcg_cluster_solves", 0) else "k_pcg (persistent Jacobi-PCG)")
+    roofline = {"bound": "hbm", "kernel": pcg_kernel, "achieved": achieved,
                 "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                 "peak_source": peak_kind, "traffic": traffic, "bytes_per_iter": bytes_iter,
                 "iters": prof["pcg_iters"], "share_of_step": prof["pcg_ms"] / ms}

@@ -1614,7 +1614,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
   __shared__ double wq[16][kClNq];     // per-warp partial sums
   __shared__ double s_part[2][kClNq];  // this CTA's partials, two buffers (consecutive reductions)
   __shared__ double s_tot[kClNq];
-  __shared__ double s_gather[16][kClNq];  // every CTA's partials, gathered in one round of remote loads
+  __shared__ double s_gather[16][kClNq];  // every CTA's partials, gathered by one pass of remote loads
   __shared__ unsigned s_cnt;           // the cluster barrier counter (used in CTA 0)
   __shared__ int s_env, s_env_here, s_ok;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
