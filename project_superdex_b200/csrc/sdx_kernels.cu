@@ -1979,7 +1979,6 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
       a.out_conv[e] = status;
     }
   }
-  (void)fail;
   cluster_hw_sync();  // no CTA leaves while another may still read its shared memory
 }
 

@@ -64,6 +64,8 @@ def test_no_gpu_is_reported_not_faked():
     lib = capi.lib()
     assert not lib.sdx_create(0)
     assert b"device" in lib.sdx_last_error().lower() or b"cuda" in lib.sdx_last_error().lower()
+    with pytest.raises(capi.SdxError, match="no CUDA device"):
+        capi.pcg_cluster_shape(16)  # the cluster PCG's launch shape needs the device it would run on
 
 
 def test_missing_library_fails_loudly(monkeypatch, tmp_path):
