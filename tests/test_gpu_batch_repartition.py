@@ -1,9 +1,9 @@
 """Batched envs whose CG solves end at very different iteration counts.
 
 The grid kernel: once half of the rows have converged, the persistent PCG saves its per-env CG scalars,
-re-partitions the envs still iterating over all CTAs and resumes. The cluster kernel (the default for
-batches of small envs): one thread-block cluster per env at a time, envs taken largest first from a
-queue. Either way a batched step must agree with each env stepped on its own (a single env always runs
+re-partitions the envs still iterating over all CTAs and resumes. The cluster kernel (taken for long
+queues of small envs; these tests lower the queue threshold so that it runs on their small batches):
+one thread-block cluster per env at a time, envs taken largest first from a queue. Either way a batched step must agree with each env stepped on its own (a single env always runs
 on the grid kernel, never re-partitioned), and the path under test must have run."""
 import numpy as np
 import pytest
