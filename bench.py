@@ -321,9 +321,10 @@ def run_ours(args, rank, world, local_rank):
             if arm == "learned":
                 Mlp(w._ctx).set_params(params)
             w.set_params(warm_start={"learned": capi.SDX_WARM_LEARNED, "temporal": capi.SDX_WARM_TEMPORAL}.get(
-                             arm, capi.SDX_WARM_ZERO),
-                         linear_solver_impl=(capi.SDX_SOLVER_PLAIN_FP64 if arm == "plain_fp64"
-                                             else capi.SDX_SOLVER_FUSED))
+                             arm, capi.SDX_WARM_ZERO))
+            if arm == "plain_fp64":  # the comparison solver, plugged into the Newton solves (bench_arms/)
+                from bench_arms.plain import PlainFp64
+                w._plain = PlainFp64(w)
             stream = torch.cuda.ExternalStream(w.stream_handle(), device=local_rank)
             r = time_arm(w, args, stream, local_rank, dist, world)
             results[arm] = merge_runs(results[arm], r) if arm in results else r

@@ -34,7 +34,10 @@ extern "C" {
 #define SDX_ERR_INVALID_ARGUMENT -1
 #define SDX_ERR_CUDA -2
 #define SDX_ERR_NOT_READY -3      /* call order: bodies must be uploaded first */
-#define SDX_ERR_DEVICE_TIMEOUT -4 /* a bounded device-side wait gave up (grid barrier) */
+#define SDX_ERR_DEVICE_TIMEOUT -4 /* a bounded device-side wait gave up (grid barrier); the context stays
+                                     usable. The environment variable SDX_DEBUG_SPIN_LIMIT, read at each
+                                     solve, lowers the bound of the PCG grid barriers (tests use it to
+                                     make the wait run out) */
 #define SDX_ERR_OUT_OF_MEMORY -5
 #define SDX_ERR_UNSUPPORTED -6
 
@@ -73,6 +76,16 @@ extern "C" {
 #define SDX_WARM_LEARNED 2  /* dx0 = per-vertex MLP prediction (sdx_mlp_*) */
 #define SDX_WARM_TEMPORAL 3 /* dx0 = the previous step's dx of the same Newton iteration (first 4) */
 
+/* Value layouts of a host 3x3 block CSR matrix (sdx_linear_params.value_layout).
+ * ROW_STRIPS is the reference's own storage, BlockSparseMatrix<T,3>::Values(): each block row br with
+ * nb = row_ptr[br+1] - row_ptr[br] blocks is one row-major 3 x (3 nb) strip, so entry (lr, lc) of its
+ * k-th block sits at 9 row_ptr[br] + 3 (lr nb + k) + lc (FindValueIndex,
+ * mochi_core/include/mochi_core/linear_algebra/block_sparse_matrix.h:459-475). BLOCKS is 9 contiguous
+ * row-major values per block, the layout cuSPARSE BSR takes and ConvertCsrToBsr produces
+ * (mochi_core/src/linear_algebra/cuda/cuda_bsr_matrix.cu:22-47). */
+#define SDX_BSR_ROW_STRIPS 0
+#define SDX_BSR_BLOCKS 1
+
 /* Mirrors KrylovSolverParams (krylov_solver.h:43-82). Only the residual-L2 norm is supported. */
 typedef struct {
   double rel_tol;       /* ||r|| <= max(abs_tol, rel_tol ||b||) */
@@ -83,16 +96,9 @@ typedef struct {
   int abort_if_not_spd; /* stop with DIVERGED on p.Ap <= 0 */
   int polak_ribiere;    /* 1: Polak-Ribiere beta (reference default) */
   int replace_every;    /* FP64 true-residual replacement period in iterations (0: default 32) */
-  int solver_impl;      /* SDX_SOLVER_* (used by sdx_step; the sdx_pcg_solve* entry points are fused) */
+  int value_layout;     /* SDX_BSR_* of the values passed to the sdx_pcg_solve* entry points
+                           (default SDX_BSR_ROW_STRIPS, the reference's layout) */
 } sdx_linear_params;
-
-/* Linear solver implementations behind sdx_step. FUSED: this library's persistent, batched Jacobi-PCG
- * (FP32 matrix and SpMV, FP64 x, r and reductions). PLAIN_FP64: the reference's CUDA solver path
- * (krylov::CudaPCG, cuda_pcg.cpp:243-525) restated as the same-GPU comparison arm — FP64 3x3 BSR with
- * cuSPARSE bsrmv, cuBLAS vector operations, CUDA-graph bursts of 8 iterations with a host convergence
- * check after each, one env after the other; Jacobi or no preconditioner. */
-#define SDX_SOLVER_FUSED 0
-#define SDX_SOLVER_PLAIN_FP64 1
 
 /* Coulomb friction smoothing (CoulombFrictionModel, contact_params.h:307-327) */
 #define SDX_FRICTION_C1 0
@@ -171,10 +177,12 @@ void sdx_default_linear_params(sdx_linear_params* p);
 
 /* ---- linear solver boundary (LinearSolver<T>::Solve with solverType CudaCG) -------------------- */
 
-/* Solve A x = b, A symmetric positive definite in 3x3 block CSR (row-major blocks, block_rows
- * rows, nnzb blocks). values: 9*nnzb of SDX_F32 or SDX_F64. b, x: host FP64 vectors of 3*block_rows;
- * x is the initial guess on entry (ignored when hint == SDX_GUESS_ZERO) and the solution on exit.
- * The matrix is stored on the device in FP32; dot products and x, r accumulate in FP64. */
+/* Solve A x = b, A symmetric positive definite in 3x3 block CSR (block_rows rows, nnzb blocks,
+ * row_ptr / col as BlockSparseMatrix<T,3>::Pointers() / Indices(), widened to int64 row pointers).
+ * values: 9*nnzb of SDX_F32 or SDX_F64 in params->value_layout (SDX_BSR_ROW_STRIPS: the reference's
+ * BlockSparseMatrix::Values() as it is). b, x: host FP64 vectors of 3*block_rows; x is the initial guess
+ * on entry (ignored when hint == SDX_GUESS_ZERO) and the solution on exit. The matrix is stored on the
+ * device in FP32; dot products and x, r accumulate in FP64. */
 int sdx_pcg_solve(int block_rows, int64_t nnzb, const int64_t* row_ptr, const int32_t* col,
                   const void* values, int value_type, const double* b, double* x, int hint,
                   const sdx_linear_params* params, sdx_linear_status* status);
@@ -189,14 +197,17 @@ int sdx_pcg_solve_ctx(sdx_context* ctx, int block_rows, int64_t nnzb, const int6
  * when they need the solve — an engine whose pool allocator owns all device memory and forbids
  * cudaMalloc/cudaFree inside its step callbacks, or a real-time loop that must not take allocator
  * locks. Same algorithm, parameters and status as sdx_pcg_solve, but every pointer is a DEVICE pointer
- * owned by the caller (BSR with FP32 row-major 3x3 blocks, FP64 b and x) and nothing is allocated:
- * the work vectors live in one fixed array inside the library, held by every GPU that loads it until
- * the process exits. Limits: at most SDX_NOALLOC_MAX_BLOCK_ROWS block rows (larger systems return
- * SDX_ERR_INVALID_ARGUMENT). All calls on a device share that array: calls whose GPU work overlaps
- * (unordered streams or threads) race and must be serialized by the caller. The first call on a device
- * performs a one-time set-up (it looks up the array's device address); make it before any stream
- * capture. `stream` is a cudaStream_t (NULL: legacy default stream); the call returns after the solve
- * has finished on that stream. */
+ * owned by the caller (BSR with FP32 values in params->value_layout, FP64 b and x) and nothing is
+ * allocated: the work vectors live in one fixed array inside the library, held by every GPU that loads
+ * it until the process exits. Limits: at most SDX_NOALLOC_MAX_BLOCK_ROWS block rows (larger systems
+ * return SDX_ERR_INVALID_ARGUMENT). A row_ptr that is not monotone, does not start at 0 or does not end
+ * at nnzb, or a column index out of range, returns SDX_ERR_INVALID_ARGUMENT (checked on the device; no
+ * access leaves the caller's arrays). All calls on a device share that array: calls whose GPU work
+ * overlaps (unordered streams or threads) race and must be serialized by the caller. The first call on
+ * a device performs a one-time set-up (it looks up the array's device address). Every call
+ * synchronizes `stream` and copies the status to pageable host memory, so it cannot be made while
+ * that stream (or the device) is being captured into a CUDA graph. `stream` is a cudaStream_t (NULL:
+ * legacy default stream); the call returns after the solve has finished on that stream. */
 #define SDX_NOALLOC_MAX_BLOCK_ROWS 65536
 int sdx_pcg_solve_device_noalloc(int block_rows, int64_t nnzb, const int64_t* row_ptr, const int32_t* col,
                                  const float* values, const double* b, double* x, int hint,
@@ -284,6 +295,33 @@ int sdx_get_contact_pairs(sdx_context* ctx, int64_t* pairs, int64_t pairs_cap, i
 /* Advance every env n_steps backward-Euler steps from the current state (device resident). */
 int sdx_step(sdx_context* ctx, int n_steps);
 int sdx_get_stats(sdx_context* ctx, sdx_env_stats* per_env);
+
+/* ---- external linear solver (no counterpart in the reference's soft-body path) -----------------
+ * sdx_step solves each Newton system with this library's PCG. A caller may hand those solves to its own
+ * solver instead, e.g. a restatement of the reference's CUDA path (krylov::CudaPCG, cuSPARSE bsrmv and
+ * cuBLAS, mochi_core/src/linear_algebra/cuda/cuda_pcg.cpp:243-525) run as a comparison arm. The hook
+ * gets every env's Newton system on the device in user node order: the sdx_get_pattern block pattern
+ * with FP32 values in SDX_BSR_BLOCKS layout (Dirichlet rows and columns applied), b = the Newton
+ * gradient and x = the update (initial guess in, solution out), both FP64. It solves the envs with
+ * env_mask[e] != 0, writes their CG iteration counts to iters[e] and returns SDX_OK; any other value
+ * stops the step with that status. */
+typedef struct {
+  int n_envs;
+  const int64_t* node_offsets; /* host, n_envs + 1: env e owns nodes [node_offsets[e], node_offsets[e+1]) */
+  const uint8_t* env_mask;     /* host, n_envs */
+  int64_t n_nodes, nnzb;
+  const int64_t* row_ptr;      /* device, n_nodes + 1 (global node ids, columns stay inside the env) */
+  const int32_t* col;          /* device, nnzb */
+  const float* values;         /* device, 9 * nnzb */
+  const double* b;             /* device, 3 * n_nodes */
+  double* x;                   /* device, 3 * n_nodes */
+  int zero_guess;              /* 1: x holds no initial guess (start from zero) */
+  void* stream;                /* cudaStream_t the hook must order its work on */
+} sdx_device_system;
+typedef int (*sdx_linear_solve_fn)(void* user, const sdx_device_system* sys, const sdx_linear_params* params,
+                                   int* iters);
+/* fn = NULL restores this library's PCG. */
+int sdx_set_linear_solver(sdx_context* ctx, sdx_linear_solve_fn fn, void* user);
 
 /* ---- learned CG warm start (no counterpart in the reference) -------------------------------------
  * A per-vertex MLP (15 -> 128 -> 128 -> 128 -> 3, GELU; BF16 weights / activations, FP32 accumulate;

@@ -22,8 +22,8 @@ _up = C.POINTER(C.c_uint8)
 
 def build():
     """Compile the C restatement (and, where the reference tree is present, oracle/_ref)."""
-    subprocess.check_call(["make", "-s", "-C", HERE])
-    subprocess.check_call([os.path.join(HERE, "build_ref.sh")], stdout=subprocess.DEVNULL)
+    subprocess.check_call(["make", "-s", "-C", HERE, "all"])
+    subprocess.check_call(["make", "-s", "-C", HERE, "ref"], stdout=subprocess.DEVNULL)
 
 
 class OrCollider(C.Structure):
@@ -154,6 +154,10 @@ def ref():
         R.ref_pcg_csr.argtypes = [C.c_int, _lp, _ip, _dp, _dp, _dp, C.c_double, C.c_double, C.c_double,
                                   C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, C.POINTER(C.c_int)]
         R.ref_pcg_csr.restype = C.c_int
+        R.ref_bsr3_values.argtypes = [C.c_int, _ip, _ip, _dp, _dp]
+        R.ref_bsr3_pcg.argtypes = [C.c_int, _ip, _ip, _dp, _dp, _dp, C.c_double, C.c_double, C.c_double, C.c_int,
+                                   C.c_int, C.c_int, C.c_int, _dp, _dp, C.POINTER(C.c_int)]
+        R.ref_bsr3_pcg.restype = C.c_int
         _ref = R
     return _ref
 
@@ -183,6 +187,35 @@ def material(kind, mu, lam, F, project=False, psd=1, min_eig=np.finfo(np.float64
     Cm = np.zeros(81)
     lib().or_material(int(kind), mu, lam, ptr(F), int(project), psd, min_eig, ptr(e), ptr(P), ptr(Cm))
     return e[0], P.reshape(3, 3), Cm.reshape(9, 9)
+
+
+def ref_bsr3_values(row_ptr, col, blocks):
+    """Values() of the reference's BlockSparseMatrix<double,3> filled entry by entry through its own
+    SetValue: the values in the reference's storage layout (row strips)."""
+    rp = np.ascontiguousarray(row_ptr, np.int32)
+    cl = np.ascontiguousarray(col, np.int32)
+    bl = np.ascontiguousarray(np.asarray(blocks, np.float64).reshape(-1, 9))
+    out = np.zeros(bl.size)
+    ref().ref_bsr3_values(rp.size - 1, rp.ctypes.data_as(_ip), cl.ctypes.data_as(_ip), bl.ctypes.data_as(_dp),
+                          out.ctypes.data_as(_dp))
+    return out
+
+
+def ref_bsr3_pcg(row_ptr, col, values, b, x0=None, rel_tol=1e-6, abs_tol=1e-30, rel_div_tol=1e10, max_iter=10000,
+                 precond=1, polak_ribiere=True):
+    """The reference's krylov::PCG on its BlockSparseMatrix<double,3> holding `values` (row-strip layout),
+    with its BlockJacobiPrec (precond 1 Jacobi, 2 block Jacobi, 0 none). Returns (x, iters, |r|, |r|/|b|,
+    convergence)."""
+    rp = np.ascontiguousarray(row_ptr, np.int32)
+    cl = np.ascontiguousarray(col, np.int32)
+    v = np.ascontiguousarray(values, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros_like(b) if x0 is None else np.array(x0, np.float64)
+    res, rel, conv = C.c_double(), C.c_double(), C.c_int()
+    it = ref().ref_bsr3_pcg(rp.size - 1, rp.ctypes.data_as(_ip), cl.ctypes.data_as(_ip), v.ctypes.data_as(_dp),
+                            b.ctypes.data_as(_dp), x.ctypes.data_as(_dp), rel_tol, abs_tol, rel_div_tol, max_iter,
+                            precond, int(polak_ribiere), int(x0 is None), C.byref(res), C.byref(rel), C.byref(conv))
+    return x, it, res.value, rel.value, conv.value
 
 
 def ref_material(kind, mu, lam, F, project=False, psd=1):

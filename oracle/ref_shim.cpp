@@ -10,6 +10,8 @@
 #include <mochi_core/element_operations/fem_stress_damping.h>
 #include <mochi_core/materials/reference_material_stiffness.h>
 #include <mochi_core/elements/tetrahedral/finite_element.h>
+#include <mochi_core/linear_algebra/block_sparse_matrix.h>
+#include <mochi_core/linear_algebra/krylov/block_jacobi_prec.h>
 #include <mochi_core/linear_algebra/krylov/pcg.h>
 #include <mochi_core/linear_algebra/matrix.h>
 #include <mochi_core/materials/batched_arap.h>
@@ -308,6 +310,64 @@ int ref_pcg_csr(int n, const int64_t* row_ptr, const int32_t* col, const double*
   auto st = krylov::PCG(opA, bv, xv, opP, max_iter, stop, false, VerbosityLevel::Silent,
                         polak_ribiere != 0,
                         zero_guess ? InitialGuessHint::Zero : InitialGuessHint::Unknown);
+  for (int i = 0; i < n; ++i) x[i] = xv[i];
+  *res_norm = st.residualNorm;
+  *rel_res_norm = st.relativeResidualNorm;
+  *convergence = static_cast<int>(st.convergence);
+  return st.numIterDone;
+}
+
+// mochi::BlockSparseMatrix<double, 3> (mochi_core/include/mochi_core/linear_algebra/block_sparse_matrix.h:63)
+// on the block pattern (ptr, idx), every scalar entry written through its own SetValue (:230-238, which
+// places it by FindValueIndex, :459-475); copies out Values(), i.e. the values in the reference's storage
+// layout. blocks: 9 row-major values per block.
+void ref_bsr3_values(int n_block_rows, const int32_t* ptr, const int32_t* idx, const double* blocks,
+                     double* values_out) {
+  const int nnzb = ptr[n_block_rows];
+  DynamicArray<int> p(ptr, ptr + n_block_rows + 1), ix(idx, idx + nnzb);
+  DynamicArray<double> v(9 * (size_t)nnzb);
+  BlockSparseMatrix<double, 3> A(n_block_rows, std::move(p), std::move(ix), std::move(v));
+  A.SetZero();
+  for (int br = 0; br < n_block_rows; ++br)
+    for (int k = ptr[br]; k < ptr[br + 1]; ++k)
+      for (int e = 0; e < 9; ++e) A.SetValue(3 * br + e / 3, 3 * idx[k] + e % 3, blocks[9 * (size_t)k + e]);
+  auto const V = A.Values();
+  for (size_t i = 0; i < V.size(); ++i) values_out[i] = V[i];
+}
+
+// krylov::PCG (pcg.h:70) on a mochi::BlockSparseMatrix<double, 3> holding `values` as its Values() (the
+// reference's layout), applied by the matrix's own Apply (block_sparse_matrix.h:1134), with the
+// reference's BlockJacobiPrec (block_jacobi_prec.h:35): precond 1 = Jacobi (block size 1), 2 = block
+// Jacobi (3x3), 0 = none; residual-L2 stop test. Returns the iteration count.
+int ref_bsr3_pcg(int n_block_rows, const int32_t* ptr, const int32_t* idx, const double* values,
+                 const double* b, double* x, double rel_tol, double abs_tol, double rel_div_tol, int max_iter,
+                 int precond, int polak_ribiere, int zero_guess, double* res_norm, double* rel_res_norm,
+                 int* convergence) {
+  const int nnzb = ptr[n_block_rows];
+  const int n = 3 * n_block_rows;
+  DynamicArray<int> p(ptr, ptr + n_block_rows + 1), ix(idx, idx + nnzb);
+  DynamicArray<double> v(values, values + 9 * (size_t)nnzb);
+  BlockSparseMatrix<double, 3> A(n_block_rows, std::move(p), std::move(ix), std::move(v));
+  ColumnVector<double> bv(n), xv(n);
+  for (int i = 0; i < n; ++i) {
+    bv[i] = b[i];
+    xv[i] = x[i];
+  }
+  krylov::StatusResidualL2<krylov::UsualDot, double> stop{rel_tol, abs_tol, rel_div_tol};
+  auto const hint = zero_guess ? InitialGuessHint::Zero : InitialGuessHint::Unknown;
+  LinearSolverStatus st;
+  if (precond == 1) {
+    krylov::BlockJacobiPrec<double, 1> P(A);
+    st = krylov::PCG(A, bv, xv, P, max_iter, stop, false, VerbosityLevel::Silent, polak_ribiere != 0, hint);
+  } else if (precond == 2) {
+    krylov::BlockJacobiPrec<double, 3> P(A);
+    st = krylov::PCG(A, bv, xv, P, max_iter, stop, false, VerbosityLevel::Silent, polak_ribiere != 0, hint);
+  } else {
+    auto opP = [&](auto const& in, auto& out) {
+      for (int i = 0; i < n; ++i) out[i] = in[i];
+    };
+    st = krylov::PCG(A, bv, xv, opP, max_iter, stop, false, VerbosityLevel::Silent, polak_ribiere != 0, hint);
+  }
   for (int i = 0; i < n; ++i) x[i] = xv[i];
   *res_norm = st.residualNorm;
   *rel_res_norm = st.relativeResidualNorm;

@@ -9,7 +9,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsdx_b200.so")
-SOURCES = ["sdx_kernels.cu", "sdx_host.cu", "sdx_noalloc.cu", "sdx_mlp.cu", "sdx_plain.cu"]
+SOURCES = ["sdx_kernels.cu", "sdx_host.cu", "sdx_noalloc.cu", "sdx_mlp.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -34,7 +34,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return LIB
     srcs = [os.path.join(CSRC, s) for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
     cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "--extended-lambda", "-shared",
-           "-Xcompiler", "-fPIC,-fopenmp", "-ccbin", "/usr/bin/g++", "-o", LIB + ".tmp", *srcs, "-lgomp", "-lcusparse", "-lcublas", "-Xlinker", "--no-undefined"]
+           "-Xcompiler", "-fPIC,-fopenmp", "-ccbin", "/usr/bin/g++", "-o", LIB + ".tmp", *srcs, "-lgomp", "-Xlinker", "--no-undefined"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd), file=sys.stderr)

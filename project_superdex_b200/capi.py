@@ -20,7 +20,8 @@ SDX_F32, SDX_F64 = 0, 1
 SDX_PREC_NONE, SDX_PREC_JACOBI, SDX_PREC_BLOCK_JACOBI = 0, 1, 2
 SDX_WARM_ZERO, SDX_WARM_PREVIOUS, SDX_WARM_LEARNED, SDX_WARM_TEMPORAL = 0, 1, 2, 3
 SDX_LINEAR_CONVERGED, SDX_LINEAR_STOPPED, SDX_LINEAR_DIVERGED = 1, 2, 3
-SDX_SOLVER_FUSED, SDX_SOLVER_PLAIN_FP64 = 0, 1
+SDX_BSR_ROW_STRIPS, SDX_BSR_BLOCKS = 0, 1
+SDX_ERR_INVALID_ARGUMENT, SDX_ERR_DEVICE_TIMEOUT = -1, -4
 SDX_MAT_NEO_HOOKEAN, SDX_MAT_ST_VENANT_KIRCHHOFF, SDX_MAT_LINEAR_ELASTIC, SDX_MAT_ARAP = 0, 1, 2, 5
 
 # every entry point include/sdx_b200.h declares
@@ -35,7 +36,7 @@ EXPORTED = [
     "sdx_collect_training", "sdx_get_training_data", "sdx_write_state_masked", "sdx_capture_state",
     "sdx_restore_state", "sdx_release_state", "sdx_release_all_states", "sdx_is_equal_state",
     "sdx_capture_state_to_bytes", "sdx_restore_state_from_bytes", "sdx_get_pcg_cta_profile",
-    "sdx_pcg_cluster_shape",
+    "sdx_pcg_cluster_shape", "sdx_set_linear_solver",
 ]
 SDX_MLP_PARAMS = 37264
 SDX_NOALLOC_MAX_BLOCK_ROWS = 65536
@@ -46,7 +47,7 @@ class LinearParams(C.Structure):
 
     _fields_ = [("rel_tol", C.c_double), ("abs_tol", C.c_double), ("rel_div_tol", C.c_double),
                 ("max_iter", C.c_int), ("preconditioner", C.c_int), ("abort_if_not_spd", C.c_int),
-                ("polak_ribiere", C.c_int), ("replace_every", C.c_int), ("solver_impl", C.c_int)]
+                ("polak_ribiere", C.c_int), ("replace_every", C.c_int), ("value_layout", C.c_int)]
 
 
 class LinearStatus(C.Structure):
@@ -71,6 +72,19 @@ class StepParams(C.Structure):
                 ("friction_fitted_hessian", C.c_int), ("friction_fade", C.c_int),
                 ("friction_collider_normal", C.c_int), ("contact_explicit_normals", C.c_int),
                 ("contact_implicit_normal_force", C.c_int)]
+
+
+class DeviceSystem(C.Structure):
+    """sdx_device_system: one Newton system handed to an external linear solver (user node order)."""
+
+    _fields_ = [("n_envs", C.c_int), ("node_offsets", C.POINTER(C.c_int64)), ("env_mask", C.POINTER(C.c_uint8)),
+                ("n_nodes", C.c_int64), ("nnzb", C.c_int64), ("row_ptr", C.c_void_p), ("col", C.c_void_p),
+                ("values", C.c_void_p), ("b", C.c_void_p), ("x", C.c_void_p), ("zero_guess", C.c_int),
+                ("stream", C.c_void_p)]
+
+
+LINEAR_SOLVE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(DeviceSystem), C.POINTER(LinearParams),
+                              C.POINTER(C.c_int))
 
 
 class EnvStats(C.Structure):
@@ -151,6 +165,7 @@ def lib():
     L.sdx_set_profiling.argtypes = [_vp, C.c_int]
     L.sdx_get_profile.argtypes = [_vp, C.POINTER(Profile)]
     L.sdx_pcg_cluster_shape.argtypes = [C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.sdx_set_linear_solver.argtypes = [_vp, _vp, _vp]
     _fp_ = C.POINTER(C.c_float)
     L.sdx_mlp_init.argtypes = [_vp, C.c_uint64]
     L.sdx_mlp_set_params.argtypes = [_vp, _fp_, C.c_int]

@@ -19,7 +19,6 @@
 #include "../../include/sdx_b200.h"
 #include "sdx_internal.cuh"
 #include "sdx_mlp.cuh"
-#include "sdx_plain.cuh"
 #include <random>
 
 using namespace sdx;
@@ -44,6 +43,19 @@ namespace sdx {
 int record_error(int code, const char* msg, const char* detail) {
   g_last_error = detail ? std::string(msg) + ": " + detail : std::string(msg);
   return code;
+}
+
+// Bound of the grid-barrier spins of the PCG kernels (iterations of a poll with a 32 ns back-off, about
+// 2 s at the default). SDX_DEBUG_SPIN_LIMIT, read at each solve, can only lower it: a test sets it to a
+// few polls so that a wait runs out and the SDX_ERR_DEVICE_TIMEOUT path is exercised.
+constexpr long long kSpinLimit = 1ll << 26;
+long long device_spin_limit() {
+  const char* e = getenv("SDX_DEBUG_SPIN_LIMIT");
+  if (e) {
+    const long long v = atoll(e);
+    if (v > 0 && v < kSpinLimit) return v;
+  }
+  return kSpinLimit;
 }
 }  // namespace sdx
 
@@ -259,7 +271,14 @@ struct sdx_context {
   int* env_nrows = nullptr;    // padded rows per env (device)
   int* env_soff = nullptr;     // per env, its first slice (device, n_envs + 1): the cluster PCG's env ranges
   int* cl_envs = nullptr;      // the cluster PCG's env queue (device, n_envs)
-  std::unique_ptr<PlainSolver> plain;  // the plain FP64 comparison solver, built on first use
+  // external linear solver (sdx_set_linear_solver): the hook and its user-order copy of each Newton system
+  sdx_linear_solve_fn ext_fn = nullptr;
+  void* ext_user = nullptr;
+  int64_t* ext_rp = nullptr;   // user block pattern row_ptr (device)
+  int32_t* ext_col = nullptr;  // user block pattern columns (device)
+  int* ext_pos = nullptr;      // sliced-ELL block position of each user block (device)
+  float* ext_val = nullptr;    // 9 values per user block (device)
+  double *ext_b = nullptr, *ext_x = nullptr;  // b and x in user node order (device)
   // state snapshots (device-resident), keyed by handle
   std::map<uint64_t, Snapshot> snaps;
   uint64_t snap_next = 1;
@@ -347,7 +366,12 @@ static void prof_resolve(sdx_context* c) {
 }
 
 static void release_topology(sdx_context* c) {
-  c->plain.reset();
+  dfree(c->ext_rp);
+  dfree(c->ext_col);
+  dfree(c->ext_pos);
+  dfree(c->ext_val);
+  dfree(c->ext_b);
+  dfree(c->ext_x);
   c->part_dyn.release();
   dfree(c->env_nrows);
   dfree(c->env_soff);
@@ -754,7 +778,7 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
   a.out_conv = W.out_conv;
   a.sync = W.sync;
   a.env_rel_tol = env_rel_tol;
-  a.spin_limit = 1ll << 26;
+  a.spin_limit = kSpinLimit;  // the cluster kernel keeps the default bound
   a.es = W.es;
   // re-partitioning applies to batches on the context matrix (SDX_PCG_REPART=0 disables it)
   static const bool repart_on = [] {
@@ -862,6 +886,7 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
     }
   }
   int64_t target = repart_target(rows);
+  a.spin_limit = device_spin_limit();
   for (;;) {
     a.cta_slice = part->cta_slice;
     a.slice_list = part->slice_list;
@@ -921,7 +946,7 @@ extern "C" void sdx_default_linear_params(sdx_linear_params* p) {
   p->abort_if_not_spd = 0;
   p->polak_ribiere = 1;
   p->replace_every = 32;
-  p->solver_impl = SDX_SOLVER_FUSED;
+  p->value_layout = SDX_BSR_ROW_STRIPS;
 }
 
 extern "C" void sdx_default_step_params(sdx_step_params* p) {
@@ -2100,36 +2125,75 @@ static int capture_samples(sdx_context* c, const std::vector<uint8_t>& mask) {
   return SDX_OK;
 }
 
-// The plain FP64 comparison solver (sdx_plain.cu) on the envs in mask: builds its FP64 BSR structure on
-// first use, converts the assembled values, and solves env after env into c->dx.
-static int run_plain(sdx_context* c, const std::vector<uint8_t>& mask, const sdx_linear_params& lp, bool zero,
-                     std::vector<int>& it_out) {
-  if (!c->plain) {
-    PlainTopology t;
-    t.n_envs = c->n_envs;
-    t.row_off = c->h_row_off;
-    t.node_off = c->h_node_off;
-    t.prow = c->h_prow.data();
-    t.pcol = c->h_pcol.data();
-    t.row_of_node = c->h_row_of_node.data();
-    t.slice_ptr = c->h_slice_ptr.data();
-    auto ps = std::make_unique<PlainSolver>();
-    const int rc = ps->build(t);
-    if (rc != 0) return set_error(rc == -1 ? SDX_ERR_OUT_OF_MEMORY : SDX_ERR_CUDA, "plain solver set-up failed (%d)", rc);
-    c->plain = std::move(ps);
+__global__ void k_sell_to_user_bsr(int64_t nnzb, const int* __restrict__ pos, const float* __restrict__ val,
+                                   float* __restrict__ out) {
+  const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (b >= nnzb) return;
+  const int p = pos[b];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) out[9 * b + e] = val[val_index(p, e)];
+}
+
+// The Newton solve through the caller's hook (sdx_set_linear_solver): the assembled matrix, g and the
+// start vector go out in user node order (block pattern of sdx_get_pattern, SDX_BSR_BLOCKS values), the
+// hook solves the envs in mask, and its x comes back as the update dx.
+static int run_external(sdx_context* c, const std::vector<uint8_t>& mask, const sdx_linear_params& lp, bool zero,
+                        std::vector<int>& it_out) {
+  if (!c->ext_pos) {
+    std::vector<int> pos(c->nnzb);
+    for (int64_t i = 0; i < c->n_nodes; ++i) {
+      const int64_t r = c->h_row_of_node[i];
+      for (int64_t k = c->h_prow[i]; k < c->h_prow[i + 1]; ++k)
+        pos[k] = c->h_slice_ptr[r / kSlice] + (int)(k - c->h_prow[i]) * kSlice + (int)(r % kSlice);
+    }
+    SDX_TRY(upload(&c->ext_pos, pos));
+    SDX_TRY(upload(&c->ext_rp, c->h_prow));
+    SDX_TRY(upload(&c->ext_col, c->h_pcol));
+    SDX_TRY(dalloc(&c->ext_val, (size_t)9 * c->nnzb));
+    SDX_TRY(dalloc(&c->ext_b, (size_t)3 * c->n_nodes));
+    SDX_TRY(dalloc(&c->ext_x, (size_t)3 * c->n_nodes));
   }
-  if (lp.preconditioner == SDX_PREC_BLOCK_JACOBI)
-    return set_error(SDX_ERR_UNSUPPORTED, "the plain FP64 solver supports the Jacobi and no preconditioner");
   cudaEvent_t ev;
   prof_begin(c, &ev);
-  std::vector<int> conv;
-  const int rc = c->plain->solve(c->val, c->g, c->dx, mask.data(), lp, zero, c->stream, it_out, conv);
+  k_sell_to_user_bsr<<<(unsigned)((c->nnzb + 255) / 256), 256, 0, c->stream>>>(c->nnzb, c->ext_pos, c->val,
+                                                                                c->ext_val);
+  const unsigned nb = (unsigned)((c->n_nodes + 255) / 256);
+  k_gather_rows<<<nb, 256, 0, c->stream>>>(c->n_nodes, c->row_of_node, c->g, c->ext_b);
+  k_gather_rows<<<nb, 256, 0, c->stream>>>(c->n_nodes, c->row_of_node, c->dx, c->ext_x);
+  c->launches += 3;
+  sdx_device_system sys;
+  sys.n_envs = c->n_envs;
+  sys.node_offsets = c->h_node_off.data();
+  sys.env_mask = mask.data();
+  sys.n_nodes = c->n_nodes;
+  sys.nnzb = c->nnzb;
+  sys.row_ptr = c->ext_rp;
+  sys.col = c->ext_col;
+  sys.values = c->ext_val;
+  sys.b = c->ext_b;
+  sys.x = c->ext_x;
+  sys.zero_guess = zero ? 1 : 0;
+  sys.stream = (void*)c->stream;
+  std::fill(it_out.begin(), it_out.end(), 0);
+  const int rc = c->ext_fn(c->ext_user, &sys, &lp, it_out.data());
+  if (rc != SDX_OK) return set_error(rc, "external linear solver returned %d", rc);
+  // envs outside the mask keep their update: the solved envs' rows come back (padding rows as zero)
+  SDX_CUDA(cudaMemsetAsync(c->uscratch, 0, sizeof(double) * 3 * c->n_rows, c->stream));
+  k_scatter_rows<<<nb, 256, 0, c->stream>>>(c->n_nodes, c->row_of_node, c->ext_x, c->uscratch);
+  launch_copy_rows(c->n_slices, c->slice_env, c->env_mask, c->uscratch, c->dx, c->stream);
+  c->launches += 2;
   prof_end(c, PROF_PCG, ev);
-  if (rc != 0) return set_error(SDX_ERR_CUDA, "plain solver failed (%d)", rc);
   if (c->profiling) {
     c->prof.pcg_iters += *std::max_element(it_out.begin(), it_out.end());
     c->prof.pcg_launches++;
   }
+  return SDX_OK;
+}
+
+extern "C" int sdx_set_linear_solver(sdx_context* c, sdx_linear_solve_fn fn, void* user) {
+  if (!c) return set_error(SDX_ERR_INVALID_ARGUMENT, "null context");
+  c->ext_fn = fn;
+  c->ext_user = fn ? user : nullptr;
   return SDX_OK;
 }
 
@@ -2254,7 +2318,7 @@ static int step_once(sdx_context* c) {
     SDX_TRY(upload_mask(c, mask));
     if (!first_pass) assemble_dev(c, c->u, c->ut, t_end, SDX_ASM_HESS | SDX_ASM_PSD, c->env_mask, false);
     // the launch-shape autotuner (opt-in) runs on the first solve, before any start vector is written
-    if (!c->pcg_tuned && p.linear.solver_impl != SDX_SOLVER_PLAIN_FP64) SDX_TRY(autotune_pcg(c, p.linear));
+    if (!c->pcg_tuned && !c->ext_fn) SDX_TRY(autotune_pcg(c, p.linear));
     // linear solve H dx = g, warm started from zero, the previous dx, or the learned prediction
     const bool learned = p.warm_start == SDX_WARM_LEARNED;
     const bool collect = c->collect_per_solve > 0 && c->ds_n < c->ds_cap;
@@ -2298,8 +2362,8 @@ static int step_once(sdx_context* c) {
     if (p.ew_forcing == 2)
       SDX_CUDA(cudaMemcpyAsync(c->work.env_rel_tol, eta.data(), sizeof(double) * E, cudaMemcpyHostToDevice, c->stream));
     std::vector<int> it_out(E);
-    if (p.linear.solver_impl == SDX_SOLVER_PLAIN_FP64) {
-      SDX_TRY(run_plain(c, mask, p.linear, zero, it_out));
+    if (c->ext_fn) {
+      SDX_TRY(run_external(c, mask, p.linear, zero, it_out));
     } else {
       SDX_TRY(run_pcg(c, ctx_matrix(c), c->diag_pos, E, c->part, c->work, c->g, c->dx, c->env_mask, n_active,
                       p.linear, zero, p.ew_forcing == 2 ? c->work.env_rel_tol : nullptr, /*scale_guess*/ !zero,
@@ -2442,6 +2506,8 @@ extern "C" int sdx_pcg_solve_ctx(sdx_context* c, int n, int64_t nnzb, const int6
   if (!c || n <= 0 || nnzb <= 0 || !row_ptr || !bcol || !values || !b || !x || !lp || !status)
     return set_error(SDX_ERR_INVALID_ARGUMENT, "null or empty argument to sdx_pcg_solve");
   if (value_type != SDX_F32 && value_type != SDX_F64) return set_error(SDX_ERR_INVALID_ARGUMENT, "value_type");
+  if (lp->value_layout != SDX_BSR_ROW_STRIPS && lp->value_layout != SDX_BSR_BLOCKS)
+    return set_error(SDX_ERR_INVALID_ARGUMENT, "value_layout");
   if (lp->preconditioner < 0 || lp->preconditioner > 2) return set_error(SDX_ERR_INVALID_ARGUMENT, "preconditioner");
   if (lp->max_iter <= 0) return set_error(SDX_ERR_INVALID_ARGUMENT, "max_iter must be positive");
   if (row_ptr[0] != 0 || row_ptr[n] != nnzb) return set_error(SDX_ERR_INVALID_ARGUMENT, "row_ptr inconsistent with nnzb");
@@ -2483,7 +2549,8 @@ extern "C" int sdx_pcg_solve_ctx(sdx_context* c, int n, int64_t nnzb, const int6
   SDX_CUDA(cudaMemcpyAsync(c->solo_slice_ptr, sp.data(), sizeof(int) * (ns + 1), cudaMemcpyHostToDevice, c->stream));
   SDX_CUDA(cudaMemcpyAsync(c->solo_slice_w, sw.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, c->stream));
   SDX_CUDA(cudaMemcpyAsync(c->solo_slice_env, se.data(), sizeof(int) * ns, cudaMemcpyHostToDevice, c->stream));
-  // upload BSR (FP32) and convert on device (the reference converts to cuSPARSE BSR, cuda_bsr_matrix.cu:22-63)
+  // upload BSR (FP32) and convert on device, from the reference's row strips or from contiguous blocks (the
+  // reference converts its row strips to cuSPARSE BSR the same way, cuda_bsr_matrix.cu:22-63)
   int64_t* drp = nullptr;
   int32_t* dbc = nullptr;
   float* dbv = nullptr;
@@ -2503,7 +2570,8 @@ extern "C" int sdx_pcg_solve_ctx(sdx_context* c, int n, int64_t nnzb, const int6
   } else {
     SDX_CUDA(cudaMemcpyAsync(dbv, values, sizeof(float) * 9 * nnzb, cudaMemcpyHostToDevice, c->stream));
   }
-  launch_bsr_to_sell(rows, drp, dbc, dbv, c->solo_slice_ptr, c->solo_col, c->solo_val, c->solo_diag, c->stream);
+  launch_bsr_to_sell(rows, drp, dbc, dbv, lp->value_layout == SDX_BSR_ROW_STRIPS, c->solo_slice_ptr, c->solo_col,
+                     c->solo_val, c->solo_diag, c->stream);
   c->launches++;
   std::vector<double> hb((size_t)3 * rows, 0.0), hx((size_t)3 * rows, 0.0);
   std::copy(b, b + 3 * (size_t)n, hb.begin());

@@ -119,7 +119,7 @@ constexpr int kContactCinf = 32;           // CoulombFrictionModel::CinfRegulari
 
 // CG scalars of one env carried across a re-partitioning relaunch
 struct EnvSave {
-  double rz, beta, bb, conv_thr, div_thr;
+  double rz, beta, bb, conv_thr, div_thr, rr;
   int first, status;
 };
 
@@ -213,7 +213,7 @@ cudaError_t launch_pcg(const PcgArgs& a, int n_cta, int threads, cudaStream_t st
 ClusterShape pcg_cluster_shape(int n_envs);
 cudaError_t launch_pcg_cluster(const PcgArgs& a, ClusterShape shape, cudaStream_t st);
 void launch_spmv(const Matrix& A, const float4* x, float* y, int threads, cudaStream_t st);
-void launch_bsr_to_sell(int n_rows, const int64_t* row_ptr, const int32_t* bcol, const float* bval,
+void launch_bsr_to_sell(int n_rows, const int64_t* row_ptr, const int32_t* bcol, const float* bval, bool strips,
                         const int* slice_ptr, int* col, float* val, int* diag_pos, cudaStream_t st);
 void launch_pack_z(int64_t n_rows, const double* x, float4* z, cudaStream_t st);
 int pcg_shared_bytes(int threads, int wstride = kPcgMaxEnvsPerCta);

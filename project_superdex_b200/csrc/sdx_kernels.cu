@@ -753,11 +753,14 @@ void launch_spmv(const Matrix& A, const float4* x, float* y, int threads, cudaSt
 }
 
 // ------------------------------------------------------------------------------------------------
-// BSR (row-major 3x3 blocks, FP32) -> SELL-32. One thread per block row.
+// BSR (FP32) -> SELL-32. One thread per block row. Values either as contiguous row-major 3x3 blocks, or
+// as the reference's row strips (strips = true): block row br with len blocks is one row-major 3 x 3len
+// strip at 9 row_ptr[br], entry (lr, lc) of its k-th block at 3 (lr len + k) + lc (block_sparse_matrix.h:
+// 459-475).
 
 __global__ void k_bsr_to_sell(int n_rows, const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ bcol,
-                              const float* __restrict__ bval, const int* __restrict__ slice_ptr, int* col,
-                              float* val, int* diag_pos) {
+                              const float* __restrict__ bval, int strips, const int* __restrict__ slice_ptr,
+                              int* col, float* val, int* diag_pos) {
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
   if (row >= n_rows) return;
   const int s = row >> 5, lane = row & 31;
@@ -772,7 +775,8 @@ __global__ void k_bsr_to_sell(int n_rows, const int64_t* __restrict__ row_ptr, c
       col[p] = j;
       if (j == row) diag_pos[row] = p;
 #pragma unroll
-      for (int e = 0; e < 9; ++e) val[val_index(p, e)] = bval[9 * (b0 + k) + e];
+      for (int e = 0; e < 9; ++e)
+        val[val_index(p, e)] = strips ? bval[9 * b0 + 3 * ((e / 3) * len + k) + e % 3] : bval[9 * (b0 + k) + e];
     } else {
       col[p] = row | kPadBit;
 #pragma unroll
@@ -781,11 +785,11 @@ __global__ void k_bsr_to_sell(int n_rows, const int64_t* __restrict__ row_ptr, c
   }
 }
 
-void launch_bsr_to_sell(int n_rows, const int64_t* row_ptr, const int32_t* bcol, const float* bval,
+void launch_bsr_to_sell(int n_rows, const int64_t* row_ptr, const int32_t* bcol, const float* bval, bool strips,
                         const int* slice_ptr, int* col, float* val, int* diag_pos, cudaStream_t st) {
   if (n_rows == 0) return;
-  k_bsr_to_sell<<<(n_rows + 127) / 128, 128, 0, st>>>(n_rows, row_ptr, bcol, bval, slice_ptr, col, val,
-                                                       diag_pos);
+  k_bsr_to_sell<<<(n_rows + 127) / 128, 128, 0, st>>>(n_rows, row_ptr, bcol, bval, strips ? 1 : 0, slice_ptr, col,
+                                                       val, diag_pos);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -803,6 +807,7 @@ void launch_bsr_to_sell(int n_rows, const int64_t* row_ptr, const int32_t* bcol,
 
 struct EnvState {
   double rz, alpha, beta, conv_thr, div_thr, bb;
+  double rr;   // the latest checked r.r (reported on a non-SPD abort, as pcg.h:152-169 reports it)
   int status;  // 0 active, 1 converged, 2 stopped, 3 diverged, 4 not requested, 5 diverging
   int first;
 };
@@ -1087,6 +1092,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     if (a.resume) {  // continue a re-partitioned solve: the CG scalars saved at the previous exit
       const EnvSave& sv = a.es[s_env[le]];
       st[le].rz = sv.rz;
+      st[le].rr = sv.rr;
       st[le].beta = sv.beta;
       st[le].bb = sv.bb;
       st[le].conv_thr = sv.conv_thr;
@@ -1300,6 +1306,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
       st[le].conv_thr = fmax(a.abs_tol * a.abs_tol, (bb * rt) * rt);
       st[le].div_thr = (bb * a.rel_div_tol) * a.rel_div_tol;
       st[le].rz = tot[le][2];
+      st[le].rr = rr;
       if (!isfinite(rr) || rr > st[le].div_thr) {
         st[le].status = 3;
         finish_env(le, 0, rr);
@@ -1476,9 +1483,9 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     mark(3);
     reduce_tot(3, 0);
     for (int le = threadIdx.x; le < ne; le += blockDim.x) {
-      if (st[le].status == 5) {
+      if (st[le].status == 5) {  // non-SPD abort: the residual of the last completed iteration
         st[le].status = 3;
-        finish_env(le, it, 0.0);
+        finish_env(le, it, st[le].rr);
         continue;
       }
       if (st[le].status != 0) continue;
@@ -1509,6 +1516,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
       const double bpr = (a.polak_ribiere && !st[le].first) ? rzo : 0.0;
       st[le].beta = (rzn - bpr) / st[le].rz;
       st[le].rz = rzn;
+      st[le].rr = rr;
       st[le].first = 0;
     }
     __syncthreads();
@@ -1520,6 +1528,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
         if (a.env_cta0[e] != c) continue;
         EnvSave sv;
         sv.rz = st[le].rz;
+        sv.rr = st[le].rr;
         sv.beta = st[le].beta;
         sv.bb = st[le].bb;
         sv.conv_thr = st[le].conv_thr;
@@ -1876,10 +1885,9 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
       }
       const double pq = s_tot[0];
       const double al = rz / pq;
-      if (pq <= 0.0 && a.abort_spd) {  // non-SPD abort (pcg.h:152-169): x keeps the previous iterate
-        it_done = it;
+      if (pq <= 0.0 && a.abort_spd) {  // non-SPD abort (pcg.h:152-169): x keeps the previous iterate and
+        it_done = it;                  // the reported residual is the last completed iteration's
         status = 3;
-        rr = 0.0;
         break;
       }
       const bool replace = (verify_it > 0 && verify_it == it - 1) || (a.replace_every > 0 && it % a.replace_every == 0);

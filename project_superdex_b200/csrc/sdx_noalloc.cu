@@ -56,9 +56,11 @@ struct Out {
 
 struct Args {
   int n;  // block rows
+  int64_t nnzb;
   const int64_t* row_ptr;
   const int32_t* col;
-  const float* val;  // 9 per block, row-major
+  const float* val;  // 9 per block: row-major blocks, or the row strips of SDX_BSR_ROW_STRIPS
+  int strips;        // 1: entry (lr, lc) of block k of a row is val[9 ptr + 3 (lr len + k) + lc]
   const double* b;
   double* x;
   unsigned char* scratch;
@@ -74,7 +76,10 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// Thread 0's verdict (passed, or the error word set) is broadcast through shared memory, so every thread
+// of a CTA returns the same value even when another CTA sets the error word meanwhile.
 __device__ __forceinline__ bool grid_barrier(unsigned* sync, unsigned nblocks, long long spin_limit) {
+  __shared__ unsigned s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned* vgen = sync + 1;
@@ -96,27 +101,47 @@ __device__ __forceinline__ bool grid_barrier(unsigned* sync, unsigned nblocks, l
       }
     }
     __threadfence();
+    s_ok = *((volatile unsigned*)(sync + 2)) == 0u ? 1u : 0u;
   }
   __syncthreads();
-  return *((volatile unsigned*)(sync + 2)) == 0u;
+  return s_ok != 0u;
+}
+
+// Block range [b0, b1) of a row. A range outside [0, nnzb) or with b1 < b0 (a malformed row_ptr) is
+// flagged in *bad and treated as empty, so no load leaves the caller's arrays.
+__device__ __forceinline__ void row_range(const Args& a, int row, int64_t& b0, int64_t& b1, int* bad) {
+  b0 = a.row_ptr[row];
+  b1 = a.row_ptr[row + 1];
+  if (b0 < 0 || b1 < b0 || b1 > a.nnzb) {
+    *bad = 1;
+    b0 = b1 = 0;
+  }
+}
+
+// Entry e (= 3 lr + lc) of the k-th block of a row whose blocks are [b0, b1).
+__device__ __forceinline__ float block_entry(const Args& a, int64_t b0, int64_t b1, int64_t k, int e) {
+  return a.strips ? a.val[9 * b0 + 3 * ((e / 3) * (b1 - b0) + k) + e % 3] : a.val[9 * (b0 + k) + e];
 }
 
 // y_row = A_row . v for one block row; v is read through L2 (it is written by other CTAs)
 template <class V>
 __device__ __forceinline__ void row_product(const Args& a, int row, V load, double acc[3], int* bad) {
   acc[0] = acc[1] = acc[2] = 0.0;
-  for (int64_t k = a.row_ptr[row]; k < a.row_ptr[row + 1]; ++k) {
+  int64_t b0, b1;
+  row_range(a, row, b0, b1, bad);
+  for (int64_t k = b0; k < b1; ++k) {
     const int j = a.col[k];
     if (j < 0 || j >= a.n) {
       *bad = 1;
       continue;
     }
-    const float* blk = a.val + 9 * k;
     double xj[3];
     load(j, xj);
 #pragma unroll
     for (int r = 0; r < 3; ++r)
-      acc[r] += (double)blk[3 * r] * xj[0] + (double)blk[3 * r + 1] * xj[1] + (double)blk[3 * r + 2] * xj[2];
+      acc[r] += (double)block_entry(a, b0, b1, k - b0, 3 * r) * xj[0] +
+                (double)block_entry(a, b0, b1, k - b0, 3 * r + 1) * xj[1] +
+                (double)block_entry(a, b0, b1, k - b0, 3 * r + 2) * xj[2];
   }
 }
 
@@ -194,9 +219,13 @@ __global__ void k_pcg_noalloc(Args a) {
     const int row = s * kSlice + lane;
     if (row >= a.n) continue;
     float blk[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int64_t k = a.row_ptr[row]; k < a.row_ptr[row + 1]; ++k)
+    int64_t b0, b1;
+    row_range(a, row, b0, b1, &bad);
+    if (row == 0 && b0 != 0) bad = 1;
+    if (row == a.n - 1 && a.row_ptr[a.n] != a.nnzb) bad = 1;
+    for (int64_t k = b0; k < b1; ++k)
       if (a.col[k] == row)
-        for (int e = 0; e < 9; ++e) blk[e] = a.val[9 * k + e];
+        for (int e = 0; e < 9; ++e) blk[e] = block_entry(a, b0, b1, k - b0, e);
     if (a.precond == 1) {
       for (int k = 0; k < 3; ++k) D[9 * row + k] = blk[4 * k] != 0.0f ? 1.0f / blk[4 * k] : 0.0f;
     } else if (a.precond == 2) {
@@ -230,13 +259,17 @@ __global__ void k_pcg_noalloc(Args a) {
     precondition(a, D, row, r, z);
     for (int k = 0; k < 3; ++k) R[3 * row + k] = r[k];
     Z[row] = make_float4(z[0], z[1], z[2], 0.0f);
-    const double b0 = a.b[3 * row], b1 = a.b[3 * row + 1], b2 = a.b[3 * row + 2];
-    acc[0] += b0 * b0 + b1 * b1 + b2 * b2;
+    const double bx = a.b[3 * row], by = a.b[3 * row + 1], bz = a.b[3 * row + 2];
+    acc[0] += bx * bx + by * by + bz * bz;
     acc[1] += r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
     acc[2] += r[0] * z[0] + r[1] * z[1] + r[2] * z[2];
   }
+  if (bad) atomicExch(&out->bad_index, 1);
   cta_reduce(3, 0);
   if (!grid_barrier(sync, ncta, a.spin_limit)) return;
+  // a malformed matrix (row_ptr or a column index) stops every CTA before the iteration: each reads the
+  // word after the barrier that ordered all set-up writes
+  if (*((volatile int*)&out->bad_index) != 0) return;
   grid_total(3, 0);
   const double bb = tot[0];
   const double conv_thr = fmax(a.abs_tol * a.abs_tol, (bb * a.rel_tol) * a.rel_tol);
@@ -358,6 +391,7 @@ using namespace sdx_noalloc;
 
 namespace sdx {
 int record_error(int code, const char* msg, const char* detail);  // sets sdx_last_error() (sdx_host.cu)
+long long device_spin_limit();                                     // bound of the device spins (sdx_host.cu)
 }
 
 static int fail(int code, const char* msg, cudaError_t e = cudaSuccess) {
@@ -371,6 +405,8 @@ extern "C" int sdx_pcg_solve_device_noalloc(int block_rows, int64_t nnzb, const 
   if (!d_row_ptr || !d_col || !d_values || !d_b || !d_x || !params || !status)
     return fail(SDX_ERR_INVALID_ARGUMENT, "null argument");
   if (block_rows <= 0 || nnzb <= 0) return fail(SDX_ERR_INVALID_ARGUMENT, "empty system");
+  if (params->value_layout != SDX_BSR_ROW_STRIPS && params->value_layout != SDX_BSR_BLOCKS)
+    return fail(SDX_ERR_INVALID_ARGUMENT, "value_layout");
   static_assert(kMaxBlockRows == SDX_NOALLOC_MAX_BLOCK_ROWS, "limit must match the header");
   if (block_rows > kMaxBlockRows)
     return fail(SDX_ERR_INVALID_ARGUMENT, "system larger than the no-allocation limit of 65536 block rows");
@@ -406,6 +442,8 @@ extern "C" int sdx_pcg_solve_device_noalloc(int block_rows, int64_t nnzb, const 
   Args a;
   memset(&a, 0, sizeof(a));
   a.n = block_rows;
+  a.nnzb = nnzb;
+  a.strips = params->value_layout == SDX_BSR_ROW_STRIPS;
   a.row_ptr = d_row_ptr;
   a.col = d_col;
   a.val = d_values;
@@ -421,7 +459,7 @@ extern "C" int sdx_pcg_solve_device_noalloc(int block_rows, int64_t nnzb, const 
   a.replace_every = params->replace_every > 0 ? params->replace_every : 32;
   a.zero_guess = hint == SDX_GUESS_ZERO;
   a.abort_spd = params->abort_if_not_spd;
-  a.spin_limit = 1ll << 26;
+  a.spin_limit = sdx::device_spin_limit();
   void* kargs[] = {&a};
   e = cudaLaunchCooperativeKernel((const void*)k_pcg_noalloc, dim3(g_ctas[dev]), dim3(kThreads), kargs, 0, st);
   if (e != cudaSuccess) return fail(SDX_ERR_CUDA, "cooperative launch", e);
@@ -433,7 +471,7 @@ extern "C" int sdx_pcg_solve_device_noalloc(int block_rows, int64_t nnzb, const 
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return fail(SDX_ERR_CUDA, "result copy", e);
   if (flags[2] != 0u) return fail(SDX_ERR_DEVICE_TIMEOUT, "grid barrier timed out");
-  if (out.bad_index) return fail(SDX_ERR_INVALID_ARGUMENT, "column index out of range");
+  if (out.bad_index) return fail(SDX_ERR_INVALID_ARGUMENT, "row_ptr or a column index out of range");
   status->num_iter = out.iters;
   status->residual_norm = out.res;
   status->relative_residual_norm = out.relres;

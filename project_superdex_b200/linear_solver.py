@@ -67,17 +67,60 @@ class LinearSolverStatus:
     convergence: LinearSolverConvergenceStatus
 
 
+class ValueLayout(enum.IntEnum):
+    """Order of the 9 * nnzb values of a 3x3 block CSR matrix."""
+
+    RowStrips = capi.SDX_BSR_ROW_STRIPS  # BlockSparseMatrix<T,3>::Values() (block_sparse_matrix.h:459-475)
+    Blocks = capi.SDX_BSR_BLOCKS         # 9 contiguous row-major values per block (cuSPARSE BSR)
+
+
 @dataclasses.dataclass
 class BlockSparseMatrix:
-    """3x3 block CSR (block-contiguous row-major blocks)."""
+    """3x3 block CSR, as the reference's BlockSparseMatrix<T,3> (block_sparse_matrix.h:63): Pointers(),
+    Indices() and Values(). By default the values are in the reference's own row-strip layout: block row br
+    with nb blocks is one row-major 3 x 3nb strip at 9 row_ptr[br], entry (lr, lc) of its k-th block at
+    3 (lr nb + k) + lc. `layout=ValueLayout.Blocks` takes contiguous 3x3 blocks instead."""
 
-    row_ptr: np.ndarray  # int64, block_rows + 1
+    row_ptr: np.ndarray  # int64 (or int32), block_rows + 1
     col: np.ndarray      # int32, nnzb
-    values: np.ndarray   # (nnzb, 3, 3) float32 or float64
+    values: np.ndarray   # 9 * nnzb float32 or float64 (any shape) in `layout`
+    layout: ValueLayout = ValueLayout.RowStrips
 
     @property
     def block_rows(self) -> int:
         return int(self.row_ptr.size - 1)
+
+    @staticmethod
+    def from_blocks(row_ptr, col, blocks, layout: ValueLayout = ValueLayout.RowStrips) -> "BlockSparseMatrix":
+        """Matrix from (nnzb, 3, 3) blocks, its values stored in `layout`."""
+        blocks = np.asarray(blocks).reshape(-1, 3, 3)
+        if layout == ValueLayout.Blocks:
+            return BlockSparseMatrix(np.asarray(row_ptr), np.asarray(col), blocks.reshape(-1).copy(), layout)
+        return BlockSparseMatrix(np.asarray(row_ptr), np.asarray(col), blocks_to_strips(row_ptr, blocks), layout)
+
+
+def blocks_to_strips(row_ptr, blocks) -> np.ndarray:
+    """Values of (nnzb, 3, 3) blocks in the reference's row-strip order."""
+    row_ptr = np.asarray(row_ptr, np.int64)
+    blocks = np.asarray(blocks).reshape(-1, 3, 3)
+    out = np.empty(9 * blocks.shape[0], blocks.dtype)
+    for br in range(row_ptr.size - 1):
+        b0, b1 = int(row_ptr[br]), int(row_ptr[br + 1])
+        # strip[lr, 3k + lc] = block k [lr, lc]
+        out[9 * b0:9 * b1] = blocks[b0:b1].transpose(1, 0, 2).reshape(-1)
+    return out
+
+
+def strips_to_blocks(row_ptr, values) -> np.ndarray:
+    """(nnzb, 3, 3) blocks of values in the reference's row-strip order."""
+    row_ptr = np.asarray(row_ptr, np.int64)
+    values = np.asarray(values).reshape(-1)
+    nnzb = int(row_ptr[-1])
+    out = np.empty((nnzb, 3, 3), values.dtype)
+    for br in range(row_ptr.size - 1):
+        b0, b1 = int(row_ptr[br]), int(row_ptr[br + 1])
+        out[b0:b1] = values[9 * b0:9 * b1].reshape(3, b1 - b0, 3).transpose(1, 0, 2)
+    return out
 
 
 class LinearSolver:
@@ -122,6 +165,7 @@ class LinearSolver:
             raise ValueError("b and x must be float64 vectors of length 3 * block_rows")
         st = capi.LinearStatus()
         prm = self.params.to_c()
+        prm.value_layout = int(A.layout)
         rc = capi.lib().sdx_pcg_solve_ctx(self._ctx, n, col.size, capi.ptr(row_ptr, capi._lp),
                                           capi.ptr(col, capi._ip), vals.ctypes.data_as(C.c_void_p), vt,
                                           capi.ptr(b), capi.ptr(x), int(hint), C.byref(prm), C.byref(st))

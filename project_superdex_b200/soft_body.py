@@ -77,6 +77,11 @@ class SoftBodyWorld:
         capi.check(L.sdx_get_sizes(self._ctx, *[C.byref(s) for s in sizes]))
         self.n_tets, self.nnzb, self.n_faces = sizes[1].value, sizes[2].value, sizes[3].value
 
+    def set_linear_solver(self, fn, user=None):
+        """Hand every Newton solve of step() to an external solver: fn is the address of a C function of
+        type sdx_linear_solve_fn (None: this library's PCG)."""
+        capi.check(capi.lib().sdx_set_linear_solver(self._ctx, fn, user))
+
     def close(self):
         if getattr(self, "_ctx", None):
             capi.lib().sdx_destroy(self._ctx)

@@ -8,6 +8,10 @@ exists; the fixtures are committed, nothing reads the reference at test time).
     (st_venant_kirchhoff_test_data, E = 1, nu = 0.4).
   * krylov_psd100.json — the reference's 100 x 100 SPD golden system (matrix, rhs, solution) from
     mochi_core/test/data/krylov_solver_test_data.h, read as text.
+  * bsr3_reference.json — the reference's BlockSparseMatrix<double,3> storage layout and its krylov::PCG
+    on it (oracle/_ref): Values() of matrices filled through the class's own SetValue on seeded block
+    patterns, and the iteration counts / solutions of krylov::PCG with BlockJacobiPrec (none, Jacobi,
+    block Jacobi) on the 100 x 100 golden system in 3x3 blocks and on an assembled tet-grid Hessian.
   * reference_vectors.json — outputs of the reference's own compiled code (oracle/_ref, built by
     oracle/build_ref.sh from the reference sources) on seeded inputs: Smith NH with every PSD
     strategy (projected tangents), St. Venant-Kirchhoff and linear elasticity with every PSD strategy,
@@ -246,10 +250,70 @@ def reference_vectors():
     return out
 
 
+def bsr3_vectors():
+    """The reference's BSR3 value layout and its PCG on BSR3 matrices (oracle/_ref)."""
+    from oracle import oracle as O
+    from project_superdex_b200 import scenes
+    assert O.ref() is not None, "oracle/_ref/libsdx_ref.so missing: run oracle/build_ref.sh"
+    rng = np.random.default_rng(20261204)
+    out = {"layout": [], "pcg": []}
+    for nbr in (5, 17, 40):
+        ptr, idx = [0], []
+        for br in range(nbr):
+            cols = sorted(set([br] + rng.choice(nbr, size=int(rng.integers(0, 7)), replace=True).tolist()))
+            idx += cols
+            ptr.append(len(idx))
+        blocks = rng.normal(size=(len(idx), 9))
+        vals = O.ref_bsr3_values(ptr, idx, blocks)
+        out["layout"].append({"row_ptr": ptr, "col": idx, "blocks": blocks.reshape(-1).tolist(),
+                              "values": vals.tolist()})
+    # the 100 x 100 golden system in 3x3 blocks (padding rows: identity)
+    kr = parse_krylov(os.path.join(args_ns.mc, "test/data/krylov_solver_test_data.h"))
+    A = np.eye(102)
+    for r_, c_, v_ in zip(kr["rows"], kr["cols"], kr["vals"]):
+        A[r_, c_] = v_
+    b = np.zeros(102)
+    b[:100] = kr["rhs"]
+    systems = {"psd100": (A, b)}
+    # a projected Hessian and gradient of a seeded 4 x 3 x 3 tet grid (the oracle's assembly), FP32-rounded
+    body = scenes.grid_body(4, 3, 3, 0.01, rng=np.random.default_rng(5), nu=0.45)
+    body.E = np.exp(np.random.default_rng(6).uniform(np.log(1e4), np.log(1e6), size=body.n_tets))
+    sc = O.Scene(body, scenes.SceneConfig())
+    u = np.random.default_rng(7).normal(0, 5e-4, 3 * body.n_nodes) * (body.pin == 0).repeat(3)
+    a = sc.assemble(u, u - 1e-4, psd=True)
+    H = a["H"].astype(np.float32).astype(np.float64).reshape(-1, 3, 3)
+    Ad = np.zeros((3 * body.n_nodes, 3 * body.n_nodes))
+    for i in range(body.n_nodes):
+        for k in range(sc.row_ptr[i], sc.row_ptr[i + 1]):
+            j = sc.col[k]
+            Ad[3 * i:3 * i + 3, 3 * j:3 * j + 3] = H[k]
+    systems["tetgrid"] = (Ad, a["g"])
+    for name, (Ad, b) in systems.items():
+        nb = Ad.shape[0] // 3
+        ptr, idx, blocks = [0], [], []
+        for i in range(nb):
+            for j in range(nb):
+                blk = Ad[3 * i:3 * i + 3, 3 * j:3 * j + 3]
+                if np.any(blk != 0.0):
+                    idx.append(j)
+                    blocks.append(blk.reshape(-1))
+            ptr.append(len(idx))
+        vals = O.ref_bsr3_values(ptr, idx, np.asarray(blocks))
+        entry = {"system": name, "row_ptr": ptr, "col": idx, "values": vals.tolist(), "b": b.tolist(), "runs": []}
+        for prec in (0, 1, 2):
+            x, it, rn, rr, cv = O.ref_bsr3_pcg(ptr, idx, vals, b, rel_tol=1e-6, precond=prec)
+            entry["runs"].append({"precond": prec, "rel_tol": 1e-6, "iters": int(it), "convergence": int(cv),
+                                  "res_norm": rn, "rel_res_norm": rr, "x": x.tolist()})
+        out["pcg"].append(entry)
+    out["source"] = "oracle/_ref/libsdx_ref.so (reference BlockSparseMatrix, BlockJacobiPrec, krylov::PCG; FP64)"
+    return out
+
+
 def main():
     global args_ns
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference-root", default="/root/reference")
+    ap.add_argument("--only-bsr3", action="store_true")
     args_ns = ap.parse_args()
     args_ns.mc = os.path.join(args_ns.reference_root, "superdex_physics/libraries/mochi/mochi_core")
     with open(os.path.join(HERE, "smith_nh_reference.json"), "w") as f:
@@ -258,6 +322,10 @@ def main():
         json.dump(parse_stvk(os.path.join(args_ns.mc, "test/data/material_test_data.h")), f)
     with open(os.path.join(HERE, "krylov_psd100.json"), "w") as f:
         json.dump(parse_krylov(os.path.join(args_ns.mc, "test/data/krylov_solver_test_data.h")), f)
+    with open(os.path.join(HERE, "bsr3_reference.json"), "w") as f:
+        json.dump(bsr3_vectors(), f)
+    if "--only-bsr3" in sys.argv:
+        return
     with open(os.path.join(HERE, "reference_vectors.json"), "w") as f:
         json.dump(reference_vectors(), f)
     print("wrote fixtures to", HERE)

@@ -74,3 +74,16 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(capi, "LIB_PATH", str(tmp_path / "nope.so"))
     with pytest.raises(ImportError):
         capi.lib()
+
+
+def test_product_library_links_no_second_solver_backend():
+    """libsdx_b200.so has one linear solver: the cuSPARSE / cuBLAS comparison arm lives in the benchmark's
+    own library (bench_arms/libsdx_plain_fp64.so), plugged in through sdx_set_linear_solver."""
+    from project_superdex_b200 import capi
+    deps = subprocess.run(["ldd", capi.LIB_PATH], capture_output=True, text=True).stdout
+    assert "cusparse" not in deps and "cublas" not in deps
+    plain = os.path.join(ROOT, "bench_arms", "libsdx_plain_fp64.so")
+    if os.path.exists(plain):
+        out = subprocess.run(["nm", "-D", "--defined-only", plain], capture_output=True, text=True).stdout
+        for sym in ("sdx_plain_fp64_create", "sdx_plain_fp64_destroy", "sdx_plain_fp64_solve"):
+            assert f" T {sym}" in out

@@ -31,7 +31,7 @@ def test_newton_converges_to_rel_1e6(cfg1_world):
 def test_hessian_symmetric_and_linear_solve_true_residual(cfg1_world):
     import scipy.sparse as sp
     from project_superdex_b200.linear_solver import (BlockSparseMatrix, InitialGuessHint, KrylovSolverParams,
-                                                     LinearSolver)
+                                                     LinearSolver, ValueLayout)
     w, b, cfg = cfg1_world
     u, v, t = w.get_state()
     a = w.assemble(None, t=t + cfg.dt)
@@ -47,7 +47,7 @@ def test_hessian_symmetric_and_linear_solve_true_residual(cfg1_world):
     assert asym <= 1e-5 * abs(A).max()
     g = a["g"]
     x = np.zeros_like(g)
-    st = LinearSolver(KrylovSolverParams(relTol=1e-6, maxIter=20000)).Solve(BlockSparseMatrix(rp, col, a["H"]), g, x,
+    st = LinearSolver(KrylovSolverParams(relTol=1e-6, maxIter=20000)).Solve(BlockSparseMatrix(rp, col, a["H"], ValueLayout.Blocks), g, x,
                                                                             hint=InitialGuessHint.Zero)
     assert st.convergence == 1
     true_rel = np.linalg.norm(g - A @ x) / np.linalg.norm(g)

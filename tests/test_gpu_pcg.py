@@ -15,8 +15,73 @@ def _solver(**kw):
 
 
 def _bsr(rp, col, vals, dtype=np.float64):
+    """The matrix as the reference stores it: BlockSparseMatrix<T,3>::Values() row strips."""
     from project_superdex_b200.linear_solver import BlockSparseMatrix
-    return BlockSparseMatrix(rp, col, np.ascontiguousarray(vals, dtype))
+    return BlockSparseMatrix.from_blocks(rp, col, np.asarray(vals, dtype))
+
+
+def _capi_solve(rp, col, values, layout, b, prec, hint_zero=True, x0=None, value_type=None):
+    """sdx_pcg_solve called through the C-ABI as a reference-side binding would call it."""
+    import ctypes as C
+    from project_superdex_b200 import capi
+    lp = capi.default_linear_params()
+    lp.rel_tol, lp.abs_tol, lp.max_iter, lp.preconditioner, lp.value_layout = 1e-6, 1e-30, 10000, prec, layout
+    st = capi.LinearStatus()
+    rp64 = np.ascontiguousarray(rp, np.int64)
+    cl = np.ascontiguousarray(col, np.int32)
+    v = np.ascontiguousarray(values)
+    vt = capi.SDX_F64 if v.dtype == np.float64 else capi.SDX_F32
+    x = np.zeros_like(b) if x0 is None else np.array(x0, np.float64)
+    rc = capi.lib().sdx_pcg_solve(rp64.size - 1, cl.size, capi.ptr(rp64, capi._lp), capi.ptr(cl, capi._ip),
+                                  v.ctypes.data_as(C.c_void_p), vt, capi.ptr(np.ascontiguousarray(b)), capi.ptr(x),
+                                  capi.SDX_GUESS_ZERO if hint_zero else capi.SDX_GUESS_UNKNOWN, C.byref(lp),
+                                  C.byref(st))
+    capi.check(rc)
+    return x, st
+
+
+def test_reference_bsr3_matrices_through_the_c_abi(golden):
+    """The values exactly as the reference's BlockSparseMatrix<double,3>::Values() holds them (row strips,
+    filled through its own SetValue), solved through sdx_pcg_solve: the reference krylov::PCG's iteration
+    counts (with its BlockJacobiPrec: none, Jacobi, block Jacobi) and solutions, and the same result
+    bit for bit when the values are passed as contiguous blocks instead."""
+    from project_superdex_b200 import capi
+    from project_superdex_b200.linear_solver import strips_to_blocks
+    g = golden("bsr3_reference.json")
+    assert [s["system"] for s in g["pcg"]] == ["psd100", "tetgrid"]
+    for sysd in g["pcg"]:
+        rp, col = np.array(sysd["row_ptr"]), np.array(sysd["col"], np.int32)
+        vals, b = np.array(sysd["values"]), np.array(sysd["b"])
+        blocks = strips_to_blocks(rp, vals)
+        A = np.zeros((b.size, b.size))
+        for i in range(rp.size - 1):
+            for k in range(rp[i], rp[i + 1]):
+                A[3 * i:3 * i + 3, 3 * col[k]:3 * col[k] + 3] = blocks[k].astype(np.float32)
+        for run in sysd["runs"]:
+            x, st = _capi_solve(rp, col, vals, capi.SDX_BSR_ROW_STRIPS, b, run["precond"])
+            assert st.convergence == run["convergence"] == 1
+            assert abs(st.num_iter - run["iters"]) <= max(6, int(0.15 * run["iters"])), (sysd["system"], run["precond"],
+                                                                                        st.num_iter, run["iters"])
+            assert np.linalg.norm(b - A @ x) <= 1.01e-6 * np.linalg.norm(b)
+            if sysd["system"] == "tetgrid":
+                x_ref = np.array(run["x"])
+                np.testing.assert_allclose(x, x_ref, rtol=0, atol=2e-5 * np.abs(x_ref).max())
+            xb, stb = _capi_solve(rp, col, blocks.reshape(-1), capi.SDX_BSR_BLOCKS, b, run["precond"])
+            assert stb.num_iter == st.num_iter and np.array_equal(xb, x)
+
+
+def test_strip_layout_is_not_read_as_blocks(golden):
+    """A row-strip matrix declared as contiguous blocks is a different matrix: the layout flag matters for
+    every row with more than one block (the reference's Values() must not be passed as blocks)."""
+    from project_superdex_b200 import capi
+    sysd = golden("bsr3_reference.json")["pcg"][1]
+    rp, col, vals, b = np.array(sysd["row_ptr"]), np.array(sysd["col"], np.int32), np.array(sysd["values"]), np.array(sysd["b"])
+    x_ok, _ = _capi_solve(rp, col, vals, capi.SDX_BSR_ROW_STRIPS, b, 1)
+    try:
+        x_bad, _ = _capi_solve(rp, col, vals, capi.SDX_BSR_BLOCKS, b, 1)
+    except Exception:
+        return  # the misread matrix may not even be SPD
+    assert np.abs(x_bad - x_ok).max() > 1e-3 * np.abs(x_ok).max()
 
 
 @pytest.mark.parametrize("system", ["psd100", "tridiag64"])

@@ -1,10 +1,11 @@
-"""The plain FP64 comparison solver behind sdx_step (the reference's CUDA PCG path: FP64 BSR with
-cuSPARSE, cuBLAS vector operations, bursts of 8 iterations) reaches the CPU oracle's Newton states like
-the fused solver does; its CG counts are the oracle's rounded up to the burst length."""
+"""The plain FP64 comparison solver (bench_arms/libsdx_plain_fp64.so: the reference's CUDA PCG path, FP64
+BSR with cuSPARSE, cuBLAS vector operations, bursts of 8 iterations), plugged into sdx_step through the
+external linear-solver hook, reaches the CPU oracle's Newton states like the library's own solver does;
+its CG counts are the oracle's rounded up to the burst length."""
 import numpy as np
 import pytest
 
-from project_superdex_b200 import capi, scenes
+from project_superdex_b200 import scenes
 from test_gpu_step import _run
 
 pytestmark = pytest.mark.gpu
@@ -24,9 +25,14 @@ def _check_plain(bodies, ug, states, hist):
                 (g["cg_iters"], o.cg_iters)
 
 
+def _plain(world):
+    from bench_arms.plain import PlainFp64
+    return PlainFp64(world)
+
+
 def test_plain_fp64_steps_match_oracle(oracle):
     bodies, cfg = scenes.config0()
-    w, ug, vg, states, hist = _run(oracle, bodies, cfg, 3, linear_solver_impl=capi.SDX_SOLVER_PLAIN_FP64)
+    w, ug, vg, states, hist = _run(oracle, bodies, cfg, 3, setup=_plain)
     _check_plain(bodies, ug, states, hist)
 
 
@@ -39,5 +45,5 @@ def test_plain_fp64_batched_envs_match_oracle(oracle):
                                       (0, 0, -0.1))]
         bodies.append(b)
     cfg = scenes.SceneConfig(k_contact=1e6)
-    w, ug, vg, states, hist = _run(oracle, bodies, cfg, 3, linear_solver_impl=capi.SDX_SOLVER_PLAIN_FP64)
+    w, ug, vg, states, hist = _run(oracle, bodies, cfg, 3, setup=_plain)
     _check_plain(bodies, ug, states, hist)

@@ -9,9 +9,10 @@ from project_superdex_b200 import scenes
 pytestmark = pytest.mark.gpu
 
 
-def _run(oracle, bodies, cfg, steps, **kw):
+def _run(oracle, bodies, cfg, steps, setup=None, **kw):
     from project_superdex_b200.soft_body import SoftBodyWorld
     w = SoftBodyWorld(bodies, cfg, **kw)
+    w._test_attachment = setup(w) if setup else None  # e.g. an external linear solver kept alive with w
     states = [(np.zeros(3 * b.n_nodes), np.zeros(3 * b.n_nodes)) for b in bodies]
     sc = [oracle.Scene(b, cfg, min_eig=float(np.finfo(np.float32).eps)) for b in bodies]
     p = oracle.default_newton_params()
