@@ -1,34 +1,40 @@
 #!/usr/bin/env python
 """Benchmark of the B200 implicit soft-body step (one JSON line on rank 0).
 
-Workload (default): the single large body with contact — a 64^3-cell tet grid (274,625 nodes,
-1,572,864 tets) of heterogeneous stable Neo-Hookean (E log-uniform [1e4, 1e6] Pa, nu = 0.45) pressed
-by 5 moving capsules (penalty stiffness 1e4, activation distance 1 mm), backward Euler dt = 1/240,
-Newton to rel 1e-6 with Jacobi-PCG at rel. residual 1e-6. A step is one backward-Euler step of every
-env of the batch. Inputs (matrix ~160 MB, tet data ~300 MB) exceed the 126 MB L2.
+Workload (default, cfg2): 1,024 independent soft bodies of uneven size in one batch — tet boxes with
+cells per axis U{8..40} (seed 0: 16,189,547 nodes, 86,022,012 tets), stable Neo-Hookean with E in
+[1e4, 1e6] Pa and nu in [0.3, 0.48] per body, each pressed by 5 capsule fingertips onto a ground plane
+(penalty contact); backward Euler dt = 1/240, Newton to rel 1e-6 (capped at 12 iterations) with
+Jacobi-PCG at rel. residual 1e-6. A step is one backward-Euler step of every env of the batch. The working
+set (~10 GB) is far larger than the 126 MB L2.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload cfg1|cfg0|cfg2|cfg3|cfg4] [--arms plain_fp64,fused_zero,temporal,learned]
+                  [--workload cfg2|cfg1|cfg0|cfg3|cfg4] [--arms fused_zero,temporal,learned]
 
-`--workload cfg3` is the learned warm start's own protocol on the batched distribution: the MLP is trained
-on plain-solver episodes of 50 seeds (episodes of 16 uneven bodies, cells/axis U{8..40}, 5 capsules and a
-ground plane each; Adam, lr 1e-3), then each arm is timed on 20 held-out seeded episodes and the line
-aggregates them (env-steps over the summed timed seconds, CG iterations per step).
+Solver arms, on the same GPU, the same workload and the same steps (each restored from one snapshot taken
+after the W warm-up steps):
+  plain_fp64  the reference's CUDA PCG path restated (bench_arms/libsdx_plain_fp64.so: FP64 3x3 BSR with
+              cuSPARSE bsrmv, cuBLAS vector operations, graph bursts of 8 iterations with a host convergence
+              check, one env after the other), zero initial guess; single-body workloads only (minutes per
+              step on the batch);
+  fused_zero  this library's persistent batched PCG (FP32 matrix / SpMV, FP64 x, r and reductions), zero
+              initial guess: the plain PCG start of the reference's Newton loop;
+  temporal    the same, started from the previous step's Newton update at the same Newton iteration;
+  learned     the headline: the same, started by a Galerkin step on span{temporal guess, MLP correction}.
+              The per-vertex MLP is trained first, on the GPU, on the learned part's own protocol: (state,
+              RHS, solution) triples of the plain solver on 50 held-out seeded episodes of 16 bodies of the
+              same distribution (seeds 1000..1049, run as one batch of 800 bodies, 2 steps), Adam lr 1e-3.
+The headline arm is timed on K steps through the public API (sdx_set_state / sdx_step / sdx_get_state with
+pinned host buffers): `value` is the device time of the steps (CUDA events on the library stream around
+each sdx_step), `e2e` the whole loop with the host<->device copies, on the same steps. The comparison arms
+are timed on the first min(K, --compare-steps) of those steps, and the ratios use the headline arm's time on
+the same steps.
 
-Four solver arms on the same GPU and the same seeded workload, each a full Newton step:
-  plain_fp64  the reference's CUDA PCG path restated (FP64 3x3 BSR with cuSPARSE bsrmv, cuBLAS vector
-              operations, CUDA-graph bursts of 8 iterations with a host convergence check, one env after
-              the other), zero initial guess;
-  fused_zero  this library's persistent batched PCG (FP32 matrix / SpMV, FP64 x, r and reductions),
-              zero initial guess (the reference's Newton behaviour);
-  temporal    the same, started from the previous step's Newton update at the same Newton iteration
-              (energy-optimal scaling; zero when it would raise the residual);
-  learned     the same, started by a Galerkin step on span{temporal guess, MLP correction} (per-vertex
-              MLP trained first, on the GPU, from plain-solver episodes of held-out seeds).
-The headline `value` is the last arm (learned); `arms` gives each and the ratios.
+`--workload cfg3` times each arm on 20 held-out seeded episodes of 16 bodies (the learned part's evaluation
+protocol); cfg1 is the single 64^3 body with 5 capsules, cfg0 the 10^3 soft cube, cfg4 the 96^3 stiff body.
 
-N > 1 runs one independent replica per GPU (the path shards by environment and has no exchange),
-launched by torchrun; timing is the max over ranks.
+N > 1 runs one independent replica per GPU (the path shards by environment and has no exchange; each rank
+its own seeded batch), launched by torchrun; timing is the max over ranks.
 """
 from __future__ import annotations
 
@@ -48,6 +54,7 @@ sys.path.insert(0, HERE)
 
 METRIC = "env-steps/sec at rel-res 1e-6: learned warm-start vs plain PCG; SpMV HBM GB/s"
 UNIT = "env-steps/s"
+TRAIN_SEED0 = 1000  # training episodes use seeds TRAIN_SEED0.. (never an evaluated seed)
 
 
 def measured_peaks():
@@ -93,6 +100,28 @@ def build_workload(name: str, seed: int = 0):
         n = int(os.environ.get("SDX_CFG2_ENVS", "1024"))
         return scenes.config2(seed, n_envs=n), f"{n} uneven bodies, cells/axis U{{8..40}}, 5 capsules + plane each"
     raise ValueError(name)
+
+
+def newton_max_iter(args):
+    """Newton iteration cap: 50 by default; 12 for the batched workloads, where 1-2 % of the envs stall
+    between relative residual 1e-5 and 1e-3 on the penalty contact's non-smooth activation (the FP64 CPU
+    oracle stalls at the same residuals), and would otherwise run every step to the cap. The line reports
+    the share of env-steps that reached rel 1e-6."""
+    if args.newton_max_iter:
+        return args.newton_max_iter
+    return 12 if args.workload in ("cfg2", "cfg3") else 50
+
+
+def workload_config(args, seed: int, bodies, desc: str, world: int):
+    """The `config` dict both arms (ours and --impl reference) print: the workload itself."""
+    n_nodes = int(sum(b.n_nodes for b in bodies))
+    n_tets = int(sum(b.n_tets for b in bodies))
+    return {"workload": f"{args.workload}: {desc}", "seed": seed, "n_envs": len(bodies), "n_nodes": n_nodes,
+            "n_tets": n_tets, "precision": "FP32 Hessian assembly + SpMV, FP64 residual / energy / CG dots / x,r",
+            "cg_rel_tol": 1e-6, "newton_rel_tol": 1e-6, "newton_max_iter": newton_max_iter(args),
+            "steps_per_measurement": args.steps, "warmup_steps": args.warmup,
+            "l2": "inputs larger than L2 (matrix + tet data > 126 MB)",
+            "parallelism": f"replicas x{world} (one seeded batch per GPU)" if world > 1 else "1 GPU"}
 
 
 class ClockSampler:
@@ -154,73 +183,94 @@ class ClockSampler:
         return out
 
 
-def cpu_oracle_sample(workload: str, seed: int = 0, steps: int = 1, warmup: int = 0):
-    """The CPU restatement of the reference path (oracle/) on a bounded sample: env 0 of the workload from
-    rest, `warmup` untimed backward-Euler steps, then `steps` timed steps continuing the trajectory, all
-    host threads."""
+# ------------------------------------------------------------------------------------------------
+# the CPU baseline (the oracle: the reference's path restated in C, all host threads)
+
+def sample_envs(bodies, tet_budget: int):
+    """The first envs of the batch whose tets sum to at most tet_budget (at least one)."""
+    idx, tot = [], 0
+    for i, b in enumerate(bodies):
+        if idx and tot + b.n_tets > tet_budget:
+            break
+        idx.append(i)
+        tot += b.n_tets
+    return idx
+
+
+def cpu_oracle_run(args, seed: int, steps: int, warmup: int, tet_budget: int):
+    """The CPU restatement of the reference path on a bounded sample: the first envs of the workload (up to
+    tet_budget tets), each stepped from rest for `warmup` untimed and `steps` timed backward-Euler steps
+    with all host threads, the envs one after the other (the reference steps independent islands as
+    parallel tasks; here the threads go to each env's assembly and CG). Returns env-steps/s over the
+    sample's timed steps."""
     from oracle import oracle as O
-    (bodies, cfg), _ = build_workload(workload, seed)
-    b = bodies[0]
-    s = O.Scene(b, cfg)
-    u = np.zeros(3 * b.n_nodes)
-    v = np.zeros_like(u)
+    (bodies, cfg), _ = build_workload(args.workload, seed)
+    envs = sample_envs(bodies, tet_budget)
     prm = O.default_newton_params()
     prm.abs_tol = 1e-9  # same Newton stopping test as the GPU arm: rel 1e-6
-    if workload in ("cfg2", "cfg3"):
-        prm.max_iter = 12  # same Newton cap as the GPU arm
-    t = 0.0
+    prm.max_iter = newton_max_iter(args)
+    states = []
+    for e in envs:
+        s = O.Scene(bodies[e], cfg)
+        u = np.zeros(3 * bodies[e].n_nodes)
+        states.append([s, u, np.zeros_like(u), 0.0])
     for _ in range(warmup):
-        t += cfg.dt
-        u, v, st = s.step(u, v, t, prm)
+        for st in states:
+            st[3] += cfg.dt
+            st[1], st[2], _ = st[0].step(st[1], st[2], st[3], prm)
     newton = cg = 0
     t0 = time.perf_counter()
     for _ in range(steps):
-        t += cfg.dt
-        u, v, st = s.step(u, v, t, prm)
-        newton += st.newton_iters
-        cg += st.cg_iters
+        for st in states:
+            st[3] += cfg.dt
+            st[1], st[2], r = st[0].step(st[1], st[2], st[3], prm)
+            newton += r.newton_iters
+            cg += r.cg_iters
     dt = time.perf_counter() - t0
-    return {"value": steps / dt, "unit": UNIT, "cores": int(O.lib().or_num_threads()), "kind": "port",
-            "sample": (f"env 0 of {workload}: {warmup} untimed + {steps} timed backward-Euler steps from rest "
-                       f"({newton} Newton, {cg} CG iterations timed) in {dt:.2f} s")}
+    tets = sum(bodies[e].n_tets for e in envs)
+    return {"value": len(envs) * steps / dt, "unit": UNIT, "cores": int(O.lib().or_num_threads()), "kind": "port",
+            "sample": (f"envs {envs[0]}..{envs[-1]} of {args.workload} seed {seed} ({len(envs)} of {len(bodies)} "
+                       f"envs, {tets} tets): {warmup} untimed + {steps} timed backward-Euler steps from rest, "
+                       f"{newton} Newton / {cg} CG iterations timed, {dt:.2f} s")}
 
 
-def vector_bytes_per_node():
-    # algorithmic bytes per node per CG iteration of the fused PCG besides the matrix:
-    # phase 1: z own 12 + z gather 12 + p r/w 24 + q r/w 24; phase 2: x r/w 48 (FP64),
-    # r r/w 48 (FP64), p 12, q 12, dinv 12, z r/w 24
-    return 12 + 12 + 24 + 24 + 48 + 48 + 12 + 12 + 12 + 24
-
-
-def newton_max_iter(args):
-    """Newton iteration cap: 50 by default; 12 for the batched workload, where 1-2 % of the envs stall
-    between relative residual 1e-5 and 1e-3 on the penalty contact's non-smooth activation (the FP64 CPU
-    oracle stalls at the same residuals), and would otherwise run every step to the cap."""
-    if args.newton_max_iter:
-        return args.newton_max_iter
-    return 12 if args.workload in ("cfg2", "cfg3") else 50
-
+# ------------------------------------------------------------------------------------------------
+# training of the learned warm start (the learned part's own protocol)
 
 def train_warm_start(args, local_rank):
-    """Train the warm-start MLP on the GPU from plain-solver episodes of held-out seeds of the same
-    workload (never the evaluated seed). Returns (params, info)."""
+    """Train the warm-start MLP on the GPU from plain-solver (zero start) episodes of held-out seeds of the
+    batched distribution: `train_episodes` episodes of 16 bodies (seeds TRAIN_SEED0..), run together as one
+    batch, `train_steps` steps, up to `train_samples` (features, solution) vertex samples; Adam lr 1e-3.
+    Returns (params, info)."""
+    from project_superdex_b200 import scenes
     from project_superdex_b200.learned import Mlp, collect
     from project_superdex_b200.soft_body import SoftBodyWorld
     t0 = time.perf_counter()
+    if args.workload in ("cfg2", "cfg3"):
+        bodies = []
+        for k in range(args.train_episodes):
+            bodies += scenes.config2(TRAIN_SEED0 + k, n_envs=16)[0]
+        cfg = scenes.config2(TRAIN_SEED0, n_envs=1)[1]
+        groups = [bodies]
+        per_solve_div = 4 * args.train_steps
+    else:  # single-body workloads: episodes of the same body with held-out seeds
+        groups = []
+        for k in range(args.train_episodes):
+            (bb, cfg), _ = build_workload(args.workload, seed=TRAIN_SEED0 + k)
+            groups.append(bb)
+        per_solve_div = 4 * args.train_steps * args.train_episodes
     Xs, Ts = [], []
-    # the training set is capped at train_samples vertices, spread evenly over the episodes (cfg3's 50
-    # episodes take a few thousand vertices from each Newton solve; cfg1's two take the first 1 M each)
-    cap = max(4096, args.train_samples // args.train_episodes)
-    per_solve = 65536 if args.workload != "cfg3" else max(1024, min(65536, cap // (4 * args.train_steps)))
-    for k in range(args.train_episodes):
-        (bodies, cfg), _ = build_workload(args.workload, seed=args.seed + 1000 + k)
-        tw = SoftBodyWorld(bodies, cfg, device=local_rank, newton_abs_tol=1e-9,
-                           newton_max_iter=newton_max_iter(args))
+    cap = args.train_samples // len(groups)
+    per_solve = max(1024, min(1 << 20, cap // per_solve_div))
+    tw = None
+    for k, bodies in enumerate(groups):
+        if tw is not None:
+            tw.close()
+        tw = SoftBodyWorld(bodies, cfg, device=local_rank, newton_abs_tol=1e-9, newton_max_iter=newton_max_iter(args))
         X, T = collect(tw, args.train_steps, samples_per_solve=per_solve, capacity=cap, seed=k)
         Xs.append(X)
         Ts.append(T)
-        if k < args.train_episodes - 1:
-            tw.close()
+    t_data = time.perf_counter() - t0
     X, T = np.concatenate(Xs), np.concatenate(Ts)
     m = Mlp(tw._ctx)
     m.init(args.seed)
@@ -228,199 +278,294 @@ def train_warm_start(args, local_rank):
     params = m.get_params()
     tw.close()
     return params, {"episodes": args.train_episodes, "steps_per_episode": args.train_steps,
-                    "samples": int(X.shape[0]), "epochs": args.train_epochs, "loss_first": float(losses[0]),
-                    "loss_last": float(losses[-1]), "seconds": time.perf_counter() - t0,
-                    "seeds": f"{args.seed + 1000}..{args.seed + 999 + args.train_episodes} (held out)"}
+                    "bodies_per_episode": 16 if args.workload in ("cfg2", "cfg3") else 1,
+                    "samples": int(X.shape[0]), "epochs": args.train_epochs, "lr": 1e-3,
+                    "loss_first": float(losses[0]), "loss_last": float(losses[-1]),
+                    "data_seconds": t_data, "seconds": time.perf_counter() - t0,
+                    "seeds": f"{TRAIN_SEED0}..{TRAIN_SEED0 + args.train_episodes - 1} (held out)"}
 
 
-def time_arm(w, args, stream, local_rank, dist, world):
-    """W untimed steps, then exactly K steps between CUDA events on the library stream."""
+# ------------------------------------------------------------------------------------------------
+# timing
+
+def _events(n):
     import torch
-    w.step(args.warmup)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    return [torch.cuda.Event(enable_timing=True) for _ in range(n)]
+
+
+def time_headline(w, args, stream, local_rank):
+    """K steps through the public API with pinned host buffers: per step sdx_set_state (host -> device),
+    sdx_step, sdx_get_state (device -> host). Device time of each sdx_step from CUDA events on the library
+    stream; the e2e time covers the whole loop, copies included. Per-step env convergence is read from the
+    statistics after each step."""
+    import torch
+    K = args.steps
+    hu = torch.empty(3 * w.n_nodes, dtype=torch.float64, pin_memory=True).numpy()
+    hv = torch.empty(3 * w.n_nodes, dtype=torch.float64, pin_memory=True).numpy()
+    _, _, t_state = w.get_state(hu, hv)
+    ev_a, ev_b, ev_c = _events(K), _events(K), _events(K)
+    ev_end = _events(1)[0]
     launches0 = w.kernel_launches()
     w.set_profiling(True)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
+    conv_steps = 0
+    newton = cg_env = 0
+    torch.cuda.synchronize()
     with ClockSampler(local_rank) as clk:
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        w.step(args.steps)
-        ev1.record(stream)
-        ev1.synchronize()
-    ms = ev0.elapsed_time(ev1)
+        for k in range(K):
+            ev_a[k].record(stream)
+            w.set_state(hu, hv, t_state)
+            ev_b[k].record(stream)
+            w.step(1)
+            ev_c[k].record(stream)
+            _, _, t_state = w.get_state(hu, hv)
+            st = w.stats()
+            conv_steps += sum(1 for s in st if s["convergence"] == 1)
+            newton += sum(s["newton_iters"] for s in st)
+            cg_env += sum(s["cg_iters"] for s in st)
+        ev_end.record(stream)
+        ev_end.synchronize()
+    step_ms = [ev_b[k].elapsed_time(ev_c[k]) for k in range(K)]
+    e2e_ms = ev_a[0].elapsed_time(ev_end)
     prof = w.profile()
     w.set_profiling(False)
-    launches = w.kernel_launches() - launches0
-    stats = w.stats()
-    if dist:
-        t = torch.tensor([ms], device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    n_envs = w.n_envs
-    # over the K timed steps: one PCG launch per Newton iteration (all envs together), and per launch the
-    # iterations of its slowest env
-    return {"value": world * n_envs * args.steps / (ms / 1000.0), "ms": ms, "prof": prof, "launches": launches,
-            "clocks": clk.summary(), "env_steps": world * n_envs * args.steps, "steps": args.steps,
-            "cg_iters_per_step": prof["pcg_iters"] / args.steps,
-            "newton_iters_per_step": prof["pcg_launches"] / args.steps,
-            "last_step_cg_iters_mean_env": [sum(s["cg_iters"] for s in stats) / max(1, n_envs)]}
+    n = w.n_envs
+    return {"step_ms": step_ms, "ms": sum(step_ms), "e2e_ms": e2e_ms, "prof": prof,
+            "launches": w.kernel_launches() - launches0, "clocks": clk.summary(), "env_steps": n * K,
+            "steps": K, "converged_env_steps": conv_steps, "newton_per_env_step": newton / (n * K),
+            "cg_per_env_step": cg_env / (n * K), "h2d_bytes_per_step": 2 * 3 * 8 * w.n_nodes,
+            "d2h_bytes_per_step": 2 * 3 * 8 * w.n_nodes}
 
 
-def merge_runs(a, b):
+def time_steps(w, n_steps, stream):
+    """n_steps of sdx_step, each between CUDA events on the library stream (inputs resident)."""
+    import torch
+    ev0, ev1 = _events(n_steps), _events(n_steps)
+    w.set_profiling(True)
+    newton = cg_env = conv = 0
+    torch.cuda.synchronize()
+    for k in range(n_steps):
+        ev0[k].record(stream)
+        w.step(1)
+        ev1[k].record(stream)
+        st = w.stats()
+        conv += sum(1 for s in st if s["convergence"] == 1)
+        newton += sum(s["newton_iters"] for s in st)
+        cg_env += sum(s["cg_iters"] for s in st)
+    ev1[-1].synchronize()
+    prof = w.profile()
+    w.set_profiling(False)
+    step_ms = [ev0[k].elapsed_time(ev1[k]) for k in range(n_steps)]
+    n = w.n_envs
+    return {"step_ms": step_ms, "ms": sum(step_ms), "prof": prof, "env_steps": n * n_steps, "steps": n_steps,
+            "converged_env_steps": conv, "newton_per_env_step": newton / (n * n_steps),
+            "cg_per_env_step": cg_env / (n * n_steps)}
+
+
+def max_over_ranks(x, dist, local_rank):
+    if not dist:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local_rank}")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def set_arm(w, arm, params):
+    from project_superdex_b200 import capi
+    from project_superdex_b200.learned import Mlp
+    if arm == "learned":
+        Mlp(w._ctx).set_params(params)
+    w.set_params(warm_start={"learned": capi.SDX_WARM_LEARNED, "temporal": capi.SDX_WARM_TEMPORAL}.get(
+        arm, capi.SDX_WARM_ZERO))
+    if getattr(w, "_plain", None) is not None:
+        w._plain.close()
+        w._plain = None
+    if arm == "plain_fp64":  # the comparison solver, plugged into the Newton solves (bench_arms/)
+        from bench_arms.plain import PlainFp64
+        w._plain = PlainFp64(w)
+
+
+def parity_env0(args, bodies, cfg, states_gpu, stats_gpu):
+    """Env 0 of the headline workload: the GPU state after each of the first steps from rest against the
+    FP64 CPU oracle (the reference's path restated) stepped the same way."""
+    from oracle import oracle as O
+    b = bodies[0]
+    s = O.Scene(b, cfg)
+    prm = O.default_newton_params()
+    prm.abs_tol = 1e-9
+    prm.max_iter = newton_max_iter(args)
+    u = np.zeros(3 * b.n_nodes)
+    v = np.zeros_like(u)
+    size = float(np.ptp(b.X, axis=0).max())
+    out = {"env": 0, "n_nodes": int(b.n_nodes), "n_tets": int(b.n_tets), "body_size_m": size, "steps": []}
+    t0 = time.perf_counter()
+    for k, (ug, sg) in enumerate(zip(states_gpu, stats_gpu)):
+        u, v, st = s.step(u, v, (k + 1) * cfg.dt, prm)
+        err = float(np.abs(ug - u).max())
+        out["steps"].append({"max_abs_err_m": err, "err_over_body_size": err / size,
+                             "newton_gpu": sg["newton_iters"], "newton_oracle": int(st.newton_iters),
+                             "cg_gpu": sg["cg_iters"], "cg_oracle": int(st.cg_iters),
+                             "converged_gpu": sg["convergence"] == 1, "converged_oracle": int(st.convergence) == 1})
+    out["max_err_over_body_size"] = max(x["err_over_body_size"] for x in out["steps"])
+    out["tolerance"] = 1e-5
+    out["ok"] = out["max_err_over_body_size"] <= 1e-5
+    out["oracle_seconds"] = time.perf_counter() - t0
+    out["reference"] = "FP64 CPU oracle (oracle/sdx_oracle.c, pinned to the reference's compiled code)"
+    return out
+
+
+def merge(a, b):
     """One arm timed on several episodes: sums of env-steps, time, launches and the solver profile."""
     out = dict(b)
-    out["env_steps"] = a["env_steps"] + b["env_steps"]
-    out["steps"] = a["steps"] + b["steps"]
-    out["ms"] = a["ms"] + b["ms"]
-    out["launches"] = a["launches"] + b["launches"]
-    out["last_step_cg_iters_mean_env"] = a["last_step_cg_iters_mean_env"] + b["last_step_cg_iters_mean_env"]
-    out["value"] = out["env_steps"] / (out["ms"] / 1000.0)
+    for k in ("env_steps", "steps", "ms", "e2e_ms", "launches", "converged_env_steps"):
+        if k in a:
+            out[k] = a[k] + b[k]
+    out["step_ms"] = a["step_ms"] + b["step_ms"]
+    for k in ("newton_per_env_step", "cg_per_env_step"):
+        out[k] = (a[k] * a["env_steps"] + b[k] * b["env_steps"]) / out["env_steps"]
     out["prof"] = {k: (a["prof"].get(k, 0) + v if k != "pcg_threads" else v) for k, v in b["prof"].items()}
-    out["cg_iters_per_step"] = out["prof"]["pcg_iters"] / out["steps"]
-    out["newton_iters_per_step"] = out["prof"]["pcg_launches"] / out["steps"]
-    ca, cb = a["clocks"], b["clocks"]
-    sm = [x for x in (ca.get("sm_mhz"), cb.get("sm_mhz")) if x is not None]
-    out["clocks"] = {"sm_mhz": statistics.median(sm) if sm else None,
-                     "sm_max_mhz": max([x for x in (ca.get("sm_max_mhz"), cb.get("sm_max_mhz")) if x is not None],
-                                       default=None),
-                     "reasons": sorted(set(ca.get("reasons", [])) | set(cb.get("reasons", []))),
-                     "samples": ca.get("samples", 0) + cb.get("samples", 0)}
+    if "clocks" in a:
+        ca, cb = a["clocks"], b["clocks"]
+        sm = [x for x in (ca.get("sm_mhz"), cb.get("sm_mhz")) if x is not None]
+        out["clocks"] = {"sm_mhz": statistics.median(sm) if sm else None,
+                         "sm_max_mhz": max([x for x in (ca.get("sm_max_mhz"), cb.get("sm_max_mhz")) if x is not None],
+                                           default=None),
+                         "reasons": sorted(set(ca.get("reasons", [])) | set(cb.get("reasons", []))),
+                         "samples": ca.get("samples", 0) + cb.get("samples", 0)}
     return out
 
 
 def run_ours(args, rank, world, local_rank):
-    # the PCG launch shape is picked by the library's autotuner on each world's first Newton solve
+    # the PCG launch shape is picked by the library's autotuner on the world's first Newton solve
     os.environ.setdefault("SDX_PCG_AUTOTUNE", "1")
     import torch
-    from project_superdex_b200 import capi
-    from project_superdex_b200.learned import Mlp
+    from project_superdex_b200.replicas import replica_seed
     from project_superdex_b200.soft_body import SoftBodyWorld
     torch.cuda.set_device(local_rank)
     dist = None
     if world > 1:
         import torch.distributed as dist
     arms = [a for a in args.arms.split(",") if a]
+    head_arm = arms[-1]
     params, train_info = (None, None)
     if "learned" in arms:
         params, train_info = train_warm_start(args, local_rank)
-    # cfg3: every arm on each held-out episode (seeds args.seed.., training used args.seed + 1000..)
-    seeds = [args.seed + i for i in range(args.eval_episodes)] if args.workload == "cfg3" else [args.seed]
-    results = {}
+    seed0 = replica_seed(args.seed, rank)
+    seeds = [seed0 + i for i in range(args.eval_episodes)] if args.workload == "cfg3" else [seed0]
+    n_cmp = min(args.steps, args.compare_steps)
+    head = None
+    comp = {a: None for a in arms[:-1]}
+    head_first = 0.0  # the headline arm's device time on the comparison steps
+    parity = None
     w = None
-    for seed in seeds:
+    for ei, seed in enumerate(seeds):
         (bodies, cfg), desc = build_workload(args.workload, seed=seed)
-        for arm in arms:
-            if w is not None:
-                w.close()
-            # Newton to rel 1e-6 (the absolute floor is only a guard for an exactly zero residual)
-            w = SoftBodyWorld(bodies, cfg, device=local_rank, newton_abs_tol=1e-9,
-                              newton_max_iter=newton_max_iter(args))
-            if arm == "learned":
-                Mlp(w._ctx).set_params(params)
-            w.set_params(warm_start={"learned": capi.SDX_WARM_LEARNED, "temporal": capi.SDX_WARM_TEMPORAL}.get(
-                             arm, capi.SDX_WARM_ZERO))
-            if arm == "plain_fp64":  # the comparison solver, plugged into the Newton solves (bench_arms/)
-                from bench_arms.plain import PlainFp64
-                w._plain = PlainFp64(w)
-            stream = torch.cuda.ExternalStream(w.stream_handle(), device=local_rank)
-            r = time_arm(w, args, stream, local_rank, dist, world)
-            results[arm] = merge_runs(results[arm], r) if arm in results else r
-    head = results[arms[-1]]  # the headline arm is the last one (learned by default); w is its world
-    n_envs = w.n_envs
-    ms, prof = head["ms"], head["prof"]
+        if ei == 0:
+            config = workload_config(args, seed, bodies, desc, world)
+        if w is not None:
+            w.close()
+        # Newton to rel 1e-6 (the absolute floor is only a guard for an exactly zero residual)
+        w = SoftBodyWorld(bodies, cfg, device=local_rank, newton_abs_tol=1e-9, newton_max_iter=newton_max_iter(args))
+        stream = torch.cuda.ExternalStream(w.stream_handle(), device=local_rank)
+        set_arm(w, head_arm, params)
+        # warm-up from rest with the headline arm; env 0's first two states for the parity check
+        par_u, par_st = [], []
+        for k in range(args.warmup):
+            w.step(1)
+            if ei == 0 and k < 2 and rank == 0:
+                u, _, _ = w.get_state()
+                par_u.append(u[:3 * bodies[0].n_nodes].copy())
+                par_st.append(w.stats()[0])
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        snap = w.capture_state()
+        r = time_headline(w, args, stream, local_rank)
+        head = r if head is None else merge(head, r)
+        head_first += sum(r["step_ms"][:n_cmp])
+        for a in arms[:-1]:
+            w.restore_state(snap)
+            set_arm(w, a, params)
+            rc = time_steps(w, n_cmp, stream)
+            comp[a] = rc if comp[a] is None else merge(comp[a], rc)
+        set_arm(w, head_arm, params)
+        w.release_all_states()
+        if ei == 0 and par_u and not args.no_parity:
+            parity = parity_env0(args, bodies, cfg, par_u, par_st)
+    ms = max_over_ranks(head["ms"], dist, local_rank)
+    e2e_ms = max_over_ranks(head["e2e_ms"], dist, local_rank)
+    prof = head["prof"]
+    value = world * head["env_steps"] / (ms / 1000.0)
 
-    # roofline of the dominant kernel (the persistent PCG)
+    # roofline of the dominant kernel (the persistent PCG): algorithmic bytes per env per CG iteration
+    # (40 B per block + 4 B per row pointer + 228 B per row) x that env's iterations, summed by the library
+    # over the timed launches, over the PCG launches' CUDA-event time
     peak, peak_kind = measured_peaks()
-    # algorithmic bytes: per env, its CG iterations x (40 B per block + 4 B per row pointer + 228 B per
-    # row), summed by the library over the timed launches (envs of a batch converge at different counts)
-    bytes_iter = w.nnzb * 40 + 4 * (w.n_nodes + 1) + vector_bytes_per_node() * w.n_nodes
     pcg_s = prof["pcg_ms"] / 1000.0
     achieved = prof["pcg_bytes"] / pcg_s / 1e9 if pcg_s > 0 else None
-    traffic = ncu_traffic("k_pcg_per_iter") if args.workload == "cfg1" else None
+    frac = (achieved / peak) if achieved else None
+    frac_note = None
+    if frac is not None and frac > 1.2:
+        # above the copy bandwidth: the vectors were L2-resident (small envs) or the byte count is stale
+        frac_note = f"frac {frac:.2f} > 1.2 rejected: the PCG ran from L2, HBM is not its bound here"
+        frac = None
+    traffic = ncu_traffic(f"k_pcg_per_iter_{args.workload}")
+    if traffic is None and args.workload == "cfg1":
+        traffic = ncu_traffic("k_pcg_per_iter")
     pcg_kernel = ("k_pcg (persistent Jacobi-PCG) and k_pcg_cluster (one cluster per env), every PCG solve"
                   if prof.get("pcg_cluster_solves", 0) else "k_pcg (persistent Jacobi-PCG)")
-    roofline = {"bound": "hbm", "kernel": pcg_kernel, "achieved": achieved,
-                "peak": peak, "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
-                "peak_source": peak_kind, "traffic": traffic, "bytes_per_iter": bytes_iter,
-                "iters": prof["pcg_iters"], "share_of_step": prof["pcg_ms"] / ms}
-    # standalone SpMV on the last assembled matrix
+    roofline = {"bound": "hbm", "kernel": pcg_kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": frac, "peak_source": peak_kind, "traffic": traffic,
+                "traffic_unit": "DRAM bytes per CG iteration of the batch (ncu, profiles/traffic.txt)",
+                "algorithmic_bytes": prof["pcg_bytes"], "launch_iters": prof["pcg_iters"],
+                "share_of_step": prof["pcg_ms"] / head["ms"]}
+    if frac_note:
+        roofline["note"] = frac_note
     spmv_ms, spmv_bytes = w.bench_spmv(reps=20)
     spmv = {"achieved_gbs": spmv_bytes / (spmv_ms / 1000.0) / 1e9, "ms": spmv_ms, "bytes": spmv_bytes}
     spmv["frac"] = spmv["achieved_gbs"] / peak
-
-    # end to end through the public API with pinned host buffers, copies inside the timed region
-    stream = torch.cuda.ExternalStream(w.stream_handle(), device=local_rank)
-    hu = torch.empty(3 * w.n_nodes, dtype=torch.float64, pin_memory=True).numpy()
-    hv = torch.empty(3 * w.n_nodes, dtype=torch.float64, pin_memory=True).numpy()
-    _, _, t_state = w.get_state(hu, hv)
-    e2e_steps = max(1, min(args.steps, 5))
-    w.set_profiling(True)  # same per-kernel event overhead as the timed arms; gives the e2e solver counts
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e2e_steps):
-        w.set_state(hu, hv, t_state)
-        w.step(1)
-        _, _, t_state = w.get_state(hu, hv)
-    e1.record(stream)
-    e1.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    eprof = w.profile()
-    w.set_profiling(False)
-    if dist:
-        t = torch.tensor([e2e_ms], device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = {"value": world * n_envs * e2e_steps / (e2e_ms / 1000.0), "unit": UNIT,
-           "h2d_bytes_per_step": 2 * 3 * 8 * w.n_nodes, "d2h_bytes_per_step": 2 * 3 * 8 * w.n_nodes,
-           "steps": e2e_steps, "warm_start": arms[-1],
-           "note": "the steps after the timed ones, continuing the trajectory",
-           "cg_iters_per_step": eprof["pcg_iters"] / e2e_steps,
-           "newton_iters_per_step": eprof["pcg_launches"] / e2e_steps}
-    arm_summary = {a: {"value": r["value"], "ms_per_step": r["ms"] / r["steps"],
-                       "cg_iters_per_step": r["cg_iters_per_step"],
-                       "newton_iters_per_step": r["newton_iters_per_step"],
-                       # each env's own CG iterations in the last timed step (a launch runs until its
-                       # slowest env converges; cg_iters_per_step counts those launch-level iterations)
-                       "cg_iters_per_env_last_step": float(np.mean(r["last_step_cg_iters_mean_env"]))}
-                   for a, r in results.items()}
-    for base in ("plain_fp64", "fused_zero", "temporal"):
-        if base in results and "learned" in results:
-            arm_summary[f"learned_over_{base}"] = results["learned"]["value"] / results[base]["value"]
-            arm_summary[f"cg_iters_learned_over_{base}"] = (results["learned"]["cg_iters_per_step"]
-                                                            / results[base]["cg_iters_per_step"])
-    reasons = sorted(set().union(*[set(r["clocks"].get("reasons", [])) for r in results.values()]))
-    clocks = dict(head["clocks"])
-    clocks["reasons_all_arms"] = reasons
+    e2e = {"value": world * head["env_steps"] / (e2e_ms / 1000.0), "unit": UNIT,
+           "h2d_bytes_per_step": head["h2d_bytes_per_step"], "d2h_bytes_per_step": head["d2h_bytes_per_step"],
+           "steps": head["steps"], "warm_start": head_arm,
+           "note": ("the same steps as value, through sdx_set_state / sdx_step / sdx_get_state with pinned host "
+                    "buffers (u and v both ways every step)")}
+    arm_summary = {head_arm: {"value": value, "ms_per_step": ms / head["steps"],
+                              "newton_iters_per_env_step": head["newton_per_env_step"],
+                              "cg_iters_per_env_step": head["cg_per_env_step"],
+                              "converged_frac": head["converged_env_steps"] / head["env_steps"]}}
+    for a, rc in comp.items():
+        v_a = world * rc["env_steps"] / (rc["ms"] / 1000.0)
+        v_h = world * rc["env_steps"] / (head_first / 1000.0)
+        arm_summary[a] = {"value": v_a, "ms_per_step": rc["ms"] / rc["steps"], "steps": rc["steps"],
+                          "newton_iters_per_env_step": rc["newton_per_env_step"],
+                          "cg_iters_per_env_step": rc["cg_per_env_step"],
+                          "converged_frac": rc["converged_env_steps"] / rc["env_steps"]}
+        # the headline arm's env-steps/s on the same steps (its first n_cmp timed steps) over this arm's
+        arm_summary[f"{head_arm}_over_{a}"] = v_h / v_a
     line = {
-        "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / head["steps"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic (seeded tet grids, random materials and collider trajectories)",
-        "config": {"workload": f"{args.workload}: {desc}", "n_envs": n_envs, "n_nodes": w.n_nodes,
-                   "n_tets": w.n_tets, "nnzb": w.nnzb,
-                   "precision": "FP32 Hessian assembly + SpMV, FP64 residual / energy / CG dots / x,r",
-                   "warm_start": arms[-1], "arms": arms,
-                   "cg_rel_tol": 1e-6, "newton_rel_tol": 1e-6, "newton_abs_tol": 1e-9,
-                   "newton_max_iter": newton_max_iter(args),
-                   "l2": "inputs larger than L2 (matrix + tet data > 126 MB)",
-                   "pcg_threads_autotuned": int(prof.get("pcg_threads", 0)),
-                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                   "episodes": len(seeds), "seeds": f"{seeds[0]}..{seeds[-1]}"},
+        "config": config,
+        "run": {"arms": arms, "headline_arm": head_arm, "compare_steps": n_cmp, "episodes": len(seeds),
+                "seeds": f"{seeds[0]}..{seeds[-1]}", "nnzb": w.nnzb,
+                "pcg_threads_autotuned": int(prof.get("pcg_threads", 0))},
+        "converged": {"env_steps": head["converged_env_steps"], "of": head["env_steps"],
+                      "frac": head["converged_env_steps"] / head["env_steps"],
+                      "note": ("value counts every env-step; an env-step that hit the Newton cap before rel 1e-6 "
+                               "is counted too (the CPU oracle stalls on the same envs)")},
         "arms": arm_summary, "training": train_info,
         "roofline": roofline, "spmv": spmv, "e2e": e2e, "gpu_launches": head["launches"],
-        "clocks": clocks,
-        "solver": {"cg_iters_per_step": head["cg_iters_per_step"],
-                   "newton_iters_per_step": head["newton_iters_per_step"],
+        "clocks": head["clocks"], "parity": parity,
+        "solver": {"newton_iters_per_env_step": head["newton_per_env_step"],
+                   "cg_iters_per_env_step": head["cg_per_env_step"],
+                   "pcg_launch_iters": prof["pcg_iters"], "pcg_launches": prof["pcg_launches"],
                    "pcg_cluster_solves": int(prof.get("pcg_cluster_solves", 0)),
                    "profile_ms": {k: v for k, v in prof.items() if k.endswith("_ms")}},
     }
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_oracle_sample(args.workload, args.seed)
+        line["cpu_baseline"] = cpu_oracle_run(args, seed0, steps=1, warmup=0, tet_budget=args.cpu_tets)
     w.close()
     return line
 
@@ -431,17 +576,16 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="cfg1", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg0", "cfg1", "cfg2", "cfg3", "cfg4"])
     ap.add_argument("--arms", default=None,
-                    help="comma list of solver arms to time, headline last: plain_fp64 (the reference's CUDA "
-                         "PCG path restated: FP64 BSR, cuSPARSE/cuBLAS, zero start), fused_zero (this "
-                         "library's PCG, zero start), temporal (start from the previous step's update at the "
-                         "same Newton iteration), learned (temporal guess + learned correction, Galerkin); "
-                         "default plain_fp64,fused_zero,temporal,learned (cfg3: fused_zero,temporal,learned)")
+                    help="comma list of solver arms, headline last: plain_fp64, fused_zero, temporal, learned "
+                         "(default fused_zero,temporal,learned; single-body workloads add plain_fp64 first)")
+    ap.add_argument("--compare-steps", type=int, default=5, dest="compare_steps",
+                    help="steps each comparison arm is timed on (the first of the headline's timed steps)")
     ap.add_argument("--train-episodes", type=int, default=None, dest="train_episodes",
-                    help="plain-solver training episodes (default 2; cfg3: 50)")
+                    help="training episodes (default 50 of 16 bodies on the batched workloads; 2 otherwise)")
     ap.add_argument("--train-steps", type=int, default=None, dest="train_steps",
-                    help="steps per training episode (default 8; cfg3: 2)")
+                    help="steps per training episode (default 2; single-body workloads 8)")
     ap.add_argument("--train-epochs", type=int, default=8, dest="train_epochs")
     ap.add_argument("--train-samples", type=int, default=1 << 21, dest="train_samples",
                     help="training vertices kept over all episodes")
@@ -449,32 +593,36 @@ def main():
                     help="cfg3: held-out episodes each arm is timed on")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--newton-max-iter", type=int, default=0, dest="newton_max_iter")
+    ap.add_argument("--cpu-tets", type=int, default=400000, dest="cpu_tets",
+                    help="tets of the envs the CPU baseline steps per step (a bounded sample)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true")
     args = ap.parse_args()
-    cfg3 = args.workload == "cfg3"
+    batched = args.workload in ("cfg2", "cfg3")
     if args.arms is None:
-        args.arms = "fused_zero,temporal,learned" if cfg3 else "plain_fp64,fused_zero,temporal,learned"
+        args.arms = "fused_zero,temporal,learned" if batched else "plain_fp64,fused_zero,temporal,learned"
     if args.train_episodes is None:
-        args.train_episodes = 50 if cfg3 else 2
+        args.train_episodes = 50 if batched else 2
     if args.train_steps is None:
-        args.train_steps = 2 if cfg3 else 8
+        args.train_steps = 2 if batched else 8
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
 
     if args.impl == "reference":
         # The reference's own implementation of this path is CPU code; its timed stand-in is the CPU
-        # restatement in oracle/ (the reference's full step needs its cmake build). Rank 0 only.
+        # restatement in oracle/ (the reference's scene-level step needs its cmake build). Rank 0 only.
         if rank != 0:
             return 0
-        cb = cpu_oracle_sample(args.workload, args.seed, steps=args.steps, warmup=args.warmup)
-        _, desc = build_workload(args.workload, seed=args.seed)
+        from project_superdex_b200.replicas import replica_seed
+        seed0 = replica_seed(args.seed, 0)
+        (bodies, _), desc = build_workload(args.workload, seed=seed0)
+        cb = cpu_oracle_run(args, seed0, steps=args.steps, warmup=args.warmup, tet_budget=args.cpu_tets)
         line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / cb["value"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded tet grids, random materials and collider trajectories)",
-                "config": {"workload": f"{args.workload}: {desc}", "sample": "env 0",
-                           "newton_max_iter": newton_max_iter(args)},
+                "config": workload_config(args, seed0, bodies, desc, args.gpus),
                 "cpu_baseline": cb,
                 "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)

@@ -1,29 +1,30 @@
-"""Host-side logic of bench.py that needs no GPU: the workloads it builds and how one arm's runs over
-several evaluation episodes are combined (the learned warm start's protocol on the batched
-distribution times each arm on 20 held-out episodes and reports the aggregate)."""
+"""Host-side logic of bench.py that needs no GPU: the workloads it builds, the config dict both arms print,
+the CPU baseline's bounded sample and how one arm's runs over several evaluation episodes are combined
+(the learned warm start's protocol on the batched distribution times each arm on 20 held-out episodes)."""
+import argparse
+
 import bench
 
 
-def _run(env_steps, steps, ms, iters, launches, sm_mhz, reasons):
-    return {"value": env_steps / (ms / 1000.0), "ms": ms, "env_steps": env_steps, "steps": steps,
-            "launches": launches, "prof": {"pcg_ms": 0.9 * ms, "pcg_iters": iters, "pcg_launches": 4 * steps,
-                                           "pcg_bytes": 1e9 * iters, "pcg_threads": 512},
+def _run(env_steps, steps, ms, iters, launches, sm_mhz, reasons, conv):
+    return {"ms": ms, "e2e_ms": 1.1 * ms, "env_steps": env_steps, "steps": steps, "launches": launches,
+            "step_ms": [ms / steps] * steps, "converged_env_steps": conv,
+            "prof": {"pcg_ms": 0.9 * ms, "pcg_iters": iters, "pcg_launches": 4 * steps,
+                     "pcg_bytes": 1e9 * iters, "pcg_threads": 512},
             "clocks": {"sm_mhz": sm_mhz, "sm_max_mhz": 1965.0, "reasons": reasons, "samples": 10},
-            "cg_iters_per_step": iters / steps, "newton_iters_per_step": 4.0,
-            "last_step_cg_iters_mean_env": [iters / steps / 16]}
+            "newton_per_env_step": 4.0, "cg_per_env_step": iters / env_steps}
 
 
-def test_merge_runs_aggregates_episodes():
-    a = _run(160, 10, 1000.0, 3000, 500, 1965.0, [])
-    b = _run(160, 10, 3000.0, 5000, 700, 1900.0, ["sw_power_cap"])
-    m = bench.merge_runs(a, b)
+def test_merge_aggregates_episodes():
+    a = _run(160, 10, 1000.0, 3000, 500, 1965.0, [], 150)
+    b = _run(160, 10, 3000.0, 5000, 700, 1900.0, ["sw_power_cap"], 160)
+    m = bench.merge(a, b)
     assert m["env_steps"] == 320 and m["steps"] == 20 and m["ms"] == 4000.0 and m["launches"] == 1200
-    assert m["value"] == 320 / 4.0  # env-steps over the summed timed seconds, not a mean of rates
+    assert m["e2e_ms"] == 1.1 * 4000.0 and m["converged_env_steps"] == 310 and len(m["step_ms"]) == 20
     assert m["prof"]["pcg_iters"] == 8000 and m["prof"]["pcg_bytes"] == 8e12
     assert m["prof"]["pcg_threads"] == 512  # a launch shape, not a sum
-    assert m["cg_iters_per_step"] == 400.0 and m["newton_iters_per_step"] == 4.0
+    assert m["cg_per_env_step"] == 8000 / 320 and m["newton_per_env_step"] == 4.0
     assert m["clocks"]["reasons"] == ["sw_power_cap"] and m["clocks"]["samples"] == 20
-    assert m["last_step_cg_iters_mean_env"] == a["last_step_cg_iters_mean_env"] + b["last_step_cg_iters_mean_env"]
 
 
 def test_batched_workloads_and_newton_caps(monkeypatch):
@@ -32,7 +33,7 @@ def test_batched_workloads_and_newton_caps(monkeypatch):
     assert len(bodies) == 3 and "3 uneven bodies" in desc
     (bodies2, _), _ = bench.build_workload("cfg3", seed=5)
     assert [b.n_nodes for b in bodies] == [b.n_nodes for b in bodies2]  # seeded
-    (held_out, _), _ = bench.build_workload("cfg3", seed=1005)
+    (held_out, _), _ = bench.build_workload("cfg3", seed=bench.TRAIN_SEED0 + 5)
     assert [b.n_nodes for b in held_out] != [b.n_nodes for b in bodies]
 
     class A:
@@ -41,3 +42,23 @@ def test_batched_workloads_and_newton_caps(monkeypatch):
     assert bench.newton_max_iter(A) == 12
     A.workload = "cfg1"
     assert bench.newton_max_iter(A) == 50
+
+
+def test_both_arms_print_the_same_config(monkeypatch):
+    """--impl reference and ours build `config` from the workload alone."""
+    monkeypatch.setenv("SDX_CFG2_ENVS", "4")
+    args = argparse.Namespace(workload="cfg2", newton_max_iter=0, steps=20, warmup=5)
+    (bodies, _), desc = bench.build_workload("cfg2", seed=0)
+    c1 = bench.workload_config(args, 0, bodies, desc, 1)
+    (bodies2, _), desc2 = bench.build_workload("cfg2", seed=0)
+    c2 = bench.workload_config(args, 0, bodies2, desc2, 1)
+    assert c1 == c2 and c1["n_envs"] == 4 and c1["n_tets"] == sum(b.n_tets for b in bodies)
+
+
+def test_cpu_sample_is_bounded(monkeypatch):
+    monkeypatch.setenv("SDX_CFG2_ENVS", "64")
+    (bodies, _), _ = bench.build_workload("cfg2", seed=0)
+    idx = bench.sample_envs(bodies, 400000)
+    assert idx == list(range(len(idx))) and len(idx) >= 1
+    assert sum(bodies[i].n_tets for i in idx) <= 400000 or len(idx) == 1
+    assert bench.sample_envs(bodies, 1) == [0]
