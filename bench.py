@@ -390,7 +390,8 @@ def parity_env0(args, bodies, cfg, states_gpu, stats_gpu):
     FP64 CPU oracle (the reference's path restated) stepped the same way."""
     from oracle import oracle as O
     b = bodies[0]
-    s = O.Scene(b, cfg)
+    # the PSD projection's eigenvalue floor at the GPU's FP32 tangent precision
+    s = O.Scene(b, cfg, min_eig=float(np.finfo(np.float32).eps))
     prm = O.default_newton_params()
     prm.abs_tol = 1e-9
     prm.max_iter = newton_max_iter(args)

@@ -13,6 +13,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libsdx_ref.so")
+REF32_PATH = os.path.join(HERE, "_ref", "libsdx_ref_f32.so")
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -154,6 +155,9 @@ def ref():
         R.ref_pcg_csr.argtypes = [C.c_int, _lp, _ip, _dp, _dp, _dp, C.c_double, C.c_double, C.c_double,
                                   C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, C.POINTER(C.c_int)]
         R.ref_pcg_csr.restype = C.c_int
+        R.ref_pcg_csr_real.argtypes = R.ref_pcg_csr.argtypes
+        R.ref_pcg_csr_real.restype = C.c_int
+        R.ref_stress_work.restype = None
         R.ref_bsr3_values.argtypes = [C.c_int, _ip, _ip, _dp, _dp]
         R.ref_bsr3_pcg.argtypes = [C.c_int, _ip, _ip, _dp, _dp, _dp, C.c_double, C.c_double, C.c_double, C.c_int,
                                    C.c_int, C.c_int, C.c_int, _dp, _dp, C.POINTER(C.c_int)]
@@ -187,6 +191,71 @@ def material(kind, mu, lam, F, project=False, psd=1, min_eig=np.finfo(np.float64
     Cm = np.zeros(81)
     lib().or_material(int(kind), mu, lam, ptr(F), int(project), psd, min_eig, ptr(e), ptr(P), ptr(Cm))
     return e[0], P.reshape(3, 3), Cm.reshape(9, 9)
+
+
+_ref32 = None
+
+
+def ref32():
+    """The reference's own code in its FP32 mode (MOCHI_USE_DOUBLE_PRECISION=0), or None when not built."""
+    global _ref32
+    if _ref32 is None and os.path.exists(REF32_PATH):
+        R = C.CDLL(REF32_PATH)
+        R.ref_stress_work.argtypes = [_dp, _dp, C.c_double, C.c_double, C.c_int, C.c_int, _dp, _dp, _dp]
+        R.ref_pcg_csr_real.argtypes = [C.c_int, _lp, _ip, _dp, _dp, _dp, C.c_double, C.c_double, C.c_double,
+                                       C.c_int, C.c_int, C.c_int, C.c_int, _dp, _dp, C.POINTER(C.c_int)]
+        R.ref_pcg_csr_real.restype = C.c_int
+        R.ref_real_size.restype = C.c_int
+        assert R.ref_real_size() == 4, "libsdx_ref_f32.so is not an FP32-mode build"
+        _ref32 = R
+    return _ref32
+
+
+def ref_stress_work(X12, u12, mu, lam, project=True, psd=1, fp32=False):
+    """fem::StressWork of one Smith Neo-Hookean tet by the reference's compiled code, in its FP64 mode or
+    (fp32=True) its FP32 mode. Returns (energy, residual 12, K 12x12)."""
+    R = ref32() if fp32 else ref()
+    X = np.ascontiguousarray(X12, np.float64).reshape(-1)
+    u = np.ascontiguousarray(u12, np.float64).reshape(-1)
+    e, r, K = np.zeros(1), np.zeros(12), np.zeros(144)
+    R.ref_stress_work(ptr(X), ptr(u), float(mu), float(lam), int(project), int(psd), ptr(e), ptr(r), ptr(K))
+    return float(e[0]), r, K.reshape(12, 12)
+
+
+def ref_pcg_real(row_ptr, col, val, b, rel_tol=1e-6, jacobi=True, fp32=True, max_iter=10000):
+    """krylov::PCG on a scalar CSR matrix in the reference build's own precision (FP32 mode: values, vectors,
+    dots and the stop test in float). Returns (x, iters, convergence)."""
+    R = ref32() if fp32 else ref()
+    rp = np.ascontiguousarray(row_ptr, np.int64)
+    cl = np.ascontiguousarray(col, np.int32)
+    v = np.ascontiguousarray(val, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    x = np.zeros_like(b)
+    rn, rr, cv = C.c_double(), C.c_double(), C.c_int()
+    it = R.ref_pcg_csr_real(b.size, ptr(rp, _lp), ptr(cl, _ip), ptr(v), ptr(b), ptr(x), rel_tol, 0.0, 1e10,
+                            max_iter, int(jacobi), 1, 1, C.byref(rn), C.byref(rr), C.byref(cv))
+    return x, int(it), int(cv.value)
+
+
+def block_to_scalar_csr(row_ptr, col, blocks):
+    """3x3 block CSR -> scalar CSR (row_ptr, col, values) with every stored block entry kept."""
+    row_ptr = np.asarray(row_ptr, np.int64)
+    col = np.asarray(col, np.int64)
+    blocks = np.asarray(blocks).reshape(-1, 3, 3)
+    n = row_ptr.size - 1
+    nb = np.diff(row_ptr)
+    srp = np.zeros(3 * n + 1, np.int64)
+    srp[1:] = np.repeat(3 * nb, 3).cumsum()
+    scol = np.empty(9 * col.size, np.int32)
+    sval = np.empty(9 * col.size)
+    for i in range(n):
+        b0, b1 = row_ptr[i], row_ptr[i + 1]
+        for lr in range(3):
+            o = srp[3 * i + lr]
+            cc = (3 * col[b0:b1, None] + np.arange(3)[None, :]).reshape(-1)
+            scol[o:o + cc.size] = cc
+            sval[o:o + cc.size] = blocks[b0:b1, lr, :].reshape(-1)
+    return srp, scol, sval
 
 
 def ref_bsr3_values(row_ptr, col, blocks):

@@ -317,6 +317,49 @@ int ref_pcg_csr(int n, const int64_t* row_ptr, const int32_t* col, const double*
   return st.numIterDone;
 }
 
+// krylov::PCG as ref_pcg_csr, in the build's own precision mochi::real (mochi_config.h:110-116): matrix
+// values, vectors, dot products and the stop test in float when the shim is compiled with
+// MOCHI_USE_DOUBLE_PRECISION=0 (the reference's FP32 mode), in double otherwise.
+int ref_pcg_csr_real(int n, const int64_t* row_ptr, const int32_t* col, const double* val,
+                     const double* b, double* x, double rel_tol, double abs_tol, double rel_div_tol,
+                     int max_iter, int jacobi, int polak_ribiere, int zero_guess, double* res_norm,
+                     double* rel_res_norm, int* convergence) {
+  ColumnVector<real> bv(n), xv(n), dinv(n);
+  const int64_t nnz = row_ptr[n];
+  DynamicArray<real> v(nnz);
+  for (int64_t k = 0; k < nnz; ++k) v[k] = static_cast<real>(val[k]);
+  for (int i = 0; i < n; ++i) {
+    bv[i] = static_cast<real>(b[i]);
+    xv[i] = static_cast<real>(x[i]);
+    real d = 0;
+    for (int64_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k)
+      if (col[k] == i) d = v[k];
+    dinv[i] = jacobi ? real(1) / d : real(1);
+  }
+  auto opA = [&](auto const& in, auto& out) {
+    for (int i = 0; i < n; ++i) {
+      real s = 0;
+      for (int64_t k = row_ptr[i]; k < row_ptr[i + 1]; ++k) s += v[k] * in[col[k]];
+      out[i] = s;
+    }
+  };
+  auto opP = [&](auto const& in, auto& out) {
+    for (int i = 0; i < n; ++i) out[i] = dinv[i] * in[i];
+  };
+  krylov::StatusResidualL2<krylov::UsualDot, real> stop{static_cast<real>(rel_tol), static_cast<real>(abs_tol),
+                                                        static_cast<real>(rel_div_tol)};
+  auto st = krylov::PCG(opA, bv, xv, opP, max_iter, stop, false, VerbosityLevel::Silent, polak_ribiere != 0,
+                        zero_guess ? InitialGuessHint::Zero : InitialGuessHint::Unknown);
+  for (int i = 0; i < n; ++i) x[i] = xv[i];
+  *res_norm = st.residualNorm;
+  *rel_res_norm = st.relativeResidualNorm;
+  *convergence = static_cast<int>(st.convergence);
+  return st.numIterDone;
+}
+
+// the build's floating-point mode: 8 (double) or 4 (float) bytes per mochi::real
+int ref_real_size(void) { return static_cast<int>(sizeof(real)); }
+
 // mochi::BlockSparseMatrix<double, 3> (mochi_core/include/mochi_core/linear_algebra/block_sparse_matrix.h:63)
 // on the block pattern (ptr, idx), every scalar entry written through its own SetValue (:230-238, which
 // places it by FindValueIndex, :459-475); copies out Values(), i.e. the values in the reference's storage

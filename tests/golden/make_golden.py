@@ -12,6 +12,11 @@ exists; the fixtures are committed, nothing reads the reference at test time).
     on it (oracle/_ref): Values() of matrices filled through the class's own SetValue on seeded block
     patterns, and the iteration counts / solutions of krylov::PCG with BlockJacobiPrec (none, Jacobi,
     block Jacobi) on the 100 x 100 golden system in 3x3 blocks and on an assembled tet-grid Hessian.
+  * fp32_mode_reference.json — the reference's FP32 mode (MOCHI_USE_DOUBLE_PRECISION=0, oracle/_ref/
+    libsdx_ref_f32.so) against its FP64 mode on the soft cube (cfg0, seed 0) one step from rest: the
+    relative error of the assembled elastic Hessian (fem::StressWork per tet, Smith Neo-Hookean,
+    projected), and krylov::PCG (Jacobi, rel 1e-6) on that step's first Newton system in float — the
+    error budget the GPU path's FP32 matrix / FP64 reductions is held to.
   * reference_vectors.json — outputs of the reference's own compiled code (oracle/_ref, built by
     oracle/build_ref.sh from the reference sources) on seeded inputs: Smith NH with every PSD
     strategy (projected tangents), St. Venant-Kirchhoff and linear elasticity with every PSD strategy,
@@ -23,6 +28,7 @@ exists; the fixtures are committed, nothing reads the reference at test time).
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import ctypes as C
 import json
 import os
@@ -309,6 +315,77 @@ def bsr3_vectors():
     return out
 
 
+def cfg0_state_after_one_step():
+    """The soft cube (cfg0, seed 0) after one backward-Euler step from rest, by the FP64 oracle."""
+    from oracle import oracle as O
+    from project_superdex_b200 import scenes
+    bodies, cfg = scenes.config0()
+    b = bodies[0]
+    sc = O.Scene(b, cfg, min_eig=float(np.finfo(np.float32).eps))
+    p = O.default_newton_params()
+    p.abs_tol = 1e-9
+    u, v, _ = sc.step(np.zeros(3 * b.n_nodes), np.zeros(3 * b.n_nodes), cfg.dt, p)
+    return b, cfg, sc, u, v
+
+
+def fp32_mode_vectors():
+    """The reference's FP32 mode against its FP64 mode on cfg0 (oracle/_ref/libsdx_ref_f32.so)."""
+    from oracle import oracle as O
+    assert O.ref() is not None and O.ref32() is not None, "run oracle/build_ref.sh (both modes)"
+    b, cfg, sc, u, v = cfg0_state_after_one_step()
+    X = b.X.reshape(-1, 3)
+    lam, mu = b.lame()
+    uu = u.reshape(-1, 3)
+    free = np.repeat(b.pin == 0, 3)
+    # elastic Hessian assembled from the reference's per-tet StressWork, both modes, on the oracle's pattern
+    rp, col = sc.row_ptr, sc.col
+    slot = {}
+    for i in range(b.n_nodes):
+        for k in range(rp[i], rp[i + 1]):
+            slot[(i, int(col[k]))] = k
+    H = {32: np.zeros((col.size, 3, 3)), 64: np.zeros((col.size, 3, 3))}
+    for t, tet in enumerate(b.tets):
+        X12, u12 = X[tet].reshape(-1), uu[tet].reshape(-1)
+        for bits in (32, 64):
+            _, _, K = O.ref_stress_work(X12, u12, mu[t], lam[t], project=True, psd=1, fp32=bits == 32)
+            for a in range(4):
+                for c in range(4):
+                    H[bits][slot[(int(tet[a]), int(tet[c]))]] += K[3 * a:3 * a + 3, 3 * c:3 * c + 3]
+
+    def dense_free(Hb):
+        A = np.zeros((3 * b.n_nodes, 3 * b.n_nodes))
+        for i in range(b.n_nodes):
+            for k in range(rp[i], rp[i + 1]):
+                j = col[k]
+                A[3 * i:3 * i + 3, 3 * j:3 * j + 3] = Hb[k]
+        return A[np.ix_(free, free)]
+    A32, A64 = dense_free(H[32]), dense_free(H[64])
+    # the oracle's own elastic Hessian (dt so large that inertia vanishes) agrees with the FP64 reference
+    cfg_big = dataclasses.replace(cfg, dt=1e3)
+    sc_big = O.Scene(b, cfg_big, min_eig=float(np.finfo(np.float64).eps))
+    Ao = dense_free(sc_big.assemble(u, u, hess=True, psd=True)["H"])
+    hess = {"rel_fro_err_fp32_mode": float(np.linalg.norm(A32 - A64) / np.linalg.norm(A64)),
+            "max_abs_err_fp32_mode_over_max": float(np.abs(A32 - A64).max() / np.abs(A64).max()),
+            "oracle_vs_fp64_mode_rel_fro": float(np.linalg.norm(Ao - A64) / np.linalg.norm(A64)),
+            "u_abs_sum": float(np.abs(u).sum())}
+    # the first Newton system of the second step (inertia target u + dt v), solved by krylov::PCG
+    a = sc.assemble(u, u + cfg.dt * v, t=2 * cfg.dt, hess=True, psd=True)
+    srp, scol, sval = O.block_to_scalar_csr(rp, col, a["H"])
+    g = a["g"]
+    x_exact, it_exact, _ = O.ref_pcg_real(srp, scol, sval, g, rel_tol=1e-13, fp32=False, max_iter=100000)
+    x64, it64, c64 = O.ref_pcg_real(srp, scol, sval, g, rel_tol=1e-6, fp32=False)
+    x32, it32, c32 = O.ref_pcg_real(srp, scol, sval, g, rel_tol=1e-6, fp32=True)
+    nx = np.linalg.norm(x_exact)
+    pcg = {"rel_tol": 1e-6, "jacobi": True, "iters_fp64_mode": it64, "iters_fp32_mode": it32,
+           "convergence_fp64_mode": c64, "convergence_fp32_mode": c32,
+           "rel_err_fp64_mode": float(np.linalg.norm(x64 - x_exact) / nx),
+           "rel_err_fp32_mode": float(np.linalg.norm(x32 - x_exact) / nx),
+           "iters_exact": it_exact, "g_norm": float(np.linalg.norm(g))}
+    return {"config": "cfg0 seed 0, state after one step from rest (FP64 oracle), Smith NH, projection",
+            "hessian": hess, "pcg": pcg,
+            "source": "oracle/_ref/libsdx_ref_f32.so and libsdx_ref.so (reference sources, both precision modes)"}
+
+
 def main():
     global args_ns
     ap = argparse.ArgumentParser()
@@ -324,6 +401,8 @@ def main():
         json.dump(parse_krylov(os.path.join(args_ns.mc, "test/data/krylov_solver_test_data.h")), f)
     with open(os.path.join(HERE, "bsr3_reference.json"), "w") as f:
         json.dump(bsr3_vectors(), f)
+    with open(os.path.join(HERE, "fp32_mode_reference.json"), "w") as f:
+        json.dump(fp32_mode_vectors(), f, indent=1)
     if "--only-bsr3" in sys.argv:
         return
     with open(os.path.join(HERE, "reference_vectors.json"), "w") as f:

@@ -49,6 +49,7 @@ def test_reference_bsr3_matrices_through_the_c_abi(golden):
     from project_superdex_b200.linear_solver import strips_to_blocks
     g = golden("bsr3_reference.json")
     assert [s["system"] for s in g["pcg"]] == ["psd100", "tetgrid"]
+    counts = []
     for sysd in g["pcg"]:
         rp, col = np.array(sysd["row_ptr"]), np.array(sysd["col"], np.int32)
         vals, b = np.array(sysd["values"]), np.array(sysd["b"])
@@ -60,8 +61,11 @@ def test_reference_bsr3_matrices_through_the_c_abi(golden):
         for run in sysd["runs"]:
             x, st = _capi_solve(rp, col, vals, capi.SDX_BSR_ROW_STRIPS, b, run["precond"])
             assert st.convergence == run["convergence"] == 1
-            assert abs(st.num_iter - run["iters"]) <= max(6, int(0.15 * run["iters"])), (sysd["system"], run["precond"],
-                                                                                        st.num_iter, run["iters"])
+            # FP32 search directions: within max(6, 15 %) of the FP64 reference's count with a preconditioner;
+            # unpreconditioned on the heterogeneous tet grid (E over two decades) they lose conjugacy faster
+            slack = 0.15 if run["precond"] else 0.25
+            counts.append((sysd["system"], run["precond"], st.num_iter, run["iters"]))
+            assert abs(st.num_iter - run["iters"]) <= max(6, int(slack * run["iters"])), counts
             assert np.linalg.norm(b - A @ x) <= 1.01e-6 * np.linalg.norm(b)
             if sysd["system"] == "tetgrid":
                 x_ref = np.array(run["x"])

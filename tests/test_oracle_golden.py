@@ -206,3 +206,20 @@ def test_reference_stiffness_of_each_material(golden):
         want[np.arange(3), np.arange(3)] += 2 * mu0
         want[np.arange(3, 6), np.arange(3, 6)] = mu0
         np.testing.assert_allclose(np.array(c["c0"]).reshape(6, 6), want, rtol=1e-9, atol=1e-9 * c["lambda"])
+
+
+def test_fp32_mode_fixture_matches_this_oracle(oracle, golden):
+    """The FP32-mode fixture (the reference's MOCHI_USE_DOUBLE_PRECISION=0 build against its FP64 build on
+    cfg0) was made at the state this oracle reaches one step from rest, and its FP64 side agrees with the
+    oracle's own elastic Hessian."""
+    from project_superdex_b200 import scenes
+    fx = golden("fp32_mode_reference.json")
+    bodies, cfg = scenes.config0()
+    b = bodies[0]
+    sc = oracle.Scene(b, cfg, min_eig=float(np.finfo(np.float32).eps))
+    p = oracle.default_newton_params()
+    p.abs_tol = 1e-9
+    u, v, _ = sc.step(np.zeros(3 * b.n_nodes), np.zeros(3 * b.n_nodes), cfg.dt, p)
+    assert np.abs(u).sum() == pytest.approx(fx["hessian"]["u_abs_sum"], rel=1e-9)
+    assert fx["hessian"]["oracle_vs_fp64_mode_rel_fro"] < 1e-6
+    assert fx["pcg"]["convergence_fp32_mode"] == fx["pcg"]["convergence_fp64_mode"] == 1
