@@ -231,59 +231,159 @@ __device__ __forceinline__ void svd3_rv(const float F[9], float U[9], float s[3]
 // (u_j v_k^T - u_k v_j^T)/sqrt(2) and the flips (u_j v_k^T + u_k v_j^T)/sqrt(2) for the pairs
 // (j,k) = (1,2), (0,2), (0,1). Eigenvalues are clamped at min_eig (psd 1) or |l| then min_eig (psd 2).
 
-__device__ __forceinline__ void modal_tangent_f32(const float U[9], const float V[9], const float A[9],
-                                                  const float tw[3], const float fl[3], int psd, float min_eig,
-                                                  float C[81]) {
-  float wa[3], Va[9];
-  sym_eig3(A, wa, Va);
-  float lam[9] = {wa[0], wa[1], wa[2], tw[0], tw[1], tw[2], fl[0], fl[1], fl[2]};
+// The element stiffness is never formed as a 9x9 tangent: every 3x3 block K_fg = vol B_f^T C B_g of
+// fem::StressWork (fem_stress.h:218-241) is evaluated from a factored form of the tangent C = dP/dF and the
+// shape-function gradients d_f, d_g of the two nodes (TanForm, tan_block). Kinds:
+//   kTanModal   C = sum_i l_i m_i m_i^T over the 9 modes above (eigenvalues clamped):
+//               K_fg = U H(y_f, y_g) U^T with y = V^T d, H_ab = Ah_ab y_f[a] y_g[b] for the scaling block
+//               Ah = Va diag(l_a) Va^T, and per pair (j, k) of twist l_t / flip l_f with sp = (l_t + l_f) / 2,
+//               sm = (l_f - l_t) / 2: H_jj += sp y_f[k] y_g[k], H_kk += sp y_f[j] y_g[j],
+//               H_jk += sm y_f[k] y_g[j], H_kj += sm y_f[j] y_g[k]; plus c_iso (d_f . d_g) I (ARAP's mu I);
+//   kTanSnh     the direct Smith Neo-Hookean tangent c3 F (x) F + lambdaHat cof (x) cof + c2 I + d2c d2J/dF2:
+//               K_fg = c3 a_f a_g^T + lambdaHat b_f b_g^T + c2 (d_f . d_g) I + d2c [F (d_f x d_g)]_x with
+//               a = F d, b = cof(F) d and [z]_x_rc = eps_rcx z_x;
+//   kTanStvk    the direct St. Venant-Kirchhoff tangent: K_fg = lambda a_f a_g^T + mu a_g a_f^T + (d_g^T S d_f) I
+//               + mu (d_f . d_g) F F^T;
+//   kTanLinear  K_fg = mu (d_f . d_g) I + mu d_g d_f^T + lambda d_f d_g^T.
+// The register footprint is a few dozen floats instead of the 81 of C (and 81 more for the modes).
+constexpr int kTanModal = 0, kTanSnh = 1, kTanStvk = 2, kTanLinear = 3;
+
+struct TanForm {
+  int kind;
+  float c0, c1, c2, c3;  // Snh: c3, lambdaHat, c2, d2c; Stvk: lambda, mu; Linear: mu, lambda; Modal: c_iso
+  float q0[9];           // Modal: U; Snh / Stvk: F
+  float q1[9];           // Modal: V; Snh: cof F; Stvk: S
+  float q2[6];           // Modal: Ah (00, 11, 22, 12, 02, 01); Stvk: F F^T (same order)
+  float sp[3], sm[3];    // Modal: pair coefficients
+};
+
+__device__ __forceinline__ void mat3_vec(const float M[9], const float d[3], float o[3]) {
 #pragma unroll
-  for (int i = 0; i < 9; ++i) {
-    float l = (psd == 2) ? fabsf(lam[i]) : lam[i];
-    lam[i] = fmaxf(l, min_eig);
-  }
-  float M[9][9];
+  for (int r = 0; r < 3; ++r) o[r] = M[r * 3 + 0] * d[0] + M[r * 3 + 1] * d[1] + M[r * 3 + 2] * d[2];
+}
+
+__device__ __forceinline__ void mat3t_vec(const float M[9], const float d[3], float o[3]) {
 #pragma unroll
-  for (int i = 0; i < 3; ++i)
+  for (int c = 0; c < 3; ++c) o[c] = M[0 * 3 + c] * d[0] + M[1 * 3 + c] * d[1] + M[2 * 3 + c] * d[2];
+}
+
+// K (row-major 3x3, without the volume factor) of the node pair (f, g) with gradients df, dg.
+__device__ __forceinline__ void tan_block(const TanForm& T, const float df[3], const float dg[3], float K[9]) {
+  const float dd = df[0] * dg[0] + df[1] * dg[1] + df[2] * dg[2];
+  if (T.kind == kTanModal) {
+    float yf[3], yg[3];
+    mat3t_vec(T.q1, df, yf);
+    mat3t_vec(T.q1, dg, yg);
+    float H[9];
+    H[0] = T.q2[0] * yf[0] * yg[0];
+    H[4] = T.q2[1] * yf[1] * yg[1];
+    H[8] = T.q2[2] * yf[2] * yg[2];
+    H[5] = T.q2[3] * yf[1] * yg[2];
+    H[7] = T.q2[3] * yf[2] * yg[1];
+    H[2] = T.q2[4] * yf[0] * yg[2];
+    H[6] = T.q2[4] * yf[2] * yg[0];
+    H[1] = T.q2[5] * yf[0] * yg[1];
+    H[3] = T.q2[5] * yf[1] * yg[0];
+#pragma unroll
+    for (int n = 0; n < 3; ++n) {
+      const int j = (n == 0) ? 1 : 0;
+      const int k = (n == 2) ? 1 : 2;
+      H[j * 3 + j] += T.sp[n] * yf[k] * yg[k];
+      H[k * 3 + k] += T.sp[n] * yf[j] * yg[j];
+      H[j * 3 + k] += T.sm[n] * yf[k] * yg[j];
+      H[k * 3 + j] += T.sm[n] * yf[j] * yg[k];
+    }
+    float HU[9];  // H U^T
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        HU[a * 3 + c] = H[a * 3 + 0] * T.q0[c * 3 + 0] + H[a * 3 + 1] * T.q0[c * 3 + 1] + H[a * 3 + 2] * T.q0[c * 3 + 2];
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
       for (int c = 0; c < 3; ++c)
-        M[i][r * 3 + c] = U[r * 3 + 0] * Va[0 * 3 + i] * V[c * 3 + 0] + U[r * 3 + 1] * Va[1 * 3 + i] * V[c * 3 + 1] +
-                          U[r * 3 + 2] * Va[2 * 3 + i] * V[c * 3 + 2];
-  const float rs2 = 0.70710678118654752f;
-#pragma unroll
-  for (int n = 0; n < 3; ++n) {
-    const int j = (n == 0) ? 1 : 0;
-    const int k = (n == 2) ? 1 : 2;
+        K[r * 3 + c] = T.q0[r * 3 + 0] * HU[0 * 3 + c] + T.q0[r * 3 + 1] * HU[1 * 3 + c] + T.q0[r * 3 + 2] * HU[2 * 3 + c] +
+                       (r == c ? T.c0 * dd : 0.0f);
+  } else if (T.kind == kTanSnh) {
+    float af[3], ag[3], bf[3], bg[3], w[3], z[3];
+    mat3_vec(T.q0, df, af);
+    mat3_vec(T.q0, dg, ag);
+    mat3_vec(T.q1, df, bf);
+    mat3_vec(T.q1, dg, bg);
+    w[0] = df[1] * dg[2] - df[2] * dg[1];
+    w[1] = df[2] * dg[0] - df[0] * dg[2];
+    w[2] = df[0] * dg[1] - df[1] * dg[0];
+    mat3_vec(T.q0, w, z);
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const float a = U[r * 3 + j] * V[c * 3 + k];
-        const float b = U[r * 3 + k] * V[c * 3 + j];
-        M[3 + n][r * 3 + c] = (a - b) * rs2;
-        M[6 + n][r * 3 + c] = (a + b) * rs2;
-      }
+      for (int c = 0; c < 3; ++c) K[r * 3 + c] = T.c0 * af[r] * ag[c] + T.c1 * bf[r] * bg[c] + (r == c ? T.c2 * dd : 0.0f);
+    K[1] += T.c3 * z[2];
+    K[2] -= T.c3 * z[1];
+    K[3] -= T.c3 * z[2];
+    K[5] += T.c3 * z[0];
+    K[6] += T.c3 * z[1];
+    K[7] -= T.c3 * z[0];
+  } else if (T.kind == kTanStvk) {
+    float af[3], ag[3], sf[3];
+    mat3_vec(T.q0, df, af);
+    mat3_vec(T.q0, dg, ag);
+    mat3_vec(T.q1, df, sf);
+    const float dsd = dg[0] * sf[0] + dg[1] * sf[1] + dg[2] * sf[2];
+    const float FFt[9] = {T.q2[0], T.q2[5], T.q2[4], T.q2[5], T.q2[1], T.q2[3], T.q2[4], T.q2[3], T.q2[2]};
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        K[r * 3 + c] = T.c0 * af[r] * ag[c] + T.c1 * ag[r] * af[c] + T.c1 * dd * FFt[r * 3 + c] + (r == c ? dsd : 0.0f);
+  } else {  // kTanLinear
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+        K[r * 3 + c] = T.c0 * dg[r] * df[c] + T.c1 * df[r] * dg[c] + (r == c ? T.c0 * dd : 0.0f);
+  }
+}
+
+// Modal form from the SVD F = U diag(s) V^T, the 3x3 scaling block A (singular basis) and the twist / flip
+// eigenvalues, every eigenvalue clamped at min_eig (psd 1) or |l| then min_eig (psd 2).
+__device__ __forceinline__ void modal_tanform(const float U[9], const float V[9], const float A[9], const float tw[3],
+                                              const float fl[3], int psd, float min_eig, TanForm& T) {
+  float wa[3], Va[9];
+  sym_eig3(A, wa, Va);
+  auto clamp = [&](float l) { return fmaxf(psd == 2 ? fabsf(l) : l, min_eig); };
+#pragma unroll
+  for (int i = 0; i < 3; ++i) wa[i] = clamp(wa[i]);
+  auto ah = [&](int a, int b) { return Va[a * 3 + 0] * wa[0] * Va[b * 3 + 0] + Va[a * 3 + 1] * wa[1] * Va[b * 3 + 1] +
+                                       Va[a * 3 + 2] * wa[2] * Va[b * 3 + 2]; };
+  T.kind = kTanModal;
+  T.c0 = 0.0f;
+  T.q2[0] = ah(0, 0);
+  T.q2[1] = ah(1, 1);
+  T.q2[2] = ah(2, 2);
+  T.q2[3] = ah(1, 2);
+  T.q2[4] = ah(0, 2);
+  T.q2[5] = ah(0, 1);
+#pragma unroll
+  for (int n = 0; n < 3; ++n) {
+    const float lt = clamp(tw[n]), lf = clamp(fl[n]);
+    T.sp[n] = 0.5f * (lt + lf);
+    T.sm[n] = 0.5f * (lf - lt);
   }
 #pragma unroll
-  for (int a = 0; a < 9; ++a)
-#pragma unroll
-    for (int b = a; b < 9; ++b) {
-      float v = 0.0f;
-#pragma unroll
-      for (int i = 0; i < 9; ++i) v = fmaf(lam[i] * M[i][a], M[i][b], v);
-      C[a * 9 + b] = v;
-      C[b * 9 + a] = v;
-    }
+  for (int i = 0; i < 9; ++i) {
+    T.q0[i] = U[i];
+    T.q1[i] = V[i];
+  }
 }
 
 // ------------------------------------------------------------------------------------------------
-// FP32 tangent dP/dF (9x9, symmetric, full storage C[a*9+b]) with the reference's PSD handling.
+// FP32 tangent dP/dF in factored form (TanForm) with the reference's PSD handling.
 // psd: 0 none, 1 projection (max(l, eps)), 2 |l| projection, 3 fast (drop d2J when indefinite).
 
-__device__ __forceinline__ void snh_tangent_f32(float mu, float lambda, const float F[9], int project,
-                                                int psd, float min_eig, float C[81]) {
+__device__ __forceinline__ void snh_tanform(float mu, float lambda, const float F[9], int project,
+                                            int psd, float min_eig, TanForm& T) {
   const float muHat = mu * (4.0f / 3.0f);
   const float lambdaHat = lambda + mu * (5.0f / 6.0f);
   const float alpha = 1.0f + 0.75f * muHat / lambdaHat;
@@ -340,24 +440,20 @@ __device__ __forceinline__ void snh_tangent_f32(float mu, float lambda, const fl
     A[1] = A[3] = J2al * s[2] + mu2 * s[0] * s[1] * Ic2inv;
     A[2] = A[6] = J2al * s[1] + mu2 * s[0] * s[2] * Ic2inv;
     A[5] = A[7] = J2al * s[0] + mu2 * s[1] * s[2] * Ic2inv;
-    modal_tangent_f32(U, V, A, tw, fl, psd, min_eig, C);
+    modal_tanform(U, V, A, tw, fl, psd, min_eig, T);
     return;
   }
 
-  // Direct tangent (batched_smith_neo_hookean.cpp:204-266).
-  float cof[9];
-  cof3(F, cof);
-  const float d2c = (projecting && psd == 3) ? 0.0f : lambdaHat * Jma;
+  // Direct tangent (batched_smith_neo_hookean.cpp:204-266): c3 F (x) F + lambdaHat cof (x) cof + c2 I +
+  // d2c d2J/dF2 (the last dropped by the fast strategy when indefinite).
+  T.kind = kTanSnh;
+  cof3(F, T.q1);
 #pragma unroll
-  for (int a = 0; a < 9; ++a)
-#pragma unroll
-    for (int b = a; b < 9; ++b) {
-      float v = c3 * F[a] * F[b] + lambdaHat * cof[a] * cof[b];
-      if (a == b) v += c2;
-      if (hj_sign(a, b) != 0) v += float(hj_sign(a, b)) * d2c * F[hj_index(a, b)];
-      C[a * 9 + b] = v;
-      C[b * 9 + a] = v;
-    }
+  for (int i = 0; i < 9; ++i) T.q0[i] = F[i];
+  T.c0 = c3;
+  T.c1 = lambdaHat;
+  T.c2 = c2;
+  T.c3 = (projecting && psd == 3) ? 0.0f : lambdaHat * Jma;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -396,8 +492,8 @@ __device__ __forceinline__ void stvk_energy_pk1_f64(double mu, double lambda, co
   }
 }
 
-__device__ __forceinline__ void stvk_tangent_f32(float mu, float lambda, const float F[9], int project, int psd,
-                                                 float min_eig, float C[81]) {
+__device__ __forceinline__ void stvk_tanform(float mu, float lambda, const float F[9], int project, int psd,
+                                             float min_eig, TanForm& T) {
   if (project && (psd == 1 || psd == 2)) {
     // eigensystem (batched_st_venant_kirchhoff.cpp:96-154): base = -mu + lambda (I2 - 3) / 2
     float U[9], s[3], V[9];
@@ -419,7 +515,7 @@ __device__ __forceinline__ void stvk_tangent_f32(float mu, float lambda, const f
     A[1] = A[3] = lambda * s[0] * s[1];
     A[2] = A[6] = lambda * s[0] * s[2];
     A[5] = A[7] = lambda * s[1] * s[2];
-    modal_tangent_f32(U, V, A, tw, fl, psd, min_eig, C);
+    modal_tanform(U, V, A, tw, fl, psd, min_eig, T);
     return;
   }
   // direct tangent dP_rc/dF_ij = delta_ri S_jc + mu F_rj F_ic + mu delta_jc (F F^T)_ri + lambda F_ij F_rc
@@ -435,27 +531,21 @@ __device__ __forceinline__ void stvk_tangent_f32(float mu, float lambda, const f
     for (int i = 0; i < 9; ++i) G[i] = (i % 4 == 0) ? fmaxf(G[i], 0.0f) : 0.0f;
   }
   const float trG = G[0] + G[4] + G[8];
-  float S[9], FFt[9];
+  T.kind = kTanStvk;
+  T.c0 = lambda;
+  T.c1 = mu;
 #pragma unroll
-  for (int i = 0; i < 9; ++i) S[i] = 2.0f * mu * G[i] + ((i % 4 == 0) ? lambda * trG : 0.0f);
-#pragma unroll
-  for (int r = 0; r < 3; ++r)
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-      FFt[r * 3 + i] = F[r * 3 + 0] * F[i * 3 + 0] + F[r * 3 + 1] * F[i * 3 + 1] + F[r * 3 + 2] * F[i * 3 + 2];
-#pragma unroll
-  for (int r = 0; r < 3; ++r)
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          float v = mu * F[r * 3 + j] * F[i * 3 + c] + lambda * F[i * 3 + j] * F[r * 3 + c];
-          if (r == i) v += S[j * 3 + c];
-          if (j == c) v += mu * FFt[r * 3 + i];
-          C[(r * 3 + c) * 9 + (i * 3 + j)] = v;
-        }
+  for (int i = 0; i < 9; ++i) {
+    T.q0[i] = F[i];
+    T.q1[i] = 2.0f * mu * G[i] + ((i % 4 == 0) ? lambda * trG : 0.0f);  // S
+  }
+  auto fft = [&](int r, int i) { return F[r * 3 + 0] * F[i * 3 + 0] + F[r * 3 + 1] * F[i * 3 + 1] + F[r * 3 + 2] * F[i * 3 + 2]; };
+  T.q2[0] = fft(0, 0);
+  T.q2[1] = fft(1, 1);
+  T.q2[2] = fft(2, 2);
+  T.q2[3] = fft(1, 2);
+  T.q2[4] = fft(0, 2);
+  T.q2[5] = fft(0, 1);
 }
 
 // eps = (F + F^T)/2 - I ; psi = mu eps:eps + lambda/2 tr(eps)^2 ; P = 2 mu eps + lambda tr(eps) I
@@ -590,11 +680,17 @@ __device__ __forceinline__ void arap_energy_pk1_f64(double mu, const double F[9]
   }
 }
 
-__device__ __forceinline__ void arap_tangent_f32(float mu, const float F[9], int project, int psd, float min_eig,
-                                                 float C[81]) {
+// ARAP (batched_arap.cpp:29-136): C = mu I + sum_n l_n T_n T_n^T over the three twists T_n = U (e_k e_j^T -
+// e_j e_k^T) V^T, l_n = -mu / (s_j + s_k) (projected: 2 l + mu clamped). In modal form: twist eigenvalue 2 l_n
+// and flip eigenvalue 0 of the normalized modes, no scaling block, plus mu I.
+__device__ __forceinline__ void arap_tanform(float mu, const float F[9], int project, int psd, float min_eig,
+                                             TanForm& T) {
   float U[9], s[3], V[9];
   svd3_rv(F, U, s, V);
-  float lam[3];
+  T.kind = kTanModal;
+  T.c0 = mu;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) T.q2[i] = 0.0f;
 #pragma unroll
   for (int n = 0; n < 3; ++n) {
     const int j = (n == 0) ? 1 : 0;
@@ -604,41 +700,20 @@ __device__ __forceinline__ void arap_tangent_f32(float mu, const float F[9], int
       const float e = 2.0f * l + mu;
       l = 0.5f * (fmaxf(psd == 2 ? fabsf(e) : e, min_eig) - mu);
     }
-    lam[n] = l;
-  }
-  float T[3][9];
-#pragma unroll
-  for (int n = 0; n < 3; ++n) {
-    const int j = (n == 0) ? 1 : 0;
-    const int k = (n == 2) ? 1 : 2;
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) T[n][r * 3 + c] = U[r * 3 + k] * V[c * 3 + j] - U[r * 3 + j] * V[c * 3 + k];
+    T.sp[n] = l;
+    T.sm[n] = -l;
   }
 #pragma unroll
-  for (int a = 0; a < 9; ++a)
-#pragma unroll
-    for (int b = a; b < 9; ++b) {
-      float v = (a == b) ? mu : 0.0f;
-#pragma unroll
-      for (int n = 0; n < 3; ++n) v = fmaf(lam[n] * T[n][a], T[n][b], v);
-      C[a * 9 + b] = v;
-      C[b * 9 + a] = v;
-    }
+  for (int i = 0; i < 9; ++i) {
+    T.q0[i] = U[i];
+    T.q1[i] = V[i];
+  }
 }
 
-__device__ __forceinline__ void linear_tangent_f32(float mu, float lambda, float C[81]) {
-#pragma unroll
-  for (int r = 0; r < 3; ++r)
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-          C[(r * 3 + c) * 9 + (i * 3 + j)] = mu * (float)((r == i && c == j) + (c == i && r == j)) +
-                                             lambda * (float)(r == c && i == j);
+__device__ __forceinline__ void linear_tanform(float mu, float lambda, TanForm& T) {
+  T.kind = kTanLinear;
+  T.c0 = mu;
+  T.c1 = lambda;
 }
 
 // ------------------------------------------------------------------------------------------------

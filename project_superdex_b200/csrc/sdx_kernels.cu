@@ -99,9 +99,11 @@ __device__ __forceinline__ void warp_env_add(double* obj, int env, double v) {
 }
 
 // kArap: the variant that also evaluates ARAP envs (SVD-based, more registers); launched only when some
-// env uses ARAP, so the other materials keep the lean variant.
-template <bool kArap>
-__global__ void __launch_bounds__(128) k_element(ElemArgs a) {
+// env uses ARAP, so the other materials keep the lean variant. kDamp: the variant with Rayleigh stiffness
+// damping (viscous stress, its residual, energy and Hessian terms), launched only when it is on. The lean
+// variant fits 128 registers, so 4 CTAs of 128 threads share an SM.
+template <bool kArap, bool kDamp>
+__global__ void __launch_bounds__(128, (kArap || kDamp) ? 1 : 4) k_element(ElemArgs a) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= a.n_tets) return;
   const int4 nd = a.tets[t];
@@ -129,7 +131,7 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
   // Rayleigh stiffness damping: viscous stress about the stage-start displacement
   // (fem_stress_damping.h:29-501; reference stiffness = the tet's lambda, mu)
   double Sv[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, dE[6];
-  if (a.kdamp > 0.0) {
+  if (kDamp && a.kdamp > 0.0) {
     double Fs[9] = {1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0};
 #pragma unroll
     for (int f = 0; f < 4; ++f)
@@ -148,18 +150,22 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
     const SnhConsts kc = snh_consts((double)mu, (double)lam);
     const double w = (double)vol;
     const double m = (double)rho * w / 20.0;
-    double acc[4][3], asum[3] = {0.0, 0.0, 0.0};
-    // mass damping (mochi_physics/src/mochi_soft.h:408-420): InertiaWork with scale alpha/dt about the
-    // stage-start displacement
-    double dmp[4][3], dsum[3] = {0.0, 0.0, 0.0};
+    // inertia about the target ut and mass damping about the stage start u0 (mochi_physics/src/mochi_soft.h:
+    // 408-420), P1Q4 consistent mass m (1 + delta_fg): per component the node sums, and for the energy the
+    // squares; the per-node differences are formed again where they are used (the targets come from L1)
+    double asum[3] = {0.0, 0.0, 0.0}, dsum[3] = {0.0, 0.0, 0.0}, ein = 0.0, edm = 0.0;
 #pragma unroll
     for (int f = 0; f < 4; ++f)
 #pragma unroll
       for (int r = 0; r < 3; ++r) {
-        acc[f][r] = uf[f][r] - a.ut[3 * (int64_t)rows[f] + r];
-        asum[r] += acc[f][r];
-        dmp[f][r] = a.mdamp > 0.0 ? uf[f][r] - a.u0[3 * (int64_t)rows[f] + r] : 0.0;
-        dsum[r] += dmp[f][r];
+        const double d_in = uf[f][r] - a.ut[3 * (int64_t)rows[f] + r];
+        asum[r] += d_in;
+        ein += d_in * d_in;
+        if (a.mdamp > 0.0) {
+          const double d_dm = uf[f][r] - a.u0[3 * (int64_t)rows[f] + r];
+          dsum[r] += d_dm;
+          edm += d_dm * d_dm;
+        }
       }
     if (want_res) {
       double P[9];
@@ -171,13 +177,16 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
         arap_energy_pk1_f64((double)mu, F, nullptr, P);
       else
         snh_pk1_f64(kc, F, P);
-      if (a.kdamp > 0.0) {  // + F S_visc
+      if (kDamp && a.kdamp > 0.0) {  // + F S_visc
         const double S[9] = {Sv[0], Sv[5], Sv[4], Sv[5], Sv[1], Sv[3], Sv[4], Sv[3], Sv[2]};
+        double FS[9];
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
           for (int c = 0; c < 3; ++c)
-            P[r * 3 + c] += F[r * 3 + 0] * S[c] + F[r * 3 + 1] * S[3 + c] + F[r * 3 + 2] * S[6 + c];
+            FS[r * 3 + c] = F[r * 3 + 0] * S[c] + F[r * 3 + 1] * S[3 + c] + F[r * 3 + 2] * S[6 + c];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) P[i] += FS[i];
       }
 #pragma unroll
       for (int f = 0; f < 4; ++f) {
@@ -185,12 +194,13 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
 #pragma unroll
         for (int r = 0; r < 3; ++r) {
           if ((pf >> r) & 1) continue;
+          const int64_t idx = 3 * (int64_t)rows[f] + r;
           double v = (P[r * 3 + 0] * dN[3 * f + 0] + P[r * 3 + 1] * dN[3 * f + 1] +
                       P[r * 3 + 2] * dN[3 * f + 2]) * w;
           v -= (double)rho * a.grav[r] * w * 0.25;
-          v += a.dtfi2 * m * (acc[f][r] + asum[r]);
-          v += a.mdamp * m * (dmp[f][r] + dsum[r]);
-          atomicAdd(a.g + 3 * (int64_t)rows[f] + r, v);
+          v += a.dtfi2 * m * ((uf[f][r] - a.ut[idx]) + asum[r]);
+          if (a.mdamp > 0.0) v += a.mdamp * m * ((uf[f][r] - a.u0[idx]) + dsum[r]);
+          atomicAdd(a.g + idx, v);
         }
       }
     }
@@ -200,18 +210,8 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
       for (int f = 0; f < 4; ++f)
 #pragma unroll
         for (int r = 0; r < 3; ++r) xc[r] += 0.25 * (a.X[3 * (int64_t)rows[f] + r] + uf[f][r]);
-      double ein = 0.0, edm = 0.0;
-#pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        double sq = 0.0, sd = 0.0;
-#pragma unroll
-        for (int f = 0; f < 4; ++f) {
-          sq += acc[f][r] * acc[f][r];
-          sd += dmp[f][r] * dmp[f][r];
-        }
-        ein += m * (sq + asum[r] * asum[r]);
-        edm += m * (sd + dsum[r] * dsum[r]);
-      }
+      ein = m * (ein + asum[0] * asum[0] + asum[1] * asum[1] + asum[2] * asum[2]);
+      edm = m * (edm + dsum[0] * dsum[0] + dsum[1] * dsum[1] + dsum[2] * dsum[2]);
       double psi;
       if (mat == 1)
         stvk_energy_pk1_f64((double)mu, (double)lam, F, &psi, nullptr);
@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
         arap_energy_pk1_f64((double)mu, F, &psi, nullptr);
       else
         psi = snh_energy_f64(kc, F);
-      if (a.kdamp > 0.0) psi += 0.5 * (Sv[0] * dE[0] + Sv[1] * dE[1] + Sv[2] * dE[2] + Sv[3] * dE[3] +
+      if (kDamp && a.kdamp > 0.0) psi += 0.5 * (Sv[0] * dE[0] + Sv[1] * dE[1] + Sv[2] * dE[2] + Sv[3] * dE[3] +
                                        Sv[4] * dE[4] + Sv[5] * dE[5]);
       const double e = psi * w -
                        (double)rho * w * (a.grav[0] * xc[0] + a.grav[1] * xc[1] + a.grav[2] * xc[2]) +
@@ -234,15 +234,15 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
     float Ff[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i) Ff[i] = (float)F[i];
-    float C[81];
+    TanForm T;
     if (mat == 1)
-      stvk_tangent_f32(mu, lam, Ff, (a.flags & 8) != 0, a.psd, a.min_eig, C);
+      stvk_tanform(mu, lam, Ff, (a.flags & 8) != 0, a.psd, a.min_eig, T);
     else if (mat == 2)
-      linear_tangent_f32(mu, lam, C);
+      linear_tanform(mu, lam, T);
     else if (kArap && mat == 5)
-      arap_tangent_f32(mu, Ff, (a.flags & 8) != 0, a.psd, a.min_eig, C);
+      arap_tanform(mu, Ff, (a.flags & 8) != 0, a.psd, a.min_eig, T);
     else
-      snh_tangent_f32(mu, lam, Ff, (a.flags & 8) != 0, a.psd, a.min_eig, C);
+      snh_tanform(mu, lam, Ff, (a.flags & 8) != 0, a.psd, a.min_eig, T);
     const int4 S0 = a.slots0[t], S1 = a.slots1[t], S2 = a.slots2[t], S3 = a.slots3[t];
     const int slot[16] = {S0.x, S0.y, S0.z, S0.w, S1.x, S1.y, S1.z, S1.w,
                           S2.x, S2.y, S2.z, S2.w, S3.x, S3.y, S3.z, S3.w};
@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
 #pragma unroll
     for (int f = 0; f < 4; ++f) pins[f] = a.pin[rows[f]];
     // stiffness damping: Gauss-Newton part kappa B^T C0 B and the (projected) geometric part
-    const bool kd = a.kdamp > 0.0;
+    const bool kd = kDamp && a.kdamp > 0.0;
     float aF[4][3], FFt[9], Sg[9];
     const bool arap_h = kArap && mat == 5;
     const float kl = arap_h ? 0.0f : (float)(a.kdamp * (double)lam);
@@ -273,41 +273,52 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
       Sg[1] = Sg[3] = s6[5];
       if (a.kdamp_geo && (a.flags & 8)) project_sym3_f32(Sg);
     }
-#pragma unroll
+    // Blocks K_fg = vol B_f^T C B_g (fem_stress.h:218-241) from the factored tangent, for f <= g; K_gf is the
+    // transpose (C and the damping terms are symmetric). Pinned rows and columns stay zero. A block is
+    // scattered whole: entries 0-3 and 4-7 are 16-byte aligned runs in the sliced-ELL value layout, so it
+    // takes two float4 reductions and one scalar one.
+    auto scatter = [&](int p, const float kb[9]) {
+      atomicAdd(reinterpret_cast<float4*>(a.val + val_index(p, 0)), make_float4(kb[0], kb[1], kb[2], kb[3]));
+      atomicAdd(reinterpret_cast<float4*>(a.val + val_index(p, 4)), make_float4(kb[4], kb[5], kb[6], kb[7]));
+      atomicAdd(a.val + val_index(p, 8), kb[8]);
+    };
+#pragma unroll 1
     for (int f = 0; f < 4; ++f) {
+#pragma unroll 1
+      for (int g = f; g < 4; ++g) {
+        const float df[3] = {dN[3 * f], dN[3 * f + 1], dN[3 * f + 2]};
+        const float dg[3] = {dN[3 * g], dN[3 * g + 1], dN[3 * g + 2]};
+        float kb[9];
+        tan_block(T, df, dg, kb);
 #pragma unroll
-      for (int r = 0; r < 3; ++r) {
-        if ((pins[f] >> r) & 1) continue;
-        // Cf_r[c][l] = sum_j dN_f[j] C[(3r+j)][(3c+l)]  (fem_stress.h:218-241)
-        float Cf[9];
-#pragma unroll
-        for (int cl = 0; cl < 9; ++cl)
-          Cf[cl] = dN[3 * f + 0] * C[(3 * r + 0) * 9 + cl] + dN[3 * f + 1] * C[(3 * r + 1) * 9 + cl] +
-                   dN[3 * f + 2] * C[(3 * r + 2) * 9 + cl];
-#pragma unroll
-        for (int g = 0; g < 4; ++g) {
-          const int p = slot[f * 4 + g];
+        for (int r = 0; r < 3; ++r)
 #pragma unroll
           for (int c = 0; c < 3; ++c) {
-            if ((pins[g] >> c) & 1) continue;
-            float k = vol * (Cf[c * 3 + 0] * dN[3 * g + 0] + Cf[c * 3 + 1] * dN[3 * g + 1] +
-                             Cf[c * 3 + 2] * dN[3 * g + 2]);
+            float k = vol * kb[3 * r + c];
             if (kd) {
-              const float dd = dN[3 * f] * dN[3 * g] + dN[3 * f + 1] * dN[3 * g + 1] + dN[3 * f + 2] * dN[3 * g + 2];
+              const float dd = df[0] * dg[0] + df[1] * dg[1] + df[2] * dg[2];
               float v = kl * aF[f][r] * aF[g][c] + km * (FFt[r * 3 + c] * dd + aF[g][r] * aF[f][c]);
               if (a.kdamp_geo && r == c) {
                 float geo = 0.0f;
 #pragma unroll
                 for (int kk = 0; kk < 3; ++kk)
-                  geo += dN[3 * f + kk] * (Sg[kk * 3 + 0] * dN[3 * g + 0] + Sg[kk * 3 + 1] * dN[3 * g + 1] +
-                                           Sg[kk * 3 + 2] * dN[3 * g + 2]);
+                  geo += df[kk] * (Sg[kk * 3 + 0] * dg[0] + Sg[kk * 3 + 1] * dg[1] + Sg[kk * 3 + 2] * dg[2]);
                 v += geo;
               }
               k += vol * v;
             }
-            atomicAdd(a.val + val_index(p, 3 * r + c), k);
+            kb[3 * r + c] = k;
           }
-        }
+        float kt[9];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            kt[3 * c + r] = (((pins[g] >> c) & 1) || ((pins[f] >> r) & 1)) ? 0.0f : kb[3 * r + c];
+            if (((pins[f] >> r) & 1) || ((pins[g] >> c) & 1)) kb[3 * r + c] = 0.0f;
+          }
+        scatter(slot[f * 4 + g], kb);
+        if (g != f) scatter(slot[g * 4 + f], kt);
       }
     }
   }
@@ -316,10 +327,16 @@ __global__ void __launch_bounds__(128) k_element(ElemArgs a) {
 void launch_element(const ElemArgs& a, cudaStream_t st) {
   if (a.n_tets == 0) return;
   const int th = 128;
-  if (a.has_arap)
-    k_element<true><<<(unsigned)((a.n_tets + th - 1) / th), th, 0, st>>>(a);
+  const unsigned nb = (unsigned)((a.n_tets + th - 1) / th);
+  const bool damp = a.kdamp > 0.0;
+  if (a.has_arap && damp)
+    k_element<true, true><<<nb, th, 0, st>>>(a);
+  else if (a.has_arap)
+    k_element<true, false><<<nb, th, 0, st>>>(a);
+  else if (damp)
+    k_element<false, true><<<nb, th, 0, st>>>(a);
   else
-    k_element<false><<<(unsigned)((a.n_tets + th - 1) / th), th, 0, st>>>(a);
+    k_element<false, false><<<nb, th, 0, st>>>(a);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -963,6 +980,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
   constexpr int kB64 = kPipe ? 4 : 2;  // groups per batch of the FP64 SpMVs (register budget of the variant)
   __shared__ double tot[kPcgMaxEnvsPerCta][kPcgNq];
   __shared__ int s_exit, s_replace;
+  __shared__ float s_tr[(kPipe ? 16 : 32) * 3 * kSlice];  // per warp: a slice's row products, DoF order
   const int c = blockIdx.x;
   const unsigned ncta = gridDim.x;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
@@ -1344,21 +1362,26 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
   mark(-1);
   for (int it = a.resume ? a.it0 : 1;; ++it) {
     // ---- phase 1 ----
+    // The row product runs one row per lane; the vector updates run DoF-linear: DoF dl = lane + 32 j
+    // (j = 0, 1, 2) of the slice, i.e. row 32 s + dl / 3, component dl % 3, so every load and store of p
+    // and q is one contiguous 128-byte line per warp. The row products reach the DoF layout through the
+    // warp's 96-float staging row in shared memory; z (just gathered by the product) comes from L1.
     clear_acc();
+    float* tr = s_tr + warp * (3 * kSlice);
+    const float* zf = reinterpret_cast<const float*>(a.z);
     for (int i = s0 + warp; i < s1; i += nwarps) {
       const int s = slice_of(i);
       const int le = local_env(a.A.slice_env[s]);
       if (st[le].status != 0) continue;
-      const int64_t row = (int64_t)s * kSlice + lane;
-      // own-row operands are loaded before the row product so that their latency overlaps it
+      const int64_t d0 = (int64_t)s * (3 * kSlice);
+      // own DoF operands are loaded before the row product so that their latency overlaps it
       const bool first = st[le].first != 0;
-      const float4 zr = a.z[row];
       float po[3] = {0.0f, 0.0f, 0.0f}, qo[3] = {0.0f, 0.0f, 0.0f};
       if (!first) {
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          po[k] = a.p[3 * row + k];
-          qo[k] = a.q[3 * row + k];
+        for (int j = 0; j < 3; ++j) {
+          po[j] = a.p[d0 + lane + 32 * j];
+          qo[j] = a.q[d0 + lane + 32 * j];
         }
       }
       float a0, a1, a2;
@@ -1369,20 +1392,24 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
         sell_row_product_pipe(a.A, s, lane, [&](int j) { return a.z[j]; }, a0, a1, a2);
       else
         sell_row_product(a.A, s, lane, [&](int j) { return a.z[j]; }, a0, a1, a2);
+      tr[3 * lane] = a0;
+      tr[3 * lane + 1] = a1;
+      tr[3 * lane + 2] = a2;
+      __syncwarp();
       const float beta = first ? 0.0f : (float)st[le].beta;
-      float pn[3], qn[3];
-      pn[0] = fmaf(beta, po[0], zr.x);
-      pn[1] = fmaf(beta, po[1], zr.y);
-      pn[2] = fmaf(beta, po[2], zr.z);
-      qn[0] = fmaf(beta, qo[0], a0);
-      qn[1] = fmaf(beta, qo[1], a1);
-      qn[2] = fmaf(beta, qo[2], a2);
+      double pq = 0.0;
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        a.p[3 * row + k] = pn[k];
-        a.q[3 * row + k] = qn[k];
+      for (int j = 0; j < 3; ++j) {
+        const int dl = lane + 32 * j;
+        const float zv = zf[4 * ((int64_t)s * kSlice + dl / 3) + dl % 3];
+        const float pn = fmaf(beta, po[j], zv);
+        const float qn = fmaf(beta, qo[j], tr[dl]);
+        a.p[d0 + dl] = pn;
+        a.q[d0 + dl] = qn;
+        pq += (double)pn * qn;
       }
-      acc_add(le, 0, (double)pn[0] * qn[0] + (double)pn[1] * qn[1] + (double)pn[2] * qn[2]);
+      __syncwarp();
+      acc_add(le, 0, pq);
     }
     acc_end(1);
     flush_acc(1, 1);
@@ -1415,22 +1442,65 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
 
     // ---- phase 2 ----
     clear_acc();
+    if (a.precond != 2) {
+      // none / Jacobi: element-wise, DoF-linear (contiguous 256-byte lines of x and r per warp instruction)
+      float* zw = reinterpret_cast<float*>(a.z);
+      for (int i = s0 + warp; i < s1; i += nwarps) {
+        const int s = slice_of(i);
+        const int le = local_env(a.A.slice_env[s]);
+        if (st[le].status != 0) continue;
+        const int64_t d0 = (int64_t)s * (3 * kSlice);
+        // every operand load is issued before the first store (the update is latency bound)
+        double xo[3], ro[3];
+        float pp[3], qq[3], dd[3], zo[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const int dl = lane + 32 * j;
+          xo[j] = a.x[d0 + dl];
+          pp[j] = a.p[d0 + dl];
+          ro[j] = a.r[d0 + dl];
+          qq[j] = a.q[d0 + dl];
+          dd[j] = (!replace && a.precond == 1) ? a.dinv[d0 + dl] : 1.0f;
+          zo[j] = replace ? 0.0f : zw[4 * ((int64_t)s * kSlice + dl / 3) + dl % 3];
+        }
+        const double al = st[le].alpha;
+        double r[3];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          a.x[d0 + lane + 32 * j] = xo[j] + al * (double)pp[j];
+          r[j] = ro[j] - al * (double)qq[j];
+        }
+        if (replace) continue;
+        double rr = 0.0, rzo = 0.0, rz = 0.0;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const int dl = lane + 32 * j;
+          const float z = (float)(dd[j] * r[j]);
+          a.r[d0 + dl] = r[j];
+          zw[4 * ((int64_t)s * kSlice + dl / 3) + dl % 3] = z;
+          rr += r[j] * r[j];
+          rzo += r[j] * zo[j];
+          rz += r[j] * z;
+        }
+        acc_add(le, 0, rr);
+        acc_add(le, 1, rzo);
+        acc_add(le, 2, rz);
+      }
+    } else {
     for (int i = s0 + warp; i < s1; i += nwarps) {
       const int s = slice_of(i);
       const int le = local_env(a.A.slice_env[s]);
       if (st[le].status != 0) continue;
       const int64_t row = (int64_t)s * kSlice + lane;
-      // every operand load is issued before the first store (the row update is latency bound, operands
-      // in L2)
+      // block Jacobi: the row's 3x3 inverse diagonal block, one row per lane
       double xo[3], ro[3];
-      float pp[3], qq[3], dd[3];
+      float pp[3], qq[3];
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         xo[k] = a.x[3 * row + k];
         pp[k] = a.p[3 * row + k];
         ro[k] = a.r[3 * row + k];
         qq[k] = a.q[3 * row + k];
-        dd[k] = (!replace && a.precond == 1) ? a.dinv[3 * row + k] : 1.0f;
       }
       const float4 zo = replace ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : a.z[row];
       const double al = st[le].alpha;
@@ -1442,18 +1512,14 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
       }
       if (replace) continue;
       float z[3];
-      if (a.precond == 1) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) z[k] = (float)(dd[k] * r[k]);
-      } else {
-        prec_apply(a, row, r, z);
-      }
+      prec_apply(a, row, r, z);
 #pragma unroll
       for (int k = 0; k < 3; ++k) a.r[3 * row + k] = r[k];
       a.z[row] = make_float4(z[0], z[1], z[2], 0.0f);
       acc_add(le, 0, r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
       acc_add(le, 1, r[0] * zo.x + r[1] * zo.y + r[2] * zo.z);
       acc_add(le, 2, r[0] * z[0] + r[1] * z[1] + r[2] * z[2]);
+    }
     }
     acc_end(3);
     if (replace) {
@@ -1626,7 +1692,11 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
   __shared__ double s_gather[16][kClNq];  // every CTA's partials, gathered by one pass of remote loads
   __shared__ unsigned s_cnt;           // the cluster barrier counter (used in CTA 0)
   __shared__ int s_env, s_env_here, s_ok;
+  __shared__ float s_tr[16 * 3 * kSlice];  // per warp: a slice's row products, DoF order
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  float* const tr = s_tr + warp * (3 * kSlice);
+  const float* const zf = reinterpret_cast<const float*>(a.z);
+  float* const zw = reinterpret_cast<float*>(a.z);
   const uint32_t rank = cluster_rank(), csize = cluster_size();
   if (threadIdx.x == 0) s_cnt = 0u;
   cluster_hw_sync();  // every CTA's shared memory is live before any remote access
@@ -1849,35 +1919,38 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
 
     // ---- iterations ----
     for (int it = 1; status == 0; ++it) {
-      // phase 1: p = z + beta p, q = A z + beta q, p.q
+      // phase 1: p = z + beta p, q = A z + beta q, p.q (vector updates DoF-linear, as in k_pcg)
       acc_reset();
       for (int s = c0 + warp; s < c1; s += nwarps) {
-        const int64_t row = (int64_t)s * kSlice + lane;
-        const float4 zr = a.z[row];
+        const int64_t d0 = (int64_t)s * (3 * kSlice);
         float po[3] = {0.0f, 0.0f, 0.0f}, qo[3] = {0.0f, 0.0f, 0.0f};
         if (!first) {
 #pragma unroll
-          for (int k = 0; k < 3; ++k) {
-            po[k] = a.p[3 * row + k];
-            qo[k] = a.q[3 * row + k];
+          for (int j = 0; j < 3; ++j) {
+            po[j] = a.p[d0 + lane + 32 * j];
+            qo[j] = a.q[d0 + lane + 32 * j];
           }
         }
         float a0, a1, a2;
         sell_row_product_pipe(a.A, s, lane, [&](int j) { return a.z[j]; }, a0, a1, a2);
+        tr[3 * lane] = a0;
+        tr[3 * lane + 1] = a1;
+        tr[3 * lane + 2] = a2;
+        __syncwarp();
         const float fb = first ? 0.0f : (float)beta;
-        float pn[3], qn[3];
-        pn[0] = fmaf(fb, po[0], zr.x);
-        pn[1] = fmaf(fb, po[1], zr.y);
-        pn[2] = fmaf(fb, po[2], zr.z);
-        qn[0] = fmaf(fb, qo[0], a0);
-        qn[1] = fmaf(fb, qo[1], a1);
-        qn[2] = fmaf(fb, qo[2], a2);
+        double pq = 0.0;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          a.p[3 * row + k] = pn[k];
-          a.q[3 * row + k] = qn[k];
+        for (int j = 0; j < 3; ++j) {
+          const int dl = lane + 32 * j;
+          const float zv = zf[4 * ((int64_t)s * kSlice + dl / 3) + dl % 3];
+          const float pn = fmaf(fb, po[j], zv);
+          const float qn = fmaf(fb, qo[j], tr[dl]);
+          a.p[d0 + dl] = pn;
+          a.q[d0 + dl] = qn;
+          pq += (double)pn * qn;
         }
-        acc_add(0, (double)pn[0] * qn[0] + (double)pn[1] * qn[1] + (double)pn[2] * qn[2]);
+        __syncwarp();
+        acc_add(0, pq);
       }
       if (!reduce(1)) {
         fail = true;
@@ -1891,41 +1964,74 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
         break;
       }
       const bool replace = (verify_it > 0 && verify_it == it - 1) || (a.replace_every > 0 && it % a.replace_every == 0);
-      // phase 2: x += alpha p, r -= alpha q, z = M^-1 r, r.r, r.z_old, r.z
+      // phase 2: x += alpha p, r -= alpha q, z = M^-1 r, r.r, r.z_old, r.z (DoF-linear unless block Jacobi)
       acc_reset();
-      for (int s = c0 + warp; s < c1; s += nwarps) {
-        const int64_t row = (int64_t)s * kSlice + lane;
-        double xo[3], ro[3];
-        float pp[3], qq[3], dd[3];
+      if (a.precond != 2) {
+        for (int s = c0 + warp; s < c1; s += nwarps) {
+          const int64_t d0 = (int64_t)s * (3 * kSlice);
+          double xo[3], ro[3];
+          float pp[3], qq[3], dd[3], zo[3];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          xo[k] = a.x[3 * row + k];
-          pp[k] = a.p[3 * row + k];
-          ro[k] = a.r[3 * row + k];
-          qq[k] = a.q[3 * row + k];
-          dd[k] = (!replace && a.precond == 1) ? a.dinv[3 * row + k] : 1.0f;
+          for (int j = 0; j < 3; ++j) {
+            const int dl = lane + 32 * j;
+            xo[j] = a.x[d0 + dl];
+            pp[j] = a.p[d0 + dl];
+            ro[j] = a.r[d0 + dl];
+            qq[j] = a.q[d0 + dl];
+            dd[j] = (!replace && a.precond == 1) ? a.dinv[d0 + dl] : 1.0f;
+            zo[j] = replace ? 0.0f : zw[4 * ((int64_t)s * kSlice + dl / 3) + dl % 3];
+          }
+          double r[3];
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            a.x[d0 + lane + 32 * j] = xo[j] + al * (double)pp[j];
+            r[j] = ro[j] - al * (double)qq[j];
+          }
+          if (replace) continue;
+          double rr2 = 0.0, rzo2 = 0.0, rz2 = 0.0;
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            const int dl = lane + 32 * j;
+            const float z = (float)(dd[j] * r[j]);
+            a.r[d0 + dl] = r[j];
+            zw[4 * ((int64_t)s * kSlice + dl / 3) + dl % 3] = z;
+            rr2 += r[j] * r[j];
+            rzo2 += r[j] * zo[j];
+            rz2 += r[j] * z;
+          }
+          acc_add(0, rr2);
+          acc_add(1, rzo2);
+          acc_add(2, rz2);
         }
-        const float4 zo = replace ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : a.z[row];
-        double r[3];
+      } else {
+        for (int s = c0 + warp; s < c1; s += nwarps) {
+          const int64_t row = (int64_t)s * kSlice + lane;
+          double xo[3], ro[3];
+          float pp[3], qq[3];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          a.x[3 * row + k] = xo[k] + al * (double)pp[k];
-          r[k] = ro[k] - al * (double)qq[k];
-        }
-        if (replace) continue;
-        float z[3];
-        if (a.precond == 1) {
+          for (int k = 0; k < 3; ++k) {
+            xo[k] = a.x[3 * row + k];
+            pp[k] = a.p[3 * row + k];
+            ro[k] = a.r[3 * row + k];
+            qq[k] = a.q[3 * row + k];
+          }
+          const float4 zo = replace ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : a.z[row];
+          double r[3];
 #pragma unroll
-          for (int k = 0; k < 3; ++k) z[k] = (float)(dd[k] * r[k]);
-        } else {
+          for (int k = 0; k < 3; ++k) {
+            a.x[3 * row + k] = xo[k] + al * (double)pp[k];
+            r[k] = ro[k] - al * (double)qq[k];
+          }
+          if (replace) continue;
+          float z[3];
           prec_apply(a, row, r, z);
-        }
 #pragma unroll
-        for (int k = 0; k < 3; ++k) a.r[3 * row + k] = r[k];
-        a.z[row] = make_float4(z[0], z[1], z[2], 0.0f);
-        acc_add(0, r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-        acc_add(1, r[0] * zo.x + r[1] * zo.y + r[2] * zo.z);
-        acc_add(2, r[0] * z[0] + r[1] * z[1] + r[2] * z[2]);
+          for (int k = 0; k < 3; ++k) a.r[3 * row + k] = r[k];
+          a.z[row] = make_float4(z[0], z[1], z[2], 0.0f);
+          acc_add(0, r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+          acc_add(1, r[0] * zo.x + r[1] * zo.y + r[2] * zo.z);
+          acc_add(2, r[0] * z[0] + r[1] * z[1] + r[2] * z[2]);
+        }
       }
       if (replace) {
         // true residual in FP64 (needs the neighbours' x updates)
