@@ -566,7 +566,7 @@ def run_ours(args, rank, world, local_rank):
                    "profile_ms": {k: v for k, v in prof.items() if k.endswith("_ms")}},
     }
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_oracle_run(args, seed0, steps=1, warmup=0, tet_budget=args.cpu_tets)
+        line["cpu_baseline"] = cpu_oracle_run(args, seed0, steps=3, warmup=0, tet_budget=args.cpu_tets)
     w.close()
     return line
 
@@ -594,7 +594,7 @@ def main():
                     help="cfg3: held-out episodes each arm is timed on")
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--newton-max-iter", type=int, default=0, dest="newton_max_iter")
-    ap.add_argument("--cpu-tets", type=int, default=400000, dest="cpu_tets",
+    ap.add_argument("--cpu-tets", type=int, default=1000000, dest="cpu_tets",
                     help="tets of the envs the CPU baseline steps per step (a bounded sample)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity", action="store_true")

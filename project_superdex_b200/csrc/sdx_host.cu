@@ -2255,6 +2255,18 @@ static int autotune_pcg(sdx_context* c, const sdx_linear_params& lp) {
   return SDX_OK;
 }
 
+// Zero the active-pair counters of the envs in the current device mask, before an assembly that recounts
+// them; the other envs keep the count of their own last assembly (sdx_env_stats.n_contacts).
+__global__ void k_zero_env_pairs(int n_envs, const uint8_t* __restrict__ env_mask, unsigned long long* pairs) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n_envs && (!env_mask || env_mask[e])) pairs[e] = 0ull;
+}
+
+static void zero_env_pairs(sdx_context* c) {
+  k_zero_env_pairs<<<(c->n_envs + 255) / 256, 256, 0, c->stream>>>(c->n_envs, c->env_mask, c->env_pairs);
+  c->launches++;
+}
+
 static int step_once(sdx_context* c) {
   const sdx_step_params& p = c->params;
   const int E = c->n_envs;
@@ -2316,7 +2328,10 @@ static int step_once(sdx_context* c) {
     }
     if (n_active == 0) break;
     SDX_TRY(upload_mask(c, mask));
-    if (!first_pass) assemble_dev(c, c->u, c->ut, t_end, SDX_ASM_HESS | SDX_ASM_PSD, c->env_mask, false);
+    if (!first_pass) {
+      zero_env_pairs(c);
+      assemble_dev(c, c->u, c->ut, t_end, SDX_ASM_HESS | SDX_ASM_PSD, c->env_mask, false);
+    }
     // the launch-shape autotuner (opt-in) runs on the first solve, before any start vector is written
     if (!c->pcg_tuned && !c->ext_fn) SDX_TRY(autotune_pcg(c, p.linear));
     // linear solve H dx = g, warm started from zero, the previous dx, or the learned prediction
@@ -2344,8 +2359,10 @@ static int step_once(sdx_context* c) {
       c->launches += 3;
     }
     if (learned) {
-      if (launch_mlp_forward(mlp_forward_args(c->mlp, c->feat_X, (int)c->n_rows, c->feat_Y, nullptr, c->mlp_error),
-                             c->num_sms, c->stream) != 0)
+      MlpForwardArgs fa = mlp_forward_args(c->mlp, c->feat_X, (int)c->n_rows, c->feat_Y, nullptr, c->mlp_error);
+      fa.slice_env = c->slice_env;  // only the tiles of envs in this solve
+      fa.env_mask = c->env_mask;
+      if (launch_mlp_forward(fa, c->num_sms, c->stream) != 0)
         return set_error(SDX_ERR_CUDA, "MLP forward launch failed");
       launch_warm_start(c->n_rows, c->slice_env, c->env_mask, c->feat_Y, c->pin, c->diag_pos, c->dx_prev2,
                         c->env_hnorm, c->env_rows, c->dx, c->uscratch, c->stream);
@@ -2404,7 +2421,7 @@ static int step_once(sdx_context* c) {
       SDX_CUDA(cudaMemcpyAsync(c->env_scale, scale.data(), sizeof(double) * E, cudaMemcpyHostToDevice, c->stream));
       launch_ls_candidate(c->n_slices, c->slice_env, c->env_mask, c->ubase, c->dx, c->env_scale, c->u, c->stream);
       c->launches++;
-      SDX_CUDA(cudaMemsetAsync(c->env_pairs, 0, sizeof(unsigned long long) * E, c->stream));
+      zero_env_pairs(c);  // only the envs this assembly recounts keep their last assembly's pairs otherwise
       assemble_dev(c, c->u, c->ut, t_end, SDX_ASM_RES, c->env_mask, false);
       SDX_TRY(env_dot_host(c, c->g, c->g, c->env_mask, nrm));
       int left = 0;

@@ -158,7 +158,17 @@ __global__ void __launch_bounds__(kMlpThreads, 1) k_mlp_forward(MlpForwardArgs a
   bool ok = true;
 
   const int n_tiles = (a.n + kTile - 1) / kTile;
+  const int n_slices = (a.n + 31) / 32;
   for (int tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+    if (a.env_mask) {  // the same answer in every thread of the CTA
+      bool any = false;
+#pragma unroll
+      for (int q = 0; q < kTile / 32; ++q) {
+        const int sl = tile * (kTile / 32) + q;
+        any |= sl < n_slices && a.env_mask[a.slice_env[sl]] != 0;
+      }
+      if (!any) continue;
+    }
     const int row = tile * kTile + lrow;  // this thread's vertex (TMEM lane lrow)
     // input tile: 16 features -> bf16 (first column half)
     if (half == 0) {
@@ -393,6 +403,8 @@ MlpForwardArgs mlp_forward_args(const MlpParams& P, const float* X, int n, float
   a.b2 = P.p + kOffB2;
   a.b3 = P.p + kOffB3;
   a.b4 = P.p + kOffB4;
+  a.slice_env = nullptr;
+  a.env_mask = nullptr;
   return a;
 }
 
@@ -450,12 +462,14 @@ void mlp_adam(const MlpParams& P, float lr, int step, cudaStream_t st) {
 
 // raw per-row quantities: u, dt v, the last Newton update dx1, the previous step's update at the same
 // Newton iteration dx2 (zero when there is none), D^-1 g (Jacobi-preconditioned Newton gradient)
-__global__ void k_feature_raw(int64_t n_rows, const double* __restrict__ u, const double* __restrict__ v, double dt,
+__global__ void k_feature_raw(int64_t n_rows, const int* __restrict__ slice_env, const uint8_t* __restrict__ env_mask,
+                              const double* __restrict__ u, const double* __restrict__ v, double dt,
                               const double* __restrict__ dx1, const double* __restrict__ dx2,
                               const double* __restrict__ g, const float* __restrict__ val,
                               const int* __restrict__ diag_pos, const uint8_t* __restrict__ pin, float* raw) {
   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n_rows) return;
+  if (env_mask && !env_mask[slice_env[r >> 5]]) return;  // envs outside this solve: nothing to predict
   const int dp = diag_pos[r];
   float o[16];
 #pragma unroll
@@ -519,6 +533,12 @@ __global__ void k_feature_ring(Matrix A, const uint8_t* __restrict__ env_mask, c
   if (s >= A.n_slices) return;
   const int e = A.slice_env[s];
   const int64_t row = (int64_t)s * 32 + lane;
+  if (env_mask && !env_mask[e]) {  // outside this solve: zero inputs, no neighbour gathers
+    float4* xo = reinterpret_cast<float4*>(X + 16 * row);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) xo[q] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    return;
+  }
   float acc[15];
 #pragma unroll
   for (int i = 0; i < 15; ++i) acc[i] = 0.0f;
@@ -577,8 +597,8 @@ void launch_features(const Matrix& A, int64_t n_rows, const uint8_t* env_mask, c
                      const uint8_t* pin, const int* env_rows, float* raw, double* sumsq, int n_envs, float* X,
                      cudaStream_t st) {
   if (n_rows == 0) return;
-  k_feature_raw<<<(unsigned)((n_rows + 255) / 256), 256, 0, st>>>(n_rows, u, v, dt, dx1, dx2, g, A.val, diag_pos,
-                                                                   pin, raw);
+  k_feature_raw<<<(unsigned)((n_rows + 255) / 256), 256, 0, st>>>(n_rows, A.slice_env, env_mask, u, v, dt, dx1, dx2, g,
+                                                                   A.val, diag_pos, pin, raw);
   cudaMemsetAsync(sumsq, 0, sizeof(double) * 5 * n_envs, st);
   const int64_t t = (int64_t)A.n_slices * 32;
   {

@@ -46,6 +46,10 @@ struct MlpForwardArgs {
   int* error;
   const __nv_bfloat16 *W1, *W2, *W3, *W4;
   const float *b1, *b2, *b3, *b4;
+  // optional (NULL: every tile): 128-row tiles whose four 32-row slices all belong to envs outside the
+  // mask are skipped (their Y rows are left as they are)
+  const int* slice_env;
+  const uint8_t* env_mask;
 };
 
 int launch_mlp_forward(const MlpForwardArgs& a, int num_sms, cudaStream_t st);

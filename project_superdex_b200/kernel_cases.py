@@ -11,7 +11,8 @@
 The workload is the single-body 64^3-cell grid (274,625 nodes, 1,572,864 tets, 5 capsules) unless
 `--cells` says otherwise; `--workload batch` takes the 1,024 uneven bodies (cells per axis U{8..40},
 16.2 M nodes, 86 M tets) instead, whose device footprint (~25 GB) is too large for multi-pass profiler
-captures: use its CUDA-event timing (`us_per_iter`). One JSON line reports the sizes and the algorithmic bytes of one launch (or one
+captures: use its CUDA-event timing (`us_per_iter`), or `--envs N` for the first N bodies of the batch
+(128: about 3 GB). One JSON line reports the sizes and the algorithmic bytes of one launch (or one
 CG iteration), so that DRAM counters from a capture divide into per-unit traffic. Only the measured
 launches run between cudaProfilerStart and cudaProfilerStop (capture with `ncu --profile-from-start off`).
 """
@@ -47,11 +48,12 @@ def main(argv=None):
     ap.add_argument("--iters", type=int, default=100)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--envs", type=int, default=1024, help="batch workload: the first N bodies of the batch")
     ap.add_argument("--cta-profile", default=None,
                     help="pcg: also time each CTA's phases over two launches and save them to this .npy")
     args = ap.parse_args(argv)
     if args.workload == "batch":
-        bodies, cfg = scenes.config2(args.seed)
+        bodies, cfg = scenes.config2(args.seed, n_envs=args.envs)
     else:
         bodies, cfg = scenes.config1(args.seed, n=args.cells)
     w = SoftBodyWorld(bodies, cfg, newton_abs_tol=1e-9, newton_max_iter=12)

