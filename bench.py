@@ -310,6 +310,8 @@ def time_headline(w, args, stream, local_rank):
     conv_steps = 0
     newton = cg_env = 0
     torch.cuda.synchronize()
+    # the timed steps are the only region a profiler started with --profile-from-start off records
+    torch.cuda.profiler.start()
     with ClockSampler(local_rank) as clk:
         for k in range(K):
             ev_a[k].record(stream)
@@ -324,6 +326,7 @@ def time_headline(w, args, stream, local_rank):
             cg_env += sum(s["cg_iters"] for s in st)
         ev_end.record(stream)
         ev_end.synchronize()
+    torch.cuda.profiler.stop()
     step_ms = [ev_b[k].elapsed_time(ev_c[k]) for k in range(K)]
     e2e_ms = ev_a[0].elapsed_time(ev_end)
     prof = w.profile()

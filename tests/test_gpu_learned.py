@@ -89,7 +89,10 @@ def test_learned_start_gains_over_the_plain_start():
     """What the trained network gains: CG iterations of 8 steps of a body pressed by a capsule, from the
     zero start (the reference's behaviour), the temporal start (previous step's update at the same Newton
     iteration) and the learned start (Galerkin step on the temporal guess and the network's correction,
-    trained on another seed of the same scene)."""
+    trained on another seed of the same scene, so the evaluated seed is held out). The learned start needs
+    strictly fewer CG iterations than the temporal one; the gain is small (about 1 %, measured 4,936 vs
+    4,993), and in wall-clock time the start's own kernels cost more than it saves (the benchmark's
+    learned_over_temporal)."""
     from project_superdex_b200.learned import Mlp, collect
     from project_superdex_b200.soft_body import SoftBodyWorld
 
@@ -123,5 +126,4 @@ def test_learned_start_gains_over_the_plain_start():
         cg[ws] = total
     zero, temporal, learned = cg[capi.SDX_WARM_ZERO], cg[capi.SDX_WARM_TEMPORAL], cg[capi.SDX_WARM_LEARNED]
     print("CG iterations over 8 steps: zero %d, temporal %d, learned %d" % (zero, temporal, learned))
-    assert learned < zero
-    assert learned <= 1.05 * temporal
+    assert learned < temporal < zero
