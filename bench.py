@@ -427,7 +427,8 @@ def merge(a, b):
     out["step_ms"] = a["step_ms"] + b["step_ms"]
     for k in ("newton_per_env_step", "cg_per_env_step"):
         out[k] = (a[k] * a["env_steps"] + b[k] * b["env_steps"]) / out["env_steps"]
-    out["prof"] = {k: (a["prof"].get(k, 0) + v if k != "pcg_threads" else v) for k, v in b["prof"].items()}
+    out["prof"] = {k: (a["prof"].get(k, 0) + v if k not in ("pcg_threads", "pcg_cluster_size") else v)
+                   for k, v in b["prof"].items()}
     if "clocks" in a:
         ca, cb = a["clocks"], b["clocks"]
         sm = [x for x in (ca.get("sm_mhz"), cb.get("sm_mhz")) if x is not None]
@@ -554,7 +555,8 @@ def run_ours(args, rank, world, local_rank):
         "config": config,
         "run": {"arms": arms, "headline_arm": head_arm, "compare_steps": n_cmp, "episodes": len(seeds),
                 "seeds": f"{seeds[0]}..{seeds[-1]}", "nnzb": w.nnzb,
-                "pcg_threads_autotuned": int(prof.get("pcg_threads", 0))},
+                "pcg_threads_autotuned": int(prof.get("pcg_threads", 0)),
+                "pcg_cluster_size_autotuned": int(prof.get("pcg_cluster_size", 0))},
         "converged": {"env_steps": head["converged_env_steps"], "of": head["env_steps"],
                       "frac": head["converged_env_steps"] / head["env_steps"],
                       "note": ("value counts every env-step; an env-step that hit the Newton cap before rel 1e-6 "

@@ -100,7 +100,7 @@ class Profile(C.Structure):
                 ("contact_ms", C.c_double), ("contact_launches", C.c_int64),
                 ("seed_ms", C.c_double), ("seed_launches", C.c_int64), ("pcg_bytes", C.c_double),
                 ("pcg_relaunches", C.c_int64), ("pcg_threads", C.c_int64), ("warm_ms", C.c_double),
-                ("warm_launches", C.c_int64), ("pcg_cluster_solves", C.c_int64)]
+                ("warm_launches", C.c_int64), ("pcg_cluster_solves", C.c_int64), ("pcg_cluster_size", C.c_int64)]
 
 
 _dp = C.POINTER(C.c_double)
@@ -200,6 +200,23 @@ def default_linear_params() -> LinearParams:
     p = LinearParams()
     lib().sdx_default_linear_params(C.byref(p))
     return p
+
+
+def pcg_cluster_shape_sized(n_envs: int, cluster_size: int):
+    """(clusters, CTAs per cluster) of the cluster PCG on the current device with cluster_size forced (the
+    shape the autotuner would time), (0, 0) when that size does not fit on the device."""
+    import os
+    old = os.environ.get("SDX_PCG_CLUSTER_SIZE")
+    os.environ["SDX_PCG_CLUSTER_SIZE"] = str(int(cluster_size))
+    try:
+        return pcg_cluster_shape(n_envs)
+    except SdxError:
+        return 0, 0
+    finally:
+        if old is None:
+            del os.environ["SDX_PCG_CLUSTER_SIZE"]
+        else:
+            os.environ["SDX_PCG_CLUSTER_SIZE"] = old
 
 
 def pcg_cluster_shape(n_envs: int):

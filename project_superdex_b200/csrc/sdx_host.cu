@@ -180,6 +180,7 @@ constexpr int kSnapVectors = 5 + kSnapHist;  // u, v, dx, dx_prev1, dx_prev2, dx
 struct sdx_context {
   int device = 0;
   int num_sms = 0;
+  int l2_bytes = 0;
   cudaStream_t stream = nullptr;
   int64_t launches = 0;
   sdx_step_params params;
@@ -268,6 +269,7 @@ struct sdx_context {
   double* dx_hist = nullptr;
   bool hist_valid[kHist] = {false, false, false, false};
   int pcg_threads = 0;         // threads per CTA of the context's PCG partition
+  int cl_size = 0;             // cluster size of the cluster PCG picked by the autotuner (0: by occupancy)
   int* env_nrows = nullptr;    // padded rows per env (device)
   int* env_soff = nullptr;     // per env, its first slice (device, n_envs + 1): the cluster PCG's env ranges
   int* cl_envs = nullptr;      // the cluster PCG's env queue (device, n_envs)
@@ -779,6 +781,10 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
   a.sync = W.sync;
   a.env_rel_tol = env_rel_tol;
   a.spin_limit = kSpinLimit;  // the cluster kernel keeps the default bound
+  // Prefetching the next slice's operands into L2 pays when the CG vectors stream from HBM (a large batch:
+  // measured -11 % per CG iteration on 1,024 bodies) and costs when they stay in L2 (the 64^3 body's 27 MB
+  // of vectors: +19 %).
+  a.prefetch = (double)W.arena_bytes > 0.5 * (double)c->l2_bytes ? 1 : 0;
   a.es = W.es;
   // re-partitioning applies to batches on the context matrix (SDX_PCG_REPART=0 disables it)
   static const bool repart_on = [] {
@@ -838,7 +844,8 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
         list.push_back(e);
         max_rows = std::max<int64_t>(max_rows, c->h_row_off[e + 1] - c->h_row_off[e]);
       }
-    const ClusterShape shape = (ce && atoi(ce) == 0) ? ClusterShape{0, 0, 0} : pcg_cluster_shape((int)list.size());
+    const ClusterShape shape =
+        (ce && atoi(ce) == 0) ? ClusterShape{0, 0, 0} : pcg_cluster_shape((int)list.size(), c->cl_size);
     const char* qf = getenv("SDX_PCG_CLUSTER_QUEUE");
     const char* tl = getenv("SDX_PCG_CLUSTER_TAIL");
     const int queue_factor = qf ? atoi(qf) : kClusterQueueFactor, tail_envs = tl ? atoi(tl) : kClusterTailEnvs;
@@ -994,6 +1001,7 @@ extern "C" sdx_context* sdx_create(int device) {
   sdx_context* c = new sdx_context();
   c->device = device;
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+  cudaDeviceGetAttribute(&c->l2_bytes, cudaDevAttrL2CacheSize, device);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete c;
     set_error(SDX_ERR_CUDA, "stream creation failed");
@@ -1079,6 +1087,7 @@ extern "C" int sdx_get_profile(sdx_context* c, sdx_profile* out) {
   prof_resolve(c);
   *out = c->prof;
   out->pcg_threads = c->pcg_threads;
+  out->pcg_cluster_size = c->cl_size;
   return SDX_OK;
 }
 
@@ -2201,7 +2210,8 @@ extern "C" int sdx_set_linear_solver(sdx_context* c, sdx_linear_solve_fn fn, voi
 // uploaded batch, each candidate shape runs a fixed 24-iteration solve of the real system (right-hand
 // side g, solution into a scratch vector, statistics off) and the fastest per iteration becomes the
 // context's partition. Candidates: 512 threads with the software-pipelined SpMV (128 registers),
-// 1024 / 768 threads with the batched SpMV (64 / 80 registers), 384 pipelined.
+// 1024 / 768 threads with the batched SpMV (64 / 80 registers), 384 pipelined; and, for a batch that the
+// cluster PCG takes, the cluster sizes 2, 4, 8 and 16.
 static int autotune_pcg(sdx_context* c, const sdx_linear_params& lp) {
   c->pcg_tuned = true;
   const char* env = getenv("SDX_PCG_AUTOTUNE");
@@ -2245,13 +2255,44 @@ static int autotune_pcg(sdx_context* c, const sdx_linear_params& lp) {
       best = t;
     }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  c->profiling = prof;
   if (best != c->pcg_threads) {
     SDX_TRY(choose_partition(c, c->n_slices, c->h_slice_env, c->n_envs, c->h_slice_ptr, c->part, best, 1));
     c->pcg_threads = best;
   }
+  // A batch that goes to the cluster PCG: time the same 24-iteration solve for each cluster size that fits
+  // (one thread-block cluster per env at a time, 2 to 16 CTAs) and keep the fastest for this batch.
+  if (c->n_envs > 1 && !getenv("SDX_PCG_CLUSTER_SIZE")) {
+    const ClusterShape base = pcg_cluster_shape(c->n_envs);
+    if (base.n_clusters > 0 && c->n_envs >= kClusterQueueFactor * base.n_clusters) {
+      int best_cs = 0;
+      double best_cl = 1e30;
+      for (int cs : {2, 4, 8, 16}) {
+        const ClusterShape sh = pcg_cluster_shape(c->n_envs, cs);
+        if (sh.size != cs || c->n_envs < kClusterQueueFactor * sh.n_clusters) continue;
+        c->cl_size = cs;
+        double us = 1e30;
+        for (int rep = 0; rep < 2; ++rep) {
+          SDX_CUDA(cudaEventRecord(e0, c->stream));
+          const int rc = run_pcg(c, ctx_matrix(c), c->diag_pos, c->n_envs, c->part, c->work, c->g, c->uscratch,
+                                 nullptr, c->n_envs, tl, /*zero_guess*/ true, nullptr);
+          SDX_CUDA(cudaEventRecord(e1, c->stream));
+          SDX_CUDA(cudaEventSynchronize(e1));
+          if (rc != SDX_OK) break;
+          float ms = 0.0f;
+          cudaEventElapsedTime(&ms, e0, e1);
+          us = 1e3 * ms;
+        }
+        if (us < best_cl) {
+          best_cl = us;
+          best_cs = cs;
+        }
+      }
+      c->cl_size = best_cs;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->profiling = prof;
   return SDX_OK;
 }
 

@@ -161,6 +161,8 @@ struct PcgArgs {
   unsigned* sync;  // [0] barrier arrivals (monotonic), [1] unused, [2] error, [3] active envs,
                    // [4] verify_iter, [5] active rows, [6] resume iteration, [7] repartition exit
   long long spin_limit;
+  int prefetch;  // bulk L2 prefetch of each warp's next slice (matrix and update operands): set when the
+                 // CG vectors cannot stay in L2, so every operand comes from HBM
   // Re-partitioning: once the rows of the envs still iterating fall to repart_rows (0: never), the
   // kernel saves every env's CG scalars in es[] and exits after the iteration; the host re-partitions
   // the remaining envs over all CTAs and relaunches with resume = 1 from iteration it0.
@@ -210,7 +212,8 @@ void launch_copy_rows(int n_slices, const int* slice_env, const uint8_t* env_mas
 void launch_velocity(int64_t n3, const double* u, const double* u0, double dt, double* v,
                      cudaStream_t st);
 cudaError_t launch_pcg(const PcgArgs& a, int n_cta, int threads, cudaStream_t st);
-ClusterShape pcg_cluster_shape(int n_envs);
+// want_size > 0 asks for that cluster size (when it fits); SDX_PCG_CLUSTER_SIZE overrides both
+ClusterShape pcg_cluster_shape(int n_envs, int want_size = 0);
 cudaError_t launch_pcg_cluster(const PcgArgs& a, ClusterShape shape, cudaStream_t st);
 void launch_spmv(const Matrix& A, const float4* x, float* y, int threads, cudaStream_t st);
 void launch_bsr_to_sell(int n_rows, const int64_t* row_ptr, const int32_t* bcol, const float* bval, bool strips,

@@ -969,6 +969,35 @@ __device__ __forceinline__ void true_residual(const PcgArgs& a, int s, int lane,
   r[2] = a.b[3 * row + 2] - ax[2];
 }
 
+// Bulk L2 prefetch of [ptr, ptr + bytes) (one instruction, no registers held; address and size multiples of
+// 16 bytes). A warp issues these for the slice it will process next, so that slice's loads hit L2.
+__device__ __forceinline__ void prefetch_l2(const void* ptr, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(ptr), "r"(bytes) : "memory");
+}
+
+// Phase-2 operands of slice s (DoF-linear: x, r FP64, p, q, Jacobi diagonal FP32, z float4 rows), one array per
+// lane 0..5.
+__device__ __forceinline__ void prefetch_update_operands(const PcgArgs& a, int s, int lane) {
+  const int64_t d0 = (int64_t)s * (3 * kSlice);
+  if (lane == 0) prefetch_l2(a.x + d0, 3 * kSlice * 8);
+  if (lane == 1) prefetch_l2(a.r + d0, 3 * kSlice * 8);
+  if (lane == 2) prefetch_l2(a.p + d0, 3 * kSlice * 4);
+  if (lane == 3) prefetch_l2(a.q + d0, 3 * kSlice * 4);
+  if (lane == 4 && a.precond == 1) prefetch_l2(a.dinv + d0, 3 * kSlice * 4);
+  if (lane == 5) prefetch_l2(a.z + (int64_t)s * kSlice, kSlice * 16);
+}
+
+// Matrix range of slice s (column indices and the 9 values of every block position), lanes 6 and 7.
+__device__ __forceinline__ void prefetch_slice_matrix(const Matrix& A, int s, int lane) {
+  if (lane != 6 && lane != 7) return;
+  const int base = A.slice_ptr[s], w = A.slice_w[s];
+  if (w <= 0) return;
+  if (lane == 6)
+    prefetch_l2(A.col + base, (uint32_t)(w * kSlice * 4));
+  else
+    prefetch_l2(A.val + (size_t)base * 9, (uint32_t)(w * kSlice * 36));
+}
+
 // kPipe: SpMV phase with the software-pipelined row product (128 registers, so at most 512 threads per
 // SM); otherwise the batched product that fits 64 registers at 1024 threads.
 // kTimed: the variant with the per-CTA phase timers (launched only when they are asked for, so that the
@@ -1373,6 +1402,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
       const int s = slice_of(i);
       const int le = local_env(a.A.slice_env[s]);
       if (st[le].status != 0) continue;
+      if (a.prefetch && i + nwarps < s1) prefetch_slice_matrix(a.A, slice_of(i + nwarps), lane);
       const int64_t d0 = (int64_t)s * (3 * kSlice);
       // own DoF operands are loaded before the row product so that their latency overlaps it
       const bool first = st[le].first != 0;
@@ -1445,8 +1475,14 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     if (a.precond != 2) {
       // none / Jacobi: element-wise, DoF-linear (contiguous 256-byte lines of x and r per warp instruction)
       float* zw = reinterpret_cast<float*>(a.z);
+      // prefetch distance: kAhead slices of this warp (one slice's update is shorter than an HBM round trip)
+      constexpr int kAhead = 3;
+      if (a.prefetch)
+        for (int k = 0; k < kAhead && s0 + warp + k * nwarps < s1; ++k)
+          prefetch_update_operands(a, slice_of(s0 + warp + k * nwarps), lane);
       for (int i = s0 + warp; i < s1; i += nwarps) {
         const int s = slice_of(i);
+        if (a.prefetch && i + kAhead * nwarps < s1) prefetch_update_operands(a, slice_of(i + kAhead * nwarps), lane);
         const int le = local_env(a.A.slice_env[s]);
         if (st[le].status != 0) continue;
         const int64_t d0 = (int64_t)s * (3 * kSlice);
@@ -1922,6 +1958,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
       // phase 1: p = z + beta p, q = A z + beta q, p.q (vector updates DoF-linear, as in k_pcg)
       acc_reset();
       for (int s = c0 + warp; s < c1; s += nwarps) {
+        if (a.prefetch && s + nwarps < c1) prefetch_slice_matrix(a.A, s + nwarps, lane);
         const int64_t d0 = (int64_t)s * (3 * kSlice);
         float po[3] = {0.0f, 0.0f, 0.0f}, qo[3] = {0.0f, 0.0f, 0.0f};
         if (!first) {
@@ -1967,7 +2004,12 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
       // phase 2: x += alpha p, r -= alpha q, z = M^-1 r, r.r, r.z_old, r.z (DoF-linear unless block Jacobi)
       acc_reset();
       if (a.precond != 2) {
+        constexpr int kAhead = 3;  // prefetch distance in this warp's slices (as in k_pcg)
+        if (a.prefetch)
+          for (int k = 0; k < kAhead && c0 + warp + k * nwarps < c1; ++k)
+            prefetch_update_operands(a, c0 + warp + k * nwarps, lane);
         for (int s = c0 + warp; s < c1; s += nwarps) {
+          if (a.prefetch && s + kAhead * nwarps < c1) prefetch_update_operands(a, s + kAhead * nwarps, lane);
           const int64_t d0 = (int64_t)s * (3 * kSlice);
           double xo[3], ro[3];
           float pp[3], qq[3], dd[3], zo[3];
@@ -2155,11 +2197,11 @@ static const int* pcg_cluster_counts(int* last_error) {
 // co-resident clusters) clusters, ties to the larger clusters (an env's iterations are latency bound
 // well before its rows fill a cluster; on the 1,024-body batch 37 x 4 beats 74 x 2 by 3 %).
 // SDX_PCG_CLUSTER_SIZE=16/8/4/2 forces a size.
-ClusterShape pcg_cluster_shape(int n_envs) {
+ClusterShape pcg_cluster_shape(int n_envs, int want_size) {
   int err = 0;
   const int* counts = pcg_cluster_counts(&err);
   const char* force = getenv("SDX_PCG_CLUSTER_SIZE");
-  const int want = force ? atoi(force) : 0;
+  const int want = force ? atoi(force) : want_size;
   ClusterShape best{0, 0, err};
   int best_busy = 0;
   for (int i = 0; i < 4; ++i) {

@@ -96,3 +96,31 @@ def test_cluster_and_grid_kernels_agree_on_a_contact_batch(monkeypatch, warm):
         assert sa["convergence"] == sb["convergence"]
         assert abs(sa["newton_iters"] - sb["newton_iters"]) <= 1
         assert abs(sa["cg_iters"] - sb["cg_iters"]) <= max(6, int(0.15 * sa["cg_iters"]))
+
+
+def test_autotuner_picks_a_cluster_size_and_keeps_the_result(monkeypatch):
+    """SDX_PCG_AUTOTUNE=1 on a long queue of small envs (160 bodies, taken by the cluster PCG): the tuner
+    times the cluster sizes whose clusters the queue keeps busy and keeps the fastest; the steps equal
+    the untuned ones to the CG tolerance."""
+    from project_superdex_b200 import capi
+    from project_superdex_b200.soft_body import SoftBodyWorld
+    bodies = []
+    for i in range(160):
+        rng = np.random.default_rng(500 + i)
+        n = 3 + i % 3
+        bodies.append(scenes.grid_body(n, n, n + 1, 0.004, rng=rng, E=float(rng.uniform(3e4, 3e5)), nu=0.4))
+    cfg = scenes.SceneConfig()
+    n_cl = {cs: capi.pcg_cluster_shape_sized(160, cs) for cs in (2, 4, 8, 16)}
+    fits = {cs for cs, (n, size) in n_cl.items() if size == cs and 160 >= 4 * n}
+    monkeypatch.setenv("SDX_PCG_AUTOTUNE", "1")
+    monkeypatch.delenv("SDX_PCG_CLUSTER_SIZE", raising=False)
+    w = SoftBodyWorld(bodies, cfg, newton_abs_tol=1e-9)
+    w.set_profiling(True)
+    w.step(2)
+    prof = w.profile()
+    assert prof["pcg_cluster_size"] in fits and prof["pcg_cluster_solves"] > 0
+    u_tuned = w.get_state()[0]
+    monkeypatch.setenv("SDX_PCG_AUTOTUNE", "0")
+    w0 = SoftBodyWorld(bodies, cfg, newton_abs_tol=1e-9)
+    w0.step(2)
+    assert np.abs(w0.get_state()[0] - u_tuned).max() <= 1e-5 * 0.02
