@@ -427,7 +427,7 @@ def merge(a, b):
     out["step_ms"] = a["step_ms"] + b["step_ms"]
     for k in ("newton_per_env_step", "cg_per_env_step"):
         out[k] = (a[k] * a["env_steps"] + b[k] * b["env_steps"]) / out["env_steps"]
-    out["prof"] = {k: (a["prof"].get(k, 0) + v if k not in ("pcg_threads", "pcg_cluster_size") else v)
+    out["prof"] = {k: (a["prof"].get(k, 0) + v if k not in ("pcg_threads", "pcg_cluster_size", "tune_grid_us", "tune_cluster_us") else v)
                    for k, v in b["prof"].items()}
     if "clocks" in a:
         ca, cb = a["clocks"], b["clocks"]
@@ -556,7 +556,8 @@ def run_ours(args, rank, world, local_rank):
         "run": {"arms": arms, "headline_arm": head_arm, "compare_steps": n_cmp, "episodes": len(seeds),
                 "seeds": f"{seeds[0]}..{seeds[-1]}", "nnzb": w.nnzb,
                 "pcg_threads_autotuned": int(prof.get("pcg_threads", 0)),
-                "pcg_cluster_size_autotuned": int(prof.get("pcg_cluster_size", 0))},
+                "pcg_cluster_size_autotuned": int(prof.get("pcg_cluster_size", 0)),
+                "autotune_us": {"grid": prof.get("tune_grid_us", 0.0), "cluster": prof.get("tune_cluster_us", 0.0)}},
         "converged": {"env_steps": head["converged_env_steps"], "of": head["env_steps"],
                       "frac": head["converged_env_steps"] / head["env_steps"],
                       "note": ("value counts every env-step; an env-step that hit the Newton cap before rel 1e-6 "

@@ -376,7 +376,10 @@ typedef struct {
   int64_t warm_launches;
   int64_t pcg_cluster_solves; /* PCG solves that ran on the cluster kernel (a batch of small envs, one
                                  thread-block cluster per env at a time) instead of the grid kernel */
-  int64_t pcg_cluster_size;   /* cluster size the autotuner picked for this batch (0: chosen by occupancy) */
+  int64_t pcg_cluster_size;   /* cluster size the autotuner picked for this batch (0: chosen by occupancy;
+                                 -1: the grid kernel won, long queues stay on it) */
+  double tune_grid_us;        /* autotuner: best grid-kernel time of its 24-iteration solve (0: not tuned) */
+  double tune_cluster_us;     /* autotuner: best cluster-kernel time of the same solve (0: none timed) */
 } sdx_profile;
 /* enable: 0 off, 1 per-kernel event timing, 2 also the per-CTA PCG phase timers (sdx_get_pcg_cta_profile) */
 int sdx_set_profiling(sdx_context* ctx, int enable);

@@ -100,7 +100,8 @@ class Profile(C.Structure):
                 ("contact_ms", C.c_double), ("contact_launches", C.c_int64),
                 ("seed_ms", C.c_double), ("seed_launches", C.c_int64), ("pcg_bytes", C.c_double),
                 ("pcg_relaunches", C.c_int64), ("pcg_threads", C.c_int64), ("warm_ms", C.c_double),
-                ("warm_launches", C.c_int64), ("pcg_cluster_solves", C.c_int64), ("pcg_cluster_size", C.c_int64)]
+                ("warm_launches", C.c_int64), ("pcg_cluster_solves", C.c_int64), ("pcg_cluster_size", C.c_int64),
+                ("tune_grid_us", C.c_double), ("tune_cluster_us", C.c_double)]
 
 
 _dp = C.POINTER(C.c_double)

@@ -269,7 +269,9 @@ struct sdx_context {
   double* dx_hist = nullptr;
   bool hist_valid[kHist] = {false, false, false, false};
   int pcg_threads = 0;         // threads per CTA of the context's PCG partition
-  int cl_size = 0;             // cluster size of the cluster PCG picked by the autotuner (0: by occupancy)
+  int cl_size = 0;             // cluster PCG size picked by the autotuner (0: by occupancy; -1: long queues
+                               // stay on the grid kernel)
+  double tune_grid_us = 0.0, tune_cluster_us = 0.0;  // the autotuner's best grid / cluster solve times
   int* env_nrows = nullptr;    // padded rows per env (device)
   int* env_soff = nullptr;     // per env, its first slice (device, n_envs + 1): the cluster PCG's env ranges
   int* cl_envs = nullptr;      // the cluster PCG's env queue (device, n_envs)
@@ -734,6 +736,9 @@ static int alloc_work(PcgWork& W, int64_t n_rows, int n_envs, bool newton_vector
   return SDX_OK;
 }
 
+// Prefetch distance (in a warp's slices) of the PCG update phase when the vectors stream from HBM.
+constexpr int kPcgPrefetchAhead = 3;
+
 // Runs the persistent PCG on matrix A for the envs in env_mask (NULL = all), b -> x.
 // share of the rows still iterating at which a batched PCG launch re-partitions
 constexpr double kPcgRepartRatio = 0.5;
@@ -783,8 +788,13 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
   a.spin_limit = kSpinLimit;  // the cluster kernel keeps the default bound
   // Prefetching the next slice's operands into L2 pays when the CG vectors stream from HBM (a large batch:
   // measured -11 % per CG iteration on 1,024 bodies) and costs when they stay in L2 (the 64^3 body's 27 MB
-  // of vectors: +19 %).
-  a.prefetch = (double)W.arena_bytes > 0.5 * (double)c->l2_bytes ? 1 : 0;
+  // of vectors: +19 %). SDX_PCG_PREFETCH sets the distance in slices (0: off) for every size.
+  static const int prefetch_env = [] {
+    const char* v = getenv("SDX_PCG_PREFETCH");
+    return v ? std::max(0, std::min(8, atoi(v))) : -1;
+  }();
+  a.prefetch = prefetch_env >= 0 ? prefetch_env
+                                 : ((double)W.arena_bytes > 0.5 * (double)c->l2_bytes ? kPcgPrefetchAhead : 0);
   a.es = W.es;
   // re-partitioning applies to batches on the context matrix (SDX_PCG_REPART=0 disables it)
   static const bool repart_on = [] {
@@ -850,7 +860,7 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
     const char* tl = getenv("SDX_PCG_CLUSTER_TAIL");
     const int queue_factor = qf ? atoi(qf) : kClusterQueueFactor, tail_envs = tl ? atoi(tl) : kClusterTailEnvs;
     const int n_list = (int)list.size();
-    const bool long_queue = queue_factor > 0 && n_list >= queue_factor * shape.n_clusters;
+    const bool long_queue = queue_factor > 0 && c->cl_size >= 0 && n_list >= queue_factor * shape.n_clusters;
     const char* tr = getenv("SDX_PCG_CLUSTER_TAIL_ROWS");
     const int64_t tail_rows = tr ? atoll(tr) : kClusterLatencyRows;
     const bool tail = n_list <= tail_envs && max_rows <= tail_rows;
@@ -1088,6 +1098,8 @@ extern "C" int sdx_get_profile(sdx_context* c, sdx_profile* out) {
   *out = c->prof;
   out->pcg_threads = c->pcg_threads;
   out->pcg_cluster_size = c->cl_size;
+  out->tune_grid_us = c->tune_grid_us;
+  out->tune_cluster_us = c->tune_cluster_us;
   return SDX_OK;
 }
 
@@ -2210,8 +2222,9 @@ extern "C" int sdx_set_linear_solver(sdx_context* c, sdx_linear_solve_fn fn, voi
 // uploaded batch, each candidate shape runs a fixed 24-iteration solve of the real system (right-hand
 // side g, solution into a scratch vector, statistics off) and the fastest per iteration becomes the
 // context's partition. Candidates: 512 threads with the software-pipelined SpMV (128 registers),
-// 1024 / 768 threads with the batched SpMV (64 / 80 registers), 384 pipelined; and, for a batch that the
-// cluster PCG takes, the cluster sizes 2, 4, 8 and 16.
+// 1024 / 768 threads with the batched SpMV (64 / 80 registers), 384 pipelined, all on the grid kernel;
+// then, for a batch whose queue keeps the clusters of some size busy, the cluster PCG with each such
+// cluster size (2, 4, 8, 16) against the best grid shape.
 static int autotune_pcg(sdx_context* c, const sdx_linear_params& lp) {
   c->pcg_tuned = true;
   const char* env = getenv("SDX_PCG_AUTOTUNE");
@@ -2223,6 +2236,8 @@ static int autotune_pcg(sdx_context* c, const sdx_linear_params& lp) {
   tl.rel_tol = 0.0;
   tl.abs_tol = 0.0;
   const int cand[4] = {512, 1024, 768, 384};
+  const int cl_keep = c->cl_size;
+  c->cl_size = -1;  // the thread shapes are timed on the grid kernel
   double best_us = 1e30;
   int best = c->pcg_threads > 0 ? c->pcg_threads : 512;
   cudaEvent_t e0, e1;
@@ -2259,36 +2274,43 @@ static int autotune_pcg(sdx_context* c, const sdx_linear_params& lp) {
     SDX_TRY(choose_partition(c, c->n_slices, c->h_slice_env, c->n_envs, c->h_slice_ptr, c->part, best, 1));
     c->pcg_threads = best;
   }
-  // A batch that goes to the cluster PCG: time the same 24-iteration solve for each cluster size that fits
-  // (one thread-block cluster per env at a time, 2 to 16 CTAs) and keep the fastest for this batch.
+  // The cluster PCG with each cluster size whose co-resident clusters the queue keeps busy (at least
+  // kClusterQueueFactor envs per cluster), timed on the same 24-iteration solve. The grid kernel's
+  // lockstep loses rows to envs that converged early, which the cluster queue does not, and this
+  // balanced solve cannot show: the grid replaces the fastest cluster size only when it is faster by
+  // more than kGridOverClusterMargin. cl_size = -1 keeps the long queue on the grid kernel.
+  c->cl_size = cl_keep;
   if (c->n_envs > 1 && !getenv("SDX_PCG_CLUSTER_SIZE")) {
-    const ClusterShape base = pcg_cluster_shape(c->n_envs);
-    if (base.n_clusters > 0 && c->n_envs >= kClusterQueueFactor * base.n_clusters) {
-      int best_cs = 0;
-      double best_cl = 1e30;
-      for (int cs : {2, 4, 8, 16}) {
-        const ClusterShape sh = pcg_cluster_shape(c->n_envs, cs);
-        if (sh.size != cs || c->n_envs < kClusterQueueFactor * sh.n_clusters) continue;
-        c->cl_size = cs;
-        double us = 1e30;
-        for (int rep = 0; rep < 2; ++rep) {
-          SDX_CUDA(cudaEventRecord(e0, c->stream));
-          const int rc = run_pcg(c, ctx_matrix(c), c->diag_pos, c->n_envs, c->part, c->work, c->g, c->uscratch,
-                                 nullptr, c->n_envs, tl, /*zero_guess*/ true, nullptr);
-          SDX_CUDA(cudaEventRecord(e1, c->stream));
-          SDX_CUDA(cudaEventSynchronize(e1));
-          if (rc != SDX_OK) break;
-          float ms = 0.0f;
-          cudaEventElapsedTime(&ms, e0, e1);
-          us = 1e3 * ms;
+    constexpr double kGridOverClusterMargin = 1.10;
+    int best_cs = 0;
+    double best_cl = 1e30;
+    for (int cs : {2, 4, 8, 16}) {
+      const ClusterShape sh = pcg_cluster_shape(c->n_envs, cs);
+      if (sh.size != cs || sh.n_clusters <= 0 || c->n_envs < kClusterQueueFactor * sh.n_clusters) continue;
+      c->cl_size = cs;
+      double us = 1e30;
+      for (int rep = 0; rep < 2; ++rep) {
+        SDX_CUDA(cudaEventRecord(e0, c->stream));
+        const int rc = run_pcg(c, ctx_matrix(c), c->diag_pos, c->n_envs, c->part, c->work, c->g, c->uscratch,
+                               nullptr, c->n_envs, tl, /*zero_guess*/ true, nullptr);
+        SDX_CUDA(cudaEventRecord(e1, c->stream));
+        SDX_CUDA(cudaEventSynchronize(e1));
+        if (rc != SDX_OK) {
+          us = 1e30;
+          break;
         }
-        if (us < best_cl) {
-          best_cl = us;
-          best_cs = cs;
-        }
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        us = 1e3 * ms;
       }
-      c->cl_size = best_cs;
+      if (us < best_cl) {
+        best_cl = us;
+        best_cs = cs;
+      }
     }
+    c->cl_size = best_cs == 0 ? cl_keep : (best_cl > kGridOverClusterMargin * best_us ? -1 : best_cs);
+    c->tune_grid_us = best_us;
+    c->tune_cluster_us = best_cs ? best_cl : 0.0;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

@@ -6,7 +6,9 @@
     python -m project_superdex_b200.kernel_cases element
         one full assembly (energy, residual, PSD-projected Hessian) of the current state;
     python -m project_superdex_b200.kernel_cases spmv --reps 3
-        `reps` standalone SpMVs of the last assembled matrix.
+        `reps` standalone SpMVs of the last assembled matrix;
+    python -m project_superdex_b200.kernel_cases mlp --rows 274656 --reps 3
+        `reps` tensor-core forwards of the warm-start MLP (random weights) over `rows` feature rows.
 
 The workload is the single-body 64^3-cell grid (274,625 nodes, 1,572,864 tets, 5 capsules) unless
 `--cells` says otherwise; `--workload batch` takes the 1,024 uneven bodies (cells per axis U{8..40},
@@ -40,9 +42,40 @@ def element_bytes(n_tets: int, n_nodes: int, nnzb: int) -> int:
     return n_tets * (16 + 64 + 64) + n_nodes * (48 + 48) + nnzb * 36
 
 
+def mlp_flops_per_row() -> int:
+    """Tensor-core FLOPs of one forward row: 2 x (16 x 128 + 128 x 128 + 128 x 128 + 128 x 16) (the input is
+    padded to 16 features and the 3 outputs to 16 columns, as the MMA shapes require)."""
+    return 2 * (16 * 128 + 128 * 128 + 128 * 128 + 128 * 16)
+
+
+def mlp_case(rows: int, reps: int):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from . import capi
+    from .learned import Mlp
+    L = capi.lib()
+    ctx = L.sdx_create(0)
+    m = Mlp(ctx)
+    m.init(0)
+    X = np.random.default_rng(0).standard_normal((rows, 16)).astype(np.float32)
+    m.forward(X[:1024])  # warm-up (weights to the device, kernel attributes)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    for _ in range(reps):
+        m.forward(X)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    L.sdx_destroy(ctx)
+    return {"case": "mlp", "rows": rows, "reps": reps, "flops_per_forward": mlp_flops_per_row() * rows}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["pcg", "element", "spmv"])
+    ap.add_argument("case", choices=["pcg", "element", "spmv", "mlp"])
+    ap.add_argument("--rows", type=int, default=274656, help="mlp: feature rows per forward")
     ap.add_argument("--workload", choices=["cube", "batch"], default="cube")
     ap.add_argument("--cells", type=int, default=64)
     ap.add_argument("--iters", type=int, default=100)
@@ -52,6 +85,9 @@ def main(argv=None):
     ap.add_argument("--cta-profile", default=None,
                     help="pcg: also time each CTA's phases over two launches and save them to this .npy")
     args = ap.parse_args(argv)
+    if args.case == "mlp":
+        print(json.dumps(mlp_case(args.rows, args.reps)))
+        return
     if args.workload == "batch":
         bodies, cfg = scenes.config2(args.seed, n_envs=args.envs)
     else:

@@ -99,9 +99,9 @@ def test_cluster_and_grid_kernels_agree_on_a_contact_batch(monkeypatch, warm):
 
 
 def test_autotuner_picks_a_cluster_size_and_keeps_the_result(monkeypatch):
-    """SDX_PCG_AUTOTUNE=1 on a long queue of small envs (160 bodies, taken by the cluster PCG): the tuner
-    times the cluster sizes whose clusters the queue keeps busy and keeps the fastest; the steps equal
-    the untuned ones to the CG tolerance."""
+    """SDX_PCG_AUTOTUNE=1 on a long queue of small envs (160 bodies): the tuner times the grid kernel and
+    every cluster size whose clusters the queue keeps busy and keeps the fastest (-1: the grid); the
+    steps equal the untuned ones to the CG tolerance."""
     from project_superdex_b200 import capi
     from project_superdex_b200.soft_body import SoftBodyWorld
     bodies = []
@@ -118,7 +118,12 @@ def test_autotuner_picks_a_cluster_size_and_keeps_the_result(monkeypatch):
     w.set_profiling(True)
     w.step(2)
     prof = w.profile()
-    assert prof["pcg_cluster_size"] in fits and prof["pcg_cluster_solves"] > 0
+    assert fits and prof["tune_grid_us"] > 0 and prof["tune_cluster_us"] > 0
+    cs = prof["pcg_cluster_size"]
+    assert cs in fits | {-1}
+    assert (cs == -1) == (prof["tune_cluster_us"] > 1.10 * prof["tune_grid_us"])
+    if cs > 0:
+        assert prof["pcg_cluster_solves"] > 0
     u_tuned = w.get_state()[0]
     monkeypatch.setenv("SDX_PCG_AUTOTUNE", "0")
     w0 = SoftBodyWorld(bodies, cfg, newton_abs_tol=1e-9)
