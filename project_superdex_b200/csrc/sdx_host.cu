@@ -194,7 +194,7 @@ struct sdx_context {
   // host topology
   std::vector<int64_t> h_node_off, h_tet_off, h_row_off;
   std::vector<int32_t> h_row_of_node;
-  std::vector<double> h_env_pcg_bytes;  // algorithmic bytes of one CG iteration of each env
+  std::vector<double> h_env_pcg_bytes;  // algorithmic matrix bytes of one CG iteration of each env
   std::vector<int64_t> h_prow;  // user pattern row_ptr
   std::vector<int32_t> h_pcol;  // user pattern columns (user node ids)
   std::vector<int> h_slice_ptr, h_slice_w, h_slice_env;
@@ -786,15 +786,25 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
   a.sync = W.sync;
   a.env_rel_tol = env_rel_tol;
   a.spin_limit = kSpinLimit;  // the cluster kernel keeps the default bound
-  // Prefetching the next slice's operands into L2 pays when the CG vectors stream from HBM (a large batch:
-  // measured -11 % per CG iteration on 1,024 bodies) and costs when they stay in L2 (the 64^3 body's 27 MB
-  // of vectors: +19 %). SDX_PCG_PREFETCH sets the distance in slices (0: off) for every size.
+  // Prefetching the next slice's operands into L2 pays when the CG vectors stream from HBM (a large batch on
+  // the cluster kernel: 2,888 -> 2,513 us per CG iteration on 1,024 bodies) and costs when they stay in L2
+  // (the 64^3 body's 27 MB of vectors: +19 %). SDX_PCG_PREFETCH sets the distance in slices (0: off).
   static const int prefetch_env = [] {
     const char* v = getenv("SDX_PCG_PREFETCH");
     return v ? std::max(0, std::min(8, atoi(v))) : -1;
   }();
-  a.prefetch = prefetch_env >= 0 ? prefetch_env
-                                 : ((double)W.arena_bytes > 0.5 * (double)c->l2_bytes ? kPcgPrefetchAhead : 0);
+  const bool streamed = (double)W.arena_bytes > 0.5 * (double)c->l2_bytes;
+  a.prefetch = prefetch_env >= 0 ? prefetch_env : (streamed ? kPcgPrefetchAhead : 0);
+  // When the CG vectors stream from HBM, r is carried by z between true-residual replacements
+  // (SDX_PCG_R_IN_Z=0/1 forces it off/on): the update phase then reads and writes no FP64 r (1,024 bodies:
+  // 2,843 -> 2,483 us per CG iteration on the grid kernel, CG iteration counts unchanged). With the vectors
+  // in L2 the update phase is short, and the exact FP64 r keeps CG's iteration counts: a system that
+  // converges by finite termination (the 64-row tridiagonal golden system, 32 iterations) needs it.
+  static const int r_in_z_env = [] {
+    const char* v = getenv("SDX_PCG_R_IN_Z");
+    return v ? (atoi(v) != 0) : -1;
+  }();
+  a.r_in_z = r_in_z_env >= 0 ? r_in_z_env : (streamed ? 1 : 0);
   a.es = W.es;
   // re-partitioning applies to batches on the context matrix (SDX_PCG_REPART=0 disables it)
   static const bool repart_on = [] {
@@ -833,8 +843,13 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
         if (h_mask && !h_mask[e]) its[e] = 0;  // the envs this solve was asked for
       c->prof.pcg_iters += *std::max_element(its.begin(), its.end());
       c->prof.pcg_launches++;
-      if (A.val == c->val && (int)c->h_env_pcg_bytes.size() == n_envs)
-        for (int e = 0; e < n_envs; ++e) c->prof.pcg_bytes += its[e] * c->h_env_pcg_bytes[e];
+      if (A.val == c->val && (int)c->h_env_pcg_bytes.size() == n_envs) {
+        // vector bytes per row: 228 with FP64 r; r carried by z saves its FP64 read and write (48)
+        const double per_row = 228.0 - (a.r_in_z && a.precond != 2 ? 48.0 : 0.0);
+        for (int e = 0; e < n_envs; ++e)
+          c->prof.pcg_bytes += its[e] * (c->h_env_pcg_bytes[e] +
+                                         per_row * (double)(c->h_node_off[e + 1] - c->h_node_off[e]));
+      }
     }
     return SDX_OK;
   };
@@ -1252,7 +1267,7 @@ extern "C" int sdx_upload_bodies(sdx_context* c, int n_envs, const int64_t* node
   for (int e = 0; e < n_envs; ++e) {
     const int64_t n_e = node_off[e + 1] - node_off[e];
     const int64_t b_e = c->h_prow[node_off[e + 1]] - c->h_prow[node_off[e]];
-    c->h_env_pcg_bytes[e] = 40.0 * (double)b_e + 4.0 * (double)(n_e + 1) + 228.0 * (double)n_e;
+    c->h_env_pcg_bytes[e] = 40.0 * (double)b_e + 4.0 * (double)(n_e + 1);
   }
   c->h_pcol.resize(c->nnzb);
 #pragma omp parallel

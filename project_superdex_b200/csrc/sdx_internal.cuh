@@ -161,9 +161,11 @@ struct PcgArgs {
   unsigned* sync;  // [0] barrier arrivals (monotonic), [1] unused, [2] error, [3] active envs,
                    // [4] verify_iter, [5] active rows, [6] resume iteration, [7] repartition exit
   long long spin_limit;
-  int prefetch;  // bulk L2 prefetch of each warp's next slices (0: none): the phase-2 distance in slices (the
-                 // matrix of the next slice in phase 1 whenever it is set); set when the CG vectors cannot stay
-                 // in L2, so every operand comes from HBM
+  int r_in_z;    // Jacobi / no preconditioner: r is carried by z between true-residual replacements
+                 // (r = z / d, FP32 precision), so the update phase reads and writes no FP64 r
+  int prefetch;  // bulk L2 prefetch of each warp's next slices (0: none): the update phase's distance in
+                 // slices (the matrix of the next slice in the SpMV phase whenever it is set); set when the
+                 // CG vectors cannot stay in L2, so every operand comes from HBM
   // Re-partitioning: once the rows of the envs still iterating fall to repart_rows (0: never), the
   // kernel saves every env's CG scalars in es[] and exits after the iteration; the host re-partitions
   // the remaining envs over all CTAs and relaunches with resume = 1 from iteration it0.

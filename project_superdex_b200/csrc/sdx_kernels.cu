@@ -975,12 +975,12 @@ __device__ __forceinline__ void prefetch_l2(const void* ptr, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(ptr), "r"(bytes) : "memory");
 }
 
-// Phase-2 operands of slice s (DoF-linear: x, r FP64, p, q, Jacobi diagonal FP32, z float4 rows), one array per
-// lane 0..5.
+// Phase-2 operands of slice s (DoF-linear: x FP64, p, q, Jacobi diagonal FP32, z float4 rows; r FP64 unless z
+// carries it), one array per lane 0..5.
 __device__ __forceinline__ void prefetch_update_operands(const PcgArgs& a, int s, int lane) {
   const int64_t d0 = (int64_t)s * (3 * kSlice);
   if (lane == 0) prefetch_l2(a.x + d0, 3 * kSlice * 8);
-  if (lane == 1) prefetch_l2(a.r + d0, 3 * kSlice * 8);
+  if (lane == 1 && !a.r_in_z) prefetch_l2(a.r + d0, 3 * kSlice * 8);
   if (lane == 2) prefetch_l2(a.p + d0, 3 * kSlice * 4);
   if (lane == 3) prefetch_l2(a.q + d0, 3 * kSlice * 4);
   if (lane == 4 && a.precond == 1) prefetch_l2(a.dinv + d0, 3 * kSlice * 4);
@@ -1296,7 +1296,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
   #pragma unroll
         for (int k = 0; k < 3; ++k) {
           const float d = dp >= 0 ? a.A.val[val_index(dp, 4 * k)] : 0.0f;
-          a.dinv[3 * row + k] = d != 0.0f ? 1.0f / d : 0.0f;
+          a.dinv[3 * row + k] = d != 0.0f ? 1.0f / d : 1.0f;
         }
       } else if (a.precond == 2) {
         float B[9];
@@ -1473,51 +1473,67 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     // ---- phase 2 ----
     clear_acc();
     if (a.precond != 2) {
-      // none / Jacobi: element-wise, DoF-linear (contiguous 256-byte lines of x and r per warp instruction)
-      float* zw = reinterpret_cast<float*>(a.z);
-      // prefetch distance: kAhead slices of this warp (one slice's update is shorter than an HBM round trip)
-      constexpr int kAhead = 3;
-      if (a.prefetch)
-        for (int k = 0; k < kAhead && s0 + warp + k * nwarps < s1; ++k)
-          prefetch_update_operands(a, slice_of(s0 + warp + k * nwarps), lane);
+      // none / Jacobi: element-wise, DoF-linear (contiguous 256-byte lines of x and r per warp instruction);
+      // prefetch distance a.prefetch slices of this warp (one slice's update is shorter than an HBM round
+      // trip)
+      const int ahead = a.prefetch;
+      for (int k = 0; k < ahead && s0 + warp + k * nwarps < s1; ++k)
+        prefetch_update_operands(a, slice_of(s0 + warp + k * nwarps), lane);
       for (int i = s0 + warp; i < s1; i += nwarps) {
         const int s = slice_of(i);
-        if (a.prefetch && i + kAhead * nwarps < s1) prefetch_update_operands(a, slice_of(i + kAhead * nwarps), lane);
+        if (ahead > 0 && i + ahead * nwarps < s1) prefetch_update_operands(a, slice_of(i + ahead * nwarps), lane);
         const int le = local_env(a.A.slice_env[s]);
         if (st[le].status != 0) continue;
         const int64_t d0 = (int64_t)s * (3 * kSlice);
-        // every operand load is issued before the first store (the update is latency bound)
-        double xo[3], ro[3];
+        const double al = st[le].alpha;
+        if (replace) {  // only x: the true residual that follows recomputes r and z
+#pragma unroll
+          for (int j = 0; j < 3; ++j) a.x[d0 + lane + 32 * j] += al * (double)a.p[d0 + lane + 32 * j];
+          continue;
+        }
+        // With r_in_z, r is carried by z between true-residual replacements: r = z / d (FP32 precision;
+        // d = 1 without a preconditioner), so the update reads and writes no FP64 r. Every operand load is
+        // issued before the first store (the update is latency bound).
+        double xo[3], ro[3] = {0.0, 0.0, 0.0};
         float pp[3], qq[3], dd[3], zo[3];
+        // the old z arrives as whole float4 rows (one per lane) and reaches the DoF layout through the
+        // warp's staging row
+        const float4 zrow = a.z[(int64_t)s * kSlice + lane];
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
           const int dl = lane + 32 * j;
           xo[j] = a.x[d0 + dl];
           pp[j] = a.p[d0 + dl];
-          ro[j] = a.r[d0 + dl];
+          if (!a.r_in_z) ro[j] = a.r[d0 + dl];
           qq[j] = a.q[d0 + dl];
-          dd[j] = (!replace && a.precond == 1) ? a.dinv[d0 + dl] : 1.0f;
-          zo[j] = replace ? 0.0f : zw[4 * ((int64_t)s * kSlice + dl / 3) + dl % 3];
+          dd[j] = a.precond == 1 ? a.dinv[d0 + dl] : 1.0f;
         }
-        const double al = st[le].alpha;
-        double r[3];
+        tr[3 * lane] = zrow.x;
+        tr[3 * lane + 1] = zrow.y;
+        tr[3 * lane + 2] = zrow.z;
+        __syncwarp();
 #pragma unroll
-        for (int j = 0; j < 3; ++j) {
-          a.x[d0 + lane + 32 * j] = xo[j] + al * (double)pp[j];
-          r[j] = ro[j] - al * (double)qq[j];
-        }
-        if (replace) continue;
+        for (int j = 0; j < 3; ++j) zo[j] = tr[lane + 32 * j];
+        __syncwarp();
         double rr = 0.0, rzo = 0.0, rz = 0.0;
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
           const int dl = lane + 32 * j;
-          const float z = (float)(dd[j] * r[j]);
-          a.r[d0 + dl] = r[j];
-          zw[4 * ((int64_t)s * kSlice + dl / 3) + dl % 3] = z;
-          rr += r[j] * r[j];
-          rzo += r[j] * zo[j];
-          rz += r[j] * z;
+          a.x[d0 + dl] = xo[j] + al * (double)pp[j];
+          const double rp =
+              !a.r_in_z ? ro[j] : (a.precond == 1 ? (double)zo[j] / (double)dd[j] : (double)zo[j]);
+          const double r = rp - al * (double)qq[j];
+          if (!a.r_in_z) a.r[d0 + dl] = r;
+          const float z = (float)(dd[j] * r);
+          tr[dl] = z;
+          rr += r * r;
+          rzo += r * zo[j];
+          rz += r * z;
         }
+        __syncwarp();
+        // new z: whole float4 rows (full sectors, no partial writes)
+        a.z[(int64_t)s * kSlice + lane] = make_float4(tr[3 * lane], tr[3 * lane + 1], tr[3 * lane + 2], 0.0f);
+        __syncwarp();
         acc_add(le, 0, rr);
         acc_add(le, 1, rzo);
         acc_add(le, 2, rz);
@@ -1732,7 +1748,6 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   float* const tr = s_tr + warp * (3 * kSlice);
   const float* const zf = reinterpret_cast<const float*>(a.z);
-  float* const zw = reinterpret_cast<float*>(a.z);
   const uint32_t rank = cluster_rank(), csize = cluster_size();
   if (threadIdx.x == 0) s_cnt = 0u;
   cluster_hw_sync();  // every CTA's shared memory is live before any remote access
@@ -1893,7 +1908,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
           const float d = dp >= 0 ? a.A.val[val_index(dp, 4 * k)] : 0.0f;
-          a.dinv[3 * row + k] = d != 0.0f ? 1.0f / d : 0.0f;
+          a.dinv[3 * row + k] = d != 0.0f ? 1.0f / d : 1.0f;
         }
       } else if (a.precond == 2) {
         float B[9];
@@ -2004,43 +2019,56 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
       // phase 2: x += alpha p, r -= alpha q, z = M^-1 r, r.r, r.z_old, r.z (DoF-linear unless block Jacobi)
       acc_reset();
       if (a.precond != 2) {
-        constexpr int kAhead = 3;  // prefetch distance in this warp's slices (as in k_pcg)
-        if (a.prefetch)
-          for (int k = 0; k < kAhead && c0 + warp + k * nwarps < c1; ++k)
-            prefetch_update_operands(a, c0 + warp + k * nwarps, lane);
+        const int ahead = a.prefetch;  // prefetch distance in this warp's slices (as in k_pcg)
+        for (int k = 0; k < ahead && c0 + warp + k * nwarps < c1; ++k)
+          prefetch_update_operands(a, c0 + warp + k * nwarps, lane);
         for (int s = c0 + warp; s < c1; s += nwarps) {
-          if (a.prefetch && s + kAhead * nwarps < c1) prefetch_update_operands(a, s + kAhead * nwarps, lane);
+          if (ahead > 0 && s + ahead * nwarps < c1) prefetch_update_operands(a, s + ahead * nwarps, lane);
           const int64_t d0 = (int64_t)s * (3 * kSlice);
-          double xo[3], ro[3];
+          if (replace) {  // only x: the true residual that follows recomputes r and z
+#pragma unroll
+            for (int j = 0; j < 3; ++j) a.x[d0 + lane + 32 * j] += al * (double)a.p[d0 + lane + 32 * j];
+            continue;
+          }
+          // r carried by z (r = z / d) between true-residual replacements with r_in_z; old z as whole
+          // float4 rows through the warp's staging row (as in k_pcg)
+          double xo[3], ro[3] = {0.0, 0.0, 0.0};
           float pp[3], qq[3], dd[3], zo[3];
+          const float4 zrow = a.z[(int64_t)s * kSlice + lane];
 #pragma unroll
           for (int j = 0; j < 3; ++j) {
             const int dl = lane + 32 * j;
             xo[j] = a.x[d0 + dl];
             pp[j] = a.p[d0 + dl];
-            ro[j] = a.r[d0 + dl];
+            if (!a.r_in_z) ro[j] = a.r[d0 + dl];
             qq[j] = a.q[d0 + dl];
-            dd[j] = (!replace && a.precond == 1) ? a.dinv[d0 + dl] : 1.0f;
-            zo[j] = replace ? 0.0f : zw[4 * ((int64_t)s * kSlice + dl / 3) + dl % 3];
+            dd[j] = a.precond == 1 ? a.dinv[d0 + dl] : 1.0f;
           }
-          double r[3];
+          tr[3 * lane] = zrow.x;
+          tr[3 * lane + 1] = zrow.y;
+          tr[3 * lane + 2] = zrow.z;
+          __syncwarp();
 #pragma unroll
-          for (int j = 0; j < 3; ++j) {
-            a.x[d0 + lane + 32 * j] = xo[j] + al * (double)pp[j];
-            r[j] = ro[j] - al * (double)qq[j];
-          }
-          if (replace) continue;
+          for (int j = 0; j < 3; ++j) zo[j] = tr[lane + 32 * j];
+          __syncwarp();
           double rr2 = 0.0, rzo2 = 0.0, rz2 = 0.0;
 #pragma unroll
           for (int j = 0; j < 3; ++j) {
             const int dl = lane + 32 * j;
-            const float z = (float)(dd[j] * r[j]);
-            a.r[d0 + dl] = r[j];
-            zw[4 * ((int64_t)s * kSlice + dl / 3) + dl % 3] = z;
-            rr2 += r[j] * r[j];
-            rzo2 += r[j] * zo[j];
-            rz2 += r[j] * z;
+            a.x[d0 + dl] = xo[j] + al * (double)pp[j];
+            const double rp =
+                !a.r_in_z ? ro[j] : (a.precond == 1 ? (double)zo[j] / (double)dd[j] : (double)zo[j]);
+            const double r = rp - al * (double)qq[j];
+            if (!a.r_in_z) a.r[d0 + dl] = r;
+            const float z = (float)(dd[j] * r);
+            tr[dl] = z;
+            rr2 += r * r;
+            rzo2 += r * zo[j];
+            rz2 += r * z;
           }
+          __syncwarp();
+          a.z[(int64_t)s * kSlice + lane] = make_float4(tr[3 * lane], tr[3 * lane + 1], tr[3 * lane + 2], 0.0f);
+          __syncwarp();
           acc_add(0, rr2);
           acc_add(1, rzo2);
           acc_add(2, rz2);

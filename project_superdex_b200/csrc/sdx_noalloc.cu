@@ -227,7 +227,7 @@ __global__ void k_pcg_noalloc(Args a) {
       if (a.col[k] == row)
         for (int e = 0; e < 9; ++e) blk[e] = block_entry(a, b0, b1, k - b0, e);
     if (a.precond == 1) {
-      for (int k = 0; k < 3; ++k) D[9 * row + k] = blk[4 * k] != 0.0f ? 1.0f / blk[4 * k] : 0.0f;
+      for (int k = 0; k < 3; ++k) D[9 * row + k] = blk[4 * k] != 0.0f ? 1.0f / blk[4 * k] : 1.0f;
     } else if (a.precond == 2) {
       float cf[9];
       cf[0] = blk[4] * blk[8] - blk[5] * blk[7];

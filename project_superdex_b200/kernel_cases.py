@@ -27,12 +27,13 @@ from . import scenes
 from .soft_body import SoftBodyWorld
 
 
-def pcg_bytes_per_iter(nnzb: int, n_rows: int) -> int:
+def pcg_bytes_per_iter(nnzb: int, n_rows: int, r_in_z: bool) -> int:
     """Algorithmic HBM bytes of one fused Jacobi-PCG iteration: the matrix once (36 B values + 4 B column
-    per 3x3 block), the slice pointers, and per row 228 B of vector traffic (phase 1: own z 12 + gathered
-    z 12 + p and q read/write 48; phase 2: FP64 x and r read/write 96, p 12, q 12, Jacobi diagonal 12,
-    z read/write 24)."""
-    return nnzb * 40 + 4 * (n_rows + 1) + 228 * n_rows
+    per 3x3 block), the slice pointers, and per row the vector traffic: 228 B with FP64 r (phase 1: own z
+    12 + gathered z 12 + p and q read/write 48; phase 2: FP64 x and r read/write 96, p 12, q 12, Jacobi
+    diagonal 12, z read/write 24); r carried by z saves r's 48. The library adds up the same figure per
+    env (sdx_profile.pcg_bytes)."""
+    return nnzb * 40 + 4 * (n_rows + 1) + (228 - 48 * r_in_z) * n_rows
 
 
 def element_bytes(n_tets: int, n_nodes: int, nnzb: int) -> int:
@@ -107,7 +108,8 @@ def main(argv=None):
         torch.cuda.profiler.stop()
         prof = w.profile()
         st = w.stats()[0]
-        bpi = pcg_bytes_per_iter(w.nnzb, w.n_nodes)
+        # the library's own count for the mode it ran (all envs run the same fixed iteration count)
+        bpi = prof["pcg_bytes"] / max(1, prof["pcg_iters"])
         us = prof["pcg_ms"] * 1e3 / max(1, prof["pcg_iters"])
         out.update(cg_iters=st["cg_iters"], bytes_per_iter=bpi, us_per_iter=us,
                    algorithmic_tbs=bpi / (us * 1e-6) / 1e12)
