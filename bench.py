@@ -503,7 +503,7 @@ def run_ours(args, rank, world, local_rank):
     value = world * head["env_steps"] / (ms / 1000.0)
 
     # roofline of the dominant kernel (the persistent PCG): algorithmic bytes per env per CG iteration
-    # (40 B per block + 4 B per row pointer + 228 B per row, 180 with r carried by z) x that env's
+    # (40 B per block + 4 B per row pointer + 228 B per row, 156 with r and x carried in FP32) x that env's
     # iterations, summed by the library
     # over the timed launches, over the PCG launches' CUDA-event time
     peak, peak_kind = measured_peaks()

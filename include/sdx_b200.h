@@ -369,8 +369,9 @@ typedef struct {
   double seed_ms;           /* Hessian seeding with the scaled mass matrix */
   int64_t seed_launches;
   double pcg_bytes;         /* algorithmic HBM bytes of the PCG launches: per env, its CG iterations x
-                               (40 B per block + 4 B per row pointer + 228 B per row, 180 B per row when
-                               z carries r between true-residual replacements) */
+                               (40 B per block + 4 B per row pointer + 228 B per row, 156 B per row when
+                               z carries r and an FP32 increment carries x between true-residual
+                               replacements) */
   int64_t pcg_relaunches;   /* re-partitioned PCG relaunches (batches whose slow envs got all CTAs) */
   int64_t pcg_threads;      /* threads per CTA of the PCG launch shape in use (autotuned or default) */
   double warm_ms;           /* learned warm start: features, MLP inference and the start-vector kernel */

@@ -134,6 +134,7 @@ struct PcgWork {
   double* r = nullptr;
   float* p = nullptr;
   float* q = nullptr;
+  float* xi = nullptr;  // FP32 increment of the CG solution between true-residual replacements
   float4* z = nullptr;
   float* dinv = nullptr;
   unsigned* sync = nullptr;
@@ -151,7 +152,7 @@ struct PcgWork {
     arena_bytes = 0;
     hot_b = hot_x = nullptr;
     r = nullptr;
-    p = q = dinv = nullptr;
+    p = q = xi = dinv = nullptr;
     z = nullptr;
     dfree(sync);
     dfree(out_iters);
@@ -705,7 +706,7 @@ static int alloc_work(PcgWork& W, int64_t n_rows, int n_envs, bool newton_vector
   auto al = [](size_t b) { return (b + 255) / 256 * 256; };
   const size_t d3 = al(sizeof(double) * 3 * n_rows), f3 = al(sizeof(float) * 3 * n_rows),
                f4 = al(sizeof(float4) * n_rows), f9 = al(sizeof(float) * 9 * n_rows);
-  W.arena_bytes = d3 * (newton_vectors ? 3 : 1) + 2 * f3 + f4 + f9;
+  W.arena_bytes = d3 * (newton_vectors ? 3 : 1) + 3 * f3 + f4 + f9;
   SDX_TRY(dalloc(&W.arena, W.arena_bytes));
   char* q = W.arena;
   W.r = (double*)q;
@@ -719,6 +720,8 @@ static int alloc_work(PcgWork& W, int64_t n_rows, int n_envs, bool newton_vector
   W.p = (float*)q;
   q += f3;
   W.q = (float*)q;
+  q += f3;
+  W.xi = (float*)q;
   q += f3;
   W.z = (float4*)q;
   q += f4;
@@ -769,6 +772,7 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
   a.q = W.q;
   a.z = W.z;
   a.dinv = W.dinv;
+  a.xi = W.xi;
   a.env_mask = env_mask;
   a.rel_tol = lp.rel_tol;
   a.abs_tol = lp.abs_tol;
@@ -844,8 +848,9 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
       c->prof.pcg_iters += *std::max_element(its.begin(), its.end());
       c->prof.pcg_launches++;
       if (A.val == c->val && (int)c->h_env_pcg_bytes.size() == n_envs) {
-        // vector bytes per row: 228 with FP64 r; r carried by z saves its FP64 read and write (48)
-        const double per_row = 228.0 - (a.r_in_z && a.precond != 2 ? 48.0 : 0.0);
+        // vector bytes per row: 228 with FP64 r and x; r carried by z saves its FP64 read and write (48),
+        // x carried by its FP32 increment half of x's (24)
+        const double per_row = 228.0 - (a.r_in_z && a.precond != 2 ? 72.0 : 0.0);
         for (int e = 0; e < n_envs; ++e)
           c->prof.pcg_bytes += its[e] * (c->h_env_pcg_bytes[e] +
                                          per_row * (double)(c->h_node_off[e + 1] - c->h_node_off[e]));

@@ -162,7 +162,9 @@ struct PcgArgs {
                    // [4] verify_iter, [5] active rows, [6] resume iteration, [7] repartition exit
   long long spin_limit;
   int r_in_z;    // Jacobi / no preconditioner: r is carried by z between true-residual replacements
-                 // (r = z / d, FP32 precision), so the update phase reads and writes no FP64 r
+                 // (r = z / d, FP32 precision) and x by its FP64 value at the last replacement plus the FP32
+                 // increment xi, so the update phase reads and writes no FP64 vector
+  float* xi;     // FP32 increment of x since the last true-residual replacement (r_in_z)
   int prefetch;  // bulk L2 prefetch of each warp's next slices (0: none): the update phase's distance in
                  // slices (the matrix of the next slice in the SpMV phase whenever it is set); set when the
                  // CG vectors cannot stay in L2, so every operand comes from HBM

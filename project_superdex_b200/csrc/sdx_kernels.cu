@@ -975,16 +975,33 @@ __device__ __forceinline__ void prefetch_l2(const void* ptr, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(ptr), "r"(bytes) : "memory");
 }
 
-// Phase-2 operands of slice s (DoF-linear: x FP64, p, q, Jacobi diagonal FP32, z float4 rows; r FP64 unless z
-// carries it), one array per lane 0..5.
+// Phase-2 operands of slice s (DoF-linear: p, q, Jacobi diagonal FP32, z float4 rows; x and r FP64, or the
+// FP32 increment of x when z carries r), one array per lane 0..5.
 __device__ __forceinline__ void prefetch_update_operands(const PcgArgs& a, int s, int lane) {
   const int64_t d0 = (int64_t)s * (3 * kSlice);
-  if (lane == 0) prefetch_l2(a.x + d0, 3 * kSlice * 8);
+  if (lane == 0) {
+    if (a.r_in_z)
+      prefetch_l2(a.xi + d0, 3 * kSlice * 4);
+    else
+      prefetch_l2(a.x + d0, 3 * kSlice * 8);
+  }
   if (lane == 1 && !a.r_in_z) prefetch_l2(a.r + d0, 3 * kSlice * 8);
   if (lane == 2) prefetch_l2(a.p + d0, 3 * kSlice * 4);
   if (lane == 3) prefetch_l2(a.q + d0, 3 * kSlice * 4);
   if (lane == 4 && a.precond == 1) prefetch_l2(a.dinv + d0, 3 * kSlice * 4);
   if (lane == 5) prefetch_l2(a.z + (int64_t)s * kSlice, kSlice * 16);
+}
+
+// x += xi, xi = 0 on slice s (DoF-linear): folds the FP32 increment of x accumulated since the last
+// true-residual replacement into the FP64 x.
+__device__ __forceinline__ void fold_x_increment(const PcgArgs& a, int s, int lane) {
+  const int64_t d0 = (int64_t)s * (3 * kSlice);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    const int64_t d = d0 + lane + 32 * j;
+    a.x[d] += (double)a.xi[d];
+    a.xi[d] = 0.0f;
+  }
 }
 
 // Matrix range of slice s (column indices and the 9 values of every block position), lanes 6 and 7.
@@ -1335,7 +1352,10 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
       float z[3];
       prec_apply(a, row, r, z);
   #pragma unroll
-      for (int k = 0; k < 3; ++k) a.r[3 * row + k] = r[k];
+      for (int k = 0; k < 3; ++k) {
+        a.r[3 * row + k] = r[k];
+        if (a.r_in_z) a.xi[3 * row + k] = 0.0f;
+      }
       a.z[row] = make_float4(z[0], z[1], z[2], 0.0f);
       const double b0 = a.b[3 * row], b1 = a.b[3 * row + 1], b2 = a.b[3 * row + 2];
       add_acc(le, 0, b0 * b0 + b1 * b1 + b2 * b2);
@@ -1386,6 +1406,16 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     if constexpr (kTimed) {
       if (threadIdx.x == 0)
         for (int k = 0; k < 4; ++k) atomicAdd(a.cta_ns + 4 * c + k, t_ph[k]);
+    }
+  };
+  // At a launch's exit every env of this CTA's slices that took part gets its x increment folded in (an
+  // env that stopped between replacements, or every env before a re-partition relaunch).
+  auto fold_all = [&]() {
+    if (!a.r_in_z || a.precond == 2) return;
+    for (int i = s0 + warp; i < s1; i += nwarps) {
+      const int s = slice_of(i);
+      if (st[local_env(a.A.slice_env[s])].status == 4) continue;
+      fold_x_increment(a, s, lane);
     }
   };
   mark(-1);
@@ -1456,6 +1486,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
     }
     reduce_tot(1, 1);
     if (s_exit) {
+      fold_all();
       mark_out();
       break;
     }
@@ -1486,15 +1517,22 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
         if (st[le].status != 0) continue;
         const int64_t d0 = (int64_t)s * (3 * kSlice);
         const double al = st[le].alpha;
-        if (replace) {  // only x: the true residual that follows recomputes r and z
+        if (replace) {  // only x (and its folded increment): the true residual that follows recomputes r, z
 #pragma unroll
-          for (int j = 0; j < 3; ++j) a.x[d0 + lane + 32 * j] += al * (double)a.p[d0 + lane + 32 * j];
+          for (int j = 0; j < 3; ++j) {
+            const int64_t d = d0 + lane + 32 * j;
+            const double inc = a.r_in_z ? (double)a.xi[d] : 0.0;
+            a.x[d] += inc + al * (double)a.p[d];
+            if (a.r_in_z) a.xi[d] = 0.0f;
+          }
           continue;
         }
         // With r_in_z, r is carried by z between true-residual replacements: r = z / d (FP32 precision;
-        // d = 1 without a preconditioner), so the update reads and writes no FP64 r. Every operand load is
-        // issued before the first store (the update is latency bound).
-        double xo[3], ro[3] = {0.0, 0.0, 0.0};
+        // d = 1 without a preconditioner), and x by its FP64 value at the last replacement plus the FP32
+        // increment xi, so the update reads and writes no FP64 vector. Every operand load is issued before
+        // the first store (the update is latency bound).
+        double xo[3] = {0.0, 0.0, 0.0}, ro[3] = {0.0, 0.0, 0.0};
+        float xio[3] = {0.0f, 0.0f, 0.0f};
         float pp[3], qq[3], dd[3], zo[3];
         // the old z arrives as whole float4 rows (one per lane) and reaches the DoF layout through the
         // warp's staging row
@@ -1502,9 +1540,13 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
           const int dl = lane + 32 * j;
-          xo[j] = a.x[d0 + dl];
+          if (a.r_in_z) {
+            xio[j] = a.xi[d0 + dl];
+          } else {
+            xo[j] = a.x[d0 + dl];
+            ro[j] = a.r[d0 + dl];
+          }
           pp[j] = a.p[d0 + dl];
-          if (!a.r_in_z) ro[j] = a.r[d0 + dl];
           qq[j] = a.q[d0 + dl];
           dd[j] = a.precond == 1 ? a.dinv[d0 + dl] : 1.0f;
         }
@@ -1519,7 +1561,10 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
           const int dl = lane + 32 * j;
-          a.x[d0 + dl] = xo[j] + al * (double)pp[j];
+          if (a.r_in_z)
+            a.xi[d0 + dl] = (float)((double)xio[j] + al * (double)pp[j]);
+          else
+            a.x[d0 + dl] = xo[j] + al * (double)pp[j];
           const double rp =
               !a.r_in_z ? ro[j] : (a.precond == 1 ? (double)zo[j] / (double)dd[j] : (double)zo[j]);
           const double r = rp - al * (double)qq[j];
@@ -1659,6 +1704,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
         a.sync[6] = (unsigned)(it + 1);
         a.sync[7] = 1u;
       }
+      fold_all();
       mark_out();
       return;
     }
@@ -1945,7 +1991,10 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
       float z[3];
       prec_apply(a, row, r, z);
 #pragma unroll
-      for (int k = 0; k < 3; ++k) a.r[3 * row + k] = r[k];
+      for (int k = 0; k < 3; ++k) {
+        a.r[3 * row + k] = r[k];
+        if (a.r_in_z) a.xi[3 * row + k] = 0.0f;
+      }
       a.z[row] = make_float4(z[0], z[1], z[2], 0.0f);
       const double b0 = a.b[3 * row], b1 = a.b[3 * row + 1], b2 = a.b[3 * row + 2];
       acc_add(0, b0 * b0 + b1 * b1 + b2 * b2);
@@ -2025,22 +2074,32 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
         for (int s = c0 + warp; s < c1; s += nwarps) {
           if (ahead > 0 && s + ahead * nwarps < c1) prefetch_update_operands(a, s + ahead * nwarps, lane);
           const int64_t d0 = (int64_t)s * (3 * kSlice);
-          if (replace) {  // only x: the true residual that follows recomputes r and z
+          if (replace) {  // only x (and its folded increment): the true residual that follows recomputes r, z
 #pragma unroll
-            for (int j = 0; j < 3; ++j) a.x[d0 + lane + 32 * j] += al * (double)a.p[d0 + lane + 32 * j];
+            for (int j = 0; j < 3; ++j) {
+              const int64_t d = d0 + lane + 32 * j;
+              const double inc = a.r_in_z ? (double)a.xi[d] : 0.0;
+              a.x[d] += inc + al * (double)a.p[d];
+              if (a.r_in_z) a.xi[d] = 0.0f;
+            }
             continue;
           }
-          // r carried by z (r = z / d) between true-residual replacements with r_in_z; old z as whole
-          // float4 rows through the warp's staging row (as in k_pcg)
-          double xo[3], ro[3] = {0.0, 0.0, 0.0};
+          // r carried by z (r = z / d) and x by its FP32 increment between true-residual replacements with
+          // r_in_z; old z as whole float4 rows through the warp's staging row (as in k_pcg)
+          double xo[3] = {0.0, 0.0, 0.0}, ro[3] = {0.0, 0.0, 0.0};
+          float xio[3] = {0.0f, 0.0f, 0.0f};
           float pp[3], qq[3], dd[3], zo[3];
           const float4 zrow = a.z[(int64_t)s * kSlice + lane];
 #pragma unroll
           for (int j = 0; j < 3; ++j) {
             const int dl = lane + 32 * j;
-            xo[j] = a.x[d0 + dl];
+            if (a.r_in_z) {
+              xio[j] = a.xi[d0 + dl];
+            } else {
+              xo[j] = a.x[d0 + dl];
+              ro[j] = a.r[d0 + dl];
+            }
             pp[j] = a.p[d0 + dl];
-            if (!a.r_in_z) ro[j] = a.r[d0 + dl];
             qq[j] = a.q[d0 + dl];
             dd[j] = a.precond == 1 ? a.dinv[d0 + dl] : 1.0f;
           }
@@ -2055,7 +2114,10 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
 #pragma unroll
           for (int j = 0; j < 3; ++j) {
             const int dl = lane + 32 * j;
-            a.x[d0 + dl] = xo[j] + al * (double)pp[j];
+            if (a.r_in_z)
+              a.xi[d0 + dl] = (float)((double)xio[j] + al * (double)pp[j]);
+            else
+              a.x[d0 + dl] = xo[j] + al * (double)pp[j];
             const double rp =
                 !a.r_in_z ? ro[j] : (a.precond == 1 ? (double)zo[j] / (double)dd[j] : (double)zo[j]);
             const double r = rp - al * (double)qq[j];
@@ -2156,6 +2218,9 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
       first = false;
     }
     if (fail) break;
+    // this CTA's rows of the env: the x increment since the last replacement into x
+    if (a.r_in_z && a.precond != 2)
+      for (int s = c0 + warp; s < c1; s += nwarps) fold_x_increment(a, s, lane);
     if (rank == 0 && threadIdx.x == 0) {
       a.out_iters[e] = it_done;
       a.out_res[e] = sqrt(fmax(rr, 0.0));

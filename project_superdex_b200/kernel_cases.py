@@ -31,9 +31,9 @@ def pcg_bytes_per_iter(nnzb: int, n_rows: int, r_in_z: bool) -> int:
     """Algorithmic HBM bytes of one fused Jacobi-PCG iteration: the matrix once (36 B values + 4 B column
     per 3x3 block), the slice pointers, and per row the vector traffic: 228 B with FP64 r (phase 1: own z
     12 + gathered z 12 + p and q read/write 48; phase 2: FP64 x and r read/write 96, p 12, q 12, Jacobi
-    diagonal 12, z read/write 24); r carried by z saves r's 48. The library adds up the same figure per
-    env (sdx_profile.pcg_bytes)."""
-    return nnzb * 40 + 4 * (n_rows + 1) + (228 - 48 * r_in_z) * n_rows
+    diagonal 12, z read/write 24); r carried by z and x by its FP32 increment save 48 + 24. The library
+    adds up the same figure per env (sdx_profile.pcg_bytes)."""
+    return nnzb * 40 + 4 * (n_rows + 1) + (228 - 72 * r_in_z) * n_rows
 
 
 def element_bytes(n_tets: int, n_nodes: int, nnzb: int) -> int:
