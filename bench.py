@@ -24,6 +24,9 @@ after the W warm-up steps):
               The per-vertex MLP is trained first, on the GPU, on the learned part's own protocol: (state,
               RHS, solution) triples of the plain solver on 50 held-out seeded episodes of 16 bodies of the
               same distribution (seeds 1000..1049, run as one batch of 800 bodies, 2 steps), Adam lr 1e-3.
+  <arm>_refined  any of the above with mixed-precision iterative refinement: PCG passes to relative 1e-2 of
+              each pass's right-hand side, corrected against the FP64 residual until rel 1e-6 (the default
+              arms of the stiff cfg4 case: plain_fp64, fused_zero, learned_refined).
 The headline arm is timed on K steps through the public API (sdx_set_state / sdx_step / sdx_get_state with
 pinned host buffers): `value` is the device time of the steps (CUDA events on the library stream around
 each sdx_step), `e2e` the whole loop with the host<->device copies, on the same steps. The comparison arms
@@ -52,6 +55,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
+# profile entries that describe launch shapes (kept, not summed, when runs are merged)
+SHAPE_KEYS = ("pcg_threads", "pcg_cluster_size", "tune_grid_us", "tune_cluster_us", "elem_threads",
+              "elem_res_threads", "elem_aggregated", "contact_threads", "tune_elem_us", "tune_elem_default_us")
 METRIC = "env-steps/sec at rel-res 1e-6: learned warm-start vs plain PCG; SpMV HBM GB/s"
 UNIT = "env-steps/s"
 TRAIN_SEED0 = 1000  # training episodes use seeds TRAIN_SEED0.. (never an evaluated seed)
@@ -373,13 +379,19 @@ def max_over_ranks(x, dist, local_rank):
     return float(t.item())
 
 
+# inner relative tolerance of the arms with mixed-precision iterative refinement ("<start>_refined")
+REFINE_INNER_REL_TOL = 1e-2
+
+
 def set_arm(w, arm, params):
     from project_superdex_b200 import capi
     from project_superdex_b200.learned import Mlp
+    refined = arm.endswith("_refined")
+    arm = arm[:-len("_refined")] if refined else arm
     if arm == "learned":
         Mlp(w._ctx).set_params(params)
     w.set_params(warm_start={"learned": capi.SDX_WARM_LEARNED, "temporal": capi.SDX_WARM_TEMPORAL}.get(
-        arm, capi.SDX_WARM_ZERO))
+        arm, capi.SDX_WARM_ZERO), linear_refine_inner_rel_tol=REFINE_INNER_REL_TOL if refined else 0.0)
     if getattr(w, "_plain", None) is not None:
         w._plain.close()
         w._plain = None
@@ -427,8 +439,7 @@ def merge(a, b):
     out["step_ms"] = a["step_ms"] + b["step_ms"]
     for k in ("newton_per_env_step", "cg_per_env_step"):
         out[k] = (a[k] * a["env_steps"] + b[k] * b["env_steps"]) / out["env_steps"]
-    out["prof"] = {k: (a["prof"].get(k, 0) + v if k not in ("pcg_threads", "pcg_cluster_size", "tune_grid_us", "tune_cluster_us") else v)
-                   for k, v in b["prof"].items()}
+    out["prof"] = {k: (a["prof"].get(k, 0) + v if k not in SHAPE_KEYS else v) for k, v in b["prof"].items()}
     if "clocks" in a:
         ca, cb = a["clocks"], b["clocks"]
         sm = [x for x in (ca.get("sm_mhz"), cb.get("sm_mhz")) if x is not None]
@@ -441,8 +452,9 @@ def merge(a, b):
 
 
 def run_ours(args, rank, world, local_rank):
-    # the PCG launch shape is picked by the library's autotuner on the world's first Newton solve
-    os.environ.setdefault("SDX_PCG_AUTOTUNE", "1")
+    # the PCG and assembly launch shapes are picked by the library's autotuners on the world's first Newton
+    # pass
+    os.environ.setdefault("SDX_AUTOTUNE", "1")
     import torch
     from project_superdex_b200.replicas import replica_seed
     from project_superdex_b200.soft_body import SoftBodyWorld
@@ -453,7 +465,7 @@ def run_ours(args, rank, world, local_rank):
     arms = [a for a in args.arms.split(",") if a]
     head_arm = arms[-1]
     params, train_info = (None, None)
-    if "learned" in arms:
+    if any(a.startswith("learned") for a in arms):
         params, train_info = train_warm_start(args, local_rank)
     seed0 = replica_seed(args.seed, rank)
     seeds = [seed0 + i for i in range(args.eval_episodes)] if args.workload == "cfg3" else [seed0]
@@ -558,7 +570,13 @@ def run_ours(args, rank, world, local_rank):
                 "seeds": f"{seeds[0]}..{seeds[-1]}", "nnzb": w.nnzb,
                 "pcg_threads_autotuned": int(prof.get("pcg_threads", 0)),
                 "pcg_cluster_size_autotuned": int(prof.get("pcg_cluster_size", 0)),
-                "autotune_us": {"grid": prof.get("tune_grid_us", 0.0), "cluster": prof.get("tune_cluster_us", 0.0)}},
+                "autotune_us": {"grid": prof.get("tune_grid_us", 0.0), "cluster": prof.get("tune_cluster_us", 0.0),
+                                "element_hessian": prof.get("tune_elem_us", 0.0),
+                                "element_hessian_default_shape": prof.get("tune_elem_default_us", 0.0)},
+                "assembly_shapes_autotuned": {"element_threads": int(prof.get("elem_threads", 0)),
+                                              "element_aggregated_scatter": bool(prof.get("elem_aggregated", 0)),
+                                              "element_residual_threads": int(prof.get("elem_res_threads", 0)),
+                                              "contact_threads": int(prof.get("contact_threads", 0))}},
         "converged": {"env_steps": head["converged_env_steps"], "of": head["env_steps"],
                       "frac": head["converged_env_steps"] / head["env_steps"],
                       "note": ("value counts every env-step; an env-step that hit the Newton cap before rel 1e-6 "
@@ -608,7 +626,12 @@ def main():
     args = ap.parse_args()
     batched = args.workload in ("cfg2", "cfg3")
     if args.arms is None:
-        args.arms = "fused_zero,temporal,learned" if batched else "plain_fp64,fused_zero,temporal,learned"
+        if batched:
+            args.arms = "fused_zero,temporal,learned"
+        elif args.workload == "cfg4":  # the stiff case compares the refined learned-start solver with plain FP64
+            args.arms = "plain_fp64,fused_zero,learned_refined"
+        else:
+            args.arms = "plain_fp64,fused_zero,temporal,learned"
     if args.train_episodes is None:
         args.train_episodes = 50 if batched else 2
     if args.train_steps is None:

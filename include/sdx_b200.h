@@ -98,6 +98,13 @@ typedef struct {
   int replace_every;    /* FP64 true-residual replacement period in iterations (0: default 32) */
   int value_layout;     /* SDX_BSR_* of the values passed to the sdx_pcg_solve* entry points
                            (default SDX_BSR_ROW_STRIPS, the reference's layout) */
+  /* Mixed-precision iterative refinement (no counterpart in the reference; 0 = off): when > 0, the solve
+   * runs as passes of the PCG to this relative tolerance of each pass's right-hand side. Pass 0 solves
+   * A x = b from the initial guess (warm starts included); each later pass computes r = b - A x in FP64,
+   * stops the env when ||r|| meets rel_tol / abs_tol, else solves A d = r from zero and adds d to x. The
+   * iteration count is the sum over the passes; max_iter bounds each pass. */
+  double refine_inner_rel_tol;
+  int refine_max_passes;  /* passes after pass 0 (default 8); an env still above tolerance then stops */
 } sdx_linear_params;
 
 /* Coulomb friction smoothing (CoulombFrictionModel, contact_params.h:307-327) */
@@ -382,6 +389,12 @@ typedef struct {
                                  -1: the grid kernel won, long queues stay on it) */
   double tune_grid_us;        /* autotuner: best grid-kernel time of its 24-iteration solve (0: not tuned) */
   double tune_cluster_us;     /* autotuner: best cluster-kernel time of the same solve (0: none timed) */
+  int64_t elem_threads;       /* element kernel CTA size of Hessian assemblies (autotuned or 128) */
+  int64_t elem_res_threads;   /* element kernel CTA size of residual-only assemblies */
+  int64_t elem_aggregated;    /* 1: Hessian blocks are warp-aggregated before their reductions */
+  int64_t contact_threads;    /* contact kernel CTA size */
+  double tune_elem_us;        /* assembly tuner: fastest Hessian element launch (0: not tuned) */
+  double tune_elem_default_us;/* the same launch with the default shape (128 threads, plain scatter) */
 } sdx_profile;
 /* enable: 0 off, 1 per-kernel event timing, 2 also the per-CTA PCG phase timers (sdx_get_pcg_cta_profile) */
 int sdx_set_profiling(sdx_context* ctx, int enable);

@@ -47,7 +47,8 @@ class LinearParams(C.Structure):
 
     _fields_ = [("rel_tol", C.c_double), ("abs_tol", C.c_double), ("rel_div_tol", C.c_double),
                 ("max_iter", C.c_int), ("preconditioner", C.c_int), ("abort_if_not_spd", C.c_int),
-                ("polak_ribiere", C.c_int), ("replace_every", C.c_int), ("value_layout", C.c_int)]
+                ("polak_ribiere", C.c_int), ("replace_every", C.c_int), ("value_layout", C.c_int),
+                ("refine_inner_rel_tol", C.c_double), ("refine_max_passes", C.c_int)]
 
 
 class LinearStatus(C.Structure):
@@ -101,7 +102,9 @@ class Profile(C.Structure):
                 ("seed_ms", C.c_double), ("seed_launches", C.c_int64), ("pcg_bytes", C.c_double),
                 ("pcg_relaunches", C.c_int64), ("pcg_threads", C.c_int64), ("warm_ms", C.c_double),
                 ("warm_launches", C.c_int64), ("pcg_cluster_solves", C.c_int64), ("pcg_cluster_size", C.c_int64),
-                ("tune_grid_us", C.c_double), ("tune_cluster_us", C.c_double)]
+                ("tune_grid_us", C.c_double), ("tune_cluster_us", C.c_double),
+                ("elem_threads", C.c_int64), ("elem_res_threads", C.c_int64), ("elem_aggregated", C.c_int64),
+                ("contact_threads", C.c_int64), ("tune_elem_us", C.c_double), ("tune_elem_default_us", C.c_double)]
 
 
 _dp = C.POINTER(C.c_double)

@@ -146,8 +146,17 @@ struct PcgWork {
   EnvSave* es = nullptr;  // per env CG scalars across re-partitioning relaunches
   int n_envs_alloc = 0;
   double* gal = nullptr;  // A x2 of the Galerkin start (allocated on first use)
+  // iterative refinement (allocated on first use): FP64 residual, correction, per-env norms, pass mask
+  double* ir_r = nullptr;
+  double* ir_d = nullptr;
+  double* ir_norm = nullptr;
+  uint8_t* ir_mask = nullptr;
   void release() {
     dfree(gal);
+    dfree(ir_r);
+    dfree(ir_d);
+    dfree(ir_norm);
+    dfree(ir_mask);
     dfree(arena);
     arena_bytes = 0;
     hot_b = hot_x = nullptr;
@@ -273,6 +282,11 @@ struct sdx_context {
   int cl_size = 0;             // cluster PCG size picked by the autotuner (0: by occupancy; -1: long queues
                                // stay on the grid kernel)
   double tune_grid_us = 0.0, tune_cluster_us = 0.0;  // the autotuner's best grid / cluster solve times
+  // assembly launch shapes (autotune_assembly): element CTA size for Hessian and residual-only launches,
+  // warp-aggregated block scatter on or off, contact CTA size
+  bool asm_tuned = false;
+  int elem_threads = 128, elem_res_threads = 128, elem_agg = 0, contact_threads = 128;
+  double tune_elem_us = 0.0, tune_elem_default_us = 0.0;  // best and default-shape Hessian assembly times
   int* env_nrows = nullptr;    // padded rows per env (device)
   int* env_soff = nullptr;     // per env, its first slice (device, n_envs + 1): the cluster PCG's env ranges
   int* cl_envs = nullptr;      // the cluster PCG's env queue (device, n_envs)
@@ -968,6 +982,106 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
   return finish();
 }
 
+// Per-env squared norms of v over the slices of A for the envs in mask (device), to the host.
+static int env_sq_norms(sdx_context* c, const Matrix& A, int n_envs, const uint8_t* mask, const double* v,
+                        double* d_out, std::vector<double>& h_out) {
+  SDX_CUDA(cudaMemsetAsync(d_out, 0, sizeof(double) * n_envs, c->stream));
+  launch_env_dot(A.n_slices, A.slice_env, mask, v, v, d_out, c->stream);
+  c->launches++;
+  h_out.resize(n_envs);
+  SDX_CUDA(cudaMemcpyAsync(h_out.data(), d_out, sizeof(double) * n_envs, cudaMemcpyDeviceToHost, c->stream));
+  SDX_CUDA(cudaStreamSynchronize(c->stream));
+  return SDX_OK;
+}
+
+// Mixed-precision iterative refinement around the PCG (lp.refine_inner_rel_tol > 0). Pass 0 is the ordinary
+// solve of A x = b from the caller's start (zero, a guess, or the learned two-vector start) to the inner
+// tolerance. Each later pass forms r = b - A x in FP64 for the envs still open, closes those whose ||r||
+// meets max(abs_tol, rel_tol ||b||) (rel_tol per env under Eisenstat-Walker forcing; or whose residual
+// diverged), solves A d = r from zero to the inner
+// tolerance and adds d to x. W's per-env outputs are set as a single solve's: iterations summed over the
+// passes, the last FP64 residual, the status of the outer test (1 converged, 2 stopped at the pass cap,
+// 3 diverged; an inner solve that diverged or stopped on a non-SPD direction closes the env with its status).
+static int run_pcg_refined(sdx_context* c, const Matrix& A, const int* diag_pos, int n_envs, PcgPartition& P,
+                           PcgWork& W, const double* b, double* x, const uint8_t* env_mask, int n_active,
+                           const sdx_linear_params& lp, bool zero_guess, bool scale_guess,
+                           const uint8_t* h_mask, const double* x2, const double* h_env_rel_tol = nullptr) {
+  const int64_t n3 = 3 * (int64_t)A.n_slices * kSlice;
+  if (!W.ir_r) {
+    SDX_TRY(dalloc(&W.ir_r, (size_t)n3));
+    SDX_TRY(dalloc(&W.ir_d, (size_t)n3));
+    SDX_TRY(dalloc(&W.ir_norm, n_envs));
+    SDX_TRY(dalloc(&W.ir_mask, n_envs));
+  }
+  sdx_linear_params inner = lp;
+  inner.rel_tol = lp.refine_inner_rel_tol;
+  inner.abs_tol = 0.0;
+  inner.refine_inner_rel_tol = 0.0;
+  std::vector<uint8_t> open(n_envs, 0);
+  for (int e = 0; e < n_envs; ++e) open[e] = (!h_mask || h_mask[e]) ? 1 : 0;
+  std::vector<double> bb, rr;
+  SDX_TRY(env_sq_norms(c, A, n_envs, env_mask, b, W.ir_norm, bb));
+  std::vector<int> iters(n_envs, 0), conv(n_envs, 0), it_pass(n_envs, 0), conv_pass(n_envs, 0);
+  std::vector<double> res(n_envs, 0.0);
+  auto read_pass = [&]() -> int {
+    SDX_CUDA(cudaMemcpyAsync(it_pass.data(), W.out_iters, sizeof(int) * n_envs, cudaMemcpyDeviceToHost, c->stream));
+    SDX_CUDA(cudaMemcpyAsync(conv_pass.data(), W.out_conv, sizeof(int) * n_envs, cudaMemcpyDeviceToHost, c->stream));
+    SDX_CUDA(cudaStreamSynchronize(c->stream));
+    for (int e = 0; e < n_envs; ++e)
+      if (open[e]) {
+        iters[e] += it_pass[e];
+        if (conv_pass[e] == 3) {  // the inner solve diverged (or met a non-SPD direction): the env stops
+          conv[e] = 3;
+          open[e] = 0;
+        }
+      }
+    return SDX_OK;
+  };
+  SDX_TRY(run_pcg(c, A, diag_pos, n_envs, P, W, b, x, env_mask, n_active, inner, zero_guess, nullptr, scale_guess,
+                  h_mask, x2));
+  SDX_TRY(read_pass());
+  for (int pass = 1;; ++pass) {
+    SDX_CUDA(cudaMemcpyAsync(W.ir_mask, open.data(), n_envs, cudaMemcpyHostToDevice, c->stream));
+    launch_residual64(A, W.ir_mask, x, b, W.ir_r, c->stream);
+    c->launches++;
+    SDX_TRY(env_sq_norms(c, A, n_envs, W.ir_mask, W.ir_r, W.ir_norm, rr));
+    int left = 0;
+    for (int e = 0; e < n_envs; ++e) {
+      if (!open[e]) continue;
+      const double rn = std::sqrt(std::max(rr[e], 0.0)), bn = std::sqrt(std::max(bb[e], 0.0));
+      res[e] = rn;
+      if (!std::isfinite(rn) || rn > lp.rel_div_tol * bn) {
+        conv[e] = 3;
+        open[e] = 0;
+      } else if (rn <= std::max(lp.abs_tol, (h_env_rel_tol ? h_env_rel_tol[e] : lp.rel_tol) * bn)) {
+        conv[e] = 1;
+        open[e] = 0;
+      } else if (pass > lp.refine_max_passes) {
+        conv[e] = 2;
+        open[e] = 0;
+      } else {
+        left++;
+      }
+    }
+    if (left == 0) break;
+    SDX_CUDA(cudaMemcpyAsync(W.ir_mask, open.data(), n_envs, cudaMemcpyHostToDevice, c->stream));
+    SDX_TRY(run_pcg(c, A, diag_pos, n_envs, P, W, W.ir_r, W.ir_d, W.ir_mask, left, inner, /*zero_guess*/ true,
+                    nullptr, false, open.data(), nullptr));
+    launch_add_rows(A.n_slices, A.slice_env, W.ir_mask, W.ir_d, x, c->stream);
+    c->launches++;
+    SDX_TRY(read_pass());
+  }
+  // the outputs of one solve over all passes
+  std::vector<double> rel(n_envs, 0.0);
+  for (int e = 0; e < n_envs; ++e) rel[e] = bb[e] > 0.0 ? res[e] / std::sqrt(bb[e]) : 0.0;
+  SDX_CUDA(cudaMemcpyAsync(W.out_iters, iters.data(), sizeof(int) * n_envs, cudaMemcpyHostToDevice, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(W.out_conv, conv.data(), sizeof(int) * n_envs, cudaMemcpyHostToDevice, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(W.out_res, res.data(), sizeof(double) * n_envs, cudaMemcpyHostToDevice, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(W.out_relres, rel.data(), sizeof(double) * n_envs, cudaMemcpyHostToDevice, c->stream));
+  SDX_CUDA(cudaStreamSynchronize(c->stream));  // the host vectors above are copied before they go away
+  return SDX_OK;
+}
+
 // ------------------------------------------------------------------------------------------------
 // C-ABI: misc
 
@@ -984,6 +1098,8 @@ extern "C" void sdx_default_linear_params(sdx_linear_params* p) {
   p->polak_ribiere = 1;
   p->replace_every = 32;
   p->value_layout = SDX_BSR_ROW_STRIPS;
+  p->refine_inner_rel_tol = 0.0;
+  p->refine_max_passes = 8;
 }
 
 extern "C" void sdx_default_step_params(sdx_step_params* p) {
@@ -1120,6 +1236,12 @@ extern "C" int sdx_get_profile(sdx_context* c, sdx_profile* out) {
   out->pcg_cluster_size = c->cl_size;
   out->tune_grid_us = c->tune_grid_us;
   out->tune_cluster_us = c->tune_cluster_us;
+  out->elem_threads = c->elem_threads;
+  out->elem_res_threads = c->elem_res_threads;
+  out->elem_aggregated = c->elem_agg;
+  out->contact_threads = c->contact_threads;
+  out->tune_elem_us = c->tune_elem_us;
+  out->tune_elem_default_us = c->tune_elem_default_us;
   return SDX_OK;
 }
 
@@ -1131,6 +1253,9 @@ extern "C" int sdx_set_params(sdx_context* c, const sdx_step_params* p) {
     return set_error(SDX_ERR_INVALID_ARGUMENT, "stiffness_damping must be >= 0");
   if (p->linear.preconditioner < 0 || p->linear.preconditioner > 2)
     return set_error(SDX_ERR_INVALID_ARGUMENT, "unknown preconditioner %d", p->linear.preconditioner);
+  if (!(p->linear.refine_inner_rel_tol >= 0.0 && p->linear.refine_inner_rel_tol < 1.0) ||
+      p->linear.refine_max_passes < 0)
+    return set_error(SDX_ERR_INVALID_ARGUMENT, "refinement needs 0 <= inner tolerance < 1 and passes >= 0");
   // contact dissipation (the reference asserts the same ranges, contact_utils.h:635-640, 1040-1048)
   if (!(p->friction_coulomb >= 0.0) || !(p->friction_viscous >= 0.0) || !(p->contact_normal_damping >= 0.0))
     return set_error(SDX_ERR_INVALID_ARGUMENT, "friction and damping coefficients must be >= 0");
@@ -1490,6 +1615,7 @@ extern "C" int sdx_upload_bodies(sdx_context* c, int n_envs, const int64_t* node
   SDX_TRY(choose_partition(c, c->n_slices, c->h_slice_env, n_envs, c->h_slice_ptr, c->part, 0, 0));
   c->pcg_threads = c->part.threads;
   c->pcg_tuned = false;
+  c->asm_tuned = false;
   SDX_TRY(alloc_work(c->work, c->n_rows, n_envs, /*newton_vectors*/ true));
   c->g = c->work.hot_b;
   c->dx = c->work.hot_x;
@@ -1942,24 +2068,15 @@ static Matrix ctx_matrix(sdx_context* c) {
   return A;
 }
 
-// Assembles into c->g / c->val / c->env_obj for the envs in mask (device array, NULL = all).
-static void assemble_dev(sdx_context* c, const double* u, const double* ut, double t, int flags,
-                         const uint8_t* mask, bool record_pairs) {
+// Shape overrides of the assembly kernels (tests and experiments): SDX_ELEM_THREADS, SDX_ELEM_RES_THREADS,
+// SDX_CONTACT_THREADS (64, 128 or 256) and SDX_ELEM_AGG (0/1) replace the tuned or default choice.
+static int shape_override(const char* name, int v) {
+  const char* e = getenv(name);
+  return e ? atoi(e) : v;
+}
+
+static ElemArgs elem_args(sdx_context* c, const double* u, const double* ut, int flags, const uint8_t* mask) {
   const sdx_step_params& p = c->params;
-  const double dtfi2 = 1.0 / (p.dt * p.dt);
-  if (flags & SDX_ASM_RES) {
-    launch_zero_rows(c->n_slices, c->slice_env, mask, c->g, c->stream);
-    c->launches++;
-  }
-  cudaEvent_t ev;
-  if (flags & SDX_ASM_HESS) {
-    prof_begin(c, &ev);
-    // massScale = 1/dt^2 + alpha/dt (ComputeSoftDampingScales, mochi_physics/src/mochi_soft.h:274-290)
-    const double mdamp = p.mass_damping > 0.0 ? p.mass_damping / p.dt : 0.0;
-    launch_seed_hessian(ctx_matrix(c), c->mass, c->pin, mask, (float)(dtfi2 + mdamp), c->stream);
-    c->launches++;
-    prof_end(c, PROF_SEED, ev);
-  }
   ElemArgs ea;
   memset(&ea, 0, sizeof(ea));
   ea.n_tets = c->n_tets;
@@ -1986,56 +2103,171 @@ static void assemble_dev(sdx_context* c, const double* u, const double* ut, doub
   ea.g = c->g;
   ea.val = c->val;
   ea.obj = c->env_obj;
-  ea.dtfi2 = dtfi2;
+  ea.dtfi2 = 1.0 / (p.dt * p.dt);
   for (int k = 0; k < 3; ++k) ea.grav[k] = p.gravity[k];
   ea.min_eig = 1.1920928955078125e-07f;  // kMinProjectedEigenvalue of the FP32 build
   ea.psd = p.psd_strategy;
   ea.flags = flags;
   ea.has_arap = c->has_arap ? 1 : 0;
+  ea.threads = (flags & SDX_ASM_HESS) ? shape_override("SDX_ELEM_THREADS", c->elem_threads)
+                                      : shape_override("SDX_ELEM_RES_THREADS", c->elem_res_threads);
+  ea.aggregate = shape_override("SDX_ELEM_AGG", c->elem_agg);
+  return ea;
+}
+
+static ContactArgs contact_args(sdx_context* c, const double* u, double t, int flags, const uint8_t* mask,
+                                bool record_pairs) {
+  const sdx_step_params& p = c->params;
+  ContactArgs ca;
+  memset(&ca, 0, sizeof(ca));
+  ca.n_samples = 3 * c->n_faces;
+  ca.faces = c->faces;
+  ca.face_area = c->face_area;
+  ca.face_slots = c->face_slots;
+  ca.colliders = c->colliders;
+  ca.coll_off = c->coll_off;
+  ca.env_mask = mask;
+  ca.u = u;
+  ca.X = c->X;
+  ca.pin = c->pin;
+  ca.g = c->g;
+  ca.val = c->val;
+  ca.obj = c->env_obj;
+  ca.pair_mask = record_pairs ? c->pair_mask : nullptr;
+  ca.n_pairs = c->env_pairs;
+  ca.t = t;
+  ca.k = p.k_contact;
+  ca.t_half = p.t_half;
+  ca.thr = p.thr;
+  ca.max_align = p.max_align;
+  ca.flags = flags;
+  ca.u0 = c->u0;
+  ca.t0 = t - p.dt;
+  ca.coulomb = p.friction_coulomb;
+  ca.falloff = p.friction_falloff_vel * p.dt;
+  ca.viscous = p.friction_viscous / p.dt;
+  ca.normal_damping = p.contact_normal_damping / p.dt;
+  ca.cflags = (p.friction_collider_normal ? kContactColliderNormal : 0) |
+              (p.contact_explicit_normals ? kContactExplicit : 0) | (p.friction_fade ? kContactFade : 0) |
+              (p.contact_implicit_normal_force ? kContactImplicitFn : 0) |
+              (p.friction_fitted_hessian ? kContactFitted : 0) |
+              (p.friction_model == SDX_FRICTION_CINF ? kContactCinf : 0);
+  ca.threads = shape_override("SDX_CONTACT_THREADS", c->contact_threads);
+  return ca;
+}
+
+// Assembles into c->g / c->val / c->env_obj for the envs in mask (device array, NULL = all).
+static void assemble_dev(sdx_context* c, const double* u, const double* ut, double t, int flags,
+                         const uint8_t* mask, bool record_pairs) {
+  const sdx_step_params& p = c->params;
+  const double dtfi2 = 1.0 / (p.dt * p.dt);
+  if (flags & SDX_ASM_RES) {
+    launch_zero_rows(c->n_slices, c->slice_env, mask, c->g, c->stream);
+    c->launches++;
+  }
+  cudaEvent_t ev;
+  if (flags & SDX_ASM_HESS) {
+    prof_begin(c, &ev);
+    // massScale = 1/dt^2 + alpha/dt (ComputeSoftDampingScales, mochi_physics/src/mochi_soft.h:274-290)
+    const double mdamp = p.mass_damping > 0.0 ? p.mass_damping / p.dt : 0.0;
+    launch_seed_hessian(ctx_matrix(c), c->mass, c->pin, mask, (float)(dtfi2 + mdamp), c->stream);
+    c->launches++;
+    prof_end(c, PROF_SEED, ev);
+  }
+  const ElemArgs ea = elem_args(c, u, ut, flags, mask);
   prof_begin(c, &ev);
   launch_element(ea, c->stream);
   c->launches++;
   prof_end(c, (flags & SDX_ASM_HESS) ? PROF_HESS : PROF_RES, ev);
   if (c->n_colliders > 0 || record_pairs) {
-    ContactArgs ca;
-    memset(&ca, 0, sizeof(ca));
-    ca.n_samples = 3 * c->n_faces;
-    ca.faces = c->faces;
-    ca.face_area = c->face_area;
-    ca.face_slots = c->face_slots;
-    ca.colliders = c->colliders;
-    ca.coll_off = c->coll_off;
-    ca.env_mask = mask;
-    ca.u = u;
-    ca.X = c->X;
-    ca.pin = c->pin;
-    ca.g = c->g;
-    ca.val = c->val;
-    ca.obj = c->env_obj;
-    ca.pair_mask = record_pairs ? c->pair_mask : nullptr;
-    ca.n_pairs = c->env_pairs;
-    ca.t = t;
-    ca.k = p.k_contact;
-    ca.t_half = p.t_half;
-    ca.thr = p.thr;
-    ca.max_align = p.max_align;
-    ca.flags = flags;
-    ca.u0 = c->u0;
-    ca.t0 = t - p.dt;
-    ca.coulomb = p.friction_coulomb;
-    ca.falloff = p.friction_falloff_vel * p.dt;
-    ca.viscous = p.friction_viscous / p.dt;
-    ca.normal_damping = p.contact_normal_damping / p.dt;
-    ca.cflags = (p.friction_collider_normal ? kContactColliderNormal : 0) |
-                (p.contact_explicit_normals ? kContactExplicit : 0) | (p.friction_fade ? kContactFade : 0) |
-                (p.contact_implicit_normal_force ? kContactImplicitFn : 0) |
-                (p.friction_fitted_hessian ? kContactFitted : 0) |
-                (p.friction_model == SDX_FRICTION_CINF ? kContactCinf : 0);
+    const ContactArgs ca = contact_args(c, u, t, flags, mask, record_pairs);
     prof_begin(c, &ev);
     launch_contact(ca, c->stream);
     c->launches++;
     prof_end(c, PROF_CONTACT, ev);
   }
+}
+
+// Launch-shape tuner of the assembly kernels (SDX_AUTOTUNE=1), run once per uploaded batch before its first
+// assembly: it times the element kernel's Hessian launch for CTA sizes 64, 128 and 256 with the plain and
+// the warp-aggregated block scatter, its residual-only launch for the three sizes, and the contact kernel
+// for the three sizes, each on the real state (one untimed and one timed launch per shape), and keeps the
+// fastest. The timed launches leave garbage in g, the matrix values and the pair counters; every caller
+// assembles afresh right after (the residual rows are zeroed and the Hessian reseeded first), and the pair
+// counters of all envs are cleared here.
+static int autotune_assembly(sdx_context* c, const double* u, const double* ut, double t) {
+  c->asm_tuned = true;
+  const char* env = getenv("SDX_AUTOTUNE");
+  if (!(env && atoi(env) != 0)) return SDX_OK;
+  const bool prof = c->profiling;
+  c->profiling = false;
+  cudaEvent_t e0, e1;
+  SDX_CUDA(cudaEventCreate(&e0));
+  SDX_CUDA(cudaEventCreate(&e1));
+  auto time_launch = [&](auto&& launch, double& us) -> int {
+    us = 1e30;
+    for (int rep = 0; rep < 2; ++rep) {
+      SDX_CUDA(cudaEventRecord(e0, c->stream));
+      launch();
+      SDX_CUDA(cudaEventRecord(e1, c->stream));
+      SDX_CUDA(cudaEventSynchronize(e1));
+      SDX_CUDA(cudaGetLastError());
+      float ms = 0.0f;
+      SDX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      us = 1e3 * ms;
+    }
+    return SDX_OK;
+  };
+  const int sizes[3] = {64, 128, 256};
+  const int hess = SDX_ASM_RES | SDX_ASM_HESS | SDX_ASM_PSD;
+  double best = 1e30;
+  for (int agg = 0; agg < 2; ++agg)
+    for (int th : sizes) {
+      ElemArgs ea = elem_args(c, u, ut, hess, nullptr);
+      ea.threads = th;
+      ea.aggregate = agg;
+      double us;
+      SDX_TRY(time_launch([&] { launch_element(ea, c->stream); }, us));
+      c->launches += 2;
+      if (th == 128 && agg == 0) c->tune_elem_default_us = us;
+      if (us < best) {
+        best = us;
+        c->elem_threads = th;
+        c->elem_agg = agg;
+      }
+    }
+  c->tune_elem_us = best;
+  best = 1e30;
+  for (int th : sizes) {
+    ElemArgs ea = elem_args(c, u, ut, SDX_ASM_RES, nullptr);
+    ea.threads = th;
+    double us;
+    SDX_TRY(time_launch([&] { launch_element(ea, c->stream); }, us));
+    c->launches += 2;
+    if (us < best) {
+      best = us;
+      c->elem_res_threads = th;
+    }
+  }
+  if (c->n_colliders > 0) {
+    best = 1e30;
+    for (int th : sizes) {
+      ContactArgs ca = contact_args(c, u, t, hess, nullptr, false);
+      ca.threads = th;
+      double us;
+      SDX_TRY(time_launch([&] { launch_contact(ca, c->stream); }, us));
+      c->launches += 2;
+      if (us < best) {
+        best = us;
+        c->contact_threads = th;
+      }
+    }
+    SDX_CUDA(cudaMemsetAsync(c->env_pairs, 0, sizeof(unsigned long long) * c->n_envs, c->stream));
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->profiling = prof;
+  return SDX_OK;
 }
 
 extern "C" int sdx_assemble(sdx_context* c, const double* u, double t, int flags, double* obj, double* g,
@@ -2247,8 +2479,11 @@ extern "C" int sdx_set_linear_solver(sdx_context* c, sdx_linear_solve_fn fn, voi
 // cluster size (2, 4, 8, 16) against the best grid shape.
 static int autotune_pcg(sdx_context* c, const sdx_linear_params& lp) {
   c->pcg_tuned = true;
+  // on with SDX_PCG_AUTOTUNE=1, or with SDX_AUTOTUNE=1 (every tuner) unless SDX_PCG_AUTOTUNE=0
   const char* env = getenv("SDX_PCG_AUTOTUNE");
-  if (!(env && atoi(env) != 0) || getenv("SDX_PCG_THREADS")) return SDX_OK;
+  const char* all = getenv("SDX_AUTOTUNE");
+  const bool on = env ? atoi(env) != 0 : (all && atoi(all) != 0);
+  if (!on || getenv("SDX_PCG_THREADS")) return SDX_OK;
   const bool prof = c->profiling;
   c->profiling = false;
   sdx_linear_params tl = lp;
@@ -2363,6 +2598,7 @@ static int step_once(sdx_context* c) {
   std::vector<double> nrm, scale(E, 1.0);
   SDX_CUDA(cudaMemsetAsync(c->env_pairs, 0, sizeof(unsigned long long) * E, c->stream));
   SDX_TRY(upload_mask(c, mask));
+  if (!c->asm_tuned) SDX_TRY(autotune_assembly(c, c->u, c->ut, t_end));
   assemble_dev(c, c->u, c->ut, t_end, SDX_ASM_RES | SDX_ASM_HESS | SDX_ASM_PSD, c->env_mask, false);
   SDX_TRY(env_dot_host(c, c->g, c->g, c->env_mask, nrm));
   for (int e = 0; e < E; ++e) res[e] = std::sqrt(nrm[e]);
@@ -2465,9 +2701,14 @@ static int step_once(sdx_context* c) {
     if (c->ext_fn) {
       SDX_TRY(run_external(c, mask, p.linear, zero, it_out));
     } else {
-      SDX_TRY(run_pcg(c, ctx_matrix(c), c->diag_pos, E, c->part, c->work, c->g, c->dx, c->env_mask, n_active,
-                      p.linear, zero, p.ew_forcing == 2 ? c->work.env_rel_tol : nullptr, /*scale_guess*/ !zero,
-                      mask.data(), learned ? c->uscratch : nullptr));
+      if (p.linear.refine_inner_rel_tol > 0.0)
+        SDX_TRY(run_pcg_refined(c, ctx_matrix(c), c->diag_pos, E, c->part, c->work, c->g, c->dx, c->env_mask,
+                                n_active, p.linear, zero, /*scale_guess*/ !zero, mask.data(),
+                                learned ? c->uscratch : nullptr, p.ew_forcing == 2 ? eta.data() : nullptr));
+      else
+        SDX_TRY(run_pcg(c, ctx_matrix(c), c->diag_pos, E, c->part, c->work, c->g, c->dx, c->env_mask, n_active,
+                        p.linear, zero, p.ew_forcing == 2 ? c->work.env_rel_tol : nullptr, /*scale_guess*/ !zero,
+                        mask.data(), learned ? c->uscratch : nullptr));
       SDX_CUDA(cudaMemcpy(it_out.data(), c->work.out_iters, sizeof(int) * E, cudaMemcpyDeviceToHost));
     }
     for (int e = 0; e < E; ++e)
@@ -2610,6 +2851,8 @@ extern "C" int sdx_pcg_solve_ctx(sdx_context* c, int n, int64_t nnzb, const int6
     return set_error(SDX_ERR_INVALID_ARGUMENT, "value_layout");
   if (lp->preconditioner < 0 || lp->preconditioner > 2) return set_error(SDX_ERR_INVALID_ARGUMENT, "preconditioner");
   if (lp->max_iter <= 0) return set_error(SDX_ERR_INVALID_ARGUMENT, "max_iter must be positive");
+  if (!(lp->refine_inner_rel_tol >= 0.0 && lp->refine_inner_rel_tol < 1.0) || lp->refine_max_passes < 0)
+    return set_error(SDX_ERR_INVALID_ARGUMENT, "refinement needs 0 <= inner tolerance < 1 and passes >= 0");
   if (row_ptr[0] != 0 || row_ptr[n] != nnzb) return set_error(SDX_ERR_INVALID_ARGUMENT, "row_ptr inconsistent with nnzb");
   for (int i = 0; i < n; ++i) {
     if (row_ptr[i + 1] < row_ptr[i]) return set_error(SDX_ERR_INVALID_ARGUMENT, "row_ptr not monotone");
@@ -2685,8 +2928,11 @@ extern "C" int sdx_pcg_solve_ctx(sdx_context* c, int n, int64_t nnzb, const int6
   A.slice_env = c->solo_slice_env;
   A.col = c->solo_col;
   A.val = c->solo_val;
-  int rc = run_pcg(c, A, c->solo_diag, 1, c->solo_part, c->solo_work, c->solo_b, c->solo_x, nullptr, 1, *lp,
-                   hint == SDX_GUESS_ZERO, nullptr);
+  int rc = lp->refine_inner_rel_tol > 0.0
+               ? run_pcg_refined(c, A, c->solo_diag, 1, c->solo_part, c->solo_work, c->solo_b, c->solo_x, nullptr,
+                                 1, *lp, hint == SDX_GUESS_ZERO, false, nullptr, nullptr)
+               : run_pcg(c, A, c->solo_diag, 1, c->solo_part, c->solo_work, c->solo_b, c->solo_x, nullptr, 1, *lp,
+                         hint == SDX_GUESS_ZERO, nullptr);
   dfree(drp);
   dfree(dbc);
   dfree(dbv);

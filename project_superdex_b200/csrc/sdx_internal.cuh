@@ -49,6 +49,9 @@ struct Matrix {
   float* val;
 };
 
+// largest CTA size of the element kernel (the shape tuner picks 64, 128 or 256)
+constexpr int kElemMaxThreads = 256;
+
 struct ElemArgs {
   int64_t n_tets;
   const int4* tets;
@@ -80,6 +83,8 @@ struct ElemArgs {
   int psd;
   int flags;
   int has_arap;  // some env uses ARAP (launch the variant that evaluates it)
+  int threads;   // CTA size: 64, 128 or 256 (anything else: 128)
+  int aggregate; // Hessian launches: warp-aggregated block scatter
 };
 
 struct ContactArgs {
@@ -107,6 +112,7 @@ struct ContactArgs {
   double falloff;     // frictionFalloffVel * dt: the smoothing width in displacement
   double viscous, normal_damping;  // viscousFrictionCoefficient / dt, normalViscousDampingCoefficient / dt
   int cflags;         // kContact* bits
+  int threads;        // CTA size: 64, 128 or 256 (anything else: 128)
 };
 
 // ContactArgs::cflags
@@ -212,6 +218,10 @@ void launch_pred(int64_t n3, const double* u, const double* v, double dt, double
 void launch_ls_candidate(int n_slices, const int* slice_env, const uint8_t* env_mask,
                          const double* ubase, const double* dx, const double* scale, double* u,
                          cudaStream_t st);
+void launch_residual64(const Matrix& A, const uint8_t* env_mask, const double* x, const double* b, double* r,
+                       cudaStream_t st);
+void launch_add_rows(int n_slices, const int* slice_env, const uint8_t* env_mask, const double* d, double* x,
+                     cudaStream_t st);
 void launch_copy_rows(int n_slices, const int* slice_env, const uint8_t* env_mask, const double* src,
                       double* dst, cudaStream_t st);
 void launch_velocity(int64_t n3, const double* u, const double* u0, double dt, double* v,

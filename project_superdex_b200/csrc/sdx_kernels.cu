@@ -87,23 +87,57 @@ void launch_seed_hessian(const Matrix& A, const float* mass, const uint8_t* pin,
 
 __device__ __forceinline__ void warp_env_add(double* obj, int env, double v) {
   // aggregate lanes of the same env before one atomic
+  // (the shuffles name only the lanes of this env, which all run the same number of them)
   const unsigned mask = __activemask();
   const unsigned same = __match_any_sync(mask, env);
   const int leader = __ffs(same) - 1;
   double s = 0.0;
   for (unsigned m = same; m; m &= m - 1) {
     const int l = __ffs(m) - 1;
-    s += __shfl_sync(mask, v, l);
+    s += __shfl_sync(same, v, l);
   }
   if ((int)(threadIdx.x & 31) == leader) atomicAdd(obj + env, s);
 }
 
+// One 3x3 block into the sliced-ELL values: entries 0-3 and 4-7 are 16-byte-aligned runs, so two float4
+// reductions and one scalar one. kAgg: the lanes of the warp (those converged here) that hold a block for
+// the same position p first add their blocks in the group's lowest lane, which alone writes. On the
+// Freudenthal split of a tet grid a warp's 32 tets share the hex diagonals, so the diagonal blocks of
+// nodes 0 and 3 (and the off-diagonal pair between them) repeat up to 6 times per warp instruction.
+template <bool kAgg>
+__device__ __forceinline__ void scatter_block(float* val, int p, const float kb[9]) {
+  if (kAgg) {
+    const unsigned act = __activemask();
+    const unsigned peers = __match_any_sync(act, p);
+    const int lane = (int)(threadIdx.x & 31);
+    if (peers != (1u << lane)) {
+      float s[9];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) s[i] = 0.0f;
+      for (unsigned m = peers; m; m &= m - 1) {  // every lane of the group runs the same shuffles
+        const int l = __ffs(m) - 1;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) s[i] += __shfl_sync(peers, kb[i], l);
+      }
+      if (lane != __ffs(peers) - 1) return;
+      atomicAdd(reinterpret_cast<float4*>(val + val_index(p, 0)), make_float4(s[0], s[1], s[2], s[3]));
+      atomicAdd(reinterpret_cast<float4*>(val + val_index(p, 4)), make_float4(s[4], s[5], s[6], s[7]));
+      atomicAdd(val + val_index(p, 8), s[8]);
+      return;
+    }
+  }
+  atomicAdd(reinterpret_cast<float4*>(val + val_index(p, 0)), make_float4(kb[0], kb[1], kb[2], kb[3]));
+  atomicAdd(reinterpret_cast<float4*>(val + val_index(p, 4)), make_float4(kb[4], kb[5], kb[6], kb[7]));
+  atomicAdd(val + val_index(p, 8), kb[8]);
+}
+
 // kArap: the variant that also evaluates ARAP envs (SVD-based, more registers); launched only when some
 // env uses ARAP, so the other materials keep the lean variant. kDamp: the variant with Rayleigh stiffness
-// damping (viscous stress, its residual, energy and Hessian terms), launched only when it is on. The lean
-// variant fits 128 registers, so 4 CTAs of 128 threads share an SM.
-template <bool kArap, bool kDamp>
-__global__ void __launch_bounds__(128, (kArap || kDamp) ? 1 : 4) k_element(ElemArgs a) {
+// damping (viscous stress, its residual, energy and Hessian terms), launched only when it is on. kAgg:
+// warp-aggregated block scatter (scatter_block). The lean variant fits 128 registers, so 512 threads share
+// an SM whatever the CTA size (64, 128 or 256 threads, a launch-time choice of the shape tuner).
+template <bool kArap, bool kDamp, bool kAgg>
+__global__ void __launch_bounds__(kElemMaxThreads, (kArap || kDamp) ? 1 : 2) k_element(ElemArgs a) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= a.n_tets) return;
   const int4 nd = a.tets[t];
@@ -277,11 +311,6 @@ __global__ void __launch_bounds__(128, (kArap || kDamp) ? 1 : 4) k_element(ElemA
     // transpose (C and the damping terms are symmetric). Pinned rows and columns stay zero. A block is
     // scattered whole: entries 0-3 and 4-7 are 16-byte aligned runs in the sliced-ELL value layout, so it
     // takes two float4 reductions and one scalar one.
-    auto scatter = [&](int p, const float kb[9]) {
-      atomicAdd(reinterpret_cast<float4*>(a.val + val_index(p, 0)), make_float4(kb[0], kb[1], kb[2], kb[3]));
-      atomicAdd(reinterpret_cast<float4*>(a.val + val_index(p, 4)), make_float4(kb[4], kb[5], kb[6], kb[7]));
-      atomicAdd(a.val + val_index(p, 8), kb[8]);
-    };
 #pragma unroll 1
     for (int f = 0; f < 4; ++f) {
 #pragma unroll 1
@@ -317,26 +346,35 @@ __global__ void __launch_bounds__(128, (kArap || kDamp) ? 1 : 4) k_element(ElemA
             kt[3 * c + r] = (((pins[g] >> c) & 1) || ((pins[f] >> r) & 1)) ? 0.0f : kb[3 * r + c];
             if (((pins[f] >> r) & 1) || ((pins[g] >> c) & 1)) kb[3 * r + c] = 0.0f;
           }
-        scatter(slot[f * 4 + g], kb);
-        if (g != f) scatter(slot[g * 4 + f], kt);
+        scatter_block<kAgg>(a.val, slot[f * 4 + g], kb);
+        if (g != f) scatter_block<kAgg>(a.val, slot[g * 4 + f], kt);
       }
     }
   }
 }
 
-void launch_element(const ElemArgs& a, cudaStream_t st) {
-  if (a.n_tets == 0) return;
-  const int th = 128;
-  const unsigned nb = (unsigned)((a.n_tets + th - 1) / th);
+template <bool kAgg>
+static void launch_element_t(const ElemArgs& a, unsigned nb, int th, cudaStream_t st) {
   const bool damp = a.kdamp > 0.0;
   if (a.has_arap && damp)
-    k_element<true, true><<<nb, th, 0, st>>>(a);
+    k_element<true, true, kAgg><<<nb, th, 0, st>>>(a);
   else if (a.has_arap)
-    k_element<true, false><<<nb, th, 0, st>>>(a);
+    k_element<true, false, kAgg><<<nb, th, 0, st>>>(a);
   else if (damp)
-    k_element<false, true><<<nb, th, 0, st>>>(a);
+    k_element<false, true, kAgg><<<nb, th, 0, st>>>(a);
   else
-    k_element<false, false><<<nb, th, 0, st>>>(a);
+    k_element<false, false, kAgg><<<nb, th, 0, st>>>(a);
+}
+
+void launch_element(const ElemArgs& a, cudaStream_t st) {
+  if (a.n_tets == 0) return;
+  const int th = (a.threads == 64 || a.threads == 256) ? a.threads : 128;
+  const unsigned nb = (unsigned)((a.n_tets + th - 1) / th);
+  // the aggregated scatter only changes the Hessian's scatter; a residual-only launch takes the plain code
+  if (a.aggregate && (a.flags & 4))
+    launch_element_t<true>(a, nb, th, st);
+  else
+    launch_element_t<false>(a, nb, th, st);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -367,7 +405,7 @@ __device__ __forceinline__ void face_normal(const double xn[3][3], double nrm[3]
 // distance (contact_utils.h:1003-1230). Colliders are rigid translations, so the collider frame is the
 // world frame moved by vel t. With explicit normals the alignment, the friction plane and the normal
 // force come from the stage start, and pairs in contact only at the stage start enter with d = thr.
-__global__ void __launch_bounds__(128) k_contact(ContactArgs a) {
+__global__ void __launch_bounds__(256) k_contact(ContactArgs a) {
   const int64_t sidx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (sidx >= a.n_samples) return;
   const int64_t f = sidx / 3;
@@ -503,7 +541,7 @@ __global__ void __launch_bounds__(128) k_contact(ContactArgs a) {
 
 void launch_contact(const ContactArgs& a, cudaStream_t st) {
   if (a.n_samples == 0) return;
-  const int th = 128;
+  const int th = (a.threads == 64 || a.threads == 256) ? a.threads : 128;
   k_contact<<<(unsigned)((a.n_samples + th - 1) / th), th, 0, st>>>(a);
 }
 
@@ -967,6 +1005,44 @@ __device__ __forceinline__ void true_residual(const PcgArgs& a, int s, int lane,
   r[0] = a.b[3 * row] - ax[0];
   r[1] = a.b[3 * row + 1] - ax[1];
   r[2] = a.b[3 * row + 2] - ax[2];
+}
+
+// Iterative refinement: r = b - A x in FP64 (FP32 matrix values) for the slices of the envs in env_mask, one
+// warp per slice, one row per lane.
+__global__ void k_residual64(Matrix A, const uint8_t* __restrict__ env_mask, const double* __restrict__ x,
+                             const double* __restrict__ b, double* __restrict__ r) {
+  const int s = (int)(((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (s >= A.n_slices) return;
+  if (env_mask && !env_mask[A.slice_env[s]]) return;
+  double ax[3];
+  spmv_f64_rows<4, 1>(A, s, lane, x, nullptr, ax, nullptr);
+  const int64_t row = (int64_t)s * kSlice + lane;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) r[3 * row + c] = b[3 * row + c] - ax[c];
+}
+
+void launch_residual64(const Matrix& A, const uint8_t* env_mask, const double* x, const double* b, double* r,
+                       cudaStream_t st) {
+  if (A.n_slices == 0) return;
+  const int64_t threads = (int64_t)A.n_slices * kSlice;
+  k_residual64<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(A, env_mask, x, b, r);
+}
+
+// x += d on the rows of the envs in env_mask
+__global__ void k_add_rows(int n_slices, const int* __restrict__ slice_env, const uint8_t* __restrict__ env_mask,
+                           const double* __restrict__ d, double* x) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)n_slices * kSlice * 3) return;
+  if (env_mask && !env_mask[slice_env[i / (kSlice * 3)]]) return;
+  x[i] += d[i];
+}
+
+void launch_add_rows(int n_slices, const int* slice_env, const uint8_t* env_mask, const double* d, double* x,
+                     cudaStream_t st) {
+  const int64_t n = (int64_t)n_slices * kSlice * 3;
+  if (n == 0) return;
+  k_add_rows<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n_slices, slice_env, env_mask, d, x);
 }
 
 // Bulk L2 prefetch of [ptr, ptr + bytes) (one instruction, no registers held; address and size multiples of

@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import os
 
 from . import scenes
 from .soft_body import SoftBodyWorld
@@ -140,7 +141,28 @@ def main(argv=None):
         w.assemble(hess=True, psd=True, obj=True)
         torch.cuda.synchronize()
         torch.cuda.profiler.stop()
-        out.update(bytes_per_launch=element_bytes(w.n_tets, w.n_nodes, w.nnzb))
+        by = element_bytes(w.n_tets, w.n_nodes, w.nnzb)
+        out.update(bytes_per_launch=by)
+        # every launch shape: Hessian assembly (plain / warp-aggregated scatter) and residual-only assembly,
+        # device time per element launch from the library's event timers
+        shapes = {}
+        for th in (64, 128, 256):
+            for agg in (0, 1):
+                os.environ.update(SDX_ELEM_THREADS=str(th), SDX_ELEM_RES_THREADS=str(th), SDX_ELEM_AGG=str(agg))
+                w.set_profiling(True)
+                for _ in range(args.reps):
+                    w.assemble(hess=True, psd=True, obj=False)
+                    if agg == 0:
+                        w.assemble(hess=False, psd=True, obj=False)
+                pr = w.profile()
+                key = f"{th}{'_agg' if agg else ''}"
+                shapes[key] = {"hess_ms": pr["asm_hess_ms"] / max(1, pr["asm_hess_launches"])}
+                if agg == 0:
+                    shapes[key]["res_ms"] = pr["asm_res_ms"] / max(1, pr["asm_res_launches"])
+        for k in ("SDX_ELEM_THREADS", "SDX_ELEM_RES_THREADS", "SDX_ELEM_AGG"):
+            os.environ.pop(k, None)
+        w.set_profiling(False)
+        out.update(shapes=shapes)
     else:
         torch.cuda.profiler.start()
         ms, by = w.bench_spmv(reps=args.reps)
