@@ -162,6 +162,14 @@ typedef struct {
                                       the stage start stay in the contact set */
   int contact_implicit_normal_force; /* implicitNormalForceForDissipation (default 0; not together with
                                         explicit normals) */
+  int newton_graph;  /* no counterpart in the reference (default 0). 1: each step is one CUDA graph launch;
+                        the Newton loop and the ResidualNorm line search are conditional while-nodes whose
+                        conditions device kernels set from the same stop tests, so the step takes no host
+                        round trip. Zero, previous or temporal warm start with the constant or Eisenstat-Walker linear
+                        tolerance; the PCG runs on the grid kernel over the upload's partition (no
+                        re-partitioning, no cluster kernel) and per-kernel profiling records nothing. The
+                        graph is built on the first such step and rebuilt when the parameters or the bodies
+                        change; the launch-shape tuners only run in host-driven steps. */
 } sdx_step_params;
 
 /* Per-env statistics of the last step (StageSolverStats, mochi_physics/src/mochi_solve.cpp:1144). */

@@ -9,7 +9,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsdx_b200.so")
-SOURCES = ["sdx_kernels.cu", "sdx_host.cu", "sdx_noalloc.cu", "sdx_mlp.cu"]
+SOURCES = ["sdx_kernels.cu", "sdx_host.cu", "sdx_noalloc.cu", "sdx_mlp.cu", "sdx_newton.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -72,7 +72,7 @@ class StepParams(C.Structure):
                 ("contact_normal_damping", C.c_double), ("friction_model", C.c_int),
                 ("friction_fitted_hessian", C.c_int), ("friction_fade", C.c_int),
                 ("friction_collider_normal", C.c_int), ("contact_explicit_normals", C.c_int),
-                ("contact_implicit_normal_force", C.c_int)]
+                ("contact_implicit_normal_force", C.c_int), ("newton_graph", C.c_int)]
 
 
 class DeviceSystem(C.Structure):

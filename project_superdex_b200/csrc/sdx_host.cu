@@ -187,6 +187,27 @@ struct Snapshot {
 constexpr int kSnapHist = 4;                 // == sdx_context::kHist
 constexpr int kSnapVectors = 5 + kSnapHist;  // u, v, dx, dx_prev1, dx_prev2, dx_hist[kHist]
 
+// A step captured as one CUDA graph (sdx_step_params.newton_graph): the executable graph, the parameters
+// and topology generation it was built for, and the device-resident Newton state its kernels share.
+struct StepGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  sdx_step_params params;
+  uint64_t gen = 0;
+  char* block = nullptr;   // one allocation: the Newton state arrays, the control words and the step time
+  NewtonDev d;
+  double* t_dev = nullptr;
+  int64_t k_pro = 0, k_pass = 0, k_ls = 0;  // kernel launches recorded per prologue+epilogue, pass and trial
+  void release() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+    dfree(block);
+    t_dev = nullptr;
+  }
+};
+
 struct sdx_context {
   int device = 0;
   int num_sms = 0;
@@ -307,6 +328,9 @@ struct sdx_context {
   std::vector<double*> snap_pool;  // released snapshot buffers kept for the next capture
   unsigned long long* snap_flag = nullptr;  // device word of sdx_is_equal_state
   uint64_t fingerprint = 0;        // FNV-1a of the uploaded bodies (offsets, rest positions, tets)
+  // graph-captured step; topo_gen counts the uploads and collider / material changes a graph depends on
+  StepGraph sg;
+  uint64_t topo_gen = 0;
   // opt-in per-kernel timing: event pairs resolved lazily
   bool profiling = false;
   sdx_profile prof;
@@ -760,15 +784,12 @@ constexpr int kPcgPrefetchAhead = 3;
 // share of the rows still iterating at which a batched PCG launch re-partitions
 constexpr double kPcgRepartRatio = 0.5;
 
-// One PCG solve of every env in env_mask (host copy h_mask, NULL: all). For a batch of envs on the
-// context matrix, the persistent kernel exits each time the rows still iterating fall to a share
-// (kPcgRepartRatio) of those it started with; the envs still iterating are then re-partitioned over all CTAs (a slice list of just
-// their slices) and the kernel resumes where it stopped, so the slowest envs get the whole GPU.
-static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_envs, PcgPartition& P,
-                   PcgWork& W, const double* b, double* x, const uint8_t* env_mask, int n_active,
-                   const sdx_linear_params& lp, bool zero_guess, const double* env_rel_tol,
-                   bool scale_guess = false, const uint8_t* h_mask = nullptr, const double* x2 = nullptr) {
-  PcgArgs a;
+// The launch arguments of one PCG solve that do not depend on the partition: matrix, vectors, tolerances,
+// start mode, the streamed-vector modes (prefetch, r carried by z) and the control words.
+static int pcg_base_args(sdx_context* c, const Matrix& A, const int* diag_pos, int n_envs, PcgWork& W,
+                         const double* b, double* x, const uint8_t* env_mask, const sdx_linear_params& lp,
+                         bool zero_guess, const double* env_rel_tol, bool scale_guess, const double* x2,
+                         PcgArgs& a) {
   memset(&a, 0, sizeof(a));
   a.A = A;
   a.n_envs = n_envs;
@@ -824,11 +845,23 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
   }();
   a.r_in_z = r_in_z_env >= 0 ? r_in_z_env : (streamed ? 1 : 0);
   a.es = W.es;
+  return SDX_OK;
+}
+
+// One PCG solve of every env in env_mask (host copy h_mask, NULL: all). For a batch of envs on the
+// context matrix, the persistent kernel exits each time the rows still iterating fall to a share
+// (kPcgRepartRatio) of those it started with; the envs still iterating are then re-partitioned over all CTAs (a slice list of just
+// their slices) and the kernel resumes where it stopped, so the slowest envs get the whole GPU.
+static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_envs, PcgPartition& P,
+                   PcgWork& W, const double* b, double* x, const uint8_t* env_mask, int n_active,
+                   const sdx_linear_params& lp, bool zero_guess, const double* env_rel_tol,
+                   bool scale_guess = false, const uint8_t* h_mask = nullptr, const double* x2 = nullptr) {
+  PcgArgs a;
+  SDX_TRY(pcg_base_args(c, A, diag_pos, n_envs, W, b, x, env_mask, lp, zero_guess, env_rel_tol, scale_guess, x2,
+                        a));
   // re-partitioning applies to batches on the context matrix (SDX_PCG_REPART=0 disables it)
-  static const bool repart_on = [] {
-    const char* e = getenv("SDX_PCG_REPART");
-    return !(e && atoi(e) == 0);
-  }();
+  const char* repart_env = getenv("SDX_PCG_REPART");  // read per solve, so a process can switch it
+  const bool repart_on = !(repart_env && atoi(repart_env) == 0);
   const bool batch = repart_on && A.val == c->val && n_envs == c->n_envs && n_envs > 1 && c->env_nrows;
   int64_t rows = 0;
   if (batch) {
@@ -1161,6 +1194,7 @@ extern "C" int sdx_destroy(sdx_context* c) {
   if (!c) return SDX_OK;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  c->sg.release();
   release_topology(c);
   release_solo(c);
   release_mlp(c);
@@ -1623,6 +1657,8 @@ extern "C" int sdx_upload_bodies(sdx_context* c, int n_envs, const int64_t* node
   c->stats.assign(n_envs, sdx_env_stats{});
   c->time = 0.0;
   SDX_CUDA(cudaStreamSynchronize(c->stream));
+  c->sg.release();
+  c->topo_gen++;
   c->uploaded = true;
   return SDX_OK;
 }
@@ -1647,6 +1683,7 @@ extern "C" int sdx_set_materials(sdx_context* c, int n_envs, const int32_t* mate
   cudaSetDevice(c->device);
   SDX_CUDA(cudaMemcpy(c->env_material, m.data(), n_envs, cudaMemcpyHostToDevice));
   c->has_arap = arap;
+  c->topo_gen++;  // a captured step launches the element variant of the materials it was built for
   return SDX_OK;
 }
 
@@ -1676,6 +1713,7 @@ extern "C" int sdx_set_colliders(sdx_context* c, int n, const int32_t* env, cons
   SDX_TRY(upload(&c->colliders, h));
   c->n_colliders = n;
   c->max_coll_per_env = mx;
+  c->topo_gen++;  // a captured step holds the collider arrays it was built with
   return SDX_OK;
 }
 
@@ -2158,7 +2196,7 @@ static ContactArgs contact_args(sdx_context* c, const double* u, double t, int f
 
 // Assembles into c->g / c->val / c->env_obj for the envs in mask (device array, NULL = all).
 static void assemble_dev(sdx_context* c, const double* u, const double* ut, double t, int flags,
-                         const uint8_t* mask, bool record_pairs) {
+                         const uint8_t* mask, bool record_pairs, const double* t_dev = nullptr) {
   const sdx_step_params& p = c->params;
   const double dtfi2 = 1.0 / (p.dt * p.dt);
   if (flags & SDX_ASM_RES) {
@@ -2180,7 +2218,8 @@ static void assemble_dev(sdx_context* c, const double* u, const double* ut, doub
   c->launches++;
   prof_end(c, (flags & SDX_ASM_HESS) ? PROF_HESS : PROF_RES, ev);
   if (c->n_colliders > 0 || record_pairs) {
-    const ContactArgs ca = contact_args(c, u, t, flags, mask, record_pairs);
+    ContactArgs ca = contact_args(c, u, t, flags, mask, record_pairs);
+    ca.t_dev = t_dev;
     prof_begin(c, &ev);
     launch_contact(ca, c->stream);
     c->launches++;
@@ -2580,10 +2619,12 @@ __global__ void k_zero_env_pairs(int n_envs, const uint8_t* __restrict__ env_mas
   if (e < n_envs && (!env_mask || env_mask[e])) pairs[e] = 0ull;
 }
 
-static void zero_env_pairs(sdx_context* c) {
-  k_zero_env_pairs<<<(c->n_envs + 255) / 256, 256, 0, c->stream>>>(c->n_envs, c->env_mask, c->env_pairs);
+static void zero_env_pairs(sdx_context* c, const uint8_t* mask) {
+  k_zero_env_pairs<<<(c->n_envs + 255) / 256, 256, 0, c->stream>>>(c->n_envs, mask, c->env_pairs);
   c->launches++;
 }
+
+static void zero_env_pairs(sdx_context* c) { zero_env_pairs(c, c->env_mask); }
 
 static int step_once(sdx_context* c) {
   const sdx_step_params& p = c->params;
@@ -2790,11 +2831,280 @@ static int step_once(sdx_context* c) {
   return SDX_OK;
 }
 
+// ------------------------------------------------------------------------------------------------
+// A step as one CUDA graph (sdx_step_params.newton_graph)
+//
+// prologue   pred, pair counters, Newton state, assembly (residual + Hessian, every env), ||g||, stop tests
+// WHILE some env iterates (handle set by k_nt_control):
+//   [temporal start], PCG control words, persistent PCG (grid kernel, the upload's partition), [history],
+//   dx -> dx_prev1, ||dx||, line-search start, u -> ubase,
+//   WHILE some env is left in the line search (handle set by k_nt_after_solve / k_nt_ls_check):
+//     step length, candidate u, pair counters, residual assembly of those envs, ||g||, verdicts
+//   ||u||, explosion control + stop tests, Hessian assembly of the next pass's envs
+// epilogue   velocity
+// The step time comes from a device word written before each launch; everything else the kernels read
+// was fixed at capture, so the graph is rebuilt when the parameters or the topology change.
+
+// Appends a conditional while-node after the work captured so far on the stream and makes it the capture's
+// only dependency; returns its body graph.
+static int capture_while(sdx_context* c, cudaGraphConditionalHandle h, cudaGraph_t* body) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  SDX_CUDA(cudaStreamGetCaptureInfo(c->stream, &cs, nullptr, &g, &deps, &nd));
+  if (cs != cudaStreamCaptureStatusActive) return set_error(SDX_ERR_CUDA, "step graph: capture not active");
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  SDX_CUDA(cudaGraphAddNode(&node, g, deps, nd, &np));
+  *body = np.conditional.phGraph_out[0];
+  SDX_CUDA(cudaStreamUpdateCaptureDependencies(c->stream, &node, 1, cudaStreamSetCaptureDependencies));
+  return SDX_OK;
+}
+
+static int build_step_graph(sdx_context* c) {
+  const sdx_step_params& p = c->params;
+  const int E = c->n_envs;
+  const int64_t n3 = 3 * c->n_rows;
+  const bool temporal = p.warm_start == SDX_WARM_TEMPORAL;
+  StepGraph& G = c->sg;
+  G.release();
+  if (temporal && !c->dx_hist) SDX_TRY(dalloc(&c->dx_hist, (size_t)sdx_context::kHist * n3));
+  // the Newton state: 4 int arrays, 5 double arrays, the line-search mask, 8 control words, the history
+  // flags and the step time, each 256-byte aligned
+  auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t bi = al(sizeof(int) * E), bd = al(sizeof(double) * E), bm = al((size_t)E);
+  const size_t bytes = 4 * bi + 5 * bd + bm + 3 * 256;
+  SDX_TRY(dalloc(&G.block, bytes));
+  SDX_CUDA(cudaMemsetAsync(G.block, 0, bytes, c->stream));  // ordered before the graph's first launch
+  char* q = G.block;
+  NewtonDev& d = G.d;
+  d.n_envs = E;
+  int** ia[4] = {&d.status, &d.iters, &d.cg, &d.lsi};
+  for (int** a : ia) {
+    *a = (int*)q;
+    q += bi;
+  }
+  double** da[5] = {&d.res0, &d.res, &d.res_prev, &d.dxn, &d.unorm};
+  for (double** a : da) {
+    *a = (double*)q;
+    q += bd;
+  }
+  d.lsmask = (uint8_t*)q;
+  q += bm;
+  d.ctl = (int*)q;
+  q += 256;
+  d.hist_valid = (int*)q;
+  q += 256;
+  G.t_dev = (double*)q;
+  d.eta = c->work.env_rel_tol;
+  d.mask = c->env_mask;
+  d.scale = c->env_scale;
+  d.nrm = c->env_norm;
+  d.pcg_iters = c->work.out_iters;
+  d.pcg_conv = c->work.out_conv;
+  d.pcg_sync = c->work.sync;
+  d.env_nrows = c->env_nrows;
+  NewtonConsts k;
+  k.abs_tol = p.newton_abs_tol;
+  k.rel_tol = p.newton_rel_tol;
+  k.rel_step_tol = p.newton_rel_step_tol;
+  k.rel_div_tol = p.rel_div_tol;
+  k.abs_div_tol = p.abs_div_tol;
+  k.lin_rel_tol = p.linear.rel_tol;
+  k.ls_alpha = p.ls_alpha;
+  k.max_iter = p.newton_max_iter;
+  k.ls_max_iter = p.ls_max_iter;
+  k.ew_forcing = p.ew_forcing;
+  // the PCG launch: the upload's partition over every slice, the pass's envs by mask, no re-partitioning
+  PcgArgs a;
+  // zero start, the previous solve's dx (scaled), or this pass's update of the previous step (scaled; the
+  // zero start when there is none, decided on the device)
+  const bool zero = p.warm_start == SDX_WARM_ZERO;
+  SDX_TRY(pcg_base_args(c, ctx_matrix(c), c->diag_pos, E, c->work, c->g, c->dx, c->env_mask, p.linear,
+                        /*zero_guess*/ zero, p.ew_forcing == 2 ? c->work.env_rel_tol : nullptr,
+                        /*scale_guess*/ !zero, nullptr, a));
+  a.zero_guess_dev = temporal ? d.ctl + 4 : nullptr;
+  const PcgPartition& P = c->part;
+  a.cta_slice = P.cta_slice;
+  a.slice_list = P.slice_list;
+  a.cta_eoff = P.cta_eoff;
+  a.cta_envs = P.cta_envs;
+  a.env_cta0 = P.env_cta0;
+  a.env_cta1 = P.env_cta1;
+  a.env_poff = P.env_poff;
+  a.part = P.part;
+  a.wstride = P.max_envs;
+  a.repart_rows = 0;
+  a.resume = 0;
+  a.env_nrows = c->env_nrows;
+  a.spin_limit = device_spin_limit();
+  const double t_cap = c->time + p.dt;  // contact launches read the real time from G.t_dev
+  const bool prof = c->profiling;
+  c->profiling = false;  // no event records inside the graph
+  cudaGraphConditionalHandle h_loop, h_ls;
+  cudaGraph_t body = nullptr, ls_body = nullptr;
+  int rc = SDX_OK;
+  auto fail = [&](int code) {
+    cudaGraph_t dummy = nullptr;
+    cudaStreamCaptureStatus cs;
+    if (cudaStreamIsCapturing(c->stream, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+      cudaStreamEndCapture(c->stream, &dummy);
+      if (dummy && dummy != G.graph) cudaGraphDestroy(dummy);
+    }
+    cudaGetLastError();
+    c->profiling = prof;
+    G.release();
+    return code;
+  };
+  SDX_CUDA(cudaGraphCreate(&G.graph, 0));
+  if (cudaGraphConditionalHandleCreate(&h_loop, G.graph, 0, 0) != cudaSuccess)
+    return fail(set_error(SDX_ERR_CUDA, "step graph: conditional handle"));
+  // prologue, the Newton while-node, epilogue
+  const int64_t l0 = c->launches;
+  if (cudaStreamBeginCaptureToGraph(c->stream, G.graph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
+      cudaSuccess)
+    return fail(set_error(SDX_ERR_CUDA, "step graph: begin capture"));
+  launch_pred(n3, c->u, c->v, p.dt, c->ut, c->u0, c->stream);
+  cudaMemsetAsync(c->env_pairs, 0, sizeof(unsigned long long) * E, c->stream);
+  launch_nt_begin(d, k, c->stream);
+  assemble_dev(c, c->u, c->ut, t_cap, SDX_ASM_RES | SDX_ASM_HESS | SDX_ASM_PSD, c->env_mask, false, G.t_dev);
+  cudaMemsetAsync(d.nrm, 0, sizeof(double) * E, c->stream);
+  launch_env_dot(c->n_slices, c->slice_env, c->env_mask, c->g, c->g, d.nrm, c->stream);
+  launch_nt_control(d, k, h_loop, c->stream);
+  c->launches += 5;
+  rc = capture_while(c, h_loop, &body);
+  if (rc != SDX_OK) return fail(rc);
+  launch_velocity(n3, c->u, c->u0, p.dt, c->v, c->stream);
+  c->launches++;
+  cudaGraph_t top = nullptr;
+  if (cudaStreamEndCapture(c->stream, &top) != cudaSuccess || top != G.graph)
+    return fail(set_error(SDX_ERR_CUDA, "step graph: prologue capture: %s", cudaGetErrorString(cudaGetLastError())));
+  G.k_pro = c->launches - l0;
+  // one Newton pass
+  if (cudaGraphConditionalHandleCreate(&h_ls, body, 0, 0) != cudaSuccess)
+    return fail(set_error(SDX_ERR_CUDA, "step graph: line-search handle"));
+  const int64_t l1 = c->launches;
+  if (cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
+      cudaSuccess)
+    return fail(set_error(SDX_ERR_CUDA, "step graph: begin pass capture"));
+  if (temporal) {
+    launch_nt_temporal(d, c->n_slices, c->slice_env, sdx_context::kHist, c->dx_hist, c->dx, c->stream);
+    c->launches++;
+  }
+  launch_nt_pcg_prepare(d, c->stream);
+  cudaError_t le = launch_pcg_captured(a, P.n_cta, P.threads, c->stream);
+  c->launches += 2;
+  if (le != cudaSuccess)
+    return fail(set_error(SDX_ERR_CUDA, "step graph: PCG launch: %s", cudaGetErrorString(le)));
+  if (temporal) {
+    launch_nt_keep_hist(d, c->n_slices, c->slice_env, sdx_context::kHist, c->dx, c->dx_hist, c->stream);
+    c->launches++;
+  }
+  launch_copy_rows(c->n_slices, c->slice_env, c->env_mask, c->dx, c->dx_prev1, c->stream);
+  cudaMemsetAsync(d.nrm, 0, sizeof(double) * E, c->stream);
+  launch_env_dot(c->n_slices, c->slice_env, c->env_mask, c->dx, c->dx, d.nrm, c->stream);
+  launch_nt_after_solve(d, p.ls_max_iter, h_ls, c->stream);
+  launch_copy_rows(c->n_slices, c->slice_env, c->env_mask, c->u, c->ubase, c->stream);
+  c->launches += 4;
+  rc = capture_while(c, h_ls, &ls_body);
+  if (rc != SDX_OK) return fail(rc);
+  cudaMemsetAsync(d.unorm, 0, sizeof(double) * E, c->stream);
+  launch_env_dot(c->n_slices, c->slice_env, nullptr, c->u, c->u, d.unorm, c->stream);
+  launch_nt_control(d, k, h_loop, c->stream);
+  c->launches += 2;
+  zero_env_pairs(c, c->env_mask);
+  assemble_dev(c, c->u, c->ut, t_cap, SDX_ASM_HESS | SDX_ASM_PSD, c->env_mask, false, G.t_dev);
+  cudaGraph_t got = nullptr;
+  if (cudaStreamEndCapture(c->stream, &got) != cudaSuccess || got != body)
+    return fail(set_error(SDX_ERR_CUDA, "step graph: pass capture: %s", cudaGetErrorString(cudaGetLastError())));
+  G.k_pass = c->launches - l1;
+  // one line-search trial
+  const int64_t l2 = c->launches;
+  if (cudaStreamBeginCaptureToGraph(c->stream, ls_body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
+      cudaSuccess)
+    return fail(set_error(SDX_ERR_CUDA, "step graph: begin line-search capture"));
+  launch_nt_ls_scale(d, p.ls_alpha, c->stream);
+  launch_ls_candidate(c->n_slices, c->slice_env, d.lsmask, c->ubase, c->dx, d.scale, c->u, c->stream);
+  c->launches += 2;
+  zero_env_pairs(c, d.lsmask);
+  assemble_dev(c, c->u, c->ut, t_cap, SDX_ASM_RES, d.lsmask, false, G.t_dev);
+  cudaMemsetAsync(d.nrm, 0, sizeof(double) * E, c->stream);
+  launch_env_dot(c->n_slices, c->slice_env, d.lsmask, c->g, c->g, d.nrm, c->stream);
+  launch_nt_ls_check(d, p.ls_max_iter, h_ls, c->stream);
+  c->launches += 2;
+  if (cudaStreamEndCapture(c->stream, &got) != cudaSuccess || got != ls_body)
+    return fail(set_error(SDX_ERR_CUDA, "step graph: line-search capture: %s",
+                          cudaGetErrorString(cudaGetLastError())));
+  G.k_ls = c->launches - l2;
+  c->launches = l0;  // counted per executed launch in step_graph
+  c->profiling = prof;
+  const cudaError_t ie = cudaGraphInstantiate(&G.exec, G.graph, 0);
+  if (ie != cudaSuccess)
+    return fail(set_error(SDX_ERR_CUDA, "step graph: instantiate: %s", cudaGetErrorString(ie)));
+  G.params = p;
+  G.gen = c->topo_gen;
+  return SDX_OK;
+}
+
+static int step_graph(sdx_context* c) {
+  const sdx_step_params& p = c->params;
+  if (p.warm_start == SDX_WARM_LEARNED || c->ext_fn || p.linear.refine_inner_rel_tol > 0.0 ||
+      c->collect_per_solve > 0)
+    return set_error(SDX_ERR_UNSUPPORTED,
+                     "a graph-captured step takes the zero, previous or temporal start with the library's PCG "
+                     "(no learned start, external solver, refinement or training capture)");
+  StepGraph& G = c->sg;
+  if (!G.exec || G.gen != c->topo_gen || memcmp(&G.params, &p, sizeof(p)) != 0) SDX_TRY(build_step_graph(c));
+  const int E = c->n_envs;
+  const double t_end = c->time + p.dt;
+  int hv[sdx_context::kHist];
+  for (int k = 0; k < sdx_context::kHist; ++k) hv[k] = c->hist_valid[k] ? 1 : 0;
+  SDX_CUDA(cudaMemcpyAsync(G.d.hist_valid, hv, sizeof(hv), cudaMemcpyHostToDevice, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(G.t_dev, &t_end, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  SDX_CUDA(cudaGraphLaunch(G.exec, c->stream));
+  std::vector<int> st(E), it(E), cg(E), ls(E);
+  std::vector<double> r0(E), r(E);
+  std::vector<unsigned long long> pairs(E);
+  int ctl[8];
+  SDX_CUDA(cudaMemcpyAsync(st.data(), G.d.status, sizeof(int) * E, cudaMemcpyDeviceToHost, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(it.data(), G.d.iters, sizeof(int) * E, cudaMemcpyDeviceToHost, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(cg.data(), G.d.cg, sizeof(int) * E, cudaMemcpyDeviceToHost, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(ls.data(), G.d.lsi, sizeof(int) * E, cudaMemcpyDeviceToHost, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(r0.data(), G.d.res0, sizeof(double) * E, cudaMemcpyDeviceToHost, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(r.data(), G.d.res, sizeof(double) * E, cudaMemcpyDeviceToHost, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(pairs.data(), c->env_pairs, sizeof(unsigned long long) * E, cudaMemcpyDeviceToHost,
+                           c->stream));
+  SDX_CUDA(cudaMemcpyAsync(ctl, G.d.ctl, sizeof(ctl), cudaMemcpyDeviceToHost, c->stream));
+  SDX_CUDA(cudaMemcpyAsync(hv, G.d.hist_valid, sizeof(hv), cudaMemcpyDeviceToHost, c->stream));
+  SDX_CUDA(cudaStreamSynchronize(c->stream));
+  if (ctl[5] & 1) return set_error(SDX_ERR_DEVICE_TIMEOUT, "PCG grid barrier timed out in a graph step");
+  for (int k = 0; k < sdx_context::kHist; ++k) c->hist_valid[k] = hv[k] != 0;
+  for (int e = 0; e < E; ++e) {
+    sdx_env_stats& s = c->stats[e];
+    s.newton_iters = it[e];
+    s.cg_iters = cg[e];
+    s.ls_iters = ls[e];
+    s.convergence = st[e];
+    s.res_norm0 = r0[e];
+    s.res_norm = r[e];
+    s.n_contacts = (int64_t)pairs[e];
+  }
+  // kernels executed: the prologue and epilogue, every pass (ctl[2]) and every line-search trial (ctl[7])
+  c->launches += G.k_pro + (int64_t)ctl[2] * G.k_pass + (int64_t)ctl[7] * G.k_ls;
+  c->time = t_end;
+  return SDX_OK;
+}
+
 extern "C" int sdx_step(sdx_context* c, int n_steps) {
   if (!c || !c->uploaded) return set_error(SDX_ERR_NOT_READY, "upload bodies first");
   if (n_steps < 0) return set_error(SDX_ERR_INVALID_ARGUMENT, "negative step count");
   cudaSetDevice(c->device);
-  for (int k = 0; k < n_steps; ++k) SDX_TRY(step_once(c));
+  for (int k = 0; k < n_steps; ++k) SDX_TRY(c->params.newton_graph ? step_graph(c) : step_once(c));
   SDX_CUDA(cudaGetLastError());
   return SDX_OK;
 }

@@ -113,6 +113,7 @@ struct ContactArgs {
   double viscous, normal_damping;  // viscousFrictionCoefficient / dt, normalViscousDampingCoefficient / dt
   int cflags;         // kContact* bits
   int threads;        // CTA size: 64, 128 or 256 (anything else: 128)
+  const double* t_dev;  // evaluation time in device memory (NULL: t); the stage start is then t_dev - (t - t0)
 };
 
 // ContactArgs::cflags
@@ -158,6 +159,7 @@ struct PcgArgs {
   int polak_ribiere;
   int replace_every;
   int zero_guess;
+  const int* zero_guess_dev;  // zero_guess read from device memory at launch start (NULL: zero_guess)
   int scale_guess;  // non-zero guess: replace x0 by alpha x0, alpha = (x0.b)/(x0.A x0) (energy-optimal)
   int abort_spd;
   int* out_iters;
@@ -195,6 +197,54 @@ struct PcgArgs {
   int cl_n;
   const int* env_soff;
 };
+
+// Device-resident Newton state of a step run as one CUDA graph (the Newton loop and the line search as
+// conditional while-nodes): per env the stop-test state of NewtonSolver<T>::Solve, the masks the kernels
+// read, and the control words the decision kernels write.
+struct NewtonDev {
+  int n_envs;
+  int* status;      // 0 iterating, 1 converged, 2 stopped, 3 diverged
+  int* iters;       // Newton iterations
+  int* cg;          // CG iterations summed over the step
+  int* lsi;         // line-search evaluations
+  double* res0;     // residual norm at the first iteration
+  double* res;      // current residual norm
+  double* res_prev; // at the previous iteration (Eisenstat-Walker)
+  double* dxn;      // ||dx|| of the last update
+  double* eta;      // per-env linear tolerance (Eisenstat-Walker), read by the PCG
+  uint8_t* mask;    // envs of the current Newton pass (the kernels' env mask)
+  uint8_t* lsmask;  // envs still in the line search
+  double* scale;    // line-search step per env
+  double* nrm;      // per-env sums of squares written by k_env_dot
+  double* unorm;    // per-env ||u||^2
+  int* ctl;         // [0] envs in the pass, [1] line-search envs left, [2] Newton pass, [3] line-search trial,
+                    // [4] zero-start flag of the PCG, [5] error bits (1: PCG barrier timed out), [6] first control,
+                    // [7] line-search trials of the step
+  int* hist_valid;  // per Newton pass: the temporal history holds that pass's update
+  int* pcg_iters;         // CG iterations of the last solve, per env
+  unsigned* pcg_sync;     // the PCG's control words (reset before each solve; [2] its error word)
+  int* pcg_conv;
+  const int* env_nrows;   // rows per env
+};
+
+// Newton stop-test constants (NonLinearSolverParams)
+struct NewtonConsts {
+  double abs_tol, rel_tol, rel_step_tol, rel_div_tol, abs_div_tol, lin_rel_tol, ls_alpha;
+  int max_iter, ls_max_iter, ew_forcing;
+};
+
+cudaError_t launch_pcg_captured(const PcgArgs& a, int n_cta, int threads, cudaStream_t st);
+void launch_nt_begin(const NewtonDev& d, const NewtonConsts& k, cudaStream_t st);
+void launch_nt_control(const NewtonDev& d, const NewtonConsts& k, cudaGraphConditionalHandle loop,
+                       cudaStream_t st);
+void launch_nt_pcg_prepare(const NewtonDev& d, cudaStream_t st);
+void launch_nt_temporal(const NewtonDev& d, int n_slices, const int* slice_env, int hist_len, const double* hist,
+                        double* dx, cudaStream_t st);
+void launch_nt_keep_hist(const NewtonDev& d, int n_slices, const int* slice_env, int hist_len, const double* dx,
+                         double* hist, cudaStream_t st);
+void launch_nt_after_solve(const NewtonDev& d, int ls_max_iter, cudaGraphConditionalHandle ls, cudaStream_t st);
+void launch_nt_ls_scale(const NewtonDev& d, double alpha, cudaStream_t st);
+void launch_nt_ls_check(const NewtonDev& d, int ls_max_iter, cudaGraphConditionalHandle ls, cudaStream_t st);
 
 struct ClusterShape {
   int n_clusters, size;

@@ -412,6 +412,9 @@ __global__ void __launch_bounds__(256) k_contact(ContactArgs a) {
   const int q = (int)(sidx - 3 * f);
   const int4 fr = a.faces[f];
   const int env = fr.w;
+  // the evaluation time: a launch captured once into a graph reads it from device memory
+  const double t_now = a.t_dev ? *a.t_dev : a.t;
+  const double t_stage = t_now - (a.t - a.t0);
   unsigned bits = 0;
   if (!a.env_mask || a.env_mask[env]) {
     const int rows[3] = {fr.x, fr.y, fr.z};
@@ -449,8 +452,8 @@ __global__ void __launch_bounds__(256) k_contact(ContactArgs a) {
     for (int c = c0; c < c1; ++c) {
       const double* crow = a.colliders + 11 * (int64_t)c;
       double d, gr[3], d0 = 0.0, gr0[3] = {0.0, 0.0, 0.0};
-      collider_sdf(crow, xs, a.t, d, gr);
-      if (need_ss) collider_sdf(crow, xs0, a.t0, d0, gr0);
+      collider_sdf(crow, xs, t_now, d, gr);
+      if (need_ss) collider_sdf(crow, xs0, t_stage, d0, gr0);
       const bool cur = d < a.thr;
       if (!cur && !(expl && d0 < a.thr)) continue;
       if (!cur) {  // in contact at the stage start only
@@ -482,7 +485,7 @@ __global__ void __launch_bounds__(256) k_contact(ContactArgs a) {
                                 : 1.0;
         double prel[3];
 #pragma unroll
-        for (int r = 0; r < 3; ++r) prel[r] = (xs[r] - crow[8 + r] * a.t) - (xs0[r] - crow[8 + r] * a.t0);
+        for (int r = 0; r < 3; ++r) prel[r] = (xs[r] - crow[8 + r] * t_now) - (xs0[r] - crow[8 + r] * t_stage);
         double fP;
         if (a.cflags & kContactImplicitFn) {
           fP = afac * fn;
@@ -1250,7 +1253,8 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
 
   if (!a.resume) {
     // ---- phase 0: r = b - A x0, z = M^-1 r, partials b.b, r.r, r.z ----
-    const bool scaled = !a.zero_guess && a.scale_guess;
+    const bool zero_guess = a.zero_guess_dev ? (*a.zero_guess_dev != 0) : (a.zero_guess != 0);
+    const bool scaled = !zero_guess && a.scale_guess;
     const bool two = scaled && a.x2 != nullptr;
     if (two) {
       // Galerkin start on span{x, x2} (the temporal guess and the learned correction): with Ah = A x,
@@ -1405,14 +1409,14 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
           for (int j = 0; j < 3; ++j) a.dinv[9 * row + 3 * i + j] = cof[3 * j + i] * inv;
       }
       double r[3];
-      if (a.zero_guess) {
+      if (zero_guess) {
   #pragma unroll
         for (int k = 0; k < 3; ++k) {
           a.x[3 * row + k] = 0.0;
           r[k] = a.b[3 * row + k];
         }
       }
-      if (!a.zero_guess && !scaled) true_residual<kB64>(a, s, lane, r);
+      if (!zero_guess && !scaled) true_residual<kB64>(a, s, lane, r);
       if (two) {
   #pragma unroll
         for (int k = 0; k < 3; ++k) r[k] = a.r[3 * row + k];
@@ -1927,7 +1931,8 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
     const int c0 = sa + (int)((int64_t)ns * rank / csize), c1 = sa + (int)((int64_t)ns * (rank + 1) / csize);
 
     // ---- phase 0: diagonal, start vector, r0, z0 ----
-    const bool scaled = !a.zero_guess && a.scale_guess;
+    const bool zero_guess = a.zero_guess_dev ? (*a.zero_guess_dev != 0) : (a.zero_guess != 0);
+    const bool scaled = !zero_guess && a.scale_guess;
     const bool two = scaled && a.x2 != nullptr;
     double al0 = 0.0;
     if (two) {
@@ -2046,7 +2051,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
           for (int j = 0; j < 3; ++j) a.dinv[9 * row + 3 * i + j] = cof[3 * j + i] * inv;
       }
       double r[3];
-      if (a.zero_guess) {
+      if (zero_guess) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
           a.x[3 * row + k] = 0.0;
@@ -2411,6 +2416,26 @@ cudaError_t launch_pcg(const PcgArgs& a, int n_cta, int threads, cudaStream_t st
                        : (timed ? (const void*)k_pcg<false, true> : (const void*)k_pcg<false, false>);
   return cudaLaunchCooperativeKernel(fn, dim3(n_cta), dim3(threads), params,
                                      (size_t)pcg_shared_bytes(threads, args.wstride), st);
+}
+
+// The same launch through cudaLaunchKernelEx with the cooperative attribute, the form a graph's kernel
+// node records (steps captured into a CUDA graph); no per-CTA timers.
+cudaError_t launch_pcg_captured(const PcgArgs& a, int n_cta, int threads, cudaStream_t st) {
+  PcgArgs args = a;
+  args.wstride = (a.wstride > 0 && a.wstride < kPcgMaxEnvsPerCta) ? a.wstride : kPcgMaxEnvsPerCta;
+  args.cta_ns = nullptr;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(n_cta);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = (size_t)pcg_shared_bytes(threads, args.wstride);
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return pcg_pipelined(threads) ? cudaLaunchKernelEx(&cfg, k_pcg<true, false>, args)
+                                : cudaLaunchKernelEx(&cfg, k_pcg<false, false>, args);
 }
 
 }  // namespace sdx

@@ -74,9 +74,47 @@ def mlp_case(rows: int, reps: int):
     return {"case": "mlp", "rows": rows, "reps": reps, "flops_per_forward": mlp_flops_per_row() * rows}
 
 
+def step_case(args):
+    """Host-driven steps against graph-captured steps (sdx_step_params.newton_graph) on the same workload:
+    wall time per step of `--iters` steps after 2 warm-up steps, from the same state, with the Newton and
+    CG counts of each."""
+    import time
+    import torch
+    if args.workload == "batch":
+        bodies, cfg = scenes.config2(args.seed, n_envs=args.envs)
+    elif args.cells <= 10:
+        bodies, cfg = scenes.config0(args.seed)
+    else:
+        bodies, cfg = scenes.config1(args.seed, n=args.cells)
+    out = {"case": "step", "workload": args.workload, "cells": args.cells, "n_envs": len(bodies),
+           "warm_start": args.warm}
+    for graph in (0, 1):
+        w = SoftBodyWorld(bodies, cfg, newton_abs_tol=1e-9, newton_max_iter=12 if args.workload == "batch" else 50,
+                          warm_start=args.warm, newton_graph=graph)
+        w.step(2)
+        torch.cuda.synchronize()
+        l0 = w.kernel_launches()
+        t0 = time.perf_counter()
+        newton = cg = 0
+        for _ in range(args.iters):
+            w.step(1)
+            st = w.stats()
+            newton += sum(s["newton_iters"] for s in st)
+            cg += sum(s["cg_iters"] for s in st)
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / args.iters
+        key = "graph" if graph else "host"
+        out[key] = {"ms_per_step": dt * 1e3, "newton_per_step": newton / args.iters, "cg_per_step": cg / args.iters,
+                    "launches_per_step": (w.kernel_launches() - l0) / args.iters}
+        w.close()
+    out["graph_over_host"] = out["host"]["ms_per_step"] / out["graph"]["ms_per_step"]
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("case", choices=["pcg", "element", "spmv", "mlp"])
+    ap.add_argument("case", choices=["pcg", "element", "spmv", "mlp", "step"])
+    ap.add_argument("--warm", type=int, default=0, help="step: warm start (SDX_WARM_*: 0 zero, 1 previous, 3 temporal)")
     ap.add_argument("--rows", type=int, default=274656, help="mlp: feature rows per forward")
     ap.add_argument("--workload", choices=["cube", "batch"], default="cube")
     ap.add_argument("--cells", type=int, default=64)
@@ -89,6 +127,9 @@ def main(argv=None):
     args = ap.parse_args(argv)
     if args.case == "mlp":
         print(json.dumps(mlp_case(args.rows, args.reps)))
+        return
+    if args.case == "step":
+        print(json.dumps(step_case(args)))
         return
     if args.workload == "batch":
         bodies, cfg = scenes.config2(args.seed, n_envs=args.envs)
