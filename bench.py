@@ -383,6 +383,17 @@ def max_over_ranks(x, dist, local_rank):
 REFINE_INNER_REL_TOL = 1e-2
 
 
+def pcg_split(prof):
+    """Algorithmic GB/s of the PCG solves by kernel: the cluster kernel (long queues of envs) and the grid
+    kernel (the rest)."""
+    out = {}
+    cm, cb = prof.get("pcg_cluster_ms", 0.0), prof.get("pcg_cluster_bytes", 0.0)
+    gm, gb = prof.get("pcg_ms", 0.0) - cm, prof.get("pcg_bytes", 0.0) - cb
+    for name, ms, by in (("cluster", cm, cb), ("grid", gm, gb)):
+        out[name] = {"ms": ms, "gbs": by / (ms * 1e-3) / 1e9 if ms > 0 else None}
+    return out
+
+
 def set_arm(w, arm, params):
     from project_superdex_b200 import capi
     from project_superdex_b200.learned import Mlp
@@ -588,7 +599,8 @@ def run_ours(args, rank, world, local_rank):
                    "cg_iters_per_env_step": head["cg_per_env_step"],
                    "pcg_launch_iters": prof["pcg_iters"], "pcg_launches": prof["pcg_launches"],
                    "pcg_cluster_solves": int(prof.get("pcg_cluster_solves", 0)),
-                   "profile_ms": {k: v for k, v in prof.items() if k.endswith("_ms")}},
+                   "profile_ms": {k: v for k, v in prof.items() if k.endswith("_ms")},
+                   "pcg_gbs_by_kernel": pcg_split(prof)},
     }
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_oracle_run(args, seed0, steps=3, warmup=0, tet_budget=args.cpu_tets)

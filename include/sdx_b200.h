@@ -403,6 +403,8 @@ typedef struct {
   int64_t contact_threads;    /* contact kernel CTA size */
   double tune_elem_us;        /* assembly tuner: fastest Hessian element launch (0: not tuned) */
   double tune_elem_default_us;/* the same launch with the default shape (128 threads, plain scatter) */
+  double pcg_cluster_ms;      /* the share of pcg_ms spent in cluster-kernel solves */
+  double pcg_cluster_bytes;   /* the share of pcg_bytes of those solves */
 } sdx_profile;
 /* enable: 0 off, 1 per-kernel event timing, 2 also the per-CTA PCG phase timers (sdx_get_pcg_cta_profile) */
 int sdx_set_profiling(sdx_context* ctx, int enable);

@@ -104,7 +104,8 @@ class Profile(C.Structure):
                 ("warm_launches", C.c_int64), ("pcg_cluster_solves", C.c_int64), ("pcg_cluster_size", C.c_int64),
                 ("tune_grid_us", C.c_double), ("tune_cluster_us", C.c_double),
                 ("elem_threads", C.c_int64), ("elem_res_threads", C.c_int64), ("elem_aggregated", C.c_int64),
-                ("contact_threads", C.c_int64), ("tune_elem_us", C.c_double), ("tune_elem_default_us", C.c_double)]
+                ("contact_threads", C.c_int64), ("tune_elem_us", C.c_double), ("tune_elem_default_us", C.c_double),
+                ("pcg_cluster_ms", C.c_double), ("pcg_cluster_bytes", C.c_double)]
 
 
 _dp = C.POINTER(C.c_double)

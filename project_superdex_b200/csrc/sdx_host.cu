@@ -345,7 +345,7 @@ struct sdx_context {
   std::vector<Pending> pending;
 };
 
-enum { PROF_PCG = 0, PROF_HESS = 1, PROF_RES = 2, PROF_CONTACT = 3, PROF_SEED = 4, PROF_WARM = 5 };
+enum { PROF_PCG = 0, PROF_HESS = 1, PROF_RES = 2, PROF_CONTACT = 3, PROF_SEED = 4, PROF_WARM = 5, PROF_PCG_CLUSTER = 6 };
 
 static cudaEvent_t pool_event(sdx_context* c) {
   if (!c->ev_pool.empty()) {
@@ -380,6 +380,10 @@ static void prof_resolve(sdx_context* c) {
     switch (pd.kind) {
       case PROF_PCG:
         c->prof.pcg_ms += ms;
+        break;
+      case PROF_PCG_CLUSTER:
+        c->prof.pcg_ms += ms;
+        c->prof.pcg_cluster_ms += ms;
         break;
       case PROF_HESS:
         c->prof.asm_hess_ms += ms;
@@ -885,8 +889,9 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
   SDX_CUDA(cudaMemsetAsync(W.out_conv, 0, sizeof(int) * n_envs, c->stream));
   cudaEvent_t ev;
   prof_begin(c, &ev);
+  bool on_cluster = false;  // this solve ran on the cluster kernel
   auto finish = [&]() -> int {
-    prof_end(c, PROF_PCG, ev);
+    prof_end(c, on_cluster ? PROF_PCG_CLUSTER : PROF_PCG, ev);
     if (c->profiling) {
       std::vector<int> its(n_envs);
       SDX_CUDA(cudaMemcpy(its.data(), W.out_iters, sizeof(int) * n_envs, cudaMemcpyDeviceToHost));
@@ -898,9 +903,11 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
         // vector bytes per row: 228 with FP64 r and x; r carried by z saves its FP64 read and write (48),
         // x carried by its FP32 increment half of x's (24)
         const double per_row = 228.0 - (a.r_in_z && a.precond != 2 ? 72.0 : 0.0);
+        double by = 0.0;
         for (int e = 0; e < n_envs; ++e)
-          c->prof.pcg_bytes += its[e] * (c->h_env_pcg_bytes[e] +
-                                         per_row * (double)(c->h_node_off[e + 1] - c->h_node_off[e]));
+          by += its[e] * (c->h_env_pcg_bytes[e] + per_row * (double)(c->h_node_off[e + 1] - c->h_node_off[e]));
+        c->prof.pcg_bytes += by;
+        if (on_cluster) c->prof.pcg_cluster_bytes += by;
       }
     }
     return SDX_OK;
@@ -954,6 +961,7 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
       SDX_CUDA(cudaStreamSynchronize(c->stream));
       if (flags[2] != 0u) return set_error(SDX_ERR_DEVICE_TIMEOUT, "PCG cluster barrier timed out");
       if (c->profiling) c->prof.pcg_cluster_solves++;
+      on_cluster = true;
       return finish();
     }
   }

@@ -1646,7 +1646,7 @@ __global__ void __launch_bounds__(kPipe ? 512 : 1024, 1) k_pcg(PcgArgs a) {
           else
             a.x[d0 + dl] = xo[j] + al * (double)pp[j];
           const double rp =
-              !a.r_in_z ? ro[j] : (a.precond == 1 ? (double)zo[j] / (double)dd[j] : (double)zo[j]);
+              !a.r_in_z ? ro[j] : (a.precond == 1 ? (double)(zo[j] / dd[j]) : (double)zo[j]);
           const double r = rp - al * (double)qq[j];
           if (!a.r_in_z) a.r[d0 + dl] = r;
           const float z = (float)(dd[j] * r);
@@ -2100,8 +2100,10 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
 
     // ---- iterations ----
     for (int it = 1; status == 0; ++it) {
-      // phase 1: p = z + beta p, q = A z + beta q, p.q (vector updates DoF-linear, as in k_pcg)
+      // phase 1: p = z + beta p, q = A z + beta q, p.q (vector updates DoF-linear, as in k_pcg); every slice of
+      // the CTA belongs to its one env, so each lane sums its slices and the warp reduces once per phase
       acc_reset();
+      double pq_sum = 0.0;
       for (int s = c0 + warp; s < c1; s += nwarps) {
         if (a.prefetch && s + nwarps < c1) prefetch_slice_matrix(a.A, s + nwarps, lane);
         const int64_t d0 = (int64_t)s * (3 * kSlice);
@@ -2132,8 +2134,9 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
           pq += (double)pn * qn;
         }
         __syncwarp();
-        acc_add(0, pq);
+        pq_sum += pq;
       }
+      acc_add(0, pq_sum);
       if (!reduce(1)) {
         fail = true;
         break;
@@ -2149,6 +2152,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
       // phase 2: x += alpha p, r -= alpha q, z = M^-1 r, r.r, r.z_old, r.z (DoF-linear unless block Jacobi)
       acc_reset();
       if (a.precond != 2) {
+        double rr_sum = 0.0, rzo_sum = 0.0, rz_sum = 0.0;  // this lane's sums over the warp's slices
         const int ahead = a.prefetch;  // prefetch distance in this warp's slices (as in k_pcg)
         for (int k = 0; k < ahead && c0 + warp + k * nwarps < c1; ++k)
           prefetch_update_operands(a, c0 + warp + k * nwarps, lane);
@@ -2200,7 +2204,7 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
             else
               a.x[d0 + dl] = xo[j] + al * (double)pp[j];
             const double rp =
-                !a.r_in_z ? ro[j] : (a.precond == 1 ? (double)zo[j] / (double)dd[j] : (double)zo[j]);
+                !a.r_in_z ? ro[j] : (a.precond == 1 ? (double)(zo[j] / dd[j]) : (double)zo[j]);
             const double r = rp - al * (double)qq[j];
             if (!a.r_in_z) a.r[d0 + dl] = r;
             const float z = (float)(dd[j] * r);
@@ -2212,10 +2216,13 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
           __syncwarp();
           a.z[(int64_t)s * kSlice + lane] = make_float4(tr[3 * lane], tr[3 * lane + 1], tr[3 * lane + 2], 0.0f);
           __syncwarp();
-          acc_add(0, rr2);
-          acc_add(1, rzo2);
-          acc_add(2, rz2);
+          rr_sum += rr2;
+          rzo_sum += rzo2;
+          rz_sum += rz2;
         }
+        acc_add(0, rr_sum);
+        acc_add(1, rzo_sum);
+        acc_add(2, rz_sum);
       } else {
         for (int s = c0 + warp; s < c1; s += nwarps) {
           const int64_t row = (int64_t)s * kSlice + lane;
