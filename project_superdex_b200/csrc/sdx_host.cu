@@ -783,6 +783,8 @@ static int alloc_work(PcgWork& W, int64_t n_rows, int n_envs, bool newton_vector
 
 // Prefetch distance (in a warp's slices) of the PCG update phase when the vectors stream from HBM.
 constexpr int kPcgPrefetchAhead = 3;
+// Stage buffers per warp of the cluster PCG's update phase when the vectors stream from HBM.
+constexpr int kPcgStageDepth = 2;
 
 // Runs the persistent PCG on matrix A for the envs in env_mask (NULL = all), b -> x.
 // share of the rows still iterating at which a batched PCG launch re-partitions
@@ -848,6 +850,13 @@ static int pcg_base_args(sdx_context* c, const Matrix& A, const int* diag_pos, i
     return v ? (atoi(v) != 0) : -1;
   }();
   a.r_in_z = r_in_z_env >= 0 ? r_in_z_env : (streamed ? 1 : 0);
+  // The cluster kernel's update phase brings each warp's next kPcgStageDepth slices of operands into shared
+  // memory with bulk asynchronous copies when they stream from HBM (Jacobi, z carrying r); SDX_PCG_STAGE sets
+  // the depth (0: off, 1 is taken as 2, at most 4).
+  const char* stage_env = getenv("SDX_PCG_STAGE");
+  const int depth = stage_env ? std::min(4, atoi(stage_env) == 1 ? 2 : std::max(0, atoi(stage_env)))
+                              : (streamed ? kPcgStageDepth : 0);
+  a.stage_update = (a.r_in_z && lp.preconditioner == 1) ? depth : 0;
   a.es = W.es;
   return SDX_OK;
 }

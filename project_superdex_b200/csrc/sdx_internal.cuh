@@ -173,6 +173,9 @@ struct PcgArgs {
                  // (r = z / d, FP32 precision) and x by its FP64 value at the last replacement plus the FP32
                  // increment xi, so the update phase reads and writes no FP64 vector
   float* xi;     // FP32 increment of x since the last true-residual replacement (r_in_z)
+  int stage_update;  // cluster PCG, Jacobi, z carrying r: the update phase's operands of a warp's next
+                     // stage_update (2..4; 0: off) slices are brought into shared memory by bulk asynchronous
+                     // copies (one mbarrier per buffer)
   int prefetch;  // bulk L2 prefetch of each warp's next slices (0: none): the update phase's distance in
                  // slices (the matrix of the next slice in the SpMV phase whenever it is set); set when the
                  // CG vectors cannot stay in L2, so every operand comes from HBM

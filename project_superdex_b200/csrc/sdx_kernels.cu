@@ -1839,6 +1839,52 @@ __device__ __forceinline__ void cluster_hw_sync() {
 
 // Software cluster barrier (every thread of every CTA calls it): arrivals counted on CTA 0's shared
 // counter with a cluster-scope release, the poll acquires. false when the wait gave up (error recorded).
+// Staged update phase of the cluster PCG: per warp 2 to 4 buffers of one slice's operands (x increment,
+// p, q, Jacobi diagonal: 96 floats each; z: 32 float4 rows), filled by bulk asynchronous copies whose bytes
+// an mbarrier per buffer counts.
+constexpr int kClMaxStages = 4;  // buffers per warp: PcgArgs::stage_update (2..4) of them are used
+constexpr int kClStageBytes = 4 * (3 * kSlice * 4) + kSlice * 16;  // 2,048
+constexpr int kClWarps = 16;
+__host__ __device__ constexpr int cl_dyn_smem(int stages) { return kClWarps * stages * (kClStageBytes + 8); }
+
+__device__ __forceinline__ uint32_t shared_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
+}
+
+// bounded wait for the completion of phase `parity` of the mbarrier at `bar`; false on timeout
+__device__ __forceinline__ bool stage_wait(uint32_t bar, uint32_t parity, long long limit) {
+  for (long long i = 0; i < limit; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// lane 0: the copies of slice s's update operands into stage buffer `buf` (all addresses 16-byte aligned, all
+// sizes multiples of 16 bytes: the vectors start on 256-byte boundaries and a slice is 384 / 512 bytes)
+__device__ __forceinline__ void stage_issue(const PcgArgs& a, int s, uint32_t buf, uint32_t bar) {
+  const int64_t d0 = (int64_t)s * (3 * kSlice);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // earlier generic reads of the buffer first
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"((uint32_t)kClStageBytes)
+               : "memory");
+  bulk_g2s(buf, a.xi + d0, 3 * kSlice * 4, bar);
+  bulk_g2s(buf + 384, a.p + d0, 3 * kSlice * 4, bar);
+  bulk_g2s(buf + 768, a.q + d0, 3 * kSlice * 4, bar);
+  bulk_g2s(buf + 1152, a.dinv + d0, 3 * kSlice * 4, bar);
+  bulk_g2s(buf + 1536, a.z + (int64_t)s * kSlice, kSlice * 16, bar);
+}
+
 __device__ __forceinline__ bool cluster_sync(uint32_t cnt, unsigned n, long long limit, unsigned* err, int* s_ok) {
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -1871,11 +1917,28 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
   __shared__ unsigned s_cnt;           // the cluster barrier counter (used in CTA 0)
   __shared__ int s_env, s_env_here, s_ok;
   __shared__ float s_tr[16 * 3 * kSlice];  // per warp: a slice's row products, DoF order
+  __shared__ int s_stage_fail;              // a warp's staged copy did not arrive in time
+  extern __shared__ __align__(128) unsigned char cl_dyn[];  // staged update phase (cl_dyn_smem bytes)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   float* const tr = s_tr + warp * (3 * kSlice);
   const float* const zf = reinterpret_cast<const float*>(a.z);
   const uint32_t rank = cluster_rank(), csize = cluster_size();
-  if (threadIdx.x == 0) s_cnt = 0u;
+  // this warp's stage buffers and their mbarriers; ph holds the parity each buffer waits for next
+  const int nst = a.stage_update;  // stage buffers per warp (0: the update phase reads global memory)
+  const uint32_t stage_buf = shared_u32(cl_dyn) + (uint32_t)(warp * nst * kClStageBytes);
+  const uint32_t stage_bar = shared_u32(cl_dyn) + (uint32_t)(kClWarps * nst * kClStageBytes + warp * nst * 8);
+  const unsigned char* const stage_ptr = cl_dyn + warp * nst * kClStageBytes;
+  uint32_t ph = 0u;
+  if (nst > 0 && lane == 0) {
+    for (int b = 0; b < nst; ++b)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(stage_bar + 8u * b), "r"(1u) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  if (threadIdx.x == 0) {
+    s_cnt = 0u;
+    s_stage_fail = 0;
+  }
   cluster_hw_sync();  // every CTA's shared memory is live before any remote access
   const uint32_t cnt = cluster_map(&s_cnt, 0);
   const uint32_t env0 = cluster_map(&s_env, 0);
@@ -2151,7 +2214,73 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
       const bool replace = (verify_it > 0 && verify_it == it - 1) || (a.replace_every > 0 && it % a.replace_every == 0);
       // phase 2: x += alpha p, r -= alpha q, z = M^-1 r, r.r, r.z_old, r.z (DoF-linear unless block Jacobi)
       acc_reset();
-      if (a.precond != 2) {
+      if (nst > 0 && !replace && a.precond == 1 && a.r_in_z) {
+        // the operands of the warp's next nst slices are in flight into shared memory while it updates one
+        double rr_sum = 0.0, rzo_sum = 0.0, rz_sum = 0.0;
+        uint32_t pending = 0u;  // buffers with copies issued and not yet waited for
+        bool ok = true;
+        if (lane == 0)
+          for (int b = 0; b < nst; ++b) {
+            const int sb = c0 + warp + b * nwarps;
+            if (sb < c1) stage_issue(a, sb, stage_buf + (uint32_t)(b * kClStageBytes), stage_bar + 8u * b);
+          }
+        for (int b = 0; b < nst; ++b)
+          if (c0 + warp + b * nwarps < c1) pending |= 1u << b;
+        int k = 0;
+        for (int s = c0 + warp; s < c1; s += nwarps, ++k) {
+          const int b = k % nst;
+          const bool got = stage_wait(stage_bar + 8u * b, (ph >> b) & 1u, a.spin_limit);
+          if (!__all_sync(0xffffffffu, got)) {
+            ok = false;
+            break;
+          }
+          ph ^= 1u << b;
+          pending &= ~(1u << b);
+          const float* const sx = reinterpret_cast<const float*>(stage_ptr + b * kClStageBytes);
+          const float* const sp = sx + 3 * kSlice;
+          const float* const sq = sp + 3 * kSlice;
+          const float* const sd = sq + 3 * kSlice;
+          const float* const sz = sd + 3 * kSlice;  // 32 float4 rows
+          const int64_t d0 = (int64_t)s * (3 * kSlice);
+          double rr2 = 0.0, rzo2 = 0.0, rz2 = 0.0;
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            const int dl = lane + 32 * j;
+            const float zo = sz[4 * (dl / 3) + dl % 3], dd = sd[dl], pp = sp[dl], qq = sq[dl];
+            a.xi[d0 + dl] = (float)((double)sx[dl] + al * (double)pp);
+            const double r = (double)(zo / dd) - al * (double)qq;
+            const float z = (float)(dd * r);
+            tr[dl] = z;
+            rr2 += r * r;
+            rzo2 += r * zo;
+            rz2 += r * z;
+          }
+          __syncwarp();
+          a.z[(int64_t)s * kSlice + lane] = make_float4(tr[3 * lane], tr[3 * lane + 1], tr[3 * lane + 2], 0.0f);
+          __syncwarp();  // every lane is done with buffer b and with tr
+          rr_sum += rr2;
+          rzo_sum += rzo2;
+          rz_sum += rz2;
+          const int sn = s + nst * nwarps;
+          if (sn < c1) {
+            if (lane == 0) stage_issue(a, sn, stage_buf + (uint32_t)(b * kClStageBytes), stage_bar + 8u * b);
+            pending |= 1u << b;
+          }
+        }
+        if (!ok) {
+          // the copies still in flight land before the warp leaves (bounded again); the CTA stops after the
+          // reduction below and the error word makes the host return SDX_ERR_DEVICE_TIMEOUT
+          for (int b = 0; b < nst; ++b)
+            if (pending & (1u << b)) stage_wait(stage_bar + 8u * b, (ph >> b) & 1u, a.spin_limit);
+          if (lane == 0) {
+            atomicExch(err, 1u);
+            s_stage_fail = 1;
+          }
+        }
+        acc_add(0, rr_sum);
+        acc_add(1, rzo_sum);
+        acc_add(2, rz_sum);
+      } else if (a.precond != 2) {
         double rr_sum = 0.0, rzo_sum = 0.0, rz_sum = 0.0;  // this lane's sums over the warp's slices
         const int ahead = a.prefetch;  // prefetch distance in this warp's slices (as in k_pcg)
         for (int k = 0; k < ahead && c0 + warp + k * nwarps < c1; ++k)
@@ -2278,6 +2407,10 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
         fail = true;
         break;
       }
+      if (s_stage_fail) {  // read after the reduction's barriers: the same verdict in every thread of the CTA
+        fail = true;
+        break;
+      }
       it_done = it;
       rr = s_tot[0];
       const double rzo = s_tot[1], rzn = s_tot[2];
@@ -2350,6 +2483,7 @@ static const int* pcg_cluster_counts(int* last_error) {
   static const std::array<int, 4> counts = [] {
     std::array<int, 4> n{0, 0, 0, 0};
     cudaFuncSetAttribute(k_pcg_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    cudaFuncSetAttribute(k_pcg_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, cl_dyn_smem(kClMaxStages));
     for (int i = 0; i < 4; ++i) {
       cudaLaunchConfig_t cfg = {};
       cudaLaunchAttribute attr[1];
@@ -2359,6 +2493,7 @@ static const int* pcg_cluster_counts(int* last_error) {
       attr[0].val.clusterDim.z = 1;
       cfg.gridDim = dim3(kClSizes[i]);
       cfg.blockDim = dim3(512);
+      cfg.dynamicSmemBytes = cl_dyn_smem(kClMaxStages);  // the largest staging the launches use
       cfg.attrs = attr;
       cfg.numAttrs = 1;
       const cudaError_t e = cudaOccupancyMaxActiveClusters(&n[i], k_pcg_cluster, &cfg);
@@ -2406,7 +2541,7 @@ cudaError_t launch_pcg_cluster(const PcgArgs& a, ClusterShape shape, cudaStream_
   attr[0].val.clusterDim.z = 1;
   cfg.gridDim = dim3(shape.n_clusters * shape.size);
   cfg.blockDim = dim3(512);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = (size_t)cl_dyn_smem(std::max(0, std::min(kClMaxStages, a.stage_update)));
   cfg.stream = st;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
