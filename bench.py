@@ -240,6 +240,54 @@ def cpu_oracle_run(args, seed: int, steps: int, warmup: int, tet_budget: int):
                        f"{newton} Newton / {cg} CG iterations timed, {dt:.2f} s")}
 
 
+def reference_pcg_sample(args, seed: int):
+    """One Newton system solved three ways: env 0's first system of a step from rest (assembled by the CPU
+    oracle) by the reference's own compiled krylov::PCG on its BlockSparseMatrix<double,3> with
+    BlockJacobiPrec (oracle/_ref, built from the reference's sources; single-threaded, its serial
+    scheduler), by the oracle's PCG (all host threads), and by this library's sdx_pcg_solve through the
+    C-ABI (host arrays in and out, the matrix in the reference's row-strip layout). Jacobi, rel 1e-6.
+    None when oracle/_ref was not built."""
+    from oracle import oracle as O
+    if O.ref() is None:
+        return None
+    import ctypes as C
+    from project_superdex_b200 import capi
+    from project_superdex_b200.linear_solver import blocks_to_strips
+    (bodies, cfg), _ = build_workload(args.workload, seed)
+    b0 = bodies[0]
+    sc = O.Scene(b0, cfg)
+    u = np.zeros(3 * b0.n_nodes)
+    a = sc.assemble(u, u, t=cfg.dt, obj=False, psd=True)
+    rp, col, H, g = sc.row_ptr, sc.col, a["H"], a["g"]
+    strips = blocks_to_strips(rp, H)
+    out = {"system": f"env 0 of {args.workload} seed {seed}: first Newton system of a step from rest "
+                     f"({3 * b0.n_nodes} DoF, {int(rp[-1])} blocks), Jacobi, rel 1e-6"}
+    t0 = time.perf_counter()
+    _, it_ref, _, rel_ref, _ = O.ref_bsr3_pcg(rp, col, strips, g, rel_tol=1e-6, abs_tol=1e-9, precond=1)
+    out["reference_krylov_pcg"] = {"ms": 1e3 * (time.perf_counter() - t0), "iters": int(it_ref),
+                                   "rel_res": float(rel_ref), "threads": 1}
+    t0 = time.perf_counter()
+    _, st = O.pcg(rp, col, H, g, rel_tol=1e-6, abs_tol=1e-9)
+    out["oracle_pcg"] = {"ms": 1e3 * (time.perf_counter() - t0), "iters": int(st.num_iter),
+                         "threads": int(O.lib().or_num_threads())}
+    lp = capi.default_linear_params()
+    lp.rel_tol, lp.abs_tol = 1e-6, 1e-9
+    x = np.zeros_like(g)
+    sst = capi.LinearStatus()
+    rp64 = np.ascontiguousarray(rp, np.int64)
+    cl = np.ascontiguousarray(col, np.int32)
+    vals = np.ascontiguousarray(strips, np.float64)
+    args_c = (rp64.size - 1, cl.size, capi.ptr(rp64, capi._lp), capi.ptr(cl, capi._ip),
+              vals.ctypes.data_as(C.c_void_p), capi.SDX_F64, capi.ptr(np.ascontiguousarray(g)), capi.ptr(x),
+              capi.SDX_GUESS_ZERO, C.byref(lp), C.byref(sst))
+    capi.check(capi.lib().sdx_pcg_solve(*args_c))  # first call: device set-up
+    t0 = time.perf_counter()
+    capi.check(capi.lib().sdx_pcg_solve(*args_c))
+    out["sdx_pcg_solve"] = {"ms": 1e3 * (time.perf_counter() - t0), "iters": int(sst.num_iter),
+                            "note": "one call through the C-ABI: upload, FP32 conversion, solve, download"}
+    return out
+
+
 # ------------------------------------------------------------------------------------------------
 # training of the learned warm start (the learned part's own protocol)
 
@@ -604,6 +652,9 @@ def run_ours(args, rank, world, local_rank):
     }
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_oracle_run(args, seed0, steps=3, warmup=0, tet_budget=args.cpu_tets)
+        pcg_one = reference_pcg_sample(args, seed0)
+        if pcg_one:
+            line["cpu_baseline"]["one_linear_solve"] = pcg_one
     w.close()
     return line
 
