@@ -308,6 +308,10 @@ struct sdx_context {
   bool asm_tuned = false;
   int elem_threads = 128, elem_res_threads = 128, elem_agg = 0, contact_threads = 128;
   double tune_elem_us = 0.0, tune_elem_default_us = 0.0;  // best and default-shape Hessian assembly times
+  // CG iterations of each env's solve at Newton pass k of the last step (kHist x n_envs; 0: none yet), and
+  // the pass of the solve in progress (-1 outside a step): the cluster PCG's queue order
+  std::vector<int> h_pass_iters;
+  int cur_pass = -1;
   int* env_nrows = nullptr;    // padded rows per env (device)
   int* env_soff = nullptr;     // per env, its first slice (device, n_envs + 1): the cluster PCG's env ranges
   int* cl_envs = nullptr;      // the cluster PCG's env queue (device, n_envs)
@@ -948,9 +952,24 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
     const int64_t tail_rows = tr ? atoll(tr) : kClusterLatencyRows;
     const bool tail = n_list <= tail_envs && max_rows <= tail_rows;
     if (shape.n_clusters > 0 && n_list > 0 && max_rows <= kClusterMaxRows && (long_queue || tail)) {
-      std::stable_sort(list.begin(), list.end(), [&](int x, int y) {
-        return c->h_row_off[x + 1] - c->h_row_off[x] > c->h_row_off[y + 1] - c->h_row_off[y];
-      });
+      // Longest expected solve first: rows x the CG iterations the env took at this Newton pass of the last
+      // step (rows alone when there is no such count, or with SDX_PCG_LPT=0). The envs' stiffness differs,
+      // so their iteration counts do, and a queue ordered by rows alone starts some long solves late.
+      const char* lpt_env = getenv("SDX_PCG_LPT");
+      const bool lpt = !(lpt_env && atoi(lpt_env) == 0) && c->cur_pass >= 0 && c->cur_pass < sdx_context::kHist &&
+                       (int)c->h_pass_iters.size() == sdx_context::kHist * c->n_envs && n_envs == c->n_envs;
+      std::vector<double> cost(n_envs, 0.0);
+      for (int e : list) {
+        const double rows_e = (double)(c->h_row_off[e + 1] - c->h_row_off[e]);
+        const int it = lpt ? c->h_pass_iters[(size_t)c->cur_pass * c->n_envs + e] : 0;
+        cost[e] = rows_e * (it > 0 ? (double)it : 1.0);
+      }
+      bool all_known = lpt;
+      for (int e : list)
+        if (lpt && c->h_pass_iters[(size_t)c->cur_pass * c->n_envs + e] <= 0) all_known = false;
+      if (!all_known)
+        for (int e : list) cost[e] = (double)(c->h_row_off[e + 1] - c->h_row_off[e]);
+      std::stable_sort(list.begin(), list.end(), [&](int x, int y) { return cost[x] > cost[y]; });
       if (!c->env_soff) {
         std::vector<int> so(n_envs + 1);
         for (int e = 0; e <= n_envs; ++e) so[e] = (int)(c->h_row_off[e] / kSlice);
@@ -2756,6 +2775,7 @@ static int step_once(sdx_context* c) {
     if (p.ew_forcing == 2)
       SDX_CUDA(cudaMemcpyAsync(c->work.env_rel_tol, eta.data(), sizeof(double) * E, cudaMemcpyHostToDevice, c->stream));
     std::vector<int> it_out(E);
+    c->cur_pass = pass;
     if (c->ext_fn) {
       SDX_TRY(run_external(c, mask, p.linear, zero, it_out));
     } else {
@@ -2771,6 +2791,12 @@ static int step_once(sdx_context* c) {
     }
     for (int e = 0; e < E; ++e)
       if (mask[e]) cg[e] += it_out[e];
+    if (pass < sdx_context::kHist) {
+      if ((int)c->h_pass_iters.size() != sdx_context::kHist * E) c->h_pass_iters.assign((size_t)sdx_context::kHist * E, 0);
+      for (int e = 0; e < E; ++e)
+        if (mask[e]) c->h_pass_iters[(size_t)pass * E + e] = it_out[e];
+    }
+    c->cur_pass = -1;
     if (learned) SDX_TRY(mlp_check_error(c));
     if (collect) {
       SDX_CUDA(cudaMemsetAsync(c->env_norm, 0, sizeof(double) * E, c->stream));
