@@ -941,13 +941,30 @@ static int run_pcg(sdx_context* c, const Matrix& A, const int* diag_pos, int n_e
         list.push_back(e);
         max_rows = std::max<int64_t>(max_rows, c->h_row_off[e + 1] - c->h_row_off[e]);
       }
-    const ClusterShape shape =
+    ClusterShape shape =
         (ce && atoi(ce) == 0) ? ClusterShape{0, 0, 0} : pcg_cluster_shape((int)list.size(), c->cl_size);
     const char* qf = getenv("SDX_PCG_CLUSTER_QUEUE");
     const char* tl = getenv("SDX_PCG_CLUSTER_TAIL");
     const int queue_factor = qf ? atoi(qf) : kClusterQueueFactor, tail_envs = tl ? atoi(tl) : kClusterTailEnvs;
     const int n_list = (int)list.size();
-    const bool long_queue = queue_factor > 0 && c->cl_size >= 0 && n_list >= queue_factor * shape.n_clusters;
+    bool long_queue = queue_factor > 0 && c->cl_size >= 0 && n_list >= queue_factor * shape.n_clusters;
+    // A queue too short for the batch's cluster size may still keep larger clusters busy: the most clusters
+    // (of 4, 8 or 16 CTAs) that get queue_factor envs each. On the 1,024-body batch's later Newton passes
+    // (a few hundred envs left) this moved the solves off the grid kernel's lockstep: 178.2 -> 186.1
+    // env-steps/s on the zero-start arm over 10 steps (SDX_PCG_CLUSTER_MEDIUM=0 turns it off).
+    const char* med = getenv("SDX_PCG_CLUSTER_MEDIUM");
+    const bool medium = !(med && atoi(med) == 0);
+    if (!long_queue && shape.n_clusters > 0 && medium && queue_factor > 0 && c->cl_size >= 0) {
+      for (int cs : {4, 8, 16}) {
+        if (cs <= shape.size) continue;
+        const ClusterShape sh = pcg_cluster_shape(n_list, cs);
+        if (sh.size == cs && sh.n_clusters > 0 && n_list >= queue_factor * sh.n_clusters) {
+          shape = sh;
+          long_queue = true;
+          break;
+        }
+      }
+    }
     const char* tr = getenv("SDX_PCG_CLUSTER_TAIL_ROWS");
     const int64_t tail_rows = tr ? atoll(tr) : kClusterLatencyRows;
     const bool tail = n_list <= tail_envs && max_rows <= tail_rows;
