@@ -197,6 +197,7 @@ struct StepGraph {
   char* block = nullptr;   // one allocation: the Newton state arrays, the control words and the step time
   NewtonDev d;
   double* t_dev = nullptr;
+  int* queue = nullptr;    // every env, largest first: the cluster PCG's queue in the graph
   int64_t k_pro = 0, k_pass = 0, k_ls = 0;  // kernel launches recorded per prologue+epilogue, pass and trial
   void release() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -204,6 +205,7 @@ struct StepGraph {
     exec = nullptr;
     graph = nullptr;
     dfree(block);
+    dfree(queue);
     t_dev = nullptr;
   }
 };
@@ -2905,9 +2907,10 @@ static int step_once(sdx_context* c) {
 // The step time comes from a device word written before each launch; everything else the kernels read
 // was fixed at capture, so the graph is rebuilt when the parameters or the topology change.
 
-// Appends a conditional while-node after the work captured so far on the stream and makes it the capture's
-// only dependency; returns its body graph.
-static int capture_while(sdx_context* c, cudaGraphConditionalHandle h, cudaGraph_t* body) {
+// Appends a conditional node (while, or a switch over n bodies) after the work captured so far on the stream
+// and makes it the capture's only dependency; returns its body graphs.
+static int capture_conditional(sdx_context* c, cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                               int n, cudaGraph_t* bodies) {
   cudaStreamCaptureStatus cs;
   cudaGraph_t g;
   const cudaGraphNode_t* deps = nullptr;
@@ -2917,13 +2920,17 @@ static int capture_while(sdx_context* c, cudaGraphConditionalHandle h, cudaGraph
   cudaGraphNodeParams np = {};
   np.type = cudaGraphNodeTypeConditional;
   np.conditional.handle = h;
-  np.conditional.type = cudaGraphCondTypeWhile;
-  np.conditional.size = 1;
+  np.conditional.type = type;
+  np.conditional.size = (unsigned)n;
   cudaGraphNode_t node;
   SDX_CUDA(cudaGraphAddNode(&node, g, deps, nd, &np));
-  *body = np.conditional.phGraph_out[0];
+  for (int i = 0; i < n; ++i) bodies[i] = np.conditional.phGraph_out[i];
   SDX_CUDA(cudaStreamUpdateCaptureDependencies(c->stream, &node, 1, cudaStreamSetCaptureDependencies));
   return SDX_OK;
+}
+
+static int capture_while(sdx_context* c, cudaGraphConditionalHandle h, cudaGraph_t* body) {
+  return capture_conditional(c, h, cudaGraphCondTypeWhile, 1, body);
 }
 
 static int build_step_graph(sdx_context* c) {
@@ -3003,11 +3010,57 @@ static int build_step_graph(sdx_context* c) {
   a.resume = 0;
   a.env_nrows = c->env_nrows;
   a.spin_limit = device_spin_limit();
+  // The PCG kernel of each pass, chosen on the device from the envs in it: the cluster kernel at the batch's
+  // cluster size while at least kClusterQueueFactor envs per co-resident cluster iterate, then larger
+  // clusters (4, 8, 16 CTAs) that still get that many, the largest clusters for the rest. The clusters take
+  // envs from one queue of every env, largest first, passing over those outside the pass. Batches too small
+  // for any cluster shape (and single envs) take the grid kernel.
+  std::vector<ClusterShape> shapes;
+  {
+    int64_t max_rows = 0;
+    for (int e = 0; e < E; ++e) max_rows = std::max<int64_t>(max_rows, c->h_row_off[e + 1] - c->h_row_off[e]);
+    const char* ce = getenv("SDX_PCG_CLUSTER");
+    if (E > 1 && max_rows <= kClusterMaxRows && !(ce && atoi(ce) == 0) && c->cl_size >= 0) {
+      const ClusterShape sh = pcg_cluster_shape(E, c->cl_size);
+      if (sh.n_clusters > 0) shapes.push_back(sh);
+      for (int cs : {4, 8, 16}) {
+        if (shapes.empty() || cs <= shapes[0].size) continue;
+        const ClusterShape s2 = pcg_cluster_shape(E, cs);
+        if (s2.size == cs && s2.n_clusters > 0) shapes.push_back(s2);
+      }
+    }
+  }
+  d.n_branch = shapes.empty() ? 0 : (int)shapes.size() + 1;
+  for (int k = 0; k < 4; ++k) d.min_envs[k] = k < (int)shapes.size() ? kClusterQueueFactor * shapes[k].n_clusters : 0;
+  // The last passes, with few envs left, also stay on the largest clusters: the graph's grid kernel runs
+  // over the upload's partition of every env (no re-partitioning onto the envs still iterating), which
+  // measured 0.48x the host-driven step on the 1,024-body batch when those passes took it.
+  if (!shapes.empty()) d.min_envs[shapes.size() - 1] = 1;
+  PcgArgs ac = a;  // the cluster kernel's launch
+  if (!shapes.empty()) {
+    if (!c->env_soff) {
+      std::vector<int> so(E + 1);
+      for (int e = 0; e <= E; ++e) so[e] = (int)(c->h_row_off[e] / kSlice);
+      SDX_TRY(upload(&c->env_soff, so));
+      SDX_TRY(dalloc(&c->cl_envs, E));
+    }
+    std::vector<int> q(E);
+    for (int e = 0; e < E; ++e) q[e] = e;
+    std::stable_sort(q.begin(), q.end(), [&](int x, int y) {
+      return c->h_row_off[x + 1] - c->h_row_off[x] > c->h_row_off[y + 1] - c->h_row_off[y];
+    });
+    SDX_TRY(upload(&G.queue, q));
+    ac.cl_envs = G.queue;
+    ac.cl_n = E;
+    ac.env_soff = c->env_soff;
+    ac.cl_skip_masked = 1;
+    ac.spin_limit = kSpinLimit;  // the cluster kernel keeps the default bound, as in run_pcg
+  }
   const double t_cap = c->time + p.dt;  // contact launches read the real time from G.t_dev
   const bool prof = c->profiling;
   c->profiling = false;  // no event records inside the graph
-  cudaGraphConditionalHandle h_loop, h_ls;
-  cudaGraph_t body = nullptr, ls_body = nullptr;
+  cudaGraphConditionalHandle h_loop, h_ls, h_pick = 0;
+  cudaGraph_t body = nullptr, ls_body = nullptr, pick_body[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   int rc = SDX_OK;
   auto fail = [&](int code) {
     cudaGraph_t dummy = nullptr;
@@ -3048,6 +3101,8 @@ static int build_step_graph(sdx_context* c) {
   // one Newton pass
   if (cudaGraphConditionalHandleCreate(&h_ls, body, 0, 0) != cudaSuccess)
     return fail(set_error(SDX_ERR_CUDA, "step graph: line-search handle"));
+  if (d.n_branch > 0 && cudaGraphConditionalHandleCreate(&h_pick, body, 0, 0) != cudaSuccess)
+    return fail(set_error(SDX_ERR_CUDA, "step graph: PCG switch handle"));
   const int64_t l1 = c->launches;
   if (cudaStreamBeginCaptureToGraph(c->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
       cudaSuccess)
@@ -3056,11 +3111,16 @@ static int build_step_graph(sdx_context* c) {
     launch_nt_temporal(d, c->n_slices, c->slice_env, sdx_context::kHist, c->dx_hist, c->dx, c->stream);
     c->launches++;
   }
-  launch_nt_pcg_prepare(d, c->stream);
-  cudaError_t le = launch_pcg_captured(a, P.n_cta, P.threads, c->stream);
-  c->launches += 2;
-  if (le != cudaSuccess)
-    return fail(set_error(SDX_ERR_CUDA, "step graph: PCG launch: %s", cudaGetErrorString(le)));
+  launch_nt_pcg_prepare(d, h_pick, c->stream);
+  c->launches += 2;  // the prepare kernel and the pass's one PCG launch
+  if (d.n_branch == 0) {
+    const cudaError_t le = launch_pcg_captured(a, P.n_cta, P.threads, c->stream);
+    if (le != cudaSuccess)
+      return fail(set_error(SDX_ERR_CUDA, "step graph: PCG launch: %s", cudaGetErrorString(le)));
+  } else {
+    rc = capture_conditional(c, h_pick, cudaGraphCondTypeSwitch, d.n_branch, pick_body);
+    if (rc != SDX_OK) return fail(rc);
+  }
   if (temporal) {
     launch_nt_keep_hist(d, c->n_slices, c->slice_env, sdx_context::kHist, c->dx, c->dx_hist, c->stream);
     c->launches++;
@@ -3101,6 +3161,19 @@ static int build_step_graph(sdx_context* c) {
     return fail(set_error(SDX_ERR_CUDA, "step graph: line-search capture: %s",
                           cudaGetErrorString(cudaGetLastError())));
   G.k_ls = c->launches - l2;
+  // the PCG kernel of each switch branch: the cluster shapes in order, then the grid kernel
+  for (int b = 0; b < d.n_branch; ++b) {
+    if (cudaStreamBeginCaptureToGraph(c->stream, pick_body[b], nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
+        cudaSuccess)
+      return fail(set_error(SDX_ERR_CUDA, "step graph: begin PCG branch capture"));
+    const cudaError_t le = b + 1 < d.n_branch ? launch_pcg_cluster(ac, shapes[b], c->stream)
+                                              : launch_pcg_captured(a, P.n_cta, P.threads, c->stream);
+    if (le != cudaSuccess)
+      return fail(set_error(SDX_ERR_CUDA, "step graph: PCG branch launch: %s", cudaGetErrorString(le)));
+    if (cudaStreamEndCapture(c->stream, &got) != cudaSuccess || got != pick_body[b])
+      return fail(set_error(SDX_ERR_CUDA, "step graph: PCG branch capture: %s",
+                            cudaGetErrorString(cudaGetLastError())));
+  }
   c->launches = l0;  // counted per executed launch in step_graph
   c->profiling = prof;
   const cudaError_t ie = cudaGraphInstantiate(&G.exec, G.graph, 0);

@@ -199,6 +199,7 @@ struct PcgArgs {
   const int* cl_envs;
   int cl_n;
   const int* env_soff;
+  int cl_skip_masked;  // the queue holds every env: skip those whose env_mask byte is 0
 };
 
 // Device-resident Newton state of a step run as one CUDA graph (the Newton loop and the line search as
@@ -228,6 +229,10 @@ struct NewtonDev {
   unsigned* pcg_sync;     // the PCG's control words (reset before each solve; [2] its error word)
   int* pcg_conv;
   const int* env_nrows;   // rows per env
+  // PCG kernel choice per pass (a switch node): branch b is taken for the first b whose threshold the envs of
+  // the pass reach (min_envs[b] > 0), else the last branch (the grid kernel); 0 when there is no choice
+  int n_branch;
+  int min_envs[4];
 };
 
 // Newton stop-test constants (NonLinearSolverParams)
@@ -240,7 +245,7 @@ cudaError_t launch_pcg_captured(const PcgArgs& a, int n_cta, int threads, cudaSt
 void launch_nt_begin(const NewtonDev& d, const NewtonConsts& k, cudaStream_t st);
 void launch_nt_control(const NewtonDev& d, const NewtonConsts& k, cudaGraphConditionalHandle loop,
                        cudaStream_t st);
-void launch_nt_pcg_prepare(const NewtonDev& d, cudaStream_t st);
+void launch_nt_pcg_prepare(const NewtonDev& d, cudaGraphConditionalHandle pick, cudaStream_t st);
 void launch_nt_temporal(const NewtonDev& d, int n_slices, const int* slice_env, int hist_len, const double* hist,
                         double* dx, cudaStream_t st);
 void launch_nt_keep_hist(const NewtonDev& d, int n_slices, const int* slice_env, int hist_len, const double* dx,

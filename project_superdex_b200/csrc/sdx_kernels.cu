@@ -1982,7 +1982,11 @@ __global__ void __launch_bounds__(512, 1) k_pcg_cluster(PcgArgs a) {
   for (;;) {
     // ---- next env from the queue (CTA 0 takes it, every CTA reads it from CTA 0) ----
     if (rank == 0 && threadIdx.x == 0) {
-      const int h = (int)atomicAdd(a.sync + 1, 1u);
+      int h = (int)atomicAdd(a.sync + 1, 1u);
+      // a queue of every env of the batch (built once for a graph-captured step) passes over the envs
+      // outside this solve; at most cl_n takes in all
+      if (a.cl_skip_masked && a.env_mask)
+        while (h < a.cl_n && !a.env_mask[a.cl_envs[h]]) h = (int)atomicAdd(a.sync + 1, 1u);
       s_env = h < a.cl_n ? a.cl_envs[h] : -1;
     }
     if (!cluster_sync(cnt, csize, a.spin_limit, err, &s_ok)) break;

@@ -111,8 +111,10 @@ __global__ void __launch_bounds__(kNtThreads) k_nt_control(NewtonDev d, NewtonCo
   }
 }
 
-// The PCG's control words and outputs before a solve of the pass's envs (what run_pcg writes from the host).
-__global__ void __launch_bounds__(kNtThreads) k_nt_pcg_prepare(NewtonDev d) {
+// The PCG's control words and outputs before a solve of the pass's envs (what run_pcg writes from the host),
+// and the PCG kernel for the pass (the host loop's routing: the cluster kernel while the queue keeps its
+// clusters busy, the grid kernel for short queues).
+__global__ void __launch_bounds__(kNtThreads) k_nt_pcg_prepare(NewtonDev d, cudaGraphConditionalHandle pick) {
   __shared__ unsigned long long s_rows;
   if (threadIdx.x == 0) s_rows = 0ull;
   __syncthreads();
@@ -133,6 +135,12 @@ __global__ void __launch_bounds__(kNtThreads) k_nt_pcg_prepare(NewtonDev d) {
     d.pcg_sync[5] = (unsigned)s_rows;
     d.pcg_sync[6] = 0u;
     d.pcg_sync[7] = 0u;
+    if (d.n_branch > 0) {
+      int b = d.n_branch - 1;
+      for (int k = d.n_branch - 2; k >= 0; --k)
+        if (d.min_envs[k] > 0 && d.ctl[0] >= d.min_envs[k]) b = k;
+      cudaGraphSetConditional(pick, (unsigned)b);
+    }
   }
 }
 
@@ -228,8 +236,8 @@ void launch_nt_control(const NewtonDev& d, const NewtonConsts& k, cudaGraphCondi
   k_nt_control<<<1, kNtThreads, 0, st>>>(d, k, loop);
 }
 
-void launch_nt_pcg_prepare(const NewtonDev& d, cudaStream_t st) {
-  k_nt_pcg_prepare<<<1, kNtThreads, 0, st>>>(d);
+void launch_nt_pcg_prepare(const NewtonDev& d, cudaGraphConditionalHandle pick, cudaStream_t st) {
+  k_nt_pcg_prepare<<<1, kNtThreads, 0, st>>>(d, pick);
 }
 
 void launch_nt_temporal(const NewtonDev& d, int n_slices, const int* slice_env, int hist_len, const double* hist,

@@ -115,3 +115,23 @@ def test_graph_step_refuses_the_learned_start():
     with pytest.raises(capi.SdxError):
         w.step(1)
     w.close()
+
+
+def test_graph_steps_route_a_batch_to_the_cluster_kernel(monkeypatch):
+    """40 small uneven contact bodies: the graph's switch node takes the cluster kernel (9 clusters of 16 CTAs;
+    the clusters pass over the envs outside a pass in one queue of every env). The host-driven step takes it
+    for the first Newton pass and re-partitions the later, shorter solves on the grid kernel: states within
+    1e-6 of the body size, CG counts within max(6, 10 %)."""
+    monkeypatch.delenv("SDX_PCG_REPART", raising=False)
+    bodies, cfg = scenes.config2(7, n_envs=40, lo=8, hi=14)
+    host, _ = _steps(bodies, cfg, 2, set(), warm_start=3, newton_max_iter=12, newton_abs_tol=1e-9)
+    graph, _ = _steps(bodies, cfg, 2, {0, 1}, warm_start=3, newton_max_iter=12, newton_abs_tol=1e-9)
+    for (ua, _, ta, sa), (ub, _, tb, sb) in zip(host, graph):
+        off = 0
+        for e, bd in enumerate(bodies):
+            size = np.ptp(bd.X, axis=0).max()
+            assert np.abs(ua[off:off + 3 * bd.n_nodes] - ub[off:off + 3 * bd.n_nodes]).max() <= 1e-6 * size
+            off += 3 * bd.n_nodes
+        for x, y in zip(sa, sb):
+            assert x["convergence"] == y["convergence"] and abs(x["newton_iters"] - y["newton_iters"]) <= 1
+            assert abs(x["cg_iters"] - y["cg_iters"]) <= max(6, 0.1 * x["cg_iters"]), (x["cg_iters"], y["cg_iters"])
