@@ -95,7 +95,8 @@ def test_refinement_rejects_bad_parameters(oracle):
 
 @pytest.mark.parametrize("warm", [0, 1])
 def test_refined_newton_steps_match_oracle(oracle, warm):
-    """Zero and temporal starts, a single body and a batch of three uneven bodies with contact."""
+    """Zero and previous-solve starts (SDX_WARM_ZERO, SDX_WARM_PREVIOUS), a single body and a batch of three
+    uneven bodies with contact."""
     import test_gpu_step as ts
 
     def check(bodies, ug, states, hist):
