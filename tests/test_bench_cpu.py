@@ -62,3 +62,40 @@ def test_cpu_sample_is_bounded(monkeypatch):
     assert idx == list(range(len(idx))) and len(idx) >= 1
     assert sum(bodies[i].n_tets for i in idx) <= 400000 or len(idx) == 1
     assert bench.sample_envs(bodies, 1) == [0]
+
+
+def test_pcg_time_split_by_kernel_and_shape_keys():
+    """The bench line's PCG split: the cluster kernel's share of the time and bytes, the grid kernel the rest;
+    launch-shape entries of the profile are kept, not summed, across merged runs."""
+    prof = {"pcg_ms": 1000.0, "pcg_bytes": 4.0e12, "pcg_cluster_ms": 800.0, "pcg_cluster_bytes": 3.6e12}
+    sp = bench.pcg_split(prof)
+    assert sp["cluster"]["ms"] == 800.0 and abs(sp["cluster"]["gbs"] - 4500.0) < 1e-9
+    assert sp["grid"]["ms"] == 200.0 and abs(sp["grid"]["gbs"] - 2000.0) < 1e-9
+    assert bench.pcg_split({"pcg_ms": 0.0, "pcg_bytes": 0.0})["grid"]["gbs"] is None
+    a = _run(160, 10, 1000.0, 3000, 500, 1965.0, [], 150)
+    b = _run(160, 10, 3000.0, 5000, 700, 1900.0, [], 160)
+    for r in (a, b):
+        r["prof"].update(elem_threads=64, tune_elem_us=19.5, pcg_cluster_ms=100.0)
+    m = bench.merge(a, b)
+    assert m["prof"]["elem_threads"] == 64 and m["prof"]["tune_elem_us"] == 19.5
+    assert m["prof"]["pcg_cluster_ms"] == 200.0
+
+
+def test_refined_arm_names_set_the_start_and_the_refinement():
+    """`<arm>_refined` selects the same warm start with mixed-precision iterative refinement (inner relative
+    tolerance bench.REFINE_INNER_REL_TOL); the plain names turn refinement off."""
+    from project_superdex_b200 import capi
+
+    class FakeWorld:
+        def __init__(self):
+            self.calls = []
+
+        def set_params(self, **kw):
+            self.calls.append(kw)
+
+    w = FakeWorld()
+    for arm in ("fused_zero_refined", "temporal_refined", "temporal", "fused_zero"):
+        bench.set_arm(w, arm, None)
+    want = [(capi.SDX_WARM_ZERO, bench.REFINE_INNER_REL_TOL), (capi.SDX_WARM_TEMPORAL, bench.REFINE_INNER_REL_TOL),
+            (capi.SDX_WARM_TEMPORAL, 0.0), (capi.SDX_WARM_ZERO, 0.0)]
+    assert [(c["warm_start"], c["linear_refine_inner_rel_tol"]) for c in w.calls] == want
