@@ -53,6 +53,10 @@ def test_defaults_mirror_reference_defaults():
     assert p.psd_strategy == capi.SDX_PSD_PROJECTION if hasattr(capi, "SDX_PSD_PROJECTION") else p.psd_strategy == 1
     lp = capi.default_linear_params()
     assert lp.abs_tol == 1e-9 and lp.rel_div_tol == 1e10 and lp.polak_ribiere == 1 and lp.preconditioner == 1
+    # the options with no counterpart in the reference are off by default: a plain unrestarted PCG and a
+    # host-driven Newton loop, as the reference runs them
+    assert lp.refine_inner_rel_tol == 0.0 and lp.refine_max_passes == 8
+    assert p.newton_graph == 0 and p.linear.refine_inner_rel_tol == 0.0 and p.warm_start == capi.SDX_WARM_ZERO
 
 
 def test_no_gpu_is_reported_not_faked():
