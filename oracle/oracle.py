@@ -128,6 +128,8 @@ def lib():
         L.or_pcg.argtypes = [C.c_int, _lp, _ip, _dp, _dp, _dp, C.POINTER(OrPcgParams)]
         L.or_pcg.restype = OrPcgStatus
         L.or_bsr_apply.argtypes = [C.c_int, _lp, _ip, _dp, _dp, _dp]
+        L.or_stop_status.argtypes = [C.c_double] * 5
+        L.or_stop_status.restype = C.c_int
         L.or_step.argtypes = [C.POINTER(OrScene), _dp, _dp, C.c_double, C.POINTER(OrNewtonParams), _dp]
         L.or_step.restype = OrNewtonStatus
         L.or_default_newton_params.argtypes = [C.POINTER(OrNewtonParams)]
@@ -468,6 +470,11 @@ def pcg(row_ptr, col, H, b, x=None, rel_tol=1e-6, abs_tol=1e-9, rel_div_tol=1e10
                       ptr(np.ascontiguousarray(col, np.int32), _ip), ptr(Hc), ptr(b), ptr(x),
                       C.byref(p))
     return x, st
+
+
+def stop_status(rr, bb, rel_tol, abs_tol, rel_div_tol):
+    """or_stop_status: 0 active, 1 converged (relative), 2 converged (absolute), 3 diverged."""
+    return int(lib().or_stop_status(float(rr), float(bb), float(rel_tol), float(abs_tol), float(rel_div_tol)))
 
 
 def bsr_to_dense(row_ptr, col, H):

@@ -1201,6 +1201,15 @@ static void prec_apply(int n, int kind, const double* P, const double* r, double
   }
 }
 
+int or_stop_status(double rr, double bb, double rel_tol, double abs_tol, double rel_div_tol) {
+  const double div = (bb * rel_div_tol) * rel_div_tol;
+  const double conv = fmax(abs_tol * abs_tol, (bb * rel_tol) * rel_tol);
+  if (!isfinite(rr) || rr > div || rr < -conv) return 3;
+  if (rr < 0.0) rr = 0.0;
+  if (rr <= conv) return rr <= abs_tol * abs_tol ? 2 : 1;
+  return 0;
+}
+
 or_pcg_status or_pcg(int n, const int64_t* row_ptr, const int32_t* col, const double* H,
                      const double* b, double* x, const or_pcg_params* prm) {
   const int64_t m = 3 * (int64_t)n;
@@ -1214,27 +1223,22 @@ or_pcg_status or_pcg(int n, const int64_t* row_ptr, const int32_t* col, const do
   memcpy(r, b, sizeof(double) * (size_t)m);
   /* StatusResidualL2::SetScaling: scale = |b|^2 (stopping_criterion.h:140-144, 92-98). */
   const double bb = dotv(m, b, b);
-  const double conv = fmax(prm->abs_tol * prm->abs_tol, (bb * prm->rel_tol) * prm->rel_tol);
-  const double div = (bb * prm->rel_div_tol) * prm->rel_div_tol;
+  /* thresholds: or_stop_status */
   if (!prm->zero_guess) {
     or_bsr_apply(n, row_ptr, col, H, x, q);
     for (int64_t i = 0; i < m; ++i) r[i] -= q[i];
   }
   double rr = dotv(m, r, r);
-#define OR_CHECK(it_)                                                  \
-  do {                                                                 \
-    st.res_norm = sqrt(rr < 0 ? 0 : rr);                               \
-    st.rel_res_norm = bb == 0.0 ? 0.0 : sqrt((rr < 0 ? 0 : rr) / bb);  \
-    if (!isfinite(rr) || rr > div) {                                   \
-      st.num_iter = (it_);                                             \
-      st.convergence = 3;                                              \
-      goto done;                                                       \
-    }                                                                  \
-    if (rr <= conv) {                                                  \
-      st.num_iter = (it_);                                             \
-      st.convergence = 1;                                              \
-      goto done;                                                       \
-    }                                                                  \
+#define OR_CHECK(it_)                                                                      \
+  do {                                                                                     \
+    st.res_norm = sqrt(rr < 0 ? 0 : rr);                                                   \
+    st.rel_res_norm = bb == 0.0 ? 0.0 : sqrt((rr < 0 ? 0 : rr) / bb);                      \
+    const int cls_ = or_stop_status(rr, bb, prm->rel_tol, prm->abs_tol, prm->rel_div_tol); \
+    if (cls_ != 0) {                                                                       \
+      st.num_iter = (it_);                                                                 \
+      st.convergence = cls_ == 3 ? 3 : 1;                                                  \
+      goto done;                                                                           \
+    }                                                                                      \
   } while (0)
   OR_CHECK(0);
   prec_apply(n, prm->precond, P, r, z);

@@ -213,6 +213,11 @@ typedef struct {
   int convergence;    /* 0 none, 1 converged, 2 stopped, 3 diverged (LinearSolverConvergenceStatus) */
 } or_pcg_status;
 
+/* StopTest::CheckStatus with SetScaling(bb) (stopping_criterion.h:65-78, 92-98): the classification of a
+ * squared residual norm rr: 0 active, 1 converged (relative), 2 converged (absolute), 3 diverged. A negative
+ * rr within the convergence threshold is round-off and counts as 0; a more negative one diverges. */
+int or_stop_status(double rr, double bb, double rel_tol, double abs_tol, double rel_div_tol);
+
 /* Left-preconditioned CG with the residual-L2 stop test.
  * mochi_core/.../linear_algebra/krylov/pcg.h:70-238, stopping_criterion.h:31-166. */
 or_pcg_status or_pcg(int n_rows_blk, const int64_t* row_ptr, const int32_t* col, const double* H,

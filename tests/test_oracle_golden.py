@@ -139,6 +139,24 @@ def test_pcg_stop_and_divergence_statuses(oracle):
     assert st.convergence == 1 and st.num_iter == 0  # b = 0: converged at iteration 0
 
 
+def test_stop_test_classification_known_answers(oracle):
+    """The reference's StopTest known answers (mochi_core/test/stopping_criterion_test.cpp:24-39, 41-46):
+    relTol 1e-3, absTol 1e-6, relDivTol 10, scaling 1, by squared residual norm. 0 active, 1 converged
+    (relative), 2 converged (absolute), 3 diverged."""
+    eps = np.finfo(np.float64).eps
+
+    def cls(rr):
+        return oracle.stop_status(rr, 1.0, 1e-3, 1e-6, 10.0)
+
+    assert cls(-1.0) == 3                    # negative beyond round-off: DivergedRes
+    assert cls(-eps) == 2                    # round-off below zero counts as 0: ConvergedAtol
+    assert cls(1e-14) == 2                   # ConvergedAtol
+    assert cls(1e-8) == 1                    # ConvergedRtol
+    assert cls(1e-3) == 0                    # Active
+    assert cls(101.0) == 3                   # DivergedRes
+    assert cls(float("nan")) == 3 and cls(float("inf")) == 3
+
+
 def test_stiffness_damping_matches_reference_code(oracle, golden):
     """The oracle's viscous-stress damping against fem::StressDampingWork compiled from the reference."""
     import ctypes as C
