@@ -241,3 +241,65 @@ def test_fp32_mode_fixture_matches_this_oracle(oracle, golden):
     assert np.abs(u).sum() == pytest.approx(fx["hessian"]["u_abs_sum"], rel=1e-9)
     assert fx["hessian"]["oracle_vs_fp64_mode_rel_fro"] < 1e-6
     assert fx["pcg"]["convergence_fp32_mode"] == fx["pcg"]["convergence_fp64_mode"] == 1
+
+
+def test_gravity_work_analytic_properties(oracle):
+    """The reference's gravity known answers (mochi_core/test/fem_gravity_test.cpp:96-170, the analytic
+    check) on the oracle's assembled system: with a non-axis-aligned gravity g, the gravity part of the
+    residual (assembly with g minus assembly with g = 0 at the same state) is -rho vol/4 g at each of a tet's
+    nodes, summed over the tets (zero on pinned DoFs), independent of the displacement; and its energy obeys
+    E(u) - E(0) = <r, u>."""
+    from project_superdex_b200 import scenes
+    rng = np.random.default_rng(3)
+    b = scenes.grid_body(4, 3, 3, 0.01, rng=rng, rho=1234.5)
+    g = (0.31, -9.81, 1.73)
+    cfg_g, cfg_0 = scenes.SceneConfig(gravity=g), scenes.SceneConfig(gravity=(0.0, 0.0, 0.0))
+    free = (b.pin == 0).repeat(3)
+    X, T = b.X, b.tets
+    vol = np.abs(np.einsum("ij,ij->i", np.cross(X[T[:, 1]] - X[T[:, 0]], X[T[:, 2]] - X[T[:, 0]]),
+                           X[T[:, 3]] - X[T[:, 0]])) / 6.0
+    want = np.zeros((b.n_nodes, 3))
+    for k in range(4):
+        np.add.at(want, T[:, k], -(b.rho * vol / 4.0)[:, None] * np.asarray(g)[None, :])
+    want = want.reshape(-1) * free
+    parts = []
+    for u in (np.zeros(3 * b.n_nodes), rng.normal(0, 1e-3, 3 * b.n_nodes) * free):
+        ag = oracle.Scene(b, cfg_g).assemble(u, u, hess=False)
+        a0 = oracle.Scene(b, cfg_0).assemble(u, u, hess=False)
+        parts.append((ag["obj"] - a0["obj"], ag["g"] - a0["g"], u))
+    for _, r, _ in parts:
+        np.testing.assert_allclose(r, want, rtol=1e-12, atol=1e-12 * np.abs(want).max())
+    (e0, _, _), (e1, r1, u1) = parts
+    assert e1 - e0 == pytest.approx(float(r1 @ u1), rel=1e-9)
+
+
+def test_inertia_work_matches_the_consistent_mass_matrix(oracle):
+    """The reference's inertia identities (mochi_core/test/fem_inertia_test.cpp:30-37) on the oracle's
+    assembly: with a = u - ut and M the P1 consistent mass matrix (rho vol / 20 (1 + delta_fg) per node
+    pair, assembled here independently of the oracle), the inertia part of the residual is M a / dt^2 and of
+    the energy a^T M a / (2 dt^2); the elastic part cancels between two assemblies at the same u."""
+    from project_superdex_b200 import scenes
+    rng = np.random.default_rng(5)
+    b = scenes.grid_body(3, 3, 2, 0.01, rng=rng, rho=870.0, pin_bottom=False)
+    cfg = scenes.SceneConfig(gravity=(0.0, 0.0, 0.0))
+    X, T = b.X, b.tets
+    vol = np.abs(np.einsum("ij,ij->i", np.cross(X[T[:, 1]] - X[T[:, 0]], X[T[:, 2]] - X[T[:, 0]]),
+                           X[T[:, 3]] - X[T[:, 0]])) / 6.0
+    M = np.zeros((b.n_nodes, b.n_nodes))
+    for t in range(b.n_tets):
+        m = b.rho[t] * vol[t] / 20.0
+        for f in range(4):
+            for g in range(4):
+                M[T[t, f], T[t, g]] += m * (2.0 if f == g else 1.0)
+    u = rng.normal(0, 1e-3, 3 * b.n_nodes)
+    ut = u - rng.normal(0, 1e-3, 3 * b.n_nodes)
+    s = oracle.Scene(b, cfg)
+    a_in = s.assemble(u, ut, hess=False)
+    a_el = s.assemble(u, u, hess=False)
+    inv_dt2 = 1.0 / cfg.dt ** 2
+    a = (u - ut).reshape(-1, 3)
+    want_r = inv_dt2 * (M @ a).reshape(-1)
+    np.testing.assert_allclose(a_in["g"] - a_el["g"], want_r, rtol=1e-10, atol=1e-10 * np.abs(want_r).max())
+    want_e = 0.5 * inv_dt2 * float(np.sum(a * (M @ a)))
+    assert a_in["obj"] - a_el["obj"] == pytest.approx(want_e, rel=1e-9)
+    assert M.sum() == pytest.approx(float(np.sum(b.rho * vol)), rel=1e-12)  # total mass
